@@ -1,0 +1,221 @@
+/*
+ * setsm_vll.h -- C ABI of the B200 vertical-line-locus matcher.
+ *
+ * This is the drop-in boundary for SETSM's matching hot path:
+ *   int VerticalLineLocus(VOXEL **grid_voxel, const ProInfo *proinfo,
+ *                         NCCresult *nccresult, LevelInfo &plevelinfo,
+ *                         const UGRID *GridPT3, const uint8 iteration,
+ *                         const double *minmaxHeight);
+ * declared at setsm_code.hpp:81 and defined at setsm_code.cpp:6049-6548 of the
+ * reference.  That symbol is C++ (it takes a reference), so the library ships
+ * a C++ shim with the same mangled signature (setsm_vll_compat.hpp) on top of
+ * the plain-C entry points below.  Everything here takes plain pointers and
+ * sizes; all status codes are negative on failure and the library never
+ * exits the process (the reference calls exit(1) on allocation failure,
+ * setsm_code.cpp:6571-6584).
+ *
+ * Record layouts (vll_nccresult, vll_ugrid, vll_voxel, vll_transparam) are
+ * byte-identical to the reference's NCCresult, UGRID, VOXEL and TransParam
+ * (Typedefine.hpp:248-293, Typedefine.hpp:214-230) so host arrays produced by
+ * the reference's callers are passed through without repacking.
+ */
+#ifndef SETSM_VLL_H
+#define SETSM_VLL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VLL_ABI_VERSION 1
+#define VLL_MAX_IMAGES 8
+
+/* ---- status codes ------------------------------------------------------ */
+enum vll_status {
+    VLL_OK = 0,
+    VLL_ERR_INVALID = -1,      /* bad argument or inconsistent descriptor   */
+    VLL_ERR_UNSUPPORTED = -2,  /* e.g. frame (AB) sensor, too many images   */
+    VLL_ERR_CUDA = -3,         /* CUDA runtime error; see vll_last_error()  */
+    VLL_ERR_NOMEM = -4,        /* device or pinned-host allocation failed   */
+    VLL_ERR_TIMEOUT = -5,      /* persistent kernel hit its bounded wait    */
+    VLL_ERR_CAPACITY = -6      /* caller buffer too small                   */
+};
+
+/* ---- kernels ----------------------------------------------------------- */
+enum vll_kernel {
+    /* One grid node per thread, FP64 everywhere, operation order of the
+     * reference; bit-exact with VerticalLineLocus on the same inputs. */
+    VLL_KERNEL_FP64_PLAIN = 0,
+    /* FP64 RPC, FP32 tile-relative sampling and mean-centred NCC sums,
+     * persistent (node, height-chunk) work queue, in-kernel FP64 re-check of
+     * evaluations whose quantised or compared value sits within the FP32
+     * error band. */
+    VLL_KERNEL_SPLIT = 1
+};
+
+/* ---- record layouts identical to the reference ------------------------- */
+/* NCCresult, Typedefine.hpp:248-268 (24 bytes). */
+typedef struct vll_nccresult {
+    float result2;            /* first peak height  */
+    float result3;            /* second peak height */
+    int16_t minHeight;
+    int16_t maxHeight;
+    int16_t result0;          /* first peak rho x 1000 (rounded)  */
+    int16_t result1;          /* second peak rho x 1000 (rounded) */
+    int16_t max_WNCC;
+    int16_t GNCC;
+    uint16_t NumOfHeight;
+    uint8_t result4;          /* peak count, capped at 10 */
+    uint8_t check_height_change;
+} vll_nccresult;
+
+/* UGRID, Typedefine.hpp:270-283 (20 bytes). */
+typedef struct vll_ugrid {
+    float Height;
+    int16_t minHeight;
+    int16_t maxHeight;
+    int16_t roh;
+    int16_t ortho_ncc[2];
+    int16_t Mean_ortho_ncc;
+    uint8_t Matched_flag;
+    uint8_t anchor_flag;
+} vll_ugrid;
+
+/* VOXEL, Typedefine.hpp:285-291 (4 bytes). */
+typedef struct vll_voxel {
+    uint8_t flag_cal;
+    int16_t INCC;             /* rho x 1000, truncated toward zero */
+} vll_voxel;
+
+/* TransParam, Typedefine.hpp:214-230 (polar-stereographic / UTM constants). */
+typedef struct vll_transparam {
+    double t_c, m_c;
+    double sa, sb, e2, e2cuadrada, c;
+    double a, e;
+    double phi_c, lambda_0;
+    int32_t pm;
+    int32_t projection;       /* 1 = polar stereographic, otherwise UTM */
+    int32_t utm_zone;
+    char direction[2];
+    int32_t bHemisphere;
+} vll_transparam;
+
+/* ---- level descriptor (what LevelInfo + ProInfo carry for this path) --- */
+/* One image of the stereo set at the matched pyramid level (and at the next
+ * finer level when the level is matched in combined mode,
+ * setsm_code.cpp:6084-6088). */
+typedef struct vll_image_desc {
+    const uint16_t *image;       /* py_Images[ti], row-major width*height  */
+    const uint16_t *mag;         /* py_MagImages[ti]                       */
+    const uint8_t *ori;          /* py_OriImages[ti]                       */
+    uint32_t width, height;      /* py_Sizes[ti][Pyramid_step]             */
+    double startpos[2];          /* py_Startpos[ti] {x, y}                 */
+    const uint16_t *image_next;  /* py_Images_next[ti]; NULL unless combined */
+    const uint16_t *mag_next;
+    const uint8_t *ori_next;
+    uint32_t width_next, height_next;
+    double startpos_next[2];
+    /* RPC in the reference's row layout (SubFunctions.cpp:1494-1582):
+     * [0..4]  line_off, samp_off, lon_off, lat_off, h_off
+     * [5..9]  the matching scales
+     * [10..29] LINE_NUM, [30..49] LINE_DEN, [50..69] SAMP_NUM,
+     * [70..89] SAMP_DEN, RPC00B term order. */
+    double rpc[90];
+    double image_adjust[2];      /* ImageAdjust[ti] {deltaLine, deltaSamp} */
+    int32_t selected;            /* proinfo->check_selected_image[ti]      */
+    int32_t _pad;
+} vll_image_desc;
+
+typedef struct vll_level_desc {
+    int32_t num_images;          /* proinfo->number_of_images (<= VLL_MAX_IMAGES) */
+    int32_t reference_id;        /* plevelinfo.reference_id (0 in SETSM)  */
+    int32_t pyramid_step;        /* *plevelinfo.Pyramid_step              */
+    int32_t template_size;       /* *plevelinfo.Template_size             */
+    int32_t py_combined_level;   /* *plevelinfo.Py_combined_level         */
+    int32_t iteration;           /* VerticalLineLocus's `iteration`       */
+    int32_t check_matching_rate; /* 1: memory-tight route, peaks streamed  */
+    int32_t is_ra;               /* proinfo->IsRA                          */
+    int32_t pre_dem_tif;         /* proinfo->pre_DEMtif                    */
+    int32_t check_matchtag;      /* proinfo->check_Matchtag                */
+    int32_t sgm_py;              /* proinfo->SGM_py                        */
+    int32_t sensor_type;         /* 0 = SB (RPC); frame cameras unsupported */
+    double resolution;           /* proinfo->resolution (image GSD, m)     */
+    double dem_resolution;       /* proinfo->DEM_resolution                */
+    double height_step;          /* *plevelinfo.height_step                */
+    double grid_resolution;      /* *plevelinfo.grid_resolution            */
+    double bin_angle;            /* *plevelinfo.bin_angle (degrees)        */
+    double boundary[4];          /* plevelinfo.Boundary                    */
+    double minmax_height[2];     /* minmaxHeight                           */
+    int64_t grid_width;          /* Size_Grid2D->width                     */
+    int64_t grid_height;         /* Size_Grid2D->height                    */
+    const double *grid_pts;      /* GridPts  [N][2] projected metres       */
+    const double *grid_wgs;      /* Grid_wgs [N][2] lon, lat degrees       */
+    vll_transparam param;        /* *plevelinfo.param                      */
+    vll_image_desc images[VLL_MAX_IMAGES];
+} vll_level_desc;
+
+/* Per-call statistics. */
+typedef struct vll_stats {
+    int64_t accessable_grid;     /* VerticalLineLocus's return value        */
+    int64_t evals;               /* (node, height) NCC evaluations computed */
+    int64_t fp64_rechecks;       /* split kernel: evaluations redone in FP64 */
+    double kernel_ms;            /* device time of the matching kernel(s)   */
+} vll_stats;
+
+typedef struct vll_context vll_context;
+
+/* ---- context ------------------------------------------------------------ */
+int vll_create(int device, vll_context **out);
+void vll_destroy(vll_context *ctx);
+/* Last error message of this context (or of the process when ctx is NULL). */
+const char *vll_last_error(const vll_context *ctx);
+int vll_abi_version(void);
+
+/* Size of the packed voxel array for a level: sum of nccresult[i].NumOfHeight
+ * over all grid nodes.  The packed layout concatenates grid_voxel[i][0..n) in
+ * node order, which is how the shim marshals the reference's VOXEL** rows. */
+int64_t vll_voxel_count(const vll_nccresult *nccresult, int64_t n_nodes);
+
+/*
+ * One VerticalLineLocus call on HOST buffers (setsm_code.cpp:6049-6548).
+ *   gridpt3    [N] in   (UGRID)
+ *   nccresult  [N] in/out (NCCresult; range fields set by InitializeVoxel in
+ *                   the voxel route, peaks written in the memory-tight route)
+ *   voxels     packed in/out voxel rows (voxel route); may be NULL when
+ *                   desc->check_matching_rate is set
+ *   stats      optional
+ * Uploads inputs, runs `kernel`, downloads results.  Returns VLL_OK or a
+ * negative status.
+ */
+int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc,
+                            const vll_ugrid *gridpt3, vll_nccresult *nccresult,
+                            vll_voxel *voxels, int64_t voxel_capacity,
+                            int kernel, vll_stats *stats);
+
+/*
+ * Non-SGM peak loop of AWNCC (setsm_code.cpp:7511-7702) over the packed voxel
+ * rows, on HOST buffers.  Selects first/second peaks per node exactly as the
+ * reference does from quantised voxels and the node's GNCC.  Levels where the
+ * reference would run SGM (Pyramid_step <= SGM_py) return VLL_ERR_UNSUPPORTED.
+ */
+int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc,
+                    const vll_ugrid *gridpt3, vll_nccresult *nccresult,
+                    const vll_voxel *voxels, int64_t voxel_capacity,
+                    vll_stats *stats);
+
+/* ---- image preprocessing (SubFunctions.cpp:2418-2560, Template.hpp:82) -- */
+/* Sobel magnitude (uint16) and 20-degree direction bin per pixel, on host
+ * buffers; bit-exact with MakeSobelMagnitudeImage + Orientation. */
+int vll_preprocess_level(vll_context *ctx, const uint16_t *image,
+                         uint32_t width, uint32_t height, int template_size,
+                         uint16_t *mag_out, uint8_t *ori_out);
+/* 9x9 sigma=1.5 Gaussian 2x downsample, bit-exact with CreateImagePyramid. */
+int vll_pyramid_down(vll_context *ctx, const uint16_t *image, uint32_t width,
+                     uint32_t height, uint16_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SETSM_VLL_H */

@@ -1,0 +1,322 @@
+/*
+ * ref_harness.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Plain-C entry points that run the reference SETSM implementation (compiled
+ * from its own sources by oracle/Makefile into oracle/_ref/libsetsm_ref.so)
+ * on a vll_level_desc.  It is used to pin the C restatement in
+ * oracle/vll_oracle.c, to generate golden fixtures and as the timed CPU
+ * baseline.  Nothing in the product links or loads it.
+ *
+ * Every function below only marshals arguments into the reference's own
+ * structures (ProInfo, LevelInfo, VOXEL**, RPC row arrays) and calls:
+ *   InitializeVoxel      setsm_code.cpp:5759
+ *   VerticalLineLocus    setsm_code.cpp:6049
+ *   AWNCC                setsm_code.cpp:7001
+ *   MakeSobelMagnitudeImage / Orientation   SubFunctions.cpp:2418 / :2473
+ *   CreateImagePyramid   Template.hpp:82
+ *   GetObjectToImageRPC_single  CoordConversion.hpp:26
+ *   ps2wgs_single / wgs2ps_single  CoordConversion.cpp:396 / :103
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <omp.h>
+
+#include "setsm_code.hpp"
+#include "CoordConversion.hpp"
+#include "SubFunctions.hpp"
+#include "Template.hpp"
+
+#include "setsm_vll.h"
+
+namespace {
+
+struct RefLevel {
+    ProInfo *proinfo = nullptr;
+    LevelInfo li;
+    const uint16 *imgs[VLL_MAX_IMAGES];
+    const uint16 *mags[VLL_MAX_IMAGES];
+    const uint8 *oris[VLL_MAX_IMAGES];
+    const uint16 *imgs_next[VLL_MAX_IMAGES];
+    const uint16 *mags_next[VLL_MAX_IMAGES];
+    const uint8 *oris_next[VLL_MAX_IMAGES];
+    D2DPOINT startpos[VLL_MAX_IMAGES];
+    D2DPOINT startpos_next[VLL_MAX_IMAGES];
+    CSize sizes_store[VLL_MAX_IMAGES][16];
+    const CSize *sizes[VLL_MAX_IMAGES];
+    const double *rpc_rows[VLL_MAX_IMAGES][7];
+    const double *const *rpcs[VLL_MAX_IMAGES];
+    double errbias[2] = {0.0, 0.0};
+    const double *adjust[VLL_MAX_IMAGES];
+    TransParam param;
+    int pyramid_step;
+    int blunder_level;
+    unsigned char template_size;
+    unsigned char num_ia = 2;
+    unsigned char iteration;
+    double bin_angle, height_step, grid_resolution, hinterval = 0.0;
+    int py_combined_level;
+    CSize grid_size;
+    long grid_length;
+    bool check_matching_rate;
+
+    explicit RefLevel(const vll_level_desc *d) {
+        proinfo = (ProInfo *)calloc(1, sizeof(ProInfo));
+        proinfo->resolution = d->resolution;
+        proinfo->DEM_resolution = d->dem_resolution;
+        proinfo->number_of_images = d->num_images;
+        proinfo->sensor_type = SB;
+        proinfo->IsRA = d->is_ra != 0;
+        proinfo->pre_DEMtif = d->pre_dem_tif != 0;
+        proinfo->check_Matchtag = d->check_matchtag != 0;
+        proinfo->SGM_py = d->sgm_py;
+        for (int ti = 0; ti < d->num_images; ++ti)
+            proinfo->check_selected_image[ti] = d->images[ti].selected != 0;
+
+        pyramid_step = d->pyramid_step;
+        blunder_level = d->pyramid_step;
+        template_size = (unsigned char)d->template_size;
+        iteration = (unsigned char)d->iteration;
+        bin_angle = d->bin_angle;
+        height_step = d->height_step;
+        grid_resolution = d->grid_resolution;
+        py_combined_level = d->py_combined_level;
+        grid_size.width = (unsigned)d->grid_width;
+        grid_size.height = (unsigned)d->grid_height;
+        grid_length = (long)d->grid_width * (long)d->grid_height;
+        check_matching_rate = d->check_matching_rate != 0;
+
+        memset(&param, 0, sizeof(param));
+        param.t_c = d->param.t_c; param.m_c = d->param.m_c;
+        param.sa = d->param.sa; param.sb = d->param.sb; param.e2 = d->param.e2;
+        param.e2cuadrada = d->param.e2cuadrada; param.c = d->param.c;
+        param.a = d->param.a; param.e = d->param.e;
+        param.phi_c = d->param.phi_c; param.lambda_0 = d->param.lambda_0;
+        param.pm = d->param.pm; param.projection = d->param.projection;
+        param.utm_zone = d->param.utm_zone;
+        param.direction[0] = d->param.direction[0];
+        param.direction[1] = d->param.direction[1];
+        param.bHemisphere = d->param.bHemisphere;
+
+        for (int ti = 0; ti < d->num_images; ++ti) {
+            const vll_image_desc &im = d->images[ti];
+            imgs[ti] = im.image; mags[ti] = im.mag; oris[ti] = im.ori;
+            imgs_next[ti] = im.image_next; mags_next[ti] = im.mag_next; oris_next[ti] = im.ori_next;
+            startpos[ti] = D2DPOINT(im.startpos[0], im.startpos[1]);
+            startpos_next[ti] = D2DPOINT(im.startpos_next[0], im.startpos_next[1]);
+            for (int l = 0; l < 16; ++l) sizes_store[ti][l] = CSize(0, 0);
+            sizes_store[ti][pyramid_step] = CSize((int)im.width, (int)im.height);
+            if (pyramid_step >= 1)
+                sizes_store[ti][pyramid_step - 1] = CSize((int)im.width_next, (int)im.height_next);
+            sizes[ti] = sizes_store[ti];
+            rpc_rows[ti][0] = im.rpc + 0;
+            rpc_rows[ti][1] = im.rpc + 5;
+            rpc_rows[ti][2] = im.rpc + 10;
+            rpc_rows[ti][3] = im.rpc + 30;
+            rpc_rows[ti][4] = im.rpc + 50;
+            rpc_rows[ti][5] = im.rpc + 70;
+            rpc_rows[ti][6] = errbias;
+            rpcs[ti] = rpc_rows[ti];
+            adjust[ti] = im.image_adjust;
+        }
+
+        memset(&li, 0, sizeof(li));
+        li.py_Images = imgs;
+        li.py_OriImages = oris;
+        li.py_MagImages = mags;
+        li.py_BImages = imgs;
+        li.py_BMagImages = mags;
+        li.py_Images_next = imgs_next;
+        li.py_OriImages_next = oris_next;
+        li.py_MagImages_next = mags_next;
+        li.py_Startpos = startpos;
+        li.py_BStartpos = startpos;
+        li.py_Startpos_next = startpos_next;
+        li.RPCs = rpcs;
+        li.Boundary = d->boundary;
+        li.Pyramid_step = &pyramid_step;
+        li.py_Sizes = sizes;
+        li.Template_size = &template_size;
+        li.ImageAdjust = adjust;
+        li.param = &param;
+        li.NumOfIAparam = &num_ia;
+        li.bin_angle = &bin_angle;
+        li.blunder_selected_level = &blunder_level;
+        li.Size_Grid2D = &grid_size;
+        li.Grid_length = &grid_length;
+        li.GridPts = reinterpret_cast<const D2DPOINT *>(d->grid_pts);
+        li.Grid_wgs = reinterpret_cast<const D2DPOINT *>(d->grid_wgs);
+        li.reference_id = d->reference_id;
+        li.height_step = &height_step;
+        li.grid_resolution = &grid_resolution;
+        li.Hinterval = &hinterval;
+        li.Py_combined_level = &py_combined_level;
+        li.iteration = &iteration;
+        li.check_matching_rate = &check_matching_rate;
+    }
+    ~RefLevel() { free(proinfo); }
+};
+
+/* Build VOXEL** rows from the packed array (NumOfHeight entries per node). */
+VOXEL **unpack_voxels(const vll_nccresult *ncc, long n, const vll_voxel *packed) {
+    VOXEL **rows = (VOXEL **)calloc((size_t)n, sizeof(VOXEL *));
+    long off = 0;
+    for (long i = 0; i < n; ++i) {
+        const int k = ncc[i].NumOfHeight;
+        if (k > 0) {
+            rows[i] = (VOXEL *)malloc(sizeof(VOXEL) * (size_t)k);
+            for (int h = 0; h < k; ++h) {
+                rows[i][h].flag_cal = packed ? packed[off + h].flag_cal != 0 : false;
+                rows[i][h].INCC = packed ? packed[off + h].INCC : 0;
+            }
+            off += k;
+        }
+    }
+    return rows;
+}
+
+/* Pack rows back by the (possibly updated) NumOfHeight, then free them. */
+long pack_and_free_voxels(const vll_nccresult *ncc, long n, VOXEL **rows,
+                          vll_voxel *packed, long cap) {
+    long off = 0;
+    for (long i = 0; i < n; ++i) {
+        const int k = ncc[i].NumOfHeight;
+        if (k > 0 && rows[i]) {
+            for (int h = 0; h < k; ++h) {
+                if (packed && off + h < cap) {
+                    packed[off + h].flag_cal = rows[i][h].flag_cal ? 1 : 0;
+                    packed[off + h].INCC = rows[i][h].INCC;
+                }
+            }
+            off += k;
+            free(rows[i]);
+        }
+        /* rows of nodes whose NumOfHeight is now 0 were already released by
+         * InitializeVoxel (which frees without clearing the pointer). */
+    }
+    free(rows);
+    return off;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_sizeof_nccresult(void) { return (int)sizeof(NCCresult); }
+int ref_sizeof_ugrid(void) { return (int)sizeof(UGRID); }
+int ref_sizeof_voxel(void) { return (int)sizeof(VOXEL); }
+int ref_sizeof_transparam(void) { return (int)sizeof(TransParam); }
+
+void ref_set_threads(int threads) {
+    if (threads > 0) omp_set_num_threads(threads);
+}
+int ref_max_threads(void) { return omp_get_max_threads(); }
+
+/* InitializeVoxel on the packed voxel rows: `voxels_in` holds the rows of the
+ * previous iteration (by the incoming NumOfHeight), `voxels_out` receives the
+ * rows by the updated NumOfHeight.  Returns the packed count written. */
+long ref_initialize_voxel(const vll_level_desc *d, vll_ugrid *gridpt3, vll_nccresult *ncc,
+                          const vll_voxel *voxels_in, vll_voxel *voxels_out, long cap) {
+    RefLevel L(d);
+    const long n = L.grid_length;
+    VOXEL **rows = unpack_voxels(ncc, n, voxels_in);
+    InitializeVoxel(L.proinfo, rows, L.li, reinterpret_cast<UGRID *>(gridpt3),
+                    reinterpret_cast<NCCresult *>(ncc), d->iteration, d->minmax_height);
+    return pack_and_free_voxels(ncc, n, rows, voxels_out, cap);
+}
+
+/* VerticalLineLocus; voxels are in/out in packed form (ignored on the
+ * memory-tight route).  Returns Accessable_grid. */
+long ref_vertical_line_locus(const vll_level_desc *d, const vll_ugrid *gridpt3,
+                             vll_nccresult *ncc, vll_voxel *voxels, long cap) {
+    RefLevel L(d);
+    const long n = L.grid_length;
+    VOXEL **rows = nullptr;
+    if (!L.check_matching_rate) rows = unpack_voxels(ncc, n, voxels);
+    const int acc = VerticalLineLocus(rows, L.proinfo, reinterpret_cast<NCCresult *>(ncc), L.li,
+                                      reinterpret_cast<const UGRID *>(gridpt3),
+                                      (uint8)d->iteration, d->minmax_height);
+    if (rows) pack_and_free_voxels(ncc, n, rows, voxels, cap);
+    return acc;
+}
+
+/* AWNCC (peak loop; SGM too when pyramid_step <= sgm_py). */
+void ref_awncc(const vll_level_desc *d, vll_ugrid *gridpt3, vll_nccresult *ncc,
+               vll_voxel *voxels, long cap) {
+    RefLevel L(d);
+    const long n = L.grid_length;
+    VOXEL **rows = unpack_voxels(ncc, n, voxels);
+    const int max_voxel = (int)((d->minmax_height[1] - d->minmax_height[0]) / d->height_step);
+    AWNCC(L.proinfo, rows, L.grid_size, reinterpret_cast<UGRID *>(gridpt3),
+          reinterpret_cast<NCCresult *>(ncc), d->height_step, (uint8)d->pyramid_step,
+          (uint8)d->iteration, max_voxel);
+    pack_and_free_voxels(ncc, n, rows, voxels, cap);
+}
+
+void ref_sobel(uint32_t w, uint32_t h, const uint16_t *src, uint16_t *mag, int16_t *dir) {
+    MakeSobelMagnitudeImage(CSize((int)w, (int)h), src, mag, dir);
+}
+
+void ref_orientation(uint32_t w, uint32_t h, const uint16_t *mag, const int16_t *dir,
+                     int template_size, uint8_t *ori) {
+    Orientation(CSize((int)w, (int)h), mag, dir, (uint8)template_size, ori);
+}
+
+/* CreateImagePyramid<uint16>(src, size, 9, 1.5) into `out` ((w/2)*(h/2)). */
+void ref_pyramid_down(uint32_t w, uint32_t h, const uint16_t *src, uint16_t *out) {
+    uint16 *r = CreateImagePyramid((uint16 *)src, CSize((int)w, (int)h), 9, 1.5);
+    memcpy(out, r, sizeof(uint16) * (size_t)(w / 2) * (size_t)(h / 2));
+    free(r);
+}
+
+/* GetObjectToImageRPC_single for n points; xy_out[2i] = sample, [2i+1] = line. */
+void ref_rpc_project(const vll_image_desc *im, long n, const double *lon, const double *lat,
+                     const double *hgt, double *xy_out) {
+    const double *rows[7] = {im->rpc + 0, im->rpc + 5, im->rpc + 10, im->rpc + 30,
+                             im->rpc + 50, im->rpc + 70, im->rpc + 0};
+    for (long i = 0; i < n; ++i) {
+        D3DPOINT gp(lon[i], lat[i], hgt[i]);
+        D2DPOINT ip = GetObjectToImageRPC_single(rows, 2, im->image_adjust, gp);
+        xy_out[2 * i] = ip.m_X;
+        xy_out[2 * i + 1] = ip.m_Y;
+    }
+}
+
+void ref_ps2wgs(const vll_transparam *p, long n, const double *xy, double *lonlat) {
+    TransParam tp;
+    memset(&tp, 0, sizeof(tp));
+    memcpy(&tp, p, sizeof(TransParam) < sizeof(*p) ? sizeof(TransParam) : sizeof(*p));
+    for (long i = 0; i < n; ++i) {
+        D2DPOINT o = ps2wgs_single(tp, D2DPOINT(xy[2 * i], xy[2 * i + 1]));
+        lonlat[2 * i] = o.m_X;
+        lonlat[2 * i + 1] = o.m_Y;
+    }
+}
+
+void ref_wgs2ps(const vll_transparam *p, long n, const double *lonlat, double *xy) {
+    TransParam tp;
+    memset(&tp, 0, sizeof(tp));
+    memcpy(&tp, p, sizeof(TransParam) < sizeof(*p) ? sizeof(TransParam) : sizeof(*p));
+    for (long i = 0; i < n; ++i) {
+        D2DPOINT o = wgs2ps_single(tp, D2DPOINT(lonlat[2 * i], lonlat[2 * i + 1]));
+        xy[2 * i] = o.m_X;
+        xy[2 * i + 1] = o.m_Y;
+    }
+}
+
+/* SetTransParam_param (SubFunctions.cpp:1186) for the given hemisphere. */
+void ref_set_transparam(int north, int projection, vll_transparam *out) {
+    TransParam tp;
+    memset(&tp, 0, sizeof(tp));
+    tp.projection = projection;
+    SetTransParam_param(&tp, north != 0);
+    tp.bHemisphere = north ? 1 : 0;
+    memset(out, 0, sizeof(*out));
+    memcpy(out, &tp, sizeof(TransParam) < sizeof(*out) ? sizeof(TransParam) : sizeof(*out));
+}
+
+double ref_get_height_step(int pyramid_step, double im_resolution) {
+    return GetHeightStep(pyramid_step, im_resolution);
+}
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the reference SETSM build.
+
+``oracle/_ref/libsetsm_ref.so`` is the reference's own code (setsm_code.cpp,
+SubFunctions.cpp, CoordConversion.cpp, ...) compiled by ``make -C oracle ref``
+with stubbed TIFF I/O, plus the marshalling harness oracle/ref_harness.cpp.
+The same Python surface is offered by ``oracle.oraclepy`` for the C
+restatement so the two can be compared call for call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from setsm_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libsetsm_ref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} not built (make -C oracle ref)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.ref_initialize_voxel.argtypes = [C.POINTER(abi.LevelDesc), vp, vp, vp, vp, C.c_long]
+        L.ref_initialize_voxel.restype = C.c_long
+        L.ref_vertical_line_locus.argtypes = [C.POINTER(abi.LevelDesc), vp, vp, vp, C.c_long]
+        L.ref_vertical_line_locus.restype = C.c_long
+        L.ref_awncc.argtypes = [C.POINTER(abi.LevelDesc), vp, vp, vp, C.c_long]
+        L.ref_awncc.restype = None
+        L.ref_sobel.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp]
+        L.ref_orientation.argtypes = [C.c_uint32, C.c_uint32, vp, vp, C.c_int, vp]
+        L.ref_pyramid_down.argtypes = [C.c_uint32, C.c_uint32, vp, vp]
+        L.ref_rpc_project.argtypes = [C.POINTER(abi.ImageDesc), C.c_long, vp, vp, vp, vp]
+        L.ref_ps2wgs.argtypes = [C.POINTER(abi.TransParam), C.c_long, vp, vp]
+        L.ref_wgs2ps.argtypes = [C.POINTER(abi.TransParam), C.c_long, vp, vp]
+        L.ref_set_transparam.argtypes = [C.c_int, C.c_int, C.POINTER(abi.TransParam)]
+        L.ref_get_height_step.argtypes = [C.c_int, C.c_double]
+        L.ref_get_height_step.restype = C.c_double
+        L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_max_threads.restype = C.c_int
+        for f in ("ref_sizeof_nccresult", "ref_sizeof_ugrid", "ref_sizeof_voxel",
+                  "ref_sizeof_transparam"):
+            getattr(L, f).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().ref_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().ref_max_threads())
+
+
+def sizes() -> dict:
+    L = lib()
+    return {"NCCresult": L.ref_sizeof_nccresult(), "UGRID": L.ref_sizeof_ugrid(),
+            "VOXEL": L.ref_sizeof_voxel(), "TransParam": L.ref_sizeof_transparam()}
+
+
+# ---- image preprocessing ---------------------------------------------------
+def sobel(img: np.ndarray):
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    h, w = img.shape
+    mag = np.zeros_like(img)
+    d = np.zeros((h, w), dtype=np.int16)
+    lib().ref_sobel(w, h, img.ctypes.data, mag.ctypes.data, d.ctypes.data)
+    return mag, d
+
+
+def orientation(mag: np.ndarray, direction: np.ndarray, template_size: int = 15):
+    mag = np.ascontiguousarray(mag, dtype=np.uint16)
+    direction = np.ascontiguousarray(direction, dtype=np.int16)
+    h, w = mag.shape
+    out = np.zeros((h, w), dtype=np.uint8)
+    lib().ref_orientation(w, h, mag.ctypes.data, direction.ctypes.data, template_size,
+                          out.ctypes.data)
+    return out
+
+
+def preprocess(img: np.ndarray, template_size: int = 15):
+    """Magnitude and orientation images the way SetPyramidImages builds them."""
+    mag, d = sobel(img)
+    return mag, orientation(mag, d, template_size)
+
+
+def pyramid_down(img: np.ndarray):
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    h, w = img.shape
+    out = np.zeros((h // 2, w // 2), dtype=np.uint16)
+    lib().ref_pyramid_down(w, h, img.ctypes.data, out.ctypes.data)
+    return out
+
+
+# ---- geometry ----------------------------------------------------------------
+def rpc_project(rpc: np.ndarray, adjust, lon, lat, hgt):
+    im = abi.ImageDesc()
+    for k in range(90):
+        im.rpc[k] = rpc[k]
+    im.image_adjust[0], im.image_adjust[1] = adjust
+    lon = np.ascontiguousarray(lon, dtype=np.float64).ravel()
+    lat = np.ascontiguousarray(lat, dtype=np.float64).ravel()
+    hgt = np.ascontiguousarray(hgt, dtype=np.float64).ravel()
+    out = np.zeros((lon.size, 2))
+    lib().ref_rpc_project(C.byref(im), lon.size, lon.ctypes.data, lat.ctypes.data,
+                          hgt.ctypes.data, out.ctypes.data)
+    return out
+
+
+def ps2wgs(param: dict, xy: np.ndarray):
+    tp = abi.TransParam()
+    abi.set_transparam(tp, param)
+    xy = np.ascontiguousarray(xy, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros_like(xy)
+    lib().ref_ps2wgs(C.byref(tp), xy.shape[0], xy.ctypes.data, out.ctypes.data)
+    return out
+
+
+def wgs2ps(param: dict, lonlat: np.ndarray):
+    tp = abi.TransParam()
+    abi.set_transparam(tp, param)
+    ll = np.ascontiguousarray(lonlat, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros_like(ll)
+    lib().ref_wgs2ps(C.byref(tp), ll.shape[0], ll.ctypes.data, out.ctypes.data)
+    return out
+
+
+def transparam(north: bool = True, projection: int = 1) -> dict:
+    tp = abi.TransParam()
+    lib().ref_set_transparam(int(north), projection, C.byref(tp))
+    return abi.transparam_dict(tp)
+
+
+def height_step(pyramid_step: int, im_resolution: float) -> float:
+    return float(lib().ref_get_height_step(pyramid_step, im_resolution))
+
+
+# ---- the hot path --------------------------------------------------------------
+def voxel_count(ncc: np.ndarray) -> int:
+    return int(ncc["NumOfHeight"].astype(np.int64).sum())
+
+
+def initialize_voxel(inputs, ncc: np.ndarray, voxels_in: np.ndarray | None):
+    """InitializeVoxel; returns the packed voxel rows by the updated NumOfHeight.
+
+    Modifies ``inputs.gridpt3`` and ``ncc`` in place like the reference."""
+    d = inputs.desc()
+    # worst case: every node gets the full range
+    cap = int(((inputs.gridpt3["maxHeight"].astype(np.int64)
+                - inputs.gridpt3["minHeight"].astype(np.int64) + 4)
+               / inputs.height_step + 4).clip(0).sum())
+    out = np.zeros(max(cap, 1), dtype=abi.VOXEL_DTYPE)
+    vin = voxels_in.ctypes.data if voxels_in is not None and voxels_in.size else None
+    n = lib().ref_initialize_voxel(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data,
+                                   vin, out.ctypes.data, out.size)
+    assert n <= out.size
+    return out[:n].copy()
+
+
+def vertical_line_locus(inputs, ncc: np.ndarray, voxels: np.ndarray | None = None) -> int:
+    d = inputs.desc()
+    vp = voxels.ctypes.data if voxels is not None and voxels.size else None
+    cap = voxels.size if voxels is not None else 0
+    return int(lib().ref_vertical_line_locus(C.byref(d), inputs.gridpt3.ctypes.data,
+                                             ncc.ctypes.data, vp, cap))
+
+
+def awncc(inputs, ncc: np.ndarray, voxels: np.ndarray) -> None:
+    d = inputs.desc()
+    vp = voxels.ctypes.data if voxels.size else None
+    lib().ref_awncc(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data, vp, voxels.size)
