@@ -195,6 +195,24 @@ int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc,
                             int kernel, vll_stats *stats);
 
 /*
+ * Same call with every pointer on the DEVICE: the image planes and grid
+ * arrays inside `desc`, gridpt3, nccresult, the packed voxel rows and their
+ * row offsets (int64 [N+1], exclusive prefix sum of NumOfHeight; voxel route
+ * only).  Inputs stay resident; nothing is copied to or from the host.  Work
+ * is queued on the context's stream; the call waits for it only when `stats`
+ * is non-NULL.
+ */
+int vll_vertical_line_locus_device(vll_context *ctx, const vll_level_desc *desc,
+                                   const vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
+                                   vll_voxel *d_voxels, const int64_t *d_voxel_offsets,
+                                   int kernel, vll_stats *stats);
+
+/* Use `stream` (a cudaStream_t) for this context's work; NULL restores a
+ * private stream.  vll_get_stream returns the stream in use. */
+int vll_set_stream(vll_context *ctx, void *stream);
+void *vll_get_stream(vll_context *ctx);
+
+/*
  * Non-SGM peak loop of AWNCC (setsm_code.cpp:7511-7702) over the packed voxel
  * rows, on HOST buffers.  Selects first/second peaks per node exactly as the
  * reference does from quantised voxels and the node's GNCC.  Levels where the
@@ -214,6 +232,12 @@ int vll_preprocess_level(vll_context *ctx, const uint16_t *image,
 /* 9x9 sigma=1.5 Gaussian 2x downsample, bit-exact with CreateImagePyramid. */
 int vll_pyramid_down(vll_context *ctx, const uint16_t *image, uint32_t width,
                      uint32_t height, uint16_t *out);
+/* Device-pointer variants of the two preprocessing calls. */
+int vll_preprocess_level_device(vll_context *ctx, const uint16_t *d_image,
+                                uint32_t width, uint32_t height, int template_size,
+                                uint16_t *d_mag, uint8_t *d_ori);
+int vll_pyramid_down_device(vll_context *ctx, const uint16_t *d_image, uint32_t width,
+                            uint32_t height, uint16_t *d_out);
 
 #ifdef __cplusplus
 }

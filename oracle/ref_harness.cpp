@@ -17,6 +17,7 @@
  *   GetObjectToImageRPC_single  CoordConversion.hpp:26
  *   ps2wgs_single / wgs2ps_single  CoordConversion.cpp:396 / :103
  */
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -317,6 +318,61 @@ void ref_set_transparam(int north, int projection, vll_transparam *out) {
 
 double ref_get_height_step(int pyramid_step, double im_resolution) {
     return GetHeightStep(pyramid_step, im_resolution);
+}
+
+/* Byte offsets of the fields the drop-in reads, in the order of the
+ * library's vll_compat_layout(), taken from the reference's own headers. */
+int ref_layout(int64_t *out, int cap) {
+    const int64_t v[] = {
+        (int64_t)sizeof(ProInfo),
+        (int64_t)offsetof(ProInfo, resolution),
+        (int64_t)offsetof(ProInfo, DEM_resolution),
+        (int64_t)offsetof(ProInfo, number_of_images),
+        (int64_t)offsetof(ProInfo, sensor_type),
+        (int64_t)offsetof(ProInfo, IsRA),
+        (int64_t)offsetof(ProInfo, pre_DEMtif),
+        (int64_t)offsetof(ProInfo, check_Matchtag),
+        (int64_t)offsetof(ProInfo, check_selected_image),
+        (int64_t)offsetof(ProInfo, SGM_py),
+        (int64_t)sizeof(LevelInfo),
+        (int64_t)offsetof(LevelInfo, py_Images),
+        (int64_t)offsetof(LevelInfo, py_OriImages),
+        (int64_t)offsetof(LevelInfo, py_MagImages),
+        (int64_t)offsetof(LevelInfo, py_Images_next),
+        (int64_t)offsetof(LevelInfo, py_OriImages_next),
+        (int64_t)offsetof(LevelInfo, py_MagImages_next),
+        (int64_t)offsetof(LevelInfo, py_Startpos),
+        (int64_t)offsetof(LevelInfo, py_Startpos_next),
+        (int64_t)offsetof(LevelInfo, RPCs),
+        (int64_t)offsetof(LevelInfo, Boundary),
+        (int64_t)offsetof(LevelInfo, Pyramid_step),
+        (int64_t)offsetof(LevelInfo, py_Sizes),
+        (int64_t)offsetof(LevelInfo, Template_size),
+        (int64_t)offsetof(LevelInfo, ImageAdjust),
+        (int64_t)offsetof(LevelInfo, param),
+        (int64_t)offsetof(LevelInfo, bin_angle),
+        (int64_t)offsetof(LevelInfo, Size_Grid2D),
+        (int64_t)offsetof(LevelInfo, GridPts),
+        (int64_t)offsetof(LevelInfo, Grid_wgs),
+        (int64_t)offsetof(LevelInfo, reference_id),
+        (int64_t)offsetof(LevelInfo, height_step),
+        (int64_t)offsetof(LevelInfo, grid_resolution),
+        (int64_t)offsetof(LevelInfo, Py_combined_level),
+        (int64_t)offsetof(LevelInfo, check_matching_rate),
+        (int64_t)sizeof(NCCresult),
+        (int64_t)sizeof(UGRID),
+        (int64_t)offsetof(UGRID, ortho_ncc),
+        (int64_t)offsetof(UGRID, Matched_flag),
+        (int64_t)sizeof(VOXEL),
+        (int64_t)offsetof(VOXEL, INCC),
+        (int64_t)sizeof(TransParam),
+        (int64_t)offsetof(TransParam, bHemisphere),
+        (int64_t)sizeof(D2DPOINT),
+        (int64_t)sizeof(CSize),
+    };
+    const int nv = (int)(sizeof(v) / sizeof(v[0]));
+    for (int i = 0; i < nv && i < cap; ++i) out[i] = v[i];
+    return nv;
 }
 
 }  // extern "C"

@@ -1,0 +1,653 @@
+// vll_capi.cu -- the plain-C entry points of include/setsm_vll.h.
+//
+// A vll_context owns one CUDA stream and grow-only device buffers.  The
+// host-buffer entry points upload a call's inputs, run the selected kernel and
+// download the outputs; the *_device variants take device pointers and leave
+// data resident (used by the serving loop and the benchmark).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "setsm_vll.h"
+#include "vll_device.cuh"
+#include "vll_internal.h"
+#include "vll_split.h"
+
+namespace {
+
+struct Buf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+cudaError_t ensure(Buf &b, size_t n) {
+    if (n == 0) n = 1;
+    if (n <= b.cap) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, n);
+    if (e == cudaSuccess) b.cap = n;
+    return e;
+}
+
+void release(Buf &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+thread_local std::string g_last_error;
+
+}  // namespace
+
+struct vll_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    std::string err;
+    Buf level, counters;
+    Buf img[VLL_MAX_IMAGES][6];
+    Buf wgs, pts, gp3, ncc, vox, voxoff;
+    Buf ocd[VLL_MAX_IMAGES], ocdn[VLL_MAX_IMAGES], ocdptr;
+    Buf pre_tmp, pre_wt, pre_img, pre_mag, pre_ori;
+    vll::SplitBuffers split;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    vll::DevLevel *hlevel = nullptr;   // pinned host staging of the level block
+};
+
+namespace {
+
+int fail(vll_context *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(vll_context *ctx, cudaError_t e, const char *where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    return fail(ctx, VLL_ERR_CUDA, m);
+}
+
+#define VLL_CUDA(ctx, call)                                     \
+    do {                                                        \
+        cudaError_t e__ = (call);                               \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, #call); \
+    } while (0)
+
+// SetNCC_alpha, setsm_code.cpp:6014-6047
+double ncc_alpha(int L, int it, int is_ra) {
+    double a;
+    if (L >= 4) {
+        a = 1.0 - ((4 - L) * 0.2 + (it - 1) * 0.05);
+        if (a < 0.8) a = 0.8;
+    } else if (L >= 3) {
+        a = 1.0 - ((4 - L) * 0.2 + (it - 1) * 0.05);
+        if (a < 0.6) a = 0.6;
+    } else if (L == 2) {
+        a = 1.0 - (0.4 + (it - 1) * 0.05);
+        if (a < 0.4) a = 0.4;
+    } else
+        a = 1.0 - ((4 - L) * 0.2 + (it - 1) * 0.05);
+    if (a < 0.1) a = 0.1;
+    if (is_ra) a = 1.0;
+    return a;
+}
+
+}  // namespace
+
+namespace vll {
+
+// Derives the per-call constants of VerticalLineLocus (setsm_code.cpp:6050-6137)
+// from the descriptor.  Image / grid pointers are copied as given.
+int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err) {
+    memset(P, 0, sizeof(*P));
+    if (!d) {
+        *err = "null level descriptor";
+        return VLL_ERR_INVALID;
+    }
+    if (d->sensor_type != 0) {
+        *err = "only RPC (SB) sensors are supported";
+        return VLL_ERR_UNSUPPORTED;
+    }
+    if (d->num_images < 2 || d->num_images > VLL_MAX_IMAGES) {
+        *err = "num_images must be in [2, VLL_MAX_IMAGES]";
+        return VLL_ERR_INVALID;
+    }
+    if (d->reference_id < 0 || d->reference_id >= d->num_images) {
+        *err = "reference_id out of range";
+        return VLL_ERR_INVALID;
+    }
+    if (d->grid_width <= 0 || d->grid_height <= 0 || !(d->height_step > 0) ||
+        d->pyramid_step < 0 || d->pyramid_step > 12 || d->template_size < 1 ||
+        d->template_size > 255) {
+        *err = "invalid grid size, height step, pyramid step or template size";
+        return VLL_ERR_INVALID;
+    }
+    const int L = d->pyramid_step;
+    int template_size = d->template_size;
+    if (L >= 1) {
+        const double area = 5.0;
+        const int t = (int)((area / (d->resolution * (1 << L))) / 2.0) * 2 + 1;
+        if (d->template_size < t) template_size = t;
+    }
+    int H = template_size / 2;
+    if (L == 3)
+        H = H - 1;
+    else if (L < 3)
+        H = H - 2;
+    if (H < 1 || H > kMaxHalf) {
+        *err = "window half-size out of the supported range [1, 8]";
+        return VLL_ERR_UNSUPPORTED;
+    }
+    P->num_images = d->num_images;
+    P->ref = d->reference_id;
+    P->L = L;
+    P->H = H;
+    P->iteration = d->iteration;
+    P->cmr = d->check_matching_rate != 0;
+    P->is_ra = d->is_ra != 0;
+    P->check_matchtag = d->check_matchtag != 0;
+    P->pre_dem_tif = d->pre_dem_tif != 0;
+    P->sgm_py = d->sgm_py;
+    P->combined = !P->is_ra && (L > d->py_combined_level);
+    P->combined_incc = P->combined && (L >= 1 && d->iteration % 2 == 0);
+    P->im_res_next = d->resolution;
+    if (P->combined) P->im_res_next = d->resolution * (1 << (L - 1));
+    P->im_res = d->resolution * (1 << L);
+    int co = !((L == 4 && d->iteration == 1) || P->is_ra);
+    if (d->pre_dem_tif && !(L == 4 && d->iteration == 1)) co = 1;
+    if (d->check_matchtag) co = 1;
+    if (L <= d->sgm_py) co = 0;
+    P->check_ortho = co;
+    P->alpha = ncc_alpha(L, d->iteration, P->is_ra);
+    P->beta = 1.0 - P->alpha;
+    P->ortho_th = 0.7 - (4 - L) * 0.10;
+    P->th_height = d->dem_resolution <= 4 ? 500 : 1000;
+    P->height_step = d->height_step;
+    P->grid_res = d->grid_resolution;
+    P->bin_angle = d->bin_angle;
+    P->dem_res = d->dem_resolution;
+    for (int i = 0; i < 4; ++i) P->boundary[i] = d->boundary[i];
+    P->minmax[0] = d->minmax_height[0];
+    P->minmax[1] = d->minmax_height[1];
+    P->grid_w = d->grid_width;
+    P->grid_h = d->grid_height;
+    P->n_nodes = d->grid_width * d->grid_height;
+    P->grid_wgs = d->grid_wgs;
+    P->grid_pts = d->grid_pts;
+    P->param = d->param;
+    if (co) {
+        P->ow = (int64_t)((d->boundary[2] - d->boundary[0]) / P->im_res) + 1;
+        P->oh = (int64_t)((d->boundary[3] - d->boundary[1]) / P->im_res) + 1;
+        if (P->combined) {
+            P->own = (int64_t)((d->boundary[2] - d->boundary[0]) / P->im_res_next) + 1;
+            P->ohn = (int64_t)((d->boundary[3] - d->boundary[1]) / P->im_res_next) + 1;
+        }
+    }
+    // rotation table: rot_theta = (double)(diff_theta * bin_angle * PI / 180.0)
+    for (int i = 0; i < kRotTable; ++i) {
+        const double dtheta = (double)(i - kRotOffset) / 2.0;
+        const double rot = (double)(dtheta * d->bin_angle * 3.141592653589793 / 180.0);
+        P->rot_cos[i] = cos(-rot);
+        P->rot_sin[i] = sin(-rot);
+    }
+    for (int ti = 0; ti < d->num_images; ++ti) {
+        const vll_image_desc &s = d->images[ti];
+        DevImage &m = P->im[ti];
+        m.img = s.image;
+        m.mag = s.mag;
+        m.ori = s.ori;
+        m.img_n = s.image_next;
+        m.mag_n = s.mag_next;
+        m.ori_n = s.ori_next;
+        m.w = s.width;
+        m.h = s.height;
+        m.wn = s.width_next;
+        m.hn = s.height_next;
+        m.sx = s.startpos[0];
+        m.sy = s.startpos[1];
+        m.sxn = s.startpos_next[0];
+        m.syn = s.startpos_next[1];
+        memcpy(m.rpc, s.rpc, sizeof(m.rpc));
+        m.adj[0] = s.image_adjust[0];
+        m.adj[1] = s.image_adjust[1];
+        m.selected = s.selected != 0;
+        if (m.selected && (s.width < 2 || s.height < 2)) {
+            *err = "selected image with size < 2";
+            return VLL_ERR_INVALID;
+        }
+    }
+    if (!P->im[P->ref].selected) {
+        *err = "the reference image must be selected";
+        return VLL_ERR_INVALID;
+    }
+    return VLL_OK;
+}
+
+bool needs_next(const DevLevel &P) { return P.combined_incc || (P.combined && P.check_ortho); }
+
+}  // namespace vll
+
+using vll::DevLevel;
+
+namespace {
+
+// Allocates and fills the orthoimage coordinate rasters (SetOrthoImageCoord).
+int run_ortho(vll_context *ctx, DevLevel *P, const DevLevel *dP_unused) {
+    (void)dP_unused;
+    if (!P->check_ortho) return VLL_OK;
+    const size_t total = (size_t)(P->ow * P->oh);
+    const size_t totaln = P->combined ? (size_t)(P->own * P->ohn) : 0;
+    for (int ti = 0; ti < P->num_images; ++ti) {
+        if (!P->im[ti].selected) continue;
+        VLL_CUDA(ctx, ensure(ctx->ocd[ti], total * sizeof(double2)));
+        VLL_CUDA(ctx, cudaMemsetAsync(ctx->ocd[ti].p, 0, total * sizeof(double2), ctx->stream));
+        P->ocd[ti] = (const double2 *)ctx->ocd[ti].p;
+        if (P->combined) {
+            VLL_CUDA(ctx, ensure(ctx->ocdn[ti], totaln * sizeof(double2)));
+            VLL_CUDA(ctx, cudaMemsetAsync(ctx->ocdn[ti].p, 0, totaln * sizeof(double2), ctx->stream));
+            P->ocd_n[ti] = (const double2 *)ctx->ocdn[ti].p;
+        }
+    }
+    return VLL_OK;
+}
+
+int upload_level_block(vll_context *ctx, const DevLevel &P) {
+    VLL_CUDA(ctx, ensure(ctx->level, sizeof(DevLevel)));
+    if (!ctx->hlevel) VLL_CUDA(ctx, cudaMallocHost((void **)&ctx->hlevel, sizeof(DevLevel)));
+    // the pinned staging block may still be in flight from a previous call
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    memcpy(ctx->hlevel, &P, sizeof(DevLevel));
+    VLL_CUDA(ctx, cudaMemcpyAsync(ctx->level.p, ctx->hlevel, sizeof(DevLevel),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    return VLL_OK;
+}
+
+// Runs the matching kernels on a level whose pointers are all device pointers.
+int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
+    int rc = run_ortho(ctx, &P, nullptr);
+    if (rc) return rc;
+    VLL_CUDA(ctx, ensure(ctx->counters, 4 * sizeof(unsigned long long)));
+    VLL_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    rc = upload_level_block(ctx, P);
+    if (rc) return rc;
+    const DevLevel *dP = (const DevLevel *)ctx->level.p;
+    if (!ctx->e0) {
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e0));
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e1));
+    }
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e0, ctx->stream));
+    if (P.check_ortho) {
+        // device array of the per-image raster pointers
+        double2 *ptrs[2 * VLL_MAX_IMAGES] = {};
+        for (int ti = 0; ti < P.num_images; ++ti) {
+            ptrs[ti] = (double2 *)P.ocd[ti];
+            ptrs[VLL_MAX_IMAGES + ti] = (double2 *)P.ocd_n[ti];
+        }
+        VLL_CUDA(ctx, ensure(ctx->ocdptr, sizeof(ptrs)));
+        VLL_CUDA(ctx, cudaMemcpyAsync(ctx->ocdptr.p, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        double2 *const *dptr = (double2 *const *)ctx->ocdptr.p;
+        VLL_CUDA(ctx, vll::launch_ortho(dP, P.ow * P.oh, dptr, dptr + VLL_MAX_IMAGES, ctx->stream));
+    }
+    unsigned long long *counters = (unsigned long long *)ctx->counters.p;
+    if (kernel == VLL_KERNEL_FP64_PLAIN || !vll::split_supported(P)) {
+        VLL_CUDA(ctx, vll::launch_plain(dP, P.n_nodes, counters, nullptr, nullptr, ctx->stream));
+    } else if (kernel == VLL_KERNEL_SPLIT) {
+        std::string err;
+        cudaError_t e = vll::run_split(ctx->split, P, dP, counters, ctx->stream, &err);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, err.c_str());
+    } else {
+        return fail(ctx, VLL_ERR_INVALID, "unknown kernel id");
+    }
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
+    if (stats) {
+        unsigned long long h[4];
+        VLL_CUDA(ctx, cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        float ms = 0;
+        VLL_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->e0, ctx->e1));
+        stats->accessable_grid = (int64_t)h[0];
+        stats->evals = (int64_t)h[1];
+        stats->fp64_rechecks = (int64_t)h[2];
+        stats->kernel_ms = ms;
+        if (h[3] != 0) return fail(ctx, VLL_ERR_TIMEOUT, "persistent kernel reported an error flag");
+    }
+    return VLL_OK;
+}
+
+int upload(vll_context *ctx, Buf &b, const void *src, size_t n) {
+    VLL_CUDA(ctx, ensure(b, n));
+    if (n) VLL_CUDA(ctx, cudaMemcpyAsync(b.p, src, n, cudaMemcpyHostToDevice, ctx->stream));
+    return VLL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vll_abi_version(void) { return VLL_ABI_VERSION; }
+
+const char *vll_last_error(const vll_context *ctx) {
+    if (ctx) return ctx->err.c_str();
+    return g_last_error.c_str();
+}
+
+int vll_create(int device, vll_context **out) {
+    if (!out) return fail(nullptr, VLL_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
+    if (device < 0 || device >= n) return fail(nullptr, VLL_ERR_INVALID, "device index out of range");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+    vll_context *ctx = new vll_context();
+    ctx->device = device;
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return cuda_fail(nullptr, e, "cudaStreamCreate");
+    }
+    *out = ctx;
+    return VLL_OK;
+}
+
+void vll_destroy(vll_context *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    release(ctx->level);
+    release(ctx->counters);
+    for (auto &a : ctx->img)
+        for (auto &b : a) release(b);
+    release(ctx->wgs);
+    release(ctx->pts);
+    release(ctx->gp3);
+    release(ctx->ncc);
+    release(ctx->vox);
+    release(ctx->voxoff);
+    for (auto &b : ctx->ocd) release(b);
+    for (auto &b : ctx->ocdn) release(b);
+    release(ctx->ocdptr);
+    release(ctx->pre_tmp);
+    release(ctx->pre_wt);
+    release(ctx->pre_img);
+    release(ctx->pre_mag);
+    release(ctx->pre_ori);
+    vll::split_release(ctx->split);
+    if (ctx->hlevel) cudaFreeHost(ctx->hlevel);
+    if (ctx->e0) cudaEventDestroy(ctx->e0);
+    if (ctx->e1) cudaEventDestroy(ctx->e1);
+    if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int vll_set_stream(vll_context *ctx, void *stream) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (ctx->stream && ctx->own_stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+        ctx->own_stream = false;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamCreate");
+        ctx->own_stream = true;
+    }
+    return VLL_OK;
+}
+
+void *vll_get_stream(vll_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int64_t vll_voxel_count(const vll_nccresult *ncc, int64_t n) {
+    if (!ncc || n <= 0) return 0;
+    int64_t s = 0;
+    for (int64_t i = 0; i < n; ++i) s += ncc[i].NumOfHeight;
+    return s;
+}
+
+int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
+                            vll_nccresult *nccresult, vll_voxel *voxels, int64_t voxel_capacity,
+                            int kernel, vll_stats *stats) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !gridpt3 || !nccresult)
+        return fail(ctx, VLL_ERR_INVALID, "null descriptor, gridpt3 or nccresult");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err);
+    if (rc) return fail(ctx, rc, err);
+    if (!desc->grid_wgs || !desc->grid_pts) return fail(ctx, VLL_ERR_INVALID, "null grid arrays");
+    const int64_t N = P.n_nodes;
+    const bool voxel_route = !P.cmr && !P.is_ra;
+    std::vector<int64_t> off;
+    if (voxel_route) {
+        off.resize((size_t)N + 1);
+        off[0] = 0;
+        for (int64_t i = 0; i < N; ++i) off[i + 1] = off[i] + nccresult[i].NumOfHeight;
+        if (off[N] > 0 && (!voxels || voxel_capacity < off[N]))
+            return fail(ctx, VLL_ERR_CAPACITY, "voxel buffer smaller than sum(NumOfHeight)");
+    }
+    // images (only what the level reads)
+    const bool next = vll::needs_next(P);
+    for (int ti = 0; ti < P.num_images; ++ti) {
+        const vll_image_desc &s = desc->images[ti];
+        if (!s.selected) continue;
+        if (!s.image || !s.mag || !s.ori) return fail(ctx, VLL_ERR_INVALID, "null image plane");
+        const size_t n = (size_t)s.width * s.height;
+        if ((rc = upload(ctx, ctx->img[ti][0], s.image, n * 2))) return rc;
+        if ((rc = upload(ctx, ctx->img[ti][1], s.mag, n * 2))) return rc;
+        if ((rc = upload(ctx, ctx->img[ti][2], s.ori, n))) return rc;
+        P.im[ti].img = (const uint16_t *)ctx->img[ti][0].p;
+        P.im[ti].mag = (const uint16_t *)ctx->img[ti][1].p;
+        P.im[ti].ori = (const uint8_t *)ctx->img[ti][2].p;
+        if (next) {
+            if (!s.image_next || !s.mag_next || !s.ori_next || s.width_next < 2 || s.height_next < 2)
+                return fail(ctx, VLL_ERR_INVALID, "combined level needs the next pyramid level");
+            const size_t nn = (size_t)s.width_next * s.height_next;
+            if ((rc = upload(ctx, ctx->img[ti][3], s.image_next, nn * 2))) return rc;
+            if ((rc = upload(ctx, ctx->img[ti][4], s.mag_next, nn * 2))) return rc;
+            if ((rc = upload(ctx, ctx->img[ti][5], s.ori_next, nn))) return rc;
+            P.im[ti].img_n = (const uint16_t *)ctx->img[ti][3].p;
+            P.im[ti].mag_n = (const uint16_t *)ctx->img[ti][4].p;
+            P.im[ti].ori_n = (const uint8_t *)ctx->img[ti][5].p;
+        }
+    }
+    if ((rc = upload(ctx, ctx->wgs, desc->grid_wgs, (size_t)N * 16))) return rc;
+    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
+    P.grid_wgs = (const double *)ctx->wgs.p;
+    P.grid_pts = (const double *)ctx->pts.p;
+    P.gp3 = (const vll_ugrid *)ctx->gp3.p;
+    P.ncc = (vll_nccresult *)ctx->ncc.p;
+    if (voxel_route) {
+        if ((rc = upload(ctx, ctx->voxoff, off.data(), off.size() * sizeof(int64_t)))) return rc;
+        if ((rc = upload(ctx, ctx->vox, voxels, (size_t)off[N] * sizeof(vll_voxel)))) return rc;
+        P.vox = (vll_voxel *)ctx->vox.p;
+        P.vox_off = (const int64_t *)ctx->voxoff.p;
+    }
+    vll_stats local;
+    rc = run_device(ctx, P, kernel, stats ? stats : &local);
+    if (rc) return rc;
+    VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->ncc.p, (size_t)N * sizeof(vll_nccresult),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    if (voxel_route && off[N] > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(voxels, ctx->vox.p, (size_t)off[N] * sizeof(vll_voxel),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_vertical_line_locus_device(vll_context *ctx, const vll_level_desc *desc,
+                                   const vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
+                                   vll_voxel *d_voxels, const int64_t *d_voxel_offsets, int kernel,
+                                   vll_stats *stats) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !d_gridpt3 || !d_nccresult)
+        return fail(ctx, VLL_ERR_INVALID, "null descriptor, gridpt3 or nccresult");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err);
+    if (rc) return fail(ctx, rc, err);
+    if (!P.cmr && !P.is_ra && (!d_voxels || !d_voxel_offsets))
+        return fail(ctx, VLL_ERR_INVALID, "voxel route needs voxel rows and offsets");
+    P.gp3 = d_gridpt3;
+    P.ncc = d_nccresult;
+    P.vox = d_voxels;
+    P.vox_off = d_voxel_offsets;
+    return run_device(ctx, P, kernel, stats);
+}
+
+int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
+                    vll_nccresult *nccresult, const vll_voxel *voxels, int64_t voxel_capacity,
+                    vll_stats *stats) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !gridpt3 || !nccresult) return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err);
+    if (rc) return fail(ctx, rc, err);
+    if (P.L <= desc->sgm_py)
+        return fail(ctx, VLL_ERR_UNSUPPORTED, "SGM aggregation levels are not implemented");
+    const int64_t N = P.n_nodes;
+    std::vector<int64_t> off((size_t)N + 1);
+    off[0] = 0;
+    for (int64_t i = 0; i < N; ++i) off[i + 1] = off[i] + nccresult[i].NumOfHeight;
+    if (off[N] > 0 && (!voxels || voxel_capacity < off[N]))
+        return fail(ctx, VLL_ERR_CAPACITY, "voxel buffer smaller than sum(NumOfHeight)");
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
+    if ((rc = upload(ctx, ctx->voxoff, off.data(), off.size() * sizeof(int64_t)))) return rc;
+    if ((rc = upload(ctx, ctx->vox, voxels, (size_t)off[N] * sizeof(vll_voxel)))) return rc;
+    P.gp3 = (const vll_ugrid *)ctx->gp3.p;
+    P.ncc = (vll_nccresult *)ctx->ncc.p;
+    P.vox = (vll_voxel *)ctx->vox.p;
+    P.vox_off = (const int64_t *)ctx->voxoff.p;
+    if ((rc = upload_level_block(ctx, P))) return rc;
+    if (!ctx->e0) {
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e0));
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e1));
+    }
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e0, ctx->stream));
+    VLL_CUDA(ctx, vll::launch_awncc((const DevLevel *)ctx->level.p, N, ctx->stream));
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->ncc.p, (size_t)N * sizeof(vll_nccresult),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (stats) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->e0, ctx->e1);
+        memset(stats, 0, sizeof(*stats));
+        stats->kernel_ms = ms;
+    }
+    return VLL_OK;
+}
+
+int vll_preprocess_level_device(vll_context *ctx, const uint16_t *d_image, uint32_t width,
+                                uint32_t height, int template_size, uint16_t *d_mag,
+                                uint8_t *d_ori) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!d_image || !d_mag || !d_ori || width < 1 || height < 1)
+        return fail(ctx, VLL_ERR_INVALID, "invalid preprocessing arguments");
+    // Orientation's column extents (numcols, SubFunctions.cpp:8) are sized for
+    // the 15-pixel template SetPyramidImages uses (SubFunctions.cpp:3399).
+    if (template_size != 15)
+        return fail(ctx, VLL_ERR_UNSUPPORTED, "orientation template size must be 15");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = (size_t)width * height;
+    VLL_CUDA(ctx, ensure(ctx->pre_tmp, n));
+    // Gaussian weights exp(-(r^2+c^2)/4.5) of Orientation, SubFunctions.cpp:2489-2497
+    const int half = template_size / 2;
+    const int sz = 2 * half - 1;
+    std::vector<double> wt((size_t)sz * sz);
+    for (int r = -half + 1; r <= half - 1; ++r)
+        for (int c = -half + 1; c <= half - 1; ++c)
+            wt[(size_t)(half - 1 + r) * sz + (half - 1 + c)] = exp(-(double)(r * r + c * c) / 4.5);
+    VLL_CUDA(ctx, ensure(ctx->pre_wt, wt.size() * sizeof(double)));
+    VLL_CUDA(ctx, cudaMemcpyAsync(ctx->pre_wt.p, wt.data(), wt.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    VLL_CUDA(ctx, vll::launch_sobel(d_image, width, height, d_mag, (uint8_t *)ctx->pre_tmp.p,
+                                    ctx->stream));
+    VLL_CUDA(ctx, vll::launch_orientation(d_mag, (const uint8_t *)ctx->pre_tmp.p, width, height,
+                                          half, (const double *)ctx->pre_wt.p, d_ori, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_preprocess_level(vll_context *ctx, const uint16_t *image, uint32_t width, uint32_t height,
+                         int template_size, uint16_t *mag_out, uint8_t *ori_out) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!image || !mag_out || !ori_out) return fail(ctx, VLL_ERR_INVALID, "null buffer");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = (size_t)width * height;
+    int rc;
+    if ((rc = upload(ctx, ctx->pre_img, image, n * 2))) return rc;
+    VLL_CUDA(ctx, ensure(ctx->pre_mag, n * 2));
+    VLL_CUDA(ctx, ensure(ctx->pre_ori, n));
+    rc = vll_preprocess_level_device(ctx, (const uint16_t *)ctx->pre_img.p, width, height,
+                                     template_size, (uint16_t *)ctx->pre_mag.p,
+                                     (uint8_t *)ctx->pre_ori.p);
+    if (rc) return rc;
+    VLL_CUDA(ctx, cudaMemcpyAsync(mag_out, ctx->pre_mag.p, n * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(ori_out, ctx->pre_ori.p, n, cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_pyramid_down_device(vll_context *ctx, const uint16_t *d_image, uint32_t width,
+                            uint32_t height, uint16_t *d_out) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!d_image || !d_out || width < 2 || height < 2)
+        return fail(ctx, VLL_ERR_INVALID, "invalid pyramid arguments");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    // CreateGaussianFilter(9, 1.5), Template.hpp:45-80
+    double f[81];
+    double sum = 0;
+    const double sigma = 1.5;
+    const double tmp = -1 / (2 * sigma * sigma);
+    const double scale = 1 / (sqrt(2 * 3.141592653589793) * sigma);
+    for (int i = -4; i <= 4; ++i)
+        for (int j = -4; j <= 4; ++j) {
+            const double val = exp((i * i + j * j) * tmp) * scale;
+            f[(i + 4) * 9 + (j + 4)] = val;
+            sum += val;
+        }
+    for (double &v : f) v /= sum;
+    VLL_CUDA(ctx, ensure(ctx->pre_wt, sizeof(f)));
+    VLL_CUDA(ctx, cudaMemcpyAsync(ctx->pre_wt.p, f, sizeof(f), cudaMemcpyHostToDevice, ctx->stream));
+    VLL_CUDA(ctx, vll::launch_pyramid(d_image, width, height, (const double *)ctx->pre_wt.p, d_out,
+                                      ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_pyramid_down(vll_context *ctx, const uint16_t *image, uint32_t width, uint32_t height,
+                     uint16_t *out) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!image || !out) return fail(ctx, VLL_ERR_INVALID, "null buffer");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t n = (size_t)width * height;
+    const size_t no = (size_t)(width / 2) * (height / 2);
+    int rc;
+    if ((rc = upload(ctx, ctx->pre_img, image, n * 2))) return rc;
+    VLL_CUDA(ctx, ensure(ctx->pre_mag, no * 2));
+    rc = vll_pyramid_down_device(ctx, (const uint16_t *)ctx->pre_img.p, width, height,
+                                 (uint16_t *)ctx->pre_mag.p);
+    if (rc) return rc;
+    VLL_CUDA(ctx, cudaMemcpyAsync(out, ctx->pre_mag.p, no * 2, cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,32 @@
+// vll_internal.h -- launchers shared between the CUDA translation units and
+// the C-ABI layer.  Not part of the public interface.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vll {
+
+struct DevLevel;
+
+// vll_plain.cu
+cudaError_t launch_plain(const DevLevel *dP, int64_t n_nodes, unsigned long long *counters,
+                         double *rho_out, const int64_t *rho_off, cudaStream_t s);
+cudaError_t launch_ortho(const DevLevel *dP, int64_t total, double2 *const *cd,
+                         double2 *const *cdn, cudaStream_t s);
+cudaError_t launch_awncc(const DevLevel *dP, int64_t n_nodes, cudaStream_t s);
+cudaError_t launch_gncc(const DevLevel *dP, int64_t n_nodes, double *gsum, double *gcnt,
+                        cudaStream_t s);
+cudaError_t launch_recheck(const DevLevel *dP, const int64_t *items,
+                           const unsigned long long *n_items, int64_t max_items,
+                           const double *gsum, const double *gcnt, double *out, cudaStream_t s);
+
+// vll_preprocess.cu
+cudaError_t launch_sobel(const uint16_t *src, uint32_t w, uint32_t h, uint16_t *mag, uint8_t *bin,
+                         cudaStream_t s);
+cudaError_t launch_orientation(const uint16_t *mag, const uint8_t *bin, uint32_t w, uint32_t h,
+                               int half, const double *wt, uint8_t *ori, cudaStream_t s);
+cudaError_t launch_pyramid(const uint16_t *src, uint32_t w, uint32_t h, const double *f,
+                           uint16_t *out, cudaStream_t s);
+
+}  // namespace vll

@@ -1,0 +1,201 @@
+// vll_shim.cu -- the C++ VerticalLineLocus drop-in (setsm_code.hpp:81) on
+// top of the C ABI.  Marshals the caller's ProInfo / LevelInfo into a
+// vll_level_desc, packs the VOXEL** rows (voxel route), runs the GPU, unpacks.
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "setsm_vll_compat.hpp"
+
+namespace {
+
+struct ShimState {
+    vll_context *ctx = nullptr;
+    int kernel = VLL_KERNEL_SPLIT;
+    std::vector<vll_voxel> packed;
+};
+
+ShimState &state() {
+    thread_local ShimState s;
+    return s;
+}
+
+[[noreturn]] void die(const char *what, const char *detail) {
+    fprintf(stderr, "setsm_vll: VerticalLineLocus: %s%s%s\n", what, detail ? ": " : "",
+            detail ? detail : "");
+    fflush(stderr);
+    abort();
+}
+
+vll_context *shim_context() {
+    ShimState &s = state();
+    if (!s.ctx) {
+        const char *dev = getenv("SETSM_VLL_DEVICE");
+        const char *ker = getenv("SETSM_VLL_KERNEL");
+        if (ker && strcmp(ker, "plain") == 0) s.kernel = VLL_KERNEL_FP64_PLAIN;
+        if (vll_create(dev ? atoi(dev) : 0, &s.ctx) != VLL_OK)
+            die("cannot create the GPU context", vll_last_error(nullptr));
+    }
+    return s.ctx;
+}
+
+}  // namespace
+
+int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
+                      tagNCCresult *nccresult, taglevelinfo &pl, const UpdateGrid *GridPT3,
+                      const unsigned char iteration, const double *minmaxHeight) {
+    if (proinfo->sensor_type != kSensorSB) die("frame (AB) sensors are not supported", nullptr);
+    if (proinfo->number_of_images > VLL_MAX_IMAGES) die("too many images", nullptr);
+    vll_context *ctx = shim_context();
+    ShimState &st = state();
+
+    vll_level_desc d;
+    memset(&d, 0, sizeof(d));
+    const int L = *pl.Pyramid_step;
+    d.num_images = proinfo->number_of_images;
+    d.reference_id = pl.reference_id;
+    d.pyramid_step = L;
+    d.template_size = *pl.Template_size;
+    d.py_combined_level = *pl.Py_combined_level;
+    d.iteration = iteration;
+    d.check_matching_rate = *pl.check_matching_rate ? 1 : 0;
+    d.is_ra = proinfo->IsRA;
+    d.pre_dem_tif = proinfo->pre_DEMtif;
+    d.check_matchtag = proinfo->check_Matchtag;
+    d.sgm_py = proinfo->SGM_py;
+    d.sensor_type = 0;
+    d.resolution = proinfo->resolution;
+    d.dem_resolution = proinfo->DEM_resolution;
+    d.height_step = *pl.height_step;
+    d.grid_resolution = *pl.grid_resolution;
+    d.bin_angle = *pl.bin_angle;
+    for (int i = 0; i < 4; ++i) d.boundary[i] = pl.Boundary[i];
+    d.minmax_height[0] = minmaxHeight[0];
+    d.minmax_height[1] = minmaxHeight[1];
+    d.grid_width = pl.Size_Grid2D->width;
+    d.grid_height = pl.Size_Grid2D->height;
+    d.grid_pts = reinterpret_cast<const double *>(pl.GridPts);
+    d.grid_wgs = reinterpret_cast<const double *>(pl.Grid_wgs);
+    memcpy(&d.param, pl.param, sizeof(d.param));
+    const bool combined = !proinfo->IsRA && L > *pl.Py_combined_level;
+    for (int ti = 0; ti < d.num_images; ++ti) {
+        vll_image_desc &im = d.images[ti];
+        im.selected = proinfo->check_selected_image[ti] ? 1 : 0;
+        if (!im.selected) continue;
+        im.image = pl.py_Images[ti];
+        im.mag = pl.py_MagImages[ti];
+        im.ori = pl.py_OriImages[ti];
+        im.width = pl.py_Sizes[ti][L].width;
+        im.height = pl.py_Sizes[ti][L].height;
+        im.startpos[0] = pl.py_Startpos[ti].m_X;
+        im.startpos[1] = pl.py_Startpos[ti].m_Y;
+        if (combined && L >= 1 && pl.py_Images_next) {
+            im.image_next = pl.py_Images_next[ti];
+            im.mag_next = pl.py_MagImages_next[ti];
+            im.ori_next = pl.py_OriImages_next[ti];
+            im.width_next = pl.py_Sizes[ti][L - 1].width;
+            im.height_next = pl.py_Sizes[ti][L - 1].height;
+            if (pl.py_Startpos_next) {
+                im.startpos_next[0] = pl.py_Startpos_next[ti].m_X;
+                im.startpos_next[1] = pl.py_Startpos_next[ti].m_Y;
+            }
+        }
+        // RPC rows: offsets[5], scales[5], 4 x 20 coefficients
+        const double *const *rpc = pl.RPCs[ti];
+        memcpy(im.rpc + 0, rpc[0], 5 * sizeof(double));
+        memcpy(im.rpc + 5, rpc[1], 5 * sizeof(double));
+        for (int j = 0; j < 4; ++j) memcpy(im.rpc + 10 + 20 * j, rpc[2 + j], 20 * sizeof(double));
+        im.image_adjust[0] = pl.ImageAdjust[ti][0];
+        im.image_adjust[1] = pl.ImageAdjust[ti][1];
+    }
+
+    const int64_t n = d.grid_width * d.grid_height;
+    const bool voxel_route = !d.check_matching_rate && !d.is_ra;
+    vll_voxel *vox = nullptr;
+    int64_t nvox = 0;
+    if (voxel_route && grid_voxel) {
+        for (int64_t i = 0; i < n; ++i) nvox += nccresult[i].NumOfHeight;
+        st.packed.resize((size_t)(nvox > 0 ? nvox : 1));
+        vox = st.packed.data();
+        int64_t o = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const int k = nccresult[i].NumOfHeight;
+            if (k > 0) {
+                memcpy(vox + o, grid_voxel[i], (size_t)k * sizeof(vll_voxel));
+                o += k;
+            }
+        }
+    }
+    vll_stats stats;
+    const int rc = vll_vertical_line_locus(ctx, &d, reinterpret_cast<const vll_ugrid *>(GridPT3),
+                                           reinterpret_cast<vll_nccresult *>(nccresult), vox, nvox,
+                                           st.kernel, &stats);
+    if (rc != VLL_OK) die("GPU call failed", vll_last_error(ctx));
+    if (vox) {
+        int64_t o = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const int k = nccresult[i].NumOfHeight;
+            if (k > 0) {
+                memcpy(grid_voxel[i], vox + o, (size_t)k * sizeof(vll_voxel));
+                o += k;
+            }
+        }
+    }
+    return (int)stats.accessable_grid;
+}
+
+extern "C" int vll_compat_layout(int64_t *out, int cap) {
+    const int64_t v[] = {
+        (int64_t)sizeof(ProjectInfo),
+        (int64_t)offsetof(ProjectInfo, resolution),
+        (int64_t)offsetof(ProjectInfo, DEM_resolution),
+        (int64_t)offsetof(ProjectInfo, number_of_images),
+        (int64_t)offsetof(ProjectInfo, sensor_type),
+        (int64_t)offsetof(ProjectInfo, IsRA),
+        (int64_t)offsetof(ProjectInfo, pre_DEMtif),
+        (int64_t)offsetof(ProjectInfo, check_Matchtag),
+        (int64_t)offsetof(ProjectInfo, check_selected_image),
+        (int64_t)offsetof(ProjectInfo, SGM_py),
+        (int64_t)sizeof(taglevelinfo),
+        (int64_t)offsetof(taglevelinfo, py_Images),
+        (int64_t)offsetof(taglevelinfo, py_OriImages),
+        (int64_t)offsetof(taglevelinfo, py_MagImages),
+        (int64_t)offsetof(taglevelinfo, py_Images_next),
+        (int64_t)offsetof(taglevelinfo, py_OriImages_next),
+        (int64_t)offsetof(taglevelinfo, py_MagImages_next),
+        (int64_t)offsetof(taglevelinfo, py_Startpos),
+        (int64_t)offsetof(taglevelinfo, py_Startpos_next),
+        (int64_t)offsetof(taglevelinfo, RPCs),
+        (int64_t)offsetof(taglevelinfo, Boundary),
+        (int64_t)offsetof(taglevelinfo, Pyramid_step),
+        (int64_t)offsetof(taglevelinfo, py_Sizes),
+        (int64_t)offsetof(taglevelinfo, Template_size),
+        (int64_t)offsetof(taglevelinfo, ImageAdjust),
+        (int64_t)offsetof(taglevelinfo, param),
+        (int64_t)offsetof(taglevelinfo, bin_angle),
+        (int64_t)offsetof(taglevelinfo, Size_Grid2D),
+        (int64_t)offsetof(taglevelinfo, GridPts),
+        (int64_t)offsetof(taglevelinfo, Grid_wgs),
+        (int64_t)offsetof(taglevelinfo, reference_id),
+        (int64_t)offsetof(taglevelinfo, height_step),
+        (int64_t)offsetof(taglevelinfo, grid_resolution),
+        (int64_t)offsetof(taglevelinfo, Py_combined_level),
+        (int64_t)offsetof(taglevelinfo, check_matching_rate),
+        (int64_t)sizeof(tagNCCresult),
+        (int64_t)sizeof(UpdateGrid),
+        (int64_t)offsetof(UpdateGrid, ortho_ncc),
+        (int64_t)offsetof(UpdateGrid, Matched_flag),
+        (int64_t)sizeof(tagVoxelinfo),
+        (int64_t)offsetof(tagVoxelinfo, INCC),
+        (int64_t)sizeof(tagTransParam),
+        (int64_t)offsetof(tagTransParam, bHemisphere),
+        (int64_t)sizeof(tagD2DPoint),
+        (int64_t)sizeof(tagCSize),
+    };
+    const int nv = (int)(sizeof(v) / sizeof(v[0]));
+    for (int i = 0; i < nv && i < cap; ++i) out[i] = v[i];
+    return nv;
+}

@@ -1,0 +1,45 @@
+// vll_split.h -- the split-precision pipeline (FP64 geometry, FP32 window
+// statistics, exact FP64 re-evaluation inside the FP32 error band).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+namespace vll {
+
+struct DevLevel;
+
+// Device scratch of the split pipeline, grown on demand and owned by a context.
+struct SplitBuffers {
+    void *node_k = nullptr;        // int32  [N]   slots per active node (0 = inactive)
+    void *slot_off = nullptr;      // int64  [N+1] slot offsets
+    void *item_cnt = nullptr;      // int32  [N]   work items per node
+    void *item_off = nullptr;      // int64  [N+1]
+    void *items = nullptr;         // int64  [n_items]  (node << 16 | k0)
+    void *rho = nullptr;           // float2 [slots] (temp_rho, INCC average)
+    void *gsum = nullptr;          // double [N] GNCC sums (FP64)
+    void *gcnt = nullptr;          // double [N]
+    void *re_items = nullptr;      // int64  [max_re] (node << 16 | k)
+    void *re_out = nullptr;        // double [2 * max_re]
+    void *node_re = nullptr;       // int64  [N] (start << 8 | count) of a node's re-checks
+    void *scan_tmp = nullptr;      // cub temporary storage
+    void *ctl = nullptr;           // uint64 [8] queue head, counts, flags
+    void *pending = nullptr;       // int64  [N]  nodes awaiting the exact re-scan
+    size_t cap_nodes = 0, cap_slots = 0, cap_items = 0, cap_re = 0, cap_scan = 0;
+};
+
+void split_release(SplitBuffers &b);
+
+// Whether the split kernel implements this level (stereo, no frame sensor,
+// no relative-adjustment mode, H within the compiled window sizes); other
+// levels run the plain FP64 kernel.
+bool split_supported(const DevLevel &P);
+
+// Runs the split pipeline for a level whose DevLevel block is at dP (device)
+// and mirrored in P (host).  counters: [0] accessable, [1] evals,
+// [2] FP64 re-checks, [3] error flag.
+cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
+                      unsigned long long *counters, cudaStream_t s, std::string *err);
+
+}  // namespace vll

@@ -1,0 +1,198 @@
+"""Python host interface of the B200 vertical-line-locus matcher.
+
+Mirrors the reference's operator surface for this path
+(VerticalLineLocus, setsm_code.cpp:6049; AWNCC's peak loop, :7511;
+MakeSobelMagnitudeImage + Orientation, SubFunctions.cpp:2418/:2473;
+CreateImagePyramid, Template.hpp:82) over the C ABI of include/setsm_vll.h.
+Everything runs in ``setsm_b200/lib/libsetsm_vll.so`` on the GPU; if that
+library is missing or no GPU is present the calls raise -- there is no CPU
+path in the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libsetsm_vll.so")
+
+KERNELS = {"plain": abi.VLL_KERNEL_FP64_PLAIN, "split": abi.VLL_KERNEL_SPLIT}
+
+EXPORTED = [
+    "vll_abi_version", "vll_last_error", "vll_create", "vll_destroy", "vll_set_stream",
+    "vll_get_stream", "vll_voxel_count", "vll_vertical_line_locus",
+    "vll_vertical_line_locus_device", "vll_awncc_peaks", "vll_preprocess_level",
+    "vll_preprocess_level_device", "vll_pyramid_down", "vll_pyramid_down_device",
+    "vll_compat_layout",
+]
+
+_lib = None
+
+
+class VLLError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `python -m setsm_b200.build` "
+            "(the matcher has no CPU implementation)")
+    L = C.CDLL(LIB_PATH)
+    vp, i64, i32 = C.c_void_p, C.c_int64, C.c_int
+    L.vll_abi_version.restype = i32
+    L.vll_last_error.argtypes = [vp]
+    L.vll_last_error.restype = C.c_char_p
+    L.vll_create.argtypes = [i32, C.POINTER(vp)]
+    L.vll_destroy.argtypes = [vp]
+    L.vll_destroy.restype = None
+    L.vll_set_stream.argtypes = [vp, vp]
+    L.vll_get_stream.argtypes = [vp]
+    L.vll_get_stream.restype = vp
+    L.vll_voxel_count.argtypes = [vp, i64]
+    L.vll_voxel_count.restype = i64
+    L.vll_vertical_line_locus.argtypes = [vp, C.POINTER(abi.LevelDesc), vp, vp, vp, i64, i32,
+                                          C.POINTER(abi.Stats)]
+    L.vll_vertical_line_locus_device.argtypes = [vp, C.POINTER(abi.LevelDesc), vp, vp, vp, vp, i32,
+                                                 C.POINTER(abi.Stats)]
+    L.vll_awncc_peaks.argtypes = [vp, C.POINTER(abi.LevelDesc), vp, vp, vp, i64,
+                                  C.POINTER(abi.Stats)]
+    L.vll_preprocess_level.argtypes = [vp, vp, C.c_uint32, C.c_uint32, i32, vp, vp]
+    L.vll_preprocess_level_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, i32, vp, vp]
+    L.vll_pyramid_down.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
+    L.vll_pyramid_down_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
+    L.vll_compat_layout.argtypes = [vp, i32]
+    L.vll_compat_layout.restype = i32
+    _lib = L
+    return L
+
+
+def compat_layout() -> list[int]:
+    out = np.zeros(128, dtype=np.int64)
+    n = load().vll_compat_layout(out.ctypes.data, out.size)
+    return out[:n].tolist()
+
+
+class Context:
+    """One GPU context (stream + device buffers) of the matcher."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = C.c_void_p()
+        rc = L.vll_create(int(device), C.byref(h))
+        if rc != abi.VLL_OK:
+            raise VLLError(rc, L.vll_last_error(None).decode())
+        self._h = h
+        self.device = int(device)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            load().vll_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != abi.VLL_OK:
+            raise VLLError(rc, load().vll_last_error(self._h).decode())
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._check(load().vll_set_stream(self._h, stream_ptr))
+
+    # ---- the hot path ---------------------------------------------------------
+    def vertical_line_locus(self, inputs, nccresult: np.ndarray, voxels: np.ndarray | None = None,
+                            kernel: str = "split") -> abi.Stats:
+        """VerticalLineLocus on host arrays (nccresult / voxels updated in place)."""
+        d = inputs.desc()
+        assert nccresult.dtype == abi.NCCRESULT_DTYPE and nccresult.flags.c_contiguous
+        st = abi.Stats()
+        vptr = voxels.ctypes.data if voxels is not None and voxels.size else None
+        cap = voxels.size if voxels is not None else 0
+        self._check(load().vll_vertical_line_locus(
+            self._h, C.byref(d), inputs.gridpt3.ctypes.data, nccresult.ctypes.data, vptr, cap,
+            KERNELS[kernel], C.byref(st)))
+        return st
+
+    def vertical_line_locus_device(self, desc: abi.LevelDesc, d_gridpt3: int, d_ncc: int,
+                                   d_vox: int | None = None, d_voxoff: int | None = None,
+                                   kernel: str = "split", stats: bool = False):
+        st = abi.Stats() if stats else None
+        self._check(load().vll_vertical_line_locus_device(
+            self._h, C.byref(desc), d_gridpt3, d_ncc, d_vox, d_voxoff, KERNELS[kernel],
+            C.byref(st) if st is not None else None))
+        return st
+
+    def awncc(self, inputs, nccresult: np.ndarray, voxels: np.ndarray) -> abi.Stats:
+        """Non-SGM peak loop of AWNCC over the packed voxel rows."""
+        d = inputs.desc()
+        st = abi.Stats()
+        vptr = voxels.ctypes.data if voxels.size else None
+        self._check(load().vll_awncc_peaks(self._h, C.byref(d), inputs.gridpt3.ctypes.data,
+                                           nccresult.ctypes.data, vptr, voxels.size, C.byref(st)))
+        return st
+
+    # ---- preprocessing -----------------------------------------------------------
+    def preprocess(self, image: np.ndarray, template_size: int = 15):
+        """Sobel magnitude + orientation images (SetPyramidImages' per-level step)."""
+        image = np.ascontiguousarray(image, dtype=np.uint16)
+        h, w = image.shape
+        mag = np.zeros_like(image)
+        ori = np.zeros((h, w), dtype=np.uint8)
+        self._check(load().vll_preprocess_level(self._h, image.ctypes.data, w, h, template_size,
+                                                mag.ctypes.data, ori.ctypes.data))
+        return mag, ori
+
+    def preprocess_device(self, d_image: int, w: int, h: int, d_mag: int, d_ori: int,
+                          template_size: int = 15) -> None:
+        self._check(load().vll_preprocess_level_device(self._h, d_image, w, h, template_size,
+                                                       d_mag, d_ori))
+
+    def pyramid_down(self, image: np.ndarray) -> np.ndarray:
+        image = np.ascontiguousarray(image, dtype=np.uint16)
+        h, w = image.shape
+        out = np.zeros((h // 2, w // 2), dtype=np.uint16)
+        self._check(load().vll_pyramid_down(self._h, image.ctypes.data, w, h, out.ctypes.data))
+        return out
+
+    def pyramid_down_device(self, d_image: int, w: int, h: int, d_out: int) -> None:
+        self._check(load().vll_pyramid_down_device(self._h, d_image, w, h, d_out))
+
+
+_default: Context | None = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(int(os.environ.get("SETSM_VLL_DEVICE", "0")))
+    return _default
+
+
+def VerticalLineLocus(inputs, nccresult: np.ndarray, voxels: np.ndarray | None = None,
+                      kernel: str = "split") -> int:
+    """Drop-in for VerticalLineLocus (setsm_code.cpp:6049): returns
+    Accessable_grid and updates ``nccresult`` (and the voxel rows) in place."""
+    return int(default_context().vertical_line_locus(inputs, nccresult, voxels, kernel).accessable_grid)
+
+
+def AWNCC(inputs, nccresult: np.ndarray, voxels: np.ndarray) -> None:
+    """AWNCC's peak selection without SGM (setsm_code.cpp:7511-7702)."""
+    default_context().awncc(inputs, nccresult, voxels)

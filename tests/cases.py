@@ -1,0 +1,126 @@
+"""Seeded synthetic VerticalLineLocus cases shared by the tests.
+
+Inputs only: images from setsm_b200.synth; magnitude / orientation / pyramid
+images from the C oracle (so every implementation reads the same bytes).
+"""
+from __future__ import annotations
+
+import functools
+
+import numpy as np
+
+from setsm_b200 import level, synth
+from oracle import oraclepy as op
+
+
+@functools.lru_cache(maxsize=8)
+def scene(seed: int, size: int):
+    return synth.make_scene(synth.SceneSpec(seed=seed, image_size=size))
+
+
+@functools.lru_cache(maxsize=32)
+def pyramid(seed: int, size: int, ci: int, lev: int):
+    """(image, mag, ori) of camera ci at pyramid level lev."""
+    if lev == 0:
+        im = scene(seed, size).images[ci].numpy().view(np.uint16).copy()
+    else:
+        im = op.pyramid_down(pyramid(seed, size, ci, lev - 1)[0])
+    mag, ori = op.preprocess(im)
+    return im, mag, ori
+
+
+def make_case(*, seed=3, size=768, nodes=48, res=7.5, template=11, cmr=True, L=0, it=1,
+              sgm=0, n_heights=64, hs=1.0, sigma=20.0, ortho_frac=0.0, unmatched_frac=0.0,
+              zero_patch=False, minmax=(-500.0, 3000.0), dem_res=2.0, combined_level=0,
+              iters=None):
+    sc = scene(seed, size)
+    g = synth.make_grid(sc, nodes, res)
+    lo, hi, _ = synth.ranges_uniform(g, n_heights, hs, sigma, seed=seed + 1)
+    rng = np.random.default_rng(seed + 2)
+    imgs = []
+    for ci in range(2):
+        im, mag, ori = pyramid(seed, size, ci, L)
+        if zero_patch:
+            im = im.copy()
+            h, w = im.shape
+            im[h // 3: h // 3 + h // 10, w // 4: w // 4 + w // 8] = 0
+        kw = {}
+        if L >= 1:
+            imn, magn, orin = pyramid(seed, size, ci, L - 1)
+            kw = dict(image_next=imn, mag_next=magn, ori_next=orin)
+        imgs.append(level.ImageLevel(image=im, mag=mag, ori=ori, rpc=sc.rpcs[ci], **kw))
+    on = None
+    if ortho_frac > 0:
+        on = np.where(rng.random(lo.shape) < ortho_frac, 800, 100)
+    matched = np.where(rng.random(lo.shape) < unmatched_frac, 0, 1)
+    gp3 = level.make_gridpt3(lo, hi, g.truth, matched_flag=matched, ortho_ncc=on)
+    inp = level.LevelInputs(imgs, g.pts, g.wgs, g.width, g.height, g.boundary, gp3,
+                            pyramid_step=L, template_size=template, iteration=it,
+                            check_matching_rate=cmr, height_step=hs, grid_resolution=g.resolution,
+                            resolution=sc.spec.gsd, dem_resolution=dem_res, minmax_height=minmax,
+                            sgm_py=sgm, param=sc.param, py_combined_level=combined_level)
+    inp.iters = list(iters) if iters else [it]
+    return inp
+
+
+# name -> kwargs
+CASES = {
+    "m7": dict(),
+    "m11": dict(template=15),
+    "m7_edges": dict(zero_patch=True, unmatched_frac=0.1, minmax=(0.0, 260.0), nodes=56, res=7.0),
+    "v7_gncc": dict(cmr=False, sgm=-1, ortho_frac=0.5),
+    "v11": dict(cmr=False, sgm=-1, template=15, ortho_frac=0.3, n_heights=40),
+    "l2_combined": dict(L=2, it=2, iters=(1, 2), cmr=False, sgm=-1, ortho_frac=0.5, nodes=24,
+                        res=16.0, n_heights=24, hs=2.0, template=15),
+    "l2_max": dict(L=2, it=1, cmr=False, sgm=-1, ortho_frac=0.5, nodes=24, res=16.0,
+                   n_heights=24, hs=2.0, template=15),
+    "l3_m": dict(L=3, it=1, cmr=True, nodes=16, res=24.0, n_heights=20, hs=3.0, template=15),
+    "v7_it2": dict(cmr=False, sgm=-1, it=2, iters=(1, 2), ortho_frac=0.5, n_heights=48),
+}
+
+
+def field_mismatch(a: np.ndarray, b: np.ndarray) -> dict:
+    """Per-field count of differing records (structured arrays)."""
+    out = {}
+    for f in a.dtype.names:
+        x, y = a[f], b[f]
+        if x.dtype.kind == "f":
+            bad = ~((x == y) | (np.isnan(x) & np.isnan(y)))
+        else:
+            bad = x != y
+        n = int(np.count_nonzero(bad))
+        if n:
+            out[f] = n
+    return out
+
+
+def run_cpu(impl, inp, iterations=None):
+    """Runs a case through `impl` (oracle.refpy or oracle.oraclepy) the way
+    Matching_SETSM does (setsm_code.cpp:3774-3845), once per iteration:
+    [InitializeVoxel ->] VerticalLineLocus [-> AWNCC].  The returned state
+    (init_* = inputs of the last VerticalLineLocus call) lets a GPU test
+    replay exactly the last call."""
+    import copy
+    inp = copy.copy(inp)
+    inp.gridpt3 = inp.gridpt3.copy()
+    iters = iterations or [inp.iteration]
+    ncc = inp.new_nccresult()
+    vox = None
+    out = {}
+    for it in iters:
+        inp.iteration = it
+        if not inp.check_matching_rate:
+            vox = impl.initialize_voxel(inp, ncc, vox)
+        out["init_ncc"] = ncc.copy()
+        out["init_vox"] = None if vox is None else vox.copy()
+        out["init_gp3"] = inp.gridpt3.copy()
+        out["acc"] = impl.vertical_line_locus(inp, ncc, vox)
+        out["vll_ncc"] = ncc.copy()
+        if vox is not None:
+            out["vll_vox"] = vox.copy()
+            impl.awncc(inp, ncc, vox)
+    out["ncc"] = ncc
+    out["vox"] = vox
+    out["gp3"] = inp.gridpt3
+    out["inputs"] = inp
+    return out
