@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark of the vertical-line-locus hot path (node x height NCC evals/s).
+
+Workload (default ``c2``): level-0 full scene -- a seeded synthetic 16384^2
+uint16 stereo pair (pushbroom cameras, cubic RPCs), a 4096^2 grid at 2 m with
+TIN-derived height ranges of 8-512 candidates at 0.5 m, matched with the 7x7
+and 11x11 windows on the memory-tight route (inline first/second peak
+selection).  One step = one VerticalLineLocus pass per window over the whole
+grid.
+
+* value: evals/s with inputs resident in HBM (device-pointer C ABI), K steps
+  timed with CUDA events on the library's stream; max over ranks.
+* e2e: the same metric through the host-buffer C ABI call
+  (vll_vertical_line_locus) from pinned host memory, uploads and downloads
+  inside the timed region.
+* roofline: the window kernel's algorithmic bytes (8 B per window sample,
+  2 orientation bytes, 4 B NCC out) per launch over its average duration.
+* fp64_plain_gpu: the plain FP64 one-node-per-thread kernel on the same
+  workload (untimed leg, CUDA events), with identical-peak and tie rates.
+* cpu_baseline: the reference SETSM code (oracle/_ref, OpenMP, all host
+  cores) on a bounded band of grid rows of the same workload.
+
+``--impl reference`` times the reference CPU implementation alone (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "node x height NCC evals/s"
+UNIT = "evals/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_setup(gpus: int):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU reference leg
+# ---------------------------------------------------------------------------
+def cpu_reference(wl, ctx, budget_s: float, templates) -> dict:
+    """Reference SETSM (oracle/_ref, OpenMP on every host core) on a band of
+    grid rows sized for about `budget_s` seconds of CPU work per window."""
+    from oracle import refpy
+    from setsm_b200 import workloads
+    if not refpy.available():
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                "sample": "reference build missing (oracle/_ref not built)"}
+    cores = os.cpu_count() or 1
+    refpy.set_threads(cores)
+    total_evals, total_s, parts = 0, 0.0, []
+    for tmpl in templates:
+        rate_guess = (2.0e5 if tmpl == 11 else 1.0e5) * cores
+        rows = workloads.rows_for_budget(wl, rate_guess * budget_s)
+        r0 = max(0, wl.grid.height // 2 - rows // 2)
+        inp = wl.host_inputs(tmpl, rows=(r0, r0 + rows))
+        # evaluation count of the band, from the GPU on the identical inputs
+        ncc_g = inp.new_nccresult()
+        st = ctx.vertical_line_locus(inp, ncc_g, None, "split")
+        ncc = inp.new_nccresult()
+        t = time.perf_counter()
+        refpy.vertical_line_locus(inp, ncc)
+        dt = time.perf_counter() - t
+        total_evals += st.evals
+        total_s += dt
+        parts.append(f"{rows} rows x {wl.grid.width} nodes, {workloads.WINDOW_OF_TEMPLATE[tmpl]}: "
+                     f"{st.evals} evals in {dt:.2f} s")
+    return {"value": total_evals / total_s, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "; ".join(parts)}
+
+
+def run_reference_arm(args):
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import torch
+    from setsm_b200 import vll, workloads
+    ctx = vll.Context(0)
+    t0 = time.time()
+    wl = workloads.build(args.config, ctx, device="cuda:0", seed=1)
+    log(f"workload built in {time.time() - t0:.1f} s")
+    templates = workloads.CONFIGS[args.config]["templates"]
+    for _ in range(args.warmup):
+        cpu_reference(wl, ctx, 2.0, templates)
+    vals = []
+    cb = None
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        cb = cpu_reference(wl, ctx, args.cpu_seconds / max(1, args.steps), templates)
+        vals.append(cb["value"] or 0.0)
+    elapsed = time.perf_counter() - t
+    value = statistics.mean(vals) if vals else None
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": elapsed * 1e3 / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_block(args, wl),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
+                         "sample": cb["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    del torch
+
+
+def config_block(args, wl) -> dict:
+    from setsm_b200 import workloads
+    cfg = workloads.CONFIGS[args.config]
+    return {
+        "workload": {
+            "c2": "C2 level-0 full scene: 16384^2 uint16 stereo pair, 4096^2 grid at 2 m, "
+                  "TIN ranges K=8-512 log-uniform at 0.5 m, 7x7 and 11x11 windows, "
+                  "memory-tight route (inline peaks)",
+            "c1": "C1: 2048^2 pair, 256^2 grid, 64 heights at 1 m, 7x7",
+            "c2_small": "C2-like reduced: 4096^2 pair, 1024^2 grid, TIN K=8-512 at 0.5 m",
+        }[args.config],
+        "nodes": int(wl.n_nodes),
+        "image": f"{cfg['image_size']}^2 uint16",
+        "windows": [workloads.WINDOW_OF_TEMPLATE[t] for t in cfg["templates"]],
+        "kernel": args.kernel,
+        "l2": "inputs larger than L2 (images 2 x 1.25 GiB with magnitude and orientation)",
+        "parallelism": f"replicas x{args.gpus} (independent scenes per GPU)",
+    }
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    from setsm_b200 import abi, vll, workloads
+
+    dev = torch.device("cuda", local)
+    ctx = vll.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.time()
+    wl = workloads.build(args.config, ctx, device=f"cuda:{local}", seed=1 + rank)
+    log(f"[rank {rank}] workload {args.config} built in {time.time() - t0:.1f} s "
+        f"({wl.n_nodes} nodes)")
+    templates = workloads.CONFIGS[args.config]["templates"]
+    descs = {t: wl.device_desc(t) for t in templates}
+
+    def one_step(kernel, stats=True):
+        out = {}
+        for t in templates:
+            st = ctx.vertical_line_locus_device(descs[t], wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr(),
+                                                None, None, kernel, stats=stats)
+            out[t] = st
+        return out
+
+    # warm-up (untimed)
+    for _ in range(max(3, args.warmup)):
+        ref_stats = one_step(args.kernel)
+    evals_step = {t: ref_stats[t].evals for t in templates}
+    ncc_split = workloads.ncc_host(wl)
+    barrier(world)
+
+    # ---- timed: resident inputs ----
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = ctx.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    e0.record(stream)
+    window_ms = {t: 0.0 for t in templates}
+    rechecks = 0
+    for _ in range(args.steps):
+        st = one_step(args.kernel)
+        for t in templates:
+            window_ms[t] += st[t].window_ms
+            rechecks += st[t].fp64_rechecks
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    elapsed_ms = e0.elapsed_time(e1)
+    launches = ctx.launch_count() - launches0
+    elapsed_ms = max_over_ranks(world, elapsed_ms)
+    evals_total_rank = sum(evals_step.values()) * args.steps
+    evals_total = sum_over_ranks(world, evals_total_rank)
+    value = evals_total / (elapsed_ms / 1e3)
+
+    # ---- roofline of the window kernel ----
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    alg_bytes = sum(evals_step[t] * workloads.BYTES_PER_EVAL[t] for t in templates)
+    win_ms_per_step = sum(window_ms.values()) / args.steps
+    achieved = alg_bytes / (win_ms_per_step / 1e3) / 1e9
+    per_window = {workloads.WINDOW_OF_TEMPLATE[t]: {
+        "evals": evals_step[t], "ms": window_ms[t] / args.steps,
+        "gbs": evals_step[t] * workloads.BYTES_PER_EVAL[t] / (window_ms[t] / args.steps / 1e3) / 1e9,
+        "evals_per_s": evals_step[t] / (window_ms[t] / args.steps / 1e3),
+        "stage_ms": ref_stats[t].as_dict()["stage_ms"]} for t in templates}
+
+    # ---- e2e through the host-buffer C ABI (pinned host memory) ----
+    e2e = None
+    if not args.skip_e2e:
+        host_inp = {t: wl.host_inputs(t) for t in templates}
+        ncc_h = host_inp[templates[0]].new_nccresult()
+        pinned_ncc = torch.empty(ncc_h.nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+        ncc_h = pinned_ncc.view(abi.NCCRESULT_DTYPE)
+        for t in templates:   # warm
+            ctx.vertical_line_locus(host_inp[t], ncc_h, None, args.kernel)
+        img_bytes = sum(a.nbytes for k in ("img", "mag", "ori") for a in wl.host[k])
+        grid_bytes = wl.host["wgs"].nbytes + wl.host["pts"].nbytes + wl.gp3.nbytes + ncc_h.nbytes
+        h2d = len(templates) * (img_bytes + grid_bytes)
+        d2h = len(templates) * ncc_h.nbytes
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        t_e2e = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            for t in templates:
+                ctx.vertical_line_locus(host_inp[t], ncc_h, None, args.kernel)
+        e2e_ms = (time.perf_counter() - t_e2e) * 1e3
+        e2e_ms = max_over_ranks(world, e2e_ms)
+        e2e_val = sum_over_ranks(world, sum(evals_step.values()) * args.e2e_steps) / (e2e_ms / 1e3)
+        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps,
+               "timing": "host wall clock around synchronous C-ABI calls"}
+
+    # ---- plain FP64 GPU drop-in on the same workload + parity ----
+    fp64 = None
+    if not args.skip_fp64 and rank == 0:
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        st_plain = one_step("plain")
+        e3.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_ms = e2.elapsed_time(e3)
+        ncc_plain = workloads.ncc_host(wl)
+        from tests.cases import field_mismatch
+        ran = ncc_plain["check_height_change"] > 0
+        valid = ran & (ncc_plain["result4"] > 0)
+        same_h = (ncc_plain["result2"] == ncc_split["result2"]) & \
+                 (ncc_plain["result0"] == ncc_split["result0"])
+        ties = valid & (ncc_plain["result0"] == ncc_plain["result1"])
+        fp64 = {"value": sum(s.evals for s in st_plain.values()) / (plain_ms / 1e3), "unit": UNIT,
+                "ms_per_step": plain_ms,
+                "speedup_split_vs_fp64": (sum(s.evals for s in st_plain.values()) / (plain_ms / 1e3))
+                and value / world / (sum(s.evals for s in st_plain.values()) / (plain_ms / 1e3)),
+                "last_window_mismatch_fields": field_mismatch(ncc_plain, ncc_split),
+                "identical_peak_rate": float(same_h[valid].mean()) if valid.any() else None,
+                "tie_rate": float(ties.sum() / max(1, valid.sum())),
+                "nodes_with_peaks": int(valid.sum())}
+        # restore the split result in the buffer (not needed further)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_reference(wl, ctx, args.cpu_seconds, templates)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 window sums, f64 RPC and decisions", "data": "synthetic",
+            "config": config_block(args, wl),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                         "kernel": "ncc_kernel (window)", "per_window": per_window},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "fp64_rechecks_per_step": rechecks / args.steps,
+            "fp64_plain_gpu": fp64,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2_small"])
+    ap.add_argument("--kernel", default="split", choices=["split", "plain"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define VLL_ABI_VERSION 1
+#define VLL_ABI_VERSION 2
 #define VLL_MAX_IMAGES 8
 
 /* ---- status codes ------------------------------------------------------ */
@@ -156,12 +156,18 @@ typedef struct vll_level_desc {
     vll_image_desc images[VLL_MAX_IMAGES];
 } vll_level_desc;
 
-/* Per-call statistics. */
+/* Per-call statistics (filled when a vll_stats pointer is passed; the call
+ * then waits for the GPU). */
 typedef struct vll_stats {
     int64_t accessable_grid;     /* VerticalLineLocus's return value        */
     int64_t evals;               /* (node, height) NCC evaluations computed */
     int64_t fp64_rechecks;       /* split kernel: evaluations redone in FP64 */
-    double kernel_ms;            /* device time of the matching kernel(s)   */
+    double kernel_ms;            /* device time of all matching kernels     */
+    double window_ms;            /* device time of the window (NCC) kernel  */
+    int64_t slots;               /* height slots scheduled                  */
+    int64_t launches;            /* kernels launched by the call            */
+    double stage_ms[8];          /* split pipeline: gncc, prep, scan, items,
+                                    ncc, peaks, recheck, rescan             */
 } vll_stats;
 
 typedef struct vll_context vll_context;
@@ -211,6 +217,8 @@ int vll_vertical_line_locus_device(vll_context *ctx, const vll_level_desc *desc,
  * private stream.  vll_get_stream returns the stream in use. */
 int vll_set_stream(vll_context *ctx, void *stream);
 void *vll_get_stream(vll_context *ctx);
+/* Number of kernels this context has launched for matching calls so far. */
+int64_t vll_launch_count(const vll_context *ctx);
 
 /*
  * Non-SGM peak loop of AWNCC (setsm_code.cpp:7511-7702) over the packed voxel

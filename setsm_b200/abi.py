@@ -110,7 +110,16 @@ class Stats(C.Structure):
     _fields_ = [
         ("accessable_grid", C.c_int64), ("evals", C.c_int64),
         ("fp64_rechecks", C.c_int64), ("kernel_ms", C.c_double),
+        ("window_ms", C.c_double), ("slots", C.c_int64), ("launches", C.c_int64),
+        ("stage_ms", C.c_double * 8),
     ]
+
+    STAGES = ("gncc", "prep", "scan", "items", "ncc", "peaks", "recheck", "rescan")
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "stage_ms"}
+        d["stage_ms"] = dict(zip(self.STAGES, list(self.stage_ms)))
+        return d
 
 
 def ptr(a) -> int | None:

@@ -57,6 +57,8 @@ struct vll_context {
     Buf pre_tmp, pre_wt, pre_img, pre_mag, pre_ori;
     vll::SplitBuffers split;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t stage_ev[9] = {};
+    int64_t launches_total = 0;
     vll::DevLevel *hlevel = nullptr;   // pinned host staging of the level block
 };
 
@@ -296,26 +298,49 @@ int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
         VLL_CUDA(ctx, vll::launch_ortho(dP, P.ow * P.oh, dptr, dptr + VLL_MAX_IMAGES, ctx->stream));
     }
     unsigned long long *counters = (unsigned long long *)ctx->counters.p;
+    vll::SplitTiming tm;
+    tm.enabled = stats != nullptr;
+    int64_t launches = P.check_ortho ? 1 : 0;
+    bool split_ran = false;
+    if (tm.enabled && !ctx->stage_ev[0])
+        for (auto &ev : ctx->stage_ev) VLL_CUDA(ctx, cudaEventCreate(&ev));
+    for (int i = 0; i < 9; ++i) tm.ev[i] = ctx->stage_ev[i];
     if (kernel == VLL_KERNEL_FP64_PLAIN || !vll::split_supported(P)) {
+        if (kernel != VLL_KERNEL_FP64_PLAIN && kernel != VLL_KERNEL_SPLIT)
+            return fail(ctx, VLL_ERR_INVALID, "unknown kernel id");
         VLL_CUDA(ctx, vll::launch_plain(dP, P.n_nodes, counters, nullptr, nullptr, ctx->stream));
-    } else if (kernel == VLL_KERNEL_SPLIT) {
-        std::string err;
-        cudaError_t e = vll::run_split(ctx->split, P, dP, counters, ctx->stream, &err);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, err.c_str());
+        launches += 1;
     } else {
-        return fail(ctx, VLL_ERR_INVALID, "unknown kernel id");
+        std::string err;
+        cudaError_t e = vll::run_split(ctx->split, P, dP, counters, ctx->stream, &err, &tm);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, err.c_str());
+        launches += tm.launches;
+        split_ran = true;
     }
     VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
+    ctx->launches_total += launches;
     if (stats) {
         unsigned long long h[4];
         VLL_CUDA(ctx, cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
         VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         float ms = 0;
         VLL_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->e0, ctx->e1));
+        memset(stats, 0, sizeof(*stats));
         stats->accessable_grid = (int64_t)h[0];
         stats->evals = (int64_t)h[1];
         stats->fp64_rechecks = (int64_t)h[2];
         stats->kernel_ms = ms;
+        stats->launches = launches;
+        stats->window_ms = ms;
+        if (split_ran) {
+            for (int i = 0; i < 8; ++i) {
+                float t = 0;
+                cudaEventElapsedTime(&t, tm.ev[i], tm.ev[i + 1]);
+                stats->stage_ms[i] = t;
+            }
+            stats->window_ms = stats->stage_ms[4];
+            stats->slots = tm.slots;
+        }
         if (h[3] != 0) return fail(ctx, VLL_ERR_TIMEOUT, "persistent kernel reported an error flag");
     }
     return VLL_OK;
@@ -384,6 +409,8 @@ void vll_destroy(vll_context *ctx) {
     if (ctx->hlevel) cudaFreeHost(ctx->hlevel);
     if (ctx->e0) cudaEventDestroy(ctx->e0);
     if (ctx->e1) cudaEventDestroy(ctx->e1);
+    for (auto &ev : ctx->stage_ev)
+        if (ev) cudaEventDestroy(ev);
     if (ctx->stream && ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -406,6 +433,8 @@ int vll_set_stream(vll_context *ctx, void *stream) {
 }
 
 void *vll_get_stream(vll_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int64_t vll_launch_count(const vll_context *ctx) { return ctx ? ctx->launches_total : 0; }
 
 int64_t vll_voxel_count(const vll_nccresult *ncc, int64_t n) {
     if (!ncc || n <= 0) return 0;

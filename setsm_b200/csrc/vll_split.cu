@@ -727,8 +727,13 @@ void split_release(SplitBuffers &b) {
     } while (0)
 
 cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
-                      unsigned long long *counters, cudaStream_t s, std::string *err) {
+                      unsigned long long *counters, cudaStream_t s, std::string *err,
+                      SplitTiming *tm) {
     const int64_t N = P.n_nodes;
+    auto mark = [&](int i) {
+        if (tm && tm->enabled) cudaEventRecord(tm->ev[i], s);
+    };
+    int64_t launches = 0;
     size_t cap;
     // node-sized buffers
     if ((size_t)(N + 1) > b.cap_nodes) {
@@ -753,14 +758,19 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
     SPLIT_CUDA(cudaMemsetAsync(b.node_k, 0, (size_t)(N + 1) * sizeof(int32_t), s));
     SPLIT_CUDA(cudaMemsetAsync(b.item_cnt, 0, (size_t)(N + 1) * sizeof(int32_t), s));
     double *gsum = nullptr, *gcnt = nullptr;
+    mark(0);
     if (P.check_ortho) {
         gsum = (double *)b.gsum;
         gcnt = (double *)b.gcnt;
         SPLIT_CUDA(launch_gncc(dP, N, gsum, gcnt, s));
+        ++launches;
     }
+    mark(1);
     prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(dP, gsum, gcnt, (int32_t *)b.node_k,
                                                           (int32_t *)b.item_cnt, counters);
     SPLIT_CUDA(cudaGetLastError());
+    ++launches;
+    mark(2);
     // prefix sums (int32 counts -> int64 offsets)
     size_t tmp1 = 0, tmp2 = 0;
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp1, (const int32_t *)b.node_k,
@@ -775,6 +785,8 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
     tmp2 = b.cap_scan;
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp2, (const int32_t *)b.item_cnt,
                                              (int64_t *)b.item_off, (int)(N + 1), s));
+    launches += 4;   // two scans of two kernels each
+    mark(3);
     int64_t totals[2];
     SPLIT_CUDA(cudaMemcpyAsync(&totals[0], (int64_t *)b.slot_off + N, 8, cudaMemcpyDeviceToHost, s));
     SPLIT_CUDA(cudaMemcpyAsync(&totals[1], (int64_t *)b.item_off + N, 8, cudaMemcpyDeviceToHost, s));
@@ -800,6 +812,8 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
                                                                (const int64_t *)b.item_off,
                                                                (int64_t *)b.items);
         SPLIT_CUDA(cudaGetLastError());
+        ++launches;
+        mark(4);
         unsigned long long *queue = (unsigned long long *)b.ctl;
         cudaError_t e = cudaSuccess;
         switch (P.H) {
@@ -815,18 +829,33 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
             *err = "ncc_kernel launch";
             return e;
         }
+        ++launches;
+        mark(5);
         unsigned long long *ctl = (unsigned long long *)b.ctl;
         peaks_kernel<<<grid_1d(N, 128, 148 * 64), 128, 0, s>>>(
             dP, (const int64_t *)b.slot_off, (const float2 *)b.rho, (int64_t *)b.re_items,
             (int64_t)b.cap_re, (int64_t *)b.node_re, (int64_t *)b.pending, ctl, counters);
         SPLIT_CUDA(cudaGetLastError());
+        mark(6);
         SPLIT_CUDA(launch_recheck(dP, (const int64_t *)b.re_items, ctl + 1, (int64_t)b.cap_re, gsum,
                                   gcnt, (double *)b.re_out, s));
+        mark(7);
         rescan_kernel<<<148 * 8, 64, 0, s>>>(dP, (const int64_t *)b.slot_off, (const float2 *)b.rho,
                                              (const int64_t *)b.node_re, (const int64_t *)b.pending,
                                              (const int64_t *)b.re_items, (const double *)b.re_out,
                                              ctl);
         SPLIT_CUDA(cudaGetLastError());
+        launches += 3;
+    } else {
+        mark(4);
+        mark(5);
+        mark(6);
+        mark(7);
+    }
+    mark(8);
+    if (tm) {
+        tm->slots = n_slots;
+        tm->launches = launches;
     }
     return cudaSuccess;
 }

@@ -39,7 +39,16 @@ bool split_supported(const DevLevel &P);
 // Runs the split pipeline for a level whose DevLevel block is at dP (device)
 // and mirrored in P (host).  counters: [0] accessable, [1] evals,
 // [2] FP64 re-checks, [3] error flag.
+// Per-call timing / launch bookkeeping of the split pipeline.
+struct SplitTiming {
+    bool enabled = false;
+    cudaEvent_t ev[9] = {};
+    int64_t slots = 0;
+    int64_t launches = 0;
+};
+
 cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
-                      unsigned long long *counters, cudaStream_t s, std::string *err);
+                      unsigned long long *counters, cudaStream_t s, std::string *err,
+                      SplitTiming *timing);
 
 }  // namespace vll

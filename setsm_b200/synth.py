@@ -429,12 +429,16 @@ def ranges_uniform(grid: Grid, n_heights: int, step: float, sigma: float, seed: 
     return lo, hi, centre
 
 
-def ranges_tin(grid: Grid, n_seeds: int, k_min: int, k_max: int, step: float,
-               noise: float, seed: int):
+def ranges_tin(scene: Scene, grid: Grid, n_seeds: int, k_min: int, k_max: int, step: float,
+               noise: float, seed: int, lattice: int = 512, device="cpu"):
     """Per-node ranges from a coarse Delaunay TIN of jittered, noisy seeds.
 
-    The TIN interpolates a prior height at every node; the candidate count is
-    log-uniform in [k_min, k_max] at `step` metres.
+    The TIN (scipy Delaunay over ``n_seeds`` jittered lattice points whose
+    heights are the DEM plus N(0, noise)) is evaluated on a ``lattice`` x
+    ``lattice`` raster over the grid and bilinearly refined to every node,
+    which gives each node a prior height.  The candidate count is log-uniform
+    in [k_min, k_max] at ``step`` metres; ranges are whole metres (UGRID keeps
+    heights as short).  Returns (lo, hi, prior) as numpy arrays.
     """
     from scipy.spatial import Delaunay
 
@@ -448,20 +452,32 @@ def ranges_tin(grid: Grid, n_seeds: int, k_min: int, k_max: int, step: float,
     corners = np.array([[b[0], b[1]], [b[2], b[1]], [b[0], b[3]], [b[2], b[3]]])
     sx = np.concatenate([sx, corners[:, 0]])
     sy = np.concatenate([sy, corners[:, 1]])
-    # seed heights: truth at the seed + noise (nearest grid node)
-    ci = np.clip(((sx - b[0]) / grid.resolution).astype(np.int64), 0, grid.width - 1)
-    ri = np.clip(((sy - b[1]) / grid.resolution).astype(np.int64), 0, grid.height - 1)
-    sh = grid.truth[ri * grid.width + ci] + rng.normal(0.0, noise, sx.size)
+    sh = scene.dem_at(torch.tensor(sx, dtype=torch.float64, device=scene.dem.device),
+                      torch.tensor(sy, dtype=torch.float64, device=scene.dem.device)).cpu().numpy()
+    sh = sh + rng.normal(0.0, noise, sx.size)
     tri = Delaunay(np.stack([sx, sy], 1))
-    simplex = tri.find_simplex(grid.pts)
+    lx = np.linspace(b[0], b[2], lattice)
+    ly = np.linspace(b[1], b[3], lattice)
+    LX, LY = np.meshgrid(lx, ly)
+    q = np.stack([LX.ravel(), LY.ravel()], 1)
+    simplex = tri.find_simplex(q)
     simplex = np.where(simplex < 0, 0, simplex)
     T = tri.transform[simplex]
-    d = grid.pts - T[:, 2]
-    bary = np.einsum("nij,nj->ni", T[:, :2], d)
+    bary = np.einsum("nij,nj->ni", T[:, :2], q - T[:, 2])
     w3 = np.concatenate([bary, 1 - bary.sum(1, keepdims=True)], 1)
-    verts = tri.simplices[simplex]
-    prior = (w3 * sh[verts]).sum(1)
-    k = np.exp(rng.uniform(math.log(k_min), math.log(k_max), grid.truth.shape))
+    lat_prior = (w3 * sh[tri.simplices[simplex]]).sum(1).reshape(lattice, lattice)
+    # bilinear refinement to the node grid
+    dev = torch.device(device)
+    P = torch.tensor(lat_prior, dtype=torch.float64, device=dev)
+    u = (torch.tensor(grid.pts[:, 0], device=dev) - b[0]) / (b[2] - b[0]) * (lattice - 1)
+    v = (torch.tensor(grid.pts[:, 1], device=dev) - b[1]) / (b[3] - b[1]) * (lattice - 1)
+    u = u.clamp(0, lattice - 1.000001)
+    v = v.clamp(0, lattice - 1.000001)
+    iu, iv = torch.floor(u).long(), torch.floor(v).long()
+    fu, fv = u - iu, v - iv
+    prior = ((P[iv, iu] * (1 - fu) + P[iv, iu + 1] * fu) * (1 - fv)
+             + (P[iv + 1, iu] * (1 - fu) + P[iv + 1, iu + 1] * fu) * fv).cpu().numpy()
+    k = np.exp(rng.uniform(math.log(k_min), math.log(k_max), prior.shape))
     span = np.maximum(1, np.round(k * step)).astype(np.int64)
     lo = np.floor(prior - span / 2).astype(np.int64)
     hi = lo + span

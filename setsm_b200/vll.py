@@ -27,7 +27,7 @@ EXPORTED = [
     "vll_get_stream", "vll_voxel_count", "vll_vertical_line_locus",
     "vll_vertical_line_locus_device", "vll_awncc_peaks", "vll_preprocess_level",
     "vll_preprocess_level_device", "vll_pyramid_down", "vll_pyramid_down_device",
-    "vll_compat_layout",
+    "vll_compat_layout", "vll_launch_count",
 ]
 
 _lib = None
@@ -71,6 +71,8 @@ def load():
     L.vll_preprocess_level_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, i32, vp, vp]
     L.vll_pyramid_down.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
     L.vll_pyramid_down_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
+    L.vll_launch_count.argtypes = [vp]
+    L.vll_launch_count.restype = i64
     L.vll_compat_layout.argtypes = [vp, i32]
     L.vll_compat_layout.restype = i32
     _lib = L
@@ -113,6 +115,9 @@ class Context:
     def _check(self, rc: int) -> None:
         if rc != abi.VLL_OK:
             raise VLLError(rc, load().vll_last_error(self._h).decode())
+
+    def launch_count(self) -> int:
+        return int(load().vll_launch_count(self._h))
 
     def set_stream(self, stream_ptr: int | None) -> None:
         self._check(load().vll_set_stream(self._h, stream_ptr))
