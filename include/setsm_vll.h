@@ -221,6 +221,34 @@ void *vll_get_stream(vll_context *ctx);
 int64_t vll_launch_count(const vll_context *ctx);
 
 /*
+ * Allocation-free VerticalLineLocus.  This entry point has no counterpart in
+ * the reference; it exists for callers that cannot allocate device memory at
+ * call time (a pool allocator that owns the whole GPU, another framework's
+ * memory manager, a latency-critical loop that cannot absorb cudaMalloc's
+ * implicit synchronisation).  It runs the split-precision pipeline with every
+ * scratch buffer taken from one file-scope device array of 64 MiB that each
+ * GPU loading this library holds until process exit, and calls no
+ * cudaMalloc, cudaFree or allocating library routine; no vll_context is used.
+ *   - All pointers are DEVICE pointers (as for
+ *     vll_vertical_line_locus_device); `stream` is a cudaStream_t (NULL =
+ *     legacy default stream).  The call waits for its work to finish.
+ *   - Memory-tight route only (check_matching_rate = 1), stereo, levels
+ *     without orthoimage GNCC; anything else returns VLL_ERR_UNSUPPORTED.
+ *   - Grids whose nodes and height slots do not fit the 64 MiB array (roughly
+ *     55k nodes at ~120 slots each) return VLL_ERR_CAPACITY before any output
+ *     is written; `err_buf` receives a message.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Every call shares the one array, which keeps the previous call's
+ *     contents; calls that overlap on the GPU (different streams or threads
+ *     at the same time) race on it and must be serialised by the caller.
+ */
+int vll_vertical_line_locus_noalloc(const vll_level_desc *desc, const vll_ugrid *d_gridpt3,
+                                    vll_nccresult *d_nccresult, void *stream,
+                                    int64_t *accessable_grid, char *err_buf, int err_len);
+
+/*
  * Non-SGM peak loop of AWNCC (setsm_code.cpp:7511-7702) over the packed voxel
  * rows, on HOST buffers.  Selects first/second peaks per node exactly as the
  * reference does from quantised voxels and the node's GNCC.  Levels where the

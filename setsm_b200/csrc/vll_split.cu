@@ -20,6 +20,9 @@
 // The result is identical to the FP64 kernel's; FP32 only decides when it is
 // provably far enough from every boundary.
 #include <cfloat>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
 #include <cub/device/device_scan.cuh>
 
 #include "vll_exact.cuh"
@@ -861,3 +864,212 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
 }
 
 }  // namespace vll
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the split pipeline.
+//
+// Some callers cannot allocate device memory at call time: code running under
+// a memory pool that owns the whole device, inside another framework's
+// allocator, or in a real-time loop where cudaMalloc's implicit device
+// synchronisation is not acceptable.  vll_vertical_line_locus_noalloc runs the
+// same split pipeline with every scratch buffer carved out of the file-scope
+// array below, so it calls no cudaMalloc / cudaFree / allocating library
+// routine.  The array is kNoAllocScratchBytes (64 MiB) and every GPU that
+// loads this library holds it until the process exits.
+// ---------------------------------------------------------------------------
+namespace vll {
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[256] = {};
+
+// Device address of the scratch array for the current device, looked up once
+// per device (host code cannot use the symbol's address directly).
+cudaError_t noalloc_scratch(void **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+// Slot count per node without touching any output (same tests as prep_kernel
+// on the memory-tight route), so that capacity is checked before writing.
+__global__ void __launch_bounds__(256) noalloc_count_kernel(const DevLevel *__restrict__ Pp,
+                                                            int32_t *__restrict__ node_k,
+                                                            int32_t *__restrict__ item_cnt) {
+    const DevLevel &P = *Pp;
+    for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.n_nodes;
+         pt += (int64_t)gridDim.x * blockDim.x) {
+        int K = 0;
+        const vll_ugrid g = P.gp3[pt];
+        const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
+        if (check_image_boundary(P, lon, lat, (double)g.minHeight, (double)g.maxHeight, P.H) &&
+            !blunder_cell(P, g))
+            K = (uint16_t)(int)__ddiv_rn((double)(g.maxHeight - g.minHeight), P.height_step);
+        node_k[pt] = K;
+        item_cnt[pt] = (K + 31) / 32;
+    }
+}
+
+struct Carver {
+    unsigned char *base;
+    size_t used, cap;
+    void *take(size_t n) {
+        const size_t a = (used + 255) & ~(size_t)255;
+        if (a + n > cap) return nullptr;
+        used = a + n;
+        return base + a;
+    }
+};
+
+thread_local DevLevel g_noalloc_level_host;
+
+}  // namespace
+
+int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err);
+
+}  // namespace vll
+
+extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
+                                               const vll_ugrid *d_gridpt3,
+                                               vll_nccresult *d_nccresult, void *stream,
+                                               int64_t *accessable_grid, char *err_buf,
+                                               int err_len) {
+    using namespace vll;
+    auto fail = [&](int code, const char *msg) {
+        if (err_buf && err_len > 0) {
+            strncpy(err_buf, msg, (size_t)err_len - 1);
+            err_buf[err_len - 1] = 0;
+        }
+        return code;
+    };
+    if (!desc || !d_gridpt3 || !d_nccresult) return fail(VLL_ERR_INVALID, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    DevLevel &P = g_noalloc_level_host;
+    std::string err;
+    int rc = derive_level(desc, &P, &err);
+    if (rc) return fail(rc, err.c_str());
+    if (!P.cmr || P.check_ortho || !split_supported(P))
+        return fail(VLL_ERR_UNSUPPORTED,
+                    "the allocation-free call covers the memory-tight route of stereo levels "
+                    "without orthoimage GNCC");
+    P.gp3 = d_gridpt3;
+    P.ncc = d_nccresult;
+    P.vox = nullptr;
+    P.vox_off = nullptr;
+    void *base = nullptr;
+    if (noalloc_scratch(&base) != cudaSuccess)
+        return fail(VLL_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
+    const int64_t N = P.n_nodes;
+    Carver cv{(unsigned char *)base, 0, kNoAllocScratchBytes};
+    DevLevel *dP = (DevLevel *)cv.take(sizeof(DevLevel));
+    unsigned long long *ctl = (unsigned long long *)cv.take(8 * sizeof(unsigned long long));
+    unsigned long long *counters = (unsigned long long *)cv.take(4 * sizeof(unsigned long long));
+    int32_t *node_k = (int32_t *)cv.take((size_t)(N + 1) * 4);
+    int32_t *item_cnt = (int32_t *)cv.take((size_t)(N + 1) * 4);
+    int64_t *slot_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
+    int64_t *item_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
+    int64_t *node_re = (int64_t *)cv.take((size_t)(N + 1) * 8);
+    int64_t *pending = (int64_t *)cv.take((size_t)(N + 1) * 8);
+    size_t scan_bytes = 0;
+    if (cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int32_t *)node_k, slot_off,
+                                      (int)(N + 1), s) != cudaSuccess)
+        return fail(VLL_ERR_CUDA, "scan size query failed");
+    void *scan_tmp = cv.take(scan_bytes);
+    if (!dP || !ctl || !counters || !node_k || !item_cnt || !slot_off || !item_off || !node_re ||
+        !pending || !scan_tmp) {
+        char m[160];
+        snprintf(m, sizeof m, "grid of %lld nodes exceeds the %zu MiB scratch array",
+                 (long long)N, kNoAllocScratchBytes >> 20);
+        return fail(VLL_ERR_CAPACITY, m);
+    }
+#define NA_CUDA(call)                                                     \
+    do {                                                                  \
+        if ((call) != cudaSuccess) return fail(VLL_ERR_CUDA, #call);      \
+    } while (0)
+    NA_CUDA(cudaMemcpyAsync(dP, &P, sizeof(DevLevel), cudaMemcpyHostToDevice, s));
+    // the array keeps the previous call's contents: clear what must start at zero
+    NA_CUDA(cudaMemsetAsync(ctl, 0, 8 * sizeof(unsigned long long), s));
+    NA_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), s));
+    NA_CUDA(cudaMemsetAsync(node_k, 0, (size_t)(N + 1) * 4, s));
+    NA_CUDA(cudaMemsetAsync(item_cnt, 0, (size_t)(N + 1) * 4, s));
+    // capacity: count slots and items first, without writing any output
+    noalloc_count_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(dP, node_k, item_cnt);
+    NA_CUDA(cudaGetLastError());
+    size_t t1 = scan_bytes;
+    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)node_k, slot_off,
+                                          (int)(N + 1), s));
+    t1 = scan_bytes;
+    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
+                                          (int)(N + 1), s));
+    int64_t totals[2] = {0, 0};
+    NA_CUDA(cudaMemcpyAsync(&totals[0], slot_off + N, 8, cudaMemcpyDeviceToHost, s));
+    NA_CUDA(cudaMemcpyAsync(&totals[1], item_off + N, 8, cudaMemcpyDeviceToHost, s));
+    NA_CUDA(cudaStreamSynchronize(s));
+    const int64_t n_slots = totals[0], n_items = totals[1];
+    const int64_t max_re = N * 4 + 1024;
+    int64_t *items = (int64_t *)cv.take((size_t)(n_items > 0 ? n_items : 1) * 8);
+    float2 *rho = (float2 *)cv.take((size_t)(n_slots > 0 ? n_slots : 1) * sizeof(float2));
+    int64_t *re_items = (int64_t *)cv.take((size_t)max_re * 8);
+    double *re_out = (double *)cv.take((size_t)max_re * 2 * sizeof(double));
+    if (!items || !rho || !re_items || !re_out) {
+        char m[200];
+        snprintf(m, sizeof m,
+                 "%lld nodes with %lld height slots exceed the %zu MiB scratch array",
+                 (long long)N, (long long)n_slots, kNoAllocScratchBytes >> 20);
+        return fail(VLL_ERR_CAPACITY, m);
+    }
+    // the pipeline proper (same kernels and order as run_split)
+    NA_CUDA(cudaMemsetAsync(node_k, 0, (size_t)(N + 1) * 4, s));
+    NA_CUDA(cudaMemsetAsync(item_cnt, 0, (size_t)(N + 1) * 4, s));
+    prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(dP, nullptr, nullptr, node_k, item_cnt,
+                                                          counters);
+    NA_CUDA(cudaGetLastError());
+    t1 = scan_bytes;
+    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)node_k, slot_off,
+                                          (int)(N + 1), s));
+    t1 = scan_bytes;
+    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
+                                          (int)(N + 1), s));
+    if (n_items > 0) {
+        items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, item_cnt, item_off, items);
+        NA_CUDA(cudaGetLastError());
+        cudaError_t e = cudaSuccess;
+        switch (P.H) {
+            case 2: e = launch_ncc<2>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
+            case 3: e = launch_ncc<3>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
+            case 4: e = launch_ncc<4>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
+            case 5: e = launch_ncc<5>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
+            case 6: e = launch_ncc<6>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
+            case 7: e = launch_ncc<7>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
+            default: e = cudaErrorInvalidValue;
+        }
+        NA_CUDA(e);
+        peaks_kernel<<<grid_1d(N, 128, 148 * 64), 128, 0, s>>>(dP, slot_off, rho, re_items, max_re,
+                                                              node_re, pending, ctl, counters);
+        NA_CUDA(cudaGetLastError());
+        NA_CUDA(launch_recheck(dP, re_items, ctl + 1, max_re, nullptr, nullptr, re_out, s));
+        rescan_kernel<<<148 * 8, 64, 0, s>>>(dP, slot_off, rho, node_re, pending, re_items, re_out,
+                                             ctl);
+        NA_CUDA(cudaGetLastError());
+    }
+    unsigned long long acc = 0;
+    NA_CUDA(cudaMemcpyAsync(&acc, counters, sizeof(acc), cudaMemcpyDeviceToHost, s));
+    NA_CUDA(cudaStreamSynchronize(s));
+#undef NA_CUDA
+    if (accessable_grid) *accessable_grid = (int64_t)acc;
+    return VLL_OK;
+}
