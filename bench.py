@@ -302,7 +302,10 @@ def run_ours(args):
         "evals": evals_step[t], "ms": window_ms[t] / args.steps,
         "gbs": evals_step[t] * workloads.BYTES_PER_EVAL[t] / (window_ms[t] / args.steps / 1e3) / 1e9,
         "evals_per_s": evals_step[t] / (window_ms[t] / args.steps / 1e3),
-        "stage_ms": ref_stats[t].as_dict()["stage_ms"]} for t in templates}
+        "stage_ms": ref_stats[t].as_dict()["stage_ms"],
+        "exact_nodes": ref_stats[t].exact_nodes, "fp64_nodes": ref_stats[t].fp64_nodes,
+        "scan_rounds": ref_stats[t].scan_rounds, "fp64_rechecks": ref_stats[t].fp64_rechecks}
+        for t in templates}
 
     # ---- e2e through the host-buffer C ABI (pinned host memory) ----
     e2e = None

@@ -166,8 +166,11 @@ typedef struct vll_stats {
     double window_ms;            /* device time of the window (NCC) kernel  */
     int64_t slots;               /* height slots scheduled                  */
     int64_t launches;            /* kernels launched by the call            */
-    double stage_ms[8];          /* split pipeline: gncc, prep, scan, items,
-                                    ncc, peaks, recheck, rescan             */
+    double stage_ms[8];          /* split pipeline: gncc, prep, prefix sums,
+                                    items, window, scan, exact path, tail   */
+    int64_t exact_nodes;         /* split: nodes sent to the exact path     */
+    int64_t fp64_nodes;          /* split: nodes recomputed wholly in FP64  */
+    int64_t scan_rounds;         /* split: scan rounds on the exact path    */
 } vll_stats;
 
 typedef struct vll_context vll_context;
@@ -212,6 +215,20 @@ int vll_vertical_line_locus_device(vll_context *ctx, const vll_level_desc *desc,
                                    const vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
                                    vll_voxel *d_voxels, const int64_t *d_voxel_offsets,
                                    int kernel, vll_stats *stats);
+
+/* Diagnostics (memory-tight route): runs `kernel` on host inputs and returns
+ * the per-slot rho it computed, at offset prefix(K)[node] + slot where
+ * K = (int)((maxHeight - minHeight) / height_step) of each node's UGRID;
+ * slots that were not evaluated are NaN.  For VLL_KERNEL_SPLIT these are the
+ * FP32 values before any FP64 re-check; for VLL_KERNEL_FP64_PLAIN the exact
+ * FP64 temp_rho. */
+int vll_debug_slot_rho(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
+                       vll_nccresult *nccresult, int kernel, double *rho_out, int64_t capacity,
+                       uint64_t *diag_out);
+/* diag_out (optional, 16 entries, split kernel): cycles summed over warps in
+ * node setup, coordinates, staging, window, scan, re-check and fold, then
+ * counts of nodes, 32-slot passes, FP64 slow-path lanes, un-staged passes,
+ * whole-node FP64 fallbacks, scan rounds and re-checked slots. */
 
 /* Use `stream` (a cudaStream_t) for this context's work; NULL restores a
  * private stream.  vll_get_stream returns the stream in use. */

@@ -112,9 +112,10 @@ class Stats(C.Structure):
         ("fp64_rechecks", C.c_int64), ("kernel_ms", C.c_double),
         ("window_ms", C.c_double), ("slots", C.c_int64), ("launches", C.c_int64),
         ("stage_ms", C.c_double * 8),
+        ("exact_nodes", C.c_int64), ("fp64_nodes", C.c_int64), ("scan_rounds", C.c_int64),
     ]
 
-    STAGES = ("gncc", "prep", "scan", "items", "ncc", "peaks", "recheck", "rescan")
+    STAGES = ("gncc", "prep", "prefix", "items", "window", "scan", "exact", "tail")
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "stage_ms"}

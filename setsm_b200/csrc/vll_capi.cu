@@ -52,7 +52,7 @@ struct vll_context {
     std::string err;
     Buf level, counters;
     Buf img[VLL_MAX_IMAGES][6];
-    Buf wgs, pts, gp3, ncc, vox, voxoff;
+    Buf wgs, pts, gp3, ncc, vox, voxoff, gsum, gcnt;
     Buf ocd[VLL_MAX_IMAGES], ocdn[VLL_MAX_IMAGES], ocdptr;
     Buf pre_tmp, pre_wt, pre_img, pre_mag, pre_ori;
     vll::SplitBuffers split;
@@ -274,8 +274,8 @@ int upload_level_block(vll_context *ctx, const DevLevel &P) {
 int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
     int rc = run_ortho(ctx, &P, nullptr);
     if (rc) return rc;
-    VLL_CUDA(ctx, ensure(ctx->counters, 4 * sizeof(unsigned long long)));
-    VLL_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    VLL_CUDA(ctx, ensure(ctx->counters, 8 * sizeof(unsigned long long)));
+    VLL_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned long long), ctx->stream));
     rc = upload_level_block(ctx, P);
     if (rc) return rc;
     const DevLevel *dP = (const DevLevel *)ctx->level.p;
@@ -320,8 +320,12 @@ int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
     VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
     ctx->launches_total += launches;
     if (stats) {
-        unsigned long long h[4];
+        unsigned long long h[8];
         VLL_CUDA(ctx, cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        unsigned long long ctlh[4] = {0, 0, 0, 0};
+        if (split_ran && ctx->split.ctl)
+            VLL_CUDA(ctx, cudaMemcpyAsync(ctlh, ctx->split.ctl, sizeof(ctlh), cudaMemcpyDeviceToHost,
+                                          ctx->stream));
         VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         float ms = 0;
         VLL_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->e0, ctx->e1));
@@ -340,6 +344,9 @@ int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
             }
             stats->window_ms = stats->stage_ms[4];
             stats->slots = tm.slots;
+            stats->exact_nodes = (int64_t)ctlh[2];
+            stats->fp64_nodes = (int64_t)h[5];
+            stats->scan_rounds = (int64_t)h[6];
         }
         if (h[3] != 0) return fail(ctx, VLL_ERR_TIMEOUT, "persistent kernel reported an error flag");
     }
@@ -397,6 +404,8 @@ void vll_destroy(vll_context *ctx) {
     release(ctx->ncc);
     release(ctx->vox);
     release(ctx->voxoff);
+    release(ctx->gsum);
+    release(ctx->gcnt);
     for (auto &b : ctx->ocd) release(b);
     for (auto &b : ctx->ocdn) release(b);
     release(ctx->ocdptr);
@@ -535,6 +544,86 @@ int vll_vertical_line_locus_device(vll_context *ctx, const vll_level_desc *desc,
     P.vox = d_voxels;
     P.vox_off = d_voxel_offsets;
     return run_device(ctx, P, kernel, stats);
+}
+
+int vll_debug_slot_rho(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
+                       vll_nccresult *nccresult, int kernel, double *rho_out, int64_t capacity,
+                       uint64_t *diag_out) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !gridpt3 || !nccresult || !rho_out) return fail(ctx, VLL_ERR_INVALID, "null argument");
+    if (!desc->check_matching_rate)
+        return fail(ctx, VLL_ERR_UNSUPPORTED, "slot diagnostics cover the memory-tight route");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err);
+    if (rc) return fail(ctx, rc, err);
+    const int64_t N = P.n_nodes;
+    std::vector<int64_t> off((size_t)N + 1);
+    off[0] = 0;
+    for (int64_t i = 0; i < N; ++i) {
+        const int nh = (uint16_t)(int)((gridpt3[i].maxHeight - gridpt3[i].minHeight) / desc->height_step);
+        off[i + 1] = off[i] + nh;
+    }
+    if (capacity < off[N]) return fail(ctx, VLL_ERR_CAPACITY, "rho buffer too small");
+    for (int ti = 0; ti < P.num_images; ++ti) {
+        const vll_image_desc &s = desc->images[ti];
+        if (!s.selected) continue;
+        const size_t n = (size_t)s.width * s.height;
+        if ((rc = upload(ctx, ctx->img[ti][0], s.image, n * 2))) return rc;
+        if ((rc = upload(ctx, ctx->img[ti][1], s.mag, n * 2))) return rc;
+        if ((rc = upload(ctx, ctx->img[ti][2], s.ori, n))) return rc;
+        P.im[ti].img = (const uint16_t *)ctx->img[ti][0].p;
+        P.im[ti].mag = (const uint16_t *)ctx->img[ti][1].p;
+        P.im[ti].ori = (const uint8_t *)ctx->img[ti][2].p;
+    }
+    if ((rc = upload(ctx, ctx->wgs, desc->grid_wgs, (size_t)N * 16))) return rc;
+    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
+    P.grid_wgs = (const double *)ctx->wgs.p;
+    P.grid_pts = (const double *)ctx->pts.p;
+    P.gp3 = (const vll_ugrid *)ctx->gp3.p;
+    P.ncc = (vll_nccresult *)ctx->ncc.p;
+    Buf dbg, dbgoff;
+    VLL_CUDA(ctx, ensure(dbg, (size_t)off[N] * sizeof(double)));
+    VLL_CUDA(ctx, cudaMemsetAsync(dbg.p, 0xff, (size_t)off[N] * sizeof(double), ctx->stream));
+    rc = upload(ctx, dbgoff, off.data(), off.size() * sizeof(int64_t));
+    if (rc) return rc;
+    Buf diag;
+    if (kernel == VLL_KERNEL_SPLIT) {
+        P.dbg_rho = (double *)dbg.p;
+        P.dbg_off = (const int64_t *)dbgoff.p;
+        if (diag_out) {
+            VLL_CUDA(ctx, ensure(diag, 16 * sizeof(unsigned long long)));
+            VLL_CUDA(ctx, cudaMemsetAsync(diag.p, 0, 16 * sizeof(unsigned long long), ctx->stream));
+            P.diag = (unsigned long long *)diag.p;
+        }
+        rc = run_device(ctx, P, kernel, nullptr);
+        if (!rc && diag_out) {
+            VLL_CUDA(ctx, cudaMemcpyAsync(diag_out, diag.p, 16 * sizeof(unsigned long long),
+                                          cudaMemcpyDeviceToHost, ctx->stream));
+        }
+    } else {
+        VLL_CUDA(ctx, ensure(ctx->counters, 8 * sizeof(unsigned long long)));
+        VLL_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned long long), ctx->stream));
+        rc = upload_level_block(ctx, P);
+        if (!rc)
+            VLL_CUDA(ctx, vll::launch_plain((const DevLevel *)ctx->level.p, N,
+                                            (unsigned long long *)ctx->counters.p, (double *)dbg.p,
+                                            (const int64_t *)dbgoff.p, ctx->stream));
+    }
+    if (!rc) {
+        VLL_CUDA(ctx, cudaMemcpyAsync(rho_out, dbg.p, (size_t)off[N] * sizeof(double),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->ncc.p, (size_t)N * sizeof(vll_nccresult),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    release(dbg);
+    release(dbgoff);
+    release(diag);
+    return rc;
 }
 
 int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,

@@ -60,6 +60,13 @@ struct DevLevel {
     const double2 *ocd[VLL_MAX_IMAGES];
     const double2 *ocd_n[VLL_MAX_IMAGES];
     int64_t ow, oh, own, ohn;
+    // diagnostics: per-slot rho as computed by the kernel (FP32 values before
+    // any FP64 re-check in the split kernel), at dbg_off[node] + slot
+    double *dbg_rho;
+    const int64_t *dbg_off;
+    // diagnostics: per-phase cycle totals and event counts of the split
+    // kernel (see fused::Diag), or nullptr
+    unsigned long long *diag;
     vll_transparam param;
     double rot_cos[kRotTable];      // cos(-theta) for diff_theta = (i-kRotOffset)/2
     double rot_sin[kRotTable];

@@ -1,25 +1,33 @@
-// vll_split.cu -- split-precision VerticalLineLocus (setsm_code.cpp:6049-6548).
+// vll_split.cu -- split-precision VerticalLineLocus (setsm_code.cpp:6049-6548
+// with FindPeakNcc, :6672-6752).
 //
-// Pipeline for one level (all on one stream, no host round trips):
+// Pipeline for one level, all on one stream:
 //   gncc    FP64 GNCC per node (height independent), when the level uses it
 //   prep    per node: image-boundary and blunder tests, the nccresult fields
 //           VerticalLineLocus sets before its height loop, slot count K
 //   scan    exclusive prefix sums -> slot offsets and (node, 32-slot) items
-//   ncc     persistent kernel draining the item queue: one warp per item,
-//           one lane per height slot.  FP64 RPC projection; the warp's
-//           window footprints in both images are staged in shared memory as
-//           FP32 (intensity, magnitude) texel pairs; bilinear sampling and
-//           shifted (mean-centred) window sums in FP32; per-slot rho.
-//   peaks   ordered FindPeakNcc scan per node over the FP32 rho; any decision
-//           whose FP32 inputs lie inside the error band (direction ties,
-//           rounding / truncation boundaries, variance threshold) queues the
-//           slots involved for exact re-evaluation
-//   recheck FP64 re-evaluation of the queued slots (the plain kernel's code)
-//   rescan  the scan again with the exact values; a node whose outcome still
-//           depends on an unverified FP32 value is recomputed entirely in FP64
-// The result is identical to the FP64 kernel's; FP32 only decides when it is
-// provably far enough from every boundary.
+//   window  persistent kernel draining the item queue: one warp per item,
+//           one lane per height slot.  The RPC numerators / denominators are
+//           cubics in the normalised height per node (FP64, Horner), with the
+//           reference-order RPC wherever a coordinate lies within 1e-7 px of
+//           an integer or a clamp, so every integer decision (orientation
+//           pixel, image bounds) equals the reference's.  The warp's window
+//           footprints in both images are staged in shared memory as FP32
+//           texel pairs; bilinear sampling and window sums in FP32, each sum
+//           centred on its window's centre sample -> per-slot rho (float2:
+//           rho, INCC average or NaN when FP32 cannot decide a variance test).
+//   peaks   one warp per node: the FindPeakNcc scan, warp-parallel (a slot's
+//           direction and whether its predecessor is a peak depend only on
+//           neighbouring evaluated values); every decision whose FP32 inputs
+//           lie within kBand of a boundary (direction ties, sign tests,
+//           rounding of a top-two peak or of the maximum, truncation of a
+//           voxel) marks the slots involved, which the warp re-evaluates in
+//           exact FP64 (the reference's operation order) before repeating the
+//           scan; then the ordered top-two fold and the nccresult write.
+// The outputs are identical to the FP64 kernel's.
+#include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -28,15 +36,18 @@
 #include "vll_exact.cuh"
 #include "vll_internal.h"
 #include "vll_split.h"
+#include "vll_window.cuh"
 
 namespace vll {
 
-// Half-width of the FP32 error band in rho units.  The measured FP32-vs-FP64
-// error of rho is below 2e-6; decisions closer than this to a boundary are
-// settled in FP64.
-constexpr float kBand = 2e-5f;
-constexpr int kMaxRecheck = 32;         // per node, beyond which the node is redone in FP64
-constexpr int kFullRedo = 255;
+// Half-width of the FP32 error band of rho.  The measured FP32-vs-FP64 error
+// of rho is below 6e-7 (tests/test_gpu_accuracy.py); decisions closer than
+// this to a boundary are settled in FP64.
+constexpr float kBand = 2e-6f;
+constexpr double kEdge = 1e-7;          // coordinate distance to an integer / clamp
+constexpr int kSlotCap = 512;           // slots per node the peak kernel holds in shared memory
+constexpr int kExactCap = 64;           // exact slot values per node before a full FP64 pass
+constexpr int kMaxRounds = 3;           // scan / re-check rounds before a full FP64 pass
 
 // Per-slot markers in the rho buffer (.x):
 constexpr float kNotEvaluated = INFINITY;    // slot skipped (range / image bounds)
@@ -102,186 +113,102 @@ __global__ void __launch_bounds__(256) items_kernel(int64_t n, const int32_t *__
 }
 
 // ---------------------------------------------------------------------------
-// ncc: the FP32 window kernel
+// geometry helpers of the window kernel
 // ---------------------------------------------------------------------------
-// Ring of a window offset: 2 = innermost sub-window, 1 = middle, 0 = outer.
-__host__ __device__ constexpr int ring_of(int H, int row, int col) {
-    const int r2 = row * row + col * col;
-    const int s1 = H / 2;
-    const int s2 = s1 + (int)((s1 / 2.0) + 0.5);
-    const bool w1 = r2 <= (H - s1 + 1) * (H - s1 + 1) && row >= -H + s1 && row <= H - s1 &&
-                    col >= -H + s1 && col <= H - s1;
-    const bool w2 = r2 <= (H - s2 + 1) * (H - s2 + 1) && row >= -H + s2 && row <= H - s2 &&
-                    col >= -H + s2 && col <= H - s2;
-    return w2 ? 2 : (w1 ? 1 : 0);
+// Per-node RPC: normalised L, P (with the reference's +-360 wrap) and the
+// four cubics in the normalised height.  RPC00B terms grouped by power of H:
+//   a0: 1 L P LP LL PP LLL LPP LLP PPP   a1: H LH PH PLH LLH PPH
+//   a2: HH LHH PHH                        a3: HHH
+__device__ __forceinline__ void node_horner(const double *rpc, double lon, double lat, double *coef4x4,
+                            double *hn) {
+    double L = (lon - rpc[2]) / rpc[7];
+    double P = (lat - rpc[3]) / rpc[8];
+    if (L < -10.0 || L > 10.0) {
+        const double X = lon > 0 ? lon - 360 : lon + 360;
+        L = (X - rpc[2]) / rpc[7];
+    }
+    if (P < -10.0 || P > 10.0) {
+        const double Y = lat > 0 ? lat - 360 : lat + 360;
+        P = (Y - rpc[3]) / rpc[8];
+    }
+    for (int j = 0; j < 4; ++j) {
+        const double *c = rpc + 10 + 20 * j;
+        double *a = coef4x4 + 4 * j;
+        a[0] = c[0] + c[1] * L + c[2] * P + c[4] * L * P + c[7] * L * L + c[8] * P * P +
+               c[11] * L * L * L + c[12] * L * P * P + c[14] * L * L * P + c[15] * P * P * P;
+        a[1] = c[3] + c[5] * L + c[6] * P + c[10] * P * L + c[17] * L * L + c[18] * P * P;
+        a[2] = c[9] + c[13] * L + c[16] * P;
+        a[3] = c[19];
+    }
+    hn[0] = rpc[4];
+    hn[1] = rpc[9];
 }
 
-__host__ __device__ constexpr int ring_count(int H, int ring) {
-    int n = 0;
-    for (int row = -H; row <= H; ++row)
-        for (int col = -H; col <= H; ++col)
-            if (row * row + col * col <= (H + 1) * (H + 1) && ring_of(H, row, col) == ring) ++n;
-    return n;
+// Image coordinate (pyramid level) of one slot from the per-node cubics.
+// Sets `edge` when a coordinate is too close to an integer, or to a clamp,
+// for the Horner rounding to be trusted with the reference's integer tests.
+__device__ __forceinline__ double2 fast_coord(const double (*a)[4], const double *hn,
+                                              const DevImage &im, double hgt, int L, bool &edge) {
+    const double H = (hgt - hn[0]) / hn[1];
+    double v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = fma(fma(fma(a[j][3], H, a[j][2]), H, a[j][1]), H, a[j][0]);
+    double y = im.adj[0] + ((v[0] / v[1]) * im.rpc[5] + im.rpc[0]);
+    double x = im.adj[1] + ((v[2] / v[3]) * im.rpc[6] + im.rpc[1]);
+    const double ymax = im.rpc[0] + im.rpc[5] * 1.2, xmax = im.rpc[1] + im.rpc[6] * 1.2;
+    if (fabs(y) < kEdge || fabs(y - ymax) < kEdge || fabs(x) < kEdge || fabs(x - xmax) < kEdge)
+        edge = true;
+    y = y < 0 ? 0 : (y > ymax ? ymax : y);
+    x = x < 0 ? 0 : (x > xmax ? xmax : x);
+    const double s = (double)(1 << L);
+    const double px = x / s - im.sx, py = y / s - im.sy;
+    const double fx = px - floor(px), fy = py - floor(py);
+    if (fx < kEdge || fx > 1.0 - kEdge || fy < kEdge || fy > 1.0 - kEdge) edge = true;
+    return make_double2(px, py);
 }
 
-// floor and fraction of a small float with full-rate ALU ops only:
-// round-to-nearest of (x - 0.5) through the 1.5*2^23 magic constant.
-__device__ __forceinline__ int floor_frac(float x, float &frac) {
-    const float t = __fadd_rn(__fadd_rn(x, -0.5f), 12582912.0f);
-    const float r = __fadd_rn(t, -12582912.0f);
-    frac = x - r;
-    return __float_as_int(t) - 0x4B400000;
+__device__ __forceinline__ bool near_round(double v) {
+    const double x = v * 1000.0;
+    return fabs(x - floor(x) - 0.5) < (double)kBand * 1000.0;
+}
+__device__ __forceinline__ bool near_trunc(double v) {
+    const double x = v * 1000.0;
+    return fabs(x - rint(x)) < (double)kBand * 1000.0;
 }
 
-struct Acc {
-    float sl, sr, sll, srr, slr;
+
+// ---------------------------------------------------------------------------
+// window kernel
+// ---------------------------------------------------------------------------
+constexpr int kWinWarps = 4;
+
+struct WinShared {
+    double horner[2][4][4];          // [image][num/den poly][a0..a3]
+    double hnorm[2][2];              // [image] {h_off, h_scale}
 };
 
-// Pearson rho from shifted sums; returns -99 when a variance is below the
-// reference's 1e-8 threshold and flags results whose variance is too small
-// for FP32 to decide that threshold safely.
-__device__ __forceinline__ float corr_from(const Acc &a, float n, bool &unsure) {
-    const float inv = 1.0f / n;
-    const float vl = a.sll - a.sl * a.sl * inv;
-    const float vr = a.srr - a.sr * a.sr * inv;
-    const float cv = a.slr - a.sl * a.sr * inv;
-    // FP32 relative error of vl is ~n * 6e-8 * (sll / vl); treat anything
-    // within a factor of the threshold, or heavily cancelled, as uncertain.
-    if (vl < 1e-3f * a.sll + 1e-4f || vr < 1e-3f * a.srr + 1e-4f) unsure = true;
-    if (!(vl > 1e-8f && vr > 1e-8f)) return -99.0f;
-    return cv * rsqrtf(vl * vr);
+__host__ __device__ constexpr size_t win_boxes_offset() {
+    return (sizeof(WinShared) * kWinWarps + 15) & ~(size_t)15;
 }
 
 template <int H>
-__device__ __forceinline__ void window_fp32(const float4 *__restrict__ qr, int rbw, float rfx,
-                                            float rfy, const float4 *__restrict__ qt, int tbw,
-                                            float tfx, float tfy, float c, float s, float &incc_avg,
-                                            bool &unsure) {
-    Acc acc[3][2];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int p = 0; p < 2; ++p) acc[r][p] = Acc{0.f, 0.f, 0.f, 0.f, 0.f};
-    const float w00 = (1.f - rfx) * (1.f - rfy), w10 = rfx * (1.f - rfy);
-    const float w01 = (1.f - rfx) * rfy, w11 = rfx * rfy;
-#pragma unroll
-    for (int row = -H; row <= H; ++row) {
-        const float4 *q0 = qr + (row + H) * rbw;
-        const float4 *q1 = q0 + rbw;
-        const float bx = fmaf(-s, (float)row, tfx);
-        const float by = fmaf(c, (float)row, tfy);
-#pragma unroll
-        for (int col = -H; col <= H; ++col) {
-            if (row * row + col * col > (H + 1) * (H + 1)) continue;
-            const int ring = ring_of(H, row, col);
-            const float4 a = q0[col + H];
-            const float4 b = q1[col + H];
-            const float lI = fmaf(w11, b.z, fmaf(w01, b.x, fmaf(w10, a.z, w00 * a.x)));
-            const float lM = fmaf(w11, b.w, fmaf(w01, b.y, fmaf(w10, a.w, w00 * a.y)));
-            const float fx = fmaf(c, (float)col, bx);
-            const float fy = fmaf(s, (float)col, by);
-            float frx, fry;
-            const int ix = floor_frac(fx, frx);
-            const int iy = floor_frac(fy, fry);
-            const float4 *t = qt + iy * tbw + ix;
-            const float4 ta = t[0];
-            const float4 tb = t[tbw];
-            const float topI = fmaf(frx, ta.z - ta.x, ta.x);
-            const float botI = fmaf(frx, tb.z - tb.x, tb.x);
-            const float rI = fmaf(fry, botI - topI, topI);
-            const float topM = fmaf(frx, ta.w - ta.y, ta.y);
-            const float botM = fmaf(frx, tb.w - tb.y, tb.y);
-            const float rM = fmaf(fry, botM - topM, topM);
-            Acc &x = acc[ring][0];
-            x.sl += lI;
-            x.sr += rI;
-            x.sll = fmaf(lI, lI, x.sll);
-            x.srr = fmaf(rI, rI, x.srr);
-            x.slr = fmaf(lI, rI, x.slr);
-            Acc &y = acc[ring][1];
-            y.sl += lM;
-            y.sr += rM;
-            y.sll = fmaf(lM, lM, y.sll);
-            y.srr = fmaf(rM, rM, y.srr);
-            y.slr = fmaf(lM, rM, y.slr);
-        }
-    }
-    // nested windows: 2 = ring 2; 1 = rings 1+2; 0 = all rings
-    constexpr int n2 = ring_count(H, 2);
-    constexpr int n1 = n2 + ring_count(H, 1);
-    constexpr int n0 = n1 + ring_count(H, 0);
-    float tot = 0.f;
-    int nv = 0;
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-        Acc w = acc[2][p];
-        const float r2 = corr_from(w, (float)n2, unsure);
-        w.sl += acc[1][p].sl;
-        w.sr += acc[1][p].sr;
-        w.sll += acc[1][p].sll;
-        w.srr += acc[1][p].srr;
-        w.slr += acc[1][p].slr;
-        const float r1 = corr_from(w, (float)n1, unsure);
-        w.sl += acc[0][p].sl;
-        w.sr += acc[0][p].sr;
-        w.sll += acc[0][p].sll;
-        w.srr += acc[0][p].srr;
-        w.slr += acc[0][p].slr;
-        const float r0 = corr_from(w, (float)n0, unsure);
-        if (r0 != -99.0f) { tot += r0; ++nv; }
-        if (r1 != -99.0f) { tot += r1; ++nv; }
-        if (r2 != -99.0f) { tot += r2; ++nv; }
-    }
-    // count_incc is 1 when any of the six correlations is defined
-    incc_avg = nv > 0 ? tot / (float)nv : -1.0f;
-    if (nv == 0) incc_avg = -2.0f;   // no valid correlation: count_incc stays 0
-}
-
-struct ItemCtx {
-    int64_t node;
-    int k0;
-    int K;
-};
-
-// Stages the texel pairs of box [x0, x0+bw) x [y0, y0+bh) of one image into
-// shared memory as float4 {I(x)-sI, M(x)-sM, I(x+1)-sI, M(x+1)-sM}; returns
-// true (warp-uniform) when some intensity texel in the box is zero.
-__device__ __forceinline__ bool stage_box(float4 *__restrict__ dst, const uint16_t *__restrict__ I,
-                                          const uint16_t *__restrict__ M, uint32_t W, int x0, int y0,
-                                          int bw, int bh, float sI, float sM, int lane) {
-    bool zero = false;
-    const int n = bw * bh;
-    for (int i = lane; i < n; i += 32) {
-        const int by = i / bw;
-        const int bx = i - by * bw;
-        const int64_t p = (int64_t)(y0 + by) * W + (x0 + bx);
-        const uint16_t a = __ldg(I + p), b = __ldg(I + p + 1);
-        const uint16_t cm = __ldg(M + p), d = __ldg(M + p + 1);
-        zero |= (a == 0) | (b == 0);
-        dst[i] = make_float4((float)a - sI, (float)cm - sM, (float)b - sI, (float)d - sM);
-    }
-    return __any_sync(0xffffffffu, zero);
-}
-
-template <int H>
-__global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ Pp,
-                                                  const int64_t *__restrict__ items, int64_t n_items,
-                                                  const int64_t *__restrict__ slot_off,
-                                                  const double *__restrict__ gsum,
-                                                  const double *__restrict__ gcnt,
-                                                  float2 *__restrict__ rho,
-                                                  unsigned long long *__restrict__ counters,
-                                                  unsigned long long *__restrict__ queue,
-                                                  int warp_quads) {
-    extern __shared__ float4 smem[];
+__global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
+    const DevLevel *__restrict__ Pp, const int64_t *__restrict__ items, int64_t n_items,
+    const int64_t *__restrict__ slot_off, const double *__restrict__ gsum,
+    const double *__restrict__ gcnt, float2 *__restrict__ rho,
+    unsigned long long *__restrict__ counters, unsigned long long *__restrict__ queue,
+    int warp_quads) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const DevLevel &P = *Pp;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float4 *sw = smem + (size_t)warp * warp_quads;
+    WinShared &W = reinterpret_cast<WinShared *>(smem_raw)[warp];
+    float4 *boxes = reinterpret_cast<float4 *>(smem_raw + win_boxes_offset()) + (size_t)warp * warp_quads;
     const DevImage &ri = P.im[P.ref];
     const DevImage &tI = P.im[1];
     PatchSrc S, Sn;
     make_src(P, 1, S, Sn);
+    const bool voxels = P.vox && !P.cmr && !P.is_ra;
     unsigned long long evals = 0;
     constexpr int kGrab = 4;
     for (;;) {
@@ -301,8 +228,22 @@ __global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ P
             const vll_ugrid gg = P.gp3[pt];
             const int start_H = gg.minHeight, end_H = gg.maxHeight;
             const int ncc_min = P.ncc[pt].minHeight;
+            const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
             const double cnt_g = gcnt ? gcnt[pt] : 0.0, sum_g = gsum ? gsum[pt] : 0.0;
-            // ---- per-lane geometry (FP64) ----
+            // per-node RPC cubics: lanes 0..7 = (image, polynomial)
+            if (lane < 8) {
+                const int im = lane >> 2, j = lane & 3;
+                const double *rpc = (im == 0 ? ri : tI).rpc;
+                double cf[16], hn[2];
+                node_horner(rpc, lon, lat, cf, hn);
+                for (int q = 0; q < 4; ++q) W.horner[im][j][q] = cf[4 * j + q];
+                if (j == 0) {
+                    W.hnorm[im][0] = hn[0];
+                    W.hnorm[im][1] = hn[1];
+                }
+            }
+            __syncwarp();
+            // ---- per-lane geometry ----
             int status = 0;   // 0 idle/skip, 1 orientation reject, 2 evaluate
             double2 rp = make_double2(0, 0), tp = make_double2(0, 0);
             int rot = kRotOffset;
@@ -310,9 +251,13 @@ __global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ P
             if (k < K) {
                 hgt = slot_height(P, start_H, ncc_min, k);
                 if (hgt >= (float)start_H && hgt <= (float)end_H) {
-                    const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
-                    rp = to_pyramid(rpc_project(ri.rpc, ri.adj, lon, lat, (double)hgt), ri.sx, ri.sy, P.L);
-                    tp = to_pyramid(rpc_project(tI.rpc, tI.adj, lon, lat, (double)hgt), tI.sx, tI.sy, P.L);
+                    bool edge = false;
+                    rp = fast_coord(W.horner[0], W.hnorm[0], ri, (double)hgt, P.L, edge);
+                    tp = fast_coord(W.horner[1], W.hnorm[1], tI, (double)hgt, P.L, edge);
+                    if (edge) {
+                        rp = to_pyramid(rpc_project(ri.rpc, ri.adj, lon, lat, (double)hgt), ri.sx, ri.sy, P.L);
+                        tp = to_pyramid(rpc_project(tI.rpc, tI.adj, lon, lat, (double)hgt), tI.sx, tI.sy, P.L);
+                    }
                     if (in_image(rp, ri.w, ri.h) && in_image(tp, tI.w, tI.h)) {
                         const int od = (int)ri.ori[(int64_t)(int)rp.y * ri.w + (int)rp.x] -
                                        (int)tI.ori[(int64_t)(int)tp.y * tI.w + (int)tp.x];
@@ -331,9 +276,9 @@ __global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ P
             const int rix = (int)floor(rp.x), riy = (int)floor(rp.y);
             const int tix = (int)floor(tp.x), tiy = (int)floor(tp.y);
             const int R = (int)ceilf((fabsf(cf) + fabsf(sf)) * (float)H) + 1;
-            bool inside = status == 2 && rix - H >= 0 && riy - H >= 0 &&
-                          rix + H + 2 < (int)ri.w && riy + H + 2 < (int)ri.h && tix - R >= 0 &&
-                          tiy - R >= 0 && tix + R + 2 < (int)tI.w && tiy + R + 2 < (int)tI.h;
+            const bool inside = status == 2 && rix - H >= 0 && riy - H >= 0 &&
+                                rix + H + 2 < (int)ri.w && riy + H + 2 < (int)ri.h && tix - R >= 0 &&
+                                tiy - R >= 0 && tix + R + 2 < (int)tI.w && tiy + R + 2 < (int)tI.h;
             int rx0 = inside ? rix - H : INT_MAX, ry0 = inside ? riy - H : INT_MAX;
             int rx1 = inside ? rix + H + 1 : INT_MIN, ry1 = inside ? riy + H + 1 : INT_MIN;
             int tx0 = inside ? tix - R : INT_MAX, ty0 = inside ? tiy - R : INT_MAX;
@@ -349,33 +294,30 @@ __global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ P
                 tx1 = max(tx1, __shfl_xor_sync(0xffffffffu, tx1, o));
                 ty1 = max(ty1, __shfl_xor_sync(0xffffffffu, ty1, o));
             }
-            const bool any_inside = __any_sync(0xffffffffu, inside);
             bool staged = false;
-            int rbw = 0, tbw = 0;
-            if (any_inside) {
+            int rbw = 0, rbh = 0, tbw = 0;
+            if (__any_sync(0xffffffffu, inside)) {
                 rbw = rx1 - rx0 + 1;
-                const int rbh = ry1 - ry0 + 1;
+                rbh = ry1 - ry0 + 1;
                 tbw = tx1 - tx0 + 1;
                 const int tbh = ty1 - ty0 + 1;
                 if (rbw * rbh + tbw * tbh <= warp_quads) {
-                    // shift: texel at the centre of the reference box
                     float sI = 0.f, sM = 0.f, tsI = 0.f, tsM = 0.f;
                     if (lane == 0) {
                         const int64_t pc = (int64_t)(ry0 + rbh / 2) * ri.w + (rx0 + rbw / 2);
                         sI = (float)__ldg(ri.img + pc);
                         sM = (float)__ldg(ri.mag + pc);
-                        const int64_t pt2 = (int64_t)(ty0 + tbh / 2) * tI.w + (tx0 + tbw / 2);
-                        tsI = (float)__ldg(tI.img + pt2);
-                        tsM = (float)__ldg(tI.mag + pt2);
+                        const int64_t p2 = (int64_t)(ty0 + tbh / 2) * tI.w + (tx0 + tbw / 2);
+                        tsI = (float)__ldg(tI.img + p2);
+                        tsM = (float)__ldg(tI.mag + p2);
                     }
                     sI = __shfl_sync(0xffffffffu, sI, 0);
                     sM = __shfl_sync(0xffffffffu, sM, 0);
                     tsI = __shfl_sync(0xffffffffu, tsI, 0);
                     tsM = __shfl_sync(0xffffffffu, tsM, 0);
-                    __syncwarp();
-                    const bool z1 = stage_box(sw, ri.img, ri.mag, ri.w, rx0, ry0, rbw, rbh, sI, sM, lane);
-                    const bool z2 = stage_box(sw + rbw * rbh, tI.img, tI.mag, tI.w, tx0, ty0, tbw, tbh,
-                                              tsI, tsM, lane);
+                    const bool z1 = stage_box(boxes, ri.img, ri.mag, ri.w, rx0, ry0, rbw, rbh, sI, sM, lane);
+                    const bool z2 = stage_box(boxes + rbw * rbh, tI.img, tI.mag, tI.w, tx0, ty0, tbw,
+                                              tbh, tsI, tsM, lane);
                     __syncwarp();
                     staged = !(z1 || z2);
                 }
@@ -388,17 +330,16 @@ __global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ P
                 if (staged && inside) {
                     float incc;
                     bool unsure = false;
-                    window_fp32<H>(sw + (riy - H - ry0) * rbw + (rix - H - rx0), rbw,
+                    window_fp32<H>(boxes + (riy - H - ry0) * rbw + (rix - H - rx0), rbw,
                                    (float)(rp.x - (double)rix), (float)(rp.y - (double)riy),
-                                   sw + rbw * (ry1 - ry0 + 1) + (tiy - ty0) * tbw + (tix - tx0), tbw,
+                                   boxes + rbw * rbh + (tiy - ty0) * tbw + (tix - tx0), tbw,
                                    (float)(tp.x - (double)tix), (float)(tp.y - (double)tiy), cf, sf,
                                    incc, unsure);
-                    double rho_d;
-                    const double incc_d = incc == -2.0f ? -1.0 : (double)incc;
                     const bool has = incc != -2.0f;
+                    const double incc_d = has ? (double)incc : -1.0;
+                    double rho_d;
                     if (P.check_ortho && cnt_g > 0)
-                        rho_d = has ? incc_d * P.alpha + __ddiv_rn(sum_g, cnt_g) * P.beta
-                                    : __ddiv_rn(0.0, 0.0);
+                        rho_d = has ? incc_d * P.alpha + (sum_g / cnt_g) * P.beta : __ddiv_rn(0.0, 0.0);
                     else
                         rho_d = incc_d;
                     rho_v = (float)rho_d;
@@ -413,12 +354,13 @@ __global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ P
                 evals++;
             }
             if (k < K) rho[so + k] = make_float2(rho_v, incc_v);
-            if (k < K && P.vox && !P.cmr && !P.is_ra) {
+            if (P.dbg_rho && status == 2) P.dbg_rho[P.dbg_off[pt] + k] = (double)rho_v;
+            if (k < K && voxels) {
                 vll_voxel *v = P.vox + P.vox_off[pt] + k;
                 if (status == 1) v->flag_cal = 0;
                 if (status == 2) {
                     if (all_pos) v->flag_cal = 1;
-                    v->INCC = q_voxel((double)incc_v);
+                    v->INCC = q_voxel(isnan(incc_v) ? 0.0 : (double)incc_v);
                 }
             }
             __syncwarp();
@@ -429,100 +371,71 @@ __global__ void __launch_bounds__(128) ncc_kernel(const DevLevel *__restrict__ P
 }
 
 // ---------------------------------------------------------------------------
-// peaks / rescan
+// scan kernel: one thread per node over the FP32 slot values
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool near_round(double v) {
-    const double x = v * 1000.0;
-    return fabs(x - floor(x) - 0.5) < (double)kBand * 1000.0;
-}
-__device__ __forceinline__ bool near_trunc(double v) {
-    const double x = v * 1000.0;
-    return fabs(x - rint(x)) < (double)kBand * 1000.0;
-}
-
-struct Overrides {
-    int n;
-    int k[kMaxRecheck];
-    double rho[kMaxRecheck];
-    double incc[kMaxRecheck];
-};
-
-struct NeedList {
-    int n = 0;
-    bool overflow = false;
-    int k[kMaxRecheck];
-    __device__ void add(int kk) {
-        for (int i = 0; i < n; ++i)
-            if (k[i] == kk) return;
-        if (n < kMaxRecheck)
-            k[n++] = kk;
-        else
-            overflow = true;
-    }
-};
-
-__device__ __forceinline__ bool lookup(const Overrides &ov, int k, int &oi, double &v, double &incc) {
-    while (oi < ov.n && ov.k[oi] < k) ++oi;
-    if (oi < ov.n && ov.k[oi] == k) {
-        v = ov.rho[oi];
-        incc = ov.incc[oi];
-        return true;
-    }
-    return false;
+// FindPeakNcc's sign rule for the direction from b to a (setsm_code.cpp:6676-6692)
+__device__ __forceinline__ int dir_sign(double a, double b) {
+    double d;
+    if (a >= 0 && b >= 0)
+        d = a - b;
+    else if (a < 0 && b < 0)
+        d = -(fabs(a) - fabs(b));
+    else if (a >= 0 && b < 0)
+        d = 1;
+    else
+        d = -1;
+    return d > 0 ? 1 : (d < 0 ? -1 : 0);
 }
 
-// One node's FindPeakNcc scan (setsm_code.cpp:6672-6752) and max_WNCC over
-// the slot values (FP32 from the window kernel, or exact FP64 for slots in
-// `ov`).  Every decision whose FP32 inputs lie within kBand of a boundary --
-// the sign tests and the difference of the direction rule, the rounding of a
-// peak value or of the maximum, the truncation of a voxel -- adds the FP32
-// slot(s) to `need`.  The outcome is exact when `need` stays empty.
-__device__ void scan_node(const DevLevel &P, int64_t pt, const float2 *__restrict__ rv, int K,
-                          const Overrides &ov, NeedList &need, vll_nccresult &R) {
-    R = P.ncc[pt];
-    const bool voxels = !P.cmr && !P.is_ra;
-    const int start_H = P.gp3[pt].minHeight;
-    int check_rho = 0, direction = 0, pre_k = -1;
-    double pre_rho = -1.0;
-    float pre_height = 0.0f;
-    bool pre_exact = true;
-    double max_w = -100;
-    int oi = 0;
-    for (int k = 0; k < K; ++k) {
-        const float2 v2 = rv[k];
-        if (v2.x == kNotEvaluated || v2.x == kRejected) continue;
-        double v = (double)v2.x, incc = (double)v2.y;
-        const bool exact = lookup(ov, k, oi, v, incc);
-        if (!exact && (isnan(v2.y) || (voxels && near_trunc(incc)))) need.add(k);
-        if (P.cmr) {
-            if (check_rho && !(exact && pre_exact) &&
-                (fabs(v - pre_rho) < kBand || fabs(v) < kBand || fabs(pre_rho) < kBand)) {
-                if (!exact) need.add(k);
-                if (!pre_exact) need.add(pre_k);
-            }
-            double diff;
-            if (v >= 0 && pre_rho >= 0)
-                diff = v - pre_rho;
-            else if (v < 0 && pre_rho < 0)
-                diff = -(fabs(v) - fabs(pre_rho));
-            else if (v >= 0 && pre_rho < 0)
-                diff = 1;
-            else
-                diff = -1;
-            int td = diff > 0 ? 1 : (diff < 0 ? -1 : 0);
-            if (!check_rho) {
-                check_rho = 1;
-                td = -1;
-            } else if (pre_rho != -1) {
-                if (direction > 0 && td < 0) {
-                    if (!pre_exact && near_round(pre_rho)) need.add(pre_k);
+// Runs the whole FindPeakNcc scan / max_WNCC of a node on its FP32 values and
+// writes the results when no decision lies within kBand of a boundary;
+// otherwise queues the node for the exact (warp) path.
+__global__ void __launch_bounds__(256) scan_thread_kernel(const DevLevel *__restrict__ Pp,
+                                                          const int64_t *__restrict__ slot_off,
+                                                          const float2 *__restrict__ rho,
+                                                          int64_t *__restrict__ pending,
+                                                          unsigned long long *__restrict__ ctl) {
+    const DevLevel &P = *Pp;
+    const bool voxels = P.vox && !P.cmr && !P.is_ra;
+    for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.n_nodes;
+         pt += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t so = slot_off[pt];
+        const int K = (int)(slot_off[pt + 1] - so);
+        if (K == 0) continue;
+        const float2 *rv = rho + so;
+        vll_nccresult R = P.ncc[pt];
+        const int start_H = P.gp3[pt].minHeight;
+        bool need = K > kSlotCap;
+        int check_rho = 0, direction = 0;
+        double pre_rho = -1.0, max_w = -100, b1 = -1e30, b2 = -1e30;
+        float pre_h = 0.f;
+        for (int k = 0; k < K && !need; ++k) {
+            const float2 v2 = rv[k];
+            if (v2.x == kNotEvaluated || v2.x == kRejected) continue;
+            const double v = (double)v2.x;
+            if (isnan(v2.y) || (voxels && near_trunc((double)v2.y))) need = true;
+            if (P.cmr) {
+                if (check_rho &&
+                    (fabs(v - pre_rho) < kBand || fabs(v) < kBand || fabs(pre_rho) < kBand))
+                    need = true;
+                int td = dir_sign(v, pre_rho);
+                if (!check_rho) {
+                    check_rho = 1;
+                    td = -1;
+                } else if (pre_rho != -1 && direction > 0 && td < 0) {
+                    if (pre_rho > b1) {
+                        b2 = b1;
+                        b1 = pre_rho;
+                    } else if (pre_rho > b2) {
+                        b2 = pre_rho;
+                    }
                     if (R.result4 < 10) R.result4 += 1;
                     const int16_t qpre = q_result(pre_rho);
                     if (R.result0 < qpre) {
                         const double t1 = dq_result(R.result0);
                         R.result0 = qpre;
                         const float t2 = R.result2;
-                        R.result2 = pre_height;
+                        R.result2 = pre_h;
                         const int16_t q1 = q_result(t1);
                         if (R.result1 < q1) {
                             R.result1 = q1;
@@ -530,129 +443,528 @@ __device__ void scan_node(const DevLevel &P, int64_t pt, const float2 *__restric
                         }
                     } else if (R.result1 < qpre) {
                         R.result1 = qpre;
-                        R.result3 = pre_height;
+                        R.result3 = pre_h;
                     }
                 }
+                pre_rho = v;
+                pre_h = slot_height(P, start_H, R.minHeight, k);
+                direction = td;
             }
-            pre_rho = v;
-            pre_height = slot_height(P, start_H, R.minHeight, k);
-            direction = td;
-            pre_k = k;
-            pre_exact = exact;
+            if (max_w < v) max_w = v;
         }
-        if (max_w < v) max_w = v;
-    }
-    if (R.check_height_change) {
-        // the rounded maximum: any FP32 value within the band of the maximum
-        // that sits near a rounding boundary must be exact
-        oi = 0;
-        for (int k = 0; k < K; ++k) {
-            const float2 v2 = rv[k];
-            if (v2.x == kNotEvaluated || v2.x == kRejected) continue;
-            double v = (double)v2.x, incc = (double)v2.y;
-            if (lookup(ov, k, oi, v, incc)) continue;
-            if (v >= max_w - kBand && near_round(v)) need.add(k);
+        if (!need) {
+            // rounding of the top-two peak values and of the maximum
+            const double thr = (b2 > -1e29 ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
+            check_rho = 0;
+            direction = 0;
+            pre_rho = -1.0;
+            for (int k = 0; k < K && !need; ++k) {
+                const float2 v2 = rv[k];
+                if (v2.x == kNotEvaluated || v2.x == kRejected) continue;
+                const double v = (double)v2.x;
+                if (R.check_height_change && v >= max_w - kBand && near_round(v)) need = true;
+                if (P.cmr) {
+                    int td = dir_sign(v, pre_rho);
+                    if (!check_rho) {
+                        check_rho = 1;
+                        td = -1;
+                    } else if (pre_rho != -1 && direction > 0 && td < 0 && pre_rho >= thr &&
+                               near_round(pre_rho)) {
+                        need = true;
+                    }
+                    pre_rho = v;
+                    direction = td;
+                }
+            }
         }
-        R.max_WNCC = q_result(max_w);
+        if (need) {
+            pending[atomicAdd(&ctl[2], 1ull)] = pt;
+            atomicAdd(&ctl[3], 1ull);
+        } else {
+            if (R.check_height_change) R.max_WNCC = q_result(max_w);
+            P.ncc[pt] = R;
+        }
     }
 }
 
-__global__ void __launch_bounds__(128) peaks_kernel(const DevLevel *__restrict__ Pp,
-                                                    const int64_t *__restrict__ slot_off,
-                                                    const float2 *__restrict__ rho,
-                                                    int64_t *__restrict__ re_items, int64_t cap_re,
-                                                    int64_t *__restrict__ node_re,
-                                                    int64_t *__restrict__ pending,
-                                                    unsigned long long *__restrict__ ctl,
-                                                    unsigned long long *__restrict__ counters) {
+// ---------------------------------------------------------------------------
+// peak kernel: one warp per node
+// ---------------------------------------------------------------------------
+constexpr int kPeakWarps = 4;
+
+struct WarpShared {
+    float rho[kSlotCap];
+    uint32_t evaluated[kSlotCap / 32];
+    uint32_t need[kSlotCap / 32];
+    uint32_t exact[kSlotCap / 32];
+    uint32_t peak[kSlotCap / 32];
+    int exact_k[kExactCap];
+    double exact_rho[kExactCap];
+    double exact_incc[kExactCap];
+    int n_exact;
+};
+
+__device__ __forceinline__ bool bit(const uint32_t *m, int k) { return (m[k >> 5] >> (k & 31)) & 1u; }
+__device__ __forceinline__ void set_bit(uint32_t *m, int k) { atomicOr(&m[k >> 5], 1u << (k & 31)); }
+
+// value of slot k for the scan: exact if re-checked, else the FP32 one
+__device__ __forceinline__ double slot_value(const WarpShared &w, int k, bool &ex) {
+    ex = bit(w.exact, k);
+    if (ex) {
+        for (int i = 0; i < w.n_exact; ++i)
+            if (w.exact_k[i] == k) return w.exact_rho[i];
+    }
+    return (double)w.rho[k];
+}
+
+// Index of the last evaluated slot before k (or -1); `carry` is the last
+// evaluated slot of earlier 32-slot groups.
+__device__ __forceinline__ int prev_eval(uint32_t mask, int lane, int carry) {
+    const uint32_t below = mask & ((1u << lane) - 1u);
+    return below ? (31 - __clz(below)) : carry;
+}
+
+// Exact FP64 evaluation of one slot by the whole warp, bit-identical with
+// eval_slot (the reference's operation order): lanes 0/1 project into the two
+// images; every lane bilinear-samples its share of the window offsets (each
+// sample is computed independently, so this is exact); lanes 0..5 then run
+// the six two-pass Pearson sums (3 sub-windows x {intensity, magnitude}) over
+// the samples in the reference's scan order; lane 0 combines them in
+// ComputeMultiNCC's order.  `scratch` holds (2H+1)^2 x 4 doubles + flags.
+template <int H>
+__device__ __noinline__ SlotOut eval_slot_warp(const DevLevel &P, int64_t pt, const PatchSrc &S, float hgt,
+                                  double cnt_g, double sum_g, double *scratch, int lane) {
+    constexpr int D = 2 * H + 1;
+    SlotOut o;
+    o.evaluated = false;
+    o.orient_reject = false;
+    o.all_pos = false;
+    o.rho = -1.0;
+    o.count_incc = 0;
+    o.sum_incc = 0;
+    const DevImage &ri = P.im[P.ref];
+    const DevImage &tI = P.im[1];
+    const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
+    double2 c = make_double2(0, 0);
+    if (lane < 2) {
+        const DevImage &im = lane == 0 ? ri : tI;
+        c = rpc_project(im.rpc, im.adj, lon, lat, (double)hgt);
+    }
+    const double2 rc = make_double2(__shfl_sync(0xffffffffu, c.x, 0), __shfl_sync(0xffffffffu, c.y, 0));
+    const double2 tc = make_double2(__shfl_sync(0xffffffffu, c.x, 1), __shfl_sync(0xffffffffu, c.y, 1));
+    const double2 rp = to_pyramid(rc, ri.sx, ri.sy, P.L);
+    const double2 tp = to_pyramid(tc, tI.sx, tI.sy, P.L);
+    if (!(in_image(rp, ri.w, ri.h) && in_image(tp, tI.w, tI.h))) return o;
+    const int od = (int)ri.ori[(int64_t)(int)rp.y * ri.w + (int)rp.x] -
+                   (int)tI.ori[(int64_t)(int)tp.y * tI.w + (int)tp.x];
+    if (!P.is_ra && P.L >= 3) {
+        const double a = __dmul_rn((double)od, P.bin_angle);
+        if (!(a < 90 && a > -90)) {
+            o.orient_reject = true;
+            return o;
+        }
+    }
+    o.evaluated = true;
+    const double c0 = P.rot_cos[2 * od + kRotOffset], s0 = P.rot_sin[2 * od + kRotOffset];
+    unsigned char *flag = reinterpret_cast<unsigned char *>(scratch + 4 * D * D);
+    for (int idx = lane; idx < D * D; idx += 32) {
+        const int row = idx / D - H, col = idx % D - H;
+        const int r2 = row * row + col * col;
+        unsigned char f = 0;
+        if (r2 <= (H + 1) * (H + 1)) {
+            const double ox = __dadd_rn(__dmul_rn(c0, (double)col), -__dmul_rn(s0, (double)row));
+            const double oy = __dadd_rn(__dmul_rn(s0, (double)col), __dmul_rn(c0, (double)row));
+            const double2 pl = make_double2(__dadd_rn(rp.x, (double)col), __dadd_rn(rp.y, (double)row));
+            const double2 pr = make_double2(__dadd_rn(tp.x, ox), __dadd_rn(tp.y, oy));
+            double v[4];
+            if (sample4(S, pl, pr, v)) {
+                f = (unsigned char)(1 + window_depth(H, row, col, r2));   // 1 + depth
+#pragma unroll
+                for (int ch = 0; ch < 4; ++ch) scratch[4 * idx + ch] = v[ch];
+            }
+        }
+        flag[idx] = f;
+    }
+    __syncwarp();
+    // lanes 0..5: Correlate for (window w, channel pair p), SubFunctions.cpp:974-1018
+    double r = -99.0;
+    int n = 0;
+    if (lane < 6) {
+        const int w = lane >> 1, p = lane & 1;
+        double Ls = 0, Rs = 0;
+        for (int idx = 0; idx < D * D; ++idx) {
+            const int f = flag[idx];
+            if (f == 0 || f - 1 < w) continue;
+            Ls = __dadd_rn(Ls, scratch[4 * idx + p]);
+            Rs = __dadd_rn(Rs, scratch[4 * idx + p + 2]);
+            ++n;
+        }
+        if (n > 0) {
+            const double Lm = __ddiv_rn(Ls, (double)n), Rm = __ddiv_rn(Rs, (double)n);
+            double slr = 0, sl2 = 0, sr2 = 0;
+            for (int idx = 0; idx < D * D; ++idx) {
+                const int f = flag[idx];
+                if (f == 0 || f - 1 < w) continue;
+                const double dl = __dadd_rn(scratch[4 * idx + p], -Lm);
+                const double dr = __dadd_rn(scratch[4 * idx + p + 2], -Rm);
+                slr = __dadd_rn(slr, __dmul_rn(dl, dr));
+                sl2 = __dadd_rn(sl2, __dmul_rn(dl, dl));
+                sr2 = __dadd_rn(sr2, __dmul_rn(dr, dr));
+            }
+            if (sl2 > 1e-8 && sr2 > 1e-8) r = __ddiv_rn(slr, sqrt(__dmul_rn(sl2, sr2)));
+        }
+    }
+    double rv[6];
+    int nv[3];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) rv[j] = __shfl_sync(0xffffffffu, r, j);
+#pragma unroll
+    for (int w = 0; w < 3; ++w) nv[w] = __shfl_sync(0xffffffffu, n, 2 * w);
+    __syncwarp();
+    o.all_pos = nv[0] > 0 && nv[1] > 0 && nv[2] > 0;
+    double count = 0, sum = 0;
+    if (o.all_pos) {
+        double tot = 0, cntv = 0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            if (rv[j] != -99.0) {
+                cntv = __dadd_rn(cntv, 1.0);
+                tot = __dadd_rn(tot, rv[j]);
+            }
+        }
+        if (cntv > 0) {
+            sum = __ddiv_rn(tot, cntv);
+            count = 1.0;
+        }
+    }
+    o.count_incc = count;
+    o.sum_incc = sum;
+    if (P.check_ortho && cnt_g > 0)
+        o.rho = __dadd_rn(__dmul_rn(__ddiv_rn(sum, count), P.alpha),
+                          __dmul_rn(__ddiv_rn(sum_g, cnt_g), P.beta));
+    else
+        o.rho = count > 0 ? __ddiv_rn(sum, count) : -1.0;
+    return o;
+}
+
+// A node settled entirely in exact FP64, the warp's lanes evaluating 32 slots
+// at a time (eval_slot: the reference's operation order).  The exact values
+// overwrite the node's slot buffer (one double per float2 slot, markers kept
+// as +-inf), then lane 0 runs FindPeakNcc and the maximum over them and writes
+// the node's results; voxel rows get the exact INCC.
+__device__ void node_exact_warp(const DevLevel &P, int64_t pt, int K, float2 *rv,
+                                const PatchSrc &S, const PatchSrc &Sn, double cnt_g, double sum_g,
+                                vll_nccresult R, vll_voxel *vrow, int lane,
+                                unsigned long long &rechecks) {
+    const int start_H = P.gp3[pt].minHeight;
+    double *dv = reinterpret_cast<double *>(rv);
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        const int k = k0 + lane;
+        if (k < K) {
+            const float2 v = rv[k];
+            double out = (double)v.x;   // markers stay +-inf
+            if (v.x != kNotEvaluated && v.x != kRejected) {
+                const float hgt = slot_height(P, start_H, R.minHeight, k);
+                const SlotOut o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
+                out = o.rho;
+                if (vrow) {
+                    if (o.all_pos) vrow[k].flag_cal = 1;
+                    vrow[k].INCC = o.count_incc > 0 ? q_voxel(__ddiv_rn(o.sum_incc, o.count_incc))
+                                                     : q_voxel(-1.0);
+                }
+                rechecks++;
+            }
+            dv[k] = out;
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        PeakState st;
+        peak_init(st);
+        double max_w = -100;
+        for (int k = 0; k < K; ++k) {
+            const double v = dv[k];
+            if (isinf(v)) continue;
+            if (P.cmr) find_peak(st, v, slot_height(P, start_H, R.minHeight, k), R);
+            if (max_w < v) max_w = v;
+        }
+        if (R.check_height_change) R.max_WNCC = q_result(max_w);
+        P.ncc[pt] = R;
+    }
+    __syncwarp();
+}
+
+// bytes of eval_slot_warp scratch for window half-size H
+__host__ __device__ constexpr size_t exact_scratch_bytes(int H) {
+    return (size_t)(2 * H + 1) * (2 * H + 1) * 33 + 16;
+}
+
+// The exact path for the nodes the scan kernel could not settle in FP32.
+template <int H>
+__global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
+    const DevLevel *__restrict__ Pp, const int64_t *__restrict__ slot_off,
+    const float2 *__restrict__ rho, const double *__restrict__ gsum, const double *__restrict__ gcnt,
+    unsigned long long *__restrict__ counters, unsigned long long *__restrict__ queue,
+    const int64_t *__restrict__ pending, const unsigned long long *__restrict__ n_pending) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const DevLevel &P = *Pp;
-    for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.n_nodes;
-         pt += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    WarpShared &W = reinterpret_cast<WarpShared *>(smem_raw)[warp];
+    constexpr size_t ws = (sizeof(WarpShared) + 15) & ~(size_t)15;
+    constexpr size_t xs = (exact_scratch_bytes(H) + 15) & ~(size_t)15;
+    double *boxes = reinterpret_cast<double *>(smem_raw + ws * kPeakWarps + xs * warp);
+    PatchSrc S, Sn;
+    make_src(P, 1, S, Sn);
+    const bool voxels = P.vox && !P.cmr && !P.is_ra;
+    unsigned long long rechecks = 0;
+    const unsigned long long n_pend = *n_pending;
+    for (;;) {
+        unsigned long long idx = 0;
+        if (lane == 0) idx = atomicAdd(queue, 1ull);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= n_pend) break;
+        const int64_t pt = pending[idx];
         const int64_t so = slot_off[pt];
         const int K = (int)(slot_off[pt + 1] - so);
         if (K == 0) continue;
-        Overrides none;
-        none.n = 0;
-        NeedList need;
-        vll_nccresult R;
-        scan_node(P, pt, rho + so, K, none, need, R);
-        if (need.n == 0 && !need.overflow) {
-            P.ncc[pt] = R;
+        vll_nccresult R = P.ncc[pt];
+        const int start_H = P.gp3[pt].minHeight;
+        const double cnt_g = gcnt ? gcnt[pt] : 0.0, sum_g = gsum ? gsum[pt] : 0.0;
+        vll_voxel *vrow = voxels ? P.vox + P.vox_off[pt] : nullptr;
+        if (K > kSlotCap) {
+            // more slots than the shared scan buffer holds: all slots exactly
+            node_exact_warp(P, pt, K, const_cast<float2 *>(rho) + so, S, Sn, cnt_g, sum_g, R, vrow,
+                            lane, rechecks);
             continue;
         }
-        int64_t code = kFullRedo;
-        if (!need.overflow) {
-            // ascending slot order for the re-scan's merge
-            for (int i = 1; i < need.n; ++i) {
-                const int x = need.k[i];
-                int j = i - 1;
-                while (j >= 0 && need.k[j] > x) {
-                    need.k[j + 1] = need.k[j];
-                    --j;
+        for (int i = lane; i < kSlotCap / 32; i += 32) {
+            W.evaluated[i] = 0;
+            W.need[i] = 0;
+            W.exact[i] = 0;
+            W.peak[i] = 0;
+        }
+        if (lane == 0) W.n_exact = 0;
+        __syncwarp();
+        for (int k0 = 0; k0 < K; k0 += 32) {
+            const int k = k0 + lane;
+            float2 v = make_float2(kNotEvaluated, 0.f);
+            if (k < K) v = rho[so + k];
+            const bool ev = k < K && v.x != kNotEvaluated && v.x != kRejected;
+            const bool nd = ev && (isnan(v.y) || (voxels && near_trunc((double)v.y)));
+            const uint32_t em = __ballot_sync(0xffffffffu, ev);
+            const uint32_t nm = __ballot_sync(0xffffffffu, nd);
+            if (k < K) W.rho[k] = v.x;
+            if (lane == 0) {
+                W.evaluated[k0 >> 5] = em;
+                W.need[k0 >> 5] = nm;
+            }
+        }
+        __syncwarp();
+        // ---- scan, re-check, repeat ----
+        double max_w = -100;
+        bool redone = false;
+        for (int round = 0;; ++round) {
+            // (a) directions, near ties and peaks, lane-parallel per 32-slot group
+            int carry = -1;
+            for (int k0 = 0; k0 < K; k0 += 32) {
+                const int k = k0 + lane;
+                const uint32_t em = W.evaluated[k0 >> 5];
+                const bool ev = k < K && ((em >> lane) & 1u);
+                // previous evaluated slot, and the one before it
+                const int p_in = prev_eval(em, lane, -1);
+                const int p = p_in >= 0 ? k0 + p_in : carry;
+                int pp = -1;
+                if (p >= 0) {
+                    const int pg = p >> 5, pl = p & 31;
+                    const uint32_t pm = W.evaluated[pg] & ((1u << pl) - 1u);
+                    if (pm)
+                        pp = (pg << 5) + 31 - __clz(pm);
+                    else {
+                        for (int gi = pg - 1; gi >= 0 && pp < 0; --gi)
+                            if (W.evaluated[gi]) pp = (gi << 5) + 31 - __clz(W.evaluated[gi]);
+                    }
                 }
-                need.k[j + 1] = x;
-            }
-            const unsigned long long start = atomicAdd(&ctl[1], (unsigned long long)need.n);
-            if ((int64_t)(start + need.n) <= cap_re) {
-                for (int i = 0; i < need.n; ++i) re_items[start + i] = (pt << 16) | need.k[i];
-                code = ((int64_t)start << 8) | need.n;
-                atomicAdd(&counters[2], (unsigned long long)need.n);
-            }
-        }
-        if (code == kFullRedo) atomicAdd(&counters[2], (unsigned long long)K);
-        node_re[pt] = code;
-        const unsigned long long slot = atomicAdd(&ctl[2], 1ull);
-        pending[slot] = pt;
-    }
-}
-
-__global__ void __launch_bounds__(64) rescan_kernel(const DevLevel *__restrict__ Pp,
-                                                    const int64_t *__restrict__ slot_off,
-                                                    const float2 *__restrict__ rho,
-                                                    const int64_t *__restrict__ node_re,
-                                                    const int64_t *__restrict__ pending,
-                                                    const int64_t *__restrict__ re_items,
-                                                    const double *__restrict__ re_out,
-                                                    const unsigned long long *__restrict__ ctl) {
-    const DevLevel &P = *Pp;
-    const unsigned long long n = ctl[2];
-    const bool voxels = P.vox && !P.cmr && !P.is_ra;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        const int64_t pt = pending[i];
-        const int64_t code = node_re[pt];
-        bool redo = code == kFullRedo;
-        if (!redo) {
-            const int64_t start = code >> 8;
-            Overrides ov;
-            ov.n = (int)(code & 0xFF);
-            for (int j = 0; j < ov.n; ++j) {
-                ov.k[j] = (int)(re_items[start + j] & 0xFFFF);
-                ov.rho[j] = re_out[2 * (start + j)];
-                ov.incc[j] = re_out[2 * (start + j) + 1];
-            }
-            const int64_t so = slot_off[pt];
-            const int K = (int)(slot_off[pt + 1] - so);
-            NeedList need;
-            vll_nccresult R;
-            scan_node(P, pt, rho + so, K, ov, need, R);
-            if (need.n == 0 && !need.overflow) {
-                P.ncc[pt] = R;
-                if (voxels) {
-                    vll_voxel *row = P.vox + P.vox_off[pt];
-                    for (int j = 0; j < ov.n; ++j) row[ov.k[j]].INCC = q_voxel(ov.incc[j]);
+                bool need_me = false, need_p = false;
+                if (ev) {
+                    bool ex_k, ex_p = true;
+                    const double v = slot_value(W, k, ex_k);
+                    if (P.cmr && p >= 0) {
+                        const double pv = slot_value(W, p, ex_p);
+                        if (!(ex_k && ex_p) &&
+                            (fabs(v - pv) < kBand || fabs(v) < kBand || fabs(pv) < kBand)) {
+                            need_me = !ex_k;
+                            need_p = !ex_p;
+                        }
+                        // direction of k (td) and of p (dp): a peak at p needs
+                        // dp > 0 and td < 0 (first evaluated slot: td = -1)
+                        auto sgn = [](double a, double b) {
+                            double d;
+                            if (a >= 0 && b >= 0)
+                                d = a - b;
+                            else if (a < 0 && b < 0)
+                                d = -(fabs(a) - fabs(b));
+                            else if (a >= 0 && b < 0)
+                                d = 1;
+                            else
+                                d = -1;
+                            return d > 0 ? 1 : (d < 0 ? -1 : 0);
+                        };
+                        const int td = sgn(v, pv);
+                        int dp = -1;
+                        if (pp >= 0) {
+                            bool ex_pp;
+                            const double ppv = slot_value(W, pp, ex_pp);
+                            dp = sgn(pv, ppv);
+                        }
+                        const bool is_peak = pv != -1 && dp > 0 && td < 0;
+                        if (is_peak) set_bit(W.peak, p);
+                    }
                 }
-            } else {
-                redo = true;
+                if (need_me) set_bit(W.need, k);
+                if (need_p) set_bit(W.need, p);
+                const uint32_t any = em & ((k0 + 32 <= K) ? 0xffffffffu : ((1u << (K - k0)) - 1u));
+                if (any) carry = k0 + 31 - __clz(any);
+            }
+            __syncwarp();
+            // (a2) rounding of peak values that can reach the top two: a peak
+            // more than 0.002 (+ the band) below the second-best peak rounds
+            // strictly below it and can neither enter nor reorder the top two
+            if (P.cmr) {
+                double b1 = -1e30, b2 = -1e30;
+                for (int k = lane; k < K; k += 32) {
+                    if (!bit(W.peak, k)) continue;
+                    bool ex;
+                    const double v = slot_value(W, k, ex);
+                    if (v > b1) {
+                        b2 = b1;
+                        b1 = v;
+                    } else if (v > b2) {
+                        b2 = v;
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o; o >>= 1) {
+                    const double o1 = __shfl_xor_sync(0xffffffffu, b1, o);
+                    const double o2 = __shfl_xor_sync(0xffffffffu, b2, o);
+                    const double n1 = fmax(b1, o1);
+                    const double n2 = fmax(fmin(b1, o1), fmax(b2, o2));
+                    b1 = n1;
+                    b2 = n2;
+                }
+                const double thr = (b2 > -1e29 ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
+                for (int k = lane; k < K; k += 32) {
+                    if (!bit(W.peak, k)) continue;
+                    bool ex;
+                    const double v = slot_value(W, k, ex);
+                    if (!ex && v >= thr && near_round(v)) set_bit(W.need, k);
+                }
+            }
+            __syncwarp();
+            // (b) the maximum and its rounding
+            double m = -100;
+            for (int k = lane; k < K; k += 32) {
+                if (!bit(W.evaluated, k)) continue;
+                bool ex;
+                const double v = slot_value(W, k, ex);
+                if (m < v) m = v;
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            max_w = m;
+            if (R.check_height_change) {
+                for (int k = lane; k < K; k += 32) {
+                    if (!bit(W.evaluated, k)) continue;
+                    bool ex;
+                    const double v = slot_value(W, k, ex);
+                    if (!ex && v >= max_w - kBand && near_round(v)) set_bit(W.need, k);
+                }
+            }
+            __syncwarp();
+            // (c) slots still needing an exact value
+            int n_need = 0;
+            for (int i = 0; i < (K + 31) / 32; ++i) n_need += __popc(W.need[i] & ~W.exact[i]);
+            if (n_need == 0) break;
+            const bool overflow = W.n_exact + n_need > kExactCap || round + 1 >= kMaxRounds;
+            if (lane == 0) atomicAdd(&counters[6], 1ull);
+            if (overflow) {
+                if (lane == 0) atomicAdd(&counters[5], 1ull);
+                // give up on the FP32 values: the whole node exactly
+                node_exact_warp(P, pt, K, const_cast<float2 *>(rho) + so, S, Sn, cnt_g, sum_g, R,
+                                vrow, lane, rechecks);
+                redone = true;   // results already written
+                break;
+            }
+            // compact the list and evaluate it lane-parallel in FP64
+            int base = W.n_exact;
+            for (int i = 0; i < (K + 31) / 32; ++i) {
+                const uint32_t todo = W.need[i] & ~W.exact[i];
+                const int k = (i << 5) + lane;
+                const bool mine = (todo >> lane) & 1u;
+                const int off = __popc(todo & ((1u << lane) - 1u));
+                if (mine) W.exact_k[base + off] = k;
+                base += __popc(todo);
+            }
+            __syncwarp();
+            // exact values, one slot at a time, the whole warp per slot
+            for (int j = W.n_exact; j < base; ++j) {
+                const int k = W.exact_k[j];
+                const float hh = slot_height(P, start_H, R.minHeight, k);
+                const SlotOut o = eval_slot_warp<H>(P, pt, S, hh, cnt_g, sum_g,
+                                                    reinterpret_cast<double *>(boxes), lane);
+                if (lane == 0) {
+                    W.exact_rho[j] = o.rho;
+                    W.exact_incc[j] = o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc) : -1.0;
+                    if (vrow) vrow[k].INCC = q_voxel(W.exact_incc[j]);
+                    rechecks++;
+                }
+                __syncwarp();
+            }
+            __syncwarp();
+            for (int j = W.n_exact + lane; j < base; j += 32) set_bit(W.exact, W.exact_k[j]);
+            if (lane == 0) W.n_exact = base;
+            for (int i = lane; i < kSlotCap / 32; i += 32) W.peak[i] = 0;
+            __syncwarp();
+        }
+        if (redone) continue;   // the node went through the FP64 path
+        // ---- ordered fold over the peaks (FindPeakNcc's top-2 rule) ----
+        if (P.cmr && lane == 0) {
+            for (int i = 0; i < (K + 31) / 32; ++i) {
+                uint32_t pm = W.peak[i];
+                while (pm) {
+                    const int b = __ffs(pm) - 1;
+                    pm &= pm - 1;
+                    const int p = (i << 5) + b;
+                    bool ex;
+                    const double pv = slot_value(W, p, ex);
+                    const float ph = slot_height(P, start_H, R.minHeight, p);
+                    if (R.result4 < 10) R.result4 += 1;
+                    const int16_t qpre = q_result(pv);
+                    if (R.result0 < qpre) {
+                        const double t1 = dq_result(R.result0);
+                        R.result0 = qpre;
+                        const float t2 = R.result2;
+                        R.result2 = ph;
+                        const int16_t q1 = q_result(t1);
+                        if (R.result1 < q1) {
+                            R.result1 = q1;
+                            R.result3 = t2;
+                        }
+                    } else if (R.result1 < qpre) {
+                        R.result1 = qpre;
+                        R.result3 = ph;
+                    }
+                }
             }
         }
-        if (redo) {
-            // outcome still depends on FP32 values near a boundary: recompute
-            // the node exactly (resets its results like VerticalLineLocus)
-            unsigned long long a = 0, e = 0;
-            plain_node(P, pt, a, e, nullptr, nullptr);
+        if (lane == 0) {
+            if (R.check_height_change) R.max_WNCC = q_result(max_w);
+            P.ncc[pt] = R;
         }
+        __syncwarp();
     }
+    for (int o = 16; o; o >>= 1) rechecks += __shfl_down_sync(0xffffffffu, rechecks, o);
+    if (lane == 0 && rechecks) atomicAdd(&counters[2], rechecks);
 }
 
 // ---------------------------------------------------------------------------
@@ -678,36 +990,129 @@ unsigned grid_1d(int64_t n, int threads, int64_t cap_blocks) {
     return (unsigned)b;
 }
 
-template <int H>
-cudaError_t launch_ncc(const DevLevel *dP, const int64_t *items, int64_t n_items,
-                       const int64_t *slot_off, const double *gsum, const double *gcnt, float2 *rho,
-                       unsigned long long *counters, unsigned long long *queue, cudaStream_t s) {
-    // per-warp shared footprint: both images' boxes, float4 texel pairs
-    const int warp_quads = 1024;
-    const int threads = 128;
-    const size_t smem = (size_t)(threads / 32) * warp_quads * sizeof(float4);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(ncc_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
+// Host-side RPC line/sample (no clamp) for footprint estimates.
+void host_rpc(const double *rpc, double lon, double lat, double h, double &x, double &y) {
+    const double L = (lon - rpc[2]) / rpc[7], Pn = (lat - rpc[3]) / rpc[8], Hn = (h - rpc[4]) / rpc[9];
+    const double t[20] = {1, L, Pn, Hn, L * Pn, L * Hn, Pn * Hn, L * L, Pn * Pn, Hn * Hn,
+                          Pn * L * Hn, L * L * L, L * Pn * Pn, L * Hn * Hn, L * L * Pn,
+                          Pn * Pn * Pn, Pn * Hn * Hn, L * L * Hn, Pn * Pn * Hn, Hn * Hn * Hn};
+    double c[4] = {0, 0, 0, 0};
+    for (int j = 0; j < 4; ++j)
+        for (int i = 0; i < 20; ++i) c[j] += rpc[10 + 20 * j + i] * t[i];
+    y = c[0] / c[1] * rpc[5] + rpc[0];
+    x = c[2] / c[3] * rpc[6] + rpc[1];
+}
+
+// Texel-pair budget per warp: the boxes covering 32 consecutive height slots
+// of one node in both images -- the reference window and the target window
+// (rotated up to 45 degrees) swept along their epipolar lines.  The sweep
+// per slot is measured from the RPCs over the image footprint; the budget is
+// the worst case with a 25% margin (a larger footprint falls back to FP64).
+int window_warp_quads(const DevLevel &P) {
+    const int H = P.H;
+    double rate[2] = {0, 0};
+    for (int ti = 0; ti < 2; ++ti) {
+        const double *r = P.im[ti].rpc;
+        for (int a = -1; a <= 1; ++a)
+            for (int b = -1; b <= 1; ++b) {
+                const double lon = r[2] + 0.8 * a * r[7], lat = r[3] + 0.8 * b * r[8];
+                double x0, y0, x1, y1;
+                host_rpc(r, lon, lat, r[4] - 50.0, x0, y0);
+                host_rpc(r, lon, lat, r[4] + 50.0, x1, y1);
+                const double d = std::max(fabs(x1 - x0), fabs(y1 - y0)) / 100.0 / (1 << P.L);
+                rate[ti] = std::max(rate[ti], d);
+            }
     }
-    int dev = 0, sms = 148, per_sm = 1;
+    const double sweep0 = 31.0 * P.height_step * rate[0], sweep1 = 31.0 * P.height_step * rate[1];
+    const int side = 2 * H + 3;
+    const int rside = 2 * ((int)ceilf(1.4143f * H) + 1) + 3;
+    const double need = (side + 1.0) * (side + sweep0 + 2.0) + (rside + 1.0) * (rside + sweep1 + 2.0);
+    int q = (int)(need * 1.25) + 32;
+    const int cap = (int)((200 * 1024 - win_boxes_offset()) / (kWinWarps * sizeof(float4)));
+    return std::min(q, cap);
+}
+
+
+template <int H>
+cudaError_t launch_window(const DevLevel &P, const DevLevel *dP, const int64_t *items,
+                          int64_t n_items, const int64_t *slot_off, const double *gsum,
+                          const double *gcnt, float2 *rho, unsigned long long *counters,
+                          unsigned long long *queue, cudaStream_t s) {
+    const int wq = window_warp_quads(P);
+    const size_t smem = win_boxes_offset() + (size_t)kWinWarps * wq * sizeof(float4);
+    int dev = 0;
     cudaGetDevice(&dev);
+    cudaError_t e = cudaFuncSetAttribute(window_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ncc_kernel<H>, threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<H>, kWinWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
-    ncc_kernel<H><<<sms * per_sm, threads, smem, s>>>(dP, items, n_items, slot_off, gsum, gcnt, rho,
-                                                      counters, queue, warp_quads);
+    window_kernel<H><<<sms * per_sm, kWinWarps * 32, smem, s>>>(dP, items, n_items, slot_off, gsum,
+                                                                gcnt, rho, counters, queue, wq);
     return cudaGetLastError();
+}
+
+template <int H>
+cudaError_t launch_peaks(const DevLevel *dP, const int64_t *slot_off, const float2 *rho,
+                         const double *gsum, const double *gcnt, unsigned long long *counters,
+                         unsigned long long *queue, const int64_t *pending,
+                         const unsigned long long *n_pending, cudaStream_t s) {
+    const size_t ws = (sizeof(WarpShared) + 15) & ~(size_t)15;
+    const size_t xs = (exact_scratch_bytes(H) + 15) & ~(size_t)15;
+    const size_t smem = (ws + xs) * kPeakWarps;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaError_t e = cudaFuncSetAttribute(peaks_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peaks_kernel<H>, kPeakWarps * 32, smem);
+    if (per_sm < 1) per_sm = 1;
+    peaks_kernel<H><<<sms * per_sm, kPeakWarps * 32, smem, s>>>(dP, slot_off, rho, gsum, gcnt,
+                                                                counters, queue, pending, n_pending);
+    return cudaGetLastError();
+}
+
+#define VLL_DISPATCH_H(Hv, call)                   \
+    switch (Hv) {                                  \
+        case 2: { constexpr int HH = 2; call; } break; \
+        case 3: { constexpr int HH = 3; call; } break; \
+        case 4: { constexpr int HH = 4; call; } break; \
+        case 5: { constexpr int HH = 5; call; } break; \
+        case 6: { constexpr int HH = 6; call; } break; \
+        case 7: { constexpr int HH = 7; call; } break; \
+        default: e = cudaErrorInvalidValue;        \
+    }
+
+// the window / peak stages of the pipeline on given buffers
+cudaError_t window_and_peaks(const DevLevel &P, const DevLevel *dP, const int64_t *items,
+                             int64_t n_items, const int64_t *slot_off, const double *gsum,
+                             const double *gcnt, float2 *rho, unsigned long long *counters,
+                             unsigned long long *ctl, int64_t *pending, cudaStream_t s,
+                             SplitTiming *tm) {
+    cudaError_t e = cudaSuccess;
+    VLL_DISPATCH_H(P.H, e = launch_window<HH>(P, dP, items, n_items, slot_off, gsum, gcnt, rho,
+                                              counters, ctl + 0, s));
+    if (e != cudaSuccess) return e;
+    if (tm && tm->enabled) cudaEventRecord(tm->ev[5], s);
+    scan_thread_kernel<<<grid_1d(P.n_nodes, 256, 148 * 32), 256, 0, s>>>(dP, slot_off, rho, pending,
+                                                                        ctl);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (tm && tm->enabled) cudaEventRecord(tm->ev[6], s);
+    VLL_DISPATCH_H(P.H, e = launch_peaks<HH>(dP, slot_off, rho, gsum, gcnt, counters, ctl + 1,
+                                             pending, ctl + 2, s));
+    return e;
 }
 
 }  // namespace
 
 bool split_supported(const DevLevel &P) {
     return P.num_images == 2 && P.ref == 0 && P.im[1].selected && !P.is_ra && !P.combined_incc &&
-           (P.H == 2 || P.H == 3 || P.H == 4 || P.H == 5 || P.H == 6 || P.H == 7);
+           P.H >= 2 && P.H <= 7;
 }
 
 void split_release(SplitBuffers &b) {
@@ -737,23 +1142,19 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
         if (tm && tm->enabled) cudaEventRecord(tm->ev[i], s);
     };
     int64_t launches = 0;
-    size_t cap;
-    // node-sized buffers
     if ((size_t)(N + 1) > b.cap_nodes) {
-        size_t c8 = 0;
         void **nb[] = {&b.node_k, &b.item_cnt};
         for (void **p : nb) {
             if (*p) cudaFree(*p);
             *p = nullptr;
             SPLIT_CUDA(cudaMalloc(p, (size_t)(N + 1) * sizeof(int32_t)));
         }
-        void **nb8[] = {&b.slot_off, &b.item_off, &b.gsum, &b.gcnt, &b.node_re, &b.pending};
+        void **nb8[] = {&b.slot_off, &b.item_off, &b.gsum, &b.gcnt, &b.pending};
         for (void **p : nb8) {
             if (*p) cudaFree(*p);
             *p = nullptr;
             SPLIT_CUDA(cudaMalloc(p, (size_t)(N + 1) * 8));
         }
-        (void)c8;
         b.cap_nodes = (size_t)(N + 1);
     }
     if (!b.ctl) SPLIT_CUDA(cudaMalloc(&b.ctl, 8 * sizeof(unsigned long long)));
@@ -774,14 +1175,12 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
     SPLIT_CUDA(cudaGetLastError());
     ++launches;
     mark(2);
-    // prefix sums (int32 counts -> int64 offsets)
     size_t tmp1 = 0, tmp2 = 0;
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp1, (const int32_t *)b.node_k,
                                              (int64_t *)b.slot_off, (int)(N + 1), s));
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, (const int32_t *)b.item_cnt,
                                              (int64_t *)b.item_off, (int)(N + 1), s));
-    cap = tmp1 > tmp2 ? tmp1 : tmp2;
-    SPLIT_CUDA(grow(b.scan_tmp, b.cap_scan, cap));
+    SPLIT_CUDA(grow(b.scan_tmp, b.cap_scan, std::max(tmp1, tmp2)));
     tmp1 = b.cap_scan;
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp1, (const int32_t *)b.node_k,
                                              (int64_t *)b.slot_off, (int)(N + 1), s));
@@ -801,15 +1200,6 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
     c = b.cap_items;
     SPLIT_CUDA(grow(b.items, c, (size_t)n_items * sizeof(int64_t)));
     b.cap_items = c;
-    const int64_t max_re = N * 4 + 1024;
-    if ((size_t)max_re > b.cap_re) {
-        if (b.re_items) cudaFree(b.re_items);
-        if (b.re_out) cudaFree(b.re_out);
-        b.re_items = b.re_out = nullptr;
-        SPLIT_CUDA(cudaMalloc(&b.re_items, (size_t)max_re * sizeof(int64_t)));
-        SPLIT_CUDA(cudaMalloc(&b.re_out, (size_t)max_re * 2 * sizeof(double)));
-        b.cap_re = (size_t)max_re;
-    }
     if (n_items > 0) {
         items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, (const int32_t *)b.item_cnt,
                                                                (const int64_t *)b.item_off,
@@ -817,38 +1207,16 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
         SPLIT_CUDA(cudaGetLastError());
         ++launches;
         mark(4);
-        unsigned long long *queue = (unsigned long long *)b.ctl;
-        cudaError_t e = cudaSuccess;
-        switch (P.H) {
-            case 2: e = launch_ncc<2>(dP, (const int64_t *)b.items, n_items, (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho, counters, queue, s); break;
-            case 3: e = launch_ncc<3>(dP, (const int64_t *)b.items, n_items, (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho, counters, queue, s); break;
-            case 4: e = launch_ncc<4>(dP, (const int64_t *)b.items, n_items, (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho, counters, queue, s); break;
-            case 5: e = launch_ncc<5>(dP, (const int64_t *)b.items, n_items, (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho, counters, queue, s); break;
-            case 6: e = launch_ncc<6>(dP, (const int64_t *)b.items, n_items, (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho, counters, queue, s); break;
-            case 7: e = launch_ncc<7>(dP, (const int64_t *)b.items, n_items, (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho, counters, queue, s); break;
-            default: e = cudaErrorInvalidValue;
-        }
+        cudaError_t e = window_and_peaks(P, dP, (const int64_t *)b.items, n_items,
+                                         (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho,
+                                         counters, (unsigned long long *)b.ctl,
+                                         (int64_t *)b.pending, s, tm);
         if (e != cudaSuccess) {
-            *err = "ncc_kernel launch";
+            *err = "window / peak kernel launch";
             return e;
         }
-        ++launches;
-        mark(5);
-        unsigned long long *ctl = (unsigned long long *)b.ctl;
-        peaks_kernel<<<grid_1d(N, 128, 148 * 64), 128, 0, s>>>(
-            dP, (const int64_t *)b.slot_off, (const float2 *)b.rho, (int64_t *)b.re_items,
-            (int64_t)b.cap_re, (int64_t *)b.node_re, (int64_t *)b.pending, ctl, counters);
-        SPLIT_CUDA(cudaGetLastError());
-        mark(6);
-        SPLIT_CUDA(launch_recheck(dP, (const int64_t *)b.re_items, ctl + 1, (int64_t)b.cap_re, gsum,
-                                  gcnt, (double *)b.re_out, s));
-        mark(7);
-        rescan_kernel<<<148 * 8, 64, 0, s>>>(dP, (const int64_t *)b.slot_off, (const float2 *)b.rho,
-                                             (const int64_t *)b.node_re, (const int64_t *)b.pending,
-                                             (const int64_t *)b.re_items, (const double *)b.re_out,
-                                             ctl);
-        SPLIT_CUDA(cudaGetLastError());
         launches += 3;
+        mark(7);
     } else {
         mark(4);
         mark(5);
@@ -982,15 +1350,14 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     int32_t *item_cnt = (int32_t *)cv.take((size_t)(N + 1) * 4);
     int64_t *slot_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
     int64_t *item_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
-    int64_t *node_re = (int64_t *)cv.take((size_t)(N + 1) * 8);
     int64_t *pending = (int64_t *)cv.take((size_t)(N + 1) * 8);
     size_t scan_bytes = 0;
     if (cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int32_t *)node_k, slot_off,
                                       (int)(N + 1), s) != cudaSuccess)
         return fail(VLL_ERR_CUDA, "scan size query failed");
     void *scan_tmp = cv.take(scan_bytes);
-    if (!dP || !ctl || !counters || !node_k || !item_cnt || !slot_off || !item_off || !node_re ||
-        !pending || !scan_tmp) {
+    if (!dP || !ctl || !counters || !node_k || !item_cnt || !slot_off || !item_off || !pending ||
+        !scan_tmp) {
         char m[160];
         snprintf(m, sizeof m, "grid of %lld nodes exceeds the %zu MiB scratch array",
                  (long long)N, kNoAllocScratchBytes >> 20);
@@ -1020,12 +1387,9 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     NA_CUDA(cudaMemcpyAsync(&totals[1], item_off + N, 8, cudaMemcpyDeviceToHost, s));
     NA_CUDA(cudaStreamSynchronize(s));
     const int64_t n_slots = totals[0], n_items = totals[1];
-    const int64_t max_re = N * 4 + 1024;
     int64_t *items = (int64_t *)cv.take((size_t)(n_items > 0 ? n_items : 1) * 8);
     float2 *rho = (float2 *)cv.take((size_t)(n_slots > 0 ? n_slots : 1) * sizeof(float2));
-    int64_t *re_items = (int64_t *)cv.take((size_t)max_re * 8);
-    double *re_out = (double *)cv.take((size_t)max_re * 2 * sizeof(double));
-    if (!items || !rho || !re_items || !re_out) {
+    if (!items || !rho) {
         char m[200];
         snprintf(m, sizeof m,
                  "%lld nodes with %lld height slots exceed the %zu MiB scratch array",
@@ -1047,24 +1411,8 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     if (n_items > 0) {
         items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, item_cnt, item_off, items);
         NA_CUDA(cudaGetLastError());
-        cudaError_t e = cudaSuccess;
-        switch (P.H) {
-            case 2: e = launch_ncc<2>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
-            case 3: e = launch_ncc<3>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
-            case 4: e = launch_ncc<4>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
-            case 5: e = launch_ncc<5>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
-            case 6: e = launch_ncc<6>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
-            case 7: e = launch_ncc<7>(dP, items, n_items, slot_off, nullptr, nullptr, rho, counters, ctl, s); break;
-            default: e = cudaErrorInvalidValue;
-        }
-        NA_CUDA(e);
-        peaks_kernel<<<grid_1d(N, 128, 148 * 64), 128, 0, s>>>(dP, slot_off, rho, re_items, max_re,
-                                                              node_re, pending, ctl, counters);
-        NA_CUDA(cudaGetLastError());
-        NA_CUDA(launch_recheck(dP, re_items, ctl + 1, max_re, nullptr, nullptr, re_out, s));
-        rescan_kernel<<<148 * 8, 64, 0, s>>>(dP, slot_off, rho, node_re, pending, re_items, re_out,
-                                             ctl);
-        NA_CUDA(cudaGetLastError());
+        NA_CUDA(window_and_peaks(P, dP, items, n_items, slot_off, nullptr, nullptr, rho, counters,
+                                 ctl, pending, s, nullptr));
     }
     unsigned long long acc = 0;
     NA_CUDA(cudaMemcpyAsync(&acc, counters, sizeof(acc), cudaMemcpyDeviceToHost, s));

@@ -18,7 +18,8 @@ import numpy as np
 from . import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libsetsm_vll.so")
+# SETSM_VLL_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("SETSM_VLL_LIB") or os.path.join(HERE, "lib", "libsetsm_vll.so")
 
 KERNELS = {"plain": abi.VLL_KERNEL_FP64_PLAIN, "split": abi.VLL_KERNEL_SPLIT}
 
@@ -27,7 +28,7 @@ EXPORTED = [
     "vll_get_stream", "vll_voxel_count", "vll_vertical_line_locus",
     "vll_vertical_line_locus_device", "vll_awncc_peaks", "vll_preprocess_level",
     "vll_preprocess_level_device", "vll_pyramid_down", "vll_pyramid_down_device",
-    "vll_compat_layout", "vll_launch_count",
+    "vll_compat_layout", "vll_launch_count", "vll_debug_slot_rho",
 ]
 
 _lib = None
@@ -71,6 +72,7 @@ def load():
     L.vll_preprocess_level_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, i32, vp, vp]
     L.vll_pyramid_down.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
     L.vll_pyramid_down_device.argtypes = [vp, vp, C.c_uint32, C.c_uint32, vp]
+    L.vll_debug_slot_rho.argtypes = [vp, C.POINTER(abi.LevelDesc), vp, vp, i32, vp, i64, vp]
     L.vll_launch_count.argtypes = [vp]
     L.vll_launch_count.restype = i64
     L.vll_compat_layout.argtypes = [vp, i32]
@@ -144,6 +146,26 @@ class Context:
             self._h, C.byref(desc), d_gridpt3, d_ncc, d_vox, d_voxoff, KERNELS[kernel],
             C.byref(st) if st is not None else None))
         return st
+
+    DIAG_NAMES = ("cyc_setup", "cyc_coords", "cyc_stage", "cyc_window", "cyc_scan", "cyc_recheck",
+                  "cyc_fold", "_", "nodes", "chunks", "slow_lanes", "unstaged_chunks",
+                  "plain_nodes", "rounds", "rechecks", "_")
+
+    def debug_slot_rho(self, inputs, nccresult: np.ndarray, kernel: str, diag: dict | None = None) -> tuple:
+        """Per-slot rho of `kernel` (FP32 values before re-checks for the split
+        kernel); returns (rho, offsets) with NaN for slots not evaluated."""
+        k = ((inputs.gridpt3["maxHeight"].astype(np.int64) - inputs.gridpt3["minHeight"])
+             / inputs.height_step).astype(np.int64) & 0xFFFF
+        off = np.concatenate([[0], np.cumsum(k)]).astype(np.int64)
+        out = np.empty(max(int(off[-1]), 1))
+        d = inputs.desc()
+        dg = np.zeros(16, dtype=np.uint64)
+        self._check(load().vll_debug_slot_rho(self._h, C.byref(d), inputs.gridpt3.ctypes.data,
+                                              nccresult.ctypes.data, KERNELS[kernel],
+                                              out.ctypes.data, out.size, dg.ctypes.data))
+        if diag is not None:
+            diag.update({n: int(v) for n, v in zip(self.DIAG_NAMES, dg) if n != "_"})
+        return out[:off[-1]], off
 
     def awncc(self, inputs, nccresult: np.ndarray, voxels: np.ndarray) -> abi.Stats:
         """Non-SGM peak loop of AWNCC over the packed voxel rows."""
