@@ -119,6 +119,29 @@ __global__ void __launch_bounds__(256) items_kernel(int64_t n, const int32_t *__
 // four cubics in the normalised height.  RPC00B terms grouped by power of H:
 //   a0: 1 L P LP LL PP LLL LPP LLP PPP   a1: H LH PH PLH LLH PPH
 //   a2: HH LHH PHH                        a3: HHH
+// Coefficients a0..a3 of one of the four RPC cubics (j: LINE_NUM, LINE_DEN,
+// SAMP_NUM, SAMP_DEN) as a polynomial in the normalised height, for fixed
+// normalised L, P (with the reference's +-360 wrap).
+__device__ __forceinline__ void node_horner_poly(const double *rpc, double lon, double lat, int j,
+                                                 double *a) {
+    double L = (lon - rpc[2]) / rpc[7];
+    double P = (lat - rpc[3]) / rpc[8];
+    if (L < -10.0 || L > 10.0) {
+        const double X = lon > 0 ? lon - 360 : lon + 360;
+        L = (X - rpc[2]) / rpc[7];
+    }
+    if (P < -10.0 || P > 10.0) {
+        const double Y = lat > 0 ? lat - 360 : lat + 360;
+        P = (Y - rpc[3]) / rpc[8];
+    }
+    const double *c = rpc + 10 + 20 * j;
+    a[0] = c[0] + c[1] * L + c[2] * P + c[4] * L * P + c[7] * L * L + c[8] * P * P +
+           c[11] * L * L * L + c[12] * L * P * P + c[14] * L * L * P + c[15] * P * P * P;
+    a[1] = c[3] + c[5] * L + c[6] * P + c[10] * P * L + c[17] * L * L + c[18] * P * P;
+    a[2] = c[9] + c[13] * L + c[16] * P;
+    a[3] = c[19];
+}
+
 __device__ __forceinline__ void node_horner(const double *rpc, double lon, double lat, double *coef4x4,
                             double *hn) {
     double L = (lon - rpc[2]) / rpc[7];
@@ -209,6 +232,10 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
     PatchSrc S, Sn;
     make_src(P, 1, S, Sn);
     const bool voxels = P.vox && !P.cmr && !P.is_ra;
+    // 16-byte aligned image rows allow 128-bit staging loads
+    const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
+                        ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
+                          reinterpret_cast<uintptr_t>(tI.img) | reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
     unsigned long long evals = 0;
     constexpr int kGrab = 4;
     for (;;) {
@@ -234,12 +261,10 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
             if (lane < 8) {
                 const int im = lane >> 2, j = lane & 3;
                 const double *rpc = (im == 0 ? ri : tI).rpc;
-                double cf[16], hn[2];
-                node_horner(rpc, lon, lat, cf, hn);
-                for (int q = 0; q < 4; ++q) W.horner[im][j][q] = cf[4 * j + q];
+                node_horner_poly(rpc, lon, lat, j, W.horner[im][j]);
                 if (j == 0) {
-                    W.hnorm[im][0] = hn[0];
-                    W.hnorm[im][1] = hn[1];
+                    W.hnorm[im][0] = rpc[4];
+                    W.hnorm[im][1] = rpc[9];
                 }
             }
             __syncwarp();
@@ -297,9 +322,11 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
             bool staged = false;
             int rbw = 0, rbh = 0, tbw = 0;
             if (__any_sync(0xffffffffu, inside)) {
-                rbw = rx1 - rx0 + 1;
+                const int rw = rx1 - rx0 + 1, tw = tx1 - tx0 + 1;
+                // odd row strides spread consecutive rows over the shared-memory bank groups
+                rbw = rw | 1;
                 rbh = ry1 - ry0 + 1;
-                tbw = tx1 - tx0 + 1;
+                tbw = tw | 1;
                 const int tbh = ty1 - ty0 + 1;
                 if (rbw * rbh + tbw * tbh <= warp_quads) {
                     float sI = 0.f, sM = 0.f, tsI = 0.f, tsM = 0.f;
@@ -315,9 +342,18 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
                     sM = __shfl_sync(0xffffffffu, sM, 0);
                     tsI = __shfl_sync(0xffffffffu, tsI, 0);
                     tsM = __shfl_sync(0xffffffffu, tsM, 0);
-                    const bool z1 = stage_box(boxes, ri.img, ri.mag, ri.w, rx0, ry0, rbw, rbh, sI, sM, lane);
-                    const bool z2 = stage_box(boxes + rbw * rbh, tI.img, tI.mag, tI.w, tx0, ty0, tbw,
-                                              tbh, tsI, tsM, lane);
+                    bool z1, z2;
+                    if (vec_ok) {
+                        z1 = stage_box_vec(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh, sI,
+                                           sM, lane);
+                        z2 = stage_box_vec(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0, ty0,
+                                           tw, tbh, tsI, tsM, lane);
+                    } else {
+                        z1 = stage_box_strided(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh,
+                                               sI, sM, lane);
+                        z2 = stage_box_strided(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0,
+                                               ty0, tw, tbh, tsI, tsM, lane);
+                    }
                     __syncwarp();
                     staged = !(z1 || z2);
                 }

@@ -198,6 +198,75 @@ __device__ __forceinline__ void window_fp32(const float4 *__restrict__ qr, int r
     if (nv == 0) incc_avg = -2.0f;   // no valid correlation: count_incc stays 0
 }
 
+// Vectorised staging of the same box: each lane converts one 8-texel,
+// 16-byte-aligned chunk of a box row per plane (two 128-bit loads) into up to
+// eight texel pairs.  Requires the image rows to start on 16-byte boundaries
+// (width multiple of 8 and 16-byte aligned planes); `dst` rows have stride
+// `ds` pairs.  Returns (warp-uniform) whether an intensity texel is zero.
+__device__ __forceinline__ bool stage_box_vec(float4 *__restrict__ dst, int ds,
+                                              const uint16_t *__restrict__ I,
+                                              const uint16_t *__restrict__ M, uint32_t W, int x0,
+                                              int y0, int bw, int bh, float sI, float sM, int lane) {
+    bool zero = false;
+    const int xa = x0 & ~7;
+    const int x1 = x0 + bw - 1;                 // last pair's left texel
+    const int nch = ((x1 + 1) - xa) / 8 + 1;    // chunks covering [xa, x1 + 1]
+    const int n = nch * bh;
+    for (int i = lane; i < n; i += 32) {
+        const int by = i / nch;
+        const int c = i - by * nch;
+        const int xc = xa + 8 * c;
+        const int64_t row = (int64_t)(y0 + by) * W;
+        const uint4 vi = __ldg(reinterpret_cast<const uint4 *>(I + row + xc));
+        const uint4 vm = __ldg(reinterpret_cast<const uint4 *>(M + row + xc));
+        const bool need9 = xc + 7 <= x1;        // the 8th pair needs texel xc + 8
+        const uint16_t i8 = need9 ? __ldg(I + row + xc + 8) : (uint16_t)0;
+        const uint16_t m8 = need9 ? __ldg(M + row + xc + 8) : (uint16_t)0;
+        float fi[9], fm[9];
+        const uint32_t wi[4] = {vi.x, vi.y, vi.z, vi.w};
+        const uint32_t wm[4] = {vm.x, vm.y, vm.z, vm.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            fi[2 * q] = (float)(wi[q] & 0xFFFFu) - sI;
+            fi[2 * q + 1] = (float)(wi[q] >> 16) - sI;
+            fm[2 * q] = (float)(wm[q] & 0xFFFFu) - sM;
+            fm[2 * q + 1] = (float)(wm[q] >> 16) - sM;
+            zero |= (xc + 2 * q >= x0 && xc + 2 * q <= x1 + 1 && (wi[q] & 0xFFFFu) == 0);
+            zero |= (xc + 2 * q + 1 >= x0 && xc + 2 * q + 1 <= x1 + 1 && (wi[q] >> 16) == 0);
+        }
+        fi[8] = (float)i8 - sI;
+        fm[8] = (float)m8 - sM;
+        zero |= need9 && i8 == 0;
+        float4 *drow = dst + by * ds;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int x = xc + t;
+            if (x >= x0 && x <= x1) drow[x - x0] = make_float4(fi[t], fm[t], fi[t + 1], fm[t + 1]);
+        }
+    }
+    return __any_sync(0xffffffffu, zero);
+}
+
+// Scalar staging of a box whose destination rows have stride `ds` pairs
+// (used when image rows are not 16-byte aligned).
+__device__ __forceinline__ bool stage_box_strided(float4 *__restrict__ dst, int ds,
+                                                  const uint16_t *__restrict__ I,
+                                                  const uint16_t *__restrict__ M, uint32_t W, int x0,
+                                                  int y0, int bw, int bh, float sI, float sM, int lane) {
+    bool zero = false;
+    const int n = bw * bh;
+    for (int i = lane; i < n; i += 32) {
+        const int by = i / bw;
+        const int bx = i - by * bw;
+        const int64_t p = (int64_t)(y0 + by) * W + (x0 + bx);
+        const uint16_t a = __ldg(I + p), b = __ldg(I + p + 1);
+        const uint16_t cm = __ldg(M + p), d = __ldg(M + p + 1);
+        zero |= (a == 0) | (b == 0);
+        dst[by * ds + bx] = make_float4((float)a - sI, (float)cm - sM, (float)b - sI, (float)d - sM);
+    }
+    return __any_sync(0xffffffffu, zero);
+}
+
 // Stages the texel pairs of box [x0, x0+bw) x [y0, y0+bh) of one image into
 // shared memory as float4 {I(x)-sI, M(x)-sM, I(x+1)-sI, M(x+1)-sM}; returns
 // true (warp-uniform) when some intensity texel in the box is zero.
