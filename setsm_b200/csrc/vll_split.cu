@@ -142,49 +142,36 @@ __device__ __forceinline__ void node_horner_poly(const double *rpc, double lon, 
     a[3] = c[19];
 }
 
-__device__ __forceinline__ void node_horner(const double *rpc, double lon, double lat, double *coef4x4,
-                            double *hn) {
-    double L = (lon - rpc[2]) / rpc[7];
-    double P = (lat - rpc[3]) / rpc[8];
-    if (L < -10.0 || L > 10.0) {
-        const double X = lon > 0 ? lon - 360 : lon + 360;
-        L = (X - rpc[2]) / rpc[7];
-    }
-    if (P < -10.0 || P > 10.0) {
-        const double Y = lat > 0 ? lat - 360 : lat + 360;
-        P = (Y - rpc[3]) / rpc[8];
-    }
-    for (int j = 0; j < 4; ++j) {
-        const double *c = rpc + 10 + 20 * j;
-        double *a = coef4x4 + 4 * j;
-        a[0] = c[0] + c[1] * L + c[2] * P + c[4] * L * P + c[7] * L * L + c[8] * P * P +
-               c[11] * L * L * L + c[12] * L * P * P + c[14] * L * L * P + c[15] * P * P * P;
-        a[1] = c[3] + c[5] * L + c[6] * P + c[10] * P * L + c[17] * L * L + c[18] * P * P;
-        a[2] = c[9] + c[13] * L + c[16] * P;
-        a[3] = c[19];
-    }
-    hn[0] = rpc[4];
-    hn[1] = rpc[9];
+// Reciprocal for the fast geometry path: FP32 seed refined by two Newton
+// steps (relative error ~1e-16).  A seed that is not a finite non-zero float
+// sends the slot to the exact projection.
+__device__ __forceinline__ double fast_rcp(double v, bool &edge) {
+    const float f = __frcp_rn((float)v);
+    if (!(fabsf(f) > 0.f && fabsf(f) < 3.0e38f)) edge = true;
+    double r = (double)f;
+    r = fma(r, fma(-v, r, 1.0), r);
+    r = fma(r, fma(-v, r, 1.0), r);
+    return r;
 }
 
 // Image coordinate (pyramid level) of one slot from the per-node cubics.
 // Sets `edge` when a coordinate is too close to an integer, or to a clamp,
 // for the Horner rounding to be trusted with the reference's integer tests.
 __device__ __forceinline__ double2 fast_coord(const double (*a)[4], const double *hn,
-                                              const DevImage &im, double hgt, int L, bool &edge) {
-    const double H = (hgt - hn[0]) / hn[1];
+                                              const DevImage &im, double hgt, double inv_s,
+                                              bool &edge) {
+    const double H = (hgt - hn[0]) * hn[1];   // hn[1]: reciprocal of the height scale
     double v[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) v[j] = fma(fma(fma(a[j][3], H, a[j][2]), H, a[j][1]), H, a[j][0]);
-    double y = im.adj[0] + ((v[0] / v[1]) * im.rpc[5] + im.rpc[0]);
-    double x = im.adj[1] + ((v[2] / v[3]) * im.rpc[6] + im.rpc[1]);
+    double y = im.adj[0] + ((v[0] * fast_rcp(v[1], edge)) * im.rpc[5] + im.rpc[0]);
+    double x = im.adj[1] + ((v[2] * fast_rcp(v[3], edge)) * im.rpc[6] + im.rpc[1]);
     const double ymax = im.rpc[0] + im.rpc[5] * 1.2, xmax = im.rpc[1] + im.rpc[6] * 1.2;
     if (fabs(y) < kEdge || fabs(y - ymax) < kEdge || fabs(x) < kEdge || fabs(x - xmax) < kEdge)
         edge = true;
     y = y < 0 ? 0 : (y > ymax ? ymax : y);
     x = x < 0 ? 0 : (x > xmax ? xmax : x);
-    const double s = (double)(1 << L);
-    const double px = x / s - im.sx, py = y / s - im.sy;
+    const double px = x * inv_s - im.sx, py = y * inv_s - im.sy;   // inv_s = 2^-L (exact)
     const double fx = px - floor(px), fy = py - floor(py);
     if (fx < kEdge || fx > 1.0 - kEdge || fy < kEdge || fy > 1.0 - kEdge) edge = true;
     return make_double2(px, py);
@@ -203,11 +190,19 @@ __device__ __forceinline__ bool near_trunc(double v) {
 // ---------------------------------------------------------------------------
 // window kernel
 // ---------------------------------------------------------------------------
-constexpr int kWinWarps = 4;
+// Warps per window block and the minimum resident blocks per SM (the latter
+// sets the register budget: 65536 / (warps * 32 * blocks)).
+#ifndef VLL_WIN_WARPS
+#define VLL_WIN_WARPS 4
+#endif
+#ifndef VLL_WIN_MINB
+#define VLL_WIN_MINB 3
+#endif
+constexpr int kWinWarps = VLL_WIN_WARPS;
 
 struct WinShared {
     double horner[2][4][4];          // [image][num/den poly][a0..a3]
-    double hnorm[2][2];              // [image] {h_off, h_scale}
+    double hnorm[2][2];              // [image] {h_off, 1 / h_scale}
 };
 
 __host__ __device__ constexpr size_t win_boxes_offset() {
@@ -215,7 +210,7 @@ __host__ __device__ constexpr size_t win_boxes_offset() {
 }
 
 template <int H>
-__global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
+__global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     const DevLevel *__restrict__ Pp, const int64_t *__restrict__ items, int64_t n_items,
     const int64_t *__restrict__ slot_off, const double *__restrict__ gsum,
     const double *__restrict__ gcnt, float2 *__restrict__ rho,
@@ -236,6 +231,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
     const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
                         ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
                           reinterpret_cast<uintptr_t>(tI.img) | reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
+    const double inv_s = 1.0 / (double)(1 << P.L);
     unsigned long long evals = 0;
     constexpr int kGrab = 4;
     for (;;) {
@@ -264,7 +260,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
                 node_horner_poly(rpc, lon, lat, j, W.horner[im][j]);
                 if (j == 0) {
                     W.hnorm[im][0] = rpc[4];
-                    W.hnorm[im][1] = rpc[9];
+                    W.hnorm[im][1] = 1.0 / rpc[9];
                 }
             }
             __syncwarp();
@@ -277,8 +273,8 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
                 hgt = slot_height(P, start_H, ncc_min, k);
                 if (hgt >= (float)start_H && hgt <= (float)end_H) {
                     bool edge = false;
-                    rp = fast_coord(W.horner[0], W.hnorm[0], ri, (double)hgt, P.L, edge);
-                    tp = fast_coord(W.horner[1], W.hnorm[1], tI, (double)hgt, P.L, edge);
+                    rp = fast_coord(W.horner[0], W.hnorm[0], ri, (double)hgt, inv_s, edge);
+                    tp = fast_coord(W.horner[1], W.hnorm[1], tI, (double)hgt, inv_s, edge);
                     if (edge) {
                         rp = to_pyramid(rpc_project(ri.rpc, ri.adj, lon, lat, (double)hgt), ri.sx, ri.sy, P.L);
                         tp = to_pyramid(rpc_project(tI.rpc, tI.adj, lon, lat, (double)hgt), tI.sx, tI.sy, P.L);
@@ -308,17 +304,14 @@ __global__ void __launch_bounds__(kWinWarps * 32, 3) window_kernel(
             int rx1 = inside ? rix + H + 1 : INT_MIN, ry1 = inside ? riy + H + 1 : INT_MIN;
             int tx0 = inside ? tix - R : INT_MAX, ty0 = inside ? tiy - R : INT_MAX;
             int tx1 = inside ? tix + R + 1 : INT_MIN, ty1 = inside ? tiy + R + 1 : INT_MIN;
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                rx0 = min(rx0, __shfl_xor_sync(0xffffffffu, rx0, o));
-                ry0 = min(ry0, __shfl_xor_sync(0xffffffffu, ry0, o));
-                rx1 = max(rx1, __shfl_xor_sync(0xffffffffu, rx1, o));
-                ry1 = max(ry1, __shfl_xor_sync(0xffffffffu, ry1, o));
-                tx0 = min(tx0, __shfl_xor_sync(0xffffffffu, tx0, o));
-                ty0 = min(ty0, __shfl_xor_sync(0xffffffffu, ty0, o));
-                tx1 = max(tx1, __shfl_xor_sync(0xffffffffu, tx1, o));
-                ty1 = max(ty1, __shfl_xor_sync(0xffffffffu, ty1, o));
-            }
+            rx0 = __reduce_min_sync(0xffffffffu, rx0);
+            ry0 = __reduce_min_sync(0xffffffffu, ry0);
+            rx1 = __reduce_max_sync(0xffffffffu, rx1);
+            ry1 = __reduce_max_sync(0xffffffffu, ry1);
+            tx0 = __reduce_min_sync(0xffffffffu, tx0);
+            ty0 = __reduce_min_sync(0xffffffffu, ty0);
+            tx1 = __reduce_max_sync(0xffffffffu, tx1);
+            ty1 = __reduce_max_sync(0xffffffffu, ty1);
             bool staged = false;
             int rbw = 0, rbh = 0, tbw = 0;
             if (__any_sync(0xffffffffu, inside)) {

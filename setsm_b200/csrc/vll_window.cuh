@@ -28,15 +28,6 @@ __host__ __device__ constexpr int ring_count(int H, int ring) {
     return n;
 }
 
-// floor and fraction of a small float with full-rate ALU ops only:
-// round-to-nearest of (x - 0.5) through the 1.5*2^23 magic constant.
-__device__ __forceinline__ int floor_frac(float x, float &frac) {
-    const float t = __fadd_rn(__fadd_rn(x, -0.5f), 12582912.0f);
-    const float r = __fadd_rn(t, -12582912.0f);
-    frac = x - r;
-    return __float_as_int(t) - 0x4B400000;
-}
-
 struct Acc {
     float sl, sr, sll, srr, slr;
 };
@@ -56,57 +47,80 @@ __device__ __forceinline__ float corr_from(const Acc &a, float n, bool &unsure) 
     return cv * rsqrtf(vl * vr);
 }
 
-struct WinCtx {
-    float w00, w10, w01, w11;    // reference bilinear weights (same for all samples)
-    float c, s;                  // target rotation cos(-theta), sin(-theta)
-    float cI, cM, tcI, tcM;      // centring samples (window centre)
-    int rbw, tbw;                // staged box widths (texel pairs)
+// Packed (intensity, magnitude) arithmetic: sm_100 issues one FFMA2/FADD2
+// for both planes of a sample.
+__device__ __forceinline__ float2 lo2(const float4 &v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4 &v) { return make_float2(v.z, v.w); }
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+// b - a with a single rounding (fma with a -1 multiplier)
+__device__ __forceinline__ float2 sub2(float2 b, float2 a) {
+    return __ffma2_rn(a, make_float2(-1.f, -1.f), b);
+}
+
+constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
+
+// Window sums of one ring for both planes: .x intensity, .y magnitude.
+struct Acc2 {
+    float2 sl, sr, sll, srr, slr;
 };
+
+struct WinCtx {
+    float2 w00, w10, w01, w11;   // reference bilinear weights (same for all samples), broadcast
+    float2 ncl;                  // -(reference centre sample) per plane
+    float2 ntc;                  // -(target centre sample) per plane
+    float2 cs;                   // target rotation (cos(-theta), sin(-theta))
+    float2 nsc;                  // (-sin(-theta), cos(-theta))
+    int rbw, tbw;                // staged box row strides (texel pairs)
+};
+
+// Reference-window sample from the staged pairs of rows y (a) and y+1 (b),
+// plus `init` (the negated centre, or zero).
+__device__ __forceinline__ float2 ref_sample(const WinCtx &x, const float4 &a, const float4 &b,
+                                             float2 init) {
+    float2 l = __ffma2_rn(x.w00, lo2(a), init);
+    l = __ffma2_rn(x.w10, hi2(a), l);
+    l = __ffma2_rn(x.w01, lo2(b), l);
+    return __ffma2_rn(x.w11, hi2(b), l);
+}
+
+// Target sample at box-relative position f (x, y): floor and fraction through
+// the 1.5*2^23 round-to-nearest constant, then bilinear on both planes.
+__device__ __forceinline__ float2 tgt_sample(const float4 *__restrict__ qt, int tbw, float2 f,
+                                             float2 init) {
+    const float2 t = __fadd2_rn(__fadd2_rn(f, make_float2(-0.5f, -0.5f)), bc2(kMagic));
+    const float2 fr = __fadd2_rn(f, __ffma2_rn(t, make_float2(-1.f, -1.f), bc2(kMagic)));
+    const int ix = __float_as_int(t.x) - 0x4B400000;
+    const int iy = __float_as_int(t.y) - 0x4B400000;
+    const float4 *p = qt + iy * tbw + ix;
+    const float4 ta = p[0];
+    const float4 tb = p[tbw];
+    const float2 fx = bc2(fr.x), fy = bc2(fr.y);
+    const float2 top = __ffma2_rn(fx, sub2(hi2(ta), lo2(ta)), lo2(ta));
+    const float2 bot = __ffma2_rn(fx, sub2(hi2(tb), lo2(tb)), lo2(tb));
+    return __fadd2_rn(__ffma2_rn(fy, sub2(bot, top), top), init);
+}
 
 // One window row of sub-window pattern |row| = AR at signed offset `row`:
 // columns unrolled, each accumulating into its compile-time ring.
 template <int H, int AR>
 __device__ __forceinline__ void win_row(const WinCtx &x, int row, const float4 *__restrict__ qr,
-                                        const float4 *__restrict__ qt, float tfx, float tfy,
-                                        Acc (&acc)[3][2]) {
+                                        const float4 *__restrict__ qt, float2 tf,
+                                        Acc2 (&acc)[3]) {
     const float4 *q0 = qr + (row + H) * x.rbw;
     const float4 *q1 = q0 + x.rbw;
-    const float bx = fmaf(-x.s, (float)row, tfx);
-    const float by = fmaf(x.c, (float)row, tfy);
+    const float2 b = __ffma2_rn(x.nsc, bc2((float)row), tf);
 #pragma unroll
     for (int col = -H; col <= H; ++col) {
         if (AR * AR + col * col > (H + 1) * (H + 1)) continue;
         const int ring = ring_of(H, AR, col);
-        const float4 a = q0[col + H];
-        const float4 b = q1[col + H];
-        const float lI = fmaf(x.w11, b.z, fmaf(x.w01, b.x, fmaf(x.w10, a.z, x.w00 * a.x))) - x.cI;
-        const float lM = fmaf(x.w11, b.w, fmaf(x.w01, b.y, fmaf(x.w10, a.w, x.w00 * a.y))) - x.cM;
-        const float fx = fmaf(x.c, (float)col, bx);
-        const float fy = fmaf(x.s, (float)col, by);
-        float frx, fry;
-        const int ix = floor_frac(fx, frx);
-        const int iy = floor_frac(fy, fry);
-        const float4 *t = qt + iy * x.tbw + ix;
-        const float4 ta = t[0];
-        const float4 tb = t[x.tbw];
-        const float topI = fmaf(frx, ta.z - ta.x, ta.x);
-        const float botI = fmaf(frx, tb.z - tb.x, tb.x);
-        const float rI = fmaf(fry, botI - topI, topI) - x.tcI;
-        const float topM = fmaf(frx, ta.w - ta.y, ta.y);
-        const float botM = fmaf(frx, tb.w - tb.y, tb.y);
-        const float rM = fmaf(fry, botM - topM, topM) - x.tcM;
-        Acc &u = acc[ring][0];
-        u.sl += lI;
-        u.sr += rI;
-        u.sll = fmaf(lI, lI, u.sll);
-        u.srr = fmaf(rI, rI, u.srr);
-        u.slr = fmaf(lI, rI, u.slr);
-        Acc &v = acc[ring][1];
-        v.sl += lM;
-        v.sr += rM;
-        v.sll = fmaf(lM, lM, v.sll);
-        v.srr = fmaf(rM, rM, v.srr);
-        v.slr = fmaf(lM, rM, v.slr);
+        const float2 l = ref_sample(x, q0[col + H], q1[col + H], x.ncl);
+        const float2 r = tgt_sample(qt, x.tbw, __ffma2_rn(x.cs, bc2((float)col), b), x.ntc);
+        Acc2 &u = acc[ring];
+        u.sl = __fadd2_rn(u.sl, l);
+        u.sr = __fadd2_rn(u.sr, r);
+        u.sll = __ffma2_rn(l, l, u.sll);
+        u.srr = __ffma2_rn(r, r, u.srr);
+        u.slr = __ffma2_rn(l, r, u.slr);
     }
 }
 
@@ -114,14 +128,27 @@ __device__ __forceinline__ void win_row(const WinCtx &x, int row, const float4 *
 // symmetric), so each pattern's unrolled code serves two rows.
 template <int H, int AR>
 __device__ __forceinline__ void win_rows(const WinCtx &x, const float4 *__restrict__ qr,
-                                         const float4 *__restrict__ qt, float tfx, float tfy,
-                                         Acc (&acc)[3][2]) {
+                                         const float4 *__restrict__ qt, float2 tf,
+                                         Acc2 (&acc)[3]) {
     if constexpr (AR <= H) {
 #pragma unroll 1
         for (int sgn = (AR == 0 ? 1 : -1); sgn <= 1; sgn += 2)
-            win_row<H, AR>(x, sgn * AR, qr, qt, tfx, tfy, acc);
-        win_rows<H, AR + 1>(x, qr, qt, tfx, tfy, acc);
+            win_row<H, AR>(x, sgn * AR, qr, qt, tf, acc);
+        win_rows<H, AR + 1>(x, qr, qt, tf, acc);
     }
+}
+
+__device__ __forceinline__ Acc plane(const Acc2 &a, int p) {
+    return p == 0 ? Acc{a.sl.x, a.sr.x, a.sll.x, a.srr.x, a.slr.x}
+                  : Acc{a.sl.y, a.sr.y, a.sll.y, a.srr.y, a.slr.y};
+}
+
+__device__ __forceinline__ void add_to(Acc2 &w, const Acc2 &a) {
+    w.sl = __fadd2_rn(w.sl, a.sl);
+    w.sr = __fadd2_rn(w.sr, a.sr);
+    w.sll = __fadd2_rn(w.sll, a.sll);
+    w.srr = __fadd2_rn(w.srr, a.srr);
+    w.slr = __fadd2_rn(w.slr, a.slr);
 }
 
 // FP32 multi-window NCC of one slot (ComputeMultiNCC over the three nested
@@ -134,61 +161,42 @@ __device__ __forceinline__ void window_fp32(const float4 *__restrict__ qr, int r
                                             float rfy, const float4 *__restrict__ qt, int tbw,
                                             float tfx, float tfy, float c, float s,
                                             float &incc_avg, bool &unsure) {
-    Acc acc[3][2];
+    Acc2 acc[3];
+    const float2 z = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int p = 0; p < 2; ++p) acc[r][p] = Acc{0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int r = 0; r < 3; ++r) acc[r] = Acc2{z, z, z, z, z};
     WinCtx x;
-    x.w00 = (1.f - rfx) * (1.f - rfy);
-    x.w10 = rfx * (1.f - rfy);
-    x.w01 = (1.f - rfx) * rfy;
-    x.w11 = rfx * rfy;
-    x.c = c;
-    x.s = s;
+    x.w00 = bc2((1.f - rfx) * (1.f - rfy));
+    x.w10 = bc2(rfx * (1.f - rfy));
+    x.w01 = bc2((1.f - rfx) * rfy);
+    x.w11 = bc2(rfx * rfy);
+    x.cs = make_float2(c, s);
+    x.nsc = make_float2(-s, c);
     x.rbw = rbw;
     x.tbw = tbw;
+    const float2 tf = make_float2(tfx, tfy);
     {
-        const float4 a = qr[H * rbw + H];
-        const float4 b = qr[(H + 1) * rbw + H];
-        x.cI = fmaf(x.w11, b.z, fmaf(x.w01, b.x, fmaf(x.w10, a.z, x.w00 * a.x)));
-        x.cM = fmaf(x.w11, b.w, fmaf(x.w01, b.y, fmaf(x.w10, a.w, x.w00 * a.y)));
-        float frx, fry;
-        const int ix = floor_frac(tfx, frx);
-        const int iy = floor_frac(tfy, fry);
-        const float4 *t = qt + iy * tbw + ix;
-        const float4 ta = t[0];
-        const float4 tb = t[tbw];
-        const float topI = fmaf(frx, ta.z - ta.x, ta.x);
-        const float botI = fmaf(frx, tb.z - tb.x, tb.x);
-        x.tcI = fmaf(fry, botI - topI, topI);
-        const float topM = fmaf(frx, ta.w - ta.y, ta.y);
-        const float botM = fmaf(frx, tb.w - tb.y, tb.y);
-        x.tcM = fmaf(fry, botM - topM, topM);
+        const float2 cl = ref_sample(x, qr[H * rbw + H], qr[(H + 1) * rbw + H], z);
+        const float2 ct = tgt_sample(qt, tbw, tf, z);
+        x.ncl = make_float2(-cl.x, -cl.y);
+        x.ntc = make_float2(-ct.x, -ct.y);
     }
-    win_rows<H, 0>(x, qr, qt, tfx, tfy, acc);
+    win_rows<H, 0>(x, qr, qt, tf, acc);
     // nested windows: 2 = ring 2; 1 = rings 1+2; 0 = all rings
     constexpr int n2 = ring_count(H, 2);
     constexpr int n1 = n2 + ring_count(H, 1);
     constexpr int n0 = n1 + ring_count(H, 0);
+    Acc2 w1 = acc[2];
+    add_to(w1, acc[1]);
+    Acc2 w0 = w1;
+    add_to(w0, acc[0]);
     float tot = 0.f;
     int nv = 0;
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
-        Acc w = acc[2][p];
-        const float r2 = corr_from(w, (float)n2, unsure);
-        w.sl += acc[1][p].sl;
-        w.sr += acc[1][p].sr;
-        w.sll += acc[1][p].sll;
-        w.srr += acc[1][p].srr;
-        w.slr += acc[1][p].slr;
-        const float r1 = corr_from(w, (float)n1, unsure);
-        w.sl += acc[0][p].sl;
-        w.sr += acc[0][p].sr;
-        w.sll += acc[0][p].sll;
-        w.srr += acc[0][p].srr;
-        w.slr += acc[0][p].slr;
-        const float r0 = corr_from(w, (float)n0, unsure);
+        const float r2 = corr_from(plane(acc[2], p), (float)n2, unsure);
+        const float r1 = corr_from(plane(w1, p), (float)n1, unsure);
+        const float r0 = corr_from(plane(w0, p), (float)n0, unsure);
         if (r0 != -99.0f) { tot += r0; ++nv; }
         if (r1 != -99.0f) { tot += r1; ++nv; }
         if (r2 != -99.0f) { tot += r2; ++nv; }
@@ -198,16 +206,31 @@ __device__ __forceinline__ void window_fp32(const float4 *__restrict__ qr, int r
     if (nv == 0) incc_avg = -2.0f;   // no valid correlation: count_incc stays 0
 }
 
-// Vectorised staging of the same box: each lane converts one 8-texel,
+// u16 texel pair (intensity word, magnitude word; low or high halves by
+// `sel`) as floats minus the box shift: the texel is placed in the mantissa
+// of 2^23 (exact), and `nshift` = -(2^23 + shift) removes both at once.
+__device__ __forceinline__ float2 texel_pair(uint32_t wi, uint32_t wm, uint32_t sel, float2 nshift) {
+    const float a = __int_as_float(__byte_perm(wi, 0x4B000000u, sel));
+    const float b = __int_as_float(__byte_perm(wm, 0x4B000000u, sel));
+    return __fadd2_rn(make_float2(a, b), nshift);
+}
+
+// Non-zero when some 16-bit half of w is zero.
+__device__ __forceinline__ uint32_t zero_half(uint32_t w) { return (w - 0x00010001u) & ~w; }
+
+// Vectorised staging of the box: each lane converts one 8-texel,
 // 16-byte-aligned chunk of a box row per plane (two 128-bit loads) into up to
 // eight texel pairs.  Requires the image rows to start on 16-byte boundaries
 // (width multiple of 8 and 16-byte aligned planes); `dst` rows have stride
-// `ds` pairs.  Returns (warp-uniform) whether an intensity texel is zero.
+// `ds` pairs.  Returns (warp-uniform) whether an intensity texel of the loaded
+// chunks is zero (a superset of the box: the caller then takes the exact path).
 __device__ __forceinline__ bool stage_box_vec(float4 *__restrict__ dst, int ds,
                                               const uint16_t *__restrict__ I,
                                               const uint16_t *__restrict__ M, uint32_t W, int x0,
                                               int y0, int bw, int bh, float sI, float sM, int lane) {
-    bool zero = false;
+    uint32_t zacc = 0;
+    bool z8 = false;
+    const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
     const int xa = x0 & ~7;
     const int x1 = x0 + bw - 1;                 // last pair's left texel
     const int nch = ((x1 + 1) - xa) / 8 + 1;    // chunks covering [xa, x1 + 1]
@@ -220,31 +243,28 @@ __device__ __forceinline__ bool stage_box_vec(float4 *__restrict__ dst, int ds,
         const uint4 vi = __ldg(reinterpret_cast<const uint4 *>(I + row + xc));
         const uint4 vm = __ldg(reinterpret_cast<const uint4 *>(M + row + xc));
         const bool need9 = xc + 7 <= x1;        // the 8th pair needs texel xc + 8
-        const uint16_t i8 = need9 ? __ldg(I + row + xc + 8) : (uint16_t)0;
-        const uint16_t m8 = need9 ? __ldg(M + row + xc + 8) : (uint16_t)0;
-        float fi[9], fm[9];
-        const uint32_t wi[4] = {vi.x, vi.y, vi.z, vi.w};
-        const uint32_t wm[4] = {vm.x, vm.y, vm.z, vm.w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            fi[2 * q] = (float)(wi[q] & 0xFFFFu) - sI;
-            fi[2 * q + 1] = (float)(wi[q] >> 16) - sI;
-            fm[2 * q] = (float)(wm[q] & 0xFFFFu) - sM;
-            fm[2 * q + 1] = (float)(wm[q] >> 16) - sM;
-            zero |= (xc + 2 * q >= x0 && xc + 2 * q <= x1 + 1 && (wi[q] & 0xFFFFu) == 0);
-            zero |= (xc + 2 * q + 1 >= x0 && xc + 2 * q + 1 <= x1 + 1 && (wi[q] >> 16) == 0);
-        }
-        fi[8] = (float)i8 - sI;
-        fm[8] = (float)m8 - sM;
-        zero |= need9 && i8 == 0;
+        const uint32_t i8 = need9 ? __ldg(I + row + xc + 8) : 1u;
+        const uint32_t m8 = need9 ? __ldg(M + row + xc + 8) : 0u;
+        zacc |= zero_half(vi.x) | zero_half(vi.y) | zero_half(vi.z) | zero_half(vi.w);
+        z8 |= i8 == 0;
+        float2 f[9];
+        f[0] = texel_pair(vi.x, vm.x, 0x7610, ns);
+        f[1] = texel_pair(vi.x, vm.x, 0x7632, ns);
+        f[2] = texel_pair(vi.y, vm.y, 0x7610, ns);
+        f[3] = texel_pair(vi.y, vm.y, 0x7632, ns);
+        f[4] = texel_pair(vi.z, vm.z, 0x7610, ns);
+        f[5] = texel_pair(vi.z, vm.z, 0x7632, ns);
+        f[6] = texel_pair(vi.w, vm.w, 0x7610, ns);
+        f[7] = texel_pair(vi.w, vm.w, 0x7632, ns);
+        f[8] = texel_pair(i8, m8, 0x7610, ns);
         float4 *drow = dst + by * ds;
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
             const int x = xc + t;
-            if (x >= x0 && x <= x1) drow[x - x0] = make_float4(fi[t], fm[t], fi[t + 1], fm[t + 1]);
+            if (x >= x0 && x <= x1) drow[x - x0] = make_float4(f[t].x, f[t].y, f[t + 1].x, f[t + 1].y);
         }
     }
-    return __any_sync(0xffffffffu, zero);
+    return __any_sync(0xffffffffu, (zacc & 0x80008000u) != 0 || z8);
 }
 
 // Scalar staging of a box whose destination rows have stride `ds` pairs
