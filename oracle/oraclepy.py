@@ -44,6 +44,13 @@ def lib():
                                              vp, vp, vp]
         L.vo_vertical_line_locus.restype = C.c_long
         L.vo_awncc_peaks.argtypes = [C.POINTER(abi.LevelDesc), vp, vp, vp, C.c_long]
+        L.vo_correlate.argtypes = [vp, vp, C.c_int]
+        L.vo_correlate.restype = C.c_double
+        L.vo_quantize_result.argtypes = [C.c_double]
+        L.vo_quantize_result.restype = C.c_int16
+        L.vo_quantize_voxel.argtypes = [C.c_double]
+        L.vo_quantize_voxel.restype = C.c_int16
+        L.vo_window_counts.argtypes = [C.c_int, vp]
         _lib = L
     return _lib
 
@@ -164,3 +171,24 @@ def awncc(inputs, ncc: np.ndarray, voxels: np.ndarray) -> None:
     vp = voxels.ctypes.data if voxels.size else None
     lib().vo_awncc_peaks(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data, vp,
                          voxels.size)
+
+
+def correlate(left, right) -> float:
+    """Correlate (SubFunctions.cpp:974-1018) on two equal-length vectors."""
+    a = np.ascontiguousarray(left, dtype=np.float64)
+    b = np.ascontiguousarray(right, dtype=np.float64)
+    return float(lib().vo_correlate(a.ctypes.data, b.ctypes.data, int(min(a.size, b.size))))
+
+
+def quantize_result(v: float) -> int:
+    return int(lib().vo_quantize_result(float(v)))
+
+
+def quantize_voxel(v: float) -> int:
+    return int(lib().vo_quantize_voxel(float(v)))
+
+
+def window_counts(half: int) -> tuple:
+    out = np.zeros(3, dtype=np.int32)
+    lib().vo_window_counts(int(half), out.ctypes.data)
+    return tuple(int(x) for x in out)

@@ -320,6 +320,51 @@ double ref_get_height_step(int pyramid_step, double im_resolution) {
     return GetHeightStep(pyramid_step, im_resolution);
 }
 
+/* Known-answer hooks: the reference's own building blocks.
+ * Correlate, SubFunctions.cpp:974-1018. */
+double ref_correlate(const double *L, const double *R, int N) { return Correlate(L, R, N); }
+
+/* Sub-window counts from SetVecKernelValue (SubFunctions.cpp:3249-3315) over
+ * the window loop of VerticalLineLocus (setsm_code.cpp:6429-6453), on a
+ * constant image so every sample is valid. */
+void ref_window_counts(int half, int counts[3]) {
+    const int n = 4 * half + 8;
+    std::vector<uint16> img((size_t)n * n, 100);
+    SetKernel k(0, 1, half);
+    KernelPatchArg patch{k, CSize(n, n), CSize(n, n), img.data(), img.data(), img.data(), img.data()};
+    int cnt[3] = {0, 0, 0};
+    const double c = 0.5 * n + 0.25;
+    for (int row = -half; row <= half; row++)
+        for (int col = -half; col <= half; col++) {
+            const int r2 = row * row + col * col;
+            if (r2 <= (half + 1) * (half + 1)) {
+                D2DPOINT p(c + col, c + row);
+                SetVecKernelValue(patch, row, col, p, p, r2, cnt);
+            }
+        }
+    for (int w = 0; w < 3; ++w) counts[w] = cnt[w];
+}
+
+/* Calls a VerticalLineLocus with the reference's exact C++ signature
+ * (setsm_code.hpp:81) -- e.g. the drop-in exported by libsetsm_vll.so -- on
+ * structures built by the reference's own headers, the way Matching_SETSM
+ * calls it (setsm_code.cpp:3829).  Voxels are packed in/out as in
+ * ref_vertical_line_locus. */
+typedef int (*vll_signature)(VOXEL **, const ProInfo *, NCCresult *, LevelInfo &, const UGRID *,
+                             const uint8, const double *);
+long ref_call_vertical_line_locus(void *fn, const vll_level_desc *d, const vll_ugrid *gridpt3,
+                                  vll_nccresult *ncc, vll_voxel *voxels, long cap) {
+    RefLevel L(d);
+    const long n = L.grid_length;
+    VOXEL **rows = nullptr;
+    if (!L.check_matching_rate) rows = unpack_voxels(ncc, n, voxels);
+    const int acc = reinterpret_cast<vll_signature>(fn)(
+        rows, L.proinfo, reinterpret_cast<NCCresult *>(ncc), L.li,
+        reinterpret_cast<const UGRID *>(gridpt3), (uint8)d->iteration, d->minmax_height);
+    if (rows) pack_and_free_voxels(ncc, n, rows, voxels, cap);
+    return acc;
+}
+
 /* Byte offsets of the fields the drop-in reads, in the order of the
  * library's vll_compat_layout(), taken from the reference's own headers. */
 int ref_layout(int64_t *out, int cap) {

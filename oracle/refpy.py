@@ -181,3 +181,52 @@ def awncc(inputs, ncc: np.ndarray, voxels: np.ndarray) -> None:
     d = inputs.desc()
     vp = voxels.ctypes.data if voxels.size else None
     lib().ref_awncc(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data, vp, voxels.size)
+
+
+def _kat_lib():
+    L = lib()
+    if not getattr(L, "_kat", False):
+        L.ref_correlate.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_correlate.restype = C.c_double
+        L.ref_window_counts.argtypes = [C.c_int, C.c_void_p]
+        L.ref_call_vertical_line_locus.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc),
+                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]
+        L.ref_call_vertical_line_locus.restype = C.c_long
+        L._kat = True
+    return L
+
+
+def correlate(left, right) -> float:
+    """The reference's Correlate (SubFunctions.cpp:974-1018)."""
+    a = np.ascontiguousarray(left, dtype=np.float64)
+    b = np.ascontiguousarray(right, dtype=np.float64)
+    return float(_kat_lib().ref_correlate(a.ctypes.data, b.ctypes.data, int(min(a.size, b.size))))
+
+
+def window_counts(half: int) -> tuple:
+    """Sub-window counts of the reference's SetVecKernelValue window loop."""
+    out = np.zeros(3, dtype=np.int32)
+    _kat_lib().ref_window_counts(int(half), out.ctypes.data)
+    return tuple(int(x) for x in out)
+
+
+def call_vertical_line_locus(fn_addr: int, inputs, ncc: np.ndarray, voxels=None) -> int:
+    """Calls the function at `fn_addr` (VerticalLineLocus's C++ signature,
+    setsm_code.hpp:81) with structures built from the reference's headers."""
+    d = inputs.desc()
+    vp = voxels.ctypes.data if voxels is not None else None
+    cap = voxels.size if voxels is not None else 0
+    return int(_kat_lib().ref_call_vertical_line_locus(fn_addr, C.byref(d),
+                                                      inputs.gridpt3.ctypes.data,
+                                                      ncc.ctypes.data, vp, cap))
+
+
+def layout() -> list:
+    """Byte offsets and sizes of the reference structures the drop-in reads,
+    from the reference's own headers (same order as vll_compat_layout)."""
+    L = lib()
+    L.ref_layout.argtypes = [C.c_void_p, C.c_int]
+    L.ref_layout.restype = C.c_int
+    out = np.zeros(128, dtype=np.int64)
+    n = L.ref_layout(out.ctypes.data, out.size)
+    return out[:n].tolist()

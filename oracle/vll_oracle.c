@@ -1085,3 +1085,33 @@ void vo_pyramid_down(uint32_t w, uint32_t h, const uint16_t *src, uint16_t *out)
         }
     }
 }
+
+/* ---- known-answer hooks ---------------------------------------------------- */
+double vo_correlate(const double *L, const double *R, int N) { return correlate(L, R, N); }
+int16_t vo_quantize_result(double v) { return q_result(v); }
+int16_t vo_quantize_voxel(double v) { return q_voxel(v); }
+
+/* Drives set_vec over the window loop of VerticalLineLocus (setsm_code.cpp:
+ * 6429-6453) on a constant image, so every sample passes the positivity test
+ * and the counts are those of the window geometry alone. */
+void vo_window_counts(int half, int counts[3]) {
+    const uint32_t n = (uint32_t)(4 * half + 8);
+    uint16_t *img = (uint16_t *)malloc(sizeof(uint16_t) * n * n);
+    for (uint32_t i = 0; i < n * n; ++i) img[i] = 100;
+    patch_src s = {img, img, img, img, n, n, n, n};
+    kernel_buf k;
+    kbuf_init(&k, half);
+    int cnt[3] = {0, 0, 0};
+    const double c = 0.5 * n + 0.25;
+    for (int row = -half; row <= half; row++)
+        for (int col = -half; col <= half; col++) {
+            const int r2 = row * row + col * col;
+            if (r2 <= (half + 1) * (half + 1)) {
+                pt2 p = {c + col, c + row};
+                set_vec(&k, &s, row, col, p, p, r2, cnt);
+            }
+        }
+    for (int w = 0; w < 3; ++w) counts[w] = cnt[w];
+    kbuf_free(&k);
+    free(img);
+}

@@ -49,6 +49,17 @@ long vo_vertical_line_locus(const vll_level_desc *d, const vll_ugrid *gridpt3,
 void vo_awncc_peaks(const vll_level_desc *d, const vll_ugrid *gridpt3, vll_nccresult *ncc,
                     const vll_voxel *voxels, long cap);
 
+/* Known-answer hooks on the building blocks of the window evaluation. */
+/* Correlate, SubFunctions.cpp:974-1018 */
+double vo_correlate(const double *L, const double *R, int N);
+/* _result / _voxel quantisers, Template.hpp:964-993 */
+int16_t vo_quantize_result(double v);
+int16_t vo_quantize_voxel(double v);
+/* Sub-window sample counts of the circular window of half-size `half` when
+ * every sample is valid: SetVecKernelValue (SubFunctions.cpp:3249-3315)
+ * driven by VerticalLineLocus's window loop (setsm_code.cpp:6429-6453). */
+void vo_window_counts(int half, int counts[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,7 @@ import ctypes as C
 
 import numpy as np
 
+VLL_ABI_VERSION = 2
 VLL_MAX_IMAGES = 8
 
 VLL_OK = 0

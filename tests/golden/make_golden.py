@@ -1,0 +1,84 @@
+"""Generates the golden vectors in this folder from the reference SETSM code.
+
+The reference ships no tests, fixtures or sample imagery, so its known answers
+are produced here: seeded synthetic cases (tests/cases.py) are run through the
+reference's own InitializeVoxel / VerticalLineLocus / AWNCC, compiled from its
+sources into oracle/_ref/libsetsm_ref.so (``make -C oracle ref``).  Each
+fixture holds a digest of the case's inputs and the reference's outputs, so
+tests/test_oracle_golden.py can pin the oracle (and the CUDA kernels) on a
+machine without the reference sources.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+# small versions of the parity cases: every route the matcher takes
+GOLDEN = {
+    "m7": dict(size=512, nodes=24, res=8.0, n_heights=32),
+    "m11": dict(size=512, nodes=24, res=8.0, n_heights=32, template=15),
+    "m7_edges": dict(size=512, nodes=24, res=8.0, n_heights=32, zero_patch=True,
+                     unmatched_frac=0.1, minmax=(0.0, 260.0)),
+    "v7_gncc": dict(size=512, nodes=20, res=9.0, n_heights=24, cmr=False, sgm=-1,
+                    ortho_frac=0.5),
+    "v11_it2": dict(size=512, nodes=16, res=10.0, n_heights=24, cmr=False, sgm=-1, it=2,
+                    iters=(1, 2), template=15, ortho_frac=0.5),
+    "l2_combined": dict(L=2, it=2, iters=(1, 2), cmr=False, sgm=-1, ortho_frac=0.5, nodes=16,
+                        res=16.0, n_heights=16, hs=2.0, template=15),
+    "l3_m": dict(L=3, it=1, cmr=True, nodes=12, res=24.0, n_heights=16, hs=3.0, template=15),
+}
+
+
+def input_digest(inp) -> str:
+    h = hashlib.sha256()
+    for im in inp.images:
+        for a in (im.image, im.mag, im.ori, np.asarray(im.rpc, dtype=np.float64)):
+            h.update(np.ascontiguousarray(a).tobytes())
+        for a in (im.image_next, im.mag_next, im.ori_next):
+            if a is not None:
+                h.update(np.ascontiguousarray(a).tobytes())
+    for a in (inp.grid_pts, inp.grid_wgs, inp.gridpt3):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def fixture_path(name: str) -> str:
+    return os.path.join(HERE, f"{name}.npz")
+
+
+def main() -> None:
+    from oracle import refpy
+    from tests import cases
+    if not refpy.available():
+        raise SystemExit("reference build missing: make -C oracle ref")
+    refpy.set_threads(os.cpu_count() or 1)
+    for name, kw in GOLDEN.items():
+        inp = cases.make_case(**kw)
+        r = cases.run_cpu(refpy, inp, inp.iters)
+        arrays = {
+            "digest": np.array(input_digest(inp)),
+            "acc": np.array(r["acc"]),
+            "init_ncc": r["init_ncc"].view(np.uint8),
+            "init_gp3": r["init_gp3"].view(np.uint8),
+            "vll_ncc": r["vll_ncc"].view(np.uint8),
+            "ncc": r["ncc"].view(np.uint8),
+        }
+        if r["vox"] is not None:
+            arrays["init_vox"] = r["init_vox"].view(np.uint8)
+            arrays["vll_vox"] = r["vll_vox"].view(np.uint8)
+        np.savez_compressed(fixture_path(name), **arrays)
+        print(f"{name}: acc {r['acc']}, peaks {(r['ncc']['result4'] > 0).sum()}, "
+              f"{os.path.getsize(fixture_path(name))} bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,53 @@
+"""The oracle against golden vectors produced by the reference SETSM code
+(tests/golden/*.npz, written by tests/golden/make_golden.py from the
+reference's own InitializeVoxel / VerticalLineLocus / AWNCC).  Bit-exact on
+every NCCresult, UGRID and voxel field.  This pins the oracle wherever the
+reference sources are absent."""
+import numpy as np
+import pytest
+
+from oracle import oraclepy as op
+from setsm_b200 import abi
+from tests import cases
+from tests.golden import make_golden as mg
+
+
+def load_fixture(name):
+    z = np.load(mg.fixture_path(name))
+    out = {"digest": str(z["digest"]), "acc": int(z["acc"])}
+    for k, dt in (("init_ncc", abi.NCCRESULT_DTYPE), ("vll_ncc", abi.NCCRESULT_DTYPE),
+                  ("ncc", abi.NCCRESULT_DTYPE), ("init_gp3", abi.UGRID_DTYPE),
+                  ("init_vox", abi.VOXEL_DTYPE), ("vll_vox", abi.VOXEL_DTYPE)):
+        out[k] = z[k].view(dt) if k in z.files else None
+    return out
+
+
+def golden_case(name):
+    inp = cases.make_case(**mg.GOLDEN[name])
+    g = load_fixture(name)
+    assert mg.input_digest(inp) == g["digest"], \
+        "regenerated inputs differ from the ones the golden vectors were made from"
+    return inp, g
+
+
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN))
+def test_oracle_matches_reference_golden(name):
+    inp, g = golden_case(name)
+    o = cases.run_cpu(op, inp, inp.iters)
+    assert o["acc"] == g["acc"] > 0
+    for k in ("init_ncc", "init_gp3", "vll_ncc", "ncc", "init_vox", "vll_vox"):
+        if g[k] is None:
+            assert o.get(k) is None
+            continue
+        assert cases.field_mismatch(o[k], g[k]) == {}, k
+    # every fixture carries peaks
+    assert (g["ncc"]["result4"] > 0).sum() > 0
+
+
+def test_golden_set_covers_the_routes():
+    routes = set()
+    for name, kw in mg.GOLDEN.items():
+        routes.add(("voxel" if kw.get("cmr", True) is False else "memory-tight",
+                    kw.get("L", 0) > 0, kw.get("template", 11)))
+    assert ("memory-tight", False, 11) in routes and ("memory-tight", False, 15) in routes
+    assert ("voxel", False, 11) in routes and ("voxel", True, 15) in routes
