@@ -100,6 +100,13 @@ __device__ __forceinline__ float2 tgt_sample(const float4 *__restrict__ qt, int 
     return __fadd2_rn(__ffma2_rn(fy, sub2(bot, top), top), init);
 }
 
+// First window column of rows with |row| = AR (the circle r^2 <= (H+1)^2).
+__host__ __device__ constexpr int row_cmin(int H, int AR) {
+    int c = -H;
+    while (AR * AR + c * c > (H + 1) * (H + 1)) ++c;
+    return c;
+}
+
 // One window row of sub-window pattern |row| = AR at signed offset `row`:
 // columns unrolled, each accumulating into its compile-time ring.
 template <int H, int AR>
@@ -109,11 +116,30 @@ __device__ __forceinline__ void win_row(const WinCtx &x, int row, const float4 *
     const float4 *q0 = qr + (row + H) * x.rbw;
     const float4 *q1 = q0 + x.rbw;
     const float2 b = __ffma2_rn(x.nsc, bc2((float)row), tf);
+    // Reference texel pairs {I(c), M(c), I(c+1), M(c+1)} are read only at even
+    // offsets from the row's first column: a sample at an odd offset takes
+    // its left texel from the previous pair's high half and its right texel
+    // from the next pair's low half, so each pair feeds two samples.
+    constexpr int c0 = row_cmin(H, AR);
+    float4 a0 = q0[c0 + H], b0 = q1[c0 + H];   // pair at the last even offset
+    float4 a1 = a0, b1 = b0;                   // pair at the next even offset
 #pragma unroll
     for (int col = -H; col <= H; ++col) {
         if (AR * AR + col * col > (H + 1) * (H + 1)) continue;
         const int ring = ring_of(H, AR, col);
-        const float2 l = ref_sample(x, q0[col + H], q1[col + H], x.ncl);
+        float2 l;
+        if (((col - c0) & 1) == 0) {
+            if (col != c0) {
+                a0 = a1;
+                b0 = b1;
+            }
+            l = ref_sample(x, a0, b0, x.ncl);
+        } else {
+            a1 = q0[col + 1 + H];
+            b1 = q1[col + 1 + H];
+            l = ref_sample(x, make_float4(a0.z, a0.w, a1.x, a1.y),
+                           make_float4(b0.z, b0.w, b1.x, b1.y), x.ncl);
+        }
         const float2 r = tgt_sample(qt, x.tbw, __ffma2_rn(x.cs, bc2((float)col), b), x.ntc);
         Acc2 &u = acc[ring];
         u.sl = __fadd2_rn(u.sl, l);
