@@ -265,6 +265,57 @@ int vll_vertical_line_locus_noalloc(const vll_level_desc *desc, const vll_ugrid 
                                     vll_nccresult *d_nccresult, void *stream,
                                     int64_t *accessable_grid, char *err_buf, int err_len);
 
+/* ---- batches: many tiles / pyramid levels in one pass ------------------- */
+/* One level of a batch: a descriptor whose every pointer is on the DEVICE (as
+ * for vll_vertical_line_locus_device) and the level's device arrays. */
+typedef struct vll_level_io {
+    const vll_level_desc *desc;
+    const vll_ugrid *d_gridpt3;
+    vll_nccresult *d_nccresult;
+    vll_voxel *d_voxels;              /* voxel route only, else NULL */
+    const int64_t *d_voxel_offsets;   /* int64 [N+1], voxel route only */
+} vll_level_io;
+
+/*
+ * VerticalLineLocus (setsm_code.cpp:6049-6548) on n_levels independent
+ * levels -- tiles of one or several scenes, pyramid levels, window sizes --
+ * in ONE pass of the split pipeline: one prep pass over all their nodes, ONE
+ * persistent window launch draining every level's (node, 32-slot) work items,
+ * one peak scan and one exact FP64 pass.  Each level's outputs are exactly
+ * those of vll_vertical_line_locus_device on that level alone.  Every level
+ * must be one the split kernel implements (stereo, no combined-level INCC);
+ * otherwise VLL_ERR_UNSUPPORTED.  accessable (optional, host, n_levels)
+ * receives each level's Accessable_grid.  Waits for the GPU.
+ */
+int vll_vertical_line_locus_batch(vll_context *ctx, const vll_level_io *levels, int n_levels,
+                                  int64_t *accessable, vll_stats *stats);
+
+/*
+ * The same batch as a CUDA graph.  vll_plan_create sizes every buffer (one
+ * uncaptured pass of the pipeline's front half, which initialises the
+ * outputs' per-node fields) and captures the whole
+ * pipeline; vll_plan_run replays it on the context's stream with no host
+ * synchronisation inside (it waits only when `accessable` or `stats` is
+ * given).  The plan owns its scratch; the level arrays and images must stay
+ * valid and unmoved while it is used.  It holds while each level's height
+ * ranges keep the plan's total of height slots: a replay after ranges change
+ * that total does no matching and returns VLL_ERR_INVALID (create a new plan).
+ */
+typedef struct vll_plan vll_plan;
+int vll_plan_create(vll_context *ctx, const vll_level_io *levels, int n_levels, vll_plan **out);
+int vll_plan_run(vll_plan *plan, int64_t *accessable, vll_stats *stats);
+void vll_plan_destroy(vll_plan *plan);
+
+/* ---- launch tuning (chosen by setsm_b200/autotune.py) -------------------- */
+typedef struct vll_tuning {
+    int32_t blocks_per_sm;   /* window kernel CTAs per SM; 0 = occupancy maximum   */
+    int32_t grab;            /* work items a warp takes per queue access (1..64)  */
+    float box_margin;        /* shared-memory footprint budget over the estimate  */
+    int32_t _pad;
+} vll_tuning;
+int vll_set_tuning(vll_context *ctx, const vll_tuning *t);
+int vll_get_tuning(const vll_context *ctx, vll_tuning *t);
+
 /*
  * Non-SGM peak loop of AWNCC (setsm_code.cpp:7511-7702) over the packed voxel
  * rows, on HOST buffers.  Selects first/second peaks per node exactly as the

@@ -107,6 +107,24 @@ class LevelDesc(C.Structure):
     ]
 
 
+class LevelIO(C.Structure):
+    """vll_level_io: one level of a batch (device pointers)."""
+    _fields_ = [
+        ("desc", C.POINTER(LevelDesc)), ("d_gridpt3", C.c_void_p), ("d_nccresult", C.c_void_p),
+        ("d_voxels", C.c_void_p), ("d_voxel_offsets", C.c_void_p),
+    ]
+
+
+class Tuning(C.Structure):
+    """vll_tuning: launch parameters of the window kernel."""
+    _fields_ = [("blocks_per_sm", C.c_int32), ("grab", C.c_int32), ("box_margin", C.c_float),
+                ("_pad", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"blocks_per_sm": self.blocks_per_sm, "grab": self.grab,
+                "box_margin": round(float(self.box_margin), 4)}
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("accessable_grid", C.c_int64), ("evals", C.c_int64),

@@ -56,6 +56,8 @@ struct vll_context {
     Buf ocd[VLL_MAX_IMAGES], ocdn[VLL_MAX_IMAGES], ocdptr;
     Buf pre_tmp, pre_wt, pre_img, pre_mag, pre_ori;
     vll::SplitBuffers split;
+    vll::SplitTuning tuning;
+    void *set = nullptr;               // SetResources of batch calls (vll_capi.cu)
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEvent_t stage_ev[9] = {};
     int64_t launches_total = 0;
@@ -312,7 +314,8 @@ int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
         launches += 1;
     } else {
         std::string err;
-        cudaError_t e = vll::run_split(ctx->split, P, dP, counters, ctx->stream, &err, &tm);
+        cudaError_t e = vll::run_split(ctx->split, P, dP, counters, ctx->stream, &err, &tm,
+                                       ctx->tuning);
         if (e != cudaSuccess) return cuda_fail(ctx, e, err.c_str());
         launches += tm.launches;
         split_ran = true;
@@ -350,6 +353,161 @@ int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
         }
         if (h[3] != 0) return fail(ctx, VLL_ERR_TIMEOUT, "persistent kernel reported an error flag");
     }
+    return VLL_OK;
+}
+
+// Device resources of a level set: the level blocks, the orthoimage rasters
+// of the levels that use GNCC, counters and the split pipeline's scratch.
+struct SetResources {
+    std::vector<DevLevel> hl;           // host copies of the level blocks
+    Buf dl;                             // device array of the level blocks
+    DevLevel *staging = nullptr;        // pinned staging of the upload
+    size_t staging_cap = 0;
+    std::vector<Buf> ocd;               // [level][image][level, next level]
+    Buf ocdptr;                         // [level][2 * VLL_MAX_IMAGES] raster pointers
+    Buf counters;
+    vll::SplitBuffers split;
+    std::vector<int64_t> ortho_total;   // per level: raster pixels (0 = no GNCC)
+};
+
+void release_set(SetResources &r) {
+    release(r.dl);
+    if (r.staging) cudaFreeHost(r.staging);
+    r.staging = nullptr;
+    r.staging_cap = 0;
+    for (auto &b : r.ocd) release(b);
+    r.ocd.clear();
+    release(r.ocdptr);
+    release(r.counters);
+    vll::split_release(r.split);
+}
+
+SetResources *ctx_set(vll_context *ctx) {
+    if (!ctx->set) ctx->set = new SetResources();
+    return (SetResources *)ctx->set;
+}
+
+// Derives, checks and uploads the level blocks of a batch; allocates the
+// orthoimage rasters (filled by enqueue_set_ortho).
+int prepare_set(vll_context *ctx, SetResources &r, const vll_level_io *levels, int n) {
+    if (!levels || n < 1) return fail(ctx, VLL_ERR_INVALID, "empty level list");
+    r.hl.assign((size_t)n, DevLevel());
+    r.ortho_total.assign((size_t)n, 0);
+    for (int l = 0; l < n; ++l) {
+        const vll_level_io &io = levels[l];
+        if (!io.desc || !io.d_gridpt3 || !io.d_nccresult)
+            return fail(ctx, VLL_ERR_INVALID, "level " + std::to_string(l) + ": null pointer");
+        DevLevel &P = r.hl[l];
+        std::string err;
+        const int rc = vll::derive_level(io.desc, &P, &err);
+        if (rc) return fail(ctx, rc, "level " + std::to_string(l) + ": " + err);
+        if (!vll::split_supported(P))
+            return fail(ctx, VLL_ERR_UNSUPPORTED,
+                        "level " + std::to_string(l) +
+                            ": not a level the batched split pipeline implements (stereo, "
+                            "no combined-level INCC)");
+        if (!P.cmr && !P.is_ra && (!io.d_voxels || !io.d_voxel_offsets))
+            return fail(ctx, VLL_ERR_INVALID,
+                        "level " + std::to_string(l) + ": voxel route needs voxel rows and offsets");
+        P.gp3 = io.d_gridpt3;
+        P.ncc = io.d_nccresult;
+        P.vox = io.d_voxels;
+        P.vox_off = io.d_voxel_offsets;
+    }
+    // orthoimage rasters, one set per GNCC level
+    r.ocd.resize((size_t)n * VLL_MAX_IMAGES * 2);
+    VLL_CUDA(ctx, ensure(r.ocdptr, (size_t)n * 2 * VLL_MAX_IMAGES * sizeof(void *)));
+    std::vector<const void *> ptrs((size_t)n * 2 * VLL_MAX_IMAGES, nullptr);
+    for (int l = 0; l < n; ++l) {
+        DevLevel &P = r.hl[l];
+        if (!P.check_ortho) continue;
+        r.ortho_total[l] = P.ow * P.oh;
+        for (int ti = 0; ti < P.num_images; ++ti) {
+            if (!P.im[ti].selected) continue;
+            Buf &a = r.ocd[((size_t)l * VLL_MAX_IMAGES + ti) * 2];
+            VLL_CUDA(ctx, ensure(a, (size_t)(P.ow * P.oh) * sizeof(double2)));
+            P.ocd[ti] = (const double2 *)a.p;
+            ptrs[(size_t)l * 2 * VLL_MAX_IMAGES + ti] = a.p;
+            if (P.combined) {
+                Buf &b = r.ocd[((size_t)l * VLL_MAX_IMAGES + ti) * 2 + 1];
+                VLL_CUDA(ctx, ensure(b, (size_t)(P.own * P.ohn) * sizeof(double2)));
+                P.ocd_n[ti] = (const double2 *)b.p;
+                ptrs[(size_t)l * 2 * VLL_MAX_IMAGES + VLL_MAX_IMAGES + ti] = b.p;
+            }
+        }
+    }
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // staging may be in flight
+    if (r.staging_cap < (size_t)n) {
+        if (r.staging) cudaFreeHost(r.staging);
+        r.staging = nullptr;
+        r.staging_cap = 0;
+        VLL_CUDA(ctx, cudaMallocHost((void **)&r.staging, (size_t)n * sizeof(DevLevel)));
+        r.staging_cap = (size_t)n;
+    }
+    memcpy(r.staging, r.hl.data(), (size_t)n * sizeof(DevLevel));
+    VLL_CUDA(ctx, ensure(r.dl, (size_t)n * sizeof(DevLevel)));
+    VLL_CUDA(ctx, cudaMemcpyAsync(r.dl.p, r.staging, (size_t)n * sizeof(DevLevel),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(r.ocdptr.p, ptrs.data(), ptrs.size() * sizeof(void *),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // ptrs is pageable and local
+    VLL_CUDA(ctx, ensure(r.counters, 8 * sizeof(unsigned long long)));
+    return VLL_OK;
+}
+
+// SetOrthoImageCoord of every GNCC level of the set (clear + fill).
+cudaError_t enqueue_set_ortho(SetResources &r, cudaStream_t s) {
+    const int n = (int)r.hl.size();
+    for (int l = 0; l < n; ++l) {
+        if (!r.ortho_total[l]) continue;
+        const DevLevel &P = r.hl[l];
+        for (int ti = 0; ti < P.num_images; ++ti) {
+            if (!P.im[ti].selected) continue;
+            Buf &a = r.ocd[((size_t)l * VLL_MAX_IMAGES + ti) * 2];
+            cudaError_t e = cudaMemsetAsync(a.p, 0, a.cap, s);
+            if (e != cudaSuccess) return e;
+            if (P.combined) {
+                Buf &b = r.ocd[((size_t)l * VLL_MAX_IMAGES + ti) * 2 + 1];
+                e = cudaMemsetAsync(b.p, 0, b.cap, s);
+                if (e != cudaSuccess) return e;
+            }
+        }
+        double2 *const *dptr = (double2 *const *)r.ocdptr.p + (size_t)l * 2 * VLL_MAX_IMAGES;
+        cudaError_t e = vll::launch_ortho((const DevLevel *)r.dl.p + l, r.ortho_total[l], dptr,
+                                          dptr + VLL_MAX_IMAGES, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Copies per-level Accessable_grid and the totals after a pass (waits).
+int finish_set(vll_context *ctx, SetResources &r, const vll::SplitBuffers &b, int n,
+               int64_t *accessable, vll_stats *stats, float ms, int64_t launches) {
+    unsigned long long h[8] = {};
+    std::vector<unsigned long long> acc((size_t)n, 0);
+    VLL_CUDA(ctx, cudaMemcpyAsync(h, r.counters.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(acc.data(), b.acc_level, (size_t)n * 8, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    unsigned long long ctl[8] = {};
+    VLL_CUDA(ctx, cudaMemcpyAsync(ctl, b.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctl[5]) return fail(ctx, VLL_ERR_INVALID,
+                            "the levels' height slots changed since the plan was made");
+    if (accessable)
+        for (int l = 0; l < n; ++l) accessable[l] = (int64_t)acc[l];
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->accessable_grid = (int64_t)h[0];
+        stats->evals = (int64_t)h[1];
+        stats->fp64_rechecks = (int64_t)h[2];
+        stats->kernel_ms = ms;
+        stats->window_ms = ms;
+        stats->launches = launches;
+        stats->fp64_nodes = (int64_t)h[5];
+        stats->scan_rounds = (int64_t)h[6];
+        stats->exact_nodes = (int64_t)ctl[2];
+    }
+    if (h[3] != 0) return fail(ctx, VLL_ERR_TIMEOUT, "persistent kernel reported an error flag");
     return VLL_OK;
 }
 
@@ -415,6 +573,10 @@ void vll_destroy(vll_context *ctx) {
     release(ctx->pre_mag);
     release(ctx->pre_ori);
     vll::split_release(ctx->split);
+    if (ctx->set) {
+        release_set(*(SetResources *)ctx->set);
+        delete (SetResources *)ctx->set;
+    }
     if (ctx->hlevel) cudaFreeHost(ctx->hlevel);
     if (ctx->e0) cudaEventDestroy(ctx->e0);
     if (ctx->e1) cudaEventDestroy(ctx->e1);
@@ -765,6 +927,139 @@ int vll_pyramid_down(vll_context *ctx, const uint16_t *image, uint32_t width, ui
     if (rc) return rc;
     VLL_CUDA(ctx, cudaMemcpyAsync(out, ctx->pre_mag.p, no * 2, cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+// ---- batches, plans, tuning ------------------------------------------------
+struct vll_plan {
+    vll_context *ctx = nullptr;
+    SetResources res;
+    vll::SplitPlan plan;
+    int n_levels = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+int vll_vertical_line_locus_batch(vll_context *ctx, const vll_level_io *levels, int n_levels,
+                                  int64_t *accessable, vll_stats *stats) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    SetResources &r = *ctx_set(ctx);
+    int rc = prepare_set(ctx, r, levels, n_levels);
+    if (rc) return rc;
+    VLL_CUDA(ctx, cudaMemsetAsync(r.counters.p, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    if (!ctx->e0) {
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e0));
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e1));
+    }
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e0, ctx->stream));
+    VLL_CUDA(ctx, enqueue_set_ortho(r, ctx->stream));
+    std::string err;
+    vll::SplitTiming tm;
+    cudaError_t e = vll::run_split_set(r.split, r.hl.data(), (const DevLevel *)r.dl.p, n_levels,
+                                       (unsigned long long *)r.counters.p, ctx->stream, &err, &tm,
+                                       ctx->tuning);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, err.c_str());
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
+    VLL_CUDA(ctx, cudaEventSynchronize(ctx->e1));
+    float ms = 0;
+    VLL_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->e0, ctx->e1));
+    ctx->launches_total += tm.launches;
+    rc = finish_set(ctx, r, r.split, n_levels, accessable, stats, ms, tm.launches);
+    if (!rc && stats) stats->slots = tm.slots;
+    return rc;
+}
+
+int vll_plan_create(vll_context *ctx, const vll_level_io *levels, int n_levels, vll_plan **out) {
+    if (!ctx || !out) return fail(ctx, VLL_ERR_INVALID, "null context or output pointer");
+    *out = nullptr;
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    vll_plan *pl = new vll_plan();
+    pl->ctx = ctx;
+    pl->n_levels = n_levels;
+    int rc = prepare_set(ctx, pl->res, levels, n_levels);
+    if (rc) {
+        release_set(pl->res);
+        delete pl;
+        return rc;
+    }
+    std::string err;
+    SetResources *rp = &pl->res;
+    VLL_CUDA(ctx, cudaMemsetAsync(pl->res.counters.p, 0, 8 * sizeof(unsigned long long),
+                                  ctx->stream));
+    // the graph clears the counters itself at the start of every replay
+    auto pre = [rp](cudaStream_t s) -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(rp->counters.p, 0, 8 * sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return e;
+        return enqueue_set_ortho(*rp, s);
+    };
+    cudaError_t e = vll::split_plan(pl->plan, pl->plan.bufs, pl->res.hl.data(),
+                                    (const DevLevel *)pl->res.dl.p, n_levels,
+                                    (unsigned long long *)pl->res.counters.p, ctx->stream, &err,
+                                    ctx->tuning, pre);
+    if (e != cudaSuccess) {
+        rc = cuda_fail(ctx, e, err.c_str());
+        vll_plan_destroy(pl);
+        return rc;
+    }
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = pl;
+    return VLL_OK;
+}
+
+int vll_plan_run(vll_plan *pl, int64_t *accessable, vll_stats *stats) {
+    if (!pl || !pl->ctx) return fail(nullptr, VLL_ERR_INVALID, "null plan");
+    vll_context *ctx = pl->ctx;
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const bool wait = accessable || stats;
+    if (wait && !pl->e0) {
+        VLL_CUDA(ctx, cudaEventCreate(&pl->e0));
+        VLL_CUDA(ctx, cudaEventCreate(&pl->e1));
+    }
+    if (wait) VLL_CUDA(ctx, cudaEventRecord(pl->e0, ctx->stream));
+    VLL_CUDA(ctx, cudaGraphLaunch(pl->plan.exec, ctx->stream));
+    ctx->launches_total += pl->plan.launches;
+    if (!wait) return VLL_OK;
+    VLL_CUDA(ctx, cudaEventRecord(pl->e1, ctx->stream));
+    VLL_CUDA(ctx, cudaEventSynchronize(pl->e1));
+    float ms = 0;
+    VLL_CUDA(ctx, cudaEventElapsedTime(&ms, pl->e0, pl->e1));
+    const int rc = finish_set(ctx, pl->res, pl->plan.bufs, pl->n_levels, accessable, stats, ms,
+                              pl->plan.launches);
+    if (!rc && stats) stats->slots = pl->plan.n_slots;
+    return rc;
+}
+
+void vll_plan_destroy(vll_plan *pl) {
+    if (!pl) return;
+    if (pl->ctx) {
+        cudaSetDevice(pl->ctx->device);
+        cudaStreamSynchronize(pl->ctx->stream);
+    }
+    if (pl->plan.exec) cudaGraphExecDestroy(pl->plan.exec);
+    vll::split_release(pl->plan.bufs);
+    release_set(pl->res);
+    if (pl->e0) cudaEventDestroy(pl->e0);
+    if (pl->e1) cudaEventDestroy(pl->e1);
+    delete pl;
+}
+
+int vll_set_tuning(vll_context *ctx, const vll_tuning *t) {
+    if (!ctx || !t) return fail(ctx, VLL_ERR_INVALID, "null context or tuning");
+    if (t->blocks_per_sm < 0 || t->grab < 0 || t->grab > 64 || t->box_margin < 0.f ||
+        (t->box_margin > 0.f && t->box_margin < 1.0f) || t->box_margin > 4.0f)
+        return fail(ctx, VLL_ERR_INVALID, "tuning out of range");
+    ctx->tuning.blocks_per_sm = t->blocks_per_sm;
+    ctx->tuning.grab = t->grab > 0 ? t->grab : 4;
+    ctx->tuning.box_margin = t->box_margin > 0.f ? t->box_margin : 1.25f;
+    return VLL_OK;
+}
+
+int vll_get_tuning(const vll_context *ctx, vll_tuning *t) {
+    if (!ctx || !t) return VLL_ERR_INVALID;
+    memset(t, 0, sizeof(*t));
+    t->blocks_per_sm = ctx->tuning.blocks_per_sm;
+    t->grab = ctx->tuning.grab;
+    t->box_margin = ctx->tuning.box_margin;
     return VLL_OK;
 }
 

@@ -31,6 +31,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <vector>
 #include <cub/device/device_scan.cuh>
 
 #include "vll_exact.cuh"
@@ -54,18 +55,53 @@ constexpr float kNotEvaluated = INFINITY;    // slot skipped (range / image boun
 constexpr float kRejected = -INFINITY;       // orientation check failed
 
 // ---------------------------------------------------------------------------
+// Level set: the levels matched by one pass of the pipeline (one level for a
+// VerticalLineLocus call; many tiles and pyramid levels for a batch).  Their
+// nodes are numbered consecutively: global node g belongs to the level l with
+// base[l] <= g < base[l + 1] and is that level's node g - base[l].  Per-node
+// and per-slot work arrays are indexed by g.
+// ---------------------------------------------------------------------------
+struct LevelSet {
+    const DevLevel *lv;       // [n] level blocks (device)
+    const int64_t *base;      // [n + 1] first global node of each level (device)
+    int n;
+    int64_t total;            // base[n]
+};
+
+__device__ __forceinline__ int level_of(const LevelSet &S, int64_t g) {
+    int lo = 0, hi = S.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(S.base + mid) <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
 // prep: per-node setup (setsm_code.cpp:6158-6328)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) prep_kernel(const DevLevel *__restrict__ Pp,
+__global__ void __launch_bounds__(256) prep_kernel(const LevelSet S,
                                                    const double *__restrict__ gsum,
                                                    const double *__restrict__ gcnt,
                                                    int32_t *__restrict__ node_k,
                                                    int32_t *__restrict__ item_cnt,
-                                                   unsigned long long *__restrict__ counters) {
-    const DevLevel &P = *Pp;
-    unsigned long long acc = 0;
-    for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.n_nodes;
-         pt += (int64_t)gridDim.x * blockDim.x) {
+                                                   unsigned long long *__restrict__ counters,
+                                                   unsigned long long *__restrict__ acc_level) {
+    unsigned long long acc = 0, acc_l = 0;
+    int cur = -1;
+    for (int64_t gn = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gn < S.total;
+         gn += (int64_t)gridDim.x * blockDim.x) {
+        const int l = level_of(S, gn);
+        if (l != cur) {
+            if (acc_l) atomicAdd(&acc_level[cur], acc_l);
+            acc_l = 0;
+            cur = l;
+        }
+        const DevLevel &P = S.lv[l];
+        const int64_t pt = gn - __ldg(S.base + l);
         int K = 0;
         const vll_ugrid g = P.gp3[pt];
         const int start_H = g.minHeight, end_H = g.maxHeight;
@@ -73,10 +109,11 @@ __global__ void __launch_bounds__(256) prep_kernel(const DevLevel *__restrict__ 
         if (check_image_boundary(P, lon, lat, (double)start_H, (double)end_H, P.H) &&
             !blunder_cell(P, g)) {
             acc++;
+            acc_l++;
             vll_nccresult &R = P.ncc[pt];
             const int ti = 1;
             if (P.check_ortho && dq_result(ugrid_ortho_ncc(P.gp3, P.n_nodes, pt, ti)) > P.ortho_th)
-                R.GNCC = gcnt[pt] > 0 ? q_result(__ddiv_rn(gsum[pt], gcnt[pt])) : q_result(-1.0);
+                R.GNCC = gcnt[gn] > 0 ? q_result(__ddiv_rn(gsum[gn], gcnt[gn])) : q_result(-1.0);
             else
                 R.GNCC = q_result(-1.0);
             const int num_heights = (int)__ddiv_rn((double)(end_H - start_H), P.height_step);
@@ -94,16 +131,29 @@ __global__ void __launch_bounds__(256) prep_kernel(const DevLevel *__restrict__ 
                 if (K == 0 && R.check_height_change) R.max_WNCC = q_result(-100.0);
             }
         }
-        node_k[pt] = K;
-        item_cnt[pt] = (K + 31) / 32;
+        node_k[gn] = K;
+        item_cnt[gn] = (K + 31) / 32;
     }
+    if (acc_l) atomicAdd(&acc_level[cur], acc_l);
     for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&counters[0], acc);
 }
 
+// Stops the rest of a planned (graph-replayed) pipeline when the slot or item
+// totals differ from the ones its buffers were sized for (the height ranges
+// changed since the plan was made): sets ctl[5], which the later kernels test.
+__global__ void guard_kernel(const int64_t *__restrict__ slot_total,
+                             const int64_t *__restrict__ item_total, int64_t slots, int64_t items,
+                             unsigned long long *__restrict__ ctl) {
+    if (threadIdx.x == 0 && blockIdx.x == 0 && (*slot_total != slots || *item_total != items))
+        ctl[5] = 1;
+}
+
 __global__ void __launch_bounds__(256) items_kernel(int64_t n, const int32_t *__restrict__ item_cnt,
                                                     const int64_t *__restrict__ item_off,
-                                                    int64_t *__restrict__ items) {
+                                                    int64_t *__restrict__ items,
+                                                    const unsigned long long *__restrict__ stop) {
+    if (*stop) return;
     for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < n;
          pt += (int64_t)gridDim.x * blockDim.x) {
         const int c = item_cnt[pt];
@@ -209,50 +259,69 @@ __host__ __device__ constexpr size_t win_boxes_offset() {
     return (sizeof(WinShared) * kWinWarps + 15) & ~(size_t)15;
 }
 
-template <int H>
+// FP32 window statistics of one slot for the level's window half-size
+// (the window code is unrolled per half-size; a batch may mix them).
+__device__ __forceinline__ void window_any(int H, const float4 *qr, int rbw, float rfx, float rfy,
+                                           const float4 *qt, int tbw, float tfx, float tfy,
+                                           float c, float s, float &incc, bool &unsure) {
+    switch (H) {
+        case 2: window_fp32<2>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
+        case 3: window_fp32<3>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
+        case 4: window_fp32<4>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
+        case 5: window_fp32<5>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
+        case 6: window_fp32<6>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
+        default: window_fp32<7>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
+    }
+}
+
+// One persistent launch over the (node, 32-slot) items of every level of the
+// set; items are in level order, so warps of a launch mostly run one window
+// size at a time.
 __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
-    const DevLevel *__restrict__ Pp, const int64_t *__restrict__ items, int64_t n_items,
+    const LevelSet LS, const int64_t *__restrict__ items, int64_t n_items,
     const int64_t *__restrict__ slot_off, const double *__restrict__ gsum,
     const double *__restrict__ gcnt, float2 *__restrict__ rho,
     unsigned long long *__restrict__ counters, unsigned long long *__restrict__ queue,
-    int warp_quads) {
+    int warp_quads, int grab, const unsigned long long *__restrict__ stop) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const DevLevel &P = *Pp;
+    if (*stop) return;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     WinShared &W = reinterpret_cast<WinShared *>(smem_raw)[warp];
     float4 *boxes = reinterpret_cast<float4 *>(smem_raw + win_boxes_offset()) + (size_t)warp * warp_quads;
-    const DevImage &ri = P.im[P.ref];
-    const DevImage &tI = P.im[1];
-    PatchSrc S, Sn;
-    make_src(P, 1, S, Sn);
-    const bool voxels = P.vox && !P.cmr && !P.is_ra;
-    // 16-byte aligned image rows allow 128-bit staging loads
-    const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
-                        ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
-                          reinterpret_cast<uintptr_t>(tI.img) | reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
-    const double inv_s = 1.0 / (double)(1 << P.L);
     unsigned long long evals = 0;
-    constexpr int kGrab = 4;
     for (;;) {
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(queue, (unsigned long long)kGrab);
+        if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= (unsigned long long)n_items) break;
-        for (int g = 0; g < kGrab; ++g) {
-            const int64_t it = (int64_t)base + g;
+        for (int gi = 0; gi < grab; ++gi) {
+            const int64_t it = (int64_t)base + gi;
             if (it >= n_items) break;
             const int64_t code = items[it];
-            const int64_t pt = code >> 16;
+            const int64_t gn = code >> 16;
             const int k0 = (int)(code & 0xFFFF);
-            const int64_t so = slot_off[pt];
-            const int K = (int)(slot_off[pt + 1] - so);
+            const int lvl = level_of(LS, gn);
+            const DevLevel &P = LS.lv[lvl];
+            const int64_t pt = gn - __ldg(LS.base + lvl);
+            const int H = P.H;
+            const DevImage &ri = P.im[P.ref];
+            const DevImage &tI = P.im[1];
+            const bool voxels = P.vox && !P.cmr && !P.is_ra;
+            // 16-byte aligned image rows allow 128-bit staging loads
+            const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
+                                ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
+                                  reinterpret_cast<uintptr_t>(tI.img) |
+                                  reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
+            const double inv_s = 1.0 / (double)(1 << P.L);
+            const int64_t so = slot_off[gn];
+            const int K = (int)(slot_off[gn + 1] - so);
             const int k = k0 + lane;
             const vll_ugrid gg = P.gp3[pt];
             const int start_H = gg.minHeight, end_H = gg.maxHeight;
             const int ncc_min = P.ncc[pt].minHeight;
             const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
-            const double cnt_g = gcnt ? gcnt[pt] : 0.0, sum_g = gsum ? gsum[pt] : 0.0;
+            const double cnt_g = gcnt ? gcnt[gn] : 0.0, sum_g = gsum ? gsum[gn] : 0.0;
             // per-node RPC cubics: lanes 0..7 = (image, polynomial)
             if (lane < 8) {
                 const int im = lane >> 2, j = lane & 3;
@@ -359,11 +428,11 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 if (staged && inside) {
                     float incc;
                     bool unsure = false;
-                    window_fp32<H>(boxes + (riy - H - ry0) * rbw + (rix - H - rx0), rbw,
-                                   (float)(rp.x - (double)rix), (float)(rp.y - (double)riy),
-                                   boxes + rbw * rbh + (tiy - ty0) * tbw + (tix - tx0), tbw,
-                                   (float)(tp.x - (double)tix), (float)(tp.y - (double)tiy), cf, sf,
-                                   incc, unsure);
+                    window_any(H, boxes + (riy - H - ry0) * rbw + (rix - H - rx0), rbw,
+                               (float)(rp.x - (double)rix), (float)(rp.y - (double)riy),
+                               boxes + rbw * rbh + (tiy - ty0) * tbw + (tix - tx0), tbw,
+                               (float)(tp.x - (double)tix), (float)(tp.y - (double)tiy), cf, sf,
+                               incc, unsure);
                     const bool has = incc != -2.0f;
                     const double incc_d = has ? (double)incc : -1.0;
                     double rho_d;
@@ -375,6 +444,8 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     incc_v = unsure ? __int_as_float(0x7fc00000) : (float)incc_d;
                     all_pos = true;   // window inside the image, no zero texels
                 } else {
+                    PatchSrc S, Sn;
+                    make_src(P, 1, S, Sn);
                     const SlotOut o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
                     all_pos = o.all_pos;
                     rho_v = (float)o.rho;
@@ -419,18 +490,21 @@ __device__ __forceinline__ int dir_sign(double a, double b) {
 // Runs the whole FindPeakNcc scan / max_WNCC of a node on its FP32 values and
 // writes the results when no decision lies within kBand of a boundary;
 // otherwise queues the node for the exact (warp) path.
-__global__ void __launch_bounds__(256) scan_thread_kernel(const DevLevel *__restrict__ Pp,
+__global__ void __launch_bounds__(256) scan_thread_kernel(const LevelSet LS,
                                                           const int64_t *__restrict__ slot_off,
                                                           const float2 *__restrict__ rho,
                                                           int64_t *__restrict__ pending,
                                                           unsigned long long *__restrict__ ctl) {
-    const DevLevel &P = *Pp;
-    const bool voxels = P.vox && !P.cmr && !P.is_ra;
-    for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.n_nodes;
-         pt += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t so = slot_off[pt];
-        const int K = (int)(slot_off[pt + 1] - so);
+    if (ctl[5]) return;
+    for (int64_t gn = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gn < LS.total;
+         gn += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t so = slot_off[gn];
+        const int K = (int)(slot_off[gn + 1] - so);
         if (K == 0) continue;
+        const int lvl = level_of(LS, gn);
+        const DevLevel &P = LS.lv[lvl];
+        const int64_t pt = gn - __ldg(LS.base + lvl);
+        const bool voxels = P.vox && !P.cmr && !P.is_ra;
         const float2 *rv = rho + so;
         vll_nccresult R = P.ncc[pt];
         const int start_H = P.gp3[pt].minHeight;
@@ -507,7 +581,7 @@ __global__ void __launch_bounds__(256) scan_thread_kernel(const DevLevel *__rest
             }
         }
         if (need) {
-            pending[atomicAdd(&ctl[2], 1ull)] = pt;
+            pending[atomicAdd(&ctl[2], 1ull)] = gn;
             atomicAdd(&ctl[3], 1ull);
         } else {
             if (R.check_height_change) R.max_WNCC = q_result(max_w);
@@ -728,24 +802,36 @@ __host__ __device__ constexpr size_t exact_scratch_bytes(int H) {
     return (size_t)(2 * H + 1) * (2 * H + 1) * 33 + 16;
 }
 
+// Exact FP64 evaluation of one slot by the warp for the level's half-size.
+__device__ __forceinline__ SlotOut eval_slot_warp_any(const DevLevel &P, int64_t pt,
+                                                      const PatchSrc &S, float hgt, double cnt_g,
+                                                      double sum_g, double *scratch, int lane) {
+    switch (P.H) {
+        case 2: return eval_slot_warp<2>(P, pt, S, hgt, cnt_g, sum_g, scratch, lane);
+        case 3: return eval_slot_warp<3>(P, pt, S, hgt, cnt_g, sum_g, scratch, lane);
+        case 4: return eval_slot_warp<4>(P, pt, S, hgt, cnt_g, sum_g, scratch, lane);
+        case 5: return eval_slot_warp<5>(P, pt, S, hgt, cnt_g, sum_g, scratch, lane);
+        case 6: return eval_slot_warp<6>(P, pt, S, hgt, cnt_g, sum_g, scratch, lane);
+        default: return eval_slot_warp<7>(P, pt, S, hgt, cnt_g, sum_g, scratch, lane);
+    }
+}
+
 // The exact path for the nodes the scan kernel could not settle in FP32.
-template <int H>
+// `max_h`: the largest window half-size of the level set (scratch layout).
 __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
-    const DevLevel *__restrict__ Pp, const int64_t *__restrict__ slot_off,
+    const LevelSet LS, int max_h, const int64_t *__restrict__ slot_off,
     const float2 *__restrict__ rho, const double *__restrict__ gsum, const double *__restrict__ gcnt,
     unsigned long long *__restrict__ counters, unsigned long long *__restrict__ queue,
-    const int64_t *__restrict__ pending, const unsigned long long *__restrict__ n_pending) {
+    const int64_t *__restrict__ pending, const unsigned long long *__restrict__ n_pending,
+    const unsigned long long *__restrict__ stop) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const DevLevel &P = *Pp;
+    if (*stop) return;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     WarpShared &W = reinterpret_cast<WarpShared *>(smem_raw)[warp];
     constexpr size_t ws = (sizeof(WarpShared) + 15) & ~(size_t)15;
-    constexpr size_t xs = (exact_scratch_bytes(H) + 15) & ~(size_t)15;
+    const size_t xs = (exact_scratch_bytes(max_h) + 15) & ~(size_t)15;
     double *boxes = reinterpret_cast<double *>(smem_raw + ws * kPeakWarps + xs * warp);
-    PatchSrc S, Sn;
-    make_src(P, 1, S, Sn);
-    const bool voxels = P.vox && !P.cmr && !P.is_ra;
     unsigned long long rechecks = 0;
     const unsigned long long n_pend = *n_pending;
     for (;;) {
@@ -753,13 +839,19 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
         if (lane == 0) idx = atomicAdd(queue, 1ull);
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= n_pend) break;
-        const int64_t pt = pending[idx];
-        const int64_t so = slot_off[pt];
-        const int K = (int)(slot_off[pt + 1] - so);
+        const int64_t gn = pending[idx];
+        const int64_t so = slot_off[gn];
+        const int K = (int)(slot_off[gn + 1] - so);
         if (K == 0) continue;
+        const int lvl = level_of(LS, gn);
+        const DevLevel &P = LS.lv[lvl];
+        const int64_t pt = gn - __ldg(LS.base + lvl);
+        PatchSrc S, Sn;
+        make_src(P, 1, S, Sn);
+        const bool voxels = P.vox && !P.cmr && !P.is_ra;
         vll_nccresult R = P.ncc[pt];
         const int start_H = P.gp3[pt].minHeight;
-        const double cnt_g = gcnt ? gcnt[pt] : 0.0, sum_g = gsum ? gsum[pt] : 0.0;
+        const double cnt_g = gcnt ? gcnt[gn] : 0.0, sum_g = gsum ? gsum[gn] : 0.0;
         vll_voxel *vrow = voxels ? P.vox + P.vox_off[pt] : nullptr;
         if (K > kSlotCap) {
             // more slots than the shared scan buffer holds: all slots exactly
@@ -939,7 +1031,7 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
             for (int j = W.n_exact; j < base; ++j) {
                 const int k = W.exact_k[j];
                 const float hh = slot_height(P, start_H, R.minHeight, k);
-                const SlotOut o = eval_slot_warp<H>(P, pt, S, hh, cnt_g, sum_g,
+                const SlotOut o = eval_slot_warp_any(P, pt, S, hh, cnt_g, sum_g,
                                                     reinterpret_cast<double *>(boxes), lane);
                 if (lane == 0) {
                     W.exact_rho[j] = o.rho;
@@ -1037,7 +1129,7 @@ void host_rpc(const double *rpc, double lon, double lat, double h, double &x, do
 // (rotated up to 45 degrees) swept along their epipolar lines.  The sweep
 // per slot is measured from the RPCs over the image footprint; the budget is
 // the worst case with a 25% margin (a larger footprint falls back to FP64).
-int window_warp_quads(const DevLevel &P) {
+int window_warp_quads(const DevLevel &P, float margin) {
     const int H = P.H;
     double rate[2] = {0, 0};
     for (int ti = 0; ti < 2; ++ti) {
@@ -1056,85 +1148,90 @@ int window_warp_quads(const DevLevel &P) {
     const int side = 2 * H + 3;
     const int rside = 2 * ((int)ceilf(1.4143f * H) + 1) + 3;
     const double need = (side + 1.0) * (side + sweep0 + 2.0) + (rside + 1.0) * (rside + sweep1 + 2.0);
-    int q = (int)(need * 1.25) + 32;
+    int q = (int)(need * (margin > 0 ? margin : 1.25f)) + 32;
     const int cap = (int)((200 * 1024 - win_boxes_offset()) / (kWinWarps * sizeof(float4)));
     return std::min(q, cap);
 }
 
 
-template <int H>
-cudaError_t launch_window(const DevLevel &P, const DevLevel *dP, const int64_t *items,
+// Box budget of a level set: the largest of its levels' budgets.
+int set_warp_quads(const DevLevel *hl, int n, float margin) {
+    int q = 1;
+    for (int l = 0; l < n; ++l)
+        if (hl[l].n_nodes > 0) q = std::max(q, window_warp_quads(hl[l], margin));
+    return q;
+}
+
+int set_max_h(const DevLevel *hl, int n) {
+    int h = 2;
+    for (int l = 0; l < n; ++l)
+        if (hl[l].n_nodes > 0) h = std::max(h, hl[l].H);
+    return h;
+}
+
+cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const int64_t *items,
                           int64_t n_items, const int64_t *slot_off, const double *gsum,
                           const double *gcnt, float2 *rho, unsigned long long *counters,
-                          unsigned long long *queue, cudaStream_t s) {
-    const int wq = window_warp_quads(P);
+                          unsigned long long *ctl, const SplitTuning &tu, cudaStream_t s) {
+    const int wq = set_warp_quads(hl, n, tu.box_margin);
     const size_t smem = win_boxes_offset() + (size_t)kWinWarps * wq * sizeof(float4);
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaError_t e = cudaFuncSetAttribute(window_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel<H>, kWinWarps * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel, kWinWarps * 32, smem);
+    if (tu.blocks_per_sm > 0 && tu.blocks_per_sm < per_sm) per_sm = tu.blocks_per_sm;
     if (per_sm < 1) per_sm = 1;
-    window_kernel<H><<<sms * per_sm, kWinWarps * 32, smem, s>>>(dP, items, n_items, slot_off, gsum,
-                                                                gcnt, rho, counters, queue, wq);
+    const int grab = tu.grab > 0 ? std::min(tu.grab, 64) : 4;
+    window_kernel<<<sms * per_sm, kWinWarps * 32, smem, s>>>(LS, items, n_items, slot_off, gsum,
+                                                             gcnt, rho, counters, ctl + 0, wq,
+                                                             grab, ctl + 5);
     return cudaGetLastError();
 }
 
-template <int H>
-cudaError_t launch_peaks(const DevLevel *dP, const int64_t *slot_off, const float2 *rho,
+cudaError_t launch_peaks(const LevelSet &LS, int max_h, const int64_t *slot_off, const float2 *rho,
                          const double *gsum, const double *gcnt, unsigned long long *counters,
                          unsigned long long *queue, const int64_t *pending,
-                         const unsigned long long *n_pending, cudaStream_t s) {
+                         const unsigned long long *n_pending, const unsigned long long *stop,
+                         cudaStream_t s) {
     const size_t ws = (sizeof(WarpShared) + 15) & ~(size_t)15;
-    const size_t xs = (exact_scratch_bytes(H) + 15) & ~(size_t)15;
+    const size_t xs = (exact_scratch_bytes(max_h) + 15) & ~(size_t)15;
     const size_t smem = (ws + xs) * kPeakWarps;
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaError_t e = cudaFuncSetAttribute(peaks_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(peaks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peaks_kernel<H>, kPeakWarps * 32, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peaks_kernel, kPeakWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
-    peaks_kernel<H><<<sms * per_sm, kPeakWarps * 32, smem, s>>>(dP, slot_off, rho, gsum, gcnt,
-                                                                counters, queue, pending, n_pending);
+    peaks_kernel<<<sms * per_sm, kPeakWarps * 32, smem, s>>>(LS, max_h, slot_off, rho, gsum, gcnt,
+                                                             counters, queue, pending, n_pending,
+                                                             stop);
     return cudaGetLastError();
 }
 
-#define VLL_DISPATCH_H(Hv, call)                   \
-    switch (Hv) {                                  \
-        case 2: { constexpr int HH = 2; call; } break; \
-        case 3: { constexpr int HH = 3; call; } break; \
-        case 4: { constexpr int HH = 4; call; } break; \
-        case 5: { constexpr int HH = 5; call; } break; \
-        case 6: { constexpr int HH = 6; call; } break; \
-        case 7: { constexpr int HH = 7; call; } break; \
-        default: e = cudaErrorInvalidValue;        \
-    }
-
 // the window / peak stages of the pipeline on given buffers
-cudaError_t window_and_peaks(const DevLevel &P, const DevLevel *dP, const int64_t *items,
+cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, const int64_t *items,
                              int64_t n_items, const int64_t *slot_off, const double *gsum,
                              const double *gcnt, float2 *rho, unsigned long long *counters,
-                             unsigned long long *ctl, int64_t *pending, cudaStream_t s,
-                             SplitTiming *tm) {
-    cudaError_t e = cudaSuccess;
-    VLL_DISPATCH_H(P.H, e = launch_window<HH>(P, dP, items, n_items, slot_off, gsum, gcnt, rho,
-                                              counters, ctl + 0, s));
+                             unsigned long long *ctl, int64_t *pending, const SplitTuning &tu,
+                             cudaStream_t s, SplitTiming *tm) {
+    cudaError_t e = launch_window(hl, n, LS, items, n_items, slot_off, gsum, gcnt, rho, counters,
+                                  ctl, tu, s);
     if (e != cudaSuccess) return e;
     if (tm && tm->enabled) cudaEventRecord(tm->ev[5], s);
-    scan_thread_kernel<<<grid_1d(P.n_nodes, 256, 148 * 32), 256, 0, s>>>(dP, slot_off, rho, pending,
-                                                                        ctl);
+    scan_thread_kernel<<<grid_1d(LS.total, 256, 148 * 32), 256, 0, s>>>(LS, slot_off, rho, pending,
+                                                                       ctl);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (tm && tm->enabled) cudaEventRecord(tm->ev[6], s);
-    VLL_DISPATCH_H(P.H, e = launch_peaks<HH>(dP, slot_off, rho, gsum, gcnt, counters, ctl + 1,
-                                             pending, ctl + 2, s));
-    return e;
+    return launch_peaks(LS, set_max_h(hl, n), slot_off, rho, gsum, gcnt, counters, ctl + 1,
+                        pending, ctl + 2, ctl + 5, s);
 }
 
 }  // namespace
@@ -1146,12 +1243,13 @@ bool split_supported(const DevLevel &P) {
 
 void split_release(SplitBuffers &b) {
     void **all[] = {&b.node_k, &b.slot_off, &b.item_cnt, &b.item_off, &b.items, &b.rho, &b.gsum,
-                    &b.gcnt, &b.re_items, &b.re_out, &b.node_re, &b.scan_tmp, &b.ctl, &b.pending};
+                    &b.gcnt, &b.re_items, &b.re_out, &b.node_re, &b.scan_tmp, &b.ctl, &b.pending,
+                    &b.base, &b.acc_level};
     for (void **p : all) {
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
-    b.cap_nodes = b.cap_slots = b.cap_items = b.cap_re = b.cap_scan = 0;
+    b.cap_nodes = b.cap_slots = b.cap_items = b.cap_re = b.cap_scan = b.cap_levels = 0;
 }
 
 #define SPLIT_CUDA(call)                       \
@@ -1163,14 +1261,23 @@ void split_release(SplitBuffers &b) {
         }                                      \
     } while (0)
 
-cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
-                      unsigned long long *counters, cudaStream_t s, std::string *err,
-                      SplitTiming *tm) {
-    const int64_t N = P.n_nodes;
+// Phase 1 of a pass over a level set: node-sized buffers, the level table,
+// GNCC, prep and the two prefix sums (all enqueued on s, no host wait).
+cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl, int n_levels,
+                        unsigned long long *counters, cudaStream_t s, std::string *err,
+                        SplitTiming *tm, LevelSet *LS_out, double **gsum_out, double **gcnt_out,
+                        int64_t *launches) {
     auto mark = [&](int i) {
         if (tm && tm->enabled) cudaEventRecord(tm->ev[i], s);
     };
-    int64_t launches = 0;
+    std::vector<int64_t> &base = b.h_base;
+    base.assign((size_t)n_levels + 1, 0);
+    bool any_ortho = false;
+    for (int l = 0; l < n_levels; ++l) {
+        base[l + 1] = base[l] + hl[l].n_nodes;
+        any_ortho = any_ortho || hl[l].check_ortho;
+    }
+    const int64_t N = base[n_levels];
     if ((size_t)(N + 1) > b.cap_nodes) {
         void **nb[] = {&b.node_k, &b.item_cnt};
         for (void **p : nb) {
@@ -1186,65 +1293,91 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
         }
         b.cap_nodes = (size_t)(N + 1);
     }
-    if (!b.ctl) SPLIT_CUDA(cudaMalloc(&b.ctl, 8 * sizeof(unsigned long long)));
-    SPLIT_CUDA(cudaMemsetAsync(b.ctl, 0, 8 * sizeof(unsigned long long), s));
-    SPLIT_CUDA(cudaMemsetAsync(b.node_k, 0, (size_t)(N + 1) * sizeof(int32_t), s));
-    SPLIT_CUDA(cudaMemsetAsync(b.item_cnt, 0, (size_t)(N + 1) * sizeof(int32_t), s));
-    double *gsum = nullptr, *gcnt = nullptr;
-    mark(0);
-    if (P.check_ortho) {
-        gsum = (double *)b.gsum;
-        gcnt = (double *)b.gcnt;
-        SPLIT_CUDA(launch_gncc(dP, N, gsum, gcnt, s));
-        ++launches;
+    if ((size_t)n_levels + 1 > b.cap_levels) {
+        if (b.base) cudaFree(b.base);
+        if (b.acc_level) cudaFree(b.acc_level);
+        b.base = b.acc_level = nullptr;
+        SPLIT_CUDA(cudaMalloc(&b.base, ((size_t)n_levels + 1) * 8));
+        SPLIT_CUDA(cudaMalloc(&b.acc_level, ((size_t)n_levels + 1) * 8));
+        b.cap_levels = (size_t)n_levels + 1;
     }
-    mark(1);
-    prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(dP, gsum, gcnt, (int32_t *)b.node_k,
-                                                          (int32_t *)b.item_cnt, counters);
-    SPLIT_CUDA(cudaGetLastError());
-    ++launches;
-    mark(2);
+    if (!b.ctl) SPLIT_CUDA(cudaMalloc(&b.ctl, 8 * sizeof(unsigned long long)));
     size_t tmp1 = 0, tmp2 = 0;
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp1, (const int32_t *)b.node_k,
                                              (int64_t *)b.slot_off, (int)(N + 1), s));
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, (const int32_t *)b.item_cnt,
                                              (int64_t *)b.item_off, (int)(N + 1), s));
     SPLIT_CUDA(grow(b.scan_tmp, b.cap_scan, std::max(tmp1, tmp2)));
+    // the level table is uploaded outside any capture (plan time) by the caller
+    // of split_front when capturing; here it is copied on the stream
+    if (!b.capturing)
+        SPLIT_CUDA(cudaMemcpyAsync(b.base, base.data(), base.size() * 8, cudaMemcpyHostToDevice, s));
+    SPLIT_CUDA(cudaMemsetAsync(b.acc_level, 0, ((size_t)n_levels + 1) * 8, s));
+    *LS_out = LevelSet{dl, (const int64_t *)b.base, n_levels, N};
+    SPLIT_CUDA(cudaMemsetAsync(b.ctl, 0, 8 * sizeof(unsigned long long), s));
+    SPLIT_CUDA(cudaMemsetAsync(b.node_k, 0, (size_t)(N + 1) * sizeof(int32_t), s));
+    SPLIT_CUDA(cudaMemsetAsync(b.item_cnt, 0, (size_t)(N + 1) * sizeof(int32_t), s));
+    double *gsum = nullptr, *gcnt = nullptr;
+    mark(0);
+    if (any_ortho) {
+        gsum = (double *)b.gsum;
+        gcnt = (double *)b.gcnt;
+        for (int l = 0; l < n_levels; ++l) {
+            if (!hl[l].check_ortho || hl[l].n_nodes == 0) continue;
+            SPLIT_CUDA(launch_gncc(dl + l, hl[l].n_nodes, gsum + base[l], gcnt + base[l], s));
+            ++*launches;
+        }
+    }
+    mark(1);
+    prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(*LS_out, gsum, gcnt, (int32_t *)b.node_k,
+                                                          (int32_t *)b.item_cnt, counters,
+                                                          (unsigned long long *)b.acc_level);
+    SPLIT_CUDA(cudaGetLastError());
+    ++*launches;
+    mark(2);
     tmp1 = b.cap_scan;
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp1, (const int32_t *)b.node_k,
                                              (int64_t *)b.slot_off, (int)(N + 1), s));
     tmp2 = b.cap_scan;
     SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp2, (const int32_t *)b.item_cnt,
                                              (int64_t *)b.item_off, (int)(N + 1), s));
-    launches += 4;   // two scans of two kernels each
+    *launches += 4;   // two scans of two kernels each
     mark(3);
-    int64_t totals[2];
-    SPLIT_CUDA(cudaMemcpyAsync(&totals[0], (int64_t *)b.slot_off + N, 8, cudaMemcpyDeviceToHost, s));
-    SPLIT_CUDA(cudaMemcpyAsync(&totals[1], (int64_t *)b.item_off + N, 8, cudaMemcpyDeviceToHost, s));
-    SPLIT_CUDA(cudaStreamSynchronize(s));
-    const int64_t n_slots = totals[0], n_items = totals[1];
-    size_t c = b.cap_slots;
-    SPLIT_CUDA(grow(b.rho, c, (size_t)n_slots * sizeof(float2)));
-    b.cap_slots = c;
-    c = b.cap_items;
-    SPLIT_CUDA(grow(b.items, c, (size_t)n_items * sizeof(int64_t)));
-    b.cap_items = c;
+    *gsum_out = gsum;
+    *gcnt_out = gcnt;
+    return cudaSuccess;
+}
+
+// Phase 2: the work list, the persistent window launch, the scan and the
+// exact pass, on buffers sized for n_slots / n_items.
+cudaError_t split_back(SplitBuffers &b, const DevLevel *hl, int n_levels, const LevelSet &LS,
+                       const double *gsum, const double *gcnt, int64_t n_slots, int64_t n_items,
+                       unsigned long long *counters, const SplitTuning &tu, cudaStream_t s,
+                       std::string *err, SplitTiming *tm, int64_t *launches) {
+    auto mark = [&](int i) {
+        if (tm && tm->enabled) cudaEventRecord(tm->ev[i], s);
+    };
+    const int64_t N = LS.total;
+    unsigned long long *ctl = (unsigned long long *)b.ctl;
+    guard_kernel<<<1, 32, 0, s>>>((const int64_t *)b.slot_off + N, (const int64_t *)b.item_off + N,
+                                  n_slots, n_items, ctl);
+    SPLIT_CUDA(cudaGetLastError());
+    ++*launches;
     if (n_items > 0) {
         items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, (const int32_t *)b.item_cnt,
                                                                (const int64_t *)b.item_off,
-                                                               (int64_t *)b.items);
+                                                               (int64_t *)b.items, ctl + 5);
         SPLIT_CUDA(cudaGetLastError());
-        ++launches;
+        ++*launches;
         mark(4);
-        cudaError_t e = window_and_peaks(P, dP, (const int64_t *)b.items, n_items,
+        cudaError_t e = window_and_peaks(hl, n_levels, LS, (const int64_t *)b.items, n_items,
                                          (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho,
-                                         counters, (unsigned long long *)b.ctl,
-                                         (int64_t *)b.pending, s, tm);
+                                         counters, ctl, (int64_t *)b.pending, tu, s, tm);
         if (e != cudaSuccess) {
             *err = "window / peak kernel launch";
             return e;
         }
-        launches += 3;
+        *launches += 3;
         mark(7);
     } else {
         mark(4);
@@ -1253,11 +1386,111 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
         mark(7);
     }
     mark(8);
+    return cudaSuccess;
+}
+
+// Sizes the slot and item buffers from the totals of a completed front phase.
+cudaError_t split_size(SplitBuffers &b, int64_t N, cudaStream_t s, std::string *err,
+                       int64_t *n_slots, int64_t *n_items) {
+    int64_t totals[2];
+    SPLIT_CUDA(cudaMemcpyAsync(&totals[0], (int64_t *)b.slot_off + N, 8, cudaMemcpyDeviceToHost, s));
+    SPLIT_CUDA(cudaMemcpyAsync(&totals[1], (int64_t *)b.item_off + N, 8, cudaMemcpyDeviceToHost, s));
+    SPLIT_CUDA(cudaStreamSynchronize(s));
+    *n_slots = totals[0];
+    *n_items = totals[1];
+    size_t c = b.cap_slots;
+    SPLIT_CUDA(grow(b.rho, c, (size_t)*n_slots * sizeof(float2)));
+    b.cap_slots = c;
+    c = b.cap_items;
+    SPLIT_CUDA(grow(b.items, c, (size_t)*n_items * sizeof(int64_t)));
+    b.cap_items = c;
+    return cudaSuccess;
+}
+
+cudaError_t run_split_set(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl, int n_levels,
+                          unsigned long long *counters, cudaStream_t s, std::string *err,
+                          SplitTiming *tm, const SplitTuning &tu) {
+    int64_t launches = 0;
+    LevelSet LS;
+    double *gsum = nullptr, *gcnt = nullptr;
+    b.capturing = false;
+    cudaError_t e = split_front(b, hl, dl, n_levels, counters, s, err, tm, &LS, &gsum, &gcnt,
+                                &launches);
+    if (e != cudaSuccess) return e;
+    int64_t n_slots = 0, n_items = 0;
+    e = split_size(b, LS.total, s, err, &n_slots, &n_items);
+    if (e != cudaSuccess) return e;
+    e = split_back(b, hl, n_levels, LS, gsum, gcnt, n_slots, n_items, counters, tu, s, err, tm,
+                   &launches);
+    if (e != cudaSuccess) return e;
     if (tm) {
         tm->slots = n_slots;
         tm->launches = launches;
     }
     return cudaSuccess;
+}
+
+// Planned pass: sizes every buffer with one uncaptured front phase, then
+// captures front + back into a CUDA graph that later replays with no host
+// wait.  The plan holds while the levels' height ranges keep their slot and
+// item totals; a replay with other totals sets ctl[5] and does nothing.
+cudaError_t split_plan(SplitPlan &pl, SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
+                       int n_levels, unsigned long long *counters, cudaStream_t s,
+                       std::string *err, const SplitTuning &tu,
+                       const std::function<cudaError_t(cudaStream_t)> &pre) {
+    int64_t launches = 0;
+    LevelSet LS;
+    double *gsum = nullptr, *gcnt = nullptr;
+    b.capturing = false;
+    cudaError_t e = pre ? pre(s) : cudaSuccess;
+    if (e != cudaSuccess) {
+        *err = "orthoimage rasters";
+        return e;
+    }
+    e = split_front(b, hl, dl, n_levels, counters, s, err, nullptr, &LS, &gsum, &gcnt,
+                                &launches);
+    if (e != cudaSuccess) return e;
+    e = split_size(b, LS.total, s, err, &pl.n_slots, &pl.n_items);
+    if (e != cudaSuccess) return e;
+    if (pl.exec) {
+        cudaGraphExecDestroy(pl.exec);
+        pl.exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    b.capturing = true;
+    SPLIT_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    launches = 0;
+    e = pre ? pre(s) : cudaSuccess;
+    if (e == cudaSuccess)
+        e = split_front(b, hl, dl, n_levels, counters, s, err, nullptr, &LS, &gsum, &gcnt,
+                        &launches);
+    if (e == cudaSuccess)
+        e = split_back(b, hl, n_levels, LS, gsum, gcnt, pl.n_slots, pl.n_items, counters, tu, s,
+                       err, nullptr, &launches);
+    cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+    b.capturing = false;
+    if (e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return e;
+    }
+    if (e2 != cudaSuccess) {
+        *err = "cudaStreamEndCapture";
+        return e2;
+    }
+    e = cudaGraphInstantiate(&pl.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        *err = "cudaGraphInstantiate";
+        return e;
+    }
+    pl.launches = launches;
+    return cudaSuccess;
+}
+
+cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
+                      unsigned long long *counters, cudaStream_t s, std::string *err,
+                      SplitTiming *tm, const SplitTuning &tu) {
+    return run_split_set(b, &P, dP, 1, counters, s, err, tm, tu);
 }
 
 }  // namespace vll
@@ -1380,13 +1613,15 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     int64_t *slot_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
     int64_t *item_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
     int64_t *pending = (int64_t *)cv.take((size_t)(N + 1) * 8);
+    int64_t *lbase = (int64_t *)cv.take(2 * 8);
+    unsigned long long *acc_level = (unsigned long long *)cv.take(2 * 8);
     size_t scan_bytes = 0;
     if (cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int32_t *)node_k, slot_off,
                                       (int)(N + 1), s) != cudaSuccess)
         return fail(VLL_ERR_CUDA, "scan size query failed");
     void *scan_tmp = cv.take(scan_bytes);
     if (!dP || !ctl || !counters || !node_k || !item_cnt || !slot_off || !item_off || !pending ||
-        !scan_tmp) {
+        !lbase || !acc_level || !scan_tmp) {
         char m[160];
         snprintf(m, sizeof m, "grid of %lld nodes exceeds the %zu MiB scratch array",
                  (long long)N, kNoAllocScratchBytes >> 20);
@@ -1400,6 +1635,12 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     // the array keeps the previous call's contents: clear what must start at zero
     NA_CUDA(cudaMemsetAsync(ctl, 0, 8 * sizeof(unsigned long long), s));
     NA_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), s));
+    NA_CUDA(cudaMemsetAsync(acc_level, 0, 2 * 8, s));
+    static thread_local int64_t lbase_host[2];
+    lbase_host[0] = 0;
+    lbase_host[1] = N;
+    NA_CUDA(cudaMemcpyAsync(lbase, lbase_host, sizeof(lbase_host), cudaMemcpyHostToDevice, s));
+    const LevelSet LS{dP, lbase, 1, N};
     NA_CUDA(cudaMemsetAsync(node_k, 0, (size_t)(N + 1) * 4, s));
     NA_CUDA(cudaMemsetAsync(item_cnt, 0, (size_t)(N + 1) * 4, s));
     // capacity: count slots and items first, without writing any output
@@ -1428,8 +1669,8 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     // the pipeline proper (same kernels and order as run_split)
     NA_CUDA(cudaMemsetAsync(node_k, 0, (size_t)(N + 1) * 4, s));
     NA_CUDA(cudaMemsetAsync(item_cnt, 0, (size_t)(N + 1) * 4, s));
-    prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(dP, nullptr, nullptr, node_k, item_cnt,
-                                                          counters);
+    prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(LS, nullptr, nullptr, node_k, item_cnt,
+                                                          counters, acc_level);
     NA_CUDA(cudaGetLastError());
     t1 = scan_bytes;
     NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)node_k, slot_off,
@@ -1438,10 +1679,11 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
                                           (int)(N + 1), s));
     if (n_items > 0) {
-        items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, item_cnt, item_off, items);
+        items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, item_cnt, item_off, items,
+                                                               ctl + 5);
         NA_CUDA(cudaGetLastError());
-        NA_CUDA(window_and_peaks(P, dP, items, n_items, slot_off, nullptr, nullptr, rho, counters,
-                                 ctl, pending, s, nullptr));
+        NA_CUDA(window_and_peaks(&P, 1, LS, items, n_items, slot_off, nullptr, nullptr, rho,
+                                 counters, ctl, pending, SplitTuning(), s, nullptr));
     }
     unsigned long long acc = 0;
     NA_CUDA(cudaMemcpyAsync(&acc, counters, sizeof(acc), cudaMemcpyDeviceToHost, s));

@@ -3,7 +3,9 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <string>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace vll {
@@ -26,7 +28,25 @@ struct SplitBuffers {
     void *scan_tmp = nullptr;      // cub temporary storage
     void *ctl = nullptr;           // uint64 [8] queue head, counts, flags
     void *pending = nullptr;       // int64  [N]  nodes awaiting the exact re-scan
-    size_t cap_nodes = 0, cap_slots = 0, cap_items = 0, cap_re = 0, cap_scan = 0;
+    void *base = nullptr;          // int64  [levels+1] first global node of each level
+    void *acc_level = nullptr;     // uint64 [levels+1] Accessable_grid of each level
+    size_t cap_nodes = 0, cap_slots = 0, cap_items = 0, cap_re = 0, cap_scan = 0, cap_levels = 0;
+    std::vector<int64_t> h_base;   // host copy of the level table
+    bool capturing = false;        // enqueueing into a stream capture
+};
+
+// Launch parameters of the window kernel that the autotuner chooses.
+struct SplitTuning {
+    int blocks_per_sm = 0;      // CTAs per SM (0: the occupancy maximum)
+    int grab = 4;               // work items taken per queue access
+    float box_margin = 1.25f;   // footprint budget over the swept-box estimate
+};
+
+// A level set's pipeline captured as a CUDA graph, with its own buffers.
+struct SplitPlan {
+    SplitBuffers bufs;
+    cudaGraphExec_t exec = nullptr;
+    int64_t n_slots = 0, n_items = 0, launches = 0;
 };
 
 void split_release(SplitBuffers &b);
@@ -49,6 +69,25 @@ struct SplitTiming {
 
 cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
                       unsigned long long *counters, cudaStream_t s, std::string *err,
-                      SplitTiming *timing);
+                      SplitTiming *timing, const SplitTuning &tuning);
+
+// The same pipeline over a set of levels (tiles and / or pyramid levels)
+// whose blocks are hl (host copies) and dl (device array): one prep pass, one
+// persistent window launch draining all levels' (node, 32-slot) items, one
+// scan and one exact pass.  Per-level Accessable_grid counts are left in
+// b.acc_level[0..n_levels).
+cudaError_t run_split_set(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl, int n_levels,
+                          unsigned long long *counters, cudaStream_t s, std::string *err,
+                          SplitTiming *timing, const SplitTuning &tuning);
+
+// Sizes the plan's buffers with one pass of the front phase, then captures
+// the whole pipeline of the level set into pl.exec (replayed with
+// cudaGraphLaunch).  counters and dl must stay valid while the plan is used.
+// `pre` (optional) enqueues work that belongs in front of the pipeline (the
+// orthoimage rasters) both in the sizing pass and in the captured graph.
+cudaError_t split_plan(SplitPlan &pl, SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
+                       int n_levels, unsigned long long *counters, cudaStream_t s,
+                       std::string *err, const SplitTuning &tuning,
+                       const std::function<cudaError_t(cudaStream_t)> &pre);
 
 }  // namespace vll

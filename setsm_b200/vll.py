@@ -29,6 +29,8 @@ EXPORTED = [
     "vll_vertical_line_locus_device", "vll_awncc_peaks", "vll_preprocess_level",
     "vll_preprocess_level_device", "vll_pyramid_down", "vll_pyramid_down_device",
     "vll_compat_layout", "vll_launch_count", "vll_debug_slot_rho",
+    "vll_vertical_line_locus_batch", "vll_plan_create", "vll_plan_run", "vll_plan_destroy",
+    "vll_set_tuning", "vll_get_tuning",
 ]
 
 _lib = None
@@ -77,6 +79,14 @@ def load():
     L.vll_launch_count.restype = i64
     L.vll_compat_layout.argtypes = [vp, i32]
     L.vll_compat_layout.restype = i32
+    L.vll_vertical_line_locus_batch.argtypes = [vp, C.POINTER(abi.LevelIO), i32, vp,
+                                                C.POINTER(abi.Stats)]
+    L.vll_plan_create.argtypes = [vp, C.POINTER(abi.LevelIO), i32, C.POINTER(vp)]
+    L.vll_plan_run.argtypes = [vp, vp, C.POINTER(abi.Stats)]
+    L.vll_plan_destroy.argtypes = [vp]
+    L.vll_plan_destroy.restype = None
+    L.vll_set_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
+    L.vll_get_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
     _lib = L
     return L
 
@@ -201,6 +211,82 @@ class Context:
 
     def pyramid_down_device(self, d_image: int, w: int, h: int, d_out: int) -> None:
         self._check(load().vll_pyramid_down_device(self._h, d_image, w, h, d_out))
+
+    # ---- batches of levels -------------------------------------------------
+    @staticmethod
+    def _level_ios(levels) -> tuple:
+        """levels: sequence of (desc, d_gridpt3, d_nccresult[, d_voxels, d_voxel_offsets])."""
+        n = len(levels)
+        arr = (abi.LevelIO * n)()
+        keep = []
+        for i, lv in enumerate(levels):
+            desc = lv[0]
+            keep.append(desc)
+            arr[i].desc = C.pointer(desc)
+            arr[i].d_gridpt3 = lv[1]
+            arr[i].d_nccresult = lv[2]
+            arr[i].d_voxels = lv[3] if len(lv) > 3 else None
+            arr[i].d_voxel_offsets = lv[4] if len(lv) > 4 else None
+        return arr, keep
+
+    def batch(self, levels) -> tuple:
+        """VerticalLineLocus on every level of `levels` in one pass of the
+        split pipeline (one persistent window launch).  Returns (per-level
+        Accessable_grid array, Stats)."""
+        arr, keep = self._level_ios(levels)
+        acc = np.zeros(len(levels), dtype=np.int64)
+        st = abi.Stats()
+        self._check(load().vll_vertical_line_locus_batch(self._h, arr, len(levels),
+                                                         acc.ctypes.data, C.byref(st)))
+        del keep
+        return acc, st
+
+    def plan(self, levels) -> "Plan":
+        """CUDA-graph plan of a batch (see vll_plan_create)."""
+        return Plan(self, levels)
+
+    def set_tuning(self, blocks_per_sm: int = 0, grab: int = 4, box_margin: float = 1.25) -> None:
+        t = abi.Tuning(int(blocks_per_sm), int(grab), float(box_margin), 0)
+        self._check(load().vll_set_tuning(self._h, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = abi.Tuning()
+        self._check(load().vll_get_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+
+class Plan:
+    """A batch captured as a CUDA graph; run() replays it on the context's stream."""
+
+    def __init__(self, ctx: Context, levels):
+        self.ctx = ctx
+        self.n = len(levels)
+        arr, self._keep = ctx._level_ios(levels)
+        self._arr = arr
+        h = C.c_void_p()
+        ctx._check(load().vll_plan_create(ctx._h, arr, self.n, C.byref(h)))
+        self._h = h
+
+    def run(self, wait: bool = True):
+        """Replays the graph; with `wait`, returns (per-level Accessable_grid, Stats)."""
+        if not wait:
+            self.ctx._check(load().vll_plan_run(self._h, None, None))
+            return None
+        acc = np.zeros(self.n, dtype=np.int64)
+        st = abi.Stats()
+        self.ctx._check(load().vll_plan_run(self._h, acc.ctypes.data, C.byref(st)))
+        return acc, st
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().vll_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 _default: Context | None = None

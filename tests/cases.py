@@ -124,3 +124,42 @@ def run_cpu(impl, inp, iterations=None):
     out["gp3"] = inp.gridpt3
     out["inputs"] = inp
     return out
+
+
+def device_level(torch, inp, ncc: np.ndarray, voxels: np.ndarray | None = None):
+    """Device copies of a case's inputs (planes, grid arrays, UGRID, NCCresult,
+    packed voxel rows and their offsets) and a descriptor whose every pointer
+    is a device pointer.  Returns (desc, io tuple, tensors to keep alive)."""
+    keep = []
+
+    def dev(a):
+        a = np.ascontiguousarray(a)
+        src = a.view(np.int16) if a.dtype == np.uint16 else a
+        if a.dtype.names is not None:
+            src = a.view(np.uint8)
+        t = torch.from_numpy(src.copy()).cuda()
+        keep.append(t)
+        return t
+
+    d = inp.desc()
+    for ti, im in enumerate(inp.images):
+        for name, arr in (("image", im.image), ("mag", im.mag), ("ori", im.ori)):
+            setattr(d.images[ti], name, dev(arr).data_ptr())
+        if im.image_next is not None:
+            for name, arr in (("image_next", im.image_next), ("mag_next", im.mag_next),
+                              ("ori_next", im.ori_next)):
+                setattr(d.images[ti], name, dev(arr).data_ptr())
+    d.grid_wgs = dev(inp.grid_wgs).data_ptr()
+    d.grid_pts = dev(inp.grid_pts).data_ptr()
+    gp3 = dev(inp.gridpt3)
+    d_ncc = dev(ncc)
+    io = [d, gp3.data_ptr(), d_ncc.data_ptr()]
+    if voxels is not None:
+        off = np.concatenate([[0], np.cumsum(ncc["NumOfHeight"].astype(np.int64))]).astype(np.int64)
+        io += [dev(voxels).data_ptr(), dev(off).data_ptr()]
+    return tuple(io), {"keep": keep, "gp3": gp3, "ncc": d_ncc,
+                       "vox": keep[-2] if voxels is not None else None}
+
+
+def from_device(t, dtype) -> np.ndarray:
+    return t.cpu().numpy().view(dtype)
