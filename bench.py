@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -144,6 +145,26 @@ def sum_over_ranks(world, x: float) -> float:
 # ---------------------------------------------------------------------------
 # CPU reference leg
 # ---------------------------------------------------------------------------
+_EVAL_COUNTS = {}
+
+
+def band_evals(inp, ctx, key) -> int:
+    """Evaluations (ComputeMultiNCC calls) of a band.  With a GPU context the
+    matcher counts them on the identical inputs; without one (the reference
+    arm, which runs none of this repository's GPU code on its path) the C
+    restatement of the path counts them, once per band, outside any timing."""
+    if key not in _EVAL_COUNTS:
+        if ctx is not None:
+            _EVAL_COUNTS[key] = int(ctx.vertical_line_locus(inp, inp.new_nccresult(), None,
+                                                            "split").evals)
+        else:
+            from oracle import oraclepy
+            oraclepy.set_threads(os.cpu_count() or 1)
+            _EVAL_COUNTS[key] = int(oraclepy.vertical_line_locus(inp, inp.new_nccresult(),
+                                                                 want_evals=True)[1])
+    return _EVAL_COUNTS[key]
+
+
 def cpu_reference(wl, ctx, budget_s: float, templates) -> dict:
     """Reference SETSM (oracle/_ref, OpenMP on every host core) on a band of
     grid rows sized for about `budget_s` seconds of CPU work per window."""
@@ -160,17 +181,15 @@ def cpu_reference(wl, ctx, budget_s: float, templates) -> dict:
         rows = workloads.rows_for_budget(wl, rate_guess * budget_s)
         r0 = max(0, wl.grid.height // 2 - rows // 2)
         inp = wl.host_inputs(tmpl, rows=(r0, r0 + rows))
-        # evaluation count of the band, from the GPU on the identical inputs
-        ncc_g = inp.new_nccresult()
-        st = ctx.vertical_line_locus(inp, ncc_g, None, "split")
+        evals = band_evals(inp, ctx, (tmpl, r0, rows))
         ncc = inp.new_nccresult()
         t = time.perf_counter()
         refpy.vertical_line_locus(inp, ncc)
         dt = time.perf_counter() - t
-        total_evals += st.evals
+        total_evals += evals
         total_s += dt
         parts.append(f"{rows} rows x {wl.grid.width} nodes, {workloads.WINDOW_OF_TEMPLATE[tmpl]}: "
-                     f"{st.evals} evals in {dt:.2f} s")
+                     f"{evals} evals in {dt:.2f} s")
     return {"value": total_evals / total_s, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": "; ".join(parts)}
 
@@ -186,13 +205,18 @@ def run_reference_arm(args):
     wl = workloads.build(args.config, ctx, device="cuda:0", seed=1)
     log(f"workload built in {time.time() - t0:.1f} s")
     templates = workloads.CONFIGS[args.config]["templates"]
+    budget = args.cpu_seconds / max(1, args.steps)
+    # inputs are generated on the GPU (synthetic scene, magnitude / orientation
+    # planes bit-identical with the reference's preprocessing); the timed path
+    # is the reference's own VerticalLineLocus on the host cores alone
+    del ctx
     for _ in range(args.warmup):
-        cpu_reference(wl, ctx, 2.0, templates)
+        cpu_reference(wl, None, budget, templates)
     vals = []
     cb = None
     t = time.perf_counter()
     for _ in range(args.steps):
-        cb = cpu_reference(wl, ctx, args.cpu_seconds / max(1, args.steps), templates)
+        cb = cpu_reference(wl, None, budget, templates)
         vals.append(cb["value"] or 0.0)
     elapsed = time.perf_counter() - t
     value = statistics.mean(vals) if vals else None
@@ -390,22 +414,232 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# batched multi-level configurations (C3 ragged tiles, C4 pyramid)
+# ---------------------------------------------------------------------------
+def run_multi(args):
+    """C3 / C4: every level of the workload matched in ONE pass of the split
+    pipeline, replayed as a CUDA graph (vll_plan_run) after the autotuner has
+    chosen the window kernel's launch shape.  Reported beside it: the same
+    levels as separate per-level split calls, and the plain FP64 kernel per
+    level on a sample of levels (with identical-peak and tie rates)."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    from setsm_b200 import abi, autotune, vll, workloads
+    dev = torch.device("cuda", local)
+    ctx = vll.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.time()
+    build = workloads.build_c3 if args.config == "c3" else workloads.build_c4
+    mw = build(ctx, device=f"cuda:{local}", seed=1 + rank)
+    log(f"[rank {rank}] workload {args.config}: {len(mw.levels)} levels, {mw.n_nodes} nodes, "
+        f"built in {time.time() - t0:.1f} s")
+    ios = mw.ios()
+    # tune on a spread of levels holding about 1e9 height slots
+    slots = [lv.slots(lv.host_desc_kwargs["step"]) for lv in mw.levels]
+    stride = max(1, int(math.ceil(sum(slots) / 1e9)))
+    tuned = autotune.tune(ctx, ios[::stride], repeats=1)
+    log(f"[rank {rank}] tuning {tuned['tuning']} ({tuned.get('tuned_s', 'cached')} s)")
+    acc, st0 = ctx.batch(ios)
+    evals_step = int(st0.evals)
+    plan = ctx.plan(ios)
+    for _ in range(max(3, args.warmup)):
+        plan.run(wait=False)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = ctx.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.run(wait=False)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    launches = ctx.launch_count() - launches0
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
+    acc2, st = plan.run()
+    assert (acc2 == acc).all()
+    value = sum_over_ranks(world, evals_step * args.steps) / (ms / 1e3)
+    ncc_batch = [lv.d_ncc.cpu().numpy().view(abi.NCCRESULT_DTYPE).copy() for lv in mw.levels]
+    # the same levels as separate split calls (one pipeline per level)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for lv in mw.levels:
+        ctx.vertical_line_locus_device(lv.desc, lv.d_gp3.data_ptr(), lv.d_ncc.data_ptr(), None,
+                                       None, "split")
+    e3.record(stream)
+    torch.cuda.synchronize(dev)
+    per_level_ms = e2.elapsed_time(e3)
+    # plain FP64 per level on a sample of levels (about 1e9 evaluations at most)
+    fp64 = None
+    if not args.skip_fp64 and rank == 0:
+        order = sorted(range(len(mw.levels)), key=lambda i: mw.levels[i].n_nodes)
+        sample, ev_s, ms_s, same, valid_n, ties = [], 0, 0.0, 0, 0, 0
+        for i in order:
+            lv = mw.levels[i]
+            e4 = torch.cuda.Event(enable_timing=True)
+            e5 = torch.cuda.Event(enable_timing=True)
+            e4.record(stream)
+            stp = ctx.vertical_line_locus_device(lv.desc, lv.d_gp3.data_ptr(), lv.d_ncc.data_ptr(),
+                                                 None, None, "plain", stats=True)
+            e5.record(stream)
+            torch.cuda.synchronize(dev)
+            ms_s += e4.elapsed_time(e5)
+            ev_s += stp.evals
+            nf = lv.d_ncc.cpu().numpy().view(abi.NCCRESULT_DTYPE)
+            nb = ncc_batch[i]
+            v = (nf["check_height_change"] > 0) & (nf["result4"] > 0)
+            same += int(((nf["result2"] == nb["result2"]) & (nf["result0"] == nb["result0"]))[v].sum())
+            valid_n += int(v.sum())
+            ties += int((v & (nf["result0"] == nf["result1"])).sum())
+            sample.append(lv.name)
+            if ev_s >= args.fp64_evals:
+                break
+        fp64 = {"value": ev_s / (ms_s / 1e3), "unit": UNIT, "levels": sample,
+                "evals": int(ev_s), "identical_peak_rate": same / max(1, valid_n),
+                "tie_rate": ties / max(1, valid_n), "timing": "per-level launches, CUDA events"}
+    if rank == 0:
+        wins = sorted({lv.template for lv in mw.levels})
+        alg = sum(workloads.BYTES_PER_EVAL[t] * 1.0 for t in wins) / len(wins)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 window sums, f64 RPC and decisions", "data": "synthetic",
+            "config": {"workload": {
+                "c3": "C3: 64 ragged stereo tiles (grids 128^2-2048^2 log-uniform at 2 m, images "
+                      "4 px per node, convergence 20-40 deg, own DEM and TIN ranges K 8-512 at "
+                      "0.5 m), 7x7, one persistent launch per step, CUDA graph",
+                "c4": "C4: 5-level pyramid of a 16384^2 pair (9x9 sigma 1.5 downsample), grids "
+                      "32 m -> 2 m, K 256 -> 16, 7x7 and 11x11 at every level, one persistent "
+                      "launch per step, CUDA graph"}[args.config],
+                "levels": len(mw.levels), "nodes": mw.n_nodes, "evals_per_step": evals_step,
+                "tuning": tuned["tuning"], "l2": "inputs larger than L2",
+                "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": evals_step * alg / (ms / args.steps / 1e3) / 1e9,
+                         "peak": json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+                         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0,
+                         "unit": "GB/s", "note": "whole pipeline time (graph replay), mean "
+                                                 "algorithmic bytes per evaluation of the windows"},
+            "per_level_split_calls": {"value": evals_step / (per_level_ms / 1e3), "unit": UNIT,
+                                      "ms": per_level_ms},
+            "gpu_launches": int(launches),
+            "fp64_plain_gpu": fp64,
+            "clocks": clk,
+        }
+        line["roofline"]["frac"] = line["roofline"]["achieved"] / line["roofline"]["peak"]
+        print(json.dumps(line), flush=True)
+    plan.close()
+    barrier(world)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# C5 serving
+# ---------------------------------------------------------------------------
+def run_c5(args):
+    """C5: a Poisson stream of stereo-tile requests over resident scenes,
+    served with continuous batching (setsm_b200/serving.py); p50 / p99
+    latency from arrival to result on the host, and evals/s over the
+    stream's makespan, beside sequential plain-FP64 processing of a sample."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    from setsm_b200 import serving, vll
+    dev = torch.device("cuda", local)
+    ctx = vll.Context(local)
+    t0 = time.time()
+    scenes = [serving.make_resident_scene(ctx, sid, args.c5_image, 5, dev,
+                                          seed=100 * (rank + 1) + sid)
+              for sid in range(args.c5_scenes)]
+    log(f"[rank {rank}] {len(scenes)} resident scenes built in {time.time() - t0:.1f} s "
+        f"({torch.cuda.memory_allocated(dev) / 1e9:.1f} GB)")
+    warm = serving.poisson_requests(16, 200.0, scenes, seed=1000 + rank)
+    serving.Server(scenes, device=local, hbm_budget=args.c5_budget * 1e9).run(warm, realtime=False)
+    reqs = serving.poisson_requests(args.c5_requests, args.c5_rate, scenes, seed=7 + rank)
+    clocks = Clocks(local)
+    clocks.start()
+    srv = serving.Server(scenes, device=local, hbm_budget=args.c5_budget * 1e9,
+                         max_batch=args.c5_max_batch, n_workers=2)
+    barrier(world)
+    rep = srv.run(reqs, realtime=True)
+    clk = clocks.stop()
+    # sequential plain FP64 on a sample of the same requests
+    by_sid = {rs.sid: rs for rs in scenes}
+    ev, ms = 0, 0.0
+    sample = reqs[: max(1, args.c5_fp64_sample)]
+    for r in sample:
+        ev0 = time.perf_counter()
+        _, _, e = serving.run_alone(ctx, r, by_sid[r.sid], dev, kernel="plain")
+        ms += (time.perf_counter() - ev0) * 1e3
+        ev += e
+    makespan = max_over_ranks(world, rep["makespan_s"])
+    value = sum_over_ranks(world, rep["evals"]) / makespan
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1,
+            "warmup": 1, "ms_per_step": makespan * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 window sums, f64 RPC and decisions", "data": "synthetic",
+            "config": {"workload": f"C5 serving: Poisson {args.c5_rate:g} req/s, "
+                                   f"{args.c5_requests} requests, grid 64^2-1024^2 and K 8-512 "
+                                   f"log-uniform, level 0, 7x7, {args.c5_scenes} resident "
+                                   f"{args.c5_image}^2 pairs with 5-level pyramids, HBM budget "
+                                   f"{args.c5_budget:g} GB, continuous batching on 2 streams",
+                       "parallelism": f"replicas x{world}"},
+            "serving": rep,
+            "latency_ms": {"p50": rep["p50_ms"], "p99": rep["p99_ms"]},
+            "fp64_plain_sequential": {"value": ev / (ms / 1e3), "unit": UNIT,
+                                      "requests": len(sample),
+                                      "timing": "host wall clock per request (synchronous)"},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2_small"])
+    ap.add_argument("--config", default="c2",
+                    choices=["c1", "c2", "c2_small", "c3", "c4", "c5"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--fp64-evals", type=float, default=5e8,
+                    help="evaluations of the plain FP64 comparison on multi-level configs")
+    ap.add_argument("--c5-scenes", type=int, default=8)
+    ap.add_argument("--c5-image", type=int, default=16384)
+    ap.add_argument("--c5-requests", type=int, default=400)
+    ap.add_argument("--c5-rate", type=float, default=200.0)
+    ap.add_argument("--c5-budget", type=float, default=120.0, help="HBM budget, GB")
+    ap.add_argument("--c5-max-batch", type=int, default=32)
+    ap.add_argument("--c5-fp64-sample", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.config in ("c3", "c4"):
+        run_multi(args)
+    elif args.config == "c5":
+        run_c5(args)
     else:
         run_ours(args)
 

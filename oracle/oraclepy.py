@@ -146,8 +146,9 @@ def heights_per_node(inputs, ncc: np.ndarray) -> np.ndarray:
 
 
 def vertical_line_locus(inputs, ncc: np.ndarray, voxels: np.ndarray | None = None,
-                        want_rho: bool = False):
-    """Returns Accessable_grid, or (Accessable_grid, rho, offsets, evals)."""
+                        want_rho: bool = False, want_evals: bool = False):
+    """Returns Accessable_grid, or (Accessable_grid, rho, offsets, evals), or
+    with `want_evals` (Accessable_grid, evals)."""
     d = inputs.desc()
     vp = voxels.ctypes.data if voxels is not None and voxels.size else None
     cap = voxels.size if voxels is not None else 0
@@ -163,6 +164,8 @@ def vertical_line_locus(inputs, ncc: np.ndarray, voxels: np.ndarray | None = Non
         rho.ctypes.data if rho is not None else None, ev.ctypes.data))
     if want_rho:
         return acc, rho, offs, int(ev[0])
+    if want_evals:
+        return acc, int(ev[0])
     return acc
 
 

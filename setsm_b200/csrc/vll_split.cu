@@ -41,6 +41,16 @@
 
 namespace vll {
 
+// Exclusive prefix sum of per-node int32 counts into int64 offsets, with an
+// int64 accumulator: the totals of a large level set exceed 2^31 (a 4096^2
+// grid already carries ~2 G height slots), and cub's ExclusiveSum would
+// accumulate in the input's 32-bit type.
+inline cudaError_t scan64(void *tmp, size_t &bytes, const int32_t *in, int64_t *out, int n,
+                          cudaStream_t s) {
+    return cub::DeviceScan::ExclusiveScan(tmp, bytes, in, out, cub::Sum(), (int64_t)0, n, s);
+}
+
+
 // Half-width of the FP32 error band of rho.  The measured FP32-vs-FP64 error
 // of rho is below 6e-7 (tests/test_gpu_accuracy.py); decisions closer than
 // this to a boundary are settled in FP64.
@@ -1303,9 +1313,9 @@ cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
     }
     if (!b.ctl) SPLIT_CUDA(cudaMalloc(&b.ctl, 8 * sizeof(unsigned long long)));
     size_t tmp1 = 0, tmp2 = 0;
-    SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp1, (const int32_t *)b.node_k,
+    SPLIT_CUDA(scan64(nullptr, tmp1, (const int32_t *)b.node_k,
                                              (int64_t *)b.slot_off, (int)(N + 1), s));
-    SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, (const int32_t *)b.item_cnt,
+    SPLIT_CUDA(scan64(nullptr, tmp2, (const int32_t *)b.item_cnt,
                                              (int64_t *)b.item_off, (int)(N + 1), s));
     SPLIT_CUDA(grow(b.scan_tmp, b.cap_scan, std::max(tmp1, tmp2)));
     // the level table is uploaded outside any capture (plan time) by the caller
@@ -1336,10 +1346,10 @@ cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
     ++*launches;
     mark(2);
     tmp1 = b.cap_scan;
-    SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp1, (const int32_t *)b.node_k,
+    SPLIT_CUDA(scan64(b.scan_tmp, tmp1, (const int32_t *)b.node_k,
                                              (int64_t *)b.slot_off, (int)(N + 1), s));
     tmp2 = b.cap_scan;
-    SPLIT_CUDA(cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp2, (const int32_t *)b.item_cnt,
+    SPLIT_CUDA(scan64(b.scan_tmp, tmp2, (const int32_t *)b.item_cnt,
                                              (int64_t *)b.item_off, (int)(N + 1), s));
     *launches += 4;   // two scans of two kernels each
     mark(3);
@@ -1398,6 +1408,10 @@ cudaError_t split_size(SplitBuffers &b, int64_t N, cudaStream_t s, std::string *
     SPLIT_CUDA(cudaStreamSynchronize(s));
     *n_slots = totals[0];
     *n_items = totals[1];
+    if (*n_slots < 0 || *n_items < 0) {
+        *err = "slot / item totals overflow";
+        return cudaErrorInvalidValue;
+    }
     size_t c = b.cap_slots;
     SPLIT_CUDA(grow(b.rho, c, (size_t)*n_slots * sizeof(float2)));
     b.cap_slots = c;
@@ -1616,7 +1630,7 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     int64_t *lbase = (int64_t *)cv.take(2 * 8);
     unsigned long long *acc_level = (unsigned long long *)cv.take(2 * 8);
     size_t scan_bytes = 0;
-    if (cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int32_t *)node_k, slot_off,
+    if (scan64(nullptr, scan_bytes, (const int32_t *)node_k, slot_off,
                                       (int)(N + 1), s) != cudaSuccess)
         return fail(VLL_ERR_CUDA, "scan size query failed");
     void *scan_tmp = cv.take(scan_bytes);
@@ -1647,10 +1661,10 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     noalloc_count_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(dP, node_k, item_cnt);
     NA_CUDA(cudaGetLastError());
     size_t t1 = scan_bytes;
-    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)node_k, slot_off,
+    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)node_k, slot_off,
                                           (int)(N + 1), s));
     t1 = scan_bytes;
-    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
+    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
                                           (int)(N + 1), s));
     int64_t totals[2] = {0, 0};
     NA_CUDA(cudaMemcpyAsync(&totals[0], slot_off + N, 8, cudaMemcpyDeviceToHost, s));
@@ -1673,10 +1687,10 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
                                                           counters, acc_level);
     NA_CUDA(cudaGetLastError());
     t1 = scan_bytes;
-    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)node_k, slot_off,
+    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)node_k, slot_off,
                                           (int)(N + 1), s));
     t1 = scan_bytes;
-    NA_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
+    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
                                           (int)(N + 1), s));
     if (n_items > 0) {
         items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, item_cnt, item_off, items,

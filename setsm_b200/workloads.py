@@ -167,3 +167,189 @@ def rows_for_budget(wl: Workload, evals_budget: float) -> int:
     per_row = wl.grid.width * float(np.mean((wl.gp3["maxHeight"].astype(np.int64)
                                              - wl.gp3["minHeight"]) / wl.cfg["height_step"]))
     return max(1, min(wl.grid.height, int(math.ceil(evals_budget / max(per_row, 1.0)))))
+
+
+# ---------------------------------------------------------------------------
+# Multi-level workloads: batches of levels matched in one pass
+# ---------------------------------------------------------------------------
+def height_step(pyramid_step: int, im_resolution: float) -> float:
+    """GetHeightStep (setsm_code.cpp:5741-5757): half the level's pixel size,
+    truncated to mm, capped at 3 m."""
+    hs = im_resolution * (1 << pyramid_step) / 2.0
+    hs = math.floor(hs * 1000.0 + 0.1) / 1000.0
+    return min(hs, 3.0)
+
+
+@dataclass
+class LevelWork:
+    """One level of a batch: its device planes, grid and UGRID / NCCresult."""
+    name: str
+    template: int
+    pyramid_step: int
+    grid_w: int
+    grid_h: int
+    gp3: np.ndarray                # host UGRID (pinned)
+    desc: abi.LevelDesc            # every pointer on the device
+    host_desc_kwargs: dict
+    d_gp3: torch.Tensor
+    d_ncc: torch.Tensor
+    keep: list = field(default_factory=list)
+
+    @property
+    def n_nodes(self) -> int:
+        return self.grid_w * self.grid_h
+
+    def io(self) -> tuple:
+        return (self.desc, self.d_gp3.data_ptr(), self.d_ncc.data_ptr())
+
+    def slots(self, step: float) -> int:
+        return int(np.sum(((self.gp3["maxHeight"].astype(np.int64) - self.gp3["minHeight"])
+                           / step).astype(np.int64)))
+
+
+@dataclass
+class MultiWorkload:
+    name: str
+    levels: list
+    scenes: list
+
+    @property
+    def n_nodes(self) -> int:
+        return sum(lv.n_nodes for lv in self.levels)
+
+    def ios(self) -> list:
+        return [lv.io() for lv in self.levels]
+
+
+def _level_desc(images, grid, gp3, *, pyramid_step, template, height_step_m, resolution,
+                param, boundary, keep) -> abi.LevelDesc:
+    """Descriptor of a level whose planes (dict per camera) are device tensors."""
+    li = level.LevelInputs(
+        [level.ImageLevel(image=np.zeros((2, 2), np.uint16), mag=np.zeros((2, 2), np.uint16),
+                          ori=np.zeros((2, 2), np.uint8), rpc=im["rpc"]) for im in images],
+        np.zeros((grid["n"], 2)), np.zeros((grid["n"], 2)), grid["w"], grid["h"], boundary, gp3,
+        pyramid_step=pyramid_step, template_size=template, iteration=1, check_matching_rate=True,
+        height_step=height_step_m, grid_resolution=grid["res"], resolution=resolution,
+        dem_resolution=2.0, minmax_height=(-500.0, 3000.0), sgm_py=0, param=param)
+    d = li.desc()
+    for ci, im in enumerate(images):
+        e = d.images[ci]
+        e.image, e.mag, e.ori = (im["img"].data_ptr(), im["mag"].data_ptr(), im["ori"].data_ptr())
+        e.height, e.width = im["img"].shape
+        if im.get("img_n") is not None:
+            e.image_next = im["img_n"].data_ptr()
+            e.mag_next = im["mag_n"].data_ptr()
+            e.ori_next = im["ori_n"].data_ptr()
+            e.height_next, e.width_next = im["img_n"].shape
+    d.grid_pts = grid["d_pts"].data_ptr()
+    d.grid_wgs = grid["d_wgs"].data_ptr()
+    keep.append(li)
+    return d
+
+
+def _planes(ctx, img: torch.Tensor) -> dict:
+    n_h, n_w = img.shape
+    mag = torch.empty_like(img)
+    ori = torch.empty((n_h, n_w), dtype=torch.uint8, device=img.device)
+    ctx.preprocess_device(img.data_ptr(), n_w, n_h, mag.data_ptr(), ori.data_ptr())
+    return {"img": img.contiguous(), "mag": mag, "ori": ori}
+
+
+def _grid_dev(grid, dev) -> dict:
+    return {"n": grid.width * grid.height, "w": grid.width, "h": grid.height,
+            "res": grid.resolution, "d_pts": torch.from_numpy(grid.pts).to(dev),
+            "d_wgs": torch.from_numpy(grid.wgs).to(dev)}
+
+
+def _level_work(name, images, grid, gd, lo, hi, centre, *, pyramid_step, template, step,
+                resolution, param, dev) -> LevelWork:
+    gp3 = level.make_gridpt3(lo, hi, centre)
+    keep = [gd, images]
+    d = _level_desc(images, gd, gp3, pyramid_step=pyramid_step, template=template,
+                    height_step_m=step, resolution=resolution, param=param,
+                    boundary=grid.boundary, keep=keep)
+    d_gp3 = torch.from_numpy(gp3.view(np.uint8).copy()).to(dev)
+    d_ncc = torch.zeros(gd["n"] * abi.NCCRESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    return LevelWork(name=name, template=template, pyramid_step=pyramid_step, grid_w=grid.width,
+                     grid_h=grid.height, gp3=gp3, desc=d,
+                     host_desc_kwargs=dict(step=step), d_gp3=d_gp3, d_ncc=d_ncc, keep=keep)
+
+
+def build_c3(ctx, device: str = "cuda", seed: int = 1, n_tiles: int = 64,
+             grid_min: int = 128, grid_max: int = 2048, template: int = 11) -> MultiWorkload:
+    """C3: n_tiles independent stereo tiles; grid side log-uniform in
+    [grid_min, grid_max] nodes at 2 m, images sized to match (4 px per node
+    at 0.5 m), convergence 20-40 degrees, each tile with its own fBm DEM and
+    TIN ranges of 8-512 candidates at 0.5 m; 7x7 window."""
+    dev = torch.device(device)
+    rng = np.random.default_rng(seed)
+    levels, scenes = [], []
+    for t in range(n_tiles):
+        g = int(round(math.exp(rng.uniform(math.log(grid_min), math.log(grid_max)))))
+        g = max(16, g - g % 2)
+        size = 8 * int(math.ceil(4 * g / 8))
+        conv = float(rng.uniform(20.0, 40.0))
+        cams = (synth.CameraSpec(conv / 2, float(rng.uniform(-1.5, 1.5))),
+                synth.CameraSpec(-conv / 2, float(rng.uniform(-1.5, 1.5))))
+        spec = synth.SceneSpec(seed=seed * 1000 + t, image_size=size, cameras=cams)
+        scene = synth.make_scene(spec, device=dev, rows_per_chunk=512)
+        grid = synth.make_grid(scene, g, 2.0, device=dev)
+        n_seeds = max(200, int(20000 * (g / 4096.0) ** 2))
+        lo, hi, centre = synth.ranges_tin(scene, grid, n_seeds, 8, 512, 0.5, 3.0,
+                                          seed=seed * 1000 + t + 1, device=dev)
+        ims = [dict(rpc=scene.rpcs[ci], **_planes(ctx, scene.images[ci])) for ci in range(2)]
+        scene.images = []        # the planes live in `ims`
+        gd = _grid_dev(grid, dev)
+        levels.append(_level_work(f"tile{t}", ims, grid, gd, lo, hi, centre, pyramid_step=0,
+                                  template=template, step=0.5, resolution=spec.gsd,
+                                  param=scene.param, dev=dev))
+        scenes.append(scene)
+    torch.cuda.synchronize(dev)
+    return MultiWorkload(name="c3", levels=levels, scenes=scenes)
+
+
+# C4 candidates per level (level 4 .. 0) and grid spacing (m)
+C4_LEVELS = {4: (256, 32.0), 3: (128, 16.0), 2: (64, 8.0), 1: (32, 4.0), 0: (16, 2.0)}
+
+
+def build_c4(ctx, device: str = "cuda", seed: int = 1, image_size: int = 16384,
+             templates=(11, 15)) -> MultiWorkload:
+    """C4: a 5-level pyramid of one stereo pair (the reference's 9x9,
+    sigma = 1.5 Gaussian 2x downsample, CreateImagePyramid), grid spacing 32 m
+    at level 4 down to 2 m at level 0, K = 256 .. 16 candidates per level at
+    that level's GetHeightStep around truth + N(0, sigma) with +-3 sigma
+    covering the range; every level with the 7x7 and 11x11 windows."""
+    dev = torch.device(device)
+    spec = synth.SceneSpec(seed=seed, image_size=image_size)
+    scene = synth.make_scene(spec, device=dev, rows_per_chunk=512)
+    pyr = [[scene.images[ci].contiguous()] for ci in range(2)]
+    for ci in range(2):
+        for _ in range(4):
+            src = pyr[ci][-1]
+            h, w = src.shape
+            out = torch.empty((h // 2, w // 2), dtype=torch.int16, device=dev)
+            ctx.pyramid_down_device(src.data_ptr(), w, h, out.data_ptr())
+            pyr[ci].append(out)
+    planes = [[_planes(ctx, pyr[ci][lv]) for lv in range(5)] for ci in range(2)]
+    scene.images = []
+    levels = []
+    for L in (4, 3, 2, 1, 0):
+        k, spacing = C4_LEVELS[L]
+        n = int(round(image_size * spec.gsd / spacing))
+        grid = synth.make_grid(scene, n, spacing, device=dev)
+        gd = _grid_dev(grid, dev)
+        step = height_step(L, spec.gsd)
+        lo, hi, centre = synth.ranges_uniform(grid, k, step, k * step / 6.0, seed=seed + 10 + L)
+        ims = []
+        for ci in range(2):
+            im = dict(rpc=scene.rpcs[ci], **planes[ci][L])
+            if L >= 1:
+                im.update(img_n=planes[ci][L - 1]["img"], mag_n=planes[ci][L - 1]["mag"],
+                          ori_n=planes[ci][L - 1]["ori"])
+            ims.append(im)
+        for t in templates:
+            levels.append(_level_work(f"L{L}_T{t}", ims, grid, gd, lo, hi, centre,
+                                      pyramid_step=L, template=t, step=step,
+                                      resolution=spec.gsd, param=scene.param, dev=dev))
+    torch.cuda.synchronize(dev)
+    return MultiWorkload(name="c4", levels=levels, scenes=[scene])
