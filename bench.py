@@ -234,6 +234,17 @@ def run_reference_arm(args):
     del torch
 
 
+# DRAM bytes per evaluation of the window kernel measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the reduced C2 workload:
+# 1228.4 MB / 121.53 M evaluations (7x7), 1225.9 MB / 121.28 M (11x11);
+# profiles/window_kernel_c2_small.md.  Traffic scales with the evaluations.
+DRAM_BYTES_PER_EVAL = {11: 1228.4e6 / 121.53e6, 15: 1225.9e6 / 121.28e6}
+
+
+def traffic_per_launch(evals_step: dict, templates) -> float:
+    return sum(evals_step[t] * DRAM_BYTES_PER_EVAL[t] for t in templates) / len(templates)
+
+
 def config_block(args, wl) -> dict:
     from setsm_b200 import workloads
     cfg = workloads.CONFIGS[args.config]
@@ -396,9 +407,14 @@ def run_ours(args):
             "dtype": "f32 window sums, f64 RPC and decisions", "data": "synthetic",
             "config": config_block(args, wl),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": None,
+                         "frac": achieved / hbm_peak,
+                         "traffic": traffic_per_launch(evals_step, templates),
+                         "traffic_unit": "bytes per window launch (mean of the step's windows)",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "of the window kernel on the reduced C2 case, scaled "
+                                           "by evaluations (profiles/window_kernel_c2_small.md)",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
-                         "kernel": "ncc_kernel (window)", "per_window": per_window},
+                         "kernel": "window_kernel", "per_window": per_window},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "fp64_rechecks_per_step": rechecks / args.steps,
