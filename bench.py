@@ -283,6 +283,14 @@ def run_ours(args):
         f"({wl.n_nodes} nodes)")
     templates = workloads.CONFIGS[args.config]["templates"]
     descs = {t: wl.device_desc(t) for t in templates}
+    tuned = None
+    if not args.no_tune:
+        # autotune the window kernel's launch on a band of grid rows (cached
+        # per GPU and window set; results do not depend on the tuning)
+        from setsm_b200 import autotune
+        ios = [wl.device_band_io(t, args.tune_rows) for t in templates]
+        tuned = autotune.tune(ctx, ios, repeats=1)
+        log(f"[rank {rank}] tuning {tuned['tuning']} ({tuned.get('tuned_s', 'cached')} s)")
 
     def one_step(kernel, stats=True):
         out = {}
@@ -417,6 +425,7 @@ def run_ours(args):
                          "kernel": "window_kernel", "per_window": per_window},
             "e2e": e2e,
             "gpu_launches": int(launches),
+            "tuning": tuned["tuning"] if tuned else None,
             "fp64_rechecks_per_step": rechecks / args.steps,
             "fp64_plain_gpu": fp64,
             "cpu_baseline": cpu,
@@ -640,6 +649,8 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--tune-rows", type=int, default=256)
     ap.add_argument("--fp64-evals", type=float, default=5e8,
                     help="evaluations of the plain FP64 comparison on multi-level configs")
     ap.add_argument("--c5-scenes", type=int, default=8)

@@ -21,6 +21,25 @@ LIB_PATH = os.path.join(HERE, "_ref", "libsetsm_ref.so")
 _lib = None
 
 
+class _StdoutToStderr:
+    """Sends the reference's own printf output (file descriptor 1) to stderr
+    while a reference call runs, so a caller's stdout carries only its own
+    output (bench.py prints one JSON line there)."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def available() -> bool:
     return os.path.exists(LIB_PATH)
 
@@ -163,8 +182,9 @@ def initialize_voxel(inputs, ncc: np.ndarray, voxels_in: np.ndarray | None):
                / inputs.height_step + 4).clip(0).sum())
     out = np.zeros(max(cap, 1), dtype=abi.VOXEL_DTYPE)
     vin = voxels_in.ctypes.data if voxels_in is not None and voxels_in.size else None
-    n = lib().ref_initialize_voxel(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data,
-                                   vin, out.ctypes.data, out.size)
+    with _StdoutToStderr():
+        n = lib().ref_initialize_voxel(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data,
+                                       vin, out.ctypes.data, out.size)
     assert n <= out.size
     return out[:n].copy()
 
@@ -173,14 +193,16 @@ def vertical_line_locus(inputs, ncc: np.ndarray, voxels: np.ndarray | None = Non
     d = inputs.desc()
     vp = voxels.ctypes.data if voxels is not None and voxels.size else None
     cap = voxels.size if voxels is not None else 0
-    return int(lib().ref_vertical_line_locus(C.byref(d), inputs.gridpt3.ctypes.data,
-                                             ncc.ctypes.data, vp, cap))
+    with _StdoutToStderr():
+        return int(lib().ref_vertical_line_locus(C.byref(d), inputs.gridpt3.ctypes.data,
+                                                 ncc.ctypes.data, vp, cap))
 
 
 def awncc(inputs, ncc: np.ndarray, voxels: np.ndarray) -> None:
     d = inputs.desc()
     vp = voxels.ctypes.data if voxels.size else None
-    lib().ref_awncc(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data, vp, voxels.size)
+    with _StdoutToStderr():
+        lib().ref_awncc(C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data, vp, voxels.size)
 
 
 def _kat_lib():
@@ -216,9 +238,10 @@ def call_vertical_line_locus(fn_addr: int, inputs, ncc: np.ndarray, voxels=None)
     d = inputs.desc()
     vp = voxels.ctypes.data if voxels is not None else None
     cap = voxels.size if voxels is not None else 0
-    return int(_kat_lib().ref_call_vertical_line_locus(fn_addr, C.byref(d),
-                                                      inputs.gridpt3.ctypes.data,
-                                                      ncc.ctypes.data, vp, cap))
+    with _StdoutToStderr():
+        return int(_kat_lib().ref_call_vertical_line_locus(fn_addr, C.byref(d),
+                                                          inputs.gridpt3.ctypes.data,
+                                                          ncc.ctypes.data, vp, cap))
 
 
 def layout() -> list:

@@ -25,10 +25,10 @@ import json
 import os
 import time
 
-DEFAULT = {"blocks_per_sm": 0, "grab": 4, "box_margin": 1.25}
+DEFAULT = {"blocks_per_sm": 0, "grab": 1, "box_margin": 1.1}
 
 CANDIDATES = [dict(blocks_per_sm=b, grab=g, box_margin=m)
-              for b, g, m in itertools.product((0, 2), (1, 2, 4, 8), (1.1, 1.25, 1.6))]
+              for b, g, m in itertools.product((0, 2), (1, 2, 4, 8), (1.0, 1.1, 1.25))]
 
 
 def cache_path() -> str:

@@ -1049,8 +1049,8 @@ int vll_set_tuning(vll_context *ctx, const vll_tuning *t) {
         (t->box_margin > 0.f && t->box_margin < 1.0f) || t->box_margin > 4.0f)
         return fail(ctx, VLL_ERR_INVALID, "tuning out of range");
     ctx->tuning.blocks_per_sm = t->blocks_per_sm;
-    ctx->tuning.grab = t->grab > 0 ? t->grab : 4;
-    ctx->tuning.box_margin = t->box_margin > 0.f ? t->box_margin : 1.25f;
+    ctx->tuning.grab = t->grab > 0 ? t->grab : vll::SplitTuning().grab;
+    ctx->tuning.box_margin = t->box_margin > 0.f ? t->box_margin : vll::SplitTuning().box_margin;
     return VLL_OK;
 }
 

@@ -497,105 +497,152 @@ __device__ __forceinline__ int dir_sign(double a, double b) {
     return d > 0 ? 1 : (d < 0 ? -1 : 0);
 }
 
-// Runs the whole FindPeakNcc scan / max_WNCC of a node on its FP32 values and
-// writes the results when no decision lies within kBand of a boundary;
-// otherwise queues the node for the exact (warp) path.
-__global__ void __launch_bounds__(256) scan_thread_kernel(const LevelSet LS,
-                                                          const int64_t *__restrict__ slot_off,
-                                                          const float2 *__restrict__ rho,
-                                                          int64_t *__restrict__ pending,
-                                                          unsigned long long *__restrict__ ctl) {
+// The FindPeakNcc scan and max_WNCC of every node on its FP32 values: a node
+// whose every decision lies outside the band kBand of its boundary (direction
+// ties and signs, rounding of the top-two peaks and of the maximum, voxel
+// truncation) gets its results written here; any other node is queued for the
+// exact FP64 pass (peaks_kernel).
+//
+// A persistent state machine: every lane advances one slot of its current
+// node per iteration and fetches its next node from a queue (warp-aggregated
+// atomics) when its node is done, so lanes of a warp stay busy whatever the
+// spread of K (8..512) among the nodes they hold.  One pass over the slots:
+// two of the checks need the node's final maximum and top two -- whether a
+// slot at or near the maximum rounds ambiguously, and whether a peak at or
+// above the top-two threshold does; both are monotone in the value, so the
+// maximum over the ambiguously rounding slots (and over such peaks), kept
+// during the pass, decides them exactly at its end.
+__global__ void __launch_bounds__(256) scan_queue_kernel(const LevelSet LS,
+                                                         const int64_t *__restrict__ slot_off,
+                                                         const float2 *__restrict__ rho,
+                                                         int64_t *__restrict__ pending,
+                                                         unsigned long long *__restrict__ ctl) {
     if (ctl[5]) return;
-    for (int64_t gn = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gn < LS.total;
-         gn += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t so = slot_off[gn];
-        const int K = (int)(slot_off[gn + 1] - so);
-        if (K == 0) continue;
-        const int lvl = level_of(LS, gn);
-        const DevLevel &P = LS.lv[lvl];
-        const int64_t pt = gn - __ldg(LS.base + lvl);
-        const bool voxels = P.vox && !P.cmr && !P.is_ra;
-        const float2 *rv = rho + so;
-        vll_nccresult R = P.ncc[pt];
-        const int start_H = P.gp3[pt].minHeight;
-        bool need = K > kSlotCap;
-        int check_rho = 0, direction = 0;
-        double pre_rho = -1.0, max_w = -100, b1 = -1e30, b2 = -1e30;
-        float pre_h = 0.f;
-        for (int k = 0; k < K && !need; ++k) {
-            const float2 v2 = rv[k];
-            if (v2.x == kNotEvaluated || v2.x == kRejected) continue;
-            const double v = (double)v2.x;
-            if (isnan(v2.y) || (voxels && near_trunc((double)v2.y))) need = true;
-            if (P.cmr) {
-                if (check_rho &&
-                    (fabs(v - pre_rho) < kBand || fabs(v) < kBand || fabs(pre_rho) < kBand))
-                    need = true;
-                int td = dir_sign(v, pre_rho);
-                if (!check_rho) {
-                    check_rho = 1;
-                    td = -1;
-                } else if (pre_rho != -1 && direction > 0 && td < 0) {
-                    if (pre_rho > b1) {
-                        b2 = b1;
-                        b1 = pre_rho;
-                    } else if (pre_rho > b2) {
-                        b2 = pre_rho;
+    const int lane = threadIdx.x & 31;
+    unsigned long long *queue = ctl + 4;
+    // per-lane state
+    bool active = true;       // this lane still has (or may fetch) work
+    bool have = false;        // a node is loaded
+    int64_t gn = 0, pt = 0;
+    const DevLevel *Pp = nullptr;
+    const float2 *rv = nullptr;
+    int K = 0, k = 0, check_rho = 0, direction = 0, start_H = 0;
+    bool need = false, voxels = false;
+    double pre_rho = -1.0, max_w = -100, b1 = -1e30, b2 = -1e30;
+    double max_amb = -1e30, max_amb_peak = -1e30;   // ambiguous roundings seen
+    float pre_h = 0.f;
+    vll_nccresult R;
+    for (;;) {
+        // ---- fetch nodes for the lanes that need one --------------------------
+        const bool want = active && !have;
+        const uint32_t wm = __ballot_sync(0xffffffffu, want);
+        if (wm) {
+            const int leader = __ffs(wm) - 1;
+            unsigned long long b = 0;
+            if (lane == leader) b = atomicAdd(queue, (unsigned long long)__popc(wm));
+            b = __shfl_sync(0xffffffffu, b, leader);
+            if (want) {
+                const unsigned long long idx = b + __popc(wm & ((1u << lane) - 1u));
+                if (idx >= (unsigned long long)LS.total) {
+                    active = false;
+                } else {
+                    gn = (int64_t)idx;
+                    const int64_t so = slot_off[gn];
+                    K = (int)(slot_off[gn + 1] - so);
+                    if (K > 0) {
+                        const int lvl = level_of(LS, gn);
+                        Pp = LS.lv + lvl;
+                        pt = gn - __ldg(LS.base + lvl);
+                        rv = rho + so;
+                        R = Pp->ncc[pt];
+                        start_H = Pp->gp3[pt].minHeight;
+                        voxels = Pp->vox && !Pp->cmr && !Pp->is_ra;
+                        need = K > kSlotCap;
+                        k = 0;
+                        check_rho = 0;
+                        max_amb = -1e30;
+                        max_amb_peak = -1e30;
+                        direction = 0;
+                        pre_rho = -1.0;
+                        max_w = -100;
+                        b1 = -1e30;
+                        b2 = -1e30;
+                        pre_h = 0.f;
+                        have = true;
                     }
-                    if (R.result4 < 10) R.result4 += 1;
-                    const int16_t qpre = q_result(pre_rho);
-                    if (R.result0 < qpre) {
-                        const double t1 = dq_result(R.result0);
-                        R.result0 = qpre;
-                        const float t2 = R.result2;
-                        R.result2 = pre_h;
-                        const int16_t q1 = q_result(t1);
-                        if (R.result1 < q1) {
-                            R.result1 = q1;
-                            R.result3 = t2;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        // ---- one slot of the current node -------------------------------------
+        if (have) {
+            const DevLevel &P = *Pp;
+            if (!need && k < K) {
+                const float2 v2 = __ldg(rv + k);
+                if (v2.x != kNotEvaluated && v2.x != kRejected) {
+                    const double v = (double)v2.x;
+                    if (isnan(v2.y) || (voxels && near_trunc((double)v2.y))) need = true;
+                    if (near_round(v) && v > max_amb) max_amb = v;
+                    if (P.cmr) {
+                        if (check_rho && (fabs(v - pre_rho) < kBand || fabs(v) < kBand ||
+                                          fabs(pre_rho) < kBand))
+                            need = true;
+                        int td = dir_sign(v, pre_rho);
+                        if (!check_rho) {
+                            check_rho = 1;
+                            td = -1;
+                        } else if (pre_rho != -1 && direction > 0 && td < 0) {
+                            if (near_round(pre_rho) && pre_rho > max_amb_peak)
+                                max_amb_peak = pre_rho;
+                            if (pre_rho > b1) {
+                                b2 = b1;
+                                b1 = pre_rho;
+                            } else if (pre_rho > b2) {
+                                b2 = pre_rho;
+                            }
+                            if (R.result4 < 10) R.result4 += 1;
+                            const int16_t qpre = q_result(pre_rho);
+                            if (R.result0 < qpre) {
+                                const double t1 = dq_result(R.result0);
+                                R.result0 = qpre;
+                                const float t2 = R.result2;
+                                R.result2 = pre_h;
+                                const int16_t q1 = q_result(t1);
+                                if (R.result1 < q1) {
+                                    R.result1 = q1;
+                                    R.result3 = t2;
+                                }
+                            } else if (R.result1 < qpre) {
+                                R.result1 = qpre;
+                                R.result3 = pre_h;
+                            }
                         }
-                    } else if (R.result1 < qpre) {
-                        R.result1 = qpre;
-                        R.result3 = pre_h;
+                        pre_rho = v;
+                        pre_h = slot_height(P, start_H, R.minHeight, k);
+                        direction = td;
                     }
+                    if (max_w < v) max_w = v;
                 }
-                pre_rho = v;
-                pre_h = slot_height(P, start_H, R.minHeight, k);
-                direction = td;
+                ++k;
             }
-            if (max_w < v) max_w = v;
-        }
-        if (!need) {
-            // rounding of the top-two peak values and of the maximum
-            const double thr = (b2 > -1e29 ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
-            check_rho = 0;
-            direction = 0;
-            pre_rho = -1.0;
-            for (int k = 0; k < K && !need; ++k) {
-                const float2 v2 = rv[k];
-                if (v2.x == kNotEvaluated || v2.x == kRejected) continue;
-                const double v = (double)v2.x;
-                if (R.check_height_change && v >= max_w - kBand && near_round(v)) need = true;
-                if (P.cmr) {
-                    int td = dir_sign(v, pre_rho);
-                    if (!check_rho) {
-                        check_rho = 1;
-                        td = -1;
-                    } else if (pre_rho != -1 && direction > 0 && td < 0 && pre_rho >= thr &&
-                               near_round(pre_rho)) {
-                        need = true;
-                    }
-                    pre_rho = v;
-                    direction = td;
+            if (!need && k >= K) {
+                // rounding of the maximum, and of peaks that can reach the top
+                // two (a peak more than 0.002 + 2 bands below the second best
+                // rounds strictly below it)
+                const double thr = (b2 > -1e29 ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
+                if (R.check_height_change && max_amb >= max_w - kBand) need = true;
+                if (P.cmr && max_amb_peak > -1e29 && max_amb_peak >= thr) need = true;
+            }
+            if (need || k >= K) {
+                if (need) {
+                    pending[atomicAdd(&ctl[2], 1ull)] = gn;
+                    atomicAdd(&ctl[3], 1ull);
+                } else {
+                    if (R.check_height_change) R.max_WNCC = q_result(max_w);
+                    P.ncc[pt] = R;
                 }
+                have = false;
             }
-        }
-        if (need) {
-            pending[atomicAdd(&ctl[2], 1ull)] = gn;
-            atomicAdd(&ctl[3], 1ull);
-        } else {
-            if (R.check_height_change) R.max_WNCC = q_result(max_w);
-            P.ncc[pt] = R;
         }
     }
 }
@@ -1158,7 +1205,7 @@ int window_warp_quads(const DevLevel &P, float margin) {
     const int side = 2 * H + 3;
     const int rside = 2 * ((int)ceilf(1.4143f * H) + 1) + 3;
     const double need = (side + 1.0) * (side + sweep0 + 2.0) + (rside + 1.0) * (rside + sweep1 + 2.0);
-    int q = (int)(need * (margin > 0 ? margin : 1.25f)) + 32;
+    int q = (int)(need * (margin > 0 ? margin : 1.1f)) + 32;
     const int cap = (int)((200 * 1024 - win_boxes_offset()) / (kWinWarps * sizeof(float4)));
     return std::min(q, cap);
 }
@@ -1195,7 +1242,7 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel, kWinWarps * 32, smem);
     if (tu.blocks_per_sm > 0 && tu.blocks_per_sm < per_sm) per_sm = tu.blocks_per_sm;
     if (per_sm < 1) per_sm = 1;
-    const int grab = tu.grab > 0 ? std::min(tu.grab, 64) : 4;
+    const int grab = tu.grab > 0 ? std::min(tu.grab, 64) : 1;
     window_kernel<<<sms * per_sm, kWinWarps * 32, smem, s>>>(LS, items, n_items, slot_off, gsum,
                                                              gcnt, rho, counters, ctl + 0, wq,
                                                              grab, ctl + 5);
@@ -1235,8 +1282,16 @@ cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, cons
                                   ctl, tu, s);
     if (e != cudaSuccess) return e;
     if (tm && tm->enabled) cudaEventRecord(tm->ev[5], s);
-    scan_thread_kernel<<<grid_1d(LS.total, 256, 148 * 32), 256, 0, s>>>(LS, slot_off, rho, pending,
-                                                                       ctl);
+    {
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_queue_kernel, 256, 0);
+        if (per_sm < 1) per_sm = 1;
+        const int64_t want = (LS.total + 255) / 256;
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * per_sm));
+        scan_queue_kernel<<<blocks, 256, 0, s>>>(LS, slot_off, rho, pending, ctl);
+    }
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (tm && tm->enabled) cudaEventRecord(tm->ev[6], s);

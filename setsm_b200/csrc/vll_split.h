@@ -38,8 +38,8 @@ struct SplitBuffers {
 // Launch parameters of the window kernel that the autotuner chooses.
 struct SplitTuning {
     int blocks_per_sm = 0;      // CTAs per SM (0: the occupancy maximum)
-    int grab = 4;               // work items taken per queue access
-    float box_margin = 1.25f;   // footprint budget over the swept-box estimate
+    int grab = 1;               // work items taken per queue access
+    float box_margin = 1.1f;    // footprint budget over the swept-box estimate
 };
 
 // A level set's pipeline captured as a CUDA graph, with its own buffers.

@@ -81,6 +81,20 @@ class Workload:
         d.grid_wgs = self.d_wgs.data_ptr()
         return d
 
+    def device_band_io(self, template: int, rows: int) -> tuple:
+        """(descriptor, d_gridpt3, d_nccresult) of a band of `rows` grid rows in
+        the middle of the grid, on the resident device arrays (memory-tight
+        route: no orthoimage raster depends on the band's boundary)."""
+        rows = max(1, min(rows, self.grid.height))
+        r0 = (self.grid.height - rows) // 2
+        W = self.grid.width
+        d = self.device_desc(template)
+        d.grid_height = rows
+        d.grid_pts = self.d_pts.data_ptr() + r0 * W * 16
+        d.grid_wgs = self.d_wgs.data_ptr() + r0 * W * 16
+        return (d, self.d_gp3.data_ptr() + r0 * W * abi.UGRID_DTYPE.itemsize,
+                self.d_ncc.data_ptr() + r0 * W * abi.NCCRESULT_DTYPE.itemsize)
+
     def host_inputs(self, template: int, rows: tuple | None = None) -> level.LevelInputs:
         """LevelInputs on the pinned host copies (optionally a band of grid rows)."""
         h = self.host
