@@ -283,8 +283,10 @@ typedef struct vll_level_io {
  * persistent window launch draining every level's (node, 32-slot) work items,
  * one peak scan and one exact FP64 pass.  Each level's outputs are exactly
  * those of vll_vertical_line_locus_device on that level alone.  Every level
- * must be one the split kernel implements (stereo, no combined-level INCC);
- * otherwise VLL_ERR_UNSUPPORTED.  accessable (optional, host, n_levels)
+ * must be one the split kernel implements (stereo, window half-size 2..7);
+ * otherwise VLL_ERR_UNSUPPORTED.  Levels matched in combined mode (the
+ * next finer level's window added to the INCC, setsm_code.cpp:6378-6464) are
+ * evaluated in exact FP64 inside the same launch.  accessable (optional, host, n_levels)
  * receives each level's Accessable_grid.  Waits for the GPU.
  */
 int vll_vertical_line_locus_batch(vll_context *ctx, const vll_level_io *levels, int n_levels,

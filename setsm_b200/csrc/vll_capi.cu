@@ -405,7 +405,7 @@ int prepare_set(vll_context *ctx, SetResources &r, const vll_level_io *levels, i
             return fail(ctx, VLL_ERR_UNSUPPORTED,
                         "level " + std::to_string(l) +
                             ": not a level the batched split pipeline implements (stereo, "
-                            "no combined-level INCC)");
+                            "window half-size 2..7)");
         if (!P.cmr && !P.is_ra && (!io.d_voxels || !io.d_voxel_offsets))
             return fail(ctx, VLL_ERR_INVALID,
                         "level " + std::to_string(l) + ": voxel route needs voxel rows and offsets");

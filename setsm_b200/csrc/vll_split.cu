@@ -332,6 +332,43 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             const int ncc_min = P.ncc[pt].minHeight;
             const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
             const double cnt_g = gcnt ? gcnt[gn] : 0.0, sum_g = gsum ? gsum[gn] : 0.0;
+            if (P.combined_incc) {
+                // combined-level INCC (setsm_code.cpp:6378-6464): the windows
+                // at this level and the next finer one, the averaged
+                // orientation and both bounds tests, in exact FP64
+                // (eval_slot); the exact pass settles these nodes wholly.
+                if (k < K) {
+                    float rho_v = kNotEvaluated;
+                    const float hgt = slot_height(P, start_H, ncc_min, k);
+                    SlotOut o;
+                    o.evaluated = o.orient_reject = o.all_pos = false;
+                    if (hgt >= (float)start_H && hgt <= (float)end_H) {
+                        PatchSrc S, Sn;
+                        make_src(P, 1, S, Sn);
+                        o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
+                    }
+                    double incc = -1.0;
+                    if (o.evaluated) {
+                        rho_v = (float)o.rho;
+                        incc = o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc) : -1.0;
+                        evals++;
+                    } else if (o.orient_reject) {
+                        rho_v = kRejected;
+                    }
+                    rho[so + k] = make_float2(rho_v, (float)incc);
+                    if (P.dbg_rho && o.evaluated) P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
+                    if (voxels) {
+                        vll_voxel *v = P.vox + P.vox_off[pt] + k;
+                        if (o.orient_reject) v->flag_cal = 0;
+                        if (o.evaluated) {
+                            if (o.all_pos) v->flag_cal = 1;
+                            v->INCC = q_voxel(incc);
+                        }
+                    }
+                }
+                __syncwarp();
+                continue;
+            }
             // per-node RPC cubics: lanes 0..7 = (image, polynomial)
             if (lane < 8) {
                 const int im = lane >> 2, j = lane & 3;
@@ -910,8 +947,10 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
         const int start_H = P.gp3[pt].minHeight;
         const double cnt_g = gcnt ? gcnt[gn] : 0.0, sum_g = gsum ? gsum[gn] : 0.0;
         vll_voxel *vrow = voxels ? P.vox + P.vox_off[pt] : nullptr;
-        if (K > kSlotCap) {
-            // more slots than the shared scan buffer holds: all slots exactly
+        if (K > kSlotCap || P.combined_incc) {
+            // more slots than the shared scan buffer holds, or a combined-level
+            // INCC node (whose per-slot re-checks need both levels): all slots
+            // exactly
             node_exact_warp(P, pt, K, const_cast<float2 *>(rho) + so, S, Sn, cnt_g, sum_g, R, vrow,
                             lane, rechecks);
             continue;
@@ -1302,8 +1341,8 @@ cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, cons
 }  // namespace
 
 bool split_supported(const DevLevel &P) {
-    return P.num_images == 2 && P.ref == 0 && P.im[1].selected && !P.is_ra && !P.combined_incc &&
-           P.H >= 2 && P.H <= 7;
+    return P.num_images == 2 && P.ref == 0 && P.im[1].selected && !P.is_ra && P.H >= 2 &&
+           P.H <= 7;
 }
 
 void split_release(SplitBuffers &b) {

@@ -51,9 +51,10 @@ struct SplitPlan {
 
 void split_release(SplitBuffers &b);
 
-// Whether the split kernel implements this level (stereo, no frame sensor,
-// no relative-adjustment mode, H within the compiled window sizes); other
-// levels run the plain FP64 kernel.
+// Whether the split pipeline implements this level (stereo, no frame sensor,
+// no relative-adjustment mode, H within the compiled window sizes; levels
+// with combined-level INCC are evaluated in FP64 inside it); other levels run
+// the plain FP64 kernel.
 bool split_supported(const DevLevel &P);
 
 // Runs the split pipeline for a level whose DevLevel block is at dP (device)

@@ -12,7 +12,7 @@ from tests.test_gpu_parity import oracle_run
 
 pytestmark = pytest.mark.gpu
 
-MIX = ["m7", "m11", "m7_edges", "l3_m", "v7_gncc", "v11", "l2_max", "v7_it2"]
+MIX = ["m7", "m11", "m7_edges", "l3_m", "v7_gncc", "v11", "l2_max", "v7_it2", "l2_combined"]
 
 
 def build_batch(torch, names):
@@ -117,9 +117,12 @@ def test_tuning_rejects_bad_values(gpu_ctx):
         gpu_ctx.set_tuning(box_margin=0.5)
 
 
-def test_batch_refuses_combined_incc_level(gpu_ctx):
+def test_batch_refuses_unsupported_window(gpu_ctx):
+    """A 17x17 window (half-size 8) is matched by the plain FP64 kernel only;
+    a batch containing it is refused with a status, not run partially."""
     import torch
-    levels, held = build_batch(torch, ["m7", "l2_combined"])
+    levels, held = build_batch(torch, ["m7", "m11"])
+    levels[1][0].template_size = 21
     with pytest.raises(vll.VLLError) as e:
         gpu_ctx.batch(levels)
     assert e.value.code == abi.VLL_ERR_UNSUPPORTED
