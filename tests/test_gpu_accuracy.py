@@ -2,8 +2,10 @@
 slot by slot (before the split kernel's FP64 re-checks).
 
 Tolerance (stated by the matching spec): |delta NCC| <= 1e-4 on every slot.
-The split kernel's error band for re-checks (2e-5) must also cover the
-observed error with margin, otherwise its exactness argument fails."""
+The split pipeline settles in FP32 every decision whose inputs lie further
+than its error band (kBand = 4e-6 in vll_split.cu) from the decision's
+boundary, and re-evaluates the others in FP64; that is exact only while the
+FP32 error stays below half the band, which is asserted here."""
 import numpy as np
 import pytest
 
@@ -12,12 +14,16 @@ from tests import cases
 pytestmark = pytest.mark.gpu
 
 NCC_TOL = 1e-4
-BAND = 2e-5
+BAND = 4e-6   # kBand of setsm_b200/csrc/vll_split.cu
 
 
-@pytest.mark.parametrize("name", ["m7", "m11", "m7_edges", "l3_m"])
+BIG = {"m7_wide": dict(size=1536, nodes=112, res=6.0, n_heights=160, hs=0.5),
+       "m11_wide": dict(size=1536, nodes=112, res=6.0, n_heights=160, hs=0.5, template=15)}
+
+
+@pytest.mark.parametrize("name", ["m7", "m11", "m7_edges", "l3_m", "m7_wide", "m11_wide"])
 def test_fp32_rho_error(gpu_ctx, name):
-    inp = cases.make_case(**cases.CASES[name])
+    inp = cases.make_case(**(BIG[name] if name in BIG else cases.CASES[name]))
     r32, off = gpu_ctx.debug_slot_rho(inp, inp.new_nccresult(), "split")
     r64, off2 = gpu_ctx.debug_slot_rho(inp, inp.new_nccresult(), "plain")
     assert np.array_equal(off, off2)
