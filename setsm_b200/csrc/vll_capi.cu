@@ -11,6 +11,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "setsm_vll.h"
 #include "vll_device.cuh"
@@ -42,6 +43,13 @@ void release(Buf &b) {
 }
 
 thread_local std::string g_last_error;
+
+// NVTX range around each public call (visible in Nsight Systems / Compute
+// timelines; header-only, no cost when no tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 }  // namespace
 
@@ -617,6 +625,7 @@ int64_t vll_voxel_count(const vll_nccresult *ncc, int64_t n) {
 int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
                             vll_nccresult *nccresult, vll_voxel *voxels, int64_t voxel_capacity,
                             int kernel, vll_stats *stats) {
+    NvtxRange nvtx_range("vll_vertical_line_locus");
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
     if (!desc || !gridpt3 || !nccresult)
         return fail(ctx, VLL_ERR_INVALID, "null descriptor, gridpt3 or nccresult");
@@ -691,6 +700,7 @@ int vll_vertical_line_locus_device(vll_context *ctx, const vll_level_desc *desc,
                                    const vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
                                    vll_voxel *d_voxels, const int64_t *d_voxel_offsets, int kernel,
                                    vll_stats *stats) {
+    NvtxRange nvtx_range("vll_vertical_line_locus_device");
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
     if (!desc || !d_gridpt3 || !d_nccresult)
         return fail(ctx, VLL_ERR_INVALID, "null descriptor, gridpt3 or nccresult");
@@ -791,6 +801,7 @@ int vll_debug_slot_rho(vll_context *ctx, const vll_level_desc *desc, const vll_u
 int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
                     vll_nccresult *nccresult, const vll_voxel *voxels, int64_t voxel_capacity,
                     vll_stats *stats) {
+    NvtxRange nvtx_range("vll_awncc_peaks");
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
     if (!desc || !gridpt3 || !nccresult) return fail(ctx, VLL_ERR_INVALID, "null argument");
     VLL_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -837,6 +848,7 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugri
 int vll_preprocess_level_device(vll_context *ctx, const uint16_t *d_image, uint32_t width,
                                 uint32_t height, int template_size, uint16_t *d_mag,
                                 uint8_t *d_ori) {
+    NvtxRange nvtx_range("vll_preprocess_level_device");
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
     if (!d_image || !d_mag || !d_ori || width < 1 || height < 1)
         return fail(ctx, VLL_ERR_INVALID, "invalid preprocessing arguments");
@@ -887,6 +899,7 @@ int vll_preprocess_level(vll_context *ctx, const uint16_t *image, uint32_t width
 
 int vll_pyramid_down_device(vll_context *ctx, const uint16_t *d_image, uint32_t width,
                             uint32_t height, uint16_t *d_out) {
+    NvtxRange nvtx_range("vll_pyramid_down_device");
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
     if (!d_image || !d_out || width < 2 || height < 2)
         return fail(ctx, VLL_ERR_INVALID, "invalid pyramid arguments");
@@ -941,6 +954,7 @@ struct vll_plan {
 
 int vll_vertical_line_locus_batch(vll_context *ctx, const vll_level_io *levels, int n_levels,
                                   int64_t *accessable, vll_stats *stats) {
+    NvtxRange nvtx_range("vll_vertical_line_locus_batch");
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
     VLL_CUDA(ctx, cudaSetDevice(ctx->device));
     SetResources &r = *ctx_set(ctx);
@@ -970,6 +984,7 @@ int vll_vertical_line_locus_batch(vll_context *ctx, const vll_level_io *levels, 
 }
 
 int vll_plan_create(vll_context *ctx, const vll_level_io *levels, int n_levels, vll_plan **out) {
+    NvtxRange nvtx_range("vll_plan_create");
     if (!ctx || !out) return fail(ctx, VLL_ERR_INVALID, "null context or output pointer");
     *out = nullptr;
     VLL_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -1007,6 +1022,7 @@ int vll_plan_create(vll_context *ctx, const vll_level_io *levels, int n_levels, 
 }
 
 int vll_plan_run(vll_plan *pl, int64_t *accessable, vll_stats *stats) {
+    NvtxRange nvtx_range("vll_plan_run");
     if (!pl || !pl->ctx) return fail(nullptr, VLL_ERR_INVALID, "null plan");
     vll_context *ctx = pl->ctx;
     VLL_CUDA(ctx, cudaSetDevice(ctx->device));
