@@ -319,10 +319,12 @@ int vll_set_tuning(vll_context *ctx, const vll_tuning *t);
 int vll_get_tuning(const vll_context *ctx, vll_tuning *t);
 
 /*
- * Non-SGM peak loop of AWNCC (setsm_code.cpp:7511-7702) over the packed voxel
- * rows, on HOST buffers.  Selects first/second peaks per node exactly as the
- * reference does from quantised voxels and the node's GNCC.  Levels where the
- * reference would run SGM (Pyramid_step <= SGM_py) return VLL_ERR_UNSUPPORTED.
+ * AWNCC (setsm_code.cpp:7001-7702) over the packed voxel rows, on HOST
+ * buffers: on levels with Pyramid_step <= SGM_py the 8-direction semi-global
+ * aggregation of the voxel INCC (SGM_start_pos / SGM_con_pos, :6755-6999)
+ * followed by the peak loop on the aggregated cost; on other levels the peak
+ * loop on the voxels and the node's GNCC.  First / second peaks per node are
+ * selected exactly as the reference does.
  */
 int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc,
                     const vll_ugrid *gridpt3, vll_nccresult *nccresult,

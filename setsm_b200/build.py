@@ -25,6 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC,
 SOURCES = {
     "vll_plain.cu": ["-fmad=false"],
     "vll_preprocess.cu": ["-fmad=false"],
+    "vll_sgm.cu": ["-fmad=false"],
     "vll_split.cu": [],
     "vll_capi.cu": [],
     "vll_shim.cu": [],

@@ -63,6 +63,7 @@ struct vll_context {
     Buf wgs, pts, gp3, ncc, vox, voxoff, gsum, gcnt;
     Buf ocd[VLL_MAX_IMAGES], ocdn[VLL_MAX_IMAGES], ocdptr;
     Buf pre_tmp, pre_wt, pre_img, pre_mag, pre_ori;
+    Buf sumcost;                       // SGM aggregation (float per voxel slot)
     vll::SplitBuffers split;
     vll::SplitTuning tuning;
     void *set = nullptr;               // SetResources of batch calls (vll_capi.cu)
@@ -580,6 +581,7 @@ void vll_destroy(vll_context *ctx) {
     release(ctx->pre_img);
     release(ctx->pre_mag);
     release(ctx->pre_ori);
+    release(ctx->sumcost);
     vll::split_release(ctx->split);
     if (ctx->set) {
         release_set(*(SetResources *)ctx->set);
@@ -809,12 +811,15 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugri
     std::string err;
     int rc = vll::derive_level(desc, &P, &err);
     if (rc) return fail(ctx, rc, err);
-    if (P.L <= desc->sgm_py)
-        return fail(ctx, VLL_ERR_UNSUPPORTED, "SGM aggregation levels are not implemented");
+    const bool sgm = P.L <= desc->sgm_py;   // AWNCC's check_SGM (setsm_code.cpp:7013-7015)
     const int64_t N = P.n_nodes;
     std::vector<int64_t> off((size_t)N + 1);
     off[0] = 0;
-    for (int64_t i = 0; i < N; ++i) off[i + 1] = off[i] + nccresult[i].NumOfHeight;
+    int max_h = 0;
+    for (int64_t i = 0; i < N; ++i) {
+        off[i + 1] = off[i] + nccresult[i].NumOfHeight;
+        if (nccresult[i].NumOfHeight > max_h) max_h = nccresult[i].NumOfHeight;
+    }
     if (off[N] > 0 && (!voxels || voxel_capacity < off[N]))
         return fail(ctx, VLL_ERR_CAPACITY, "voxel buffer smaller than sum(NumOfHeight)");
     if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
@@ -831,7 +836,14 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugri
         VLL_CUDA(ctx, cudaEventCreate(&ctx->e1));
     }
     VLL_CUDA(ctx, cudaEventRecord(ctx->e0, ctx->stream));
-    VLL_CUDA(ctx, vll::launch_awncc((const DevLevel *)ctx->level.p, N, ctx->stream));
+    const float *sumcost = nullptr;
+    if (sgm) {
+        VLL_CUDA(ctx, ensure(ctx->sumcost, (size_t)(off[N] > 0 ? off[N] : 1) * sizeof(float)));
+        VLL_CUDA(ctx, vll::launch_sgm((const DevLevel *)ctx->level.p, P.grid_w, P.grid_h, max_h,
+                                      (float *)ctx->sumcost.p, off[N], ctx->stream));
+        sumcost = (const float *)ctx->sumcost.p;
+    }
+    VLL_CUDA(ctx, vll::launch_awncc((const DevLevel *)ctx->level.p, N, sumcost, ctx->stream));
     VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
     VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->ncc.p, (size_t)N * sizeof(vll_nccresult),
                                   cudaMemcpyDeviceToHost, ctx->stream));

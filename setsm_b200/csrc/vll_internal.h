@@ -14,7 +14,13 @@ cudaError_t launch_plain(const DevLevel *dP, int64_t n_nodes, unsigned long long
                          double *rho_out, const int64_t *rho_off, cudaStream_t s);
 cudaError_t launch_ortho(const DevLevel *dP, int64_t total, double2 *const *cd,
                          double2 *const *cdn, cudaStream_t s);
-cudaError_t launch_awncc(const DevLevel *dP, int64_t n_nodes, cudaStream_t s);
+cudaError_t launch_awncc(const DevLevel *dP, int64_t n_nodes, const float *sumcost,
+                         cudaStream_t s);
+
+// vll_sgm.cu: the 8-direction aggregation of AWNCC into sumcost (packed like
+// the voxel rows); max_h is the level's largest NumOfHeight.
+cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int max_h,
+                       float *sumcost, int64_t n_slots, cudaStream_t s);
 cudaError_t launch_gncc(const DevLevel *dP, int64_t n_nodes, double *gsum, double *gcnt,
                         cudaStream_t s);
 cudaError_t launch_recheck(const DevLevel *dP, const int64_t *items,

@@ -171,8 +171,12 @@ __global__ void __launch_bounds__(256) ortho_kernel(const DevLevel *__restrict__
 
 // AWNCC peak loop without SGM, setsm_code.cpp:7511-7702: one node per thread
 // over the quantised voxel row.
-__global__ void __launch_bounds__(256) awncc_kernel(const DevLevel *__restrict__ Pp) {
+__global__ void __launch_bounds__(256) awncc_kernel(const DevLevel *__restrict__ Pp,
+                                                    const float *__restrict__ sumcost) {
     const DevLevel &P = *Pp;
+    // with SGM (Pyramid_step <= SGM_py) the scan runs on the aggregated
+    // SumCost, keeping the window NCC of the chosen peak (max_roh)
+    const bool sgm = sumcost != nullptr;
     const int L = P.L, it = P.iteration;
     int check_ortho = !(L == 4 && it == 1);
     if (P.pre_dem_tif && !(L == 4 && it == 1)) check_ortho = 1;
@@ -185,22 +189,25 @@ __global__ void __launch_bounds__(256) awncc_kernel(const DevLevel *__restrict__
         float pre_height = 0.0f;
         int direction = 0, check_rho = 0;
         double best = -100.0, second = -100.0;
+        double max_roh = 0, pre_wncc = -1.0;
         R.result0 = q_result(-1.0);
         R.result2 = -1000;
         R.result1 = q_result(-1.0);
         R.result3 = -1000;
         R.result4 = 0;
         const vll_voxel *row = P.vox + P.vox_off[pt];
+        const float *srow = sgm ? sumcost + P.vox_off[pt] : nullptr;
         const double gncc = dq_result(R.GNCC);
         for (int64_t k = 0; k < R.NumOfHeight; ++k) {
             const float hgt = (float)__dadd_rn((double)R.minHeight, __dmul_rn((double)k, P.height_step));
             if (!(hgt >= (float)g.minHeight && hgt <= (float)g.maxHeight)) continue;
             const double incc = dq_voxel(row[k].INCC);
-            double rho;
+            double wncc;
             if (check_ortho && gncc > -1.0)
-                rho = __dadd_rn(__dmul_rn(incc, P.alpha), __dmul_rn(gncc, P.beta));
+                wncc = __dadd_rn(__dmul_rn(incc, P.alpha), __dmul_rn(gncc, P.beta));
             else
-                rho = incc;
+                wncc = incc;
+            const double rho = sgm ? (double)srow[k] : wncc;
             double diff;
             if (rho >= 0 && pre_rho >= 0)
                 diff = __dadd_rn(rho, -pre_rho);
@@ -223,6 +230,7 @@ __global__ void __launch_bounds__(256) awncc_kernel(const DevLevel *__restrict__
                         R.result2 = hgt;
                         second = -1.0;
                         R.result3 = -9999;
+                        max_roh = wncc;
                     }
                 } else if (is_peak) {
                     if (R.result4 < 10) R.result4 += 1;
@@ -231,6 +239,7 @@ __global__ void __launch_bounds__(256) awncc_kernel(const DevLevel *__restrict__
                         best = pre_rho;
                         const float t2 = R.result2;
                         R.result2 = pre_height;
+                        max_roh = pre_wncc;
                         if (second < t1) {
                             second = t1;
                             R.result3 = t2;
@@ -242,11 +251,20 @@ __global__ void __launch_bounds__(256) awncc_kernel(const DevLevel *__restrict__
                 }
             }
             pre_rho = rho;
+            pre_wncc = wncc;
             pre_height = hgt;
             direction = td;
         }
-        R.result0 = q_result(best);
-        R.result1 = q_result(second);
+        if (sgm && P.L == 0 && it >= 2) {
+            // the final iteration at level 0 keeps the window NCC of the peak
+            // (setsm_code.cpp:7683-7688)
+            R.result0 = q_result(max_roh);
+            R.result1 = q_result(-1.0);
+            R.result3 = -9999;
+        } else {
+            R.result0 = q_result(best);
+            R.result1 = q_result(second);
+        }
         P.ncc[pt] = R;
     }
 }
@@ -272,12 +290,13 @@ cudaError_t launch_ortho(const DevLevel *dP, int64_t total, double2 *const *cd, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_awncc(const DevLevel *dP, int64_t n_nodes, cudaStream_t s) {
+cudaError_t launch_awncc(const DevLevel *dP, int64_t n_nodes, const float *sumcost,
+                         cudaStream_t s) {
     const int threads = 256;
     int64_t blocks = (n_nodes + threads - 1) / threads;
     if (blocks < 1) blocks = 1;
     if (blocks > 148 * 64) blocks = 148 * 64;
-    awncc_kernel<<<(unsigned)blocks, threads, 0, s>>>(dP);
+    awncc_kernel<<<(unsigned)blocks, threads, 0, s>>>(dP, sumcost);
     return cudaGetLastError();
 }
 

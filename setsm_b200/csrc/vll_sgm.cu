@@ -1,0 +1,254 @@
+// vll_sgm.cu -- semi-global aggregation of AWNCC (setsm_code.cpp:7017-7509,
+// SGM_start_pos / SGM_con_pos :6755-6999) on the GPU.
+//
+// SumCost[node][slot] accumulates, over 8 path directions, a cost that runs
+// along every grid row, column and diagonal: at a path's first node the
+// node's INCC, at each following node its INCC plus the best of the previous
+// node's costs at the same height (and +-1 slot with penalty P1) or its
+// maximum (penalty P2), minus that maximum.  The reference's arithmetic is
+// reproduced exactly: costs are stored as float and combined in double, and
+// SumCost is a float accumulated direction by direction in the reference's
+// order (0: left->right, 1: right->left, 2: top->bottom, 3: bottom->top,
+// 4..7: the diagonals).
+//
+// GPU mapping: one launch per direction (which keeps the per-node order of
+// the float sums), one warp per path, lanes over the height slots of the
+// current node; the previous node's costs and the current ones live in two
+// shared-memory rows of the warp.  A diagonal direction's paths start from two
+// walls (a column of rows and a row of columns); the path that starts at their
+// common corner is walked by both of the reference's loops, so its nodes get
+// the same contribution twice -- here one warp walks it and adds it twice.
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "vll_device.cuh"
+#include "vll_internal.h"
+
+namespace vll {
+
+namespace {
+
+constexpr double kP1 = 0.3;   // AWNCC's P1 (setsm_code.cpp:7004)
+constexpr double kP2 = 0.6;   // AWNCC's P2 (setsm_code.cpp:7005)
+constexpr int kPHS = 1;       // P_HS_step (:7007)
+
+// Start node and step of path `line` of direction `dir` (rows/columns of the
+// reference's loops at setsm_code.cpp:7037-7499).  Returns false if `line` is
+// beyond the direction's paths.  `twice` marks the corner path of a diagonal.
+__device__ __forceinline__ bool path_of(int dir, int64_t line, int64_t W, int64_t H, int64_t &r0,
+                                        int64_t &c0, int &dr, int &dc, bool &twice) {
+    twice = false;
+    switch (dir) {
+        case 0: if (line >= H) return false; r0 = line; c0 = 0;     dr = 0;  dc = 1;  return true;
+        case 1: if (line >= H) return false; r0 = line; c0 = W - 1; dr = 0;  dc = -1; return true;
+        case 2: if (line >= W) return false; r0 = 0;     c0 = line; dr = 1;  dc = 0;  return true;
+        case 3: if (line >= W) return false; r0 = H - 1; c0 = line; dr = -1; dc = 0;  return true;
+        default: break;
+    }
+    // diagonals: lines [0, H) start on the side wall (rows), lines [H, H + W)
+    // on the top / bottom wall (columns); the corner path is the first of both
+    // loops and is walked once here, twice-counted
+    const bool top_down = dir == 4 || dir == 5;   // rows advance +1
+    const bool rightwards = dir == 4 || dir == 6; // columns advance +1
+    dr = top_down ? 1 : -1;
+    dc = rightwards ? 1 : -1;
+    const int64_t wall_row = top_down ? 0 : H - 1;     // start row of column paths
+    const int64_t wall_col = rightwards ? 0 : W - 1;   // start column of row paths
+    if (line < H) {
+        // side wall: the reference iterates its rows from start_row; the
+        // corner row is the one equal to wall_row
+        r0 = top_down ? line : H - 1 - line;
+        c0 = wall_col;
+        if (r0 == wall_row) twice = true;
+        return true;
+    }
+    const int64_t k = line - H;
+    if (k >= W) return false;
+    c0 = rightwards ? k : W - 1 - k;
+    r0 = wall_row;
+    if (c0 == wall_col) return false;   // the corner path, walked by the side-wall line
+    return true;
+}
+
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+__global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict__ Pp, int dir,
+                                                      int64_t n_lines, float *__restrict__ sumcost,
+                                                      int max_h) {
+    extern __shared__ float sm_lh[];
+    const DevLevel &P = *Pp;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *buf0 = sm_lh + (size_t)warp * 2 * max_h;
+    float *buf1 = buf0 + max_h;
+    const int64_t W = P.grid_w, Hh = P.grid_h;
+    const double step = P.height_step;
+    const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t line = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp; line < n_lines;
+         line += warps_total) {
+        int64_t r, c;
+        int dr, dc;
+        bool twice;
+        if (!path_of(dir, line, W, Hh, r, c, dr, dc, twice)) continue;
+        float *pre = buf0, *cur = buf1;
+        // ---- first node: SGM_start_pos (:6755-6767) ----
+        {
+            const int64_t pt = r * W + c;
+            const vll_nccresult R = P.ncc[pt];
+            const vll_ugrid g = P.gp3[pt];
+            const vll_voxel *vrow = P.vox + P.vox_off[pt];
+            float *sc = sumcost + P.vox_off[pt];
+            for (int h = lane; h < R.NumOfHeight; h += 32) {
+                const float hgt = (float)__dadd_rn((double)R.minHeight, __dmul_rn((double)h, step));
+                float v = 0.f;
+                if (hgt >= (float)g.minHeight && hgt <= (float)g.maxHeight) {
+                    v = (float)dq_voxel(vrow[h].INCC);
+                    float s = sc[h] + v;
+                    if (twice) s = s + v;
+                    sc[h] = s;
+                }
+                pre[h] = v;
+            }
+            __syncwarp();
+        }
+        // ---- following nodes: SGM_con_pos (:6769-6999) ----
+        for (;;) {
+            const int64_t tr = r, tc = c;   // previous node
+            r += dr;
+            c += dc;
+            if (r < 0 || r >= Hh || c < 0 || c >= W) break;
+            const int64_t pt = r * W + c, tp = tr * W + tc;
+            const vll_nccresult R = P.ncc[pt];
+            const vll_nccresult T = P.ncc[tp];
+            const vll_ugrid g = P.gp3[pt];
+            const vll_voxel *vrow = P.vox + P.vox_off[pt];
+            const vll_voxel *trow = P.vox + P.vox_off[tp];
+            float *sc = sumcost + P.vox_off[pt];
+            const float max_w = (float)dq_result(T.max_WNCC);
+            const int tn = T.NumOfHeight;
+            for (int h = lane; h < R.NumOfHeight; h += 32) {
+                const float hgt = (float)__dadd_rn((double)R.minHeight, __dmul_rn((double)h, step));
+                float out = 0.f;
+                if (hgt >= (float)g.minHeight && hgt <= (float)g.maxHeight) {
+                    const double wncc = dq_voxel(vrow[h].INCC);
+                    // (float iter_height - short minHeight) is a float subtraction in
+                    // the reference, then divided by the double step
+                    const int i0 = (int)__ddiv_rn((double)__fsub_rn(hgt, (float)T.minHeight), step);
+                    const int i1 = i0 - kPHS, i2 = i0 + kPHS;
+                    double V1 = 0, V2 = 0, V3 = 0;
+                    const double V4 = __dadd_rn((double)max_w, -kP2);
+                    double m;
+                    if (i0 == 0 && i2 >= 0 && i2 < tn) {
+                        const bool f = trow[i0].flag_cal, f2 = trow[i2].flag_cal;
+                        if (f && f2) {
+                            V2 = __dadd_rn((double)pre[i2], -kP1);
+                            V3 = (double)pre[i0];
+                            m = dmax(dmax(V2, V3), V4);
+                        } else if (f) {
+                            V3 = (double)pre[i0];
+                            m = dmax(V3, V4);
+                        } else if (f2) {
+                            V2 = __dadd_rn((double)pre[i2], -kP1);
+                            m = dmax(V2, V4);
+                        } else {
+                            m = V4;
+                        }
+                    } else if (i0 == tn - 1 && i1 >= 0 && i1 < tn) {
+                        const bool f = trow[i0].flag_cal, f1 = trow[i1].flag_cal;
+                        if (f && f1) {
+                            V1 = __dadd_rn((double)pre[i1], -kP1);
+                            V3 = (double)pre[i0];
+                            m = dmax(dmax(V1, V3), V4);
+                        } else if (f) {
+                            V3 = (double)pre[i0];
+                            m = dmax(V3, V4);
+                        } else if (f1) {
+                            V1 = __dadd_rn((double)pre[i1], -kP1);
+                            m = dmax(V1, V4);
+                        } else {
+                            m = V4;
+                        }
+                    } else if (i0 > 0 && i0 < tn - 1 && i1 >= 0 && i1 < tn && i2 >= 0 && i2 < tn) {
+                        const bool f = trow[i0].flag_cal, f1 = trow[i1].flag_cal,
+                                   f2 = trow[i2].flag_cal;
+                        if (f && f1 && f2) {
+                            V1 = __dadd_rn((double)pre[i1], -kP1);
+                            V2 = __dadd_rn((double)pre[i2], -kP1);
+                            V3 = (double)pre[i0];
+                            m = dmax(dmax(dmax(V1, V2), V3), V4);
+                        } else if (f && f1) {
+                            V1 = __dadd_rn((double)pre[i1], -kP1);
+                            V3 = (double)pre[i0];
+                            m = dmax(dmax(V1, V3), V4);
+                        } else if (f1 && f2) {
+                            // V3 keeps its initial 0 and takes part (setsm_code.cpp:6917-6925)
+                            V1 = __dadd_rn((double)pre[i1], -kP1);
+                            V2 = __dadd_rn((double)pre[i2], -kP1);
+                            m = dmax(dmax(dmax(V1, V2), V3), V4);
+                        } else if (f && f2) {
+                            V2 = __dadd_rn((double)pre[i2], -kP1);
+                            V3 = (double)pre[i0];
+                            m = dmax(dmax(V2, V3), V4);
+                        } else if (f) {
+                            V3 = (double)pre[i0];
+                            m = dmax(V3, V4);
+                        } else if (f1) {
+                            V1 = __dadd_rn((double)pre[i1], -kP1);
+                            m = dmax(V1, V4);
+                        } else if (f2) {
+                            V2 = __dadd_rn((double)pre[i2], -kP1);
+                            m = dmax(V2, V4);
+                        } else {
+                            m = V4;
+                        }
+                    } else {
+                        m = V4;
+                    }
+                    const double t = __dadd_rn(m, -(double)max_w);
+                    out = (float)__dadd_rn(wncc, t);
+                    float s = sc[h] + out;
+                    if (twice) s = s + out;
+                    sc[h] = s;
+                }
+                cur[h] = out;
+            }
+            __syncwarp();
+            float *tmp = pre;
+            pre = cur;
+            cur = tmp;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+
+// All 8 directions of the aggregation into sumcost (float, the packed voxel
+// layout, zeroed here), one launch per direction in the reference's order.
+// max_h: the largest NumOfHeight of the level.
+cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int max_h,
+                       float *sumcost, int64_t n_slots, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(sumcost, 0, (size_t)(n_slots > 0 ? n_slots : 1) * 4, s);
+    if (e != cudaSuccess) return e;
+    if (max_h < 1) max_h = 1;
+    const size_t per_warp = (size_t)2 * max_h * sizeof(float);
+    if (per_warp > 200 * 1024) return cudaErrorInvalidValue;
+    int warps = (int)std::min<size_t>(4, (200 * 1024) / per_warp);
+    if (warps < 1) warps = 1;
+    const size_t smem = per_warp * warps;
+    e = cudaFuncSetAttribute(sgm_dir_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    for (int dir = 0; dir < 8; ++dir) {
+        const int64_t n_lines = dir < 2 ? grid_h : (dir < 4 ? grid_w : grid_h + grid_w);
+        int64_t blocks = (n_lines + warps - 1) / warps;
+        if (blocks > 148 * 64) blocks = 148 * 64;
+        if (blocks < 1) blocks = 1;
+        sgm_dir_kernel<<<(unsigned)blocks, warps * 32, smem, s>>>(dP, dir, n_lines, sumcost, max_h);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace vll

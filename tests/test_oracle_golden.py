@@ -51,3 +51,19 @@ def test_golden_set_covers_the_routes():
                     kw.get("L", 0) > 0, kw.get("template", 11)))
     assert ("memory-tight", False, 11) in routes and ("memory-tight", False, 15) in routes
     assert ("voxel", False, 11) in routes and ("voxel", True, 15) in routes
+
+
+@pytest.mark.skipif(not __import__("oracle.refpy").refpy.available(),
+                    reason="reference build not available")
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_SGM))
+def test_sgm_fixtures_are_the_reference_output(name):
+    """The SGM fixtures (checked by tests/test_gpu_sgm.py) are what the
+    reference build produces on the regenerated inputs."""
+    from oracle import refpy
+    inp = cases.make_case(**mg.GOLDEN_SGM[name])
+    g = load_fixture(name)
+    assert mg.input_digest(inp) == g["digest"]
+    r = cases.run_cpu(refpy, inp, inp.iters)
+    assert r["acc"] == g["acc"]
+    for k in ("init_ncc", "vll_ncc", "ncc", "vll_vox"):
+        assert cases.field_mismatch(r[k], g[k]) == {}, k
