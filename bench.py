@@ -569,6 +569,74 @@ def run_multi(args):
 
 
 # ---------------------------------------------------------------------------
+# SGM aggregation (AWNCC with Pyramid_step <= SGM_py)
+# ---------------------------------------------------------------------------
+def run_sgm(args):
+    """AWNCC with semi-global aggregation on the voxel route at level 0
+    (SGM_py = 1): the reduced C2 scene (4096^2 pair, 1024^2 grid, TIN ranges),
+    InitializeVoxel by the reference on the host (it stays the caller's in
+    SETSM), VerticalLineLocus (split) and AWNCC on the GPU, against the
+    reference's AWNCC with OpenMP on every host core; every NCCresult field is
+    compared.  Metric: voxel slots aggregated per second."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import torch
+    from oracle import refpy
+    from setsm_b200 import vll, workloads
+    from tests.cases import field_mismatch
+    ctx = vll.Context(0)
+    wl = workloads.build("c2_small", ctx, device="cuda:0", seed=1)
+    inp = wl.host_inputs(11)
+    inp.check_matching_rate = False
+    inp.sgm_py = 1
+    refpy.set_threads(os.cpu_count() or 1)
+    ncc0 = inp.new_nccresult()
+    gp3 = inp.gridpt3.copy()
+    inp.gridpt3 = gp3
+    vox0 = refpy.initialize_voxel(inp, ncc0, None)
+    ncc = ncc0.copy()
+    vox = vox0.copy()
+    ctx.vertical_line_locus(inp, ncc, vox, "split")
+    ncc_v, vox_v = ncc.copy(), vox.copy()
+    times = []
+    for _ in range(max(1, args.warmup)):
+        n1 = ncc_v.copy()
+        ctx.awncc(inp, n1, vox_v)
+    for _ in range(args.steps):
+        n1 = ncc_v.copy()
+        t = time.perf_counter()
+        st = ctx.awncc(inp, n1, vox_v)
+        times.append((st.kernel_ms, (time.perf_counter() - t) * 1e3))
+    slots = int(vox_v.size)
+    dev_ms = statistics.median(t[0] for t in times)
+    e2e_ms = statistics.median(t[1] for t in times)
+    n_ref = ncc_v.copy()
+    t = time.perf_counter()
+    refpy.awncc(inp, n_ref, vox_v.copy())
+    cpu_s = time.perf_counter() - t
+    mism = field_mismatch(n1, n_ref)
+    line = {
+        "metric": "voxel slots aggregated/s (AWNCC with SGM)", "value": slots / (dev_ms / 1e3),
+        "unit": "slots/s", "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup),
+        "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 path costs, f64 arithmetic (the reference's)", "data": "synthetic",
+        "config": {"workload": "SGM: reduced C2 scene (4096^2 pair, 1024^2 grid, TIN ranges "
+                               "K 8-512 at 0.5 m), voxel route, level 0, 7x7, SGM_py = 1",
+                   "nodes": int(wl.n_nodes), "slots": slots},
+        "e2e": {"value": slots / (e2e_ms / 1e3), "unit": "slots/s",
+                "timing": "host wall clock of vll_awncc_peaks (uploads voxels, downloads "
+                          "NCCresult)"},
+        "cpu_baseline": {"value": slots / cpu_s, "unit": "slots/s", "cores": os.cpu_count(),
+                         "kind": "reference", "sample": f"whole grid, {cpu_s:.2f} s"},
+        "parity_mismatch_fields": mism,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    del torch
+
+
+# ---------------------------------------------------------------------------
 # C5 serving
 # ---------------------------------------------------------------------------
 def run_c5(args):
@@ -642,7 +710,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
-                    choices=["c1", "c2", "c2_small", "c3", "c4", "c5"])
+                    choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -667,6 +735,8 @@ def main():
         run_multi(args)
     elif args.config == "c5":
         run_c5(args)
+    elif args.config == "sgm":
+        run_sgm(args)
     else:
         run_ours(args)
 

@@ -178,7 +178,8 @@ class Context:
         return out[:off[-1]], off
 
     def awncc(self, inputs, nccresult: np.ndarray, voxels: np.ndarray) -> abi.Stats:
-        """Non-SGM peak loop of AWNCC over the packed voxel rows."""
+        """AWNCC over the packed voxel rows (setsm_code.cpp:7001-7702): the
+        semi-global aggregation when Pyramid_step <= SGM_py, then the peak loop."""
         d = inputs.desc()
         st = abi.Stats()
         vptr = voxels.ctypes.data if voxels.size else None
@@ -307,5 +308,6 @@ def VerticalLineLocus(inputs, nccresult: np.ndarray, voxels: np.ndarray | None =
 
 
 def AWNCC(inputs, nccresult: np.ndarray, voxels: np.ndarray) -> None:
-    """AWNCC's peak selection without SGM (setsm_code.cpp:7511-7702)."""
+    """AWNCC (setsm_code.cpp:7001-7702): SGM aggregation when the level asks
+    for it, then the first / second peak selection."""
     default_context().awncc(inputs, nccresult, voxels)
