@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define VLL_ABI_VERSION 2
+#define VLL_ABI_VERSION 3
 #define VLL_MAX_IMAGES 8
 
 /* ---- status codes ------------------------------------------------------ */
@@ -126,6 +126,13 @@ typedef struct vll_image_desc {
     double image_adjust[2];      /* ImageAdjust[ti] {deltaLine, deltaSamp} */
     int32_t selected;            /* proinfo->check_selected_image[ti]      */
     int32_t _pad;
+    /* The blunder-selected pyramid level (LevelInfo.blunder_selected_level,
+     * setsm_code.cpp:3560-3565), read by VerticalLineLocus_blunder and by
+     * VerticalLineLocus_seeddem with check_Matchtag; NULL = the matched level. */
+    const uint16_t *image_b;     /* py_BImages[ti]                         */
+    const uint16_t *mag_b;       /* py_BMagImages[ti]                      */
+    uint32_t width_b, height_b;  /* py_Sizes[ti][blunder_selected_level]   */
+    double startpos_b[2];        /* py_BStartpos[ti]                       */
 } vll_image_desc;
 
 typedef struct vll_level_desc {
@@ -154,6 +161,9 @@ typedef struct vll_level_desc {
     const double *grid_wgs;      /* Grid_wgs [N][2] lon, lat degrees       */
     vll_transparam param;        /* *plevelinfo.param                      */
     vll_image_desc images[VLL_MAX_IMAGES];
+    int32_t blunder_level;       /* *plevelinfo.blunder_selected_level (used
+                                    when images[].image_b is set)           */
+    int32_t _pad2;
 } vll_level_desc;
 
 /* Per-call statistics (filled when a vll_stats pointer is passed; the call
@@ -330,6 +340,49 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc,
                     const vll_ugrid *gridpt3, vll_nccresult *nccresult,
                     const vll_voxel *voxels, int64_t voxel_capacity,
                     vll_stats *stats);
+
+/* ---- orthoimage-window variants (setsm_code.cpp:7720-8026) ------------- */
+/*
+ * VerticalLineLocus_seeddem (setsm_code.cpp:7720-7880): the orthoimage NCC of
+ * every grid node against each selected image at the node's height; where it
+ * is below 0.3 the node's height range is widened by 100 m (clamped to
+ * desc->minmax_height) and voided (-9999) below 0.1; ortho_ncc[ti] (and roh
+ * with check_Matchtag, which samples the blunder level's images) are set.
+ * Template size and window follow the reference (5 m template area, radius
+ * Half+1).  gridpt3 is updated in place; bit-exact with the reference.
+ * The _device forms take device pointers in the descriptor and gridpt3 and
+ * are asynchronous on the context's stream (they wait only when `stats` is
+ * given); the host forms copy in and out and wait.
+ */
+int vll_vertical_line_locus_seeddem(vll_context *ctx, const vll_level_desc *desc,
+                                    vll_ugrid *gridpt3, vll_stats *stats);
+int vll_vertical_line_locus_seeddem_device(vll_context *ctx, const vll_level_desc *desc,
+                                           vll_ugrid *d_gridpt3, vll_stats *stats);
+/*
+ * VerticalLineLocus_blunder (setsm_code.cpp:7882-8026): the same orthoimage
+ * NCC at the blunder-selected level (images[].image_b, desc->blunder_level;
+ * radius Half-1, Half from iteration and bblunder as the reference), written
+ * to ortho_ncc[ti], Mean_ortho_ncc (the maximum over images) and
+ * nccresult[node] (float).  Returns VLL_OK where the reference returns true.
+ * The UGRID fields are bit-exact; the float NCC equals the reference's but
+ * for rare last-bit differences of the map projection's libm calls (about
+ * one node in a thousand, by ~1e-10).
+ */
+int vll_vertical_line_locus_blunder(vll_context *ctx, const vll_level_desc *desc,
+                                    vll_ugrid *gridpt3, int iteration, int bblunder,
+                                    float *nccresult, vll_stats *stats);
+int vll_vertical_line_locus_blunder_device(vll_context *ctx, const vll_level_desc *desc,
+                                           vll_ugrid *d_gridpt3, int iteration, int bblunder,
+                                           float *d_nccresult, vll_stats *stats);
+
+/* Diagnostics: the orthoimage coordinate raster of image `ti`
+ * (SetOrthoImageCoord, setsm_code.cpp:6550-6670) at resolution im_res, on
+ * the matched level's pyramid (use_b = 0) or the blunder level's (1), as
+ * {x, y} doubles row-major into out[2 * capacity]; *width / *height receive
+ * the raster size. */
+int vll_debug_ortho_raster(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
+                           int use_b, double im_res, int ti, double *out, int64_t capacity,
+                           int64_t *width, int64_t *height);
 
 /* ---- image preprocessing (SubFunctions.cpp:2418-2560, Template.hpp:82) -- */
 /* Sobel magnitude (uint16) and 20-degree direction bin per pixel, on host

@@ -204,6 +204,15 @@ int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
                       tagNCCresult *nccresult, taglevelinfo &plevelinfo, const UpdateGrid *GridPT3,
                       const unsigned char iteration, const double *minmaxHeight);
 
+// The orthoimage-window variants (setsm_code.hpp:93, :95), same behaviour:
+// VerticalLineLocus_seeddem updates GridPT3; VerticalLineLocus_blunder
+// writes GridPT3's ortho NCC and nccresult[node], and returns true.
+void VerticalLineLocus_seeddem(const ProjectInfo *proinfo, taglevelinfo &plevelinfo,
+                               UpdateGrid *GridPT3, const double *minmaxHeight);
+bool VerticalLineLocus_blunder(const ProjectInfo *proinfo, taglevelinfo &plevelinfo,
+                               float *nccresult, UpdateGrid *GridPT3, unsigned char iteration,
+                               bool bblunder);
+
 extern "C" {
 // Byte offsets of the fields the drop-in reads, in a fixed order (used by the
 // layout test); returns the number of entries written.

@@ -41,6 +41,9 @@ struct RefLevel {
     const uint16 *imgs_next[VLL_MAX_IMAGES];
     const uint16 *mags_next[VLL_MAX_IMAGES];
     const uint8 *oris_next[VLL_MAX_IMAGES];
+    const uint16 *imgs_b[VLL_MAX_IMAGES];
+    const uint16 *mags_b[VLL_MAX_IMAGES];
+    D2DPOINT startpos_b[VLL_MAX_IMAGES];
     D2DPOINT startpos[VLL_MAX_IMAGES];
     D2DPOINT startpos_next[VLL_MAX_IMAGES];
     CSize sizes_store[VLL_MAX_IMAGES][16];
@@ -75,7 +78,7 @@ struct RefLevel {
             proinfo->check_selected_image[ti] = d->images[ti].selected != 0;
 
         pyramid_step = d->pyramid_step;
-        blunder_level = d->pyramid_step;
+        blunder_level = d->images[0].image_b ? d->blunder_level : d->pyramid_step;
         template_size = (unsigned char)d->template_size;
         iteration = (unsigned char)d->iteration;
         bin_angle = d->bin_angle;
@@ -109,6 +112,16 @@ struct RefLevel {
             sizes_store[ti][pyramid_step] = CSize((int)im.width, (int)im.height);
             if (pyramid_step >= 1)
                 sizes_store[ti][pyramid_step - 1] = CSize((int)im.width_next, (int)im.height_next);
+            if (im.image_b) {
+                imgs_b[ti] = im.image_b;
+                mags_b[ti] = im.mag_b;
+                startpos_b[ti] = D2DPOINT(im.startpos_b[0], im.startpos_b[1]);
+                sizes_store[ti][blunder_level] = CSize((int)im.width_b, (int)im.height_b);
+            } else {
+                imgs_b[ti] = im.image;
+                mags_b[ti] = im.mag;
+                startpos_b[ti] = startpos[ti];
+            }
             sizes[ti] = sizes_store[ti];
             rpc_rows[ti][0] = im.rpc + 0;
             rpc_rows[ti][1] = im.rpc + 5;
@@ -125,13 +138,13 @@ struct RefLevel {
         li.py_Images = imgs;
         li.py_OriImages = oris;
         li.py_MagImages = mags;
-        li.py_BImages = imgs;
-        li.py_BMagImages = mags;
+        li.py_BImages = imgs_b;
+        li.py_BMagImages = mags_b;
         li.py_Images_next = imgs_next;
         li.py_OriImages_next = oris_next;
         li.py_MagImages_next = mags_next;
         li.py_Startpos = startpos;
-        li.py_BStartpos = startpos;
+        li.py_BStartpos = startpos_b;
         li.py_Startpos_next = startpos_next;
         li.RPCs = rpcs;
         li.Boundary = d->boundary;
@@ -320,6 +333,22 @@ double ref_get_height_step(int pyramid_step, double im_resolution) {
     return GetHeightStep(pyramid_step, im_resolution);
 }
 
+/* VerticalLineLocus_seeddem (setsm_code.cpp:7720-7880): GridPT3 in/out. */
+void ref_vll_seeddem(const vll_level_desc *d, vll_ugrid *gridpt3) {
+    RefLevel L(d);
+    VerticalLineLocus_seeddem(L.proinfo, L.li, reinterpret_cast<UGRID *>(gridpt3),
+                              d->minmax_height);
+}
+
+/* VerticalLineLocus_blunder (setsm_code.cpp:7882-8026): GridPT3 in/out, the
+ * per-node ortho NCC into ncc_out. */
+void ref_vll_blunder(const vll_level_desc *d, vll_ugrid *gridpt3, int iteration, int bblunder,
+                     float *ncc_out) {
+    RefLevel L(d);
+    VerticalLineLocus_blunder(L.proinfo, L.li, ncc_out, reinterpret_cast<UGRID *>(gridpt3),
+                              (uint8)iteration, bblunder != 0);
+}
+
 /* Known-answer hooks: the reference's own building blocks.
  * Correlate, SubFunctions.cpp:974-1018. */
 double ref_correlate(const double *L, const double *R, int N) { return Correlate(L, R, N); }
@@ -365,6 +394,42 @@ long ref_call_vertical_line_locus(void *fn, const vll_level_desc *d, const vll_u
     return acc;
 }
 
+/* SetOrthoImageCoord (setsm_code.cpp:6550-6670): the orthoimage coordinate
+ * raster of image ti at im_res, OR (use_b = 0) or BD pyramid. */
+long ref_ortho_raster(const vll_level_desc *d, const vll_ugrid *gridpt3, int use_b, double im_res,
+                      int ti, double *out, long cap) {
+    RefLevel L(d);
+    D2DPOINT **cd = (D2DPOINT **)calloc((size_t)d->num_images, sizeof(D2DPOINT *));
+    long w = 0, h = 0, wn = 0, hn = 0;
+    SetOrthoImageCoord(L.proinfo, L.li, reinterpret_cast<const UGRID *>(gridpt3), false,
+                       use_b ? BD : OR, im_res, 0, w, h, wn, hn, cd, nullptr);
+    const long n = w * h;
+    if (n <= cap && cd[ti]) memcpy(out, cd[ti], (size_t)n * sizeof(D2DPOINT));
+    for (int i = 0; i < d->num_images; ++i) free(cd[i]);
+    free(cd);
+    return n <= cap ? n : -n;
+}
+
+/* The same structures handed to a function with the signature of
+ * VerticalLineLocus_seeddem (setsm_code.hpp:93) / VerticalLineLocus_blunder
+ * (:95) at `fn` (the library's C++ drop-ins). */
+typedef void (*seeddem_signature)(const ProInfo *, LevelInfo &, UGRID *, const double *);
+typedef bool (*blunder_signature)(const ProInfo *, LevelInfo &, float *, UGRID *, uint8, bool);
+void ref_call_vll_seeddem(void *fn, const vll_level_desc *d, vll_ugrid *gridpt3) {
+    RefLevel L(d);
+    reinterpret_cast<seeddem_signature>(fn)(L.proinfo, L.li, reinterpret_cast<UGRID *>(gridpt3),
+                                            d->minmax_height);
+}
+int ref_call_vll_blunder(void *fn, const vll_level_desc *d, vll_ugrid *gridpt3, int iteration,
+                         int bblunder, float *ncc_out) {
+    RefLevel L(d);
+    return reinterpret_cast<blunder_signature>(fn)(L.proinfo, L.li, ncc_out,
+                                                   reinterpret_cast<UGRID *>(gridpt3),
+                                                   (uint8)iteration, bblunder != 0)
+               ? 1
+               : 0;
+}
+
 /* Byte offsets of the fields the drop-in reads, in the order of the
  * library's vll_compat_layout(), taken from the reference's own headers. */
 int ref_layout(int64_t *out, int cap) {
@@ -404,6 +469,11 @@ int ref_layout(int64_t *out, int cap) {
         (int64_t)offsetof(LevelInfo, grid_resolution),
         (int64_t)offsetof(LevelInfo, Py_combined_level),
         (int64_t)offsetof(LevelInfo, check_matching_rate),
+        (int64_t)offsetof(LevelInfo, py_BImages),
+        (int64_t)offsetof(LevelInfo, py_BMagImages),
+        (int64_t)offsetof(LevelInfo, py_BStartpos),
+        (int64_t)offsetof(LevelInfo, blunder_selected_level),
+        (int64_t)offsetof(LevelInfo, iteration),
         (int64_t)sizeof(NCCresult),
         (int64_t)sizeof(UGRID),
         (int64_t)offsetof(UGRID, ortho_ncc),

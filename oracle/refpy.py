@@ -253,3 +253,56 @@ def layout() -> list:
     out = np.zeros(128, dtype=np.int64)
     n = L.ref_layout(out.ctypes.data, out.size)
     return out[:n].tolist()
+
+
+def vll_seeddem(inputs) -> None:
+    """VerticalLineLocus_seeddem (setsm_code.cpp:7720-7880); updates
+    inputs.gridpt3 in place."""
+    L = lib()
+    L.ref_vll_seeddem.argtypes = [C.POINTER(abi.LevelDesc), C.c_void_p]
+    L.ref_vll_seeddem.restype = None
+    d = inputs.desc()
+    with _StdoutToStderr():
+        L.ref_vll_seeddem(C.byref(d), inputs.gridpt3.ctypes.data)
+
+
+def vll_blunder(inputs, iteration: int, bblunder: bool) -> np.ndarray:
+    """VerticalLineLocus_blunder (setsm_code.cpp:7882-8026); updates
+    inputs.gridpt3 in place and returns the per-node ortho NCC."""
+    L = lib()
+    L.ref_vll_blunder.argtypes = [C.POINTER(abi.LevelDesc), C.c_void_p, C.c_int, C.c_int,
+                                  C.c_void_p]
+    L.ref_vll_blunder.restype = None
+    d = inputs.desc()
+    out = np.zeros(inputs.n, dtype=np.float32)
+    with _StdoutToStderr():
+        L.ref_vll_blunder(C.byref(d), inputs.gridpt3.ctypes.data, int(iteration), int(bblunder),
+                          out.ctypes.data)
+    return out
+
+
+def call_vll_seeddem(fn_addr: int, inputs) -> None:
+    """Calls the function at `fn_addr` (VerticalLineLocus_seeddem's C++
+    signature, setsm_code.hpp:93) with the reference's structures."""
+    L = lib()
+    L.ref_call_vll_seeddem.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_void_p]
+    L.ref_call_vll_seeddem.restype = None
+    d = inputs.desc()
+    with _StdoutToStderr():
+        L.ref_call_vll_seeddem(fn_addr, C.byref(d), inputs.gridpt3.ctypes.data)
+
+
+def call_vll_blunder(fn_addr: int, inputs, iteration: int, bblunder: bool) -> np.ndarray:
+    """Calls the function at `fn_addr` (VerticalLineLocus_blunder's C++
+    signature, setsm_code.hpp:95) with the reference's structures."""
+    L = lib()
+    L.ref_call_vll_blunder.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_void_p, C.c_int,
+                                       C.c_int, C.c_void_p]
+    L.ref_call_vll_blunder.restype = C.c_int
+    d = inputs.desc()
+    out = np.zeros(inputs.n, dtype=np.float32)
+    with _StdoutToStderr():
+        ok = L.ref_call_vll_blunder(fn_addr, C.byref(d), inputs.gridpt3.ctypes.data,
+                                    int(iteration), int(bblunder), out.ctypes.data)
+    assert ok == 1
+    return out

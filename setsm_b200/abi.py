@@ -11,7 +11,7 @@ import ctypes as C
 
 import numpy as np
 
-VLL_ABI_VERSION = 2
+VLL_ABI_VERSION = 3
 VLL_MAX_IMAGES = 8
 
 VLL_OK = 0
@@ -84,6 +84,9 @@ class ImageDesc(C.Structure):
         ("rpc", C.c_double * 90),
         ("image_adjust", C.c_double * 2),
         ("selected", C.c_int32), ("_pad", C.c_int32),
+        ("image_b", C.c_void_p), ("mag_b", C.c_void_p),
+        ("width_b", C.c_uint32), ("height_b", C.c_uint32),
+        ("startpos_b", C.c_double * 2),
     ]
 
 
@@ -104,6 +107,7 @@ class LevelDesc(C.Structure):
         ("grid_pts", C.c_void_p), ("grid_wgs", C.c_void_p),
         ("param", TransParam),
         ("images", ImageDesc * VLL_MAX_IMAGES),
+        ("blunder_level", C.c_int32), ("_pad2", C.c_int32),
     ]
 
 

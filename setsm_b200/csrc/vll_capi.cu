@@ -117,7 +117,7 @@ namespace vll {
 
 // Derives the per-call constants of VerticalLineLocus (setsm_code.cpp:6050-6137)
 // from the descriptor.  Image / grid pointers are copied as given.
-int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err) {
+int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err, bool vll_window) {
     memset(P, 0, sizeof(*P));
     if (!d) {
         *err = "null level descriptor";
@@ -153,7 +153,7 @@ int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err) {
         H = H - 1;
     else if (L < 3)
         H = H - 2;
-    if (H < 1 || H > kMaxHalf) {
+    if (vll_window && (H < 1 || H > kMaxHalf)) {
         *err = "window half-size out of the supported range [1, 8]";
         return VLL_ERR_UNSUPPORTED;
     }
@@ -167,6 +167,7 @@ int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err) {
     P->check_matchtag = d->check_matchtag != 0;
     P->pre_dem_tif = d->pre_dem_tif != 0;
     P->sgm_py = d->sgm_py;
+    P->blunder_level = d->images[0].image_b ? d->blunder_level : L;
     P->combined = !P->is_ra && (L > d->py_combined_level);
     P->combined_incc = P->combined && (L >= 1 && d->iteration % 2 == 0);
     P->im_res_next = d->resolution;
@@ -230,6 +231,21 @@ int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err) {
         m.adj[0] = s.image_adjust[0];
         m.adj[1] = s.image_adjust[1];
         m.selected = s.selected != 0;
+        if (s.image_b) {
+            m.img_b = s.image_b;
+            m.mag_b = s.mag_b;
+            m.wb = s.width_b;
+            m.hb = s.height_b;
+            m.sxb = s.startpos_b[0];
+            m.syb = s.startpos_b[1];
+        } else {
+            m.img_b = s.image;
+            m.mag_b = s.mag;
+            m.wb = s.width;
+            m.hb = s.height;
+            m.sxb = s.startpos[0];
+            m.syb = s.startpos[1];
+        }
         if (m.selected && (s.width < 2 || s.height < 2)) {
             *err = "selected image with size < 2";
             return VLL_ERR_INVALID;
@@ -523,6 +539,140 @@ int finish_set(vll_context *ctx, SetResources &r, const vll::SplitBuffers &b, in
 int upload(vll_context *ctx, Buf &b, const void *src, size_t n) {
     VLL_CUDA(ctx, ensure(b, n));
     if (n) VLL_CUDA(ctx, cudaMemcpyAsync(b.p, src, n, cudaMemcpyHostToDevice, ctx->stream));
+    return VLL_OK;
+}
+
+// Template half-size of VerticalLineLocus_seeddem (setsm_code.cpp:7722-7729):
+// the 5 m template area at the matched level, at every level.
+int seeddem_half(const vll_level_desc *d) {
+    int T = d->template_size;
+    const int t = (int)((5.0 / (d->resolution * (double)(1 << d->pyramid_step))) / 2.0) * 2 + 1;
+    if (T < t) T = t;
+    return (int)(T / 2.0);
+}
+
+// Template half-size of VerticalLineLocus_blunder (setsm_code.cpp:7884-7910):
+// the template is a uint8 there, enlarged for the blunder level's GSD.
+int blunder_half(const vll_level_desc *d, int iteration, bool bblunder, int blevel) {
+    uint8_t T = (uint8_t)d->template_size;
+    const int t = (int)((5.0 / (d->resolution * (double)(1 << blevel))) / 2.0) * 2 + 1;
+    if (T < t) T = (uint8_t)t;
+    int H = (int)(T / 2.0);
+    if (bblunder) {
+        const uint8_t it = (uint8_t)iteration;
+        if (d->pyramid_step == 4) {
+            H = T - it * 2;
+            if (H < (int)(T / 2.0)) H = (int)(T / 2.0);
+        } else if (d->pyramid_step == 3) {
+            H = T - 2 - it * 2;
+            if (H < (int)(T / 2.0)) H = (int)(T / 2.0);
+        }
+    }
+    return H;
+}
+
+// Uploads the selected images' intensity and magnitude planes the variant
+// samples (the matched level's, or the blunder level's when use_b).
+int upload_ortho_images(vll_context *ctx, const vll_level_desc *desc, DevLevel &P, bool use_b) {
+    int rc;
+    for (int ti = 0; ti < P.num_images; ++ti) {
+        const vll_image_desc &s = desc->images[ti];
+        if (!s.selected) continue;
+        vll::DevImage &m = P.im[ti];
+        const uint16_t *img = use_b ? m.img_b : m.img, *mag = use_b ? m.mag_b : m.mag;
+        const size_t n = use_b ? (size_t)m.wb * m.hb : (size_t)m.w * m.h;
+        if (!img || !mag) return fail(ctx, VLL_ERR_INVALID, "null image plane");
+        if ((rc = upload(ctx, ctx->img[ti][0], img, n * 2))) return rc;
+        if ((rc = upload(ctx, ctx->img[ti][1], mag, n * 2))) return rc;
+        if (use_b) {
+            m.img_b = (const uint16_t *)ctx->img[ti][0].p;
+            m.mag_b = (const uint16_t *)ctx->img[ti][1].p;
+        } else {
+            m.img = (const uint16_t *)ctx->img[ti][0].p;
+            m.mag = (const uint16_t *)ctx->img[ti][1].p;
+        }
+    }
+    return VLL_OK;
+}
+
+// The orthoimage variants on device data: rasterise the orthoimage
+// coordinates (SetOrthoImageCoord, OR or BD pyramid) and run the per-node
+// pass; d_ncc selects the blunder pass.  gp3 is updated in place.
+int run_ortho_variant(vll_context *ctx, DevLevel &P, vll_ugrid *d_gp3, int H, double im_res,
+                      bool use_b, float *d_ncc, vll_stats *stats) {
+    if (use_b && P.blunder_level < 0) return fail(ctx, VLL_ERR_INVALID, "negative blunder level");
+    if (use_b && P.blunder_level > 12) return fail(ctx, VLL_ERR_INVALID, "blunder level above 12");
+    for (int ti = 0; ti < P.num_images; ++ti) {
+        const vll::DevImage &m = P.im[ti];
+        if (m.selected && use_b && (m.wb < 2 || m.hb < 2))
+            return fail(ctx, VLL_ERR_INVALID, "selected blunder-level image with size < 2");
+    }
+    const int64_t ow = (int64_t)((P.boundary[2] - P.boundary[0]) / im_res) + 1;
+    const int64_t oh = (int64_t)((P.boundary[3] - P.boundary[1]) / im_res) + 1;
+    if (ow <= 0 || oh <= 0) return fail(ctx, VLL_ERR_INVALID, "empty orthoimage boundary");
+    const size_t total = (size_t)(ow * oh);
+    double2 *ptrs[2 * VLL_MAX_IMAGES] = {};
+    for (int ti = 0; ti < P.num_images; ++ti) {
+        if (!P.im[ti].selected) continue;
+        VLL_CUDA(ctx, ensure(ctx->ocd[ti], total * sizeof(double2)));
+        VLL_CUDA(ctx, cudaMemsetAsync(ctx->ocd[ti].p, 0, total * sizeof(double2), ctx->stream));
+        ptrs[ti] = (double2 *)ctx->ocd[ti].p;
+    }
+    P.gp3 = d_gp3;
+    int rc = upload_level_block(ctx, P);
+    if (rc) return rc;
+    VLL_CUDA(ctx, ensure(ctx->ocdptr, sizeof(ptrs)));
+    VLL_CUDA(ctx, cudaMemcpyAsync(ctx->ocdptr.p, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    const DevLevel *dP = (const DevLevel *)ctx->level.p;
+    double2 *const *dptr = (double2 *const *)ctx->ocdptr.p;
+    if (!ctx->e0) {
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e0));
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e1));
+    }
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e0, ctx->stream));
+    VLL_CUDA(ctx, vll::launch_ortho_raster(dP, dptr, ow, oh, im_res, use_b ? 1 : 0, ctx->stream));
+    if (d_ncc)
+        VLL_CUDA(ctx, vll::launch_blunder(dP, P.n_nodes, dptr, ow, oh, im_res, H, d_gp3, d_ncc,
+                                          ctx->stream));
+    else
+        VLL_CUDA(ctx, vll::launch_seeddem(dP, P.n_nodes, dptr, ow, oh, im_res, H, use_b ? 1 : 0,
+                                          d_gp3, ctx->stream));
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
+    ctx->launches_total += 2;
+    if (stats) {
+        VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->e0, ctx->e1);
+        memset(stats, 0, sizeof(*stats));
+        stats->kernel_ms = ms;
+    }
+    return VLL_OK;
+}
+
+// Shared front of the four variant entry points: descriptor checks and the
+// window / raster constants.  blunder: H from blunder_half, raster at the
+// blunder level; seeddem: H from seeddem_half, raster at the matched level
+// (sampling the blunder level's images with check_Matchtag).
+int prepare_variant(vll_context *ctx, const vll_level_desc *desc, bool blunder, int iteration,
+                    int bblunder, DevLevel &P, int &H, double &im_res, bool &use_b) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc) return fail(ctx, VLL_ERR_INVALID, "null descriptor");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err, false);
+    if (rc) return fail(ctx, rc, err);
+    if (!blunder && desc->pyramid_step > 12)
+        return fail(ctx, VLL_ERR_INVALID, "pyramid step above 12");
+    if (blunder) {
+        use_b = true;
+        H = blunder_half(desc, iteration, bblunder != 0, P.blunder_level);
+        im_res = desc->resolution * (double)(1 << P.blunder_level);
+    } else {
+        use_b = P.check_matchtag;
+        H = seeddem_half(desc);
+        im_res = desc->resolution * (double)(1 << P.L);
+    }
     return VLL_OK;
 }
 
@@ -854,6 +1004,130 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugri
         memset(stats, 0, sizeof(*stats));
         stats->kernel_ms = ms;
     }
+    return VLL_OK;
+}
+
+int vll_vertical_line_locus_seeddem_device(vll_context *ctx, const vll_level_desc *desc,
+                                           vll_ugrid *d_gridpt3, vll_stats *stats) {
+    NvtxRange nvtx_range("vll_vertical_line_locus_seeddem_device");
+    DevLevel P;
+    int H;
+    double im_res;
+    bool use_b;
+    int rc = prepare_variant(ctx, desc, false, 0, 0, P, H, im_res, use_b);
+    if (rc) return rc;
+    if (!d_gridpt3) return fail(ctx, VLL_ERR_INVALID, "null gridpt3");
+    return run_ortho_variant(ctx, P, d_gridpt3, H, im_res, use_b, nullptr, stats);
+}
+
+int vll_vertical_line_locus_seeddem(vll_context *ctx, const vll_level_desc *desc,
+                                    vll_ugrid *gridpt3, vll_stats *stats) {
+    NvtxRange nvtx_range("vll_vertical_line_locus_seeddem");
+    DevLevel P;
+    int H;
+    double im_res;
+    bool use_b;
+    int rc = prepare_variant(ctx, desc, false, 0, 0, P, H, im_res, use_b);
+    if (rc) return rc;
+    if (!gridpt3 || !desc->grid_pts) return fail(ctx, VLL_ERR_INVALID, "null gridpt3 or grid_pts");
+    const int64_t N = P.n_nodes;
+    if ((rc = upload_ortho_images(ctx, desc, P, use_b))) return rc;
+    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    P.grid_pts = (const double *)ctx->pts.p;
+    if ((rc = run_ortho_variant(ctx, P, (vll_ugrid *)ctx->gp3.p, H, im_res, use_b, nullptr,
+                                stats)))
+        return rc;
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_vertical_line_locus_blunder_device(vll_context *ctx, const vll_level_desc *desc,
+                                           vll_ugrid *d_gridpt3, int iteration, int bblunder,
+                                           float *d_nccresult, vll_stats *stats) {
+    NvtxRange nvtx_range("vll_vertical_line_locus_blunder_device");
+    DevLevel P;
+    int H;
+    double im_res;
+    bool use_b;
+    int rc = prepare_variant(ctx, desc, true, iteration, bblunder, P, H, im_res, use_b);
+    if (rc) return rc;
+    if (!d_gridpt3 || !d_nccresult) return fail(ctx, VLL_ERR_INVALID, "null gridpt3 or nccresult");
+    return run_ortho_variant(ctx, P, d_gridpt3, H, im_res, true, d_nccresult, stats);
+}
+
+int vll_vertical_line_locus_blunder(vll_context *ctx, const vll_level_desc *desc,
+                                    vll_ugrid *gridpt3, int iteration, int bblunder,
+                                    float *nccresult, vll_stats *stats) {
+    NvtxRange nvtx_range("vll_vertical_line_locus_blunder");
+    DevLevel P;
+    int H;
+    double im_res;
+    bool use_b;
+    int rc = prepare_variant(ctx, desc, true, iteration, bblunder, P, H, im_res, use_b);
+    if (rc) return rc;
+    if (!gridpt3 || !nccresult || !desc->grid_pts)
+        return fail(ctx, VLL_ERR_INVALID, "null gridpt3, nccresult or grid_pts");
+    const int64_t N = P.n_nodes;
+    if ((rc = upload_ortho_images(ctx, desc, P, true))) return rc;
+    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    VLL_CUDA(ctx, ensure(ctx->gsum, (size_t)N * sizeof(float)));
+    P.grid_pts = (const double *)ctx->pts.p;
+    if ((rc = run_ortho_variant(ctx, P, (vll_ugrid *)ctx->gp3.p, H, im_res, true,
+                                (float *)ctx->gsum.p, stats)))
+        return rc;
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->gsum.p, (size_t)N * sizeof(float),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_debug_ortho_raster(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
+                           int use_b, double im_res, int ti, double *out, int64_t capacity,
+                           int64_t *width, int64_t *height) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !gridpt3 || !out || !width || !height || !desc->grid_pts)
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err, false);
+    if (rc) return fail(ctx, rc, err);
+    if (ti < 0 || ti >= P.num_images || !P.im[ti].selected)
+        return fail(ctx, VLL_ERR_INVALID, "image index out of range or not selected");
+    if (!(im_res > 0)) return fail(ctx, VLL_ERR_INVALID, "non-positive resolution");
+    const int64_t ow = (int64_t)((P.boundary[2] - P.boundary[0]) / im_res) + 1;
+    const int64_t oh = (int64_t)((P.boundary[3] - P.boundary[1]) / im_res) + 1;
+    *width = ow;
+    *height = oh;
+    if (ow <= 0 || oh <= 0) return fail(ctx, VLL_ERR_INVALID, "empty orthoimage boundary");
+    if (capacity < ow * oh) return fail(ctx, VLL_ERR_CAPACITY, "raster larger than the buffer");
+    const int64_t N = P.n_nodes;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    P.gp3 = (const vll_ugrid *)ctx->gp3.p;
+    const size_t total = (size_t)(ow * oh);
+    double2 *ptrs[2 * VLL_MAX_IMAGES] = {};
+    for (int i = 0; i < P.num_images; ++i) {
+        if (!P.im[i].selected) continue;
+        VLL_CUDA(ctx, ensure(ctx->ocd[i], total * sizeof(double2)));
+        VLL_CUDA(ctx, cudaMemsetAsync(ctx->ocd[i].p, 0, total * sizeof(double2), ctx->stream));
+        ptrs[i] = (double2 *)ctx->ocd[i].p;
+    }
+    if ((rc = upload_level_block(ctx, P))) return rc;
+    VLL_CUDA(ctx, ensure(ctx->ocdptr, sizeof(ptrs)));
+    VLL_CUDA(ctx, cudaMemcpyAsync(ctx->ocdptr.p, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    VLL_CUDA(ctx, vll::launch_ortho_raster((const DevLevel *)ctx->level.p,
+                                           (double2 *const *)ctx->ocdptr.p, ow, oh, im_res,
+                                           use_b ? 1 : 0, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(out, ctx->ocd[ti].p, total * sizeof(double2),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return VLL_OK;
 }
 

@@ -35,6 +35,10 @@ struct DevImage {
     double adj[2];
     int selected;
     int pad_;
+    // the blunder-selected pyramid level (VerticalLineLocus_blunder / _seeddem)
+    const uint16_t *img_b, *mag_b;
+    uint32_t wb, hb;
+    double sxb, syb;
 };
 
 // Everything one VerticalLineLocus call needs on the device.  Lives in device
@@ -43,7 +47,7 @@ struct DevLevel {
     int num_images, ref, L, H;
     int iteration, cmr, is_ra, check_matchtag;
     int combined, combined_incc, check_ortho, sgm_py;
-    int pre_dem_tif, pad0_;
+    int pre_dem_tif, blunder_level;
     double alpha, beta, ortho_th, th_height;
     double height_step, grid_res, bin_angle, dem_res;
     double im_res, im_res_next;

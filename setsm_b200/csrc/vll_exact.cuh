@@ -64,7 +64,8 @@ __device__ __forceinline__ int window_depth(int H, int row, int col, int r2) {
 // sample positions (and may veto a window offset).  Returns true when all
 // three sub-windows received samples.
 template <class PosFn>
-__device__ bool multi_ncc(const PatchSrc &S, int H, PosFn pos, double &count_ncc, double &sum_ncc) {
+__device__ bool multi_ncc(const PatchSrc &S, int H, PosFn pos, double &count_ncc, double &sum_ncc,
+                          int *cnt0_out = nullptr) {
     double s[3][4];
     int cnt[3] = {0, 0, 0};
 #pragma unroll
@@ -86,6 +87,7 @@ __device__ bool multi_ncc(const PatchSrc &S, int H, PosFn pos, double &count_ncc
                 for (int c = 0; c < 4; ++c) s[w][c] = __dadd_rn(s[w][c], v[c]);
             }
         }
+    if (cnt0_out) *cnt0_out = cnt[0];
     const bool all_pos = cnt[0] > 0 && cnt[1] > 0 && cnt[2] > 0;
     if (!all_pos) return false;
     double m[3][4];

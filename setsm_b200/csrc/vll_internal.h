@@ -5,6 +5,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <string>
+
+#include "setsm_vll.h"
+
 namespace vll {
 
 struct DevLevel;
@@ -26,6 +30,22 @@ cudaError_t launch_gncc(const DevLevel *dP, int64_t n_nodes, double *gsum, doubl
 cudaError_t launch_recheck(const DevLevel *dP, const int64_t *items,
                            const unsigned long long *n_items, int64_t max_items,
                            const double *gsum, const double *gcnt, double *out, cudaStream_t s);
+
+// vll_capi.cu: the per-call constants of a level from its descriptor;
+// vll_window = false skips the VerticalLineLocus window-size check (the
+// orthoimage variants choose their own window).
+int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err, bool vll_window = true);
+
+// vll_ortho.cu: SetOrthoImageCoord at a chosen resolution / pyramid, and the
+// seed-DEM and blunder ortho-NCC passes (gout may alias the level's gp3).
+cudaError_t launch_ortho_raster(const DevLevel *dP, double2 *const *cd, int64_t ow, int64_t oh,
+                                double im_res, int use_b, cudaStream_t s);
+cudaError_t launch_seeddem(const DevLevel *dP, int64_t n_nodes, double2 *const *cd, int64_t ow,
+                           int64_t oh, double im_res, int H, int use_b, vll_ugrid *gout,
+                           cudaStream_t s);
+cudaError_t launch_blunder(const DevLevel *dP, int64_t n_nodes, double2 *const *cd, int64_t ow,
+                           int64_t oh, double im_res, int H, vll_ugrid *gout, float *ncc_out,
+                           cudaStream_t s);
 
 // vll_preprocess.cu
 cudaError_t launch_sobel(const uint16_t *src, uint32_t w, uint32_t h, uint16_t *mag, uint8_t *bin,

@@ -4,6 +4,7 @@
 // the baseline the split-precision kernel is measured against.  Compiled with
 // -fmad=false; the shared helpers use explicit _rn intrinsics in any case.
 #include "vll_exact.cuh"
+#include "vll_geo.cuh"
 #include "vll_internal.h"
 
 namespace vll {
@@ -72,63 +73,6 @@ __global__ void __launch_bounds__(128) gncc_kernel(const DevLevel *__restrict__ 
         gsum[pt] = s;
         gcnt[pt] = c;
     }
-}
-
-// ps2wgs_single, CoordConversion.cpp:396-490, on the device.  Same formulas;
-// the transcendental functions are CUDA's (within a few ulp of the host's).
-__device__ double2 ps2wgs_dev(const vll_transparam &p, double X, double Y) {
-    if (p.projection == 1) {
-        const double a = p.a, e = p.e, lambda_0 = p.lambda_0, t_c = p.t_c, m_c = p.m_c;
-        const int pm = p.pm;
-        const double e2 = e * e, e4 = e2 * e2, e6 = e2 * e4, e8 = e4 * e4;
-        const double x = X * pm, y = Y * pm;
-        const double rho = sqrt(x * x + y * y);
-        const double t = rho * t_c / (a * m_c);
-        const double chi = kPi / 2 - 2 * atan(t);
-        double phi = chi + (e2 / 2 + 5 * e4 / 24 + e6 / 12 + 13 * e8 / 360) * sin(2 * chi) +
-                     (7 * e4 / 48 + 29 * e6 / 240 + 811 * e8 / 11520) * sin(4 * chi) +
-                     (7 * e6 / 120 + 81 * e8 / 1120) * sin(6 * chi) +
-                     (4279 * e8 / 161280) * sin(8 * chi);
-        double lambda = lambda_0 + atan2(x, -y);
-        phi = pm * phi;
-        lambda = pm * lambda;
-        if (lambda > kPi)
-            lambda = lambda - 2 * kPi;
-        else if (lambda < -kPi)
-            lambda = lambda + 2 * kPi;
-        return make_double2(180 / kPi * lambda, 180 / kPi * phi);
-    }
-    const int hemis = p.pm;
-    const double e2c = p.e2cuadrada, c = p.c;
-    const double X0 = X - 500000;
-    double Yv = Y;
-    if (hemis < 0) Yv = Yv - 10000000;
-    const int S = ((p.utm_zone * 6) - 183);
-    const double lat = Yv / (6366197.724 * 0.9996);
-    const double cl = cos(lat);
-    const double v = (c / (sqrt(1.0 + (e2c * (cl * cl))))) * 0.9996;
-    const double a = X0 / v;
-    const double a1 = sin(2 * lat);
-    const double a2 = a1 * (cl * cl);
-    const double j2 = lat + (a1 / 2.0);
-    const double j4 = ((3 * j2) + a2) / 4.0;
-    const double j6 = ((5 * j4) + (a2 * (cl * cl))) / 3;
-    const double alfa = (3 / 4.0) * e2c;
-    const double beta = (5 / 3.0) * alfa * alfa;
-    const double gama = (35 / 27.0) * alfa * alfa * alfa;
-    const double Bm = 0.9996 * c * (lat - alfa * j2 + beta * j4 - gama * j6);
-    const double b = (Yv - Bm) / v;
-    const double Epsi = ((e2c * a * a) / 2.0) * (cl * cl);
-    const double Eps = a * (1 - (Epsi / 3.0));
-    const double nab = (b * (1 - Epsi)) + lat;
-    const double senoheps = (exp(Eps) - exp(-Eps)) / 2;
-    const double Delt = atan(senoheps / (cos(nab)));
-    const double TaO = atan(cos(Delt) * tan(nab));
-    const double lon_o = (Delt * (180 / kPi)) + S;
-    const double lat_o = (lat + (1 + e2c * (cl * cl) - (3 / 2.0) * e2c * sin(lat) * cl * (TaO - lat)) *
-                                    (TaO - lat)) *
-                         (180 / kPi);
-    return make_double2(lon_o, lat_o);
 }
 
 // SetOrthoImageCoord, setsm_code.cpp:6550-6670 (OR pyramid): image coordinates

@@ -1,5 +1,5 @@
-// vll_shim.cu -- the C++ VerticalLineLocus drop-in (setsm_code.hpp:81) on
-// top of the C ABI.  Marshals the caller's ProInfo / LevelInfo into a
+// vll_shim.cu -- the C++ drop-ins for VerticalLineLocus (setsm_code.hpp:81)
+// and its orthoimage variants (:93, :95) on top of the C ABI.  Marshals the caller's ProInfo / LevelInfo into a
 // vll_level_desc, packs the VOXEL** rows (voxel route), runs the GPU, unpacks.
 #include <cstddef>
 #include <cstdio>
@@ -42,26 +42,19 @@ vll_context *shim_context() {
     return s.ctx;
 }
 
-}  // namespace
-
-int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
-                      tagNCCresult *nccresult, taglevelinfo &pl, const UpdateGrid *GridPT3,
-                      const unsigned char iteration, const double *minmaxHeight) {
-    if (proinfo->sensor_type != kSensorSB) die("frame (AB) sensors are not supported", nullptr);
-    if (proinfo->number_of_images > VLL_MAX_IMAGES) die("too many images", nullptr);
-    vll_context *ctx = shim_context();
-    ShimState &st = state();
-
-    vll_level_desc d;
+// Fills a level descriptor from the caller's ProInfo / LevelInfo (the fields
+// VerticalLineLocus and its orthoimage variants read).
+void fill_desc(const ProjectInfo *proinfo, const taglevelinfo &pl, int iteration,
+               const double *minmaxHeight, vll_level_desc &d) {
     memset(&d, 0, sizeof(d));
     const int L = *pl.Pyramid_step;
     d.num_images = proinfo->number_of_images;
     d.reference_id = pl.reference_id;
     d.pyramid_step = L;
     d.template_size = *pl.Template_size;
-    d.py_combined_level = *pl.Py_combined_level;
+    d.py_combined_level = pl.Py_combined_level ? *pl.Py_combined_level : 0;
     d.iteration = iteration;
-    d.check_matching_rate = *pl.check_matching_rate ? 1 : 0;
+    d.check_matching_rate = pl.check_matching_rate && *pl.check_matching_rate ? 1 : 0;
     d.is_ra = proinfo->IsRA;
     d.pre_dem_tif = proinfo->pre_DEMtif;
     d.check_matchtag = proinfo->check_Matchtag;
@@ -69,29 +62,35 @@ int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
     d.sensor_type = 0;
     d.resolution = proinfo->resolution;
     d.dem_resolution = proinfo->DEM_resolution;
-    d.height_step = *pl.height_step;
+    d.height_step = pl.height_step ? *pl.height_step : 1.0;
     d.grid_resolution = *pl.grid_resolution;
-    d.bin_angle = *pl.bin_angle;
+    d.bin_angle = pl.bin_angle ? *pl.bin_angle : 0.0;
     for (int i = 0; i < 4; ++i) d.boundary[i] = pl.Boundary[i];
-    d.minmax_height[0] = minmaxHeight[0];
-    d.minmax_height[1] = minmaxHeight[1];
+    if (minmaxHeight) {
+        d.minmax_height[0] = minmaxHeight[0];
+        d.minmax_height[1] = minmaxHeight[1];
+    }
     d.grid_width = pl.Size_Grid2D->width;
     d.grid_height = pl.Size_Grid2D->height;
     d.grid_pts = reinterpret_cast<const double *>(pl.GridPts);
     d.grid_wgs = reinterpret_cast<const double *>(pl.Grid_wgs);
     memcpy(&d.param, pl.param, sizeof(d.param));
-    const bool combined = !proinfo->IsRA && L > *pl.Py_combined_level;
+    const bool combined = !proinfo->IsRA && L > d.py_combined_level;
+    const int BL = pl.blunder_selected_level ? *pl.blunder_selected_level : L;
+    d.blunder_level = BL;
     for (int ti = 0; ti < d.num_images; ++ti) {
         vll_image_desc &im = d.images[ti];
         im.selected = proinfo->check_selected_image[ti] ? 1 : 0;
         if (!im.selected) continue;
-        im.image = pl.py_Images[ti];
-        im.mag = pl.py_MagImages[ti];
-        im.ori = pl.py_OriImages[ti];
+        im.image = pl.py_Images ? pl.py_Images[ti] : nullptr;
+        im.mag = pl.py_MagImages ? pl.py_MagImages[ti] : nullptr;
+        im.ori = pl.py_OriImages ? pl.py_OriImages[ti] : nullptr;
         im.width = pl.py_Sizes[ti][L].width;
         im.height = pl.py_Sizes[ti][L].height;
-        im.startpos[0] = pl.py_Startpos[ti].m_X;
-        im.startpos[1] = pl.py_Startpos[ti].m_Y;
+        if (pl.py_Startpos) {
+            im.startpos[0] = pl.py_Startpos[ti].m_X;
+            im.startpos[1] = pl.py_Startpos[ti].m_Y;
+        }
         if (combined && L >= 1 && pl.py_Images_next) {
             im.image_next = pl.py_Images_next[ti];
             im.mag_next = pl.py_MagImages_next[ti];
@@ -103,6 +102,16 @@ int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
                 im.startpos_next[1] = pl.py_Startpos_next[ti].m_Y;
             }
         }
+        if (pl.py_BImages && pl.py_BMagImages && pl.blunder_selected_level) {
+            im.image_b = pl.py_BImages[ti];
+            im.mag_b = pl.py_BMagImages[ti];
+            im.width_b = pl.py_Sizes[ti][BL].width;
+            im.height_b = pl.py_Sizes[ti][BL].height;
+            if (pl.py_BStartpos) {
+                im.startpos_b[0] = pl.py_BStartpos[ti].m_X;
+                im.startpos_b[1] = pl.py_BStartpos[ti].m_Y;
+            }
+        }
         // RPC rows: offsets[5], scales[5], 4 x 20 coefficients
         const double *const *rpc = pl.RPCs[ti];
         memcpy(im.rpc + 0, rpc[0], 5 * sizeof(double));
@@ -111,6 +120,23 @@ int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
         im.image_adjust[0] = pl.ImageAdjust[ti][0];
         im.image_adjust[1] = pl.ImageAdjust[ti][1];
     }
+}
+
+void check_sensor(const ProjectInfo *proinfo) {
+    if (proinfo->sensor_type != kSensorSB) die("frame (AB) sensors are not supported", nullptr);
+    if (proinfo->number_of_images > VLL_MAX_IMAGES) die("too many images", nullptr);
+}
+
+}  // namespace
+
+int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
+                      tagNCCresult *nccresult, taglevelinfo &pl, const UpdateGrid *GridPT3,
+                      const unsigned char iteration, const double *minmaxHeight) {
+    check_sensor(proinfo);
+    vll_context *ctx = shim_context();
+    ShimState &st = state();
+    vll_level_desc d;
+    fill_desc(proinfo, pl, iteration, minmaxHeight, d);
 
     const int64_t n = d.grid_width * d.grid_height;
     const bool voxel_route = !d.check_matching_rate && !d.is_ra;
@@ -145,6 +171,29 @@ int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
         }
     }
     return (int)stats.accessable_grid;
+}
+
+void VerticalLineLocus_seeddem(const ProjectInfo *proinfo, taglevelinfo &pl, UpdateGrid *GridPT3,
+                               const double *minmaxHeight) {
+    check_sensor(proinfo);
+    vll_context *ctx = shim_context();
+    vll_level_desc d;
+    fill_desc(proinfo, pl, pl.iteration ? *pl.iteration : 1, minmaxHeight, d);
+    if (vll_vertical_line_locus_seeddem(ctx, &d, reinterpret_cast<vll_ugrid *>(GridPT3), nullptr) !=
+        VLL_OK)
+        die("VerticalLineLocus_seeddem: GPU call failed", vll_last_error(ctx));
+}
+
+bool VerticalLineLocus_blunder(const ProjectInfo *proinfo, taglevelinfo &pl, float *nccresult,
+                               UpdateGrid *GridPT3, unsigned char iteration, bool bblunder) {
+    check_sensor(proinfo);
+    vll_context *ctx = shim_context();
+    vll_level_desc d;
+    fill_desc(proinfo, pl, iteration, nullptr, d);
+    if (vll_vertical_line_locus_blunder(ctx, &d, reinterpret_cast<vll_ugrid *>(GridPT3), iteration,
+                                        bblunder ? 1 : 0, nccresult, nullptr) != VLL_OK)
+        die("VerticalLineLocus_blunder: GPU call failed", vll_last_error(ctx));
+    return true;
 }
 
 extern "C" int vll_compat_layout(int64_t *out, int cap) {
@@ -184,6 +233,11 @@ extern "C" int vll_compat_layout(int64_t *out, int cap) {
         (int64_t)offsetof(taglevelinfo, grid_resolution),
         (int64_t)offsetof(taglevelinfo, Py_combined_level),
         (int64_t)offsetof(taglevelinfo, check_matching_rate),
+        (int64_t)offsetof(taglevelinfo, py_BImages),
+        (int64_t)offsetof(taglevelinfo, py_BMagImages),
+        (int64_t)offsetof(taglevelinfo, py_BStartpos),
+        (int64_t)offsetof(taglevelinfo, blunder_selected_level),
+        (int64_t)offsetof(taglevelinfo, iteration),
         (int64_t)sizeof(tagNCCresult),
         (int64_t)sizeof(UpdateGrid),
         (int64_t)offsetof(UpdateGrid, ortho_ncc),

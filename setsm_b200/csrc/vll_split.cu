@@ -1678,8 +1678,6 @@ thread_local DevLevel g_noalloc_level_host;
 
 }  // namespace
 
-int derive_level(const vll_level_desc *d, DevLevel *P, std::string *err);
-
 }  // namespace vll
 
 extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,

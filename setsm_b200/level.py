@@ -28,6 +28,10 @@ class ImageLevel:
     ori_next: np.ndarray | None = None
     startpos_next: tuple = (0.0, 0.0)
     selected: bool = True
+    # the blunder-selected pyramid level (None: the matched level)
+    image_b: np.ndarray | None = None
+    mag_b: np.ndarray | None = None
+    startpos_b: tuple = (0.0, 0.0)
 
 
 def _c(a, dtype):
@@ -45,7 +49,7 @@ class LevelInputs:
                  dem_resolution: float = 2.0, minmax_height=(-500.0, 3000.0),
                  sgm_py: int = 0, py_combined_level: int = 0, bin_angle: float = 20.0,
                  is_ra: bool = False, pre_dem_tif: bool = False, check_matchtag: bool = False,
-                 param: dict | None = None, reference_id: int = 0):
+                 param: dict | None = None, reference_id: int = 0, blunder_level: int | None = None):
         self.images = []
         for im in images:
             self.images.append(ImageLevel(
@@ -53,7 +57,8 @@ class LevelInputs:
                 rpc=_c(im.rpc, np.float64), startpos=im.startpos, adjust=im.adjust,
                 image_next=_c(im.image_next, np.uint16), mag_next=_c(im.mag_next, np.uint16),
                 ori_next=_c(im.ori_next, np.uint8), startpos_next=im.startpos_next,
-                selected=im.selected))
+                selected=im.selected, image_b=_c(im.image_b, np.uint16),
+                mag_b=_c(im.mag_b, np.uint16), startpos_b=im.startpos_b))
         self.grid_pts = _c(grid_pts, np.float64)
         self.grid_wgs = _c(grid_wgs, np.float64)
         self.grid_width = int(grid_width)
@@ -80,6 +85,7 @@ class LevelInputs:
         self.check_matchtag = bool(check_matchtag)
         self.param = dict(param) if param is not None else {}
         self.reference_id = int(reference_id)
+        self.blunder_level = int(pyramid_step if blunder_level is None else blunder_level)
 
     def desc(self) -> abi.LevelDesc:
         d = abi.LevelDesc()
@@ -126,6 +132,12 @@ class LevelInputs:
                 e.rpc[k] = im.rpc[k]
             e.image_adjust[0], e.image_adjust[1] = im.adjust
             e.selected = int(im.selected)
+            if im.image_b is not None:
+                e.image_b = abi.ptr(im.image_b)
+                e.mag_b = abi.ptr(im.mag_b)
+                e.height_b, e.width_b = im.image_b.shape
+                e.startpos_b[0], e.startpos_b[1] = im.startpos_b
+        d.blunder_level = self.blunder_level
         return d
 
     def new_nccresult(self) -> np.ndarray:

@@ -31,6 +31,8 @@ EXPORTED = [
     "vll_compat_layout", "vll_launch_count", "vll_debug_slot_rho",
     "vll_vertical_line_locus_batch", "vll_plan_create", "vll_plan_run", "vll_plan_destroy",
     "vll_set_tuning", "vll_get_tuning",
+    "vll_vertical_line_locus_seeddem", "vll_vertical_line_locus_seeddem_device",
+    "vll_vertical_line_locus_blunder", "vll_vertical_line_locus_blunder_device",
 ]
 
 _lib = None
@@ -87,6 +89,11 @@ def load():
     L.vll_plan_destroy.restype = None
     L.vll_set_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
     L.vll_get_tuning.argtypes = [vp, C.POINTER(abi.Tuning)]
+    D, S = C.POINTER(abi.LevelDesc), C.POINTER(abi.Stats)
+    L.vll_vertical_line_locus_seeddem.argtypes = [vp, D, vp, S]
+    L.vll_vertical_line_locus_seeddem_device.argtypes = [vp, D, vp, S]
+    L.vll_vertical_line_locus_blunder.argtypes = [vp, D, vp, i32, i32, vp, S]
+    L.vll_vertical_line_locus_blunder_device.argtypes = [vp, D, vp, i32, i32, vp, S]
     _lib = L
     return L
 
@@ -186,6 +193,38 @@ class Context:
         self._check(load().vll_awncc_peaks(self._h, C.byref(d), inputs.gridpt3.ctypes.data,
                                            nccresult.ctypes.data, vptr, voxels.size, C.byref(st)))
         return st
+
+    # ---- orthoimage-window variants ------------------------------------------------
+    def seeddem(self, inputs, gridpt3: np.ndarray | None = None) -> abi.Stats:
+        """VerticalLineLocus_seeddem (setsm_code.cpp:7720-7880): updates
+        `gridpt3` (default: inputs.gridpt3) in place."""
+        g = inputs.gridpt3 if gridpt3 is None else gridpt3
+        d = inputs.desc()
+        st = abi.Stats()
+        self._check(load().vll_vertical_line_locus_seeddem(self._h, C.byref(d), g.ctypes.data,
+                                                           C.byref(st)))
+        return st
+
+    def blunder(self, inputs, iteration: int, bblunder: bool,
+                gridpt3: np.ndarray | None = None) -> np.ndarray:
+        """VerticalLineLocus_blunder (setsm_code.cpp:7882-8026): updates
+        `gridpt3` in place and returns the per-node float NCC."""
+        g = inputs.gridpt3 if gridpt3 is None else gridpt3
+        d = inputs.desc()
+        out = np.zeros(len(g), dtype=np.float32)
+        self._check(load().vll_vertical_line_locus_blunder(
+            self._h, C.byref(d), g.ctypes.data, int(iteration), int(bool(bblunder)),
+            out.ctypes.data, None))
+        return out
+
+    def seeddem_device(self, desc, d_gridpt3: int) -> None:
+        self._check(load().vll_vertical_line_locus_seeddem_device(self._h, C.byref(desc),
+                                                                  d_gridpt3, None))
+
+    def blunder_device(self, desc, d_gridpt3: int, iteration: int, bblunder: bool,
+                       d_ncc: int) -> None:
+        self._check(load().vll_vertical_line_locus_blunder_device(
+            self._h, C.byref(desc), d_gridpt3, int(iteration), int(bool(bblunder)), d_ncc, None))
 
     # ---- preprocessing -----------------------------------------------------------
     def preprocess(self, image: np.ndarray, template_size: int = 15):

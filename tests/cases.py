@@ -63,6 +63,30 @@ def make_case(*, seed=3, size=768, nodes=48, res=7.5, template=11, cmr=True, L=0
     return inp
 
 
+def make_variant_case(*, seed=5, size=512, nodes=32, res=8.0, template=11, L=0,
+                      blunder_level=None, matchtag=False, off_frac=0.4, off_m=40.0,
+                      void_frac=0.08, minmax=(-60.0, 420.0)):
+    """A case for the orthoimage-window variants (VerticalLineLocus_seeddem /
+    _blunder): node heights at the truth, off by up to `off_m` metres on
+    `off_frac` of the nodes (low ortho NCC) and -1000 (unmatched) on
+    `void_frac`; the blunder level's images (images[].image_b) at
+    `blunder_level` (default: the matched level)."""
+    inp = make_case(seed=seed, size=size, nodes=nodes, res=res, template=template, L=L,
+                    cmr=False, sgm=-1, n_heights=32, minmax=minmax)
+    bl = L if blunder_level is None else int(blunder_level)
+    for ci, im in enumerate(inp.images):
+        im.image_b, im.mag_b, _ = pyramid(seed, size, ci, bl)
+    inp.blunder_level = bl
+    inp.check_matchtag = bool(matchtag)
+    rng = np.random.default_rng(seed + 17)
+    g = inp.gridpt3
+    n = len(g)
+    off = rng.random(n) < off_frac
+    g["Height"][off] += rng.uniform(-off_m, off_m, int(off.sum())).astype(np.float32)
+    g["Height"][rng.random(n) < void_frac] = -1000
+    return inp
+
+
 # name -> kwargs
 CASES = {
     "m7": dict(),
@@ -148,6 +172,9 @@ def device_level(torch, inp, ncc: np.ndarray, voxels: np.ndarray | None = None):
         if im.image_next is not None:
             for name, arr in (("image_next", im.image_next), ("mag_next", im.mag_next),
                               ("ori_next", im.ori_next)):
+                setattr(d.images[ti], name, dev(arr).data_ptr())
+        if im.image_b is not None:
+            for name, arr in (("image_b", im.image_b), ("mag_b", im.mag_b)):
                 setattr(d.images[ti], name, dev(arr).data_ptr())
     d.grid_wgs = dev(inp.grid_wgs).data_ptr()
     d.grid_pts = dev(inp.grid_pts).data_ptr()

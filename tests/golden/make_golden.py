@@ -8,7 +8,7 @@ fixture holds a digest of the case's inputs and the reference's outputs, so
 tests/test_oracle_golden.py can pin the oracle (and the CUDA kernels) on a
 machine without the reference sources.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]
 """
 from __future__ import annotations
 
@@ -53,12 +53,38 @@ GOLDEN_SGM = {
 }
 
 
+# The orthoimage-window variants (VerticalLineLocus_seeddem, setsm_code.cpp:
+# 7720-7880; VerticalLineLocus_blunder, :7882-8026): kwargs of
+# tests/cases.py:make_variant_case plus the call ("seeddem", or "blunder"
+# with its iteration and bblunder flag).
+GOLDEN_VARIANTS = {
+    "sd_l0": dict(kind="seeddem", case=dict(seed=5, nodes=28, res=8.0, L=0)),
+    "sd_mt_l1": dict(kind="seeddem", case=dict(seed=6, nodes=20, res=10.0, L=1, template=15,
+                                               blunder_level=2, matchtag=True)),
+    "bl_l0": dict(kind="blunder", iteration=1, bblunder=False,
+                  case=dict(seed=7, nodes=28, res=8.0, L=0, blunder_level=1)),
+    "bl_l3_bb": dict(kind="blunder", iteration=2, bblunder=True,
+                     case=dict(seed=8, nodes=16, res=16.0, L=3, template=15, blunder_level=3)),
+}
+
+
+def variant_case(name):
+    """The inputs of variant fixture `name` (RPCs from the fixture) and the
+    fixture's arrays."""
+    from tests import cases
+    z = np.load(fixture_path(name))
+    inp = cases.make_variant_case(**GOLDEN_VARIANTS[name]["case"])
+    for im, rpc in zip(inp.images, z["rpc"]):
+        im.rpc = np.ascontiguousarray(rpc)
+    return inp, z
+
+
 def input_digest(inp) -> str:
     h = hashlib.sha256()
     for im in inp.images:
         for a in (im.image, im.mag, im.ori, np.asarray(im.rpc, dtype=np.float64)):
             h.update(np.ascontiguousarray(a).tobytes())
-        for a in (im.image_next, im.mag_next, im.ori_next):
+        for a in (im.image_next, im.mag_next, im.ori_next, im.image_b, im.mag_b):
             if a is not None:
                 h.update(np.ascontiguousarray(a).tobytes())
     for a in (inp.grid_pts, inp.grid_wgs, inp.gridpt3):
@@ -79,13 +105,16 @@ def fixture_path(name: str) -> str:
     return os.path.join(HERE, f"{name}.npz")
 
 
-def main() -> None:
+def main(only=None) -> None:
+    """Writes every fixture, or only the names in `only`."""
     from oracle import refpy
     from tests import cases
     if not refpy.available():
         raise SystemExit("reference build missing: make -C oracle ref")
     refpy.set_threads(os.cpu_count() or 1)
     for name, kw in list(GOLDEN.items()) + list(GOLDEN_SGM.items()):
+        if only and name not in only:
+            continue
         inp = cases.make_case(**kw)
         r = cases.run_cpu(refpy, inp, inp.iters)
         arrays = {
@@ -103,6 +132,23 @@ def main() -> None:
         print(f"{name}: acc {r['acc']}, peaks {(r['ncc']['result4'] > 0).sum()}, "
               f"{os.path.getsize(fixture_path(name))} bytes")
 
+    for name, v in GOLDEN_VARIANTS.items():
+        if only and name not in only:
+            continue
+        inp = cases.make_variant_case(**v["case"])
+        # the RPC fit of the synthetic scene rounds differently on other CPUs
+        # (its least-squares solve); the fixture carries the coefficients
+        arrays = {"digest": np.array(input_digest(inp)),
+                  "rpc": np.stack([np.asarray(im.rpc, dtype=np.float64) for im in inp.images]),
+                  "init_gp3": clean(inp.gridpt3).view(np.uint8)}
+        if v["kind"] == "seeddem":
+            refpy.vll_seeddem(inp)
+        else:
+            arrays["ncc"] = refpy.vll_blunder(inp, v["iteration"], v["bblunder"])
+        arrays["gp3"] = clean(inp.gridpt3).view(np.uint8)
+        np.savez_compressed(fixture_path(name), **arrays)
+        print(f"{name}: {os.path.getsize(fixture_path(name))} bytes")
+
 
 if __name__ == "__main__":
-    main()
+    main(set(sys.argv[1:]) or None)

@@ -53,6 +53,25 @@ def test_cpp_dropin_symbol_is_exported():
     assert demangled.startswith("VerticalLineLocus(tagVoxelinfo**, ProjectInfo const*")
 
 
+# setsm_code.hpp:93 and :95, the orthoimage-window variants
+VARIANTS = {
+    "_Z25VerticalLineLocus_seeddemPK11ProjectInfoR12taglevelinfoP10UpdateGridPKd":
+        "VerticalLineLocus_seeddem(ProjectInfo const*, taglevelinfo&, UpdateGrid*, double const*)",
+    "_Z25VerticalLineLocus_blunderPK11ProjectInfoR12taglevelinfoPfP10UpdateGridhb":
+        "VerticalLineLocus_blunder(ProjectInfo const*, taglevelinfo&, float*, UpdateGrid*, "
+        "unsigned char, bool)",
+}
+
+
+def test_cpp_variant_dropins_are_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", vll.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    for sym, sig in VARIANTS.items():
+        assert re.search(r"\bT " + sym + r"\b", out), sym
+        demangled = subprocess.run(["c++filt", sym], capture_output=True, text=True).stdout
+        assert demangled.strip() == sig
+
+
 def test_record_sizes():
     assert abi.NCCRESULT_DTYPE.itemsize == 24
     assert abi.UGRID_DTYPE.itemsize == 20

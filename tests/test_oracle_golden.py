@@ -67,3 +67,26 @@ def test_sgm_fixtures_are_the_reference_output(name):
     assert r["acc"] == g["acc"]
     for k in ("init_ncc", "vll_ncc", "ncc", "vll_vox"):
         assert cases.field_mismatch(r[k], g[k]) == {}, k
+
+
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_VARIANTS))
+def test_variant_fixture_inputs_are_reproducible(name):
+    """The seeded variant cases rebuild the fixtures' exact inputs."""
+    inp, z = mg.variant_case(name)
+    assert mg.input_digest(inp) == str(z["digest"])
+    assert np.array_equal(mg.clean(inp.gridpt3).view(np.uint8), z["init_gp3"])
+
+
+@pytest.mark.skipif(not __import__("oracle.refpy").refpy.available(),
+                    reason="reference build not available")
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_VARIANTS))
+def test_variant_fixtures_are_the_reference_output(name):
+    from oracle import refpy
+    v = mg.GOLDEN_VARIANTS[name]
+    inp, z = mg.variant_case(name)
+    if v["kind"] == "seeddem":
+        refpy.vll_seeddem(inp)
+    else:
+        ncc = refpy.vll_blunder(inp, v["iteration"], v["bblunder"])
+        assert np.array_equal(ncc.view(np.uint32), z["ncc"].view(np.uint32))
+    assert np.array_equal(mg.clean(inp.gridpt3).view(np.uint8), z["gp3"])
