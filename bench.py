@@ -636,6 +636,103 @@ def run_sgm(args):
     del torch
 
 
+def run_variant(args):
+    """The orthoimage-window variants on the reduced C2 scene (4096^2 pair at
+    0.5 m, 1024^2 grid, node heights from the TIN estimate): seeddem =
+    VerticalLineLocus_seeddem at level 0 (5 m template, 11x11 window);
+    blunder = VerticalLineLocus_blunder with the blunder level 1 (the level-1
+    pyramid built on the GPU) as in DecisionMPs' second call.  GPU: the C ABI
+    on host buffers (device time of the raster + node kernels; e2e = host wall
+    clock of the call with its copies); CPU: the reference's own function
+    with OpenMP on every host core, on the whole grid; outputs compared.
+    Metric: grid nodes per second."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import copy
+    import ctypes as C
+    import torch
+    from oracle import refpy
+    from setsm_b200 import abi, vll, workloads
+    from tests.cases import field_mismatch
+    ctx = vll.Context(0)
+    wl = workloads.build("c2_small", ctx, device="cuda:0", seed=1)
+    inp = wl.host_inputs(11)
+    kind = args.config
+    if kind == "blunder":
+        n = wl.d_img[0].shape[0] // 2
+        for ci, im in enumerate(inp.images):
+            d_b = torch.empty((n, n), dtype=torch.int16, device="cuda:0")
+            d_m = torch.empty_like(d_b)
+            d_o = torch.empty((n, n), dtype=torch.uint8, device="cuda:0")
+            ctx.pyramid_down_device(wl.d_img[ci].data_ptr(), 2 * n, 2 * n, d_b.data_ptr())
+            ctx.preprocess_device(d_b.data_ptr(), n, n, d_m.data_ptr(), d_o.data_ptr())
+            torch.cuda.synchronize()
+            im.image_b = d_b.cpu().numpy().view(np.uint16)
+            im.mag_b = d_m.cpu().numpy().view(np.uint16)
+        inp.blunder_level = 1
+    gp3_0 = inp.gridpt3.copy()
+
+    def call():
+        inp.gridpt3 = gp3_0.copy()
+        if kind == "seeddem":
+            return ctx.seeddem(inp), None
+        st = abi.Stats()
+        ncc = np.zeros(inp.n, dtype=np.float32)
+        d = inp.desc()
+        ctx._check(vll.load().vll_vertical_line_locus_blunder(
+            ctx._h, C.byref(d), inp.gridpt3.ctypes.data, 1, 0, ncc.ctypes.data, C.byref(st)))
+        return st, ncc
+    for _ in range(max(1, args.warmup)):
+        call()
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        st, ncc = call()
+        times.append((st.kernel_ms, (time.perf_counter() - t) * 1e3))
+    clk = clocks.stop()
+    got = inp.gridpt3.copy()
+    dev_ms = statistics.median(t[0] for t in times)
+    e2e_ms = statistics.median(t[1] for t in times)
+    ref = copy.copy(inp)
+    ref.gridpt3 = gp3_0.copy()
+    refpy.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    want = refpy.vll_seeddem(ref) if kind == "seeddem" else refpy.vll_blunder(ref, 1, False)
+    cpu_s = time.perf_counter() - t
+    parity = {"ugrid_field_mismatch": field_mismatch(got, ref.gridpt3)}
+    if ncc is not None:
+        parity["ncc_float_identical_frac"] = float(np.mean(ncc.view(np.uint32)
+                                                           == want.view(np.uint32)))
+        parity["ncc_max_abs_diff"] = float(np.abs(ncc.astype(np.float64) - want).max())
+        parity["ncc_max_ulps"] = int(np.abs(ncc.view(np.int32).astype(np.int64)
+                                            - want.view(np.int32).astype(np.int64)).max())
+    n = int(inp.n)
+    name = {"seeddem": "VerticalLineLocus_seeddem, level 0, 5 m template (11x11 window)",
+            "blunder": "VerticalLineLocus_blunder, blunder level 1, iteration 1"}[kind]
+    line = {
+        "metric": f"grid nodes/s ({kind})", "value": n / (dev_ms / 1e3), "unit": "nodes/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": dev_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (the reference's arithmetic)", "data": "synthetic",
+        "config": {"workload": f"{name}: reduced C2 scene (4096^2 pair at 0.5 m, 1024^2 grid, "
+                               "TIN height estimate)", "nodes": n},
+        "e2e": {"value": n / (e2e_ms / 1e3), "unit": "nodes/s",
+                "timing": "host wall clock of the C-ABI call on host buffers (image planes, "
+                          "grid and UGRID copied in, UGRID and NCC copied out)"},
+        "cpu_baseline": {"value": n / cpu_s, "unit": "nodes/s", "cores": os.cpu_count(),
+                         "kind": "reference", "sample": f"whole grid, {cpu_s:.2f} s"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+        "parity": parity,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    del torch
+
+
 # ---------------------------------------------------------------------------
 # C5 serving
 # ---------------------------------------------------------------------------
@@ -710,7 +807,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
-                    choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm"])
+                    choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm", "seeddem",
+                             "blunder"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -737,6 +835,8 @@ def main():
         run_c5(args)
     elif args.config == "sgm":
         run_sgm(args)
+    elif args.config in ("seeddem", "blunder"):
+        run_variant(args)
     else:
         run_ours(args)
 

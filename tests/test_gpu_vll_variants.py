@@ -36,19 +36,23 @@ def run_gpu(ctx, v, inp):
 # The blunder pass's float NCC inherits the map projection's last-bit
 # differences from the host's C library (about one raster coordinate in a
 # thousand differs by an ulp, see setsm_b200/csrc/vll_ddmath.cuh), which move
-# the NCC by ~1e-10: the floats must be identical on at least 99.5% of the
-# nodes and within NCC_TOL everywhere.  The UGRID fields (quantised to 1e-3)
-# must be identical.
-NCC_TOL = 1e-8
+# the double NCC by ~1e-10 and, rarely, its float rounding by one ulp.  The
+# tolerance: identical floats on at least 99.5% of the nodes, and adjacent
+# floats (one ulp, <= 6e-8 for |NCC| < 1) on the rest.  The UGRID fields
+# (quantised to 1e-3) must be identical.
+NCC_MAX_ULPS = 1
 NCC_EXACT_FRAC = 0.995
 
 
 def assert_same(gp3, want_gp3, ncc=None, want_ncc=None):
     assert cases.field_mismatch(mg.clean(gp3), mg.clean(want_gp3)) == {}
     if want_ncc is not None:
-        same = ncc.view(np.uint32) == want_ncc.view(np.uint32)
+        a = ncc.astype(np.float32).view(np.int32).astype(np.int64)
+        b = want_ncc.astype(np.float32).view(np.int32).astype(np.int64)
+        same = a == b
         assert same.mean() >= NCC_EXACT_FRAC, (int((~same).sum()), len(same))
-        assert np.abs(ncc.astype(np.float64) - want_ncc).max() <= NCC_TOL
+        assert np.all(np.sign(ncc) == np.sign(want_ncc))
+        assert np.abs(a - b).max() <= NCC_MAX_ULPS
 
 
 @pytest.mark.parametrize("name", sorted(mg.GOLDEN_VARIANTS))
