@@ -14,17 +14,23 @@ from oracle import oraclepy as op
 
 
 @functools.lru_cache(maxsize=8)
-def scene(seed: int, size: int):
-    return synth.make_scene(synth.SceneSpec(seed=seed, image_size=size))
+def scene(seed: int, size: int, n_cams: int = 2):
+    if n_cams == 2:
+        return synth.make_scene(synth.SceneSpec(seed=seed, image_size=size))
+    return synth.make_scene(synth.SceneSpec(seed=seed, image_size=size, cameras=CAMS[:n_cams]))
+
+
+# a third, near-nadir view for the multi-image cases
+CAMS = (synth.CameraSpec(15.0, 0.7), synth.CameraSpec(-15.0, -0.9), synth.CameraSpec(4.0, 0.25))
 
 
 @functools.lru_cache(maxsize=32)
-def pyramid(seed: int, size: int, ci: int, lev: int):
+def pyramid(seed: int, size: int, ci: int, lev: int, n_cams: int = 2):
     """(image, mag, ori) of camera ci at pyramid level lev."""
     if lev == 0:
-        im = scene(seed, size).images[ci].numpy().view(np.uint16).copy()
+        im = scene(seed, size, n_cams).images[ci].numpy().view(np.uint16).copy()
     else:
-        im = op.pyramid_down(pyramid(seed, size, ci, lev - 1)[0])
+        im = op.pyramid_down(pyramid(seed, size, ci, lev - 1, n_cams)[0])
     mag, ori = op.preprocess(im)
     return im, mag, ori
 
@@ -32,23 +38,24 @@ def pyramid(seed: int, size: int, ci: int, lev: int):
 def make_case(*, seed=3, size=768, nodes=48, res=7.5, template=11, cmr=True, L=0, it=1,
               sgm=0, n_heights=64, hs=1.0, sigma=20.0, ortho_frac=0.0, unmatched_frac=0.0,
               zero_patch=False, minmax=(-500.0, 3000.0), dem_res=2.0, combined_level=0,
-              iters=None):
-    sc = scene(seed, size)
+              iters=None, n_images=2, unselected=()):
+    sc = scene(seed, size, n_images)
     g = synth.make_grid(sc, nodes, res)
     lo, hi, _ = synth.ranges_uniform(g, n_heights, hs, sigma, seed=seed + 1)
     rng = np.random.default_rng(seed + 2)
     imgs = []
-    for ci in range(2):
-        im, mag, ori = pyramid(seed, size, ci, L)
+    for ci in range(n_images):
+        im, mag, ori = pyramid(seed, size, ci, L, n_images)
         if zero_patch:
             im = im.copy()
             h, w = im.shape
             im[h // 3: h // 3 + h // 10, w // 4: w // 4 + w // 8] = 0
         kw = {}
         if L >= 1:
-            imn, magn, orin = pyramid(seed, size, ci, L - 1)
+            imn, magn, orin = pyramid(seed, size, ci, L - 1, n_images)
             kw = dict(image_next=imn, mag_next=magn, ori_next=orin)
-        imgs.append(level.ImageLevel(image=im, mag=mag, ori=ori, rpc=sc.rpcs[ci], **kw))
+        imgs.append(level.ImageLevel(image=im, mag=mag, ori=ori, rpc=sc.rpcs[ci],
+                                     selected=ci not in unselected, **kw))
     on = None
     if ortho_frac > 0:
         on = np.where(rng.random(lo.shape) < ortho_frac, 800, 100)
@@ -65,17 +72,17 @@ def make_case(*, seed=3, size=768, nodes=48, res=7.5, template=11, cmr=True, L=0
 
 def make_variant_case(*, seed=5, size=512, nodes=32, res=8.0, template=11, L=0,
                       blunder_level=None, matchtag=False, off_frac=0.4, off_m=40.0,
-                      void_frac=0.08, minmax=(-60.0, 420.0)):
+                      void_frac=0.08, minmax=(-60.0, 420.0), n_images=2):
     """A case for the orthoimage-window variants (VerticalLineLocus_seeddem /
     _blunder): node heights at the truth, off by up to `off_m` metres on
     `off_frac` of the nodes (low ortho NCC) and -1000 (unmatched) on
     `void_frac`; the blunder level's images (images[].image_b) at
     `blunder_level` (default: the matched level)."""
     inp = make_case(seed=seed, size=size, nodes=nodes, res=res, template=template, L=L,
-                    cmr=False, sgm=-1, n_heights=32, minmax=minmax)
+                    cmr=False, sgm=-1, n_heights=32, minmax=minmax, n_images=n_images)
     bl = L if blunder_level is None else int(blunder_level)
     for ci, im in enumerate(inp.images):
-        im.image_b, im.mag_b, _ = pyramid(seed, size, ci, bl)
+        im.image_b, im.mag_b, _ = pyramid(seed, size, ci, bl, n_images)
     inp.blunder_level = bl
     inp.check_matchtag = bool(matchtag)
     rng = np.random.default_rng(seed + 17)
@@ -100,6 +107,11 @@ CASES = {
                    n_heights=24, hs=2.0, template=15),
     "l3_m": dict(L=3, it=1, cmr=True, nodes=16, res=24.0, n_heights=20, hs=3.0, template=15),
     "v7_it2": dict(cmr=False, sgm=-1, it=2, iters=(1, 2), ortho_frac=0.5, n_heights=48),
+    # three images (the FP64 kernel): every selected target image enters the sums
+    "m7_3img": dict(n_images=3, nodes=40, n_heights=48),
+    "v7_3img": dict(n_images=3, cmr=False, sgm=-1, ortho_frac=0.5, nodes=40, n_heights=40),
+    "v7_3img_unsel": dict(n_images=3, unselected=(1,), cmr=False, sgm=-1, ortho_frac=0.5,
+                          nodes=40, n_heights=40),
 }
 
 

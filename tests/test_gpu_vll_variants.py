@@ -94,6 +94,9 @@ def test_variant_device_entry_point(gpu_ctx, name):
     ("blunder1", dict(seed=25, size=768, nodes=32, res=12.0, L=2, blunder_level=2)),
     ("blunder2", dict(seed=26, size=768, nodes=24, res=16.0, L=4, template=15, blunder_level=3)),
     ("blunder3", dict(seed=27, size=768, nodes=24, res=16.0, L=3, template=15, blunder_level=3)),
+    # three images: ortho_ncc[2] lands on Mean_ortho_ncc as in the reference
+    ("seeddem", dict(seed=28, size=512, nodes=32, res=8.0, L=0, n_images=3)),
+    ("blunder1", dict(seed=29, size=512, nodes=32, res=8.0, L=0, blunder_level=1, n_images=3)),
 ])
 def test_variant_matches_reference_build(gpu_ctx, kind, kw):
     inp = cases.make_variant_case(**kw)
