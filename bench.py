@@ -733,6 +733,94 @@ def run_variant(args):
     del torch
 
 
+def run_ortho_tin(args):
+    """Ortho_blunder (TIN-triangle orthoimage height search, setsm_code.cpp:
+    8028-8533) on the reduced C2 scene (4096^2 pair at 0.5 m, 1024^2 grid at
+    2 m): matched points on 2 % of the grid nodes (60 % anchored, candidates
+    off the truth by up to 25 m, height ranges +-40 m), their Delaunay TIN,
+    MPP 1.5.  GPU: the C ABI on host buffers, timed by the host wall clock of
+    the call (each round ends by reading a flag, so the call waits for the GPU
+    anyway); CPU: the
+    reference's Ortho_blunder with OpenMP on every host core; outputs
+    compared.  Metric: triangles per second (TIN triangles / call time)."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import copy
+    import torch
+    from oracle import refpy
+    from setsm_b200 import abi, vll, workloads
+    from tests.cases import delaunay, field_mismatch
+    ctx = vll.Context(0)
+    wl = workloads.build("c2_small", ctx, device="cuda:0", seed=1)
+    inp = wl.host_inputs(11)
+    rng = np.random.default_rng(5)
+    g0 = inp.gridpt3.copy()
+    n = len(g0)
+    sel = np.sort(rng.choice(n, size=int(0.02 * n), replace=False))
+    truth = g0["Height"][sel].astype(np.float64)
+    anchor = rng.random(len(sel)) < 0.6
+    pts0 = np.zeros(len(sel), dtype=abi.POINT3_DTYPE)
+    pts0["x"], pts0["y"] = inp.grid_pts[sel, 0], inp.grid_pts[sel, 1]
+    pts0["z"] = np.where(anchor, truth, truth + rng.uniform(-25.0, 25.0, len(sel)))
+    pts0["flag"] = 1
+    g0["anchor_flag"] = 0
+    g0["anchor_flag"][sel] = np.where(anchor, 1, 2)
+    g0["minHeight"][sel] = np.floor(truth - 40.0).astype(np.int16)
+    g0["maxHeight"][sel] = np.ceil(truth + 40.0).astype(np.int16)
+    tris = delaunay(pts0)
+    mpp = 1.5
+
+    def call():
+        inp.gridpt3 = g0.copy()
+        pts = pts0.copy()
+        t = time.perf_counter()
+        rounds = ctx.ortho_blunder(inp, mpp, pts, tris)
+        return (time.perf_counter() - t) * 1e3, rounds, pts
+    for _ in range(max(1, args.warmup)):
+        call()
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    lc0 = vll.load().vll_launch_count(ctx._h)
+    for _ in range(args.steps):
+        ms, rounds, pts = call()
+        times.append(ms)
+    launches = vll.load().vll_launch_count(ctx._h) - lc0
+    clk = clocks.stop()
+    ms = statistics.median(times)
+    ref = copy.copy(inp)
+    ref.gridpt3 = g0.copy()
+    ref_pts = pts0.copy()
+    refpy.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    refpy.ortho_blunder(ref, mpp, ref_pts, tris.copy())
+    cpu_s = time.perf_counter() - t
+    same_pts = all(np.array_equal(pts[f], ref_pts[f]) for f in ("x", "y", "z", "flag"))
+    line = {
+        "metric": "TIN triangles/s (Ortho_blunder)", "value": len(tris) / (ms / 1e3),
+        "unit": "triangles/s", "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup),
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (the reference's arithmetic)", "data": "synthetic",
+        "config": {"workload": "Ortho_blunder: reduced C2 scene (4096^2 pair at 0.5 m, 1024^2 "
+                               "grid at 2 m), points on 2% of the nodes, Delaunay TIN, MPP 1.5",
+                   "points": int(len(pts0)), "triangles": int(len(tris)), "rounds": rounds},
+        "e2e": {"value": len(tris) / (ms / 1e3), "unit": "triangles/s",
+                "timing": "host wall clock of the C-ABI call on host buffers (the call waits "
+                          "for a flag after every round, so device and e2e time coincide)"},
+        "cpu_baseline": {"value": len(tris) / cpu_s, "unit": "triangles/s",
+                         "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"whole TIN, {cpu_s:.2f} s"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "parity": {"points_identical": bool(same_pts),
+                   "ugrid_field_mismatch": field_mismatch(inp.gridpt3, ref.gridpt3)},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    del torch
+
+
 # ---------------------------------------------------------------------------
 # C5 serving
 # ---------------------------------------------------------------------------
@@ -808,7 +896,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
                     choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm", "seeddem",
-                             "blunder"])
+                             "blunder", "ortho_tin"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -837,6 +925,8 @@ def main():
         run_sgm(args)
     elif args.config in ("seeddem", "blunder"):
         run_variant(args)
+    elif args.config == "ortho_tin":
+        run_ortho_tin(args)
     else:
         run_ours(args)
 

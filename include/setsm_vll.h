@@ -71,6 +71,19 @@ typedef struct vll_nccresult {
     uint8_t check_height_change;
 } vll_nccresult;
 
+/* D3DPOINT, Typedefine.hpp:139-194 (32 bytes): a matched point, projected
+ * metres and height, and its flag. */
+typedef struct vll_point3 {
+    double x, y, z;
+    uint8_t flag;
+    uint8_t _pad[7];
+} vll_point3;
+
+/* UI3DPOINT, Typedefine.hpp:74-97: a TIN triangle's vertex indices. */
+typedef struct vll_tri {
+    uint32_t a, b, c;
+} vll_tri;
+
 /* UGRID, Typedefine.hpp:270-283 (20 bytes). */
 typedef struct vll_ugrid {
     float Height;
@@ -374,6 +387,38 @@ int vll_vertical_line_locus_blunder(vll_context *ctx, const vll_level_desc *desc
 int vll_vertical_line_locus_blunder_device(vll_context *ctx, const vll_level_desc *desc,
                                            vll_ugrid *d_gridpt3, int iteration, int bblunder,
                                            float *d_nccresult, vll_stats *stats);
+
+/*
+ * VerticalLineLocus_Ortho (setsm_code.cpp:8234-8533): the height search of a
+ * TIN triangle's target vertex.  Its height is swept over the UGRID range of
+ * grid node `target_index` in steps of resolution * 2^Pyramid_step * MPP (MPP
+ * clamped to [1, 3]); at each height the triangle's plane is sampled on the
+ * grid cells inside it, both images are read at the level (images[].image,
+ * mag), and the mean Pearson correlation of intensities and magnitudes over
+ * the target images picks the height.  Outputs as the reference: *f_height
+ * (-9999 when none qualifies), *f_sncc (written when a height was found) and
+ * the selected sample count (the reference's return value).  Host buffers.
+ */
+int vll_vertical_line_locus_ortho(vll_context *ctx, const vll_level_desc *desc, double mpp,
+                                  const vll_point3 *ref1, const vll_point3 *ref2,
+                                  const vll_point3 *target, const vll_ugrid *gridpt3,
+                                  int64_t target_index, double *f_height, double *f_sncc,
+                                  int *selected_count);
+/*
+ * Ortho_blunder (setsm_code.cpp:8028-8232): up to 200 rounds of the height
+ * search over every TIN triangle with exactly two anchored vertices
+ * (UGRID.anchor_flag 1 or 3), each round applying the best height per target
+ * point in triangle order (point height, flag, node anchor_flag = 3) until a
+ * round finds none.  pts, tris and gridpt3 are updated in place exactly as the
+ * reference does; *rounds (optional) receives the number of rounds.  The
+ * _device form takes device pointers (descriptor planes included) and waits.
+ */
+int vll_ortho_blunder(vll_context *ctx, const vll_level_desc *desc, double mpp, vll_point3 *pts,
+                      int64_t n_pts, const vll_tri *tris, int64_t n_tris, vll_ugrid *gridpt3,
+                      int *rounds);
+int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, double mpp,
+                             vll_point3 *d_pts, int64_t n_pts, const vll_tri *d_tris,
+                             int64_t n_tris, vll_ugrid *d_gridpt3, int *rounds);
 
 /* Diagnostics: the orthoimage coordinate raster of image `ti`
  * (SetOrthoImageCoord, setsm_code.cpp:6550-6670) at resolution im_res, on

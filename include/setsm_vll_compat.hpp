@@ -204,6 +204,34 @@ int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
                       tagNCCresult *nccresult, taglevelinfo &plevelinfo, const UpdateGrid *GridPT3,
                       const unsigned char iteration, const double *minmaxHeight);
 
+// D3DPOINT and UI3DPOINT (Typedefine.hpp:74-97, :139-194).  D3DPOINT has a
+// user-written copy constructor in the reference, so a D3DPOINT passed by
+// value travels by hidden reference; this one must have one too.
+struct tagD3DPoint {
+    double m_X, m_Y, m_Z;
+    unsigned char flag;
+    tagD3DPoint() : m_X(0), m_Y(0), m_Z(0), flag(0) {}
+    tagD3DPoint(const tagD3DPoint &p) : m_X(p.m_X), m_Y(p.m_Y), m_Z(p.m_Z), flag(p.flag) {}
+};
+struct tagUI3DPoint {
+    uint32_t m_X, m_Y, m_Z;
+    tagUI3DPoint() : m_X(0), m_Y(0), m_Z(0) {}
+    tagUI3DPoint(const tagUI3DPoint &p) : m_X(p.m_X), m_Y(p.m_Y), m_Z(p.m_Z) {}
+};
+static_assert(sizeof(tagD3DPoint) == sizeof(vll_point3), "D3DPOINT layout");
+static_assert(sizeof(tagUI3DPoint) == sizeof(vll_tri), "UI3DPOINT layout");
+
+// The TIN-triangle height search and its driver (setsm_code.hpp:97, :118),
+// same behaviour: VerticalLineLocus_Ortho returns the selected sample count
+// and writes *F_Height (-9999 when none) and *F_sncc (when found);
+// Ortho_blunder updates pts, GridPT3 in place and returns numOfPts.
+int VerticalLineLocus_Ortho(ProjectInfo *proinfo, taglevelinfo &plevelinfo, double MPP,
+                            double *F_Height, tagD3DPoint ref1_pt, tagD3DPoint ref2_pt,
+                            tagD3DPoint target_pt, UpdateGrid *GridPT3, int target_index,
+                            double *F_sncc);
+int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &plevelinfo, double MPP, tagD3DPoint *pts,
+                  int numOfPts, tagUI3DPoint *tris, int numOfTri, UpdateGrid *GridPT3);
+
 // The orthoimage-window variants (setsm_code.hpp:93, :95), same behaviour:
 // VerticalLineLocus_seeddem updates GridPT3; VerticalLineLocus_blunder
 // writes GridPT3's ortho NCC and nccresult[node], and returns true.

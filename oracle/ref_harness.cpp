@@ -394,6 +394,58 @@ long ref_call_vertical_line_locus(void *fn, const vll_level_desc *d, const vll_u
     return acc;
 }
 
+/* VerticalLineLocus_Ortho (setsm_code.cpp:8234-8533) for the triangle
+ * three[0..2] = ref1, ref2, target; out = {F_Height, F_sncc} (F_sncc keeps
+ * the value passed in out[1] when no height is found); returns its value. */
+static D3DPOINT d3(const vll_point3 &p) { return D3DPOINT(p.x, p.y, p.z, p.flag); }
+int ref_vll_ortho(const vll_level_desc *d, double mpp, const vll_point3 *three, vll_ugrid *gridpt3,
+                  int target_index, double *out) {
+    RefLevel L(d);
+    double fh = 0, fs = out[1];
+    const int r = VerticalLineLocus_Ortho(L.proinfo, L.li, mpp, &fh, d3(three[0]), d3(three[1]),
+                                          d3(three[2]), reinterpret_cast<UGRID *>(gridpt3),
+                                          target_index, &fs);
+    out[0] = fh;
+    out[1] = fs;
+    return r;
+}
+
+/* Ortho_blunder (setsm_code.cpp:8028-8232): pts, tris and GridPT3 in/out. */
+int ref_ortho_blunder(const vll_level_desc *d, double mpp, vll_point3 *pts, int n_pts,
+                      vll_tri *tris, int n_tris, vll_ugrid *gridpt3) {
+    static_assert(sizeof(vll_point3) == sizeof(D3DPOINT), "D3DPOINT layout");
+    static_assert(sizeof(vll_tri) == sizeof(UI3DPOINT), "UI3DPOINT layout");
+    RefLevel L(d);
+    return Ortho_blunder(L.proinfo, L.li, mpp, reinterpret_cast<D3DPOINT *>(pts), n_pts,
+                         reinterpret_cast<UI3DPOINT *>(tris), n_tris,
+                         reinterpret_cast<UGRID *>(gridpt3));
+}
+
+/* The same, through functions with the reference's signatures at `fn` (the
+ * library's C++ drop-ins, setsm_code.hpp:97, :118). */
+typedef int (*vll_ortho_signature)(ProInfo *, LevelInfo &, double, double *, D3DPOINT, D3DPOINT,
+                                   D3DPOINT, UGRID *, int, double *);
+typedef int (*ortho_blunder_signature)(ProInfo *, LevelInfo &, double, D3DPOINT *, int,
+                                       UI3DPOINT *, int, UGRID *);
+int ref_call_vll_ortho(void *fn, const vll_level_desc *d, double mpp, const vll_point3 *three,
+                       vll_ugrid *gridpt3, int target_index, double *out) {
+    RefLevel L(d);
+    double fh = 0, fs = out[1];
+    const int r = reinterpret_cast<vll_ortho_signature>(fn)(
+        L.proinfo, L.li, mpp, &fh, d3(three[0]), d3(three[1]), d3(three[2]),
+        reinterpret_cast<UGRID *>(gridpt3), target_index, &fs);
+    out[0] = fh;
+    out[1] = fs;
+    return r;
+}
+int ref_call_ortho_blunder(void *fn, const vll_level_desc *d, double mpp, vll_point3 *pts,
+                           int n_pts, vll_tri *tris, int n_tris, vll_ugrid *gridpt3) {
+    RefLevel L(d);
+    return reinterpret_cast<ortho_blunder_signature>(fn)(
+        L.proinfo, L.li, mpp, reinterpret_cast<D3DPOINT *>(pts), n_pts,
+        reinterpret_cast<UI3DPOINT *>(tris), n_tris, reinterpret_cast<UGRID *>(gridpt3));
+}
+
 /* SetOrthoImageCoord (setsm_code.cpp:6550-6670): the orthoimage coordinate
  * raster of image ti at im_res, OR (use_b = 0) or BD pyramid. */
 long ref_ortho_raster(const vll_level_desc *d, const vll_ugrid *gridpt3, int use_b, double im_res,

@@ -306,3 +306,61 @@ def call_vll_blunder(fn_addr: int, inputs, iteration: int, bblunder: bool) -> np
                                     int(iteration), int(bblunder), out.ctypes.data)
     assert ok == 1
     return out
+
+
+def vll_ortho(inputs, mpp: float, three: np.ndarray, target_index: int):
+    """VerticalLineLocus_Ortho (setsm_code.cpp:8234-8533) for the triangle
+    three = (ref1, ref2, target) (abi.POINT3_DTYPE); returns (return value,
+    F_Height, F_sncc) with F_sncc NaN when the function leaves it unset."""
+    L = lib()
+    L.ref_vll_ortho.argtypes = [C.POINTER(abi.LevelDesc), C.c_double, C.c_void_p, C.c_void_p,
+                                C.c_int, C.c_void_p]
+    L.ref_vll_ortho.restype = C.c_int
+    d = inputs.desc()
+    three = np.ascontiguousarray(three, dtype=abi.POINT3_DTYPE)
+    out = np.array([0.0, np.nan])
+    with _StdoutToStderr():
+        r = L.ref_vll_ortho(C.byref(d), float(mpp), three.ctypes.data, inputs.gridpt3.ctypes.data,
+                            int(target_index), out.ctypes.data)
+    return int(r), float(out[0]), float(out[1])
+
+
+def ortho_blunder(inputs, mpp: float, pts: np.ndarray, tris: np.ndarray) -> int:
+    """Ortho_blunder (setsm_code.cpp:8028-8232); pts, tris and
+    inputs.gridpt3 are updated in place."""
+    L = lib()
+    L.ref_ortho_blunder.argtypes = [C.POINTER(abi.LevelDesc), C.c_double, C.c_void_p, C.c_int,
+                                    C.c_void_p, C.c_int, C.c_void_p]
+    L.ref_ortho_blunder.restype = C.c_int
+    d = inputs.desc()
+    with _StdoutToStderr():
+        return int(L.ref_ortho_blunder(C.byref(d), float(mpp), pts.ctypes.data, len(pts),
+                                       tris.ctypes.data, len(tris), inputs.gridpt3.ctypes.data))
+
+
+def call_vll_ortho(fn_addr: int, inputs, mpp: float, three: np.ndarray, target_index: int):
+    """As vll_ortho, through the function at fn_addr (setsm_code.hpp:97 signature)."""
+    L = lib()
+    L.ref_call_vll_ortho.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_double, C.c_void_p,
+                                     C.c_void_p, C.c_int, C.c_void_p]
+    L.ref_call_vll_ortho.restype = C.c_int
+    d = inputs.desc()
+    three = np.ascontiguousarray(three, dtype=abi.POINT3_DTYPE)
+    out = np.array([0.0, np.nan])
+    with _StdoutToStderr():
+        r = L.ref_call_vll_ortho(fn_addr, C.byref(d), float(mpp), three.ctypes.data,
+                                 inputs.gridpt3.ctypes.data, int(target_index), out.ctypes.data)
+    return int(r), float(out[0]), float(out[1])
+
+
+def call_ortho_blunder(fn_addr: int, inputs, mpp: float, pts: np.ndarray, tris: np.ndarray) -> int:
+    """As ortho_blunder, through the function at fn_addr (setsm_code.hpp:118)."""
+    L = lib()
+    L.ref_call_ortho_blunder.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_double,
+                                         C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+    L.ref_call_ortho_blunder.restype = C.c_int
+    d = inputs.desc()
+    with _StdoutToStderr():
+        return int(L.ref_call_ortho_blunder(fn_addr, C.byref(d), float(mpp), pts.ctypes.data,
+                                            len(pts), tris.ctypes.data, len(tris),
+                                            inputs.gridpt3.ctypes.data))

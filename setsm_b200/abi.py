@@ -60,6 +60,14 @@ VOXEL_DTYPE = np.dtype(
     {"names": ["flag_cal", "INCC"], "formats": ["u1", "<i2"], "offsets": [0, 2], "itemsize": 4}
 )
 
+# vll_point3 (D3DPOINT, 32 B) and vll_tri (UI3DPOINT, 12 B)
+POINT3_DTYPE = np.dtype(
+    {"names": ["x", "y", "z", "flag"], "formats": ["<f8", "<f8", "<f8", "u1"],
+     "offsets": [0, 8, 16, 24], "itemsize": 32}
+)
+TRI_DTYPE = np.dtype({"names": ["a", "b", "c"], "formats": ["<u4", "<u4", "<u4"],
+                      "offsets": [0, 4, 8], "itemsize": 12})
+
 
 class TransParam(C.Structure):
     _fields_ = [

@@ -64,6 +64,7 @@ struct vll_context {
     Buf ocd[VLL_MAX_IMAGES], ocdn[VLL_MAX_IMAGES], ocdptr;
     Buf pre_tmp, pre_wt, pre_img, pre_mag, pre_ori;
     Buf sumcost;                       // SGM aggregation (float per voxel slot)
+    Buf tin_pts, tin_tris, tin_scratch;  // Ortho_blunder: points, triangles, work arrays
     vll::SplitBuffers split;
     vll::SplitTuning tuning;
     void *set = nullptr;               // SetResources of batch calls (vll_capi.cu)
@@ -732,6 +733,9 @@ void vll_destroy(vll_context *ctx) {
     release(ctx->pre_mag);
     release(ctx->pre_ori);
     release(ctx->sumcost);
+    release(ctx->tin_pts);
+    release(ctx->tin_tris);
+    release(ctx->tin_scratch);
     vll::split_release(ctx->split);
     if (ctx->set) {
         release_set(*(SetResources *)ctx->set);
@@ -1085,6 +1089,114 @@ int vll_vertical_line_locus_blunder(vll_context *ctx, const vll_level_desc *desc
                                   cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return VLL_OK;
+}
+
+int vll_vertical_line_locus_ortho(vll_context *ctx, const vll_level_desc *desc, double mpp,
+                                  const vll_point3 *ref1, const vll_point3 *ref2,
+                                  const vll_point3 *target, const vll_ugrid *gridpt3,
+                                  int64_t target_index, double *f_height, double *f_sncc,
+                                  int *selected_count) {
+    NvtxRange nvtx_range("vll_vertical_line_locus_ortho");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !ref1 || !ref2 || !target || !gridpt3 || !f_height || !f_sncc || !selected_count)
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err, false);
+    if (rc) return fail(ctx, rc, err);
+    if (target_index < 0 || target_index >= P.n_nodes)
+        return fail(ctx, VLL_ERR_INVALID, "target_index outside the grid");
+    const int64_t N = P.n_nodes;
+    if ((rc = upload_ortho_images(ctx, desc, P, false))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    P.gp3 = (const vll_ugrid *)ctx->gp3.p;
+    const vll_point3 three[3] = {*ref1, *ref2, *target};
+    if ((rc = upload(ctx, ctx->tin_pts, three, sizeof(three)))) return rc;
+    VLL_CUDA(ctx, ensure(ctx->tin_scratch, 4 * sizeof(double)));
+    if ((rc = upload_level_block(ctx, P))) return rc;
+    VLL_CUDA(ctx, vll::launch_ortho_search((const DevLevel *)ctx->level.p, mpp,
+                                           (const vll_point3 *)ctx->tin_pts.p, target_index,
+                                           (double *)ctx->tin_scratch.p, ctx->stream));
+    double out[3];
+    VLL_CUDA(ctx, cudaMemcpyAsync(out, ctx->tin_scratch.p, sizeof(out), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->launches_total += 1;
+    *f_height = out[0];
+    if (out[0] != -9999.0) *f_sncc = out[1];
+    *selected_count = (int)out[2];
+    return VLL_OK;
+}
+
+// Ortho_blunder on device data: P's pointers (images, gp3) are device pointers.
+static int ortho_blunder_run(vll_context *ctx, DevLevel &P, double mpp, vll_point3 *d_pts,
+                             int64_t n_pts, const vll_tri *d_tris, int64_t n_tris,
+                             vll_ugrid *d_gp3, int *rounds) {
+    if (n_pts < 0 || n_tris < 0 || n_pts > 0x7fffffff || n_tris > 0x7fffffff)
+        return fail(ctx, VLL_ERR_INVALID, "point or triangle count out of range");
+    if (rounds) *rounds = 0;
+    if (n_tris == 0) return VLL_OK;
+    P.gp3 = d_gp3;
+    int rc = upload_level_block(ctx, P);
+    if (rc) return rc;
+    const size_t bytes = vll::ortho_blunder_scratch(n_pts, n_tris, P.n_nodes);
+    VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
+    int it = 0, bad = 0;
+    VLL_CUDA(ctx, vll::run_ortho_blunder((const DevLevel *)ctx->level.p, P, mpp, d_pts, n_pts,
+                                         d_tris, n_tris, d_gp3, ctx->tin_scratch.p, bytes, &it,
+                                         &bad, ctx->stream));
+    if (bad) return fail(ctx, VLL_ERR_INVALID, "a triangle vertex lies outside the grid");
+    // own kernels: the node and lon/lat passes, then search / records / apply / anchor per
+    // round (the radix sort between them is CUB's)
+    ctx->launches_total += 2 + 4 * (int64_t)it;
+    if (rounds) *rounds = it;
+    return VLL_OK;
+}
+
+int vll_ortho_blunder(vll_context *ctx, const vll_level_desc *desc, double mpp, vll_point3 *pts,
+                      int64_t n_pts, const vll_tri *tris, int64_t n_tris, vll_ugrid *gridpt3,
+                      int *rounds) {
+    NvtxRange nvtx_range("vll_ortho_blunder");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !gridpt3 || (n_pts > 0 && !pts) || (n_tris > 0 && !tris))
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err, false);
+    if (rc) return fail(ctx, rc, err);
+    const int64_t N = P.n_nodes;
+    if ((rc = upload_ortho_images(ctx, desc, P, false))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->tin_pts, pts, (size_t)n_pts * sizeof(vll_point3)))) return rc;
+    if ((rc = upload(ctx, ctx->tin_tris, tris, (size_t)n_tris * sizeof(vll_tri)))) return rc;
+    rc = ortho_blunder_run(ctx, P, mpp, (vll_point3 *)ctx->tin_pts.p, n_pts,
+                           (const vll_tri *)ctx->tin_tris.p, n_tris, (vll_ugrid *)ctx->gp3.p,
+                           rounds);
+    if (rc) return rc;
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    if (n_pts > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(pts, ctx->tin_pts.p, (size_t)n_pts * sizeof(vll_point3),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, double mpp,
+                             vll_point3 *d_pts, int64_t n_pts, const vll_tri *d_tris,
+                             int64_t n_tris, vll_ugrid *d_gridpt3, int *rounds) {
+    NvtxRange nvtx_range("vll_ortho_blunder_device");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !d_gridpt3 || (n_pts > 0 && !d_pts) || (n_tris > 0 && !d_tris))
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err, false);
+    if (rc) return fail(ctx, rc, err);
+    return ortho_blunder_run(ctx, P, mpp, d_pts, n_pts, d_tris, n_tris, d_gridpt3, rounds);
 }
 
 int vll_debug_ortho_raster(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,

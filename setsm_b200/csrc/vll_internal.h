@@ -47,6 +47,16 @@ cudaError_t launch_blunder(const DevLevel *dP, int64_t n_nodes, double2 *const *
                            int64_t oh, double im_res, int H, vll_ugrid *gout, float *ncc_out,
                            cudaStream_t s);
 
+// vll_orthotin.cu: VerticalLineLocus_Ortho (one triangle; d_out = {F_Height,
+// F_sncc, selected count}) and Ortho_blunder on device data.
+cudaError_t launch_ortho_search(const DevLevel *dP, double mpp, const vll_point3 *d_pts3,
+                                int64_t target_index, double *d_out, cudaStream_t s);
+size_t ortho_blunder_scratch(int64_t n_pts, int64_t n_tris, int64_t n_nodes);
+cudaError_t run_ortho_blunder(const DevLevel *dP, const DevLevel &hP, double mpp, vll_point3 *pts,
+                              int64_t n_pts, const vll_tri *tris, int64_t n_tris,
+                              vll_ugrid *gp3, void *scratch, size_t scratch_bytes,
+                              int *iterations, int *bad_input, cudaStream_t s);
+
 // vll_preprocess.cu
 cudaError_t launch_sobel(const uint16_t *src, uint32_t w, uint32_t h, uint16_t *mag, uint8_t *bin,
                          cudaStream_t s);

@@ -196,6 +196,45 @@ bool VerticalLineLocus_blunder(const ProjectInfo *proinfo, taglevelinfo &pl, flo
     return true;
 }
 
+static vll_point3 point_of(const tagD3DPoint &p) {
+    vll_point3 q;
+    memset(&q, 0, sizeof(q));
+    q.x = p.m_X;
+    q.y = p.m_Y;
+    q.z = p.m_Z;
+    q.flag = p.flag;
+    return q;
+}
+
+int VerticalLineLocus_Ortho(ProjectInfo *proinfo, taglevelinfo &pl, double MPP, double *F_Height,
+                            tagD3DPoint ref1_pt, tagD3DPoint ref2_pt, tagD3DPoint target_pt,
+                            UpdateGrid *GridPT3, int target_index, double *F_sncc) {
+    check_sensor(proinfo);
+    vll_context *ctx = shim_context();
+    vll_level_desc d;
+    fill_desc(proinfo, pl, pl.iteration ? *pl.iteration : 1, nullptr, d);
+    const vll_point3 r1 = point_of(ref1_pt), r2 = point_of(ref2_pt), tg = point_of(target_pt);
+    int selected = 0;
+    if (vll_vertical_line_locus_ortho(ctx, &d, MPP, &r1, &r2, &tg,
+                                      reinterpret_cast<const vll_ugrid *>(GridPT3), target_index,
+                                      F_Height, F_sncc, &selected) != VLL_OK)
+        die("VerticalLineLocus_Ortho: GPU call failed", vll_last_error(ctx));
+    return selected;
+}
+
+int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &pl, double MPP, tagD3DPoint *pts,
+                  int numOfPts, tagUI3DPoint *tris, int numOfTri, UpdateGrid *GridPT3) {
+    check_sensor(proinfo);
+    vll_context *ctx = shim_context();
+    vll_level_desc d;
+    fill_desc(proinfo, pl, pl.iteration ? *pl.iteration : 1, nullptr, d);
+    if (vll_ortho_blunder(ctx, &d, MPP, reinterpret_cast<vll_point3 *>(pts), numOfPts,
+                          reinterpret_cast<const vll_tri *>(tris), numOfTri,
+                          reinterpret_cast<vll_ugrid *>(GridPT3), nullptr) != VLL_OK)
+        die("Ortho_blunder: GPU call failed", vll_last_error(ctx));
+    return numOfPts;
+}
+
 extern "C" int vll_compat_layout(int64_t *out, int cap) {
     const int64_t v[] = {
         (int64_t)sizeof(ProjectInfo),

@@ -33,6 +33,7 @@ EXPORTED = [
     "vll_set_tuning", "vll_get_tuning",
     "vll_vertical_line_locus_seeddem", "vll_vertical_line_locus_seeddem_device",
     "vll_vertical_line_locus_blunder", "vll_vertical_line_locus_blunder_device",
+    "vll_vertical_line_locus_ortho", "vll_ortho_blunder", "vll_ortho_blunder_device",
 ]
 
 _lib = None
@@ -94,6 +95,10 @@ def load():
     L.vll_vertical_line_locus_seeddem_device.argtypes = [vp, D, vp, S]
     L.vll_vertical_line_locus_blunder.argtypes = [vp, D, vp, i32, i32, vp, S]
     L.vll_vertical_line_locus_blunder_device.argtypes = [vp, D, vp, i32, i32, vp, S]
+    L.vll_vertical_line_locus_ortho.argtypes = [vp, D, C.c_double, vp, vp, vp, vp, i64, vp, vp,
+                                                vp]
+    L.vll_ortho_blunder.argtypes = [vp, D, C.c_double, vp, i64, vp, i64, vp, vp]
+    L.vll_ortho_blunder_device.argtypes = [vp, D, C.c_double, vp, i64, vp, i64, vp, vp]
     _lib = L
     return L
 
@@ -225,6 +230,41 @@ class Context:
                        d_ncc: int) -> None:
         self._check(load().vll_vertical_line_locus_blunder_device(
             self._h, C.byref(desc), d_gridpt3, int(iteration), int(bool(bblunder)), d_ncc, None))
+
+    # ---- TIN orthoimage height search ----------------------------------------------
+    def vertical_line_locus_ortho(self, inputs, mpp: float, three: np.ndarray,
+                                  target_index: int):
+        """VerticalLineLocus_Ortho (setsm_code.cpp:8234-8533) for the triangle
+        three = (ref1, ref2, target) (abi.POINT3_DTYPE): returns (selected
+        count, F_Height, F_sncc or NaN when unset)."""
+        three = np.ascontiguousarray(three, dtype=abi.POINT3_DTYPE)
+        d = inputs.desc()
+        fh, fs, sc = C.c_double(), C.c_double(float("nan")), C.c_int()
+        self._check(load().vll_vertical_line_locus_ortho(
+            self._h, C.byref(d), float(mpp), three[0:1].ctypes.data, three[1:2].ctypes.data,
+            three[2:3].ctypes.data, inputs.gridpt3.ctypes.data, int(target_index),
+            C.byref(fh), C.byref(fs), C.byref(sc)))
+        return sc.value, fh.value, fs.value
+
+    def ortho_blunder(self, inputs, mpp: float, pts: np.ndarray, tris: np.ndarray) -> int:
+        """Ortho_blunder (setsm_code.cpp:8028-8232): updates pts
+        (abi.POINT3_DTYPE), tris' effect and inputs.gridpt3 in place; returns
+        the number of rounds run."""
+        assert pts.dtype == abi.POINT3_DTYPE and tris.dtype == abi.TRI_DTYPE
+        d = inputs.desc()
+        rounds = C.c_int()
+        self._check(load().vll_ortho_blunder(self._h, C.byref(d), float(mpp), pts.ctypes.data,
+                                             len(pts), tris.ctypes.data, len(tris),
+                                             inputs.gridpt3.ctypes.data, C.byref(rounds)))
+        return rounds.value
+
+    def ortho_blunder_device(self, desc, mpp: float, d_pts: int, n_pts: int, d_tris: int,
+                             n_tris: int, d_gridpt3: int) -> int:
+        rounds = C.c_int()
+        self._check(load().vll_ortho_blunder_device(self._h, C.byref(desc), float(mpp), d_pts,
+                                                    n_pts, d_tris, n_tris, d_gridpt3,
+                                                    C.byref(rounds)))
+        return rounds.value
 
     # ---- preprocessing -----------------------------------------------------------
     def preprocess(self, image: np.ndarray, template_size: int = 15):

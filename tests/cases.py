@@ -94,6 +94,47 @@ def make_variant_case(*, seed=5, size=512, nodes=32, res=8.0, template=11, L=0,
     return inp
 
 
+def make_tin_case(*, seed=9, size=512, nodes=32, res=8.0, template=11, L=0, point_frac=0.3,
+                  anchor_frac=0.6, off_m=25.0, range_m=40.0, n_images=2):
+    """Inputs of Ortho_blunder: matched points on a random subset of the grid
+    nodes (height = truth, candidates off by up to `off_m`), anchor flags 1
+    (anchored) or 2 (candidate) on their nodes, candidate nodes' height range
+    truth +- `range_m`, and the Delaunay triangulation of the points (scipy).
+    Returns (inputs, pts, tris)."""
+    from setsm_b200 import abi
+    inp = make_case(seed=seed, size=size, nodes=nodes, res=res, template=template, L=L,
+                    cmr=False, sgm=-1, n_heights=32, n_images=n_images)
+    rng = np.random.default_rng(seed + 31)
+    g = inp.gridpt3
+    n = len(g)
+    sel = np.sort(rng.choice(n, size=max(4, int(point_frac * n)), replace=False))
+    truth = g["Height"][sel].astype(np.float64)
+    anchor = rng.random(len(sel)) < anchor_frac
+    pts = np.zeros(len(sel), dtype=abi.POINT3_DTYPE)
+    pts["x"] = inp.grid_pts[sel, 0]
+    pts["y"] = inp.grid_pts[sel, 1]
+    pts["z"] = np.where(anchor, truth, truth + rng.uniform(-off_m, off_m, len(sel)))
+    pts["flag"] = 1
+    g["anchor_flag"] = 0
+    g["anchor_flag"][sel] = np.where(anchor, 1, 2)
+    lo = np.floor(truth - range_m).astype(np.int16)
+    hi = np.ceil(truth + range_m).astype(np.int16)
+    g["minHeight"][sel] = lo
+    g["maxHeight"][sel] = hi
+    return inp, pts, delaunay(pts)
+
+
+def delaunay(pts):
+    """Triangles (abi.TRI_DTYPE) of the Delaunay triangulation of the points'
+    x, y (scipy's Qhull) -- a stand-in for the matcher's own TIN."""
+    from scipy.spatial import Delaunay
+    from setsm_b200 import abi
+    tri = Delaunay(np.stack([pts["x"], pts["y"]], axis=1)).simplices
+    tris = np.zeros(len(tri), dtype=abi.TRI_DTYPE)
+    tris["a"], tris["b"], tris["c"] = tri[:, 0], tri[:, 1], tri[:, 2]
+    return tris
+
+
 # name -> kwargs
 CASES = {
     "m7": dict(),

@@ -68,6 +68,30 @@ GOLDEN_VARIANTS = {
 }
 
 
+# Ortho_blunder (setsm_code.cpp:8028-8232) with VerticalLineLocus_Ortho:
+# kwargs of tests/cases.py:make_tin_case; the fixture keeps the points,
+# triangles and UGRID it starts from.
+GOLDEN_TIN = {
+    "tin_l0": dict(mpp=1.5, case=dict(seed=9)),
+    "tin_l1_3img": dict(mpp=2.0, case=dict(seed=12, L=1, res=12.0, template=15, n_images=3)),
+}
+
+
+def tin_case(name):
+    """(inputs, pts, tris, fixture arrays) of TIN fixture `name`: images from
+    the seeded case, RPCs, points, triangles and UGRID from the fixture."""
+    from setsm_b200 import abi
+    from tests import cases
+    z = np.load(fixture_path(name))
+    inp, _, _ = cases.make_tin_case(**GOLDEN_TIN[name]["case"])
+    for im, rpc in zip(inp.images, z["rpc"]):
+        im.rpc = np.ascontiguousarray(rpc)
+    inp.gridpt3 = z["init_gp3"].view(abi.UGRID_DTYPE).copy()
+    pts = z["init_pts"].view(abi.POINT3_DTYPE).copy()
+    tris = z["tris"].view(abi.TRI_DTYPE).copy()
+    return inp, pts, tris, z
+
+
 def variant_case(name):
     """The inputs of variant fixture `name` (RPCs from the fixture) and the
     fixture's arrays."""
@@ -77,6 +101,14 @@ def variant_case(name):
     for im, rpc in zip(inp.images, z["rpc"]):
         im.rpc = np.ascontiguousarray(rpc)
     return inp, z
+
+
+def image_digest(inp) -> str:
+    h = hashlib.sha256()
+    for im in inp.images:
+        for a in (im.image, im.mag):
+            h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
 
 
 def input_digest(inp) -> str:
@@ -146,6 +178,20 @@ def main(only=None) -> None:
         else:
             arrays["ncc"] = refpy.vll_blunder(inp, v["iteration"], v["bblunder"])
         arrays["gp3"] = clean(inp.gridpt3).view(np.uint8)
+        np.savez_compressed(fixture_path(name), **arrays)
+        print(f"{name}: {os.path.getsize(fixture_path(name))} bytes")
+
+    for name, v in GOLDEN_TIN.items():
+        if only and name not in only:
+            continue
+        inp, pts, tris = cases.make_tin_case(**v["case"])
+        arrays = {"rpc": np.stack([np.asarray(im.rpc, dtype=np.float64) for im in inp.images]),
+                  "img_digest": np.array(image_digest(inp)),
+                  "init_gp3": clean(inp.gridpt3).view(np.uint8),
+                  "init_pts": clean(pts).view(np.uint8), "tris": tris.view(np.uint8)}
+        refpy.ortho_blunder(inp, v["mpp"], pts, tris)
+        arrays["gp3"] = clean(inp.gridpt3).view(np.uint8)
+        arrays["pts"] = clean(pts).view(np.uint8)
         np.savez_compressed(fixture_path(name), **arrays)
         print(f"{name}: {os.path.getsize(fixture_path(name))} bytes")
 

@@ -90,3 +90,16 @@ def test_variant_fixtures_are_the_reference_output(name):
         ncc = refpy.vll_blunder(inp, v["iteration"], v["bblunder"])
         assert np.array_equal(ncc.view(np.uint32), z["ncc"].view(np.uint32))
     assert np.array_equal(mg.clean(inp.gridpt3).view(np.uint8), z["gp3"])
+
+
+@pytest.mark.skipif(not __import__("oracle.refpy").refpy.available(),
+                    reason="reference build not available")
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_TIN))
+def test_tin_fixtures_are_the_reference_output(name):
+    from oracle import refpy
+    from setsm_b200 import abi
+    inp, pts, tris, z = mg.tin_case(name)
+    assert mg.image_digest(inp) == str(z["img_digest"])
+    refpy.ortho_blunder(inp, mg.GOLDEN_TIN[name]["mpp"], pts, tris)
+    assert np.array_equal(mg.clean(pts).view(np.uint8), z["pts"])
+    assert np.array_equal(mg.clean(inp.gridpt3).view(np.uint8), z["gp3"])
