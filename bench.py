@@ -733,25 +733,13 @@ def run_variant(args):
     del torch
 
 
-def run_ortho_tin(args):
-    """Ortho_blunder (TIN-triangle orthoimage height search, setsm_code.cpp:
-    8028-8533) on the reduced C2 scene (4096^2 pair at 0.5 m, 1024^2 grid at
-    2 m): matched points on 2 % of the grid nodes (60 % anchored, candidates
-    off the truth by up to 25 m, height ranges +-40 m), their Delaunay TIN,
-    MPP 1.5.  GPU: the C ABI on host buffers, timed by the host wall clock of
-    the call (each round ends by reading a flag, so the call waits for the GPU
-    anyway); CPU: the
-    reference's Ortho_blunder with OpenMP on every host core; outputs
-    compared.  Metric: triangles per second (TIN triangles / call time)."""
-    world, rank, local = dist_setup(args.gpus)
-    if rank != 0:
-        return
-    import copy
-    import torch
-    from oracle import refpy
-    from setsm_b200 import abi, vll, workloads
-    from tests.cases import delaunay, field_mismatch
-    ctx = vll.Context(0)
+def tin_workload(ctx):
+    """The reduced C2 scene (4096^2 pair at 0.5 m, 1024^2 grid at 2 m) with
+    matched points on 2 % of the grid nodes (60 % anchored, candidates off the
+    truth by up to 25 m, height ranges +-40 m) and their Delaunay TIN.
+    Returns (inputs, UGRID, points, triangles)."""
+    from setsm_b200 import abi, workloads
+    from tests.cases import delaunay
     wl = workloads.build("c2_small", ctx, device="cuda:0", seed=1)
     inp = wl.host_inputs(11)
     rng = np.random.default_rng(5)
@@ -768,7 +756,97 @@ def run_ortho_tin(args):
     g0["anchor_flag"][sel] = np.where(anchor, 1, 2)
     g0["minHeight"][sel] = np.floor(truth - 40.0).astype(np.int16)
     g0["maxHeight"][sel] = np.ceil(truth + 40.0).astype(np.int16)
-    tris = delaunay(pts0)
+    r = rng.random(n)
+    g0["Matched_flag"] = np.where(r < 0.2, 0, np.where(r < 0.4, 4, 1))
+    g0["Mean_ortho_ncc"] = rng.integers(-1000, 1000, n).astype(np.int16)
+    return inp, g0, pts0, delaunay(pts0)
+
+
+def run_height_range(args):
+    """SetHeightRange (setsm_code.cpp:9851-10255) on the TIN workload of
+    tin_workload (1024^2 grid, 21 k points, 41.8 k triangles), level 0,
+    iteration 2, MPP 1.5.  GPU: the C ABI on host buffers (host wall clock of
+    the call, copies included: the call waits); CPU: the reference's own
+    SetHeightRange (mostly sequential); returned grids compared.  Metric:
+    grid nodes per second."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import copy
+    import torch
+    from oracle import refpy
+    from setsm_b200 import vll
+    from tests.cases import field_mismatch
+    ctx = vll.Context(0)
+    inp, g0, pts, tris = tin_workload(ctx)
+    it, mpp = 2, 1.5
+
+    def call():
+        inp.gridpt3 = g0.copy()
+        t = time.perf_counter()
+        out, ext = ctx.set_height_range(inp, pts, tris, it, mpp, False)
+        return (time.perf_counter() - t) * 1e3, out, ext
+    for _ in range(max(1, args.warmup)):
+        call()
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    lc0 = vll.load().vll_launch_count(ctx._h)
+    for _ in range(args.steps):
+        ms, out, ext = call()
+        times.append(ms)
+    launches = vll.load().vll_launch_count(ctx._h) - lc0
+    clk = clocks.stop()
+    ms = statistics.median(times)
+    ref = copy.copy(inp)
+    ref.gridpt3 = g0.copy()
+    refpy.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    want, wext = refpy.set_height_range(ref, pts, tris, it, mpp, False)
+    cpu_s = time.perf_counter() - t
+    n = int(inp.n)
+    line = {
+        "metric": "grid nodes/s (SetHeightRange)", "value": n / (ms / 1e3), "unit": "nodes/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (the reference's arithmetic)", "data": "synthetic",
+        "config": {"workload": "SetHeightRange: 1024^2 grid at 2 m, 21 k matched points, "
+                               "Delaunay TIN, level 0, iteration 2, MPP 1.5",
+                   "nodes": n, "points": int(len(pts)), "triangles": int(len(tris))},
+        "e2e": {"value": n / (ms / 1e3), "unit": "nodes/s",
+                "timing": "host wall clock of the C-ABI call on host buffers (the call waits)"},
+        "cpu_baseline": {"value": n / cpu_s, "unit": "nodes/s", "cores": os.cpu_count(),
+                         "kind": "reference", "sample": f"whole grid, {cpu_s:.3f} s"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "parity": {"result_field_mismatch": field_mismatch(out, want),
+                   "extent_identical": ext == wext},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    del torch
+
+
+def run_ortho_tin(args):
+    """Ortho_blunder (TIN-triangle orthoimage height search, setsm_code.cpp:
+    8028-8533) on the reduced C2 scene (4096^2 pair at 0.5 m, 1024^2 grid at
+    2 m): matched points on 2 % of the grid nodes (60 % anchored, candidates
+    off the truth by up to 25 m, height ranges +-40 m), their Delaunay TIN,
+    MPP 1.5.  GPU: the C ABI on host buffers, timed by the host wall clock of
+    the call (each round ends by reading a flag, so the call waits for the GPU
+    anyway); CPU: the
+    reference's Ortho_blunder with OpenMP on every host core; outputs
+    compared.  Metric: triangles per second (TIN triangles / call time)."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import copy
+    import torch
+    from oracle import refpy
+    from setsm_b200 import vll
+    from tests.cases import field_mismatch
+    ctx = vll.Context(0)
+    inp, g0, pts0, tris = tin_workload(ctx)
     mpp = 1.5
 
     def call():
@@ -896,7 +974,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
                     choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm", "seeddem",
-                             "blunder", "ortho_tin"])
+                             "blunder", "ortho_tin", "height_range"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -927,6 +1005,8 @@ def main():
         run_variant(args)
     elif args.config == "ortho_tin":
         run_ortho_tin(args)
+    elif args.config == "height_range":
+        run_height_range(args)
     else:
         run_ours(args)
 

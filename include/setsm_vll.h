@@ -420,6 +420,25 @@ int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, doubl
                              vll_point3 *d_pts, int64_t n_pts, const vll_tri *d_tris,
                              int64_t n_tris, vll_ugrid *d_gridpt3, int *rounds);
 
+/*
+ * SetHeightRange (setsm_code.cpp:9851-10255): the next iteration's height
+ * ranges from the TIN of matched points.  Every grid node inside a triangle
+ * takes the plane's height (the vertex height on a vertex at levels 0-1) and
+ * a range from the triangle's height extent plus a buffer set by the level,
+ * `iteration`, `mpp`, the triangle's slope and the node's Mean_ortho_ncc
+ * (a node is set by the first triangle, in order, that contains it); nodes in
+ * no triangle take their matched neighbours' range union.  gridpt3 is updated
+ * in place as the reference updates GridPT3 before freeing it; `result` (N
+ * records) receives the returned grid, *min_h_grid / *max_h_grid the range
+ * extent.  seed_dem_sigma is proinfo->seedDEMsigma (read with pre_DEMtif).
+ * Bit-exact with the reference for up to five images.
+ */
+int vll_set_height_range(vll_context *ctx, const vll_level_desc *desc, const vll_point3 *pts,
+                         int64_t n_pts, const vll_tri *tris, int64_t n_tris, vll_ugrid *gridpt3,
+                         vll_ugrid *result, int iteration, double mpp,
+                         int level_check_matching_rate, double seed_dem_sigma,
+                         double *min_h_grid, double *max_h_grid);
+
 /* Diagnostics: the orthoimage coordinate raster of image `ti`
  * (SetOrthoImageCoord, setsm_code.cpp:6550-6670) at resolution im_res, on
  * the matched level's pyramid (use_b = 0) or the blunder level's (1), as

@@ -231,6 +231,13 @@ int VerticalLineLocus_Ortho(ProjectInfo *proinfo, taglevelinfo &plevelinfo, doub
                             double *F_sncc);
 int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &plevelinfo, double MPP, tagD3DPoint *pts,
                   int numOfPts, tagUI3DPoint *tris, int numOfTri, UpdateGrid *GridPT3);
+// SetHeightRange (setsm_code.hpp:122), same behaviour: returns a new grid
+// (calloc) and frees GridPT3, which must come from malloc / calloc.
+UpdateGrid *SetHeightRange(ProjectInfo *proinfo, taglevelinfo &plevelinfo,
+                           tagNCCresult *nccresult, const int numOfPts, const int num_triangles,
+                           UpdateGrid *GridPT3, const int iteration, double *minH_grid,
+                           double *maxH_grid, tagD3DPoint *pts, const tagUI3DPoint *tris,
+                           const double MPP, const bool level_check_matching_rate);
 
 // The orthoimage-window variants (setsm_code.hpp:93, :95), same behaviour:
 // VerticalLineLocus_seeddem updates GridPT3; VerticalLineLocus_blunder

@@ -446,6 +446,31 @@ int ref_call_ortho_blunder(void *fn, const vll_level_desc *d, double mpp, vll_po
         reinterpret_cast<UI3DPOINT *>(tris), n_tris, reinterpret_cast<UGRID *>(gridpt3));
 }
 
+/* SetHeightRange (setsm_code.cpp:9851-10255) on a copy of gridpt3 (the
+ * reference frees its GridPT3); result and the extent {min, max} out. */
+typedef UGRID *(*set_height_range_signature)(ProInfo *, LevelInfo &, NCCresult *, const int,
+                                             const int, UGRID *, const int, double *, double *,
+                                             D3DPOINT *, const UI3DPOINT *, const double,
+                                             const bool);
+int ref_set_height_range(void *fn, const vll_level_desc *d, vll_point3 *pts, int n_pts,
+                         const vll_tri *tris, int n_tris, const vll_ugrid *gridpt3,
+                         vll_ugrid *result, int iteration, double mpp, int lcmr,
+                         double seed_sigma, double *extent) {
+    RefLevel L(d);
+    L.proinfo->seedDEMsigma = seed_sigma;
+    const long n = L.grid_length;
+    UGRID *g = (UGRID *)malloc(sizeof(UGRID) * (size_t)n);
+    memcpy(g, gridpt3, sizeof(UGRID) * (size_t)n);
+    set_height_range_signature f = fn ? reinterpret_cast<set_height_range_signature>(fn)
+                                      : &SetHeightRange;
+    UGRID *r = f(L.proinfo, L.li, nullptr, n_pts, n_tris, g, iteration, &extent[0], &extent[1],
+                 reinterpret_cast<D3DPOINT *>(pts), reinterpret_cast<const UI3DPOINT *>(tris),
+                 mpp, lcmr != 0);
+    memcpy(result, r, sizeof(UGRID) * (size_t)n);
+    free(r);
+    return 0;
+}
+
 /* SetOrthoImageCoord (setsm_code.cpp:6550-6670): the orthoimage coordinate
  * raster of image ti at im_res, OR (use_b = 0) or BD pyramid. */
 long ref_ortho_raster(const vll_level_desc *d, const vll_ugrid *gridpt3, int use_b, double im_res,

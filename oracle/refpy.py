@@ -364,3 +364,24 @@ def call_ortho_blunder(fn_addr: int, inputs, mpp: float, pts: np.ndarray, tris: 
         return int(L.ref_call_ortho_blunder(fn_addr, C.byref(d), float(mpp), pts.ctypes.data,
                                             len(pts), tris.ctypes.data, len(tris),
                                             inputs.gridpt3.ctypes.data))
+
+
+def set_height_range(inputs, pts, tris, iteration: int, mpp: float, lcmr: bool,
+                     seed_sigma: float = 0.0, fn_addr: int | None = None):
+    """SetHeightRange (setsm_code.cpp:9851-10255), or the function at
+    fn_addr with its signature (setsm_code.hpp:122); inputs.gridpt3 is left
+    unchanged.  Returns (result grid, (minH_grid, maxH_grid))."""
+    L = lib()
+    L.ref_set_height_range.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_void_p, C.c_int,
+                                       C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_double, C.c_int, C.c_double, C.c_void_p]
+    L.ref_set_height_range.restype = C.c_int
+    d = inputs.desc()
+    out = np.zeros(inputs.n, dtype=abi.UGRID_DTYPE)
+    ext = np.zeros(2)
+    with _StdoutToStderr():
+        L.ref_set_height_range(fn_addr, C.byref(d), pts.ctypes.data, len(pts), tris.ctypes.data,
+                               len(tris), inputs.gridpt3.ctypes.data, out.ctypes.data,
+                               int(iteration), float(mpp), int(bool(lcmr)), float(seed_sigma),
+                               ext.ctypes.data)
+    return out, (float(ext[0]), float(ext[1]))

@@ -1199,6 +1199,100 @@ int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, doubl
     return ortho_blunder_run(ctx, P, mpp, d_pts, n_pts, d_tris, n_tris, d_gridpt3, rounds);
 }
 
+// SetHeightRange's BufferOfHeight and th_HG (setsm_code.cpp:9863-9922).
+static void height_range_constants(const vll_level_desc *d, int iteration, double mpp, bool lcmr,
+                                   double seed_sigma, double *buffer, double *th_hg) {
+    const int L = d->pyramid_step;
+    double b = mpp * 4.0 * (double)(1 << L);
+    if (L == 1) {
+        b = iteration >= 2 ? mpp * 2 : mpp * 3;
+    } else if (L == 0) {
+        b = iteration == 1 ? mpp * 2 : mpp;
+        if (b < 0.5) b = 0.5;
+    }
+    if (d->pre_dem_tif && b > seed_sigma) b = seed_sigma;
+    b = ceil(b);
+    if (b > 100) b = 100;
+    double th = 100000;
+    if (d->dem_resolution >= 4) {
+        if (L <= 1) th = 1000;
+    } else {
+        if (!lcmr) {
+            if (L == 2 && iteration >= 5)
+                th = 1000;
+            else if (L == 1)
+                th = 500;
+            else if (L == 0)
+                th = 100;
+        } else if (L <= 2) {
+            th = 100;
+        }
+        if (L == 0 && d->dem_resolution < 2 && iteration > 1) th = 50;
+    }
+    *buffer = b;
+    *th_hg = th;
+}
+
+int vll_set_height_range(vll_context *ctx, const vll_level_desc *desc, const vll_point3 *pts,
+                         int64_t n_pts, const vll_tri *tris, int64_t n_tris, vll_ugrid *gridpt3,
+                         vll_ugrid *result, int iteration, double mpp,
+                         int level_check_matching_rate, double seed_dem_sigma,
+                         double *min_h_grid, double *max_h_grid) {
+    NvtxRange nvtx_range("vll_set_height_range");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !gridpt3 || !result || !min_h_grid || !max_h_grid || (n_pts > 0 && !pts) ||
+        (n_tris > 0 && !tris))
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    if (n_pts < 0 || n_tris < 0 || n_pts > 0x7fffffff || n_tris > 0x7fffffff)
+        return fail(ctx, VLL_ERR_INVALID, "point or triangle count out of range");
+    if (desc->grid_width <= 0 || desc->grid_height <= 0 || desc->pyramid_step < 0 ||
+        desc->pyramid_step > 12 || !(desc->grid_resolution > 0) || desc->num_images < 1 ||
+        desc->num_images > VLL_MAX_IMAGES)
+        return fail(ctx, VLL_ERR_INVALID, "invalid grid, level or image count");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    // only the grid geometry, the level and the image selection are read
+    DevLevel P;
+    memset(&P, 0, sizeof(P));
+    P.num_images = desc->num_images;
+    P.ref = desc->reference_id;
+    P.L = desc->pyramid_step;
+    P.grid_res = desc->grid_resolution;
+    P.im_res = desc->resolution * (double)(1 << P.L);
+    for (int i = 0; i < 4; ++i) P.boundary[i] = desc->boundary[i];
+    P.grid_w = desc->grid_width;
+    P.grid_h = desc->grid_height;
+    P.n_nodes = P.grid_w * P.grid_h;
+    for (int ti = 0; ti < P.num_images; ++ti) P.im[ti].selected = desc->images[ti].selected != 0;
+    const int64_t N = P.n_nodes;
+    int rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->tin_pts, pts, (size_t)n_pts * sizeof(vll_point3)))) return rc;
+    if ((rc = upload(ctx, ctx->tin_tris, tris, (size_t)n_tris * sizeof(vll_tri)))) return rc;
+    // triangles with a vertex index >= n_pts are skipped, as the reference does;
+    // bounding boxes are clamped to the grid, so every node index is in range
+    VLL_CUDA(ctx, ensure(ctx->ncc, (size_t)N * sizeof(vll_ugrid)));
+    const size_t bytes = vll::height_range_scratch(N);
+    VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
+    P.gp3 = (const vll_ugrid *)ctx->gp3.p;
+    if ((rc = upload_level_block(ctx, P))) return rc;
+    double buffer, th_hg;
+    height_range_constants(desc, iteration, mpp, level_check_matching_rate != 0, seed_dem_sigma,
+                           &buffer, &th_hg);
+    VLL_CUDA(ctx, vll::run_height_range((const DevLevel *)ctx->level.p, P,
+                                        (const vll_point3 *)ctx->tin_pts.p, n_pts,
+                                        (const vll_tri *)ctx->tin_tris.p, n_tris,
+                                        (vll_ugrid *)ctx->gp3.p, (vll_ugrid *)ctx->ncc.p, buffer,
+                                        th_hg, iteration, ctx->tin_scratch.p, bytes, min_h_grid,
+                                        max_h_grid, ctx->stream));
+    ctx->launches_total += (n_tris > 0 ? 6 : 5);
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(result, ctx->ncc.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
 int vll_debug_ortho_raster(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,
                            int use_b, double im_res, int ti, double *out, int64_t capacity,
                            int64_t *width, int64_t *height) {

@@ -1,5 +1,6 @@
 // vll_ddmath.cuh -- correctly rounded double-precision sin, cos, tan, atan,
-// atan2 and exp for the map projection of the orthoimage rasters.
+// atan2, acos and exp for the map projection of the orthoimage rasters and the
+// TIN geometry.
 //
 // The host code these kernels reproduce (ps2wgs_single,
 // CoordConversion.cpp:396-490) calls the C library's functions; glibc 2.39
@@ -18,8 +19,8 @@
 //    |r| <= pi/4 by Horner's scheme in double-double.
 //  * exp: x reduced by k * ln 2 (three doubles), Taylor series on
 //    |r| <= ln2 / 2, scaled by 2^k.
-//  * atan / atan2: one Newton step on g(t) = x sin t - y cos t from the
-//    hardware estimate, with g evaluated in double-double; the step has
+//  * atan / atan2 / acos: one Newton step (on g(t) = x sin t - y cos t, or
+//    cos t - x) from the hardware estimate, with g evaluated in double-double; the step has
 //    quadratic convergence, so the corrected angle is good to ~2^-100.
 //
 // Arguments outside the ranges the projection produces (|x| >= 2^20 for the
@@ -272,6 +273,18 @@ VLL_HD double newton_angle(double t0, double sy, double cx) {
     if (!(gp != 0.0)) return t0;
     const double corr = -div(add(g.hi, g.lo), gp);
     return add(t0, corr);
+}
+
+// acos by one Newton step on g(t) = cos t - x (g' = -sin t) from the
+// hardware estimate; the endpoints and |x| > 1 return the hardware result.
+VLL_HD double acos_cr(double x) {
+    const double t0 = acos(x);
+    if (!(fabs(x) < 1.0)) return t0;
+    dd s, c;
+    sincos_dd(t0, s, c);
+    const dd g = dd_sub(c, dd{x, 0.0});
+    if (!(s.hi != 0.0)) return t0;
+    return add(t0, div(add(g.hi, g.lo), s.hi));
 }
 
 VLL_HD double atan_cr(double x) {

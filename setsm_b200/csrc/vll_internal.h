@@ -47,6 +47,15 @@ cudaError_t launch_blunder(const DevLevel *dP, int64_t n_nodes, double2 *const *
                            int64_t oh, double im_res, int H, vll_ugrid *gout, float *ncc_out,
                            cudaStream_t s);
 
+// vll_heightrange.cu: SetHeightRange on device data (gp3 updated in place,
+// out = the returned grid); waits and returns the grid's height extent.
+size_t height_range_scratch(int64_t n_nodes);
+cudaError_t run_height_range(const DevLevel *dP, const DevLevel &hP, const vll_point3 *pts,
+                             int64_t n_pts, const vll_tri *tris, int64_t n_tris, vll_ugrid *gp3,
+                             vll_ugrid *out, double buffer, double th_hg, int iteration,
+                             void *scratch, size_t scratch_bytes, double *min_h, double *max_h,
+                             cudaStream_t s);
+
 // vll_orthotin.cu: VerticalLineLocus_Ortho (one triangle; d_out = {F_Height,
 // F_sncc, selected count}) and Ortho_blunder on device data.
 cudaError_t launch_ortho_search(const DevLevel *dP, double mpp, const vll_point3 *d_pts3,

@@ -235,6 +235,41 @@ int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &pl, double MPP, tagD3DPoin
     return numOfPts;
 }
 
+UpdateGrid *SetHeightRange(ProjectInfo *proinfo, taglevelinfo &pl, tagNCCresult *nccresult,
+                           const int numOfPts, const int num_triangles, UpdateGrid *GridPT3,
+                           const int iteration, double *minH_grid, double *maxH_grid,
+                           tagD3DPoint *pts, const tagUI3DPoint *tris, const double MPP,
+                           const bool level_check_matching_rate) {
+    (void)nccresult;   // not read by the reference either
+    vll_context *ctx = shim_context();
+    vll_level_desc d;
+    memset(&d, 0, sizeof(d));
+    d.num_images = proinfo->number_of_images;
+    d.reference_id = pl.reference_id;
+    d.pyramid_step = *pl.Pyramid_step;
+    d.pre_dem_tif = proinfo->pre_DEMtif;
+    d.resolution = proinfo->resolution;
+    d.dem_resolution = proinfo->DEM_resolution;
+    d.grid_resolution = *pl.grid_resolution;
+    for (int i = 0; i < 4; ++i) d.boundary[i] = pl.Boundary[i];
+    d.grid_width = pl.Size_Grid2D->width;
+    d.grid_height = pl.Size_Grid2D->height;
+    for (int ti = 0; ti < d.num_images && ti < VLL_MAX_IMAGES; ++ti)
+        d.images[ti].selected = proinfo->check_selected_image[ti] ? 1 : 0;
+    const int64_t n = d.grid_width * d.grid_height;
+    UpdateGrid *result = (UpdateGrid *)calloc((size_t)n, sizeof(UpdateGrid));
+    if (!result) die("SetHeightRange: out of memory", nullptr);
+    if (vll_set_height_range(ctx, &d, reinterpret_cast<const vll_point3 *>(pts), numOfPts,
+                             reinterpret_cast<const vll_tri *>(tris), num_triangles,
+                             reinterpret_cast<vll_ugrid *>(GridPT3),
+                             reinterpret_cast<vll_ugrid *>(result), iteration, MPP,
+                             level_check_matching_rate ? 1 : 0, proinfo->seedDEMsigma, minH_grid,
+                             maxH_grid) != VLL_OK)
+        die("SetHeightRange: GPU call failed", vll_last_error(ctx));
+    free(GridPT3);
+    return result;
+}
+
 extern "C" int vll_compat_layout(int64_t *out, int cap) {
     const int64_t v[] = {
         (int64_t)sizeof(ProjectInfo),

@@ -34,6 +34,7 @@ EXPORTED = [
     "vll_vertical_line_locus_seeddem", "vll_vertical_line_locus_seeddem_device",
     "vll_vertical_line_locus_blunder", "vll_vertical_line_locus_blunder_device",
     "vll_vertical_line_locus_ortho", "vll_ortho_blunder", "vll_ortho_blunder_device",
+    "vll_set_height_range",
 ]
 
 _lib = None
@@ -99,6 +100,8 @@ def load():
                                                 vp]
     L.vll_ortho_blunder.argtypes = [vp, D, C.c_double, vp, i64, vp, i64, vp, vp]
     L.vll_ortho_blunder_device.argtypes = [vp, D, C.c_double, vp, i64, vp, i64, vp, vp]
+    L.vll_set_height_range.argtypes = [vp, D, vp, i64, vp, i64, vp, vp, i32, C.c_double, i32,
+                                       C.c_double, vp, vp]
     _lib = L
     return L
 
@@ -257,6 +260,21 @@ class Context:
                                              len(pts), tris.ctypes.data, len(tris),
                                              inputs.gridpt3.ctypes.data, C.byref(rounds)))
         return rounds.value
+
+    def set_height_range(self, inputs, pts: np.ndarray, tris: np.ndarray, iteration: int,
+                         mpp: float, level_check_matching_rate: bool,
+                         seed_dem_sigma: float = 0.0):
+        """SetHeightRange (setsm_code.cpp:9851-10255): updates inputs.gridpt3
+        in place and returns (the new grid, (minH_grid, maxH_grid))."""
+        d = inputs.desc()
+        out = np.zeros(inputs.n, dtype=abi.UGRID_DTYPE)
+        lo, hi = C.c_double(), C.c_double()
+        self._check(load().vll_set_height_range(
+            self._h, C.byref(d), pts.ctypes.data, len(pts), tris.ctypes.data, len(tris),
+            inputs.gridpt3.ctypes.data, out.ctypes.data, int(iteration), float(mpp),
+            int(bool(level_check_matching_rate)), float(seed_dem_sigma), C.byref(lo),
+            C.byref(hi)))
+        return out, (lo.value, hi.value)
 
     def ortho_blunder_device(self, desc, mpp: float, d_pts: int, n_pts: int, d_tris: int,
                              n_tris: int, d_gridpt3: int) -> int:

@@ -124,6 +124,22 @@ def make_tin_case(*, seed=9, size=512, nodes=32, res=8.0, template=11, L=0, poin
     return inp, pts, delaunay(pts)
 
 
+def make_range_case(*, seed=13, flag4_frac=0.2, unmatched_frac=0.2, **kw):
+    """Inputs of SetHeightRange: make_tin_case's points and TIN, with the
+    UGRID fields it reads varied: Matched_flag 0 / 1 / 4 and Mean_ortho_ncc
+    over [-1, 1]."""
+    inp, pts, tris = make_tin_case(seed=seed, **kw)
+    rng = np.random.default_rng(seed + 57)
+    g = inp.gridpt3
+    n = len(g)
+    r = rng.random(n)
+    g["Matched_flag"] = np.where(r < unmatched_frac, 0, np.where(r < unmatched_frac + flag4_frac,
+                                                                   4, 1))
+    g["Mean_ortho_ncc"] = rng.integers(-1000, 1000, n).astype(np.int16)
+    g["roh"] = rng.integers(-1000, 1000, n).astype(np.int16)
+    return inp, pts, tris
+
+
 def delaunay(pts):
     """Triangles (abi.TRI_DTYPE) of the Delaunay triangulation of the points'
     x, y (scipy's Qhull) -- a stand-in for the matcher's own TIN."""

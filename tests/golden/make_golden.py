@@ -77,6 +77,34 @@ GOLDEN_TIN = {
 }
 
 
+# SetHeightRange (setsm_code.cpp:9851-10255): kwargs of
+# tests/cases.py:make_range_case and the call's iteration / MPP / level
+# check_matching_rate / pre_DEMtif and seedDEMsigma.  It reads no image, so
+# the fixture keeps every input it reads (grid geometry, points, triangles,
+# UGRID).
+GOLDEN_RANGE = {
+    "range_l0": dict(iteration=1, mpp=1.5, lcmr=False, case=dict(seed=13)),
+    "range_l3": dict(iteration=2, mpp=2.0, lcmr=True,
+                     case=dict(seed=14, L=3, res=24.0, template=15, nodes=16)),
+    "range_l1_seed": dict(iteration=3, mpp=1.0, lcmr=False, pre_dem=True, sigma=2.5,
+                          case=dict(seed=15, L=1, res=12.0, template=15, nodes=24, n_images=3)),
+}
+
+
+def range_case(name):
+    """(inputs, pts, tris, fixture arrays) of SetHeightRange fixture `name`."""
+    from setsm_b200 import abi
+    from tests import cases
+    z = np.load(fixture_path(name))
+    v = GOLDEN_RANGE[name]
+    inp, _, _ = cases.make_range_case(**v["case"])
+    inp.boundary = z["boundary"].copy()
+    inp.grid_resolution = float(z["grid_resolution"])
+    inp.pre_dem_tif = bool(v.get("pre_dem", False))
+    inp.gridpt3 = z["init_gp3"].view(abi.UGRID_DTYPE).copy()
+    return inp, z["pts"].view(abi.POINT3_DTYPE).copy(), z["tris"].view(abi.TRI_DTYPE).copy(), z
+
+
 def tin_case(name):
     """(inputs, pts, tris, fixture arrays) of TIN fixture `name`: images from
     the seeded case, RPCs, points, triangles and UGRID from the fixture."""
@@ -194,6 +222,20 @@ def main(only=None) -> None:
         arrays["pts"] = clean(pts).view(np.uint8)
         np.savez_compressed(fixture_path(name), **arrays)
         print(f"{name}: {os.path.getsize(fixture_path(name))} bytes")
+
+    for name, v in GOLDEN_RANGE.items():
+        if only and name not in only:
+            continue
+        inp, pts, tris = cases.make_range_case(**v["case"])
+        inp.pre_dem_tif = bool(v.get("pre_dem", False))
+        out, ext = refpy.set_height_range(inp, pts, tris, v["iteration"], v["mpp"], v["lcmr"],
+                                          v.get("sigma", 0.0))
+        np.savez_compressed(fixture_path(name), boundary=np.asarray(inp.boundary),
+                            grid_resolution=np.array(inp.grid_resolution),
+                            init_gp3=clean(inp.gridpt3).view(np.uint8),
+                            pts=clean(pts).view(np.uint8), tris=tris.view(np.uint8),
+                            result=clean(out).view(np.uint8), extent=np.array(ext))
+        print(f"{name}: extent {ext}, {os.path.getsize(fixture_path(name))} bytes")
 
 
 if __name__ == "__main__":

@@ -19,8 +19,8 @@ int main(int argc, char **argv) {
     std::uniform_real_distribution<double> u(0.0, 1.0);
     auto logu = [&](double lo, double hi) { return lo * std::pow(hi / lo, u(rng)); };
     auto sgn = [&]() { return u(rng) < 0.5 ? -1.0 : 1.0; };
-    long bad[6] = {0}, cnt[6] = {0};
-    const char *names[6] = {"sin", "cos", "tan", "atan", "atan2", "exp"};
+    long bad[7] = {0}, cnt[7] = {0};
+    const char *names[7] = {"sin", "cos", "tan", "atan", "atan2", "exp", "acos"};
     auto note = [&](int f, double ours, double lib, double x, double y, bool two) {
         cnt[f]++;
         if (ours == lib) return;
@@ -43,7 +43,9 @@ int main(int argc, char **argv) {
         note(4, atan2_cr(y, xx), std::atan2(y, xx), y, xx, true);
         const double e = u(rng) < 0.5 ? (u(rng) * 2 - 1) * 3.0 : (u(rng) * 2 - 1) * 700.0;
         note(5, exp_cr(e), std::exp(e), e, 0, false);
+        const double ac = u(rng) < 0.5 ? (u(rng) * 2 - 1) : sgn() * (1.0 - logu(1e-12, 1e-2));
+        note(6, acos_cr(ac), std::acos(ac), ac, 0, false);
     }
-    for (int f = 0; f < 6; ++f) printf("count %s %ld %ld\n", names[f], cnt[f], bad[f]);
+    for (int f = 0; f < 7; ++f) printf("count %s %ld %ld\n", names[f], cnt[f], bad[f]);
     return 0;
 }

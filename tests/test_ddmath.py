@@ -1,4 +1,4 @@
-"""The correctly rounded sin / cos / tan / atan / atan2 / exp of
+"""The correctly rounded sin / cos / tan / atan / atan2 / acos / exp of
 setsm_b200/csrc/vll_ddmath.cuh (used by the orthoimage rasters' map
 projection), compiled for the host: against the C library they differ on
 about 0.1% of the arguments, and at every such argument checked, the header's
@@ -32,7 +32,7 @@ def test_mismatch_rate_against_the_c_library(check_output):
         f = line.split()
         if f[0] == "count":
             counts[f[1]] = (int(f[2]), int(f[3]))
-    assert set(counts) == {"sin", "cos", "tan", "atan", "atan2", "exp"}
+    assert set(counts) == {"sin", "cos", "tan", "atan", "atan2", "exp", "acos"}
     for name, (n, bad) in counts.items():
         assert n >= 100000
         assert bad / n < 0.003, (name, bad, n)
@@ -42,7 +42,7 @@ def test_every_mismatch_is_the_library_misrounding(check_output):
     mpmath = pytest.importorskip("mpmath")
     mpmath.mp.prec = 300
     fns = {"sin": mpmath.sin, "cos": mpmath.cos, "tan": mpmath.tan, "atan": mpmath.atan,
-           "exp": mpmath.exp}
+           "exp": mpmath.exp, "acos": mpmath.acos}
     checked = 0
     for line in check_output.splitlines():
         f = line.split()

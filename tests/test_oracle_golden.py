@@ -103,3 +103,17 @@ def test_tin_fixtures_are_the_reference_output(name):
     refpy.ortho_blunder(inp, mg.GOLDEN_TIN[name]["mpp"], pts, tris)
     assert np.array_equal(mg.clean(pts).view(np.uint8), z["pts"])
     assert np.array_equal(mg.clean(inp.gridpt3).view(np.uint8), z["gp3"])
+
+
+@pytest.mark.skipif(not __import__("oracle.refpy").refpy.available(),
+                    reason="reference build not available")
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_RANGE))
+def test_range_fixtures_are_the_reference_output(name):
+    from oracle import refpy
+    from setsm_b200 import abi
+    v = mg.GOLDEN_RANGE[name]
+    inp, pts, tris, z = mg.range_case(name)
+    out, ext = refpy.set_height_range(inp, pts, tris, v["iteration"], v["mpp"], v["lcmr"],
+                                      v.get("sigma", 0.0))
+    assert np.array_equal(mg.clean(out).view(np.uint8), z["result"])
+    assert ext == tuple(z["extent"])
