@@ -827,6 +827,76 @@ def run_height_range(args):
     del torch
 
 
+def run_select_mps(args):
+    """SelectMPs (setsm_code.cpp:8535-8895) on the reduced C2 scene: the
+    peaks of the 7x7 memory-tight matching (split kernel) of its 1024^2 grid,
+    level 0, iteration 1, its UGRID.  GPU: the C ABI on host buffers (host
+    wall clock of the call, copies included: the call waits); CPU: the
+    reference's SelectMPs (sequential); points and UGRID compared.  Metric:
+    grid nodes per second."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import copy
+    import torch
+    from oracle import refpy
+    from setsm_b200 import vll, workloads
+    from tests.cases import field_mismatch
+    ctx = vll.Context(0)
+    wl = workloads.build("c2_small", ctx, device="cuda:0", seed=1)
+    inp = wl.host_inputs(11)
+    ncc = inp.new_nccresult()
+    ctx.vertical_line_locus(inp, ncc, None, "split")
+    g0 = inp.gridpt3.copy()
+    sel_args = (0.6, 0.2, 0.8, 0.7, 1, 1.5, 1, 10.0)
+
+    def call():
+        inp.gridpt3 = g0.copy()
+        t = time.perf_counter()
+        pts = ctx.select_mps(inp, ncc, *sel_args)
+        return (time.perf_counter() - t) * 1e3, pts
+    for _ in range(max(1, args.warmup)):
+        call()
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    lc0 = vll.load().vll_launch_count(ctx._h)
+    for _ in range(args.steps):
+        ms, pts = call()
+        times.append(ms)
+    launches = vll.load().vll_launch_count(ctx._h) - lc0
+    clk = clocks.stop()
+    ms = statistics.median(times)
+    ref = copy.copy(inp)
+    ref.gridpt3 = g0.copy()
+    t = time.perf_counter()
+    _, want = refpy.select_mps(ref, ncc, *sel_args)
+    cpu_s = time.perf_counter() - t
+    same = len(pts) == len(want) and all(np.array_equal(pts[f], want[f])
+                                         for f in ("x", "y", "z", "flag"))
+    n = int(inp.n)
+    line = {
+        "metric": "grid nodes/s (SelectMPs)", "value": n / (ms / 1e3), "unit": "nodes/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (the reference's arithmetic)", "data": "synthetic",
+        "config": {"workload": "SelectMPs: peaks of the 7x7 memory-tight matching of the reduced "
+                               "C2 scene (1024^2 grid), level 0, iteration 1",
+                   "nodes": n, "points": int(len(pts))},
+        "e2e": {"value": n / (ms / 1e3), "unit": "nodes/s",
+                "timing": "host wall clock of the C-ABI call on host buffers (the call waits)"},
+        "cpu_baseline": {"value": n / cpu_s, "unit": "nodes/s", "cores": 1, "kind": "reference",
+                         "sample": f"whole grid, {cpu_s:.3f} s (the reference's loop is serial)"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "parity": {"points_identical": bool(same),
+                   "ugrid_field_mismatch": field_mismatch(inp.gridpt3, ref.gridpt3)},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    del torch
+
+
 def run_ortho_tin(args):
     """Ortho_blunder (TIN-triangle orthoimage height search, setsm_code.cpp:
     8028-8533) on the reduced C2 scene (4096^2 pair at 0.5 m, 1024^2 grid at
@@ -974,7 +1044,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
                     choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm", "seeddem",
-                             "blunder", "ortho_tin", "height_range"])
+                             "blunder", "ortho_tin", "height_range", "select_mps"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -1007,6 +1077,8 @@ def main():
         run_ortho_tin(args)
     elif args.config == "height_range":
         run_height_range(args)
+    elif args.config == "select_mps":
+        run_select_mps(args)
     else:
         run_ours(args)
 

@@ -421,6 +421,24 @@ int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, doubl
                              int64_t n_tris, vll_ugrid *d_gridpt3, int *rounds);
 
 /*
+ * SelectMPs (setsm_code.cpp:8535-8895): the matched points of an iteration.
+ * At levels > 0 the first-peak correlations of the nodes with more than two
+ * heights set the minimum threshold (a 100-bin histogram against the level's
+ * quota); every node's peaks (nccresult) and UGRID then decide whether it
+ * yields a point, update its roh, and at matched nodes with ambiguous peaks
+ * widen its range (Matched_flag 4).  The points (x, y of grid_pts, z = first
+ * peak height, flag 0) go to points[] in node order, *count receives their
+ * number; with *count > capacity the call returns VLL_ERR_CAPACITY and leaves
+ * gridpt3 and points untouched.  The other arguments are the reference's.
+ * Host buffers; bit-exact with the reference.
+ */
+int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccresult *nccresult,
+                   vll_ugrid *gridpt3, double th_roh, double th_roh_min, double th_roh_start,
+                   double th_roh_next, int iteration, double mpp, int final_level_iteration,
+                   double mpp_stereo_angle, vll_point3 *points, int64_t capacity,
+                   int64_t *count);
+
+/*
  * SetHeightRange (setsm_code.cpp:9851-10255): the next iteration's height
  * ranges from the TIN of matched points.  Every grid node inside a triangle
  * takes the plane's height (the vertex height on a vertex at levels 0-1) and

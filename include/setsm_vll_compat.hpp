@@ -16,6 +16,7 @@
 #define SETSM_VLL_COMPAT_HPP
 
 #include <cstdint>
+#include <vector>
 
 #include "setsm_vll.h"
 
@@ -231,6 +232,13 @@ int VerticalLineLocus_Ortho(ProjectInfo *proinfo, taglevelinfo &plevelinfo, doub
                             double *F_sncc);
 int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &plevelinfo, double MPP, tagD3DPoint *pts,
                   int numOfPts, tagUI3DPoint *tris, int numOfTri, UpdateGrid *GridPT3);
+// SelectMPs (setsm_code.hpp:99), same behaviour: appends the matched points
+// to *linkedlist, updates GridPT3, returns their number.
+long SelectMPs(const ProjectInfo *proinfo, taglevelinfo &plevelinfo,
+               const tagNCCresult *roh_height, UpdateGrid *GridPT3, const double Th_roh,
+               const double Th_roh_min, const double Th_roh_start, const double Th_roh_next,
+               const int iteration, const double MPP, const int final_level_iteration,
+               const double MPP_stereo_angle, std::vector<tagD3DPoint> *linkedlist);
 // SetHeightRange (setsm_code.hpp:122), same behaviour: returns a new grid
 // (calloc) and frees GridPT3, which must come from malloc / calloc.
 UpdateGrid *SetHeightRange(ProjectInfo *proinfo, taglevelinfo &plevelinfo,

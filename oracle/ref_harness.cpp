@@ -446,6 +446,32 @@ int ref_call_ortho_blunder(void *fn, const vll_level_desc *d, double mpp, vll_po
         reinterpret_cast<UI3DPOINT *>(tris), n_tris, reinterpret_cast<UGRID *>(gridpt3));
 }
 
+/* SelectMPs (setsm_code.cpp:8535-8895), or the function at `fn` with its
+ * signature; gridpt3 in/out, up to cap points out; returns its value. */
+typedef long (*select_mps_signature)(const ProInfo *, LevelInfo &, const NCCresult *, UGRID *,
+                                     const double, const double, const double, const double,
+                                     const int, const double, const int, const double,
+                                     vector<D3DPOINT> *);
+long ref_select_mps(void *fn, const vll_level_desc *d, const vll_nccresult *ncc,
+                    vll_ugrid *gridpt3, const double *params, const int *iparams,
+                    vll_point3 *out, long cap, long *n_out) {
+    RefLevel L(d);
+    vector<D3DPOINT> v;
+    select_mps_signature f = fn ? reinterpret_cast<select_mps_signature>(fn) : &SelectMPs;
+    const long r = f(L.proinfo, L.li, reinterpret_cast<const NCCresult *>(ncc),
+                     reinterpret_cast<UGRID *>(gridpt3), params[0], params[1], params[2],
+                     params[3], iparams[0], params[4], iparams[1], params[5], &v);
+    *n_out = (long)v.size();
+    for (size_t i = 0; i < v.size() && (long)i < cap; ++i) {
+        memset(&out[i], 0, sizeof(vll_point3));
+        out[i].x = v[i].m_X;
+        out[i].y = v[i].m_Y;
+        out[i].z = v[i].m_Z;
+        out[i].flag = v[i].flag;
+    }
+    return r;
+}
+
 /* SetHeightRange (setsm_code.cpp:9851-10255) on a copy of gridpt3 (the
  * reference frees its GridPT3); result and the extent {min, max} out. */
 typedef UGRID *(*set_height_range_signature)(ProInfo *, LevelInfo &, NCCresult *, const int,

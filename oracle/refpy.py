@@ -385,3 +385,26 @@ def set_height_range(inputs, pts, tris, iteration: int, mpp: float, lcmr: bool,
                                int(iteration), float(mpp), int(bool(lcmr)), float(seed_sigma),
                                ext.ctypes.data)
     return out, (float(ext[0]), float(ext[1]))
+
+
+def select_mps(inputs, ncc, th_roh, th_roh_min, th_roh_start, th_roh_next, iteration, mpp,
+               final_level_iteration, mpp_stereo_angle, fn_addr: int | None = None):
+    """SelectMPs (setsm_code.cpp:8535-8895), or the function at fn_addr with
+    its signature (setsm_code.hpp:99); inputs.gridpt3 updated in place.
+    Returns (return value, points)."""
+    L = lib()
+    L.ref_select_mps.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_long,
+                                 C.POINTER(C.c_long)]
+    L.ref_select_mps.restype = C.c_long
+    d = inputs.desc()
+    params = np.array([th_roh, th_roh_min, th_roh_start, th_roh_next, mpp, mpp_stereo_angle],
+                      dtype=np.float64)
+    iparams = np.array([iteration, final_level_iteration], dtype=np.int32)
+    out = np.zeros(inputs.n, dtype=abi.POINT3_DTYPE)
+    n = C.c_long()
+    with _StdoutToStderr():
+        r = L.ref_select_mps(fn_addr, C.byref(d), ncc.ctypes.data, inputs.gridpt3.ctypes.data,
+                             params.ctypes.data, iparams.ctypes.data, out.ctypes.data, len(out),
+                             C.byref(n))
+    return int(r), out[: n.value].copy()

@@ -1199,6 +1199,103 @@ int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, doubl
     return ortho_blunder_run(ctx, P, mpp, d_pts, n_pts, d_tris, n_tris, d_gridpt3, rounds);
 }
 
+int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccresult *nccresult,
+                   vll_ugrid *gridpt3, double th_roh, double th_roh_min, double th_roh_start,
+                   double th_roh_next, int iteration, double mpp, int final_level_iteration,
+                   double mpp_stereo_angle, vll_point3 *points, int64_t capacity,
+                   int64_t *count) {
+    NvtxRange nvtx_range("vll_select_mps");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !nccresult || !gridpt3 || !count || !desc->grid_pts ||
+        (capacity > 0 && !points) || capacity < 0)
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    if (desc->grid_width <= 0 || desc->grid_height <= 0 ||
+        desc->grid_width * desc->grid_height > 0x7fffffff)
+        return fail(ctx, VLL_ERR_INVALID, "invalid grid size");
+    const int L = desc->pyramid_step;
+    const bool is_ra = desc->is_ra != 0;
+    // the level's quota of the histogram; unset in the reference above level 4
+    double min_roh_th = 0;
+    bool quota = true;
+    if (L == 4)
+        min_roh_th = 0.05 + (iteration - 1) * 0.01;
+    else if (L == 3)
+        min_roh_th = 0.15 + (iteration - 1) * 0.01;
+    else if (L == 2)
+        min_roh_th = 0.60;
+    else if (L == 1)
+        min_roh_th = 0.80;
+    else
+        quota = false;
+    if (L <= desc->sgm_py) {
+        min_roh_th = 0.95 - L * 0.1;
+        if (min_roh_th < 0.5) min_roh_th = 0.5;
+        quota = true;
+    }
+    if (!is_ra && L > 0 && !quota)
+        return fail(ctx, VLL_ERR_UNSUPPORTED, "SelectMPs threshold undefined above level 4");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int64_t N = desc->grid_width * desc->grid_height;
+    int rc;
+    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
+    const size_t bytes = vll::select_mps_scratch(N);
+    VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
+    VLL_CUDA(ctx, ensure(ctx->tin_pts, (size_t)(capacity > 0 ? capacity : 1) * sizeof(vll_point3)));
+    double minimum_th = 0.2;
+    if (!is_ra && L > 0) {
+        int hist[100];
+        int64_t total = 0;
+        VLL_CUDA(ctx, vll::run_roh_hist((const vll_nccresult *)ctx->ncc.p, N, ctx->tin_scratch.p,
+                                        hist, &total, ctx->stream));
+        ctx->launches_total += 1;
+        if (total > 0) {
+            int roh_iter = 99;
+            int sum = 0;
+            while (roh_iter > 0) {
+                sum += hist[roh_iter];
+                if (sum / (double)total > min_roh_th) {
+                    minimum_th = (double)roh_iter / (double)100;
+                    break;
+                }
+                --roh_iter;
+            }
+            if (minimum_th > 0.95) minimum_th = 0.95;
+        }
+    }
+    vll::SelectArgs a;
+    a.pyramid_step = L;
+    a.iteration = iteration;
+    a.final_level_iteration = final_level_iteration;
+    if (L <= 3 || is_ra)
+        a.check_iter_end = th_roh - 0.10 < th_roh_min;
+    else
+        a.check_iter_end = th_roh - 0.06 < th_roh_min;
+    a.minimum_th = minimum_th;
+    a.th_roh = th_roh;
+    a.th_roh_start = th_roh_start;
+    a.th_roh_next = th_roh_next;
+    a.mpp = mpp;
+    a.mpp_stereo_angle = mpp_stereo_angle;
+    int64_t n_sel = 0;
+    VLL_CUDA(ctx, vll::run_select_mps((const vll_nccresult *)ctx->ncc.p, (vll_ugrid *)ctx->gp3.p,
+                                      (const double *)ctx->pts.p, N, a, ctx->tin_scratch.p,
+                                      (vll_point3 *)ctx->tin_pts.p, capacity, &n_sel,
+                                      ctx->stream));
+    ctx->launches_total += 2;
+    *count = n_sel;
+    if (n_sel > capacity)
+        return fail(ctx, VLL_ERR_CAPACITY, "more selected points than the points buffer holds");
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    if (n_sel > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(points, ctx->tin_pts.p, (size_t)n_sel * sizeof(vll_point3),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
 // SetHeightRange's BufferOfHeight and th_HG (setsm_code.cpp:9863-9922).
 static void height_range_constants(const vll_level_desc *d, int iteration, double mpp, bool lcmr,
                                    double seed_sigma, double *buffer, double *th_hg) {

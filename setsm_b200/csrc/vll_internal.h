@@ -47,6 +47,21 @@ cudaError_t launch_blunder(const DevLevel *dP, int64_t n_nodes, double2 *const *
                            int64_t oh, double im_res, int H, vll_ugrid *gout, float *ncc_out,
                            cudaStream_t s);
 
+// vll_selectmps.cu: SelectMPs.  run_roh_hist fills the 100-bin histogram of
+// the first-peak correlations (and the node count behind it); run_select_mps
+// decides every node, updates gp3 and writes the selected points in node
+// order to out (when *count <= cap).  Both wait.
+struct SelectArgs {
+    int pyramid_step, iteration, final_level_iteration, check_iter_end;
+    double minimum_th, th_roh, th_roh_start, th_roh_next, mpp, mpp_stereo_angle;
+};
+size_t select_mps_scratch(int64_t n_nodes);
+cudaError_t run_roh_hist(const vll_nccresult *ncc, int64_t n, void *scratch, int *hist_out,
+                         int64_t *total_out, cudaStream_t s);
+cudaError_t run_select_mps(const vll_nccresult *ncc, vll_ugrid *gp3, const double *grid_pts,
+                           int64_t n, const SelectArgs &a, void *scratch, vll_point3 *out,
+                           int64_t cap, int64_t *count, cudaStream_t s);
+
 // vll_heightrange.cu: SetHeightRange on device data (gp3 updated in place,
 // out = the returned grid); waits and returns the grid's height extent.
 size_t height_range_scratch(int64_t n_nodes);

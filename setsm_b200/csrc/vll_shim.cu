@@ -235,6 +235,40 @@ int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &pl, double MPP, tagD3DPoin
     return numOfPts;
 }
 
+long SelectMPs(const ProjectInfo *proinfo, taglevelinfo &pl, const tagNCCresult *roh_height,
+               UpdateGrid *GridPT3, const double Th_roh, const double Th_roh_min,
+               const double Th_roh_start, const double Th_roh_next, const int iteration,
+               const double MPP, const int final_level_iteration, const double MPP_stereo_angle,
+               std::vector<tagD3DPoint> *linkedlist) {
+    vll_context *ctx = shim_context();
+    vll_level_desc d;
+    memset(&d, 0, sizeof(d));
+    d.num_images = proinfo->number_of_images;
+    d.pyramid_step = *pl.Pyramid_step;
+    d.is_ra = proinfo->IsRA;
+    d.sgm_py = proinfo->SGM_py;
+    d.grid_width = pl.Size_Grid2D->width;
+    d.grid_height = pl.Size_Grid2D->height;
+    d.grid_pts = reinterpret_cast<const double *>(pl.GridPts);
+    const int64_t n = d.grid_width * d.grid_height;
+    std::vector<vll_point3> pts((size_t)(n > 0 ? n : 1));
+    int64_t count = 0;
+    if (vll_select_mps(ctx, &d, reinterpret_cast<const vll_nccresult *>(roh_height),
+                       reinterpret_cast<vll_ugrid *>(GridPT3), Th_roh, Th_roh_min, Th_roh_start,
+                       Th_roh_next, iteration, MPP, final_level_iteration, MPP_stereo_angle,
+                       pts.data(), n, &count) != VLL_OK)
+        die("SelectMPs: GPU call failed", vll_last_error(ctx));
+    for (int64_t i = 0; i < count; ++i) {
+        tagD3DPoint p;
+        p.m_X = pts[(size_t)i].x;
+        p.m_Y = pts[(size_t)i].y;
+        p.m_Z = pts[(size_t)i].z;
+        p.flag = pts[(size_t)i].flag;
+        linkedlist->push_back(p);
+    }
+    return (long)count;
+}
+
 UpdateGrid *SetHeightRange(ProjectInfo *proinfo, taglevelinfo &pl, tagNCCresult *nccresult,
                            const int numOfPts, const int num_triangles, UpdateGrid *GridPT3,
                            const int iteration, double *minH_grid, double *maxH_grid,

@@ -34,7 +34,7 @@ EXPORTED = [
     "vll_vertical_line_locus_seeddem", "vll_vertical_line_locus_seeddem_device",
     "vll_vertical_line_locus_blunder", "vll_vertical_line_locus_blunder_device",
     "vll_vertical_line_locus_ortho", "vll_ortho_blunder", "vll_ortho_blunder_device",
-    "vll_set_height_range",
+    "vll_set_height_range", "vll_select_mps",
 ]
 
 _lib = None
@@ -102,6 +102,9 @@ def load():
     L.vll_ortho_blunder_device.argtypes = [vp, D, C.c_double, vp, i64, vp, i64, vp, vp]
     L.vll_set_height_range.argtypes = [vp, D, vp, i64, vp, i64, vp, vp, i32, C.c_double, i32,
                                        C.c_double, vp, vp]
+    dbl = C.c_double
+    L.vll_select_mps.argtypes = [vp, D, vp, vp, dbl, dbl, dbl, dbl, i32, dbl, i32, dbl, vp, i64,
+                                 C.POINTER(i64)]
     _lib = L
     return L
 
@@ -260,6 +263,21 @@ class Context:
                                              len(pts), tris.ctypes.data, len(tris),
                                              inputs.gridpt3.ctypes.data, C.byref(rounds)))
         return rounds.value
+
+    def select_mps(self, inputs, ncc: np.ndarray, th_roh: float, th_roh_min: float,
+                   th_roh_start: float, th_roh_next: float, iteration: int, mpp: float,
+                   final_level_iteration: int, mpp_stereo_angle: float) -> np.ndarray:
+        """SelectMPs (setsm_code.cpp:8535-8895): updates inputs.gridpt3 in
+        place and returns the matched points (abi.POINT3_DTYPE, node order)."""
+        d = inputs.desc()
+        out = np.zeros(inputs.n, dtype=abi.POINT3_DTYPE)
+        n = C.c_int64()
+        self._check(load().vll_select_mps(
+            self._h, C.byref(d), ncc.ctypes.data, inputs.gridpt3.ctypes.data, float(th_roh),
+            float(th_roh_min), float(th_roh_start), float(th_roh_next), int(iteration),
+            float(mpp), int(final_level_iteration), float(mpp_stereo_angle), out.ctypes.data,
+            len(out), C.byref(n)))
+        return out[: n.value].copy()
 
     def set_height_range(self, inputs, pts: np.ndarray, tris: np.ndarray, iteration: int,
                          mpp: float, level_check_matching_rate: bool,

@@ -140,6 +140,34 @@ def make_range_case(*, seed=13, flag4_frac=0.2, unmatched_frac=0.2, **kw):
     return inp, pts, tris
 
 
+@functools.lru_cache(maxsize=8)
+def _matched(name: str):
+    from oracle import refpy
+    base = make_case(**CASES[name])
+    return run_cpu(refpy, base, base.iters)
+
+
+def make_select_case(name: str, seed: int = 71, flag_frac=(0.5, 0.1, 0.2)):
+    """Inputs of SelectMPs: the NCCresult of the reference build's matching
+    of case `name` (VerticalLineLocus [+ AWNCC]), and its UGRID with
+    Matched_flag drawn from 0 / 1 / 2 / 4 (fractions of 1, 2, 4 given) and
+    roh over [-0.2, 0.9].  Returns (inputs, nccresult)."""
+    import copy
+    r = _matched(name)
+    inp = copy.copy(r["inputs"])
+    inp.gridpt3 = r["gp3"].copy()
+    rng = np.random.default_rng(seed)
+    g = inp.gridpt3
+    n = len(g)
+    u = rng.random(n)
+    f1, f2, f4 = flag_frac
+    g["Matched_flag"] = np.where(u < f1, 1, np.where(u < f1 + f2, 2, np.where(u < f1 + f2 + f4,
+                                                                               4, 0)))
+    g["roh"] = rng.integers(-200, 900, n).astype(np.int16)
+    inp.grid_pts = r["inputs"].grid_pts.copy()
+    return inp, r["ncc"].copy()
+
+
 def delaunay(pts):
     """Triangles (abi.TRI_DTYPE) of the Delaunay triangulation of the points'
     x, y (scipy's Qhull) -- a stand-in for the matcher's own TIN."""

@@ -91,6 +91,30 @@ GOLDEN_RANGE = {
 }
 
 
+# SelectMPs (setsm_code.cpp:8535-8895) on the reference build's matching of
+# a case; the fixture keeps every input it reads (NCCresult, UGRID, grid
+# points) and the call's arguments: (Th_roh, Th_roh_min, Th_roh_start,
+# Th_roh_next, iteration, MPP, final_level_iteration, MPP_stereo_angle).
+GOLDEN_SELECT = {
+    "select_l0": dict(case="m7", level=0, args=(0.6, 0.2, 0.8, 0.7, 1, 1.5, 1, 10.0)),
+    "select_l1": dict(case="v7_gncc", level=1, args=(0.5, 0.45, 0.5, 0.4, 2, 2.0, 3, 10.0)),
+    "select_l3": dict(case="l3_m", level=3, args=(0.3, 0.25, 0.3, 0.2, 3, 2.0, 3, 3.0)),
+}
+
+
+def select_case(name):
+    """(inputs, nccresult, fixture arrays) of SelectMPs fixture `name`."""
+    from setsm_b200 import abi
+    from tests import cases
+    z = np.load(fixture_path(name))
+    v = GOLDEN_SELECT[name]
+    inp = cases.make_case(**cases.CASES[v["case"]])
+    inp.pyramid_step = v["level"]
+    inp.gridpt3 = z["init_gp3"].view(abi.UGRID_DTYPE).copy()
+    inp.grid_pts = z["grid_pts"].copy()
+    return inp, z["ncc"].view(abi.NCCRESULT_DTYPE).copy(), z
+
+
 def range_case(name):
     """(inputs, pts, tris, fixture arrays) of SetHeightRange fixture `name`."""
     from setsm_b200 import abi
@@ -236,6 +260,19 @@ def main(only=None) -> None:
                             pts=clean(pts).view(np.uint8), tris=tris.view(np.uint8),
                             result=clean(out).view(np.uint8), extent=np.array(ext))
         print(f"{name}: extent {ext}, {os.path.getsize(fixture_path(name))} bytes")
+
+    for name, v in GOLDEN_SELECT.items():
+        if only and name not in only:
+            continue
+        inp, ncc = cases.make_select_case(v["case"])
+        inp.pyramid_step = v["level"]
+        init = clean(inp.gridpt3)
+        r, pts = refpy.select_mps(inp, ncc, *v["args"])
+        np.savez_compressed(fixture_path(name), ncc=clean(ncc).view(np.uint8),
+                            init_gp3=init.view(np.uint8), grid_pts=inp.grid_pts,
+                            gp3=clean(inp.gridpt3).view(np.uint8), pts=clean(pts).view(np.uint8),
+                            ret=np.array(r))
+        print(f"{name}: {r} points, {os.path.getsize(fixture_path(name))} bytes")
 
 
 if __name__ == "__main__":

@@ -117,3 +117,15 @@ def test_range_fixtures_are_the_reference_output(name):
                                       v.get("sigma", 0.0))
     assert np.array_equal(mg.clean(out).view(np.uint8), z["result"])
     assert ext == tuple(z["extent"])
+
+
+@pytest.mark.skipif(not __import__("oracle.refpy").refpy.available(),
+                    reason="reference build not available")
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_SELECT))
+def test_select_fixtures_are_the_reference_output(name):
+    from oracle import refpy
+    inp, ncc, z = mg.select_case(name)
+    r, pts = refpy.select_mps(inp, ncc, *mg.GOLDEN_SELECT[name]["args"])
+    assert r == int(z["ret"])
+    assert np.array_equal(mg.clean(pts).view(np.uint8), z["pts"])
+    assert np.array_equal(mg.clean(inp.gridpt3).view(np.uint8), z["gp3"])
