@@ -421,6 +421,33 @@ int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, doubl
                              int64_t n_tris, vll_ugrid *d_gridpt3, int *rounds);
 
 /*
+ * InitializeVoxel (setsm_code.cpp:5759-6012): every node's search range for
+ * the voxel route (image-boundary test at the UGRID range, blunder-cell rules,
+ * range carried over or extended from the previous NCCresult) and its voxel
+ * row.  gridpt3 and nccresult are updated in place; voxels_in holds the rows
+ * packed by the incoming NumOfHeight (NULL on the first iteration),
+ * voxels_out receives them packed by the new NumOfHeight: rows whose range
+ * changed initialised (flag_cal 1, INCC -1000), the others carried over.
+ * *n_out receives the new voxel count; with *n_out > capacity the call
+ * returns VLL_ERR_CAPACITY and leaves every buffer untouched.  Host buffers
+ * (desc->grid_wgs, images' sizes / RPCs / startpos).  Bit-exact.
+ */
+int vll_initialize_voxel(vll_context *ctx, const vll_level_desc *desc, vll_ugrid *gridpt3,
+                         vll_nccresult *nccresult, const vll_voxel *voxels_in,
+                         vll_voxel *voxels_out, int64_t capacity, int64_t *n_out);
+/*
+ * The same on device data (desc->grid_wgs a device pointer; no image plane
+ * is read): d_voxel_offsets (N + 1 int64) receives the new row offsets, the
+ * form vll_vertical_line_locus_device takes, so the voxel route runs on the
+ * device end to end.  d_voxels_out must not overlap d_voxels_in.  On
+ * VLL_ERR_CAPACITY only *n_out and d_voxel_offsets are written.  Waits.
+ */
+int vll_initialize_voxel_device(vll_context *ctx, const vll_level_desc *desc,
+                                vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
+                                const vll_voxel *d_voxels_in, vll_voxel *d_voxels_out,
+                                int64_t capacity, int64_t *d_voxel_offsets, int64_t *n_out);
+
+/*
  * SelectMPs (setsm_code.cpp:8535-8895): the matched points of an iteration.
  * At levels > 0 the first-peak correlations of the nodes with more than two
  * heights set the minimum threshold (a 100-bin histogram against the level's

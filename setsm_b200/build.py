@@ -30,6 +30,7 @@ SOURCES = {
     "vll_orthotin.cu": ["-fmad=false"],
     "vll_heightrange.cu": ["-fmad=false"],
     "vll_selectmps.cu": ["-fmad=false"],
+    "vll_initvoxel.cu": ["-fmad=false"],
     "vll_split.cu": [],
     "vll_capi.cu": [],
     "vll_shim.cu": [],

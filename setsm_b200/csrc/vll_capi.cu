@@ -1199,6 +1199,105 @@ int vll_ortho_blunder_device(vll_context *ctx, const vll_level_desc *desc, doubl
     return ortho_blunder_run(ctx, P, mpp, d_pts, n_pts, d_tris, n_tris, d_gridpt3, rounds);
 }
 
+// InitializeVoxel on device pointers; d_off (N + 1) receives the offsets.
+static int init_voxel_run(vll_context *ctx, const vll_level_desc *desc, vll_ugrid *d_gp3,
+                          vll_nccresult *d_ncc, const vll_voxel *d_vin, vll_voxel *d_vout,
+                          int64_t capacity, int64_t *d_off, int64_t *n_out, bool grid_on_device,
+                          int64_t *old_total) {
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err, false);
+    if (rc) return fail(ctx, rc, err);
+    if (!(desc->height_step > 0)) return fail(ctx, VLL_ERR_INVALID, "height_step must be > 0");
+    const int64_t N = P.n_nodes;
+    if (N > 0x7fffffff) return fail(ctx, VLL_ERR_INVALID, "grid too large");
+    if (!grid_on_device) {
+        if ((rc = upload(ctx, ctx->wgs, desc->grid_wgs, (size_t)N * 16))) return rc;
+        P.grid_wgs = (const double *)ctx->wgs.p;
+    }
+    P.gp3 = d_gp3;
+    if ((rc = upload_level_block(ctx, P))) return rc;
+    const size_t bytes = vll::init_voxel_scratch(N);
+    VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
+    int64_t total = 0, old_tot = 0;
+    VLL_CUDA(ctx, vll::run_init_voxel((const DevLevel *)ctx->level.p, N, d_gp3, d_ncc,
+                                      ctx->tin_scratch.p, d_off, &total, &old_tot, ctx->stream));
+    ctx->launches_total += 1;
+    *n_out = total;
+    if (old_total) *old_total = old_tot;
+    if (total > capacity) return VLL_ERR_CAPACITY;
+    VLL_CUDA(ctx, vll::run_commit_voxel(N, ctx->tin_scratch.p, d_gp3, d_ncc, ctx->stream));
+    if (total > 0) {
+        VLL_CUDA(ctx, vll::run_pack_voxel(N, d_off, ctx->tin_scratch.p, d_vin, d_vout,
+                                          ctx->stream));
+        ctx->launches_total += 1;
+    }
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_initialize_voxel(vll_context *ctx, const vll_level_desc *desc, vll_ugrid *gridpt3,
+                         vll_nccresult *nccresult, const vll_voxel *voxels_in,
+                         vll_voxel *voxels_out, int64_t capacity, int64_t *n_out) {
+    NvtxRange nvtx_range("vll_initialize_voxel");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !gridpt3 || !nccresult || !n_out || !desc->grid_wgs || capacity < 0 ||
+        (capacity > 0 && !voxels_out))
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int64_t N = desc->grid_width * desc->grid_height;
+    if (N <= 0) return fail(ctx, VLL_ERR_INVALID, "empty grid");
+    int64_t old_total = 0;
+    for (int64_t i = 0; i < N; ++i) old_total += nccresult[i].NumOfHeight;
+    int rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
+    const vll_voxel *d_vin = nullptr;
+    if (voxels_in && old_total > 0) {
+        if ((rc = upload(ctx, ctx->vox, voxels_in, (size_t)old_total * sizeof(vll_voxel))))
+            return rc;
+        d_vin = (const vll_voxel *)ctx->vox.p;
+    }
+    VLL_CUDA(ctx, ensure(ctx->voxoff, (size_t)(N + 1) * sizeof(int64_t)));
+    // the output rows go to a second buffer (the input rows are read while
+    // they are written)
+    VLL_CUDA(ctx, ensure(ctx->gsum, (size_t)(capacity > 0 ? capacity : 1) * sizeof(vll_voxel)));
+    int64_t total = 0;
+    rc = init_voxel_run(ctx, desc, (vll_ugrid *)ctx->gp3.p, (vll_nccresult *)ctx->ncc.p, d_vin,
+                        (vll_voxel *)ctx->gsum.p, capacity, (int64_t *)ctx->voxoff.p, &total,
+                        false, nullptr);
+    *n_out = total;
+    if (rc == VLL_ERR_CAPACITY)
+        return fail(ctx, VLL_ERR_CAPACITY, "more voxels than the output buffer holds");
+    if (rc) return rc;
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->ncc.p, (size_t)N * sizeof(vll_nccresult),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    if (total > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(voxels_out, ctx->gsum.p, (size_t)total * sizeof(vll_voxel),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_initialize_voxel_device(vll_context *ctx, const vll_level_desc *desc,
+                                vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
+                                const vll_voxel *d_voxels_in, vll_voxel *d_voxels_out,
+                                int64_t capacity, int64_t *d_voxel_offsets, int64_t *n_out) {
+    NvtxRange nvtx_range("vll_initialize_voxel_device");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !d_gridpt3 || !d_nccresult || !d_voxel_offsets || !n_out || !desc->grid_wgs ||
+        capacity < 0 || (capacity > 0 && !d_voxels_out))
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int rc = init_voxel_run(ctx, desc, d_gridpt3, d_nccresult, d_voxels_in, d_voxels_out,
+                                  capacity, d_voxel_offsets, n_out, true, nullptr);
+    if (rc == VLL_ERR_CAPACITY)
+        return fail(ctx, VLL_ERR_CAPACITY, "more voxels than the output buffer holds");
+    return rc;
+}
+
 int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccresult *nccresult,
                    vll_ugrid *gridpt3, double th_roh, double th_roh_min, double th_roh_start,
                    double th_roh_next, int iteration, double mpp, int final_level_iteration,

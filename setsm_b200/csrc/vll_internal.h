@@ -47,6 +47,19 @@ cudaError_t launch_blunder(const DevLevel *dP, int64_t n_nodes, double2 *const *
                            int64_t oh, double im_res, int H, vll_ugrid *gout, float *ncc_out,
                            cudaStream_t s);
 
+// vll_initvoxel.cu: InitializeVoxel.  run_init_voxel decides every node
+// (into scratch) and fills new_off[0..n] with the new packing, *total the new
+// voxel count, *old_total the count of the incoming packing; run_commit_voxel
+// writes the decided records to gp3 / ncc and run_pack_voxel the rows.
+size_t init_voxel_scratch(int64_t n_nodes);
+cudaError_t run_init_voxel(const DevLevel *dP, int64_t n, vll_ugrid *gp3, vll_nccresult *ncc,
+                           void *scratch, int64_t *new_off, int64_t *total, int64_t *old_total,
+                           cudaStream_t s);
+cudaError_t run_commit_voxel(int64_t n, void *scratch, vll_ugrid *gp3, vll_nccresult *ncc,
+                             cudaStream_t s);
+cudaError_t run_pack_voxel(int64_t n, const int64_t *new_off, void *scratch, const vll_voxel *vin,
+                           vll_voxel *vout, cudaStream_t s);
+
 // vll_selectmps.cu: SelectMPs.  run_roh_hist fills the 100-bin histogram of
 // the first-peak correlations (and the node count behind it); run_select_mps
 // decides every node, updates gp3 and writes the selected points in node

@@ -34,7 +34,8 @@ EXPORTED = [
     "vll_vertical_line_locus_seeddem", "vll_vertical_line_locus_seeddem_device",
     "vll_vertical_line_locus_blunder", "vll_vertical_line_locus_blunder_device",
     "vll_vertical_line_locus_ortho", "vll_ortho_blunder", "vll_ortho_blunder_device",
-    "vll_set_height_range", "vll_select_mps",
+    "vll_set_height_range", "vll_select_mps", "vll_initialize_voxel",
+    "vll_initialize_voxel_device",
 ]
 
 _lib = None
@@ -103,6 +104,8 @@ def load():
     L.vll_set_height_range.argtypes = [vp, D, vp, i64, vp, i64, vp, vp, i32, C.c_double, i32,
                                        C.c_double, vp, vp]
     dbl = C.c_double
+    L.vll_initialize_voxel.argtypes = [vp, D, vp, vp, vp, vp, i64, C.POINTER(i64)]
+    L.vll_initialize_voxel_device.argtypes = [vp, D, vp, vp, vp, vp, i64, vp, C.POINTER(i64)]
     L.vll_select_mps.argtypes = [vp, D, vp, vp, dbl, dbl, dbl, dbl, i32, dbl, i32, dbl, vp, i64,
                                  C.POINTER(i64)]
     _lib = L
@@ -263,6 +266,32 @@ class Context:
                                              len(pts), tris.ctypes.data, len(tris),
                                              inputs.gridpt3.ctypes.data, C.byref(rounds)))
         return rounds.value
+
+    def initialize_voxel(self, inputs, ncc: np.ndarray,
+                         voxels_in: np.ndarray | None = None) -> np.ndarray:
+        """InitializeVoxel (setsm_code.cpp:5759-6012): updates inputs.gridpt3
+        and ncc in place; returns the voxel rows packed by the new
+        NumOfHeight (voxels_in: the rows packed by the incoming one)."""
+        d = inputs.desc()
+        g = inputs.gridpt3
+        cap = int(((g["maxHeight"].astype(np.int64) - g["minHeight"].astype(np.int64) + 4)
+                   / inputs.height_step + 4).clip(0).sum())
+        cap = max(cap, int(ncc["NumOfHeight"].astype(np.int64).sum()), 1)
+        out = np.zeros(cap, dtype=abi.VOXEL_DTYPE)
+        n = C.c_int64()
+        vin = voxels_in.ctypes.data if voxels_in is not None and voxels_in.size else None
+        self._check(load().vll_initialize_voxel(self._h, C.byref(d), g.ctypes.data,
+                                                ncc.ctypes.data, vin, out.ctypes.data, cap,
+                                                C.byref(n)))
+        return out[: n.value].copy()
+
+    def initialize_voxel_device(self, desc, d_gridpt3: int, d_ncc: int, d_vox_in: int | None,
+                                d_vox_out: int, capacity: int, d_offsets: int) -> int:
+        n = C.c_int64()
+        self._check(load().vll_initialize_voxel_device(self._h, C.byref(desc), d_gridpt3, d_ncc,
+                                                       d_vox_in, d_vox_out, int(capacity),
+                                                       d_offsets, C.byref(n)))
+        return n.value
 
     def select_mps(self, inputs, ncc: np.ndarray, th_roh: float, th_roh_min: float,
                    th_roh_start: float, th_roh_next: float, iteration: int, mpp: float,
