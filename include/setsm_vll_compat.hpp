@@ -30,9 +30,13 @@ struct tagD2DPoint {
     double m_Y;
 };
 
+// With a user-written copy constructor, as the reference's (a CSize passed
+// by value -- AWNCC's Size_Grid2D -- travels by hidden reference).
 struct tagCSize {
     unsigned int width;
     unsigned int height;
+    tagCSize() : width(0), height(0) {}
+    tagCSize(const tagCSize &s) : width(s.width), height(s.height) {}
 };
 
 struct tagTransParam {
@@ -232,6 +236,15 @@ int VerticalLineLocus_Ortho(ProjectInfo *proinfo, taglevelinfo &plevelinfo, doub
                             double *F_sncc);
 int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &plevelinfo, double MPP, tagD3DPoint *pts,
                   int numOfPts, tagUI3DPoint *tris, int numOfTri, UpdateGrid *GridPT3);
+// InitializeVoxel (setsm_code.hpp:75) and AWNCC (:91), same behaviour:
+// InitializeVoxel frees and (re)allocates grid_voxel rows as the reference
+// does; AWNCC reads the rows and writes the peaks.
+void InitializeVoxel(const ProjectInfo *proinfo, tagVoxelinfo **grid_voxel,
+                     taglevelinfo &plevelinfo, UpdateGrid *GridPT3, tagNCCresult *nccresult,
+                     const int iteration, const double *minmaxHeight);
+void AWNCC(ProjectInfo *proinfo, tagVoxelinfo **grid_voxel, tagCSize Size_Grid2D,
+           UpdateGrid *GridPT3, tagNCCresult *nccresult, double step_height,
+           unsigned char Pyramid_step, unsigned char iteration, int MaxNumberofHeightVoxel);
 // SelectMPs (setsm_code.hpp:99), same behaviour: appends the matched points
 // to *linkedlist, updates GridPT3, returns their number.
 long SelectMPs(const ProjectInfo *proinfo, taglevelinfo &plevelinfo,

@@ -229,14 +229,42 @@ int ref_max_threads(void) { return omp_get_max_threads(); }
 /* InitializeVoxel on the packed voxel rows: `voxels_in` holds the rows of the
  * previous iteration (by the incoming NumOfHeight), `voxels_out` receives the
  * rows by the updated NumOfHeight.  Returns the packed count written. */
-long ref_initialize_voxel(const vll_level_desc *d, vll_ugrid *gridpt3, vll_nccresult *ncc,
-                          const vll_voxel *voxels_in, vll_voxel *voxels_out, long cap) {
+typedef void (*init_voxel_signature)(const ProInfo *, VOXEL **, LevelInfo &, UGRID *,
+                                     NCCresult *, const int, const double *);
+typedef void (*awncc_signature)(ProInfo *, VOXEL **, CSize, UGRID *, NCCresult *, double, uint8,
+                                uint8, int);
+
+/* InitializeVoxel, or the function at `fn` with its signature
+ * (setsm_code.hpp:75); voxels in/out in packed form. */
+long ref_call_initialize_voxel(void *fn, const vll_level_desc *d, vll_ugrid *gridpt3,
+                               vll_nccresult *ncc, const vll_voxel *voxels_in,
+                               vll_voxel *voxels_out, long cap) {
     RefLevel L(d);
     const long n = L.grid_length;
     VOXEL **rows = unpack_voxels(ncc, n, voxels_in);
-    InitializeVoxel(L.proinfo, rows, L.li, reinterpret_cast<UGRID *>(gridpt3),
-                    reinterpret_cast<NCCresult *>(ncc), d->iteration, d->minmax_height);
+    init_voxel_signature f = fn ? reinterpret_cast<init_voxel_signature>(fn) : &InitializeVoxel;
+    f(L.proinfo, rows, L.li, reinterpret_cast<UGRID *>(gridpt3),
+      reinterpret_cast<NCCresult *>(ncc), d->iteration, d->minmax_height);
     return pack_and_free_voxels(ncc, n, rows, voxels_out, cap);
+}
+
+long ref_initialize_voxel(const vll_level_desc *d, vll_ugrid *gridpt3, vll_nccresult *ncc,
+                          const vll_voxel *voxels_in, vll_voxel *voxels_out, long cap) {
+    return ref_call_initialize_voxel(nullptr, d, gridpt3, ncc, voxels_in, voxels_out, cap);
+}
+
+/* AWNCC through the function at `fn` with its signature (setsm_code.hpp:91). */
+void ref_call_awncc(void *fn, const vll_level_desc *d, vll_ugrid *gridpt3, vll_nccresult *ncc,
+                    vll_voxel *voxels, long cap) {
+    RefLevel L(d);
+    const long n = L.grid_length;
+    VOXEL **rows = unpack_voxels(ncc, n, voxels);
+    const int max_voxel = (int)((d->minmax_height[1] - d->minmax_height[0]) / d->height_step);
+    reinterpret_cast<awncc_signature>(fn)(L.proinfo, rows, L.grid_size,
+                                          reinterpret_cast<UGRID *>(gridpt3),
+                                          reinterpret_cast<NCCresult *>(ncc), d->height_step,
+                                          (uint8)d->pyramid_step, (uint8)d->iteration, max_voxel);
+    pack_and_free_voxels(ncc, n, rows, voxels, cap);
 }
 
 /* VerticalLineLocus; voxels are in/out in packed form (ignored on the

@@ -408,3 +408,35 @@ def select_mps(inputs, ncc, th_roh, th_roh_min, th_roh_start, th_roh_next, itera
                              params.ctypes.data, iparams.ctypes.data, out.ctypes.data, len(out),
                              C.byref(n))
     return int(r), out[: n.value].copy()
+
+
+def call_initialize_voxel(fn_addr: int, inputs, ncc, voxels_in):
+    """InitializeVoxel through the function at fn_addr (setsm_code.hpp:75)."""
+    L = lib()
+    L.ref_call_initialize_voxel.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]
+    L.ref_call_initialize_voxel.restype = C.c_long
+    d = inputs.desc()
+    cap = int(((inputs.gridpt3["maxHeight"].astype(np.int64)
+                - inputs.gridpt3["minHeight"].astype(np.int64) + 4)
+               / inputs.height_step + 4).clip(0).sum())
+    cap = max(cap, int(ncc["NumOfHeight"].astype(np.int64).sum()), 1)
+    out = np.zeros(cap, dtype=abi.VOXEL_DTYPE)
+    vin = voxels_in.ctypes.data if voxels_in is not None and voxels_in.size else None
+    with _StdoutToStderr():
+        n = L.ref_call_initialize_voxel(fn_addr, C.byref(d), inputs.gridpt3.ctypes.data,
+                                        ncc.ctypes.data, vin, out.ctypes.data, out.size)
+    assert n <= out.size
+    return out[:n].copy()
+
+
+def call_awncc(fn_addr: int, inputs, ncc, voxels) -> None:
+    """AWNCC through the function at fn_addr (setsm_code.hpp:91)."""
+    L = lib()
+    L.ref_call_awncc.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_long]
+    L.ref_call_awncc.restype = None
+    d = inputs.desc()
+    with _StdoutToStderr():
+        L.ref_call_awncc(fn_addr, C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data,
+                         voxels.ctypes.data, voxels.size)

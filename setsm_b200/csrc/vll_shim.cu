@@ -235,6 +235,100 @@ int Ortho_blunder(ProjectInfo *proinfo, taglevelinfo &pl, double MPP, tagD3DPoin
     return numOfPts;
 }
 
+void InitializeVoxel(const ProjectInfo *proinfo, tagVoxelinfo **grid_voxel, taglevelinfo &pl,
+                     UpdateGrid *GridPT3, tagNCCresult *nccresult, const int iteration,
+                     const double *minmaxHeight) {
+    check_sensor(proinfo);
+    vll_context *ctx = shim_context();
+    ShimState &st = state();
+    vll_level_desc d;
+    fill_desc(proinfo, pl, iteration, minmaxHeight, d);
+    const int64_t n = d.grid_width * d.grid_height;
+    std::vector<uint16_t> old_n((size_t)n);
+    int64_t cap = 1;
+    for (int64_t i = 0; i < n; ++i) {
+        old_n[(size_t)i] = nccresult[i].NumOfHeight;
+        const int64_t span = (int64_t)GridPT3[i].maxHeight - GridPT3[i].minHeight +
+                             (int64_t)nccresult[i].maxHeight - nccresult[i].minHeight;
+        cap += (int64_t)((span < 0 ? -span : span) / d.height_step) + 8 + old_n[(size_t)i];
+    }
+    // the rows are rebuilt here from the new NumOfHeight, so no old rows go up
+    int64_t total = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        st.packed.resize((size_t)cap);
+        const int rc = vll_initialize_voxel(ctx, &d, reinterpret_cast<vll_ugrid *>(GridPT3),
+                                            reinterpret_cast<vll_nccresult *>(nccresult), nullptr,
+                                            st.packed.data(), cap, &total);
+        if (rc == VLL_OK) break;
+        if (rc != VLL_ERR_CAPACITY || attempt == 1)
+            die("InitializeVoxel: GPU call failed", vll_last_error(ctx));
+        cap = total;
+    }
+    // the reference's row management: a row whose range changed is freed and
+    // reallocated with (flag_cal, INCC -1000) voxels, a row that drops to zero
+    // heights is freed, the others are kept as they are
+    for (int64_t i = 0; i < n; ++i) {
+        const int k = nccresult[i].NumOfHeight;
+        const int k0 = old_n[(size_t)i];
+        if (k > 0 && nccresult[i].check_height_change) {
+            if (k0 > 0 && grid_voxel[i]) free(grid_voxel[i]);
+            grid_voxel[i] = (tagVoxelinfo *)calloc((size_t)k, sizeof(tagVoxelinfo));
+            if (!grid_voxel[i]) die("InitializeVoxel: out of memory", nullptr);
+            for (int h = 0; h < k; ++h) {
+                grid_voxel[i][h].flag_cal = true;
+                grid_voxel[i][h].INCC = -1000;
+            }
+        } else if (k == 0 && k0 > 0 && grid_voxel[i]) {
+            free(grid_voxel[i]);
+        }
+    }
+}
+
+void AWNCC(ProjectInfo *proinfo, tagVoxelinfo **grid_voxel, tagCSize Size_Grid2D,
+           UpdateGrid *GridPT3, tagNCCresult *nccresult, double step_height,
+           unsigned char Pyramid_step, unsigned char iteration, int MaxNumberofHeightVoxel) {
+    (void)MaxNumberofHeightVoxel;   // sizes the reference's own buffers only
+    check_sensor(proinfo);
+    vll_context *ctx = shim_context();
+    ShimState &st = state();
+    // AWNCC reads no image: the descriptor carries the level, the iteration,
+    // the switches and the grid; selected images get placeholder sizes
+    vll_level_desc d;
+    memset(&d, 0, sizeof(d));
+    d.num_images = proinfo->number_of_images;
+    d.pyramid_step = Pyramid_step;
+    d.template_size = 11;
+    d.iteration = iteration;
+    d.is_ra = proinfo->IsRA;
+    d.check_matchtag = proinfo->check_Matchtag;
+    d.sgm_py = proinfo->SGM_py;
+    d.resolution = proinfo->resolution;
+    d.dem_resolution = proinfo->DEM_resolution;
+    d.height_step = step_height;
+    d.grid_width = Size_Grid2D.width;
+    d.grid_height = Size_Grid2D.height;
+    for (int ti = 0; ti < d.num_images && ti < VLL_MAX_IMAGES; ++ti) {
+        d.images[ti].selected = proinfo->check_selected_image[ti] ? 1 : 0;
+        d.images[ti].width = d.images[ti].height = 2;
+    }
+    const int64_t n = d.grid_width * d.grid_height;
+    int64_t nvox = 0;
+    for (int64_t i = 0; i < n; ++i) nvox += nccresult[i].NumOfHeight;
+    st.packed.resize((size_t)(nvox > 0 ? nvox : 1));
+    int64_t o = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int k = nccresult[i].NumOfHeight;
+        if (k > 0) {
+            memcpy(st.packed.data() + o, grid_voxel[i], (size_t)k * sizeof(vll_voxel));
+            o += k;
+        }
+    }
+    if (vll_awncc_peaks(ctx, &d, reinterpret_cast<const vll_ugrid *>(GridPT3),
+                        reinterpret_cast<vll_nccresult *>(nccresult), st.packed.data(), nvox,
+                        nullptr) != VLL_OK)
+        die("AWNCC: GPU call failed", vll_last_error(ctx));
+}
+
 long SelectMPs(const ProjectInfo *proinfo, taglevelinfo &pl, const tagNCCresult *roh_height,
                UpdateGrid *GridPT3, const double Th_roh, const double Th_roh_min,
                const double Th_roh_start, const double Th_roh_next, const int iteration,

@@ -91,3 +91,34 @@ def test_device_voxel_route_matches_reference(gpu_ctx, name):
     assert cases.field_mismatch(got_vox, want_vox) == {}
     assert cases.field_mismatch(cases.from_device(keep["gp3"], abi.UGRID_DTYPE),
                                 ref.gridpt3) == {}
+
+
+DROPIN_IV = "_Z15InitializeVoxelPK11ProjectInfoPP12tagVoxelinfoR12taglevelinfoP10UpdateGridP12tagNCCresultiPKd"
+DROPIN_AWNCC = "_Z5AWNCCP11ProjectInfoPP12tagVoxelinfo8tagCSizeP10UpdateGridP12tagNCCresultdhhi"
+
+
+@pytest.mark.parametrize("name", ["v7_gncc", "v7_3img"])
+def test_cpp_dropins_through_reference_structures(gpu_ctx, name):
+    """InitializeVoxel and AWNCC drop-ins (setsm_code.hpp:75, :91) called the
+    way Matching_SETSM calls them (VOXEL** rows), around the reference's own
+    VerticalLineLocus: the same NCCresult, UGRID and voxels as the
+    reference's iteration."""
+    import ctypes as C
+    from setsm_b200 import vll
+    L = vll.load()
+    fn_iv = C.cast(getattr(L, DROPIN_IV), C.c_void_p).value
+    fn_aw = C.cast(getattr(L, DROPIN_AWNCC), C.c_void_p).value
+    inp, ncc, vox = first_iteration(name)
+    ref = copy.copy(inp)
+    ref.gridpt3 = inp.gridpt3.copy()
+    ref_ncc = ncc.copy()
+    want_vox = refpy.initialize_voxel(ref, ref_ncc, vox.copy())
+    refpy.vertical_line_locus(ref, ref_ncc, want_vox)
+    refpy.awncc(ref, ref_ncc, want_vox)
+    got_ncc = ncc.copy()
+    got_vox = refpy.call_initialize_voxel(fn_iv, inp, got_ncc, vox.copy())
+    refpy.vertical_line_locus(inp, got_ncc, got_vox)
+    refpy.call_awncc(fn_aw, inp, got_ncc, got_vox)
+    assert cases.field_mismatch(got_ncc, ref_ncc) == {}
+    assert cases.field_mismatch(got_vox, want_vox) == {}
+    assert cases.field_mismatch(inp.gridpt3, ref.gridpt3) == {}
