@@ -353,6 +353,13 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc,
                     const vll_ugrid *gridpt3, vll_nccresult *nccresult,
                     const vll_voxel *voxels, int64_t voxel_capacity,
                     vll_stats *stats);
+/* The same on device data: the packed voxel rows and their N + 1 int64
+ * offsets (as vll_initialize_voxel_device writes them).  Asynchronous on the
+ * context's stream unless `stats` is given. */
+int vll_awncc_peaks_device(vll_context *ctx, const vll_level_desc *desc,
+                           const vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
+                           const vll_voxel *d_voxels, const int64_t *d_voxel_offsets,
+                           vll_stats *stats);
 
 /* ---- orthoimage-window variants (setsm_code.cpp:7720-8026) ------------- */
 /*

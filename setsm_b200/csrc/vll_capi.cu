@@ -1533,6 +1533,58 @@ int vll_debug_ortho_raster(vll_context *ctx, const vll_level_desc *desc, const v
     return VLL_OK;
 }
 
+int vll_awncc_peaks_device(vll_context *ctx, const vll_level_desc *desc,
+                           const vll_ugrid *d_gridpt3, vll_nccresult *d_nccresult,
+                           const vll_voxel *d_voxels, const int64_t *d_voxel_offsets,
+                           vll_stats *stats) {
+    NvtxRange nvtx_range("vll_awncc_peaks_device");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !d_gridpt3 || !d_nccresult || !d_voxel_offsets)
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevLevel P;
+    std::string err;
+    int rc = vll::derive_level(desc, &P, &err, false);
+    if (rc) return fail(ctx, rc, err);
+    const bool sgm = P.L <= desc->sgm_py;
+    const int64_t N = P.n_nodes;
+    P.gp3 = d_gridpt3;
+    P.ncc = d_nccresult;
+    P.vox = const_cast<vll_voxel *>(d_voxels);
+    P.vox_off = d_voxel_offsets;
+    int max_h = 0;
+    int64_t total = 0;
+    VLL_CUDA(ctx, ensure(ctx->counters, 8 * sizeof(unsigned long long)));
+    VLL_CUDA(ctx, vll::row_extent(d_nccresult, N, d_voxel_offsets, (int *)ctx->counters.p,
+                                  &max_h, &total, ctx->stream));
+    if (total > 0 && !d_voxels) return fail(ctx, VLL_ERR_INVALID, "null voxel rows");
+    if ((rc = upload_level_block(ctx, P))) return rc;
+    if (!ctx->e0) {
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e0));
+        VLL_CUDA(ctx, cudaEventCreate(&ctx->e1));
+    }
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e0, ctx->stream));
+    const float *sumcost = nullptr;
+    if (sgm) {
+        VLL_CUDA(ctx, ensure(ctx->sumcost, (size_t)(total > 0 ? total : 1) * sizeof(float)));
+        VLL_CUDA(ctx, vll::launch_sgm((const DevLevel *)ctx->level.p, P.grid_w, P.grid_h, max_h,
+                                      (float *)ctx->sumcost.p, total, ctx->stream));
+        sumcost = (const float *)ctx->sumcost.p;
+        ctx->launches_total += 8;
+    }
+    VLL_CUDA(ctx, vll::launch_awncc((const DevLevel *)ctx->level.p, N, sumcost, ctx->stream));
+    VLL_CUDA(ctx, cudaEventRecord(ctx->e1, ctx->stream));
+    ctx->launches_total += 2;
+    if (stats) {
+        VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->e0, ctx->e1);
+        memset(stats, 0, sizeof(*stats));
+        stats->kernel_ms = ms;
+    }
+    return VLL_OK;
+}
+
 int vll_preprocess_level_device(vll_context *ctx, const uint16_t *d_image, uint32_t width,
                                 uint32_t height, int template_size, uint16_t *d_mag,
                                 uint8_t *d_ori) {

@@ -23,6 +23,9 @@ cudaError_t launch_awncc(const DevLevel *dP, int64_t n_nodes, const float *sumco
 
 // vll_sgm.cu: the 8-direction aggregation of AWNCC into sumcost (packed like
 // the voxel rows); max_h is the level's largest NumOfHeight.
+// vll_plain.cu: the largest row length and the total (off[n]) of a packing.
+cudaError_t row_extent(const vll_nccresult *ncc, int64_t n, const int64_t *off, int *d_max,
+                       int *max_h, int64_t *total, cudaStream_t s);
 cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int max_h,
                        float *sumcost, int64_t n_slots, cudaStream_t s);
 cudaError_t launch_gncc(const DevLevel *dP, int64_t n_nodes, double *gsum, double *gcnt,

@@ -224,6 +224,32 @@ cudaError_t launch_plain(const DevLevel *dP, int64_t n_nodes, unsigned long long
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void row_max_kernel(const vll_nccresult *ncc, int64_t n, int *out) {
+    int m = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        m = max(m, (int)ncc[i].NumOfHeight);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+}  // namespace
+
+cudaError_t row_extent(const vll_nccresult *ncc, int64_t n, const int64_t *off, int *d_max,
+                       int *max_h, int64_t *total, cudaStream_t s) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(d_max, 0, sizeof(int), s))) return e;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks < 1) blocks = 1;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    row_max_kernel<<<(unsigned)blocks, 256, 0, s>>>(ncc, n, d_max);
+    if ((e = cudaGetLastError())) return e;
+    if ((e = cudaMemcpyAsync(max_h, d_max, sizeof(int), cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaMemcpyAsync(total, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s)))
+        return e;
+    return cudaStreamSynchronize(s);
+}
+
 cudaError_t launch_ortho(const DevLevel *dP, int64_t total, double2 *const *cd, double2 *const *cdn,
                          cudaStream_t s) {
     const int threads = 256;

@@ -35,7 +35,7 @@ EXPORTED = [
     "vll_vertical_line_locus_blunder", "vll_vertical_line_locus_blunder_device",
     "vll_vertical_line_locus_ortho", "vll_ortho_blunder", "vll_ortho_blunder_device",
     "vll_set_height_range", "vll_select_mps", "vll_initialize_voxel",
-    "vll_initialize_voxel_device",
+    "vll_initialize_voxel_device", "vll_awncc_peaks_device",
 ]
 
 _lib = None
@@ -106,6 +106,7 @@ def load():
     dbl = C.c_double
     L.vll_initialize_voxel.argtypes = [vp, D, vp, vp, vp, vp, i64, C.POINTER(i64)]
     L.vll_initialize_voxel_device.argtypes = [vp, D, vp, vp, vp, vp, i64, vp, C.POINTER(i64)]
+    L.vll_awncc_peaks_device.argtypes = [vp, D, vp, vp, vp, vp, S]
     L.vll_select_mps.argtypes = [vp, D, vp, vp, dbl, dbl, dbl, dbl, i32, dbl, i32, dbl, vp, i64,
                                  C.POINTER(i64)]
     _lib = L
@@ -284,6 +285,11 @@ class Context:
                                                 ncc.ctypes.data, vin, out.ctypes.data, cap,
                                                 C.byref(n)))
         return out[: n.value].copy()
+
+    def awncc_device(self, desc, d_gridpt3: int, d_ncc: int, d_vox: int, d_offsets: int) -> None:
+        """AWNCC on device data (asynchronous on the context's stream)."""
+        self._check(load().vll_awncc_peaks_device(self._h, C.byref(desc), d_gridpt3, d_ncc, d_vox,
+                                                  d_offsets, None))
 
     def initialize_voxel_device(self, desc, d_gridpt3: int, d_ncc: int, d_vox_in: int | None,
                                 d_vox_out: int, capacity: int, d_offsets: int) -> int:

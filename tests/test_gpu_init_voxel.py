@@ -20,10 +20,14 @@ pytestmark = [pytest.mark.gpu,
 VOXEL_CASES = ["v7_gncc", "v11", "l2_combined", "l2_max", "v7_3img", "v7_3img_unsel"]
 
 
+# the SGM route too (AWNCC with semi-global aggregation at level 0)
+SGM_CASE = dict(size=512, nodes=24, res=8.0, n_heights=32, cmr=False, sgm=1, ortho_frac=0.5)
+
+
 def first_iteration(name):
-    """(inputs at iteration 2, ncc, gp3, voxels) after the reference's
-    iteration 1 of case `name`."""
-    inp = cases.make_case(**cases.CASES[name])
+    """(inputs at iteration 2, ncc, voxels) after the reference's iteration 1
+    of case `name` (a key of tests/cases.py:CASES, or "sgm")."""
+    inp = cases.make_case(**(SGM_CASE if name == "sgm" else cases.CASES[name]))
     inp = copy.copy(inp)
     inp.gridpt3 = inp.gridpt3.copy()
     inp.iteration = 1
@@ -62,10 +66,10 @@ def test_second_iteration_carries_rows(gpu_ctx, name):
     compare(gpu_ctx, inp, ncc, vox)
 
 
-@pytest.mark.parametrize("name", ["v7_gncc", "l2_combined"])
+@pytest.mark.parametrize("name", ["v7_gncc", "l2_combined", "sgm"])
 def test_device_voxel_route_matches_reference(gpu_ctx, name):
-    """InitializeVoxel and VerticalLineLocus on device-resident data, the
-    offsets of the first feeding the second."""
+    """InitializeVoxel, VerticalLineLocus and AWNCC on device-resident data,
+    the offsets of the first feeding the others."""
     import torch
     inp, ncc, vox = first_iteration(name)
     ref = copy.copy(inp)
@@ -84,6 +88,8 @@ def test_device_voxel_route_matches_reference(gpu_ctx, name):
     assert n == len(want_vox)
     gpu_ctx.vertical_line_locus_device(io[0], io[1], io[2], d_vout.data_ptr(), d_off.data_ptr(),
                                        kernel="split")
+    gpu_ctx.awncc_device(io[0], io[1], io[2], d_vout.data_ptr(), d_off.data_ptr())
+    refpy.awncc(ref, ref_ncc, want_vox)
     torch.cuda.synchronize()
     got_ncc = cases.from_device(keep["ncc"], abi.NCCRESULT_DTYPE)
     got_vox = d_vout.cpu().numpy().view(abi.VOXEL_DTYPE)[:n]
