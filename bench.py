@@ -827,6 +827,115 @@ def run_height_range(args):
     del torch
 
 
+def run_voxel_iter(args):
+    """One matching iteration of the voxel route at level 0 with SGM
+    (SGM_py = 1) on the reduced C2 scene (4096^2 pair, 1024^2 grid, TIN
+    ranges, 7x7): InitializeVoxel -> VerticalLineLocus (split) -> AWNCC with
+    semi-global aggregation.  value: the three calls on device-resident data
+    (vll_initialize_voxel_device, vll_vertical_line_locus_device,
+    vll_awncc_peaks_device; host clock around them, synchronized); e2e: the
+    host-buffer entry points (copies included); CPU: the reference's own
+    InitializeVoxel, VerticalLineLocus and AWNCC with OpenMP on every host core
+    on the whole grid; the final NCCresult compared.  Metric: node x height
+    evaluations per second of the iteration."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import copy
+    import torch
+    from oracle import refpy
+    from setsm_b200 import abi, vll, workloads
+    from tests.cases import field_mismatch
+    ctx = vll.Context(0)
+    wl = workloads.build("c2_small", ctx, device="cuda:0", seed=1)
+    n = int(wl.n_nodes)
+    d = wl.device_desc(11)
+    d.check_matching_rate = 0
+    d.sgm_py = 1
+    d.iteration = 1
+    g = wl.gp3
+    hs = wl.cfg["height_step"]
+    cap = int(((g["maxHeight"].astype(np.int64) - g["minHeight"].astype(np.int64) + 4) / hs
+               + 4).clip(0).sum())
+    d_gp3_0 = wl.d_gp3.clone()
+    d_vox = torch.empty(cap * 4, dtype=torch.uint8, device="cuda:0")
+    d_off = torch.empty(n + 1, dtype=torch.int64, device="cuda:0")
+    gp3_p, ncc_p = wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr()
+
+    def device_step():
+        wl.d_gp3.copy_(d_gp3_0)
+        wl.d_ncc.zero_()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ctx.initialize_voxel_device(d, gp3_p, ncc_p, None, d_vox.data_ptr(), cap,
+                                    d_off.data_ptr())
+        st = ctx.vertical_line_locus_device(d, gp3_p, ncc_p, d_vox.data_ptr(), d_off.data_ptr(),
+                                            kernel="split", stats=True)
+        ctx.awncc_device(d, gp3_p, ncc_p, d_vox.data_ptr(), d_off.data_ptr())
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) * 1e3, int(st.evals)
+    for _ in range(max(1, args.warmup)):
+        device_step()
+    clocks = Clocks(0)
+    clocks.start()
+    times, evals = [], 0
+    lc0 = vll.load().vll_launch_count(ctx._h)
+    for _ in range(args.steps):
+        ms, evals = device_step()
+        times.append(ms)
+    launches = vll.load().vll_launch_count(ctx._h) - lc0
+    clk = clocks.stop()
+    dev_ms = statistics.median(times)
+    dev_ncc = wl.d_ncc.cpu().numpy().view(abi.NCCRESULT_DTYPE).copy()
+    # host-buffer entry points (e2e)
+    inp = wl.host_inputs(11)
+    inp.check_matching_rate = False
+    inp.sgm_py = 1
+    g0 = inp.gridpt3.copy()
+    e2e = []
+    for _ in range(2):
+        inp.gridpt3 = g0.copy()
+        ncc = inp.new_nccresult()
+        t = time.perf_counter()
+        vox = ctx.initialize_voxel(inp, ncc, None)
+        ctx.vertical_line_locus(inp, ncc, vox, "split")
+        ctx.awncc(inp, ncc, vox)
+        e2e.append((time.perf_counter() - t) * 1e3)
+    e2e_ms = min(e2e)
+    ref = copy.copy(inp)
+    ref.gridpt3 = g0.copy()
+    ref_ncc = ref.new_nccresult()
+    refpy.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    rvox = refpy.initialize_voxel(ref, ref_ncc, None)
+    refpy.vertical_line_locus(ref, ref_ncc, rvox)
+    refpy.awncc(ref, ref_ncc, rvox)
+    cpu_s = time.perf_counter() - t
+    line = {
+        "metric": "node x height evals/s (voxel-route iteration: InitializeVoxel + "
+                  "VerticalLineLocus + AWNCC with SGM)",
+        "value": evals / (dev_ms / 1e3), "unit": "evals/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": max(1, args.warmup), "ms_per_step": dev_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 window sums, f64 RPC and decisions (the reference's)", "data": "synthetic",
+        "config": {"workload": "voxel-route iteration 1 at level 0, SGM_py 1: reduced C2 scene "
+                               "(4096^2 pair, 1024^2 grid, TIN ranges K 8-512 at 0.5 m), 7x7",
+                   "nodes": n, "evals": evals},
+        "e2e": {"value": evals / (e2e_ms / 1e3), "unit": "evals/s",
+                "timing": "host wall clock of vll_initialize_voxel + vll_vertical_line_locus + "
+                          "vll_awncc_peaks on host buffers (copies included)"},
+        "cpu_baseline": {"value": evals / cpu_s, "unit": "evals/s", "cores": os.cpu_count(),
+                         "kind": "reference", "sample": f"whole grid, {cpu_s:.1f} s"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "parity": {"device_vs_reference": field_mismatch(dev_ncc, ref_ncc),
+                   "host_api_vs_reference": field_mismatch(ncc, ref_ncc)},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    del torch
+
+
 def run_select_mps(args):
     """SelectMPs (setsm_code.cpp:8535-8895) on the reduced C2 scene: the
     peaks of the 7x7 memory-tight matching (split kernel) of its 1024^2 grid,
@@ -1044,7 +1153,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
                     choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm", "seeddem",
-                             "blunder", "ortho_tin", "height_range", "select_mps"])
+                             "blunder", "ortho_tin", "height_range", "select_mps",
+                             "voxel_iter"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -1079,6 +1189,8 @@ def main():
         run_height_range(args)
     elif args.config == "select_mps":
         run_select_mps(args)
+    elif args.config == "voxel_iter":
+        run_voxel_iter(args)
     else:
         run_ours(args)
 
