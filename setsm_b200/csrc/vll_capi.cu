@@ -6,6 +6,7 @@
 // data resident (used by the serving loop and the benchmark).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -64,6 +65,7 @@ struct vll_context {
     Buf ocd[VLL_MAX_IMAGES], ocdn[VLL_MAX_IMAGES], ocdptr;
     Buf pre_tmp, pre_wt, pre_img, pre_mag, pre_ori;
     Buf sumcost;                       // SGM aggregation (float per voxel slot)
+    Buf sgm_lr;                        // SGM: the 8 directions' costs per slot
     Buf tin_pts, tin_tris, tin_scratch;  // Ortho_blunder: points, triangles, work arrays
     vll::SplitBuffers split;
     vll::SplitTuning tuning;
@@ -537,6 +539,21 @@ int finish_set(vll_context *ctx, SetResources &r, const vll::SplitBuffers &b, in
     return VLL_OK;
 }
 
+// Scratch of the all-directions SGM, or nullptr (one launch per direction)
+// when it exceeds the budget or cannot be allocated.
+float *sgm_scratch(vll_context *ctx, int64_t n_slots) {
+    // SETSM_VLL_SGM_SEQUENTIAL=1 selects the per-direction form (same results)
+    const char *seq = getenv("SETSM_VLL_SGM_SEQUENTIAL");
+    if (seq && seq[0] == '1') return nullptr;
+    const size_t b = vll::sgm_scratch_bytes(n_slots);
+    if (!b) return nullptr;
+    if (ensure(ctx->sgm_lr, b) != cudaSuccess) {
+        cudaGetLastError();   // an allocation failure leaves no sticky error
+        return nullptr;
+    }
+    return (float *)ctx->sgm_lr.p;
+}
+
 int upload(vll_context *ctx, Buf &b, const void *src, size_t n) {
     VLL_CUDA(ctx, ensure(b, n));
     if (n) VLL_CUDA(ctx, cudaMemcpyAsync(b.p, src, n, cudaMemcpyHostToDevice, ctx->stream));
@@ -733,6 +750,7 @@ void vll_destroy(vll_context *ctx) {
     release(ctx->pre_mag);
     release(ctx->pre_ori);
     release(ctx->sumcost);
+    release(ctx->sgm_lr);
     release(ctx->tin_pts);
     release(ctx->tin_tris);
     release(ctx->tin_scratch);
@@ -994,7 +1012,8 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugri
     if (sgm) {
         VLL_CUDA(ctx, ensure(ctx->sumcost, (size_t)(off[N] > 0 ? off[N] : 1) * sizeof(float)));
         VLL_CUDA(ctx, vll::launch_sgm((const DevLevel *)ctx->level.p, P.grid_w, P.grid_h, max_h,
-                                      (float *)ctx->sumcost.p, off[N], ctx->stream));
+                                      (float *)ctx->sumcost.p, off[N], ctx->stream,
+                                      sgm_scratch(ctx, off[N])));
         sumcost = (const float *)ctx->sumcost.p;
     }
     VLL_CUDA(ctx, vll::launch_awncc((const DevLevel *)ctx->level.p, N, sumcost, ctx->stream));
@@ -1568,7 +1587,8 @@ int vll_awncc_peaks_device(vll_context *ctx, const vll_level_desc *desc,
     if (sgm) {
         VLL_CUDA(ctx, ensure(ctx->sumcost, (size_t)(total > 0 ? total : 1) * sizeof(float)));
         VLL_CUDA(ctx, vll::launch_sgm((const DevLevel *)ctx->level.p, P.grid_w, P.grid_h, max_h,
-                                      (float *)ctx->sumcost.p, total, ctx->stream));
+                                      (float *)ctx->sumcost.p, total, ctx->stream,
+                                      sgm_scratch(ctx, total)));
         sumcost = (const float *)ctx->sumcost.p;
         ctx->launches_total += 8;
     }

@@ -21,13 +21,16 @@ cudaError_t launch_ortho(const DevLevel *dP, int64_t total, double2 *const *cd,
 cudaError_t launch_awncc(const DevLevel *dP, int64_t n_nodes, const float *sumcost,
                          cudaStream_t s);
 
-// vll_sgm.cu: the 8-direction aggregation of AWNCC into sumcost (packed like
-// the voxel rows); max_h is the level's largest NumOfHeight.
 // vll_plain.cu: the largest row length and the total (off[n]) of a packing.
 cudaError_t row_extent(const vll_nccresult *ncc, int64_t n, const int64_t *off, int *d_max,
                        int *max_h, int64_t *total, cudaStream_t s);
+// vll_sgm.cu: the 8-direction aggregation of AWNCC into sumcost (packed like
+// the voxel rows); max_h is the level's largest NumOfHeight.  lr: scratch of
+// sgm_scratch_bytes(n_slots) for the all-directions form, or nullptr (one
+// launch per direction); sgm_scratch_bytes is 0 above its memory budget.
+size_t sgm_scratch_bytes(int64_t n_slots);
 cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int max_h,
-                       float *sumcost, int64_t n_slots, cudaStream_t s);
+                       float *sumcost, int64_t n_slots, cudaStream_t s, float *lr);
 cudaError_t launch_gncc(const DevLevel *dP, int64_t n_nodes, double *gsum, double *gcnt,
                         cudaStream_t s);
 cudaError_t launch_recheck(const DevLevel *dP, const int64_t *items,

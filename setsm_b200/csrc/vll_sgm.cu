@@ -11,9 +11,11 @@
 // order (0: left->right, 1: right->left, 2: top->bottom, 3: bottom->top,
 // 4..7: the diagonals).
 //
-// GPU mapping: one launch per direction (which keeps the per-node order of
-// the float sums), one warp per path, lanes over the height slots of the
-// current node; the previous node's costs and the current ones live in two
+// GPU mapping: one warp per path, lanes over the height slots of the current
+// node.  All 8 directions run in one launch, each storing its path costs per
+// slot, and a second pass adds the 8 in the reference's order (the float sums
+// come out the same); when the 8 stores do not fit the scratch budget, one
+// launch per direction accumulates in order instead.  In both, the previous node's costs and the current ones live in two
 // shared-memory rows of the warp.  A diagonal direction's paths start from two
 // walls (a column of rows and a row of columns); the path that starts at their
 // common corner is walked by both of the reference's loops, so its nodes get
@@ -73,11 +75,26 @@ __device__ __forceinline__ bool path_of(int dir, int64_t line, int64_t W, int64_
 
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
 
+// Lines of direction `dir`.
+__host__ __device__ __forceinline__ int64_t lines_of(int dir, int64_t W, int64_t H) {
+    return dir < 2 ? H : (dir < 4 ? W : H + W);
+}
+
+// One direction's path costs.  Accumulating form (lr == nullptr): the costs
+// are added into sumcost (one launch per direction, in order).  Storing form:
+// blockIdx.y is the direction and every slot's cost goes to lr[dir][slot]
+// (0 where the reference adds nothing), for sgm_sum_kernel.
 __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict__ Pp, int dir,
                                                       int64_t n_lines, float *__restrict__ sumcost,
-                                                      int max_h) {
+                                                      int max_h, float *__restrict__ lr,
+                                                      int64_t n_slots) {
     extern __shared__ float sm_lh[];
     const DevLevel &P = *Pp;
+    if (lr) {
+        dir = blockIdx.y;
+        n_lines = lines_of(dir, P.grid_w, P.grid_h);
+        lr += (int64_t)dir * n_slots;
+    }
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     float *buf0 = sm_lh + (size_t)warp * 2 * max_h;
@@ -104,10 +121,13 @@ __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict
                 float v = 0.f;
                 if (hgt >= (float)g.minHeight && hgt <= (float)g.maxHeight) {
                     v = (float)dq_voxel(vrow[h].INCC);
-                    float s = sc[h] + v;
-                    if (twice) s = s + v;
-                    sc[h] = s;
+                    if (!lr) {
+                        float s = sc[h] + v;
+                        if (twice) s = s + v;
+                        sc[h] = s;
+                    }
                 }
+                if (lr) lr[P.vox_off[pt] + h] = v;
                 pre[h] = v;
             }
             __syncwarp();
@@ -207,10 +227,13 @@ __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict
                     }
                     const double t = __dadd_rn(m, -(double)max_w);
                     out = (float)__dadd_rn(wncc, t);
-                    float s = sc[h] + out;
-                    if (twice) s = s + out;
-                    sc[h] = s;
+                    if (!lr) {
+                        float s = sc[h] + out;
+                        if (twice) s = s + out;
+                        sc[h] = s;
+                    }
                 }
+                if (lr) lr[P.vox_off[pt] + h] = out;
                 cur[h] = out;
             }
             __syncwarp();
@@ -222,15 +245,58 @@ __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict
     }
 }
 
+// SumCost of every slot from the 8 stored direction costs, added in the
+// reference's direction order, a diagonal's corner path twice (the nodes
+// (k, k) of direction 4, (k, W-1-k) of 5, (H-1-k, k) of 6, (H-1-k, W-1-k) of 7).
+__global__ void sgm_sum_kernel(const DevLevel *__restrict__ Pp, const float *__restrict__ lr,
+                               int64_t n_slots, float *__restrict__ sumcost) {
+    const DevLevel &P = *Pp;
+    const int64_t W = P.grid_w, H = P.grid_h;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t pt = warp; pt < P.n_nodes; pt += n_warps) {
+        const int64_t r = pt / W, c = pt % W;
+        const bool twice[8] = {false, false, false, false, r == c, r == W - 1 - c,
+                               H - 1 - r == c, H - 1 - r == W - 1 - c};
+        const int64_t o = P.vox_off[pt];
+        const int n = P.ncc[pt].NumOfHeight;
+        for (int h = lane; h < n; h += 32) {
+            float sc = 0.f;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                const float v = lr[(int64_t)d * n_slots + o + h];
+                sc = sc + v;
+                if (twice[d]) sc = sc + v;
+            }
+            sumcost[o + h] = sc;
+        }
+    }
+}
+
 }  // namespace
 
+// The stored-direction form needs 8 floats per slot of scratch; it runs when
+// that fits this budget, else the directions run one launch after another.
+constexpr double kSgmConcurrentBytes = 24e9;
+
+size_t sgm_scratch_bytes(int64_t n_slots) {
+    const double b = 8.0 * 4.0 * (double)(n_slots > 0 ? n_slots : 1);
+    return b <= kSgmConcurrentBytes ? (size_t)b : 0;
+}
+
 // All 8 directions of the aggregation into sumcost (float, the packed voxel
-// layout, zeroed here), one launch per direction in the reference's order.
-// max_h: the largest NumOfHeight of the level.
+// layout).  With `lr` (sgm_scratch_bytes(n_slots) bytes) the 8 directions run
+// in one launch and sgm_sum_kernel forms the sums; without, one launch per
+// direction in the reference's order accumulates them.  max_h: the largest
+// NumOfHeight of the level.
 cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int max_h,
-                       float *sumcost, int64_t n_slots, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(sumcost, 0, (size_t)(n_slots > 0 ? n_slots : 1) * 4, s);
-    if (e != cudaSuccess) return e;
+                       float *sumcost, int64_t n_slots, cudaStream_t s, float *lr) {
+    cudaError_t e;
+    if (!lr) {
+        e = cudaMemsetAsync(sumcost, 0, (size_t)(n_slots > 0 ? n_slots : 1) * 4, s);
+        if (e != cudaSuccess) return e;
+    }
     if (max_h < 1) max_h = 1;
     const size_t per_warp = (size_t)2 * max_h * sizeof(float);
     if (per_warp > 200 * 1024) return cudaErrorInvalidValue;
@@ -239,12 +305,29 @@ cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int m
     const size_t smem = per_warp * warps;
     e = cudaFuncSetAttribute(sgm_dir_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if (lr) {
+        // every direction at once (blockIdx.y); blocks beyond a direction's
+        // lines find no path and return
+        const int64_t most = grid_h + grid_w;
+        int64_t blocks = (most + warps - 1) / warps;
+        if (blocks > 148 * 64) blocks = 148 * 64;
+        if (blocks < 1) blocks = 1;
+        sgm_dir_kernel<<<dim3((unsigned)blocks, 8), warps * 32, smem, s>>>(dP, 0, 0, sumcost, max_h,
+                                                                          lr, n_slots);
+        if ((e = cudaGetLastError())) return e;
+        int64_t sb = (grid_w * grid_h + 7) / 8;
+        if (sb > 148 * 32) sb = 148 * 32;
+        if (sb < 1) sb = 1;
+        sgm_sum_kernel<<<(unsigned)sb, 256, 0, s>>>(dP, lr, n_slots, sumcost);
+        return cudaGetLastError();
+    }
     for (int dir = 0; dir < 8; ++dir) {
-        const int64_t n_lines = dir < 2 ? grid_h : (dir < 4 ? grid_w : grid_h + grid_w);
+        const int64_t n_lines = lines_of(dir, grid_w, grid_h);
         int64_t blocks = (n_lines + warps - 1) / warps;
         if (blocks > 148 * 64) blocks = 148 * 64;
         if (blocks < 1) blocks = 1;
-        sgm_dir_kernel<<<(unsigned)blocks, warps * 32, smem, s>>>(dP, dir, n_lines, sumcost, max_h);
+        sgm_dir_kernel<<<(unsigned)blocks, warps * 32, smem, s>>>(dP, dir, n_lines, sumcost, max_h,
+                                                                 nullptr, n_slots);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

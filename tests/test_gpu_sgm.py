@@ -52,3 +52,16 @@ def test_sgm_awncc_matches_reference_build(gpu_ctx, seed):
     assert cases.field_mismatch(ncc, r["vll_ncc"]) == {}
     gpu_ctx.awncc(inp2, ncc, vox)
     assert cases.field_mismatch(ncc, r["ncc"]) == {}
+
+
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_SGM))
+def test_sgm_per_direction_form_matches_fixture(gpu_ctx, name, monkeypatch):
+    """The per-direction launches (used when the 8 stored directions exceed the
+    memory budget) give the same NCCresult as the all-directions form."""
+    monkeypatch.setenv("SETSM_VLL_SGM_SEQUENTIAL", "1")
+    inp, g = golden_sgm(name)
+    inp.gridpt3 = g["init_gp3"].copy()
+    ncc = g["vll_ncc"].copy()
+    vox = g["vll_vox"].copy()
+    gpu_ctx.awncc(inp, ncc, vox)
+    assert cases.field_mismatch(ncc, g["ncc"]) == {}
