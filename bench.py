@@ -780,6 +780,24 @@ def run_height_range(args):
     ctx = vll.Context(0)
     inp, g0, pts, tris = tin_workload(ctx)
     it, mpp = 2, 1.5
+    n = int(inp.n)
+    d = inp.desc()
+    d_pts = torch.from_numpy(pts.view(np.uint8).copy()).cuda()
+    d_tris = torch.from_numpy(tris.view(np.uint8).copy()).cuda()
+    d_g0 = torch.from_numpy(g0.view(np.uint8).copy()).cuda()
+    d_g = torch.empty_like(d_g0)
+    d_out = torch.empty(n * 20, dtype=torch.uint8, device="cuda:0")
+
+    def dev_call():
+        d_g.copy_(d_g0)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ctx.set_height_range_device(d, d_pts.data_ptr(), len(pts), d_tris.data_ptr(), len(tris),
+                                    d_g.data_ptr(), d_out.data_ptr(), it, mpp, False)
+        return (time.perf_counter() - t) * 1e3
+    for _ in range(max(1, args.warmup)):
+        dev_call()
+    dev_ms = statistics.median(dev_call() for _ in range(args.steps))
 
     def call():
         inp.gridpt3 = g0.copy()
@@ -804,17 +822,17 @@ def run_height_range(args):
     t = time.perf_counter()
     want, wext = refpy.set_height_range(ref, pts, tris, it, mpp, False)
     cpu_s = time.perf_counter() - t
-    n = int(inp.n)
     line = {
-        "metric": "grid nodes/s (SetHeightRange)", "value": n / (ms / 1e3), "unit": "nodes/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": ms,
+        "metric": "grid nodes/s (SetHeightRange)", "value": n / (dev_ms / 1e3), "unit": "nodes/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": dev_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (the reference's arithmetic)", "data": "synthetic",
         "config": {"workload": "SetHeightRange: 1024^2 grid at 2 m, 21 k matched points, "
                                "Delaunay TIN, level 0, iteration 2, MPP 1.5",
                    "nodes": n, "points": int(len(pts)), "triangles": int(len(tris))},
         "e2e": {"value": n / (ms / 1e3), "unit": "nodes/s",
-                "timing": "host wall clock of the C-ABI call on host buffers (the call waits)"},
+                "timing": "host wall clock of vll_set_height_range on host buffers (copies "
+                          "included; value: vll_set_height_range_device on resident data)"},
         "cpu_baseline": {"value": n / cpu_s, "unit": "nodes/s", "cores": os.cpu_count(),
                          "kind": "reference", "sample": f"whole grid, {cpu_s:.3f} s"},
         "gpu_launches": int(launches),
@@ -942,7 +960,7 @@ def run_select_mps(args):
     level 0, iteration 1, its UGRID.  GPU: the C ABI on host buffers (host
     wall clock of the call, copies included: the call waits); CPU: the
     reference's SelectMPs (sequential); points and UGRID compared.  Metric:
-    grid nodes per second."""
+    grid nodes per second (value: device-resident inputs)."""
     world, rank, local = dist_setup(args.gpus)
     if rank != 0:
         return
@@ -958,6 +976,23 @@ def run_select_mps(args):
     ctx.vertical_line_locus(inp, ncc, None, "split")
     g0 = inp.gridpt3.copy()
     sel_args = (0.6, 0.2, 0.8, 0.7, 1, 1.5, 1, 10.0)
+    # device-resident form: NCCresult, UGRID and grid points on the GPU
+    n = int(inp.n)
+    d = wl.device_desc(11)
+    d_ncc = torch.from_numpy(ncc.view(np.uint8).copy()).cuda()
+    d_g0 = torch.from_numpy(g0.view(np.uint8).copy()).cuda()
+    d_g = torch.empty_like(d_g0)
+    d_pts = torch.empty(n * 32, dtype=torch.uint8, device="cuda:0")
+
+    def dev_call():
+        d_g.copy_(d_g0)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ctx.select_mps_device(d, d_ncc.data_ptr(), d_g.data_ptr(), d_pts.data_ptr(), n, *sel_args)
+        return (time.perf_counter() - t) * 1e3
+    for _ in range(max(1, args.warmup)):
+        dev_call()
+    dev_ms = statistics.median(dev_call() for _ in range(args.steps))
 
     def call():
         inp.gridpt3 = g0.copy()
@@ -983,17 +1018,17 @@ def run_select_mps(args):
     cpu_s = time.perf_counter() - t
     same = len(pts) == len(want) and all(np.array_equal(pts[f], want[f])
                                          for f in ("x", "y", "z", "flag"))
-    n = int(inp.n)
     line = {
-        "metric": "grid nodes/s (SelectMPs)", "value": n / (ms / 1e3), "unit": "nodes/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": ms,
+        "metric": "grid nodes/s (SelectMPs)", "value": n / (dev_ms / 1e3), "unit": "nodes/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": dev_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (the reference's arithmetic)", "data": "synthetic",
         "config": {"workload": "SelectMPs: peaks of the 7x7 memory-tight matching of the reduced "
                                "C2 scene (1024^2 grid), level 0, iteration 1",
                    "nodes": n, "points": int(len(pts))},
         "e2e": {"value": n / (ms / 1e3), "unit": "nodes/s",
-                "timing": "host wall clock of the C-ABI call on host buffers (the call waits)"},
+                "timing": "host wall clock of vll_select_mps on host buffers (copies included; "
+                          "value: vll_select_mps_device on resident data, host clock)"},
         "cpu_baseline": {"value": n / cpu_s, "unit": "nodes/s", "cores": 1, "kind": "reference",
                          "sample": f"whole grid, {cpu_s:.3f} s (the reference's loop is serial)"},
         "gpu_launches": int(launches),

@@ -471,6 +471,15 @@ int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccre
                    double th_roh_next, int iteration, double mpp, int final_level_iteration,
                    double mpp_stereo_angle, vll_point3 *points, int64_t capacity,
                    int64_t *count);
+/* The same on device data (desc->grid_pts, the NCCresult, UGRID and points
+ * buffers are device pointers); on VLL_ERR_CAPACITY d_gridpt3 has been
+ * updated and no point written.  Waits. */
+int vll_select_mps_device(vll_context *ctx, const vll_level_desc *desc,
+                          const vll_nccresult *d_nccresult, vll_ugrid *d_gridpt3, double th_roh,
+                          double th_roh_min, double th_roh_start, double th_roh_next,
+                          int iteration, double mpp, int final_level_iteration,
+                          double mpp_stereo_angle, vll_point3 *d_points, int64_t capacity,
+                          int64_t *count);
 
 /*
  * SetHeightRange (setsm_code.cpp:9851-10255): the next iteration's height
@@ -490,6 +499,12 @@ int vll_set_height_range(vll_context *ctx, const vll_level_desc *desc, const vll
                          vll_ugrid *result, int iteration, double mpp,
                          int level_check_matching_rate, double seed_dem_sigma,
                          double *min_h_grid, double *max_h_grid);
+/* The same on device data (points, triangles, UGRID and result). Waits. */
+int vll_set_height_range_device(vll_context *ctx, const vll_level_desc *desc,
+                                const vll_point3 *d_pts, int64_t n_pts, const vll_tri *d_tris,
+                                int64_t n_tris, vll_ugrid *d_gridpt3, vll_ugrid *d_result,
+                                int iteration, double mpp, int level_check_matching_rate,
+                                double seed_dem_sigma, double *min_h_grid, double *max_h_grid);
 
 /* Diagnostics: the orthoimage coordinate raster of image `ti`
  * (SetOrthoImageCoord, setsm_code.cpp:6550-6670) at resolution im_res, on

@@ -1317,19 +1317,13 @@ int vll_initialize_voxel_device(vll_context *ctx, const vll_level_desc *desc,
     return rc;
 }
 
-int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccresult *nccresult,
-                   vll_ugrid *gridpt3, double th_roh, double th_roh_min, double th_roh_start,
-                   double th_roh_next, int iteration, double mpp, int final_level_iteration,
-                   double mpp_stereo_angle, vll_point3 *points, int64_t capacity,
-                   int64_t *count) {
-    NvtxRange nvtx_range("vll_select_mps");
-    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
-    if (!desc || !nccresult || !gridpt3 || !count || !desc->grid_pts ||
-        (capacity > 0 && !points) || capacity < 0)
-        return fail(ctx, VLL_ERR_INVALID, "null argument");
-    if (desc->grid_width <= 0 || desc->grid_height <= 0 ||
-        desc->grid_width * desc->grid_height > 0x7fffffff)
-        return fail(ctx, VLL_ERR_INVALID, "invalid grid size");
+// SelectMPs on device data; out: d_points (capacity entries).
+static int select_mps_run(vll_context *ctx, const vll_level_desc *desc, const vll_nccresult *d_ncc,
+                          vll_ugrid *d_gp3, const double *d_grid_pts, double th_roh,
+                          double th_roh_min, double th_roh_start, double th_roh_next,
+                          int iteration, double mpp, int final_level_iteration,
+                          double mpp_stereo_angle, vll_point3 *d_points, int64_t capacity,
+                          int64_t *count) {
     const int L = desc->pyramid_step;
     const bool is_ra = desc->is_ra != 0;
     // the level's quota of the histogram; unset in the reference above level 4
@@ -1352,21 +1346,14 @@ int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccre
     }
     if (!is_ra && L > 0 && !quota)
         return fail(ctx, VLL_ERR_UNSUPPORTED, "SelectMPs threshold undefined above level 4");
-    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
     const int64_t N = desc->grid_width * desc->grid_height;
-    int rc;
-    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
-    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
-    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
     const size_t bytes = vll::select_mps_scratch(N);
     VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
-    VLL_CUDA(ctx, ensure(ctx->tin_pts, (size_t)(capacity > 0 ? capacity : 1) * sizeof(vll_point3)));
     double minimum_th = 0.2;
     if (!is_ra && L > 0) {
         int hist[100];
         int64_t total = 0;
-        VLL_CUDA(ctx, vll::run_roh_hist((const vll_nccresult *)ctx->ncc.p, N, ctx->tin_scratch.p,
-                                        hist, &total, ctx->stream));
+        VLL_CUDA(ctx, vll::run_roh_hist(d_ncc, N, ctx->tin_scratch.p, hist, &total, ctx->stream));
         ctx->launches_total += 1;
         if (total > 0) {
             int roh_iter = 99;
@@ -1397,21 +1384,69 @@ int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccre
     a.mpp = mpp;
     a.mpp_stereo_angle = mpp_stereo_angle;
     int64_t n_sel = 0;
-    VLL_CUDA(ctx, vll::run_select_mps((const vll_nccresult *)ctx->ncc.p, (vll_ugrid *)ctx->gp3.p,
-                                      (const double *)ctx->pts.p, N, a, ctx->tin_scratch.p,
-                                      (vll_point3 *)ctx->tin_pts.p, capacity, &n_sel,
-                                      ctx->stream));
+    VLL_CUDA(ctx, vll::run_select_mps(d_ncc, d_gp3, d_grid_pts, N, a, ctx->tin_scratch.p,
+                                      d_points, capacity, &n_sel, ctx->stream));
     ctx->launches_total += 2;
     *count = n_sel;
     if (n_sel > capacity)
         return fail(ctx, VLL_ERR_CAPACITY, "more selected points than the points buffer holds");
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+static int select_mps_check(vll_context *ctx, const vll_level_desc *desc, const void *ncc,
+                            const void *gp3, const int64_t *count, const void *points,
+                            int64_t capacity) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !ncc || !gp3 || !count || !desc->grid_pts || (capacity > 0 && !points) ||
+        capacity < 0)
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    if (desc->grid_width <= 0 || desc->grid_height <= 0 ||
+        desc->grid_width * desc->grid_height > 0x7fffffff)
+        return fail(ctx, VLL_ERR_INVALID, "invalid grid size");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    return VLL_OK;
+}
+
+int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccresult *nccresult,
+                   vll_ugrid *gridpt3, double th_roh, double th_roh_min, double th_roh_start,
+                   double th_roh_next, int iteration, double mpp, int final_level_iteration,
+                   double mpp_stereo_angle, vll_point3 *points, int64_t capacity,
+                   int64_t *count) {
+    NvtxRange nvtx_range("vll_select_mps");
+    int rc = select_mps_check(ctx, desc, nccresult, gridpt3, count, points, capacity);
+    if (rc) return rc;
+    const int64_t N = desc->grid_width * desc->grid_height;
+    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
+    VLL_CUDA(ctx, ensure(ctx->tin_pts, (size_t)(capacity > 0 ? capacity : 1) * sizeof(vll_point3)));
+    rc = select_mps_run(ctx, desc, (const vll_nccresult *)ctx->ncc.p, (vll_ugrid *)ctx->gp3.p,
+                        (const double *)ctx->pts.p, th_roh, th_roh_min, th_roh_start,
+                        th_roh_next, iteration, mpp, final_level_iteration, mpp_stereo_angle,
+                        (vll_point3 *)ctx->tin_pts.p, capacity, count);
+    if (rc) return rc;   // host buffers untouched
     VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
                                   cudaMemcpyDeviceToHost, ctx->stream));
-    if (n_sel > 0)
-        VLL_CUDA(ctx, cudaMemcpyAsync(points, ctx->tin_pts.p, (size_t)n_sel * sizeof(vll_point3),
+    if (*count > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(points, ctx->tin_pts.p, (size_t)*count * sizeof(vll_point3),
                                       cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return VLL_OK;
+}
+
+int vll_select_mps_device(vll_context *ctx, const vll_level_desc *desc,
+                          const vll_nccresult *d_nccresult, vll_ugrid *d_gridpt3, double th_roh,
+                          double th_roh_min, double th_roh_start, double th_roh_next,
+                          int iteration, double mpp, int final_level_iteration,
+                          double mpp_stereo_angle, vll_point3 *d_points, int64_t capacity,
+                          int64_t *count) {
+    NvtxRange nvtx_range("vll_select_mps_device");
+    int rc = select_mps_check(ctx, desc, d_nccresult, d_gridpt3, count, d_points, capacity);
+    if (rc) return rc;
+    return select_mps_run(ctx, desc, d_nccresult, d_gridpt3, desc->grid_pts, th_roh, th_roh_min,
+                          th_roh_start, th_roh_next, iteration, mpp, final_level_iteration,
+                          mpp_stereo_angle, d_points, capacity, count);
 }
 
 // SetHeightRange's BufferOfHeight and th_HG (setsm_code.cpp:9863-9922).
@@ -1448,14 +1483,11 @@ static void height_range_constants(const vll_level_desc *d, int iteration, doubl
     *th_hg = th;
 }
 
-int vll_set_height_range(vll_context *ctx, const vll_level_desc *desc, const vll_point3 *pts,
-                         int64_t n_pts, const vll_tri *tris, int64_t n_tris, vll_ugrid *gridpt3,
-                         vll_ugrid *result, int iteration, double mpp,
-                         int level_check_matching_rate, double seed_dem_sigma,
-                         double *min_h_grid, double *max_h_grid) {
-    NvtxRange nvtx_range("vll_set_height_range");
+static int height_range_check(vll_context *ctx, const vll_level_desc *desc, const void *pts,
+                              int64_t n_pts, const void *tris, int64_t n_tris, const void *gp3,
+                              const void *result, const double *min_h, const double *max_h) {
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
-    if (!desc || !gridpt3 || !result || !min_h_grid || !max_h_grid || (n_pts > 0 && !pts) ||
+    if (!desc || !gp3 || !result || !min_h || !max_h || (n_pts > 0 && !pts) ||
         (n_tris > 0 && !tris))
         return fail(ctx, VLL_ERR_INVALID, "null argument");
     if (n_pts < 0 || n_tris < 0 || n_pts > 0x7fffffff || n_tris > 0x7fffffff)
@@ -1465,6 +1497,14 @@ int vll_set_height_range(vll_context *ctx, const vll_level_desc *desc, const vll
         desc->num_images > VLL_MAX_IMAGES)
         return fail(ctx, VLL_ERR_INVALID, "invalid grid, level or image count");
     VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    return VLL_OK;
+}
+
+// SetHeightRange on device data.
+static int height_range_run(vll_context *ctx, const vll_level_desc *desc, const vll_point3 *d_pts,
+                            int64_t n_pts, const vll_tri *d_tris, int64_t n_tris,
+                            vll_ugrid *d_gp3, vll_ugrid *d_result, int iteration, double mpp,
+                            int lcmr, double seed_dem_sigma, double *min_h, double *max_h) {
     // only the grid geometry, the level and the image selection are read
     DevLevel P;
     memset(&P, 0, sizeof(P));
@@ -1478,34 +1518,61 @@ int vll_set_height_range(vll_context *ctx, const vll_level_desc *desc, const vll
     P.grid_h = desc->grid_height;
     P.n_nodes = P.grid_w * P.grid_h;
     for (int ti = 0; ti < P.num_images; ++ti) P.im[ti].selected = desc->images[ti].selected != 0;
-    const int64_t N = P.n_nodes;
-    int rc;
+    P.gp3 = d_gp3;
+    int rc = upload_level_block(ctx, P);
+    if (rc) return rc;
+    const size_t bytes = vll::height_range_scratch(P.n_nodes);
+    VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
+    double buffer, th_hg;
+    height_range_constants(desc, iteration, mpp, lcmr != 0, seed_dem_sigma, &buffer, &th_hg);
+    // triangles with a vertex index >= n_pts are skipped, as the reference does;
+    // bounding boxes are clamped to the grid, so every node index is in range
+    VLL_CUDA(ctx, vll::run_height_range((const DevLevel *)ctx->level.p, P, d_pts, n_pts, d_tris,
+                                        n_tris, d_gp3, d_result, buffer, th_hg, iteration,
+                                        ctx->tin_scratch.p, bytes, min_h, max_h, ctx->stream));
+    ctx->launches_total += (n_tris > 0 ? 6 : 5);
+    return VLL_OK;
+}
+
+int vll_set_height_range(vll_context *ctx, const vll_level_desc *desc, const vll_point3 *pts,
+                         int64_t n_pts, const vll_tri *tris, int64_t n_tris, vll_ugrid *gridpt3,
+                         vll_ugrid *result, int iteration, double mpp,
+                         int level_check_matching_rate, double seed_dem_sigma,
+                         double *min_h_grid, double *max_h_grid) {
+    NvtxRange nvtx_range("vll_set_height_range");
+    int rc = height_range_check(ctx, desc, pts, n_pts, tris, n_tris, gridpt3, result, min_h_grid,
+                                max_h_grid);
+    if (rc) return rc;
+    const int64_t N = desc->grid_width * desc->grid_height;
     if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
     if ((rc = upload(ctx, ctx->tin_pts, pts, (size_t)n_pts * sizeof(vll_point3)))) return rc;
     if ((rc = upload(ctx, ctx->tin_tris, tris, (size_t)n_tris * sizeof(vll_tri)))) return rc;
-    // triangles with a vertex index >= n_pts are skipped, as the reference does;
-    // bounding boxes are clamped to the grid, so every node index is in range
     VLL_CUDA(ctx, ensure(ctx->ncc, (size_t)N * sizeof(vll_ugrid)));
-    const size_t bytes = vll::height_range_scratch(N);
-    VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
-    P.gp3 = (const vll_ugrid *)ctx->gp3.p;
-    if ((rc = upload_level_block(ctx, P))) return rc;
-    double buffer, th_hg;
-    height_range_constants(desc, iteration, mpp, level_check_matching_rate != 0, seed_dem_sigma,
-                           &buffer, &th_hg);
-    VLL_CUDA(ctx, vll::run_height_range((const DevLevel *)ctx->level.p, P,
-                                        (const vll_point3 *)ctx->tin_pts.p, n_pts,
-                                        (const vll_tri *)ctx->tin_tris.p, n_tris,
-                                        (vll_ugrid *)ctx->gp3.p, (vll_ugrid *)ctx->ncc.p, buffer,
-                                        th_hg, iteration, ctx->tin_scratch.p, bytes, min_h_grid,
-                                        max_h_grid, ctx->stream));
-    ctx->launches_total += (n_tris > 0 ? 6 : 5);
+    if ((rc = height_range_run(ctx, desc, (const vll_point3 *)ctx->tin_pts.p, n_pts,
+                               (const vll_tri *)ctx->tin_tris.p, n_tris, (vll_ugrid *)ctx->gp3.p,
+                               (vll_ugrid *)ctx->ncc.p, iteration, mpp, level_check_matching_rate,
+                               seed_dem_sigma, min_h_grid, max_h_grid)))
+        return rc;
     VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
                                   cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaMemcpyAsync(result, ctx->ncc.p, (size_t)N * sizeof(vll_ugrid),
                                   cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return VLL_OK;
+}
+
+int vll_set_height_range_device(vll_context *ctx, const vll_level_desc *desc,
+                                const vll_point3 *d_pts, int64_t n_pts, const vll_tri *d_tris,
+                                int64_t n_tris, vll_ugrid *d_gridpt3, vll_ugrid *d_result,
+                                int iteration, double mpp, int level_check_matching_rate,
+                                double seed_dem_sigma, double *min_h_grid, double *max_h_grid) {
+    NvtxRange nvtx_range("vll_set_height_range_device");
+    int rc = height_range_check(ctx, desc, d_pts, n_pts, d_tris, n_tris, d_gridpt3, d_result,
+                                min_h_grid, max_h_grid);
+    if (rc) return rc;
+    return height_range_run(ctx, desc, d_pts, n_pts, d_tris, n_tris, d_gridpt3, d_result,
+                            iteration, mpp, level_check_matching_rate, seed_dem_sigma,
+                            min_h_grid, max_h_grid);
 }
 
 int vll_debug_ortho_raster(vll_context *ctx, const vll_level_desc *desc, const vll_ugrid *gridpt3,

@@ -35,7 +35,8 @@ EXPORTED = [
     "vll_vertical_line_locus_blunder", "vll_vertical_line_locus_blunder_device",
     "vll_vertical_line_locus_ortho", "vll_ortho_blunder", "vll_ortho_blunder_device",
     "vll_set_height_range", "vll_select_mps", "vll_initialize_voxel",
-    "vll_initialize_voxel_device", "vll_awncc_peaks_device",
+    "vll_initialize_voxel_device", "vll_awncc_peaks_device", "vll_select_mps_device",
+    "vll_set_height_range_device",
 ]
 
 _lib = None
@@ -109,6 +110,8 @@ def load():
     L.vll_awncc_peaks_device.argtypes = [vp, D, vp, vp, vp, vp, S]
     L.vll_select_mps.argtypes = [vp, D, vp, vp, dbl, dbl, dbl, dbl, i32, dbl, i32, dbl, vp, i64,
                                  C.POINTER(i64)]
+    L.vll_select_mps_device.argtypes = L.vll_select_mps.argtypes
+    L.vll_set_height_range_device.argtypes = L.vll_set_height_range.argtypes
     _lib = L
     return L
 
@@ -313,6 +316,28 @@ class Context:
             float(mpp), int(final_level_iteration), float(mpp_stereo_angle), out.ctypes.data,
             len(out), C.byref(n)))
         return out[: n.value].copy()
+
+    def select_mps_device(self, desc, d_ncc: int, d_gridpt3: int, d_points: int, capacity: int,
+                          *args) -> int:
+        """SelectMPs on device data (desc.grid_pts a device pointer); args as
+        select_mps's after ncc.  Returns the number of points."""
+        th_roh, th_min, th_start, th_next, it, mpp, fli, angle = args
+        n = C.c_int64()
+        self._check(load().vll_select_mps_device(
+            self._h, C.byref(desc), d_ncc, d_gridpt3, float(th_roh), float(th_min),
+            float(th_start), float(th_next), int(it), float(mpp), int(fli), float(angle),
+            d_points, int(capacity), C.byref(n)))
+        return n.value
+
+    def set_height_range_device(self, desc, d_pts: int, n_pts: int, d_tris: int, n_tris: int,
+                                d_gridpt3: int, d_result: int, iteration: int, mpp: float,
+                                lcmr: bool, seed_dem_sigma: float = 0.0):
+        lo, hi = C.c_double(), C.c_double()
+        self._check(load().vll_set_height_range_device(
+            self._h, C.byref(desc), d_pts, n_pts, d_tris, n_tris, d_gridpt3, d_result,
+            int(iteration), float(mpp), int(bool(lcmr)), float(seed_dem_sigma), C.byref(lo),
+            C.byref(hi)))
+        return lo.value, hi.value
 
     def set_height_range(self, inputs, pts: np.ndarray, tris: np.ndarray, iteration: int,
                          mpp: float, level_check_matching_rate: bool,

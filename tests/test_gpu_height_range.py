@@ -65,3 +65,22 @@ def test_empty_tin(gpu_ctx):
     inp, pts, tris, _ = mg.range_case("range_l0")
     out, ext = gpu_ctx.set_height_range(inp, pts, tris[:0], 1, 1.5, False)
     assert np.all(out["Height"] == -1000)
+
+
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_RANGE))
+def test_device_entry_point(gpu_ctx, name):
+    import torch
+    v = mg.GOLDEN_RANGE[name]
+    inp, pts, tris, z = mg.range_case(name)
+    d_pts = torch.from_numpy(pts.view(np.uint8).copy()).cuda()
+    d_tris = torch.from_numpy(tris.view(np.uint8).copy()).cuda()
+    d_gp3 = torch.from_numpy(inp.gridpt3.view(np.uint8).copy()).cuda()
+    d_out = torch.zeros(inp.n * 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ext = gpu_ctx.set_height_range_device(inp.desc(), d_pts.data_ptr(), len(pts),
+                                          d_tris.data_ptr(), len(tris), d_gp3.data_ptr(),
+                                          d_out.data_ptr(), v["iteration"], v["mpp"], v["lcmr"],
+                                          v.get("sigma", 0.0))
+    out = d_out.cpu().numpy().view(abi.UGRID_DTYPE)
+    assert cases.field_mismatch(mg.clean(out), z["result"].view(abi.UGRID_DTYPE)) == {}
+    assert ext == tuple(z["extent"])

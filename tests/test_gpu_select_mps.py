@@ -79,3 +79,19 @@ def test_capacity_error_leaves_inputs(gpu_ctx):
     assert rc == abi.VLL_ERR_CAPACITY
     assert n.value == int(z["ret"]) > 4
     assert cases.field_mismatch(inp.gridpt3, before) == {}
+
+
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_SELECT))
+def test_device_entry_point(gpu_ctx, name):
+    import torch
+    inp, ncc, z = mg.select_case(name)
+    io, keep = cases.device_level(torch, inp, ncc)
+    d_pts = torch.zeros(inp.n * 32, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    n = gpu_ctx.select_mps_device(io[0], io[2], io[1], d_pts.data_ptr(), inp.n,
+                                  *mg.GOLDEN_SELECT[name]["args"])
+    assert n == int(z["ret"])
+    pts = d_pts.cpu().numpy().view(abi.POINT3_DTYPE)[:n]
+    assert same_points(pts, z["pts"].view(abi.POINT3_DTYPE))
+    gp3 = cases.from_device(keep["gp3"], abi.UGRID_DTYPE)
+    assert cases.field_mismatch(mg.clean(gp3), z["gp3"].view(abi.UGRID_DTYPE)) == {}
