@@ -482,6 +482,25 @@ int vll_select_mps_device(vll_context *ctx, const vll_level_desc *desc,
                           int64_t *count);
 
 /*
+ * blunder_detection_TIN (setsm_code.cpp:9158-9787): marks the matched points
+ * whose TIN neighbourhood is inconsistent in height.  Statistics over the
+ * triangles (the vertices' ortho_ncc, the edges' height differences against
+ * hinterval = *LevelInfo.Hinterval) set the thresholds; each point not already
+ * flagged 1 then tests its first 30 triangles and may flag itself or a
+ * neighbour as a blunder (pts[].flag 1, detected_blunders[] set for points that
+ * were 0), resets / sets its node's anchor_flag; blunder_count[0..1] are
+ * incremented by the kept / blunder points and *minz_mp / *maxz_mp take the
+ * kept points' height extent.  Does nothing at level 0, iteration 3, as the
+ * reference.  Host buffers; bit-exact with the reference.
+ */
+int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int iteration,
+                              const float *ortho_ncc, int flag_blunder, int count_bl,
+                              double hinterval, vll_point3 *pts, uint8_t *detected_blunders,
+                              int64_t n_pts, const vll_tri *tris, int64_t n_tris,
+                              vll_ugrid *gridpt3, int64_t *blunder_count, double *minz_mp,
+                              double *maxz_mp);
+
+/*
  * SetHeightRange (setsm_code.cpp:9851-10255): the next iteration's height
  * ranges from the TIN of matched points.  Every grid node inside a triangle
  * takes the plane's height (the vertex height on a vertex at levels 0-1) and

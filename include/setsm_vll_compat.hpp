@@ -245,6 +245,13 @@ void InitializeVoxel(const ProjectInfo *proinfo, tagVoxelinfo **grid_voxel,
 void AWNCC(ProjectInfo *proinfo, tagVoxelinfo **grid_voxel, tagCSize Size_Grid2D,
            UpdateGrid *GridPT3, tagNCCresult *nccresult, double step_height,
            unsigned char Pyramid_step, unsigned char iteration, int MaxNumberofHeightVoxel);
+// blunder_detection_TIN (setsm_code.hpp:116), same behaviour; returns true.
+bool blunder_detection_TIN(const ProjectInfo *proinfo, taglevelinfo &plevelinfo,
+                           const int iteration, float *ortho_ncc, bool flag_blunder,
+                           unsigned short count_bl, tagD3DPoint *pts, bool *detectedBlunders,
+                           long num_points, tagUI3DPoint *tris, long num_triangles,
+                           UpdateGrid *Gridpts, long *blunder_count, double *minz_mp,
+                           double *maxz_mp);
 // SelectMPs (setsm_code.hpp:99), same behaviour: appends the matched points
 // to *linkedlist, updates GridPT3, returns their number.
 long SelectMPs(const ProjectInfo *proinfo, taglevelinfo &plevelinfo,

@@ -500,6 +500,29 @@ long ref_select_mps(void *fn, const vll_level_desc *d, const vll_nccresult *ncc,
     return r;
 }
 
+/* blunder_detection_TIN (setsm_code.cpp:9158-9787), or the function at `fn`
+ * with its signature (setsm_code.hpp:116); everything in / out in place,
+ * counts[2] and zext[2] (min, max) accumulated as the reference does. */
+typedef bool (*tin_blunder_signature)(const ProInfo *, LevelInfo &, const int, float *, bool,
+                                      uint16, D3DPOINT *, bool *, long, UI3DPOINT *, long,
+                                      UGRID *, long *, double *, double *);
+int ref_blunder_detection_tin(void *fn, const vll_level_desc *d, int iteration, float *ortho_ncc,
+                              int flag_blunder, int count_bl, double hinterval, vll_point3 *pts,
+                              uint8_t *detected, long n_pts, vll_tri *tris, long n_tris,
+                              vll_ugrid *gridpt3, long *counts, double *zext) {
+    RefLevel L(d);
+    L.li.Hinterval = &hinterval;
+    tin_blunder_signature f = fn ? reinterpret_cast<tin_blunder_signature>(fn)
+                                 : &blunder_detection_TIN;
+    static_assert(sizeof(bool) == 1, "bool layout");
+    return f(L.proinfo, L.li, iteration, ortho_ncc, flag_blunder != 0, (uint16)count_bl,
+             reinterpret_cast<D3DPOINT *>(pts), reinterpret_cast<bool *>(detected), n_pts,
+             reinterpret_cast<UI3DPOINT *>(tris), n_tris, reinterpret_cast<UGRID *>(gridpt3),
+             counts, &zext[0], &zext[1])
+               ? 1
+               : 0;
+}
+
 /* SetHeightRange (setsm_code.cpp:9851-10255) on a copy of gridpt3 (the
  * reference frees its GridPT3); result and the extent {min, max} out. */
 typedef UGRID *(*set_height_range_signature)(ProInfo *, LevelInfo &, NCCresult *, const int,

@@ -440,3 +440,24 @@ def call_awncc(fn_addr: int, inputs, ncc, voxels) -> None:
     with _StdoutToStderr():
         L.ref_call_awncc(fn_addr, C.byref(d), inputs.gridpt3.ctypes.data, ncc.ctypes.data,
                          voxels.ctypes.data, voxels.size)
+
+
+def blunder_detection_tin(inputs, iteration, ortho_ncc, flag_blunder, count_bl, hinterval, pts,
+                          detected, tris, counts, zext, fn_addr: int | None = None) -> int:
+    """blunder_detection_TIN (setsm_code.cpp:9158-9787), or the function at
+    fn_addr with its signature (setsm_code.hpp:116).  pts, detected (uint8),
+    inputs.gridpt3, counts (int64[2]) and zext (float64[2]: min, max) are
+    updated in place."""
+    L = lib()
+    L.ref_blunder_detection_tin.argtypes = [C.c_void_p, C.POINTER(abi.LevelDesc), C.c_int,
+                                            C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p,
+                                            C.c_void_p, C.c_long, C.c_void_p, C.c_long,
+                                            C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ref_blunder_detection_tin.restype = C.c_int
+    d = inputs.desc()
+    with _StdoutToStderr():
+        return int(L.ref_blunder_detection_tin(
+            fn_addr, C.byref(d), int(iteration), ortho_ncc.ctypes.data, int(bool(flag_blunder)),
+            int(count_bl), float(hinterval), pts.ctypes.data, detected.ctypes.data, len(pts),
+            tris.ctypes.data, len(tris), inputs.gridpt3.ctypes.data, counts.ctypes.data,
+            zext.ctypes.data))

@@ -31,6 +31,7 @@ SOURCES = {
     "vll_heightrange.cu": ["-fmad=false"],
     "vll_selectmps.cu": ["-fmad=false"],
     "vll_initvoxel.cu": ["-fmad=false"],
+    "vll_tinblunder.cu": ["-fmad=false"],
     "vll_split.cu": [],
     "vll_capi.cu": [],
     "vll_shim.cu": [],

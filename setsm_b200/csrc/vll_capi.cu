@@ -1483,6 +1483,80 @@ static void height_range_constants(const vll_level_desc *d, int iteration, doubl
     *th_hg = th;
 }
 
+int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int iteration,
+                              const float *ortho_ncc, int flag_blunder, int count_bl,
+                              double hinterval, vll_point3 *pts, uint8_t *detected_blunders,
+                              int64_t n_pts, const vll_tri *tris, int64_t n_tris,
+                              vll_ugrid *gridpt3, int64_t *blunder_count, double *minz_mp,
+                              double *maxz_mp) {
+    NvtxRange nvtx_range("vll_blunder_detection_tin");
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!desc || !ortho_ncc || !gridpt3 || !blunder_count || !minz_mp || !maxz_mp ||
+        (n_pts > 0 && (!pts || !detected_blunders)) || (n_tris > 0 && !tris))
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    if (n_pts < 0 || n_tris < 0 || n_pts > 0x7fffffff || 3 * n_tris > 0x7fffffff)
+        return fail(ctx, VLL_ERR_INVALID, "point or triangle count out of range");
+    if (desc->grid_width <= 0 || desc->grid_height <= 0 || !(desc->grid_resolution > 0) ||
+        desc->pyramid_step < 0 || desc->pyramid_step > 12)
+        return fail(ctx, VLL_ERR_INVALID, "invalid grid or level");
+    if (desc->pyramid_step == 0 && iteration == 3) return VLL_OK;   // the reference skips it
+    if (!(hinterval >= 0) || hinterval > 1e8)
+        return fail(ctx, VLL_ERR_INVALID, "Hinterval out of range");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int64_t N = desc->grid_width * desc->grid_height;
+    const uint32_t hdiffcount = (uint32_t)hinterval;
+    vll::TinArgs a;
+    a.b0 = desc->boundary[0];
+    a.b1 = desc->boundary[1];
+    a.gs = desc->grid_resolution;
+    a.width = desc->grid_width;
+    a.n_nodes = N;
+    a.n_pts = n_pts;
+    a.n_tris = n_tris;
+    a.L = desc->pyramid_step;
+    a.iteration = iteration;
+    a.is_ra = desc->is_ra != 0;
+    a.flag_blunder = flag_blunder != 0;
+    a.count_bl = count_bl;
+    a.height_th = a.ortho_ncc_th = a.th_ref_ncc = 0;
+    a.hinterval = hinterval;
+    int rc;
+    if ((rc = upload(ctx, ctx->tin_pts, pts, (size_t)n_pts * sizeof(vll_point3)))) return rc;
+    if ((rc = upload(ctx, ctx->tin_tris, tris, (size_t)n_tris * sizeof(vll_tri)))) return rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->gsum, ortho_ncc, (size_t)N * sizeof(float)))) return rc;
+    if ((rc = upload(ctx, ctx->gcnt, detected_blunders, (size_t)(n_pts > 0 ? n_pts : 1))))
+        return rc;
+    const size_t bytes = vll::tin_blunder_scratch(n_pts, n_tris, hdiffcount);
+    VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
+    vll::TinThresholds th{0, 0, 0};
+    vll::TinOutput out;
+    memset(&out, 0, sizeof(out));
+    VLL_CUDA(ctx, vll::run_tin_blunder(a, (vll_point3 *)ctx->tin_pts.p,
+                                       (const vll_tri *)ctx->tin_tris.p,
+                                       (const float *)ctx->gsum.p, (vll_ugrid *)ctx->gp3.p,
+                                       (uint8_t *)ctx->gcnt.p, hdiffcount, ctx->tin_scratch.p,
+                                       bytes, th, &out, ctx->stream));
+    if (out.bad_input) return fail(ctx, VLL_ERR_INVALID, "a point's grid node lies outside the grid");
+    ctx->launches_total += 7;
+    if (n_pts > 0) {
+        VLL_CUDA(ctx, cudaMemcpyAsync(pts, ctx->tin_pts.p, (size_t)n_pts * sizeof(vll_point3),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        VLL_CUDA(ctx, cudaMemcpyAsync(detected_blunders, ctx->gcnt.p, (size_t)n_pts,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    blunder_count[0] += out.count[0];
+    blunder_count[1] += out.count[1];
+    if (out.has_z) {
+        if (*minz_mp > out.z[0]) *minz_mp = out.z[0];
+        if (*maxz_mp < out.z[1]) *maxz_mp = out.z[1];
+    }
+    return VLL_OK;
+}
+
 static int height_range_check(vll_context *ctx, const vll_level_desc *desc, const void *pts,
                               int64_t n_pts, const void *tris, int64_t n_tris, const void *gp3,
                               const void *result, const double *min_h, const double *max_h) {

@@ -53,6 +53,34 @@ cudaError_t launch_blunder(const DevLevel *dP, int64_t n_nodes, double2 *const *
                            int64_t oh, double im_res, int H, vll_ugrid *gout, float *ncc_out,
                            cudaStream_t s);
 
+// vll_tinblunder.cu: blunder_detection_TIN.  TinArgs: the grid geometry,
+// sizes, switches and (filled by run_tin_blunder) the thresholds.
+struct TinArgs {
+    double b0, b1, gs;
+    int64_t width, n_nodes, n_pts, n_tris;
+    int L, iteration, is_ra, flag_blunder, count_bl;
+    double height_th, ortho_ncc_th, th_ref_ncc, hinterval;
+};
+struct TinThresholds {
+    double height_th, ortho_ncc_th, th_ref_ncc;
+};
+struct TinOutput {
+    int bad_input;        // a vertex's grid node outside the grid
+    int64_t count[2];     // blunder_count additions: [0] kept, [1] blunders
+    int has_z;            // z: height extent of the kept points
+    double z[2];
+    double height_th;
+};
+// The thresholds from the triangle statistics (sums: ortho NCC sum, sum of
+// squares, dh sum, sum of squares, counts), as the reference derives them.
+void tin_thresholds(const TinArgs &a, const double *sums, const uint32_t *hbin,
+                    uint32_t hdiffcount, TinThresholds *th);
+size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount);
+cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
+                            const float *ortho_ncc, vll_ugrid *gp3, uint8_t *detected,
+                            uint32_t hdiffcount, void *scratch, size_t bytes,
+                            const TinThresholds &th_in, TinOutput *out, cudaStream_t s);
+
 // vll_initvoxel.cu: InitializeVoxel.  run_init_voxel decides every node
 // (into scratch) and fills new_off[0..n] with the new packing, *total the new
 // voxel count, *old_total the count of the incoming packing; run_commit_voxel

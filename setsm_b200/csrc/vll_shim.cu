@@ -329,6 +329,35 @@ void AWNCC(ProjectInfo *proinfo, tagVoxelinfo **grid_voxel, tagCSize Size_Grid2D
         die("AWNCC: GPU call failed", vll_last_error(ctx));
 }
 
+bool blunder_detection_TIN(const ProjectInfo *proinfo, taglevelinfo &pl, const int iteration,
+                           float *ortho_ncc, bool flag_blunder, unsigned short count_bl,
+                           tagD3DPoint *pts, bool *detectedBlunders, long num_points,
+                           tagUI3DPoint *tris, long num_triangles, UpdateGrid *Gridpts,
+                           long *blunder_count, double *minz_mp, double *maxz_mp) {
+    vll_context *ctx = shim_context();
+    vll_level_desc d;
+    memset(&d, 0, sizeof(d));
+    d.pyramid_step = *pl.Pyramid_step;
+    d.is_ra = proinfo->IsRA;
+    d.grid_resolution = *pl.grid_resolution;
+    for (int i = 0; i < 4; ++i) d.boundary[i] = pl.Boundary[i];
+    d.grid_width = pl.Size_Grid2D->width;
+    d.grid_height = pl.Size_Grid2D->height;
+    int64_t counts[2] = {blunder_count[0], blunder_count[1]};
+    static_assert(sizeof(bool) == sizeof(uint8_t), "bool layout");
+    if (vll_blunder_detection_tin(ctx, &d, iteration, ortho_ncc, flag_blunder ? 1 : 0, count_bl,
+                                  pl.Hinterval ? *pl.Hinterval : 0.0,
+                                  reinterpret_cast<vll_point3 *>(pts),
+                                  reinterpret_cast<uint8_t *>(detectedBlunders), num_points,
+                                  reinterpret_cast<const vll_tri *>(tris), num_triangles,
+                                  reinterpret_cast<vll_ugrid *>(Gridpts), counts, minz_mp,
+                                  maxz_mp) != VLL_OK)
+        die("blunder_detection_TIN: GPU call failed", vll_last_error(ctx));
+    blunder_count[0] = (long)counts[0];
+    blunder_count[1] = (long)counts[1];
+    return true;
+}
+
 long SelectMPs(const ProjectInfo *proinfo, taglevelinfo &pl, const tagNCCresult *roh_height,
                UpdateGrid *GridPT3, const double Th_roh, const double Th_roh_min,
                const double Th_roh_start, const double Th_roh_next, const int iteration,

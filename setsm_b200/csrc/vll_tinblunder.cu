@@ -1,0 +1,577 @@
+// vll_tinblunder.cu -- blunder_detection_TIN (setsm_code.cpp:9158-9787): the
+// matched points whose TIN neighbourhood is inconsistent in height are marked
+// as blunders.
+//
+// The reference runs three passes: statistics over the triangles in order
+// (per point its first 30 triangles; FP64 sums of the vertices' ortho NCC and
+// of the edges' height differences; a histogram of the differences), the
+// thresholds from them, and a parallel pass over the points in which a point
+// may mark itself (flag 1) or a neighbour (flag 3).  Its marks race only on
+// which of 1 / 3 lands first on a point that was 0 (set_blunder, :9121); the
+// closing pass turns 3 into 1, so the outputs do not depend on the race.
+//
+// GPU: the per-triangle terms in parallel, the FP64 sums by one thread in the
+// reference's triangle order (a sum's rounding depends on its order), the
+// per-point triangle lists by a stable radix sort of (point, triangle), the
+// point pass one thread per point with the same compare-and-swap marking, and
+// the closing pass with atomics (order-free counts, min / max).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cuda_runtime.h>
+
+#include "vll_ddmath.cuh"
+#include "vll_device.cuh"
+#include "vll_internal.h"
+
+namespace vll {
+
+namespace {
+
+constexpr int kMaxNodes = 30;   // max_nodes (:9168)
+
+__device__ __forceinline__ int64_t grid_index(const TinArgs &a, double x, double y) {
+    const int64_t c = (int64_t)__dadd_rn(__ddiv_rn(__dadd_rn(x, -a.b0), a.gs), 0.5);
+    const int64_t r = (int64_t)__dadd_rn(__ddiv_rn(__dadd_rn(y, -a.b1), a.gs), 0.5);
+    return a.width * r + c;
+}
+
+// Per triangle: the vertices' ortho NCC terms and the edge height
+// differences, and the histogram of the differences (order-free).
+struct TriTerms {
+    float oncc[3];
+    uint8_t has_oncc[3];
+    uint8_t valid;
+    double dh[3];
+};
+
+__global__ void tri_terms_kernel(TinArgs a, const vll_point3 *pts, const vll_tri *tris,
+                                 const float *ortho_ncc, TriTerms *terms, uint32_t *hbin,
+                                 uint32_t hdiffcount, unsigned int *bad) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < a.n_tris;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const vll_tri tr = tris[t];
+        const uint32_t v[3] = {tr.a, tr.b, tr.c};
+        TriTerms T;
+        T.valid = 1;
+        for (int k = 0; k < 3; ++k) {
+            T.has_oncc[k] = 0;
+            T.oncc[k] = 0.f;
+            if (v[k] < (uint64_t)a.n_pts) {
+                const vll_point3 p = pts[v[k]];
+                // int t_col / t_row and an int index, as the reference
+                const int tc = (int)__dadd_rn(__ddiv_rn(__dadd_rn(p.x, -a.b0), a.gs), 0.5);
+                const int trw = (int)__dadd_rn(__ddiv_rn(__dadd_rn(p.y, -a.b1), a.gs), 0.5);
+                const int idx = (int)((unsigned)a.width * (unsigned)trw + (unsigned)tc);
+                if (idx < 0 || (int64_t)idx >= a.n_nodes) {
+                    atomicExch(bad, 1u);
+                    continue;
+                }
+                const float o = ortho_ncc[idx];
+                if (o > -1) {
+                    T.has_oncc[k] = 1;
+                    T.oncc[k] = o;
+                }
+            } else {
+                T.valid = 0;
+            }
+        }
+        if (T.valid) {
+            const double z0 = pts[v[0]].z, z1 = pts[v[1]].z, z2 = pts[v[2]].z;
+            T.dh[0] = fabs(__dadd_rn(z0, -z1));
+            T.dh[1] = fabs(__dadd_rn(z0, -z2));
+            T.dh[2] = fabs(__dadd_rn(z1, -z2));
+            for (int k = 0; k < 3; ++k) {
+                const double f = (double)(uint32_t)T.dh[k];
+                if (f < (double)hdiffcount) atomicAdd(hbin + (uint32_t)f, 1u);
+            }
+        }
+        terms[t] = T;
+    }
+}
+
+// The reference's FP64 sums, in triangle order (one thread).
+__global__ void tri_sums_kernel(int64_t n_tris, const TriTerms *terms, double *sums) {
+    double so = 0, so2 = 0, sd = 0, sd2 = 0;
+    long long no = 0, nd = 0;
+    for (int64_t t = 0; t < n_tris; ++t) {
+        const TriTerms T = terms[t];
+        for (int k = 0; k < 3; ++k) {
+            if (T.has_oncc[k]) {
+                so = __dadd_rn(so, (double)T.oncc[k]);
+                so2 = __dadd_rn(so2, (double)__fmul_rn(T.oncc[k], T.oncc[k]));
+                ++no;
+            }
+        }
+        if (T.valid) {
+            for (int k = 0; k < 3; ++k) {
+                sd = __dadd_rn(sd, T.dh[k]);
+                sd2 = __dadd_rn(sd2, __dmul_rn(T.dh[k], T.dh[k]));
+                ++nd;
+            }
+        }
+    }
+    sums[0] = so;
+    sums[1] = so2;
+    sums[2] = sd;
+    sums[3] = sd2;
+    sums[4] = (double)no;
+    sums[5] = (double)nd;
+}
+
+// (point, triangle) pairs in triangle order, 3 per triangle (invalid
+// vertices keyed past the points).
+__global__ void pair_kernel(TinArgs a, const vll_tri *tris, uint32_t *key, int32_t *val,
+                            unsigned int *count) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < a.n_tris;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const vll_tri tr = tris[t];
+        const uint32_t v[3] = {tr.a, tr.b, tr.c};
+        for (int k = 0; k < 3; ++k) {
+            const bool ok = v[k] < (uint64_t)a.n_pts;
+            key[3 * t + k] = ok ? v[k] : (uint32_t)a.n_pts;
+            val[3 * t + k] = (int32_t)t;
+            if (ok) atomicAdd(count + v[k], 1u);
+        }
+    }
+}
+
+// set_blunder (:9121-9156): a point that is still 0 takes `val`; the call
+// that changed it from 0 records the new blunder.
+__device__ void set_blunder(vll_point3 *pts, int64_t i, uint8_t val, uint8_t *detected) {
+    unsigned int *word = reinterpret_cast<unsigned int *>(
+        reinterpret_cast<unsigned char *>(pts + i) + 24);   // flag's 4-byte word
+    unsigned int old = *reinterpret_cast<volatile unsigned int *>(word);
+    for (;;) {
+        if ((old & 0xffu) != 0) return;
+        const unsigned int nw = (old & ~0xffu) | val;
+        const unsigned int got = atomicCAS(word, old, nw);
+        if (got == old) break;
+        old = got;
+    }
+    detected[i] = 1;
+}
+
+__device__ double normal_angle(const vll_point3 &p0, const vll_point3 &p1, const vll_point3 &p2) {
+    const double ux = __dadd_rn(p1.x, -p0.x), uy = __dadd_rn(p1.y, -p0.y), uz = __dadd_rn(p1.z, -p0.z);
+    const double vx = __dadd_rn(p2.x, -p0.x), vy = __dadd_rn(p2.y, -p0.y), vz = __dadd_rn(p2.z, -p0.z);
+    const double nx = __dadd_rn(__dmul_rn(uy, vz), -__dmul_rn(vy, uz));
+    const double ny = -__dadd_rn(__dmul_rn(ux, vz), -__dmul_rn(vx, uz));
+    const double nz = __dadd_rn(__dmul_rn(ux, vy), -__dmul_rn(vx, uy));
+    const double norm =
+        sqrt(__dadd_rn(__dadd_rn(__dmul_rn(nx, nx), __dmul_rn(ny, ny)), __dmul_rn(nz, nz)));
+    // a vertical-free triangle of a TIN has norm > 0; the reference leaves the
+    // angle unset otherwise
+    double angle = 0;
+    if (norm != 0)
+        angle = __ddiv_rn(__dmul_rn(ddm::acos_cr(__ddiv_rn(fabs(nz), norm)), 180.0), kPi);
+    if (angle <= 0 && angle >= -90)
+        angle = fabs(angle);
+    else if (angle <= -270 && angle >= -360)
+        angle = __dadd_rn(360.0, angle);
+    else if (angle >= 270 && angle <= 360)
+        angle = __dadd_rn(360.0, -angle);
+    return angle;
+}
+
+// The point pass (:9426-9756).
+__global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
+                             const float *ortho_ncc, const int32_t *sorted_tri,
+                             const int64_t *start, const unsigned int *count, vll_ugrid *gp3,
+                             uint8_t *detected, const uint8_t *flag0, unsigned int *bad) {
+    for (int64_t index = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; index < a.n_pts;
+         index += (int64_t)gridDim.x * blockDim.x) {
+        if (flag0[index] == 1) continue;
+        bool pt_is_blunder = false;
+        int count_pos = 0, count_neg = 0, cnt = 0;
+        bool check_neigh = false;
+        const int max_iter = count[index] < (unsigned)kMaxNodes ? (int)count[index] : kMaxNodes;
+        const vll_point3 rp = pts[index];
+        const int64_t ref_index = grid_index(a, rp.x, rp.y);
+        if (ref_index < 0 || ref_index >= a.n_nodes) {
+            atomicExch(bad, 1u);
+            continue;
+        }
+        gp3[ref_index].anchor_flag = 0;
+        const float ref_oncc = ortho_ncc[ref_index];
+        if (!a.is_ra && ref_oncc < a.th_ref_ncc && a.L >= 2) pt_is_blunder = true;
+        if (a.L >= 3 && a.iteration >= 4 && ref_oncc >= 0.95 && a.flag_blunder)
+            gp3[ref_index].anchor_flag = 1;
+        for (int it = 0; it < max_iter; ++it) {
+            const int64_t tc = sorted_tri[start[index] + it];
+            // triangle 0 is never used here, as in the reference (savenode > 0)
+            if (!(tc < a.n_tris && tc > 0)) continue;
+            const vll_tri tr = tris[tc];
+            const uint32_t tt[3] = {tr.a, tr.b, tr.c};
+            int64_t reference_index = 0, t0 = 0, t1 = 0;
+            bool check_index = false;
+            for (int kk = 0; kk < 3; ++kk) {
+                if (tt[kk] == (uint64_t)index)
+                    reference_index = index;
+                else if (!check_index) {
+                    t0 = tt[kk];
+                    check_index = true;
+                } else {
+                    t1 = tt[kk];
+                }
+            }
+            if (!(reference_index < a.n_pts && t0 < a.n_pts && t1 < a.n_pts)) continue;
+            const vll_point3 p0 = pts[reference_index], p1 = pts[t0], p2 = pts[t1];
+            const double angle = normal_angle(p0, p1, p2);
+            const double dh1 = __dadd_rn(p0.z, -p1.z), dh2 = __dadd_rn(p0.z, -p2.z),
+                         dh3 = __dadd_rn(p1.z, -p2.z);
+            if (dh1 >= 0 && dh2 >= 0 && angle > 30) ++count_pos;
+            if (dh1 < 0 && dh2 < 0 && angle > 30) ++count_neg;
+            bool check_match = false;
+            if (a.L > 1)
+                check_match = true;
+            else if (a.L == 1)
+                check_match = a.iteration == 1 && a.count_bl <= 5;
+            else if (a.L == 0) {
+                if (a.iteration == 1 && a.count_bl <= 5)
+                    check_match = true;
+                else if (a.iteration == 2 && a.count_bl <= 5)
+                    check_match = false;
+            }
+            if (check_match) {
+                const double d1 = __dadd_rn(fabs(dh1), -fabs(dh2));
+                const double d2 = __dadd_rn(fabs(dh1), -fabs(dh3));
+                const double d3 = __dadd_rn(fabs(dh2), -fabs(dh3));
+                if (fabs(d1) > a.height_th || fabs(d2) > a.height_th || fabs(d3) > a.height_th) {
+                    const int64_t order[3] = {reference_index, t0, t1};
+                    const double h[3] = {p0.z, p1.z, p2.z};
+                    const int64_t Index[3] = {grid_index(a, p0.x, p0.y), grid_index(a, p1.x, p1.y),
+                                              grid_index(a, p2.x, p2.y)};
+                    check_neigh = true;
+                    int mx, mn, md;
+                    if (h[0] > h[1]) {
+                        if (h[0] > h[2]) {
+                            mx = 0;
+                            if (h[1] > h[2]) {
+                                mn = 2;
+                                md = 1;
+                            } else {
+                                mn = 1;
+                                md = 2;
+                            }
+                        } else {
+                            mx = 2;
+                            mn = 1;
+                            md = 0;
+                        }
+                    } else {
+                        if (h[1] > h[2]) {
+                            mx = 1;
+                            if (h[0] > h[2]) {
+                                mn = 2;
+                                md = 0;
+                            } else {
+                                mn = 0;
+                                md = 2;
+                            }
+                        } else {
+                            mx = 2;
+                            md = 1;
+                            mn = 0;
+                        }
+                    }
+                    const double h1 = __dadd_rn(h[md], -h[mn]);
+                    const double h2 = __dadd_rn(h[mx], -h[md]);
+                    const double dh = __dadd_rn(h1, -h2);
+                    int64_t bn = -1;
+                    int pick = -1;
+                    if (dh > 0 && dh > a.height_th)
+                        pick = mn;
+                    else if (dh < 0 && fabs(dh) > a.height_th)
+                        pick = mx;
+                    if (pick >= 0) {
+                        if (a.is_ra) {
+                            bn = order[pick];
+                        } else {
+                            const int64_t gi = Index[pick];
+                            if (gi < 0 || gi >= a.n_nodes) {
+                                atomicExch(bad, 1u);
+                            } else {
+                                const double th = a.flag_blunder ? a.ortho_ncc_th : 100.0;
+                                if (ortho_ncc[gi] < th) bn = order[pick];
+                            }
+                        }
+                    }
+                    if (bn >= 0) set_blunder(pts, bn, 3, detected);
+                }
+            }
+            ++cnt;
+        }
+        if (a.is_ra) {
+            if (check_neigh && !a.flag_blunder) pt_is_blunder = true;
+            if ((count_pos >= (int)__dadd_rn(__dmul_rn((double)cnt, 0.7), 0.5) ||
+                 count_neg >= (int)__dadd_rn(__dmul_rn((double)cnt, 0.7), 0.5)) &&
+                cnt > 1)
+                pt_is_blunder = true;
+        } else {
+            if (check_neigh && !a.flag_blunder) {
+                if (ref_oncc < 100.0) pt_is_blunder = true;
+            }
+            double cth = __dmul_rn((double)cnt, 0.5);
+            if (a.L >= 2)
+                cth = __dmul_rn((double)cnt, 0.5);
+            else if (a.L == 1)
+                cth = (double)(int)__dadd_rn(__dmul_rn((double)cnt, 0.6), 0.5);
+            else
+                cth = (double)(int)__dadd_rn(__dmul_rn((double)cnt, 0.7), 0.5);
+            if ((count_pos >= cth || count_neg >= cth) && cnt > 1) {
+                if (a.flag_blunder) {
+                    double tmp = __dadd_rn(0.6, -__dmul_rn((double)(4 - a.L), 0.1));
+                    if (a.L == 1) tmp = 0.6;
+                    if (a.L >= 1) {
+                        if (ref_oncc < tmp) pt_is_blunder = true;
+                    } else {
+                        if (a.iteration <= 1) {
+                            if (ref_oncc < 0.9) pt_is_blunder = true;
+                        } else if (a.iteration == 2) {
+                            pt_is_blunder = true;
+                        } else if (ref_oncc < a.ortho_ncc_th) {
+                            pt_is_blunder = true;
+                        }
+                    }
+                } else if (ref_oncc < 100.0) {
+                    pt_is_blunder = true;
+                }
+            }
+        }
+        if (pt_is_blunder) set_blunder(pts, index, 1, detected);
+    }
+}
+
+__device__ __forceinline__ unsigned long long dkey(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// The closing pass (:9765-9781): blunder counts, 3 -> 1, the height extent
+// of the remaining points.
+__global__ void close_kernel(int64_t n_pts, vll_point3 *pts, unsigned long long *cnt,
+                             unsigned long long *zkey) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pts;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t f = pts[i].flag;
+        if (f == 1) {
+            atomicAdd(cnt + 1, 1ull);
+        } else if (f == 3) {
+            atomicAdd(cnt + 1, 1ull);
+            pts[i].flag = 1;
+        } else {
+            atomicAdd(cnt, 1ull);
+            atomicMin(zkey, dkey(pts[i].z));
+            atomicMax(zkey + 1, dkey(pts[i].z));
+        }
+    }
+}
+
+__global__ void copy_flags_kernel(int64_t n, const vll_point3 *pts, uint8_t *flag0) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        flag0[i] = pts[i].flag;
+}
+
+unsigned blocks_for(int64_t n, int threads) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148 * 32) b = 148 * 32;
+    return (unsigned)b;
+}
+
+size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t sort_tmp_bytes(int64_t n_pairs) {
+    size_t t = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)n_pairs);
+    size_t u = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, u, (const unsigned int *)nullptr, (int64_t *)nullptr,
+                                  (int)1);
+    return t > u ? t : u;
+}
+
+size_t scan_tmp_bytes(int64_t n) {
+    size_t u = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, u, (const unsigned int *)nullptr, (int64_t *)nullptr,
+                                  (int)n);
+    return u;
+}
+
+}  // namespace
+
+void tin_thresholds(const TinArgs &a, const double *sums, const uint32_t *hbin,
+                    uint32_t hdiffcount, TinThresholds *th) {
+    const int L = a.L, it = a.iteration;
+    const double sum_data = sums[2], sum_data2 = sums[3];
+    const long dh_count = (long)sums[5];
+    // the ortho-NCC threshold of the level (:9299-9308; the statistics-based
+    // value computed before it is overwritten there)
+    double ortho_ncc_th;
+    if (L == 4)
+        ortho_ncc_th = 0.6 - (it - 1) * 0.01;
+    else if (L >= 3)
+        ortho_ncc_th = 0.5 - (it - 1) * 0.01;
+    else if (L == 2)
+        ortho_ncc_th = 0.4 - (it - 1) * 0.01;
+    else if (L == 1)
+        ortho_ncc_th = 0.3;
+    else
+        ortho_ncc_th = 0.2;
+    double th_ref_ncc = 0.1 + (it - 1) * 0.05;
+    if (th_ref_ncc > ortho_ncc_th) th_ref_ncc = ortho_ncc_th;
+    bool check_dh = false;
+    if (L <= 4 && L >= 3)
+        check_dh = true;
+    else if (L == 2)
+        check_dh = it <= 4;
+    else if (L <= 1)
+        check_dh = it <= 2;
+    double height_th;
+    if (L >= 3) {
+        double gsd = a.gs;
+        if (gsd < (double)(1 << (L - 1))) gsd = (double)(1 << (L - 1));
+        double th2 = gsd * 10;
+        if (a.is_ra == 1) th2 = gsd * 30;
+        height_th = a.hinterval < th2 ? a.hinterval : th2;
+        double up;
+        if (check_dh) {
+            const double mean = sum_data / dh_count;
+            const double sd = sqrt((sum_data2 - (sum_data) * (sum_data) / dh_count) / dh_count);
+            up = mean + 3 * sd;
+        } else {
+            up = height_th;
+        }
+        if (up < height_th) height_th = up < height_th / 2.0 ? height_th / 2.0 : up;
+    } else {
+        // levels 0-2: the 99th percentile of the height differences (the
+        // reference computes a GSD-based threshold first and overwrites it)
+        uint32_t th80 = 1000, total_dh = 0;
+        long t = 0;
+        bool found = false;
+        while (t < (long)hdiffcount && !found) {
+            total_dh += hbin[t];
+            const double per = (double)total_dh / (double)dh_count * 100.0;
+            if (per > 99) {
+                th80 = (uint32_t)t;
+                found = true;
+            }
+            ++t;
+        }
+        if (!found) th80 = (uint32_t)(t - 1);
+        const double mean = sum_data / dh_count;
+        const double sd = sqrt((sum_data2 - (sum_data) * (sum_data) / dh_count) / dh_count);
+        const double up = mean + 3 * sd;
+        height_th = up < th80 ? up : (double)th80;
+        if (height_th > 50) height_th = 50;
+    }
+    th->height_th = height_th;
+    th->ortho_ncc_th = ortho_ncc_th;
+    th->th_ref_ncc = th_ref_ncc;
+}
+
+size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount) {
+    const int64_t np = 3 * n_tris;
+    size_t t = sort_tmp_bytes(np > 0 ? np : 1), u = scan_tmp_bytes(n_pts + 1);
+    return al(t > u ? t : u) + al(n_tris * sizeof(TriTerms)) + al((hdiffcount + 1) * 4) +
+           al(64) + 4 * al(np * 4) + al((n_pts + 1) * 4) + al((n_pts + 1) * 8) + al(n_pts) +
+           al(64);
+}
+
+cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
+                            const float *ortho_ncc, vll_ugrid *gp3, uint8_t *detected,
+                            uint32_t hdiffcount, void *scratch, size_t bytes,
+                            const TinThresholds &th_in, TinOutput *out, cudaStream_t s) {
+    const int64_t np = 3 * a.n_tris;
+    size_t tmp_b = sort_tmp_bytes(np > 0 ? np : 1), u = scan_tmp_bytes(a.n_pts + 1);
+    if (u > tmp_b) tmp_b = u;
+    char *p = (char *)scratch;
+    auto take = [&](size_t b) {
+        void *r = p;
+        p += al(b);
+        return r;
+    };
+    void *tmp = take(tmp_b);
+    TriTerms *terms = (TriTerms *)take(a.n_tris * sizeof(TriTerms));
+    uint32_t *hbin = (uint32_t *)take((hdiffcount + 1) * 4);
+    double *sums = (double *)take(64);
+    uint32_t *key = (uint32_t *)take(np * 4);
+    uint32_t *skey = (uint32_t *)take(np * 4);
+    int32_t *val = (int32_t *)take(np * 4);
+    int32_t *sval = (int32_t *)take(np * 4);
+    unsigned int *count = (unsigned int *)take((a.n_pts + 1) * 4);
+    int64_t *start = (int64_t *)take((a.n_pts + 1) * 8);
+    uint8_t *flag0 = (uint8_t *)take(a.n_pts);
+    unsigned long long *misc = (unsigned long long *)take(64);   // [0..1] counts, [2..3] z keys, [4] bad
+    if ((size_t)(p - (char *)scratch) > bytes) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(hbin, 0, (hdiffcount + 1) * 4, s))) return e;
+    if ((e = cudaMemsetAsync(count, 0, (a.n_pts + 1) * 4, s))) return e;
+    if ((e = cudaMemsetAsync(misc, 0, 64, s))) return e;
+    unsigned int *bad = reinterpret_cast<unsigned int *>(misc + 4);
+    if (a.n_tris > 0) {
+        tri_terms_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, pts, tris, ortho_ncc, terms,
+                                                                   hbin, hdiffcount, bad);
+        tri_sums_kernel<<<1, 1, 0, s>>>(a.n_tris, terms, sums);
+        pair_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, tris, key, val, count);
+        if ((e = cudaGetLastError())) return e;
+        int end_bit = 1;
+        while (end_bit < 32 && ((uint64_t)1 << end_bit) <= (uint64_t)a.n_pts) ++end_bit;
+        if ((e = cub::DeviceRadixSort::SortPairs(tmp, tmp_b, key, skey, val, sval, (int)np, 0,
+                                                 end_bit, s)))
+            return e;
+    } else {
+        if ((e = cudaMemsetAsync(sums, 0, 64, s))) return e;
+    }
+    if ((e = cub::DeviceScan::ExclusiveSum(tmp, tmp_b, count, start, (int)(a.n_pts + 1), s)))
+        return e;
+    // the sums, the histogram and the input check back for the thresholds
+    double hs[6];
+    std::vector<uint32_t> hb(hdiffcount + 1);
+    unsigned long long hbad = 0;
+    if ((e = cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaMemcpyAsync(hb.data(), hbin, (hdiffcount + 1) * 4, cudaMemcpyDeviceToHost, s)))
+        return e;
+    if ((e = cudaMemcpyAsync(&hbad, misc + 4, 8, cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaStreamSynchronize(s))) return e;
+    if (hbad) {
+        out->bad_input = 1;
+        return cudaSuccess;
+    }
+    TinThresholds th = th_in;
+    tin_thresholds(a, hs, hb.data(), hdiffcount, &th);
+    a.height_th = th.height_th;
+    a.ortho_ncc_th = th.ortho_ncc_th;
+    a.th_ref_ncc = th.th_ref_ncc;
+    copy_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0);
+    point_kernel<<<blocks_for(a.n_pts, 128), 128, 0, s>>>(a, pts, tris, ortho_ncc, sval, start,
+                                                         count, gp3, detected, flag0, bad);
+    const unsigned long long zinit[2] = {~0ull, 0ull};
+    if ((e = cudaMemcpyAsync(misc + 2, zinit, 16, cudaMemcpyHostToDevice, s))) return e;
+    close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2);
+    if ((e = cudaGetLastError())) return e;
+    unsigned long long m[5];
+    if ((e = cudaMemcpyAsync(m, misc, sizeof(m), cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaStreamSynchronize(s))) return e;
+    out->bad_input = m[4] != 0;
+    out->count[0] = (int64_t)m[0];
+    out->count[1] = (int64_t)m[1];
+    out->has_z = m[0] > 0;
+    for (int k = 0; k < 2; ++k) {
+        const unsigned long long b = m[2 + k];
+        const unsigned long long bits = (b >> 63) ? (b & 0x7fffffffffffffffull) : ~b;
+        double v;
+        memcpy(&v, &bits, 8);
+        out->z[k] = v;
+    }
+    out->height_th = th.height_th;
+    return cudaSuccess;
+}
+
+}  // namespace vll

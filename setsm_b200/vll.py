@@ -36,7 +36,7 @@ EXPORTED = [
     "vll_vertical_line_locus_ortho", "vll_ortho_blunder", "vll_ortho_blunder_device",
     "vll_set_height_range", "vll_select_mps", "vll_initialize_voxel",
     "vll_initialize_voxel_device", "vll_awncc_peaks_device", "vll_select_mps_device",
-    "vll_set_height_range_device",
+    "vll_set_height_range_device", "vll_blunder_detection_tin",
 ]
 
 _lib = None
@@ -111,6 +111,8 @@ def load():
     L.vll_select_mps.argtypes = [vp, D, vp, vp, dbl, dbl, dbl, dbl, i32, dbl, i32, dbl, vp, i64,
                                  C.POINTER(i64)]
     L.vll_select_mps_device.argtypes = L.vll_select_mps.argtypes
+    L.vll_blunder_detection_tin.argtypes = [vp, D, i32, vp, i32, i32, dbl, vp, vp, i64, vp, i64,
+                                            vp, vp, vp, vp]
     L.vll_set_height_range_device.argtypes = L.vll_set_height_range.argtypes
     _lib = L
     return L
@@ -316,6 +318,20 @@ class Context:
             float(mpp), int(final_level_iteration), float(mpp_stereo_angle), out.ctypes.data,
             len(out), C.byref(n)))
         return out[: n.value].copy()
+
+    def blunder_detection_tin(self, inputs, iteration: int, ortho_ncc: np.ndarray,
+                              flag_blunder: bool, count_bl: int, hinterval: float,
+                              pts: np.ndarray, detected: np.ndarray, tris: np.ndarray,
+                              counts: np.ndarray, zext: np.ndarray) -> None:
+        """blunder_detection_TIN (setsm_code.cpp:9158-9787): pts, detected
+        (uint8), inputs.gridpt3, counts (int64[2]) and zext (float64[2]: min,
+        max) updated in place."""
+        d = inputs.desc()
+        self._check(load().vll_blunder_detection_tin(
+            self._h, C.byref(d), int(iteration), ortho_ncc.ctypes.data, int(bool(flag_blunder)),
+            int(count_bl), float(hinterval), pts.ctypes.data, detected.ctypes.data, len(pts),
+            tris.ctypes.data, len(tris), inputs.gridpt3.ctypes.data, counts.ctypes.data,
+            zext[0:1].ctypes.data, zext[1:2].ctypes.data))
 
     def select_mps_device(self, desc, d_ncc: int, d_gridpt3: int, d_points: int, capacity: int,
                           *args) -> int:

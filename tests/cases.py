@@ -168,6 +168,21 @@ def make_select_case(name: str, seed: int = 71, flag_frac=(0.5, 0.1, 0.2)):
     return inp, r["ncc"].copy()
 
 
+def make_tin_blunder_case(*, seed=17, flagged_frac=0.1, low_ncc_frac=0.2, **kw):
+    """Inputs of blunder_detection_TIN: make_tin_case's points (heights off
+    the truth on its candidates) and TIN, point flags 0 with `flagged_frac`
+    already 1, and an orthoimage NCC per grid node over [-1, 1] (low on
+    `low_ncc_frac` of the nodes).  Returns (inputs, pts, tris, ortho_ncc)."""
+    inp, pts, tris = make_tin_case(seed=seed, **kw)
+    rng = np.random.default_rng(seed + 91)
+    pts["flag"] = np.where(rng.random(len(pts)) < flagged_frac, 1, 0)
+    n = inp.n
+    oncc = np.where(rng.random(n) < low_ncc_frac, rng.uniform(-1.0, 0.3, n),
+                    rng.uniform(0.3, 1.0, n)).astype(np.float32)
+    oncc[rng.random(n) < 0.05] = -1.0
+    return inp, pts, tris, oncc
+
+
 def delaunay(pts):
     """Triangles (abi.TRI_DTYPE) of the Delaunay triangulation of the points'
     x, y (scipy's Qhull) -- a stand-in for the matcher's own TIN."""

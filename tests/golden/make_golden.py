@@ -115,6 +115,31 @@ def select_case(name):
     return inp, z["ncc"].view(abi.NCCRESULT_DTYPE).copy(), z
 
 
+# blunder_detection_TIN (setsm_code.cpp:9158-9787): kwargs of
+# tests/cases.py:make_tin_blunder_case and the call's (iteration,
+# flag_blunder, count_bl, Hinterval); the fixture keeps every input it reads.
+GOLDEN_TINB = {
+    "tinb_l0": dict(call=(1, True, 1, 60.0), case=dict(seed=17)),
+    "tinb_l3": dict(call=(2, True, 2, 40.0),
+                    case=dict(seed=18, L=3, res=24.0, template=15, nodes=16)),
+    "tinb_l1_anchor": dict(call=(1, False, 3, 80.0),
+                           case=dict(seed=19, L=1, res=12.0, template=15, nodes=24)),
+}
+
+
+def tinb_case(name):
+    """(inputs, pts, tris, ortho_ncc, fixture arrays) of fixture `name`."""
+    from setsm_b200 import abi
+    from tests import cases
+    z = np.load(fixture_path(name))
+    inp, _, _, _ = cases.make_tin_blunder_case(**GOLDEN_TINB[name]["case"])
+    inp.boundary = z["boundary"].copy()
+    inp.grid_resolution = float(z["grid_resolution"])
+    inp.gridpt3 = z["init_gp3"].view(abi.UGRID_DTYPE).copy()
+    return (inp, z["init_pts"].view(abi.POINT3_DTYPE).copy(), z["tris"].view(abi.TRI_DTYPE).copy(),
+            z["oncc"].copy(), z)
+
+
 def range_case(name):
     """(inputs, pts, tris, fixture arrays) of SetHeightRange fixture `name`."""
     from setsm_b200 import abi
@@ -273,6 +298,23 @@ def main(only=None) -> None:
                             gp3=clean(inp.gridpt3).view(np.uint8), pts=clean(pts).view(np.uint8),
                             ret=np.array(r))
         print(f"{name}: {r} points, {os.path.getsize(fixture_path(name))} bytes")
+
+    for name, v in GOLDEN_TINB.items():
+        if only and name not in only:
+            continue
+        inp, pts, tris, oncc = cases.make_tin_blunder_case(**v["case"])
+        init_gp3, init_pts = clean(inp.gridpt3), clean(pts)
+        det = np.zeros(len(pts), np.uint8)
+        counts = np.zeros(2, np.int64)
+        zext = np.array([1e5, -1e5])
+        it, fb, cbl, hint = v["call"]
+        refpy.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
+        np.savez_compressed(fixture_path(name), boundary=np.asarray(inp.boundary),
+                            grid_resolution=np.array(inp.grid_resolution),
+                            init_gp3=init_gp3.view(np.uint8), init_pts=init_pts.view(np.uint8),
+                            tris=tris.view(np.uint8), oncc=oncc, gp3=clean(inp.gridpt3).view(np.uint8),
+                            pts=clean(pts).view(np.uint8), detected=det, counts=counts, zext=zext)
+        print(f"{name}: {int(det.sum())} new blunders, {os.path.getsize(fixture_path(name))} bytes")
 
 
 if __name__ == "__main__":

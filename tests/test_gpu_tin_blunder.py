@@ -1,0 +1,88 @@
+"""blunder_detection_TIN on the GPU (vll_tinblunder.cu) against the reference
+(setsm_code.cpp:9158-9787): the fixtures made by the reference build, the
+reference build itself over levels, iterations and switches, and the C++
+drop-in with the reference's signature.  Point flags, the new-blunder marks,
+every UGRID field, the counts and the height extent must be identical."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import refpy
+from setsm_b200 import abi, vll
+from tests import cases
+from tests.golden import make_golden as mg
+
+pytestmark = pytest.mark.gpu
+
+DROPIN = ("_Z21blunder_detection_TINPK11ProjectInfoR12taglevelinfoiPfbtP11tagD3DPointPblP12tag"
+          "UI3DPointlP10UpdateGridPlPdSD_")
+
+
+def fresh_out(n):
+    return np.zeros(n, np.uint8), np.zeros(2, np.int64), np.array([1e5, -1e5])
+
+
+def assert_same(pts, det, gp3, counts, zext, w_pts, w_det, w_gp3, w_counts, w_zext):
+    assert np.array_equal(pts["flag"], w_pts["flag"])
+    assert np.array_equal(pts["z"], w_pts["z"])
+    assert np.array_equal(det, w_det)
+    assert cases.field_mismatch(mg.clean(gp3), mg.clean(w_gp3)) == {}
+    assert np.array_equal(counts, w_counts)
+    assert np.array_equal(zext, w_zext)
+
+
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_TINB))
+def test_matches_reference_fixture(gpu_ctx, name):
+    inp, pts, tris, oncc, z = mg.tinb_case(name)
+    it, fb, cbl, hint = mg.GOLDEN_TINB[name]["call"]
+    det, counts, zext = fresh_out(len(pts))
+    gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
+    assert_same(pts, det, inp.gridpt3, counts, zext, z["pts"].view(abi.POINT3_DTYPE),
+                z["detected"], z["gp3"].view(abi.UGRID_DTYPE), z["counts"], z["zext"])
+
+
+@pytest.mark.skipif(not refpy.available(), reason="reference build not available")
+@pytest.mark.parametrize("kw,call", [
+    (dict(seed=41, size=768, nodes=40, res=7.0), (1, True, 1, 60.0)),
+    (dict(seed=42, size=768, nodes=40, res=7.0, point_frac=0.15), (2, True, 4, 40.0)),
+    (dict(seed=43, size=768, nodes=40, res=7.0), (4, True, 1, 60.0)),
+    (dict(seed=44, size=768, nodes=24, res=12.0, L=1, template=15), (1, True, 2, 80.0)),
+    (dict(seed=45, size=768, nodes=24, res=16.0, L=2, template=15), (3, False, 1, 70.0)),
+    (dict(seed=46, size=768, nodes=16, res=24.0, L=3, template=15), (4, True, 1, 35.0)),
+    (dict(seed=47, size=768, nodes=16, res=24.0, L=4, template=15, flagged_frac=0.3),
+     (2, True, 1, 25.0)),
+])
+def test_matches_reference_build(gpu_ctx, kw, call):
+    import copy
+    inp, pts, tris, oncc = cases.make_tin_blunder_case(**kw)
+    ref = copy.copy(inp)
+    ref.gridpt3 = inp.gridpt3.copy()
+    r_pts = pts.copy()
+    r_det, r_counts, r_zext = fresh_out(len(pts))
+    it, fb, cbl, hint = call
+    refpy.blunder_detection_tin(ref, it, oncc.copy(), fb, cbl, hint, r_pts, r_det, tris.copy(),
+                                r_counts, r_zext)
+    det, counts, zext = fresh_out(len(pts))
+    gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
+    assert_same(pts, det, inp.gridpt3, counts, zext, r_pts, r_det, ref.gridpt3, r_counts, r_zext)
+
+
+@pytest.mark.skipif(not refpy.available(), reason="reference build not available")
+def test_cpp_dropin_through_reference_structures(gpu_ctx):
+    inp, pts, tris, oncc, z = mg.tinb_case("tinb_l3")
+    it, fb, cbl, hint = mg.GOLDEN_TINB["tinb_l3"]["call"]
+    fn = C.cast(getattr(vll.load(), DROPIN), C.c_void_p).value
+    det, counts, zext = fresh_out(len(pts))
+    assert refpy.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext,
+                                       fn_addr=fn) == 1
+    assert_same(pts, det, inp.gridpt3, counts, zext, z["pts"].view(abi.POINT3_DTYPE),
+                z["detected"], z["gp3"].view(abi.UGRID_DTYPE), z["counts"], z["zext"])
+
+
+def test_level0_iteration3_does_nothing(gpu_ctx):
+    inp, pts, tris, oncc, _ = mg.tinb_case("tinb_l0")
+    before = pts.copy()
+    det, counts, zext = fresh_out(len(pts))
+    gpu_ctx.blunder_detection_tin(inp, 3, oncc, True, 1, 60.0, pts, det, tris, counts, zext)
+    assert np.array_equal(pts["flag"], before["flag"]) and not det.any() and not counts.any()

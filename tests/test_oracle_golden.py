@@ -129,3 +129,19 @@ def test_select_fixtures_are_the_reference_output(name):
     assert r == int(z["ret"])
     assert np.array_equal(mg.clean(pts).view(np.uint8), z["pts"])
     assert np.array_equal(mg.clean(inp.gridpt3).view(np.uint8), z["gp3"])
+
+
+@pytest.mark.skipif(not __import__("oracle.refpy").refpy.available(),
+                    reason="reference build not available")
+@pytest.mark.parametrize("name", sorted(mg.GOLDEN_TINB))
+def test_tinb_fixtures_are_the_reference_output(name):
+    from oracle import refpy
+    inp, pts, tris, oncc, z = mg.tinb_case(name)
+    it, fb, cbl, hint = mg.GOLDEN_TINB[name]["call"]
+    det = np.zeros(len(pts), np.uint8)
+    counts = np.zeros(2, np.int64)
+    zext = np.array([1e5, -1e5])
+    refpy.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
+    assert np.array_equal(mg.clean(pts).view(np.uint8), z["pts"])
+    assert np.array_equal(det, z["detected"])
+    assert np.array_equal(counts, z["counts"]) and np.array_equal(zext, z["zext"])
