@@ -848,6 +848,119 @@ def run_height_range(args):
     del torch
 
 
+def run_tin_blunder(args):
+    """blunder_detection_TIN (setsm_code.cpp:9158-9787) on the TIN workload of
+    tin_workload (1024^2 grid, 21 k points, 41.8 k triangles) with point flags
+    0 (10 % already 1) and an orthoimage NCC per node over [-1, 1], level 0,
+    iteration 1, flag_blunder on, Hinterval 60.  value: the device entry
+    point on resident buffers (host clock around the call, which waits; the
+    count of calls whose threshold band made it re-run the point pass is
+    reported);
+    e2e: the host-buffer entry point (copies included); CPU: the reference's
+    own blunder_detection_TIN with OpenMP on every host core.  Flags, the new
+    blunder marks, UGRID, counts and extent compared.  Metric: matched points
+    per second."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import copy
+    import torch
+    from oracle import refpy
+    from setsm_b200 import vll
+    from tests.cases import field_mismatch
+    ctx = vll.Context(0)
+    inp, g0, pts0, tris = tin_workload(ctx)
+    rng = np.random.default_rng(23)
+    pts0["flag"] = np.where(rng.random(len(pts0)) < 0.1, 1, 0)
+    n = int(inp.n)
+    oncc = np.where(rng.random(n) < 0.2, rng.uniform(-1.0, 0.3, n),
+                    rng.uniform(0.3, 1.0, n)).astype(np.float32)
+    it, fb, cbl, hint = 1, True, 1, 60.0
+    d = inp.desc()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).cuda()
+    d_pts0, d_tris, d_g0, d_o = dev(pts0), dev(tris), dev(g0), dev(oncc)
+    d_pts, d_g = torch.empty_like(d_pts0), torch.empty_like(d_g0)
+    d_det = torch.empty(len(pts0), dtype=torch.uint8, device="cuda:0")
+
+    def dev_call():
+        d_pts.copy_(d_pts0)
+        d_g.copy_(d_g0)
+        d_det.zero_()
+        torch.cuda.synchronize()
+        counts, zext = np.zeros(2, np.int64), np.array([1e5, -1e5])
+        t = time.perf_counter()
+        ctx.blunder_detection_tin_device(d, it, d_o.data_ptr(), fb, cbl, hint, d_pts.data_ptr(),
+                                         d_det.data_ptr(), len(pts0), d_tris.data_ptr(),
+                                         len(tris), d_g.data_ptr(), counts, zext)
+        return (time.perf_counter() - t) * 1e3
+    for _ in range(max(1, args.warmup)):
+        dev_call()
+    rr0 = vll.load().vll_tin_rerun_count(ctx._h)
+    dev_ms = statistics.median(dev_call() for _ in range(args.steps))
+    reruns = vll.load().vll_tin_rerun_count(ctx._h) - rr0
+
+    def call():
+        inp.gridpt3 = g0.copy()
+        pts, det = pts0.copy(), np.zeros(len(pts0), np.uint8)
+        counts, zext = np.zeros(2, np.int64), np.array([1e5, -1e5])
+        t = time.perf_counter()
+        ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
+        return (time.perf_counter() - t) * 1e3, (pts, det, inp.gridpt3, counts, zext)
+    for _ in range(max(1, args.warmup)):
+        call()
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    lc0 = vll.load().vll_launch_count(ctx._h)
+    for _ in range(args.steps):
+        ms, got = call()
+        times.append(ms)
+    launches = vll.load().vll_launch_count(ctx._h) - lc0
+    clk = clocks.stop()
+    ms = statistics.median(times)
+    ref = copy.copy(inp)
+    ref.gridpt3 = g0.copy()
+    r_pts, r_det = pts0.copy(), np.zeros(len(pts0), np.uint8)
+    r_counts, r_zext = np.zeros(2, np.int64), np.array([1e5, -1e5])
+    refpy.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    refpy.blunder_detection_tin(ref, it, oncc, fb, cbl, hint, r_pts, r_det, tris, r_counts,
+                                r_zext)
+    cpu_s = time.perf_counter() - t
+    pts, det, gp3, counts, zext = got
+    npt = len(pts0)
+    line = {
+        "metric": "matched points/s (blunder_detection_TIN)", "value": npt / (dev_ms / 1e3),
+        "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup),
+        "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (the reference's arithmetic)", "data": "synthetic",
+        "config": {"workload": "blunder_detection_TIN: 1024^2 grid at 2 m, 21 k matched points, "
+                               "Delaunay TIN, level 0, iteration 1, Hinterval 60",
+                   "nodes": n, "points": npt, "triangles": int(len(tris))},
+        "e2e": {"value": npt / (ms / 1e3), "unit": "points/s",
+                "h2d_bytes_per_step": int(pts0.nbytes + tris.nbytes + oncc.nbytes + npt),
+                "d2h_bytes_per_step": int(pts0.nbytes + npt + 9 * npt),
+                "timing": "host wall clock of vll_blunder_detection_tin on host buffers (copies "
+                          "included: points, triangles, the ortho NCC grid and the marks up; "
+                          "points, marks and the anchor_flag writes down; value: "
+                          "vll_blunder_detection_tin_device on resident data)"},
+        "cpu_baseline": {"value": npt / cpu_s, "unit": "points/s", "cores": os.cpu_count(),
+                         "kind": "reference", "sample": f"whole TIN, {cpu_s:.4f} s"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "parity": {"flags_identical": bool(np.array_equal(pts["flag"], r_pts["flag"])),
+                   "detected_identical": bool(np.array_equal(det, r_det)),
+                   "gridpt3_field_mismatch": field_mismatch(gp3, ref.gridpt3),
+                   "counts_identical": bool(np.array_equal(counts, r_counts)),
+                   "extent_identical": bool(np.array_equal(zext, r_zext)),
+                   "new_blunders": int(det.sum()),
+                   "point_pass_reruns": f"{reruns} of {args.steps} timed device calls"},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    del torch
+
+
 def run_voxel_iter(args):
     """One matching iteration of the voxel route at level 0 with SGM
     (SGM_py = 1) on the reduced C2 scene (4096^2 pair, 1024^2 grid, TIN
@@ -1192,7 +1305,7 @@ def main():
     ap.add_argument("--config", default="c2",
                     choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm", "seeddem",
                              "blunder", "ortho_tin", "height_range", "select_mps",
-                             "voxel_iter"])
+                             "voxel_iter", "tin_blunder"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -1229,6 +1342,8 @@ def main():
         run_select_mps(args)
     elif args.config == "voxel_iter":
         run_voxel_iter(args)
+    elif args.config == "tin_blunder":
+        run_tin_blunder(args)
     else:
         run_ours(args)
 

@@ -499,6 +499,21 @@ int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int 
                               int64_t n_pts, const vll_tri *tris, int64_t n_tris,
                               vll_ugrid *gridpt3, int64_t *blunder_count, double *minz_mp,
                               double *maxz_mp);
+/* The same on device data (ortho_ncc, pts, detected_blunders, tris and
+ * gridpt3 are device pointers; blunder_count, minz_mp and maxz_mp are host
+ * pointers).  Waits. */
+int vll_blunder_detection_tin_device(vll_context *ctx, const vll_level_desc *desc, int iteration,
+                                     const float *d_ortho_ncc, int flag_blunder, int count_bl,
+                                     double hinterval, vll_point3 *d_pts,
+                                     uint8_t *d_detected_blunders, int64_t n_pts,
+                                     const vll_tri *d_tris, int64_t n_tris, vll_ugrid *d_gridpt3,
+                                     int64_t *blunder_count, double *minz_mp, double *maxz_mp);
+/* blunder_detection_TIN forms its height-difference sums in parallel and
+ * bounds their distance from the reference's sequential sums; a point pass in
+ * which some comparison falls inside the resulting threshold band is undone
+ * and run again with the sequential sums.  The number of such calls on this
+ * context. */
+int64_t vll_tin_rerun_count(const vll_context *ctx);
 
 /*
  * SetHeightRange (setsm_code.cpp:9851-10255): the next iteration's height

@@ -73,6 +73,7 @@ struct vll_context {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEvent_t stage_ev[9] = {};
     int64_t launches_total = 0;
+    int64_t tin_reruns = 0;   // blunder_detection_TIN calls that re-ran the point pass
     vll::DevLevel *hlevel = nullptr;   // pinned host staging of the level block
 };
 
@@ -789,6 +790,8 @@ void *vll_get_stream(vll_context *ctx) { return ctx ? (void *)ctx->stream : null
 
 int64_t vll_launch_count(const vll_context *ctx) { return ctx ? ctx->launches_total : 0; }
 
+int64_t vll_tin_rerun_count(const vll_context *ctx) { return ctx ? ctx->tin_reruns : 0; }
+
 int64_t vll_voxel_count(const vll_nccresult *ncc, int64_t n) {
     if (!ncc || n <= 0) return 0;
     int64_t s = 0;
@@ -1483,34 +1486,43 @@ static void height_range_constants(const vll_level_desc *d, int iteration, doubl
     *th_hg = th;
 }
 
-int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int iteration,
-                              const float *ortho_ncc, int flag_blunder, int count_bl,
-                              double hinterval, vll_point3 *pts, uint8_t *detected_blunders,
-                              int64_t n_pts, const vll_tri *tris, int64_t n_tris,
-                              vll_ugrid *gridpt3, int64_t *blunder_count, double *minz_mp,
-                              double *maxz_mp) {
-    NvtxRange nvtx_range("vll_blunder_detection_tin");
+// blunder_detection_TIN's argument checks; 1 = nothing to do (level 0,
+// iteration 3, which the reference skips).
+static int tin_blunder_check(vll_context *ctx, const vll_level_desc *desc, int iteration,
+                             const void *ortho_ncc, double hinterval, const void *pts,
+                             const void *detected, int64_t n_pts, const void *tris,
+                             int64_t n_tris, const void *gridpt3, const void *blunder_count,
+                             const void *minz_mp, const void *maxz_mp) {
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
     if (!desc || !ortho_ncc || !gridpt3 || !blunder_count || !minz_mp || !maxz_mp ||
-        (n_pts > 0 && (!pts || !detected_blunders)) || (n_tris > 0 && !tris))
+        (n_pts > 0 && (!pts || !detected)) || (n_tris > 0 && !tris))
         return fail(ctx, VLL_ERR_INVALID, "null argument");
     if (n_pts < 0 || n_tris < 0 || n_pts > 0x7fffffff || 3 * n_tris > 0x7fffffff)
         return fail(ctx, VLL_ERR_INVALID, "point or triangle count out of range");
     if (desc->grid_width <= 0 || desc->grid_height <= 0 || !(desc->grid_resolution > 0) ||
         desc->pyramid_step < 0 || desc->pyramid_step > 12)
         return fail(ctx, VLL_ERR_INVALID, "invalid grid or level");
-    if (desc->pyramid_step == 0 && iteration == 3) return VLL_OK;   // the reference skips it
+    if (desc->pyramid_step == 0 && iteration == 3) return 1;   // the reference skips it
     if (!(hinterval >= 0) || hinterval > 1e8)
         return fail(ctx, VLL_ERR_INVALID, "Hinterval out of range");
     VLL_CUDA(ctx, cudaSetDevice(ctx->device));
-    const int64_t N = desc->grid_width * desc->grid_height;
+    return VLL_OK;
+}
+
+// blunder_detection_TIN on device data; counts and extent accumulate into
+// the host outputs as the reference's do.
+static int tin_blunder_run(vll_context *ctx, const vll_level_desc *desc, int iteration,
+                           const float *d_oncc, int flag_blunder, int count_bl, double hinterval,
+                           vll_point3 *d_pts, uint8_t *d_det, int64_t n_pts, const vll_tri *d_tris,
+                           int64_t n_tris, vll_ugrid *d_gp3, int64_t *blunder_count,
+                           double *minz_mp, double *maxz_mp, vll_ugrid *host_gp3 = nullptr) {
     const uint32_t hdiffcount = (uint32_t)hinterval;
     vll::TinArgs a;
     a.b0 = desc->boundary[0];
     a.b1 = desc->boundary[1];
     a.gs = desc->grid_resolution;
     a.width = desc->grid_width;
-    a.n_nodes = N;
+    a.n_nodes = desc->grid_width * desc->grid_height;
     a.n_pts = n_pts;
     a.n_tris = n_tris;
     a.L = desc->pyramid_step;
@@ -1520,34 +1532,40 @@ int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int 
     a.count_bl = count_bl;
     a.height_th = a.ortho_ncc_th = a.th_ref_ncc = 0;
     a.hinterval = hinterval;
-    int rc;
-    if ((rc = upload(ctx, ctx->tin_pts, pts, (size_t)n_pts * sizeof(vll_point3)))) return rc;
-    if ((rc = upload(ctx, ctx->tin_tris, tris, (size_t)n_tris * sizeof(vll_tri)))) return rc;
-    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
-    if ((rc = upload(ctx, ctx->gsum, ortho_ncc, (size_t)N * sizeof(float)))) return rc;
-    if ((rc = upload(ctx, ctx->gcnt, detected_blunders, (size_t)(n_pts > 0 ? n_pts : 1))))
-        return rc;
+    a.height_th_hi = 0;
+    // SETSM_VLL_TIN_SUMS=exact: the sequential sums always (no band);
+    // =wideband: the band widened by 1 m (the exact re-run on nearly every
+    // input)
+    int mode = vll::kTinSumsBand;
+    if (const char *m = getenv("SETSM_VLL_TIN_SUMS")) {
+        if (!strcmp(m, "exact")) mode = vll::kTinSumsExact;
+        else if (!strcmp(m, "wideband")) mode = vll::kTinSumsWideBand;
+    }
     const size_t bytes = vll::tin_blunder_scratch(n_pts, n_tris, hdiffcount);
     VLL_CUDA(ctx, ensure(ctx->tin_scratch, bytes));
-    vll::TinThresholds th{0, 0, 0};
     vll::TinOutput out;
     memset(&out, 0, sizeof(out));
-    VLL_CUDA(ctx, vll::run_tin_blunder(a, (vll_point3 *)ctx->tin_pts.p,
-                                       (const vll_tri *)ctx->tin_tris.p,
-                                       (const float *)ctx->gsum.p, (vll_ugrid *)ctx->gp3.p,
-                                       (uint8_t *)ctx->gcnt.p, hdiffcount, ctx->tin_scratch.p,
-                                       bytes, th, &out, ctx->stream));
+    VLL_CUDA(ctx, vll::run_tin_blunder(a, d_pts, d_tris, d_oncc, d_gp3, d_det, hdiffcount, mode,
+                                       host_gp3 != nullptr, ctx->tin_scratch.p, bytes, &out,
+                                       ctx->stream));
     if (out.bad_input) return fail(ctx, VLL_ERR_INVALID, "a point's grid node lies outside the grid");
-    ctx->launches_total += 7;
-    if (n_pts > 0) {
-        VLL_CUDA(ctx, cudaMemcpyAsync(pts, ctx->tin_pts.p, (size_t)n_pts * sizeof(vll_point3),
+    if (host_gp3 && n_pts > 0) {
+        // the pass's anchor_flag writes, applied to the caller's grid in point
+        // order (the grid itself never crosses the bus)
+        std::vector<int64_t> node((size_t)n_pts);
+        std::vector<uint8_t> val((size_t)n_pts);
+        VLL_CUDA(ctx, cudaMemcpyAsync(node.data(), out.anchor_node, (size_t)n_pts * 8,
                                       cudaMemcpyDeviceToHost, ctx->stream));
-        VLL_CUDA(ctx, cudaMemcpyAsync(detected_blunders, ctx->gcnt.p, (size_t)n_pts,
+        VLL_CUDA(ctx, cudaMemcpyAsync(val.data(), out.anchor_val, (size_t)n_pts,
                                       cudaMemcpyDeviceToHost, ctx->stream));
+        VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        for (int64_t i = 0; i < n_pts; ++i)
+            if (node[i] >= 0) host_gp3[node[i]].anchor_flag = val[i];
     }
-    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // terms, sums, pairs, radix sort (4), scan (2), snapshot, point pass, close;
+    // a re-run adds the undo, the sequential sums, the point pass and close
+    ctx->launches_total += (n_tris > 0 ? 12 : 5) + (out.rerun ? 4 : 0);
+    ctx->tin_reruns += out.rerun;
     blunder_count[0] += out.count[0];
     blunder_count[1] += out.count[1];
     if (out.has_z) {
@@ -1555,6 +1573,55 @@ int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int 
         if (*maxz_mp < out.z[1]) *maxz_mp = out.z[1];
     }
     return VLL_OK;
+}
+
+int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int iteration,
+                              const float *ortho_ncc, int flag_blunder, int count_bl,
+                              double hinterval, vll_point3 *pts, uint8_t *detected_blunders,
+                              int64_t n_pts, const vll_tri *tris, int64_t n_tris,
+                              vll_ugrid *gridpt3, int64_t *blunder_count, double *minz_mp,
+                              double *maxz_mp) {
+    NvtxRange nvtx_range("vll_blunder_detection_tin");
+    int rc = tin_blunder_check(ctx, desc, iteration, ortho_ncc, hinterval, pts, detected_blunders,
+                               n_pts, tris, n_tris, gridpt3, blunder_count, minz_mp, maxz_mp);
+    if (rc) return rc > 0 ? VLL_OK : rc;
+    const int64_t N = desc->grid_width * desc->grid_height;
+    // the pass reads no UGRID field and writes only anchor_flag at the
+    // points' nodes: the grid stays on the host and takes the listed writes
+    if ((rc = upload(ctx, ctx->tin_pts, pts, (size_t)n_pts * sizeof(vll_point3)))) return rc;
+    if ((rc = upload(ctx, ctx->tin_tris, tris, (size_t)n_tris * sizeof(vll_tri)))) return rc;
+    if ((rc = upload(ctx, ctx->gsum, ortho_ncc, (size_t)N * sizeof(float)))) return rc;
+    if ((rc = upload(ctx, ctx->gcnt, detected_blunders, (size_t)(n_pts > 0 ? n_pts : 1))))
+        return rc;
+    if ((rc = tin_blunder_run(ctx, desc, iteration, (const float *)ctx->gsum.p, flag_blunder,
+                              count_bl, hinterval, (vll_point3 *)ctx->tin_pts.p,
+                              (uint8_t *)ctx->gcnt.p, n_pts, (const vll_tri *)ctx->tin_tris.p,
+                              n_tris, nullptr, blunder_count, minz_mp, maxz_mp, gridpt3)))
+        return rc;
+    if (n_pts > 0) {
+        VLL_CUDA(ctx, cudaMemcpyAsync(pts, ctx->tin_pts.p, (size_t)n_pts * sizeof(vll_point3),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        VLL_CUDA(ctx, cudaMemcpyAsync(detected_blunders, ctx->gcnt.p, (size_t)n_pts,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+int vll_blunder_detection_tin_device(vll_context *ctx, const vll_level_desc *desc, int iteration,
+                                     const float *d_ortho_ncc, int flag_blunder, int count_bl,
+                                     double hinterval, vll_point3 *d_pts,
+                                     uint8_t *d_detected_blunders, int64_t n_pts,
+                                     const vll_tri *d_tris, int64_t n_tris, vll_ugrid *d_gridpt3,
+                                     int64_t *blunder_count, double *minz_mp, double *maxz_mp) {
+    NvtxRange nvtx_range("vll_blunder_detection_tin_device");
+    int rc = tin_blunder_check(ctx, desc, iteration, d_ortho_ncc, hinterval, d_pts,
+                               d_detected_blunders, n_pts, d_tris, n_tris, d_gridpt3,
+                               blunder_count, minz_mp, maxz_mp);
+    if (rc) return rc > 0 ? VLL_OK : rc;
+    return tin_blunder_run(ctx, desc, iteration, d_ortho_ncc, flag_blunder, count_bl, hinterval,
+                           d_pts, d_detected_blunders, n_pts, d_tris, n_tris, d_gridpt3,
+                           blunder_count, minz_mp, maxz_mp);
 }
 
 static int height_range_check(vll_context *ctx, const vll_level_desc *desc, const void *pts,

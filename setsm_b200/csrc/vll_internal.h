@@ -59,10 +59,19 @@ struct TinArgs {
     double b0, b1, gs;
     int64_t width, n_nodes, n_pts, n_tris;
     int L, iteration, is_ra, flag_blunder, count_bl;
-    double height_th, ortho_ncc_th, th_ref_ncc, hinterval;
+    // the height threshold lies in [height_th, height_th_hi] (equal when it
+    // is known exactly)
+    double height_th, height_th_hi, ortho_ncc_th, th_ref_ncc, hinterval;
 };
+// How the height-difference sums are formed: kTinSumsBand (default) in
+// parallel, with a bound on their distance from the reference's sequential
+// sums and an exact re-run when a comparison falls inside the resulting
+// threshold band; kTinSumsExact sequentially on one SM; kTinSumsWideBand as
+// kTinSumsBand with the band widened by 1 m on each side (re-runs on nearly
+// every input: exercises the re-run).
+enum { kTinSumsBand = 0, kTinSumsExact = 1, kTinSumsWideBand = 2 };
 struct TinThresholds {
-    double height_th, ortho_ncc_th, th_ref_ncc;
+    double height_th, height_th_hi, ortho_ncc_th, th_ref_ncc;
 };
 struct TinOutput {
     int bad_input;        // a vertex's grid node outside the grid
@@ -70,16 +79,26 @@ struct TinOutput {
     int has_z;            // z: height extent of the kept points
     double z[2];
     double height_th;
+    int rerun;            // the point pass ran again with the exact threshold
+    // anchor_list: per point the grid node whose anchor_flag the pass set (-1:
+    // none) and the value (device pointers into the scratch)
+    const int64_t *anchor_node;
+    const uint8_t *anchor_val;
 };
-// The thresholds from the triangle statistics (sums: ortho NCC sum, sum of
-// squares, dh sum, sum of squares, counts), as the reference derives them.
-void tin_thresholds(const TinArgs &a, const double *sums, const uint32_t *hbin,
-                    uint32_t hdiffcount, TinThresholds *th);
+// The thresholds from the triangle statistics as the reference derives them
+// (setsm_code.cpp:9289-9418): sd, sd2 = the sums of the height differences and
+// of their squares, each known to lie in [lo, hi]; dh_count their number;
+// hbin the histogram of the integer parts.  th->height_th / height_th_hi
+// bound the reference's height threshold (equal when lo == hi).
+void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], long dh_count,
+                    const uint32_t *hbin, uint32_t hdiffcount, TinThresholds *th);
+// anchor_list: the pass leaves gp3 alone and lists its anchor_flag writes
+// (TinOutput::anchor_node / anchor_val) for the caller to apply.
 size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount);
 cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                             const float *ortho_ncc, vll_ugrid *gp3, uint8_t *detected,
-                            uint32_t hdiffcount, void *scratch, size_t bytes,
-                            const TinThresholds &th_in, TinOutput *out, cudaStream_t s);
+                            uint32_t hdiffcount, int sums_mode, bool anchor_list,
+                            void *scratch, size_t bytes, TinOutput *out, cudaStream_t s);
 
 // vll_initvoxel.cu: InitializeVoxel.  run_init_voxel decides every node
 // (into scratch) and fills new_off[0..n] with the new packing, *total the new

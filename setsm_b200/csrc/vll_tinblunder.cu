@@ -10,7 +10,7 @@
 // which of 1 / 3 lands first on a point that was 0 (set_blunder, :9121); the
 // closing pass turns 3 into 1, so the outputs do not depend on the race.
 //
-// GPU: the per-triangle terms in parallel, the FP64 sums by one thread in the
+// GPU: the per-triangle terms in parallel, the FP64 sums by one warp in the
 // reference's triangle order (a sum's rounding depends on its order), the
 // per-point triangle lists by a stable radix sort of (point, triangle), the
 // point pass one thread per point with the same compare-and-swap marking, and
@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -40,87 +41,121 @@ __device__ __forceinline__ int64_t grid_index(const TinArgs &a, double x, double
     return a.width * r + c;
 }
 
-// Per triangle: the vertices' ortho NCC terms and the edge height
-// differences, and the histogram of the differences (order-free).
-struct TriTerms {
-    float oncc[3];
-    uint8_t has_oncc[3];
-    uint8_t valid;
-    double dh[3];
-};
-
+// Per triangle: its three edge height differences (+0 for a triangle with a
+// vertex past the points, which adds nothing to the sums of non-negative
+// terms: s + 0 == s for every s those sums take), the count of valid
+// triangles and the histogram of the differences (order-free), and the check
+// that every vertex's grid node lies in the grid.  The vertices' ortho NCC
+// statistics of the reference (:9200-9252) feed only an ortho-NCC threshold
+// that it overwrites with the level's constant (:9304-9313), so they are not
+// formed.
 __global__ void tri_terms_kernel(TinArgs a, const vll_point3 *pts, const vll_tri *tris,
-                                 const float *ortho_ncc, TriTerms *terms, uint32_t *hbin,
-                                 uint32_t hdiffcount, unsigned int *bad) {
+                                 double *dhv, uint32_t *hbin, uint32_t hdiffcount,
+                                 unsigned long long *n_valid, unsigned int *bad) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < a.n_tris;
          t += (int64_t)gridDim.x * blockDim.x) {
         const vll_tri tr = tris[t];
         const uint32_t v[3] = {tr.a, tr.b, tr.c};
-        TriTerms T;
-        T.valid = 1;
+        bool valid = true;
+        double z[3];
         for (int k = 0; k < 3; ++k) {
-            T.has_oncc[k] = 0;
-            T.oncc[k] = 0.f;
             if (v[k] < (uint64_t)a.n_pts) {
                 const vll_point3 p = pts[v[k]];
+                z[k] = p.z;
                 // int t_col / t_row and an int index, as the reference
                 const int tc = (int)__dadd_rn(__ddiv_rn(__dadd_rn(p.x, -a.b0), a.gs), 0.5);
                 const int trw = (int)__dadd_rn(__ddiv_rn(__dadd_rn(p.y, -a.b1), a.gs), 0.5);
                 const int idx = (int)((unsigned)a.width * (unsigned)trw + (unsigned)tc);
-                if (idx < 0 || (int64_t)idx >= a.n_nodes) {
-                    atomicExch(bad, 1u);
-                    continue;
-                }
-                const float o = ortho_ncc[idx];
-                if (o > -1) {
-                    T.has_oncc[k] = 1;
-                    T.oncc[k] = o;
-                }
+                if (idx < 0 || (int64_t)idx >= a.n_nodes) atomicExch(bad, 1u);
             } else {
-                T.valid = 0;
+                valid = false;
             }
         }
-        if (T.valid) {
-            const double z0 = pts[v[0]].z, z1 = pts[v[1]].z, z2 = pts[v[2]].z;
-            T.dh[0] = fabs(__dadd_rn(z0, -z1));
-            T.dh[1] = fabs(__dadd_rn(z0, -z2));
-            T.dh[2] = fabs(__dadd_rn(z1, -z2));
+        double dh[3] = {0.0, 0.0, 0.0};
+        if (valid) {
+            dh[0] = fabs(__dadd_rn(z[0], -z[1]));
+            dh[1] = fabs(__dadd_rn(z[0], -z[2]));
+            dh[2] = fabs(__dadd_rn(z[1], -z[2]));
             for (int k = 0; k < 3; ++k) {
-                const double f = (double)(uint32_t)T.dh[k];
+                const double f = (double)(uint32_t)dh[k];
                 if (f < (double)hdiffcount) atomicAdd(hbin + (uint32_t)f, 1u);
             }
+            atomicAdd(n_valid, 1ull);
         }
-        terms[t] = T;
+        for (int k = 0; k < 3; ++k) dhv[3 * t + k] = dh[k];
     }
 }
 
-// The reference's FP64 sums, in triangle order (one thread).
-__global__ void tri_sums_kernel(int64_t n_tris, const TriTerms *terms, double *sums) {
-    double so = 0, so2 = 0, sd = 0, sd2 = 0;
-    long long no = 0, nd = 0;
-    for (int64_t t = 0; t < n_tris; ++t) {
-        const TriTerms T = terms[t];
-        for (int k = 0; k < 3; ++k) {
-            if (T.has_oncc[k]) {
-                so = __dadd_rn(so, (double)T.oncc[k]);
-                so2 = __dadd_rn(so2, (double)__fmul_rn(T.oncc[k], T.oncc[k]));
-                ++no;
-            }
+// The sums of the differences and of their squares in any order (sums[0],
+// sums[1], zeroed before): a grid-stride pass, warp and block reduction, one
+// atomic add per block.  Any summation order of m non-negative terms lies
+// within (m-1) u (1 + O(u)) of the exact sum, as does the reference's
+// sequential order; the thresholds take the band that follows.
+__global__ void dh_psum_kernel(int64_t n_vals, const double *__restrict__ dhv, double *sums) {
+    double s = 0, s2 = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_vals;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = dhv[i];
+        s = __dadd_rn(s, v);
+        s2 = __dadd_rn(s2, __dmul_rn(v, v));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s = __dadd_rn(s, __shfl_down_sync(0xffffffffu, s, o));
+        s2 = __dadd_rn(s2, __shfl_down_sync(0xffffffffu, s2, o));
+    }
+    __shared__ double part[2][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        part[0][w] = s;
+        part[1][w] = s2;
+    }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        s = lane < nw ? part[0][lane] : 0.0;
+        s2 = lane < nw ? part[1][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            s = __dadd_rn(s, __shfl_down_sync(0xffffffffu, s, o));
+            s2 = __dadd_rn(s2, __shfl_down_sync(0xffffffffu, s2, o));
         }
-        if (T.valid) {
-            for (int k = 0; k < 3; ++k) {
-                sd = __dadd_rn(sd, T.dh[k]);
-                sd2 = __dadd_rn(sd2, __dmul_rn(T.dh[k], T.dh[k]));
-                ++nd;
-            }
+        if (lane == 0) {
+            atomicAdd(sums, s);
+            atomicAdd(sums + 1, s2);
         }
     }
-    sums[0] = so;
-    sums[1] = so2;
-    sums[2] = sd;
-    sums[3] = sd2;
-    sums[4] = (double)no;
-    sums[5] = (double)nd;
+}
+
+// The reference's sums in its order (triangle by triangle, three edges each,
+// :9257-9273) into sums[0], sums[1]: the block stages 2048 terms and their
+// squares in shared memory, one thread adds them in sequence, so the running
+// sums round as the reference's do.  A dependent FP64 add takes about 4 ns
+// here, so this is the slow path (the band's re-run).
+constexpr int kSerialChunk = 2048;
+__global__ void __launch_bounds__(512) dh_serial_sum_kernel(int64_t n_vals,
+                                                            const double *__restrict__ dhv,
+                                                            double *sums) {
+    __shared__ double val[kSerialChunk], sq[kSerialChunk];
+    double sd = 0, sd2 = 0;
+    for (int64_t base = 0; base < n_vals; base += kSerialChunk) {
+        for (int i = threadIdx.x; i < kSerialChunk; i += blockDim.x) {
+            const double v = base + i < n_vals ? dhv[base + i] : 0.0;
+            val[i] = v;
+            sq[i] = __dmul_rn(v, v);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll 16
+            for (int i = 0; i < kSerialChunk; ++i) {
+                sd = __dadd_rn(sd, val[i]);
+                sd2 = __dadd_rn(sd2, sq[i]);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        sums[0] = sd;
+        sums[1] = sd2;
+    }
 }
 
 // (point, triangle) pairs in triangle order, 3 per triangle (invalid
@@ -178,13 +213,24 @@ __device__ double normal_angle(const vll_point3 &p0, const vll_point3 &p1, const
     return angle;
 }
 
+// x > the reference's height threshold, which lies in [height_th,
+// height_th_hi]: when the two ends disagree the answer is not known and the
+// pass is marked for an exact re-run.
+__device__ __forceinline__ bool above_th(double x, const TinArgs &a, unsigned int *rerun) {
+    const bool hi = x > a.height_th_hi;
+    if (hi != (x > a.height_th)) *rerun = 1u;
+    return hi;
+}
+
 // The point pass (:9426-9756).
 __global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                              const float *ortho_ncc, const int32_t *sorted_tri,
                              const int64_t *start, const unsigned int *count, vll_ugrid *gp3,
-                             uint8_t *detected, const uint8_t *flag0, unsigned int *bad) {
+                             uint8_t *detected, const uint8_t *flag0, unsigned int *bad,
+                             unsigned int *rerun, int64_t *anchor_node, uint8_t *anchor_val) {
     for (int64_t index = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; index < a.n_pts;
          index += (int64_t)gridDim.x * blockDim.x) {
+        if (anchor_node) anchor_node[index] = -1;
         if (flag0[index] == 1) continue;
         bool pt_is_blunder = false;
         int count_pos = 0, count_neg = 0, cnt = 0;
@@ -196,11 +242,16 @@ __global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
             atomicExch(bad, 1u);
             continue;
         }
-        gp3[ref_index].anchor_flag = 0;
         const float ref_oncc = ortho_ncc[ref_index];
         if (!a.is_ra && ref_oncc < a.th_ref_ncc && a.L >= 2) pt_is_blunder = true;
-        if (a.L >= 3 && a.iteration >= 4 && ref_oncc >= 0.95 && a.flag_blunder)
-            gp3[ref_index].anchor_flag = 1;
+        const uint8_t anchor =
+            (a.L >= 3 && a.iteration >= 4 && ref_oncc >= 0.95 && a.flag_blunder) ? 1 : 0;
+        if (anchor_node) {
+            anchor_node[index] = ref_index;
+            anchor_val[index] = anchor;
+        } else {
+            gp3[ref_index].anchor_flag = anchor;
+        }
         for (int it = 0; it < max_iter; ++it) {
             const int64_t tc = sorted_tri[start[index] + it];
             // triangle 0 is never used here, as in the reference (savenode > 0)
@@ -241,7 +292,8 @@ __global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                 const double d1 = __dadd_rn(fabs(dh1), -fabs(dh2));
                 const double d2 = __dadd_rn(fabs(dh1), -fabs(dh3));
                 const double d3 = __dadd_rn(fabs(dh2), -fabs(dh3));
-                if (fabs(d1) > a.height_th || fabs(d2) > a.height_th || fabs(d3) > a.height_th) {
+                if (above_th(fabs(d1), a, rerun) || above_th(fabs(d2), a, rerun) ||
+                    above_th(fabs(d3), a, rerun)) {
                     const int64_t order[3] = {reference_index, t0, t1};
                     const double h[3] = {p0.z, p1.z, p2.z};
                     const int64_t Index[3] = {grid_index(a, p0.x, p0.y), grid_index(a, p1.x, p1.y),
@@ -284,9 +336,9 @@ __global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                     const double dh = __dadd_rn(h1, -h2);
                     int64_t bn = -1;
                     int pick = -1;
-                    if (dh > 0 && dh > a.height_th)
+                    if (dh > 0 && above_th(dh, a, rerun))
                         pick = mn;
-                    else if (dh < 0 && fabs(dh) > a.height_th)
+                    else if (dh < 0 && above_th(fabs(dh), a, rerun))
                         pick = mx;
                     if (pick >= 0) {
                         if (a.is_ra) {
@@ -355,7 +407,8 @@ __device__ __forceinline__ unsigned long long dkey(double v) {
 // The closing pass (:9765-9781): blunder counts, 3 -> 1, the height extent
 // of the remaining points.
 __global__ void close_kernel(int64_t n_pts, vll_point3 *pts, unsigned long long *cnt,
-                             unsigned long long *zkey) {
+                             unsigned long long *zkey, const unsigned int *rerun) {
+    if (*rerun) return;   // the point pass runs again first
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pts;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint8_t f = pts[i].flag;
@@ -372,10 +425,25 @@ __global__ void close_kernel(int64_t n_pts, vll_point3 *pts, unsigned long long 
     }
 }
 
-__global__ void copy_flags_kernel(int64_t n, const vll_point3 *pts, uint8_t *flag0) {
+// Snapshot of the point flags and the new-blunder marks before the point
+// pass, and its undoing before a re-run (the pass's UGRID writes do not
+// depend on the height threshold and are simply repeated).
+__global__ void copy_flags_kernel(int64_t n, const vll_point3 *pts, uint8_t *flag0,
+                                  const uint8_t *det, uint8_t *det0) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
+         i += (int64_t)gridDim.x * blockDim.x) {
         flag0[i] = pts[i].flag;
+        det0[i] = det[i];
+    }
+}
+
+__global__ void restore_flags_kernel(int64_t n, vll_point3 *pts, const uint8_t *flag0,
+                                     uint8_t *det, const uint8_t *det0) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        pts[i].flag = flag0[i];
+        det[i] = det0[i];
+    }
 }
 
 unsigned blocks_for(int64_t n, int threads) {
@@ -406,12 +474,28 @@ size_t scan_tmp_bytes(int64_t n) {
 
 }  // namespace
 
-void tin_thresholds(const TinArgs &a, const double *sums, const uint32_t *hbin,
-                    uint32_t hdiffcount, TinThresholds *th) {
+namespace {
+
+// The reference's height threshold as a function of up_3sigma (:9362-9418):
+// clamp(up, H/2, H) from level 3 on, min(up, th80, 50) below; a NaN up
+// compares false, as +inf would.  Non-decreasing in up.
+double height_th_of(bool ge3, double H, uint32_t th80, double up) {
+    if (ge3) {
+        double h = H;
+        if (up < h) h = up < h / 2.0 ? h / 2.0 : up;
+        return h;
+    }
+    double h = up < th80 ? up : (double)th80;
+    if (h > 50) h = 50;
+    return h;
+}
+
+}  // namespace
+
+void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], long dh_count,
+                    const uint32_t *hbin, uint32_t hdiffcount, TinThresholds *th) {
     const int L = a.L, it = a.iteration;
-    const double sum_data = sums[2], sum_data2 = sums[3];
-    const long dh_count = (long)sums[5];
-    // the ortho-NCC threshold of the level (:9299-9308; the statistics-based
+    // the ortho-NCC threshold of the level (:9304-9313; the statistics-based
     // value computed before it is overwritten there)
     double ortho_ncc_th;
     if (L == 4)
@@ -433,26 +517,19 @@ void tin_thresholds(const TinArgs &a, const double *sums, const uint32_t *hbin,
         check_dh = it <= 4;
     else if (L <= 1)
         check_dh = it <= 2;
-    double height_th;
-    if (L >= 3) {
+    const bool ge3 = L >= 3;
+    double H = 0;
+    if (ge3) {
         double gsd = a.gs;
         if (gsd < (double)(1 << (L - 1))) gsd = (double)(1 << (L - 1));
         double th2 = gsd * 10;
         if (a.is_ra == 1) th2 = gsd * 30;
-        height_th = a.hinterval < th2 ? a.hinterval : th2;
-        double up;
-        if (check_dh) {
-            const double mean = sum_data / dh_count;
-            const double sd = sqrt((sum_data2 - (sum_data) * (sum_data) / dh_count) / dh_count);
-            up = mean + 3 * sd;
-        } else {
-            up = height_th;
-        }
-        if (up < height_th) height_th = up < height_th / 2.0 ? height_th / 2.0 : up;
-    } else {
-        // levels 0-2: the 99th percentile of the height differences (the
-        // reference computes a GSD-based threshold first and overwrites it)
-        uint32_t th80 = 1000, total_dh = 0;
+        H = a.hinterval < th2 ? a.hinterval : th2;
+    }
+    // levels 0-2: the 99th percentile of the integer height differences
+    uint32_t th80 = 1000;
+    if (!ge3) {
+        uint32_t total_dh = 0;
         long t = 0;
         bool found = false;
         while (t < (long)hdiffcount && !found) {
@@ -465,13 +542,35 @@ void tin_thresholds(const TinArgs &a, const double *sums, const uint32_t *hbin,
             ++t;
         }
         if (!found) th80 = (uint32_t)(t - 1);
-        const double mean = sum_data / dh_count;
-        const double sd = sqrt((sum_data2 - (sum_data) * (sum_data) / dh_count) / dh_count);
-        const double up = mean + 3 * sd;
-        height_th = up < th80 ? up : (double)th80;
-        if (height_th > 50) height_th = 50;
     }
-    th->height_th = height_th;
+    double lo, hi;
+    if (ge3 && !check_dh) {
+        lo = hi = height_th_of(true, H, th80, H);
+    } else {
+        // up = mean + 3 std, evaluated as the reference does; each operation
+        // is non-decreasing in its operand (or non-increasing, for the
+        // subtrahend) over sums >= 0, and rounding to nearest is
+        // monotone, so the corners of the sums' box bound the reference's
+        // rounded value
+        const double n = (double)dh_count;
+        auto var_num = [&](double s, double s2) { return s2 - s * s / n; };
+        const double mean_lo = sd[0] / n, mean_hi = sd[1] / n;
+        const double vn_lo = var_num(sd[1], sd2[0]), vn_hi = var_num(sd[0], sd2[1]);
+        const double nan = std::numeric_limits<double>::quiet_NaN();
+        if (vn_hi < 0) {
+            lo = hi = height_th_of(ge3, H, th80, nan);   // sqrt of a negative: NaN
+        } else if (vn_lo < 0) {
+            // std >= 0, or NaN (which compares as +inf)
+            lo = height_th_of(ge3, H, th80, mean_lo);
+            hi = height_th_of(ge3, H, th80, nan);
+        } else {
+            lo = height_th_of(ge3, H, th80, mean_lo + 3 * sqrt(vn_lo / n));
+            hi = height_th_of(ge3, H, th80, mean_hi + 3 * sqrt(vn_hi / n));
+        }
+        if (hi < lo) hi = lo;
+    }
+    th->height_th = lo;
+    th->height_th_hi = hi;
     th->ortho_ncc_th = ortho_ncc_th;
     th->th_ref_ncc = th_ref_ncc;
 }
@@ -479,15 +578,29 @@ void tin_thresholds(const TinArgs &a, const double *sums, const uint32_t *hbin,
 size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount) {
     const int64_t np = 3 * n_tris;
     size_t t = sort_tmp_bytes(np > 0 ? np : 1), u = scan_tmp_bytes(n_pts + 1);
-    return al(t > u ? t : u) + al(n_tris * sizeof(TriTerms)) + al((hdiffcount + 1) * 4) +
-           al(64) + 4 * al(np * 4) + al((n_pts + 1) * 4) + al((n_pts + 1) * 8) + al(n_pts) +
-           al(64);
+    return al(t > u ? t : u) + al(3 * n_tris * sizeof(double)) + al((hdiffcount + 1) * 4) +
+           al(64) + 4 * al(np * 4) + al((n_pts + 1) * 4) + al((n_pts + 1) * 8) + 2 * al(n_pts) +
+           al(128) + al(n_pts * 8) + al(n_pts);
 }
+
+namespace {
+
+// The sums' bound (lo, hi) around the reference's sequential sums, given the
+// sums s in another order of m terms >= 0: |seq - s| <= 2 (m-1) u (1 + O(u))
+// * exact, and exact <= s (1 + (m-1) u (1 + O(u))); 3 m u covers both.
+void sum_band(double s, int64_t m, double out[2]) {
+    const double e = s * (3.0 * (double)m * 0x1p-53) * (1.0 + 0x1p-40);
+    out[0] = std::nextafter(s - e, -INFINITY);
+    if (out[0] < 0) out[0] = 0;
+    out[1] = std::nextafter(s + e, INFINITY);
+}
+
+}  // namespace
 
 cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                             const float *ortho_ncc, vll_ugrid *gp3, uint8_t *detected,
-                            uint32_t hdiffcount, void *scratch, size_t bytes,
-                            const TinThresholds &th_in, TinOutput *out, cudaStream_t s) {
+                            uint32_t hdiffcount, int sums_mode, bool anchor_list,
+                            void *scratch, size_t bytes, TinOutput *out, cudaStream_t s) {
     const int64_t np = 3 * a.n_tris;
     size_t tmp_b = sort_tmp_bytes(np > 0 ? np : 1), u = scan_tmp_bytes(a.n_pts + 1);
     if (u > tmp_b) tmp_b = u;
@@ -498,7 +611,7 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         return r;
     };
     void *tmp = take(tmp_b);
-    TriTerms *terms = (TriTerms *)take(a.n_tris * sizeof(TriTerms));
+    double *dhv = (double *)take(3 * a.n_tris * sizeof(double));
     uint32_t *hbin = (uint32_t *)take((hdiffcount + 1) * 4);
     double *sums = (double *)take(64);
     uint32_t *key = (uint32_t *)take(np * 4);
@@ -508,17 +621,29 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     unsigned int *count = (unsigned int *)take((a.n_pts + 1) * 4);
     int64_t *start = (int64_t *)take((a.n_pts + 1) * 8);
     uint8_t *flag0 = (uint8_t *)take(a.n_pts);
-    unsigned long long *misc = (unsigned long long *)take(64);   // [0..1] counts, [2..3] z keys, [4] bad
+    uint8_t *det0 = (uint8_t *)take(a.n_pts);
+    // [0..1] counts, [2..3] z keys, [4] bad input, [5] valid triangles,
+    // [6] re-run due
+    unsigned long long *misc = (unsigned long long *)take(128);
+    int64_t *anchor_node = (int64_t *)take(a.n_pts * 8);
+    uint8_t *anchor_val = (uint8_t *)take(a.n_pts);
+    if (!anchor_list) anchor_node = nullptr, anchor_val = nullptr;
     if ((size_t)(p - (char *)scratch) > bytes) return cudaErrorInvalidValue;
+    unsigned int *bad = reinterpret_cast<unsigned int *>(misc + 4);
+    unsigned int *rerun = reinterpret_cast<unsigned int *>(misc + 6);
+    const bool exact = sums_mode == kTinSumsExact;
     cudaError_t e;
     if ((e = cudaMemsetAsync(hbin, 0, (hdiffcount + 1) * 4, s))) return e;
     if ((e = cudaMemsetAsync(count, 0, (a.n_pts + 1) * 4, s))) return e;
-    if ((e = cudaMemsetAsync(misc, 0, 64, s))) return e;
-    unsigned int *bad = reinterpret_cast<unsigned int *>(misc + 4);
+    if ((e = cudaMemsetAsync(misc, 0, 128, s))) return e;
+    if ((e = cudaMemsetAsync(sums, 0, 64, s))) return e;
     if (a.n_tris > 0) {
-        tri_terms_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, pts, tris, ortho_ncc, terms,
-                                                                   hbin, hdiffcount, bad);
-        tri_sums_kernel<<<1, 1, 0, s>>>(a.n_tris, terms, sums);
+        tri_terms_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, pts, tris, dhv, hbin,
+                                                                   hdiffcount, misc + 5, bad);
+        if (exact)
+            dh_serial_sum_kernel<<<1, 512, 0, s>>>(np, dhv, sums);
+        else
+            dh_psum_kernel<<<blocks_for(np, 256), 256, 0, s>>>(np, dhv, sums);
         pair_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, tris, key, val, count);
         if ((e = cudaGetLastError())) return e;
         int end_bit = 1;
@@ -526,39 +651,91 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         if ((e = cub::DeviceRadixSort::SortPairs(tmp, tmp_b, key, skey, val, sval, (int)np, 0,
                                                  end_bit, s)))
             return e;
-    } else {
-        if ((e = cudaMemsetAsync(sums, 0, 64, s))) return e;
     }
     if ((e = cub::DeviceScan::ExclusiveSum(tmp, tmp_b, count, start, (int)(a.n_pts + 1), s)))
         return e;
-    // the sums, the histogram and the input check back for the thresholds
-    double hs[6];
+    // the sums, the histogram, the valid count and the input check back for
+    // the thresholds
+    double hs[2];
     std::vector<uint32_t> hb(hdiffcount + 1);
-    unsigned long long hbad = 0;
+    unsigned long long hm[6];
     if ((e = cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaMemcpyAsync(hb.data(), hbin, (hdiffcount + 1) * 4, cudaMemcpyDeviceToHost, s)))
         return e;
-    if ((e = cudaMemcpyAsync(&hbad, misc + 4, 8, cudaMemcpyDeviceToHost, s))) return e;
+    if ((e = cudaMemcpyAsync(hm, misc, sizeof(hm), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
-    if (hbad) {
+    if (hm[4]) {
         out->bad_input = 1;
         return cudaSuccess;
     }
-    TinThresholds th = th_in;
-    tin_thresholds(a, hs, hb.data(), hdiffcount, &th);
+    const long dh_count = (long)(3 * hm[5]);
+    double sd[2], sd2[2];
+    const bool band = !exact && std::isfinite(hs[0]) && std::isfinite(hs[1]);
+    if (band) {
+        sum_band(hs[0], np, sd);
+        sum_band(hs[1], np, sd2);
+    }
+    TinThresholds th;
+    auto exact_sums = [&]() -> cudaError_t {
+        cudaError_t e2;
+        if (a.n_tris > 0) {
+            dh_serial_sum_kernel<<<1, 512, 0, s>>>(np, dhv, sums);
+            if ((e2 = cudaGetLastError())) return e2;
+            if ((e2 = cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, s))) return e2;
+            if ((e2 = cudaStreamSynchronize(s))) return e2;
+        }
+        sd[0] = sd[1] = hs[0];
+        sd2[0] = sd2[1] = hs[1];
+        return cudaSuccess;
+    };
+    if (!band && !exact && (e = exact_sums())) return e;
+    if (exact) {
+        sd[0] = sd[1] = hs[0];
+        sd2[0] = sd2[1] = hs[1];
+    }
+    tin_thresholds(a, sd, sd2, dh_count, hb.data(), hdiffcount, &th);
+    if (band && sums_mode == kTinSumsWideBand) {
+        th.height_th -= 1.0;
+        th.height_th_hi += 1.0;
+    }
     a.height_th = th.height_th;
+    a.height_th_hi = th.height_th_hi;
     a.ortho_ncc_th = th.ortho_ncc_th;
     a.th_ref_ncc = th.th_ref_ncc;
-    copy_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0);
-    point_kernel<<<blocks_for(a.n_pts, 128), 128, 0, s>>>(a, pts, tris, ortho_ncc, sval, start,
-                                                         count, gp3, detected, flag0, bad);
     const unsigned long long zinit[2] = {~0ull, 0ull};
+    copy_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0, detected,
+                                                               det0);
+    point_kernel<<<blocks_for(a.n_pts, 128), 128, 0, s>>>(a, pts, tris, ortho_ncc, sval, start,
+                                                         count, gp3, detected, flag0, bad, rerun,
+                                                         anchor_node, anchor_val);
     if ((e = cudaMemcpyAsync(misc + 2, zinit, 16, cudaMemcpyHostToDevice, s))) return e;
-    close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2);
+    close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2, rerun);
     if ((e = cudaGetLastError())) return e;
-    unsigned long long m[5];
+    unsigned long long m[7];
     if ((e = cudaMemcpyAsync(m, misc, sizeof(m), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
+    out->rerun = 0;
+    if (m[6] && !m[4]) {
+        // a comparison fell inside the band: undo the pass and run it again
+        // with the threshold from the sequential sums
+        out->rerun = 1;
+        restore_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0,
+                                                                      detected, det0);
+        if ((e = cudaGetLastError())) return e;
+        if ((e = exact_sums())) return e;
+        tin_thresholds(a, sd, sd2, dh_count, hb.data(), hdiffcount, &th);
+        a.height_th = a.height_th_hi = th.height_th;
+        if ((e = cudaMemsetAsync(misc, 0, 128, s))) return e;
+        point_kernel<<<blocks_for(a.n_pts, 128), 128, 0, s>>>(a, pts, tris, ortho_ncc, sval,
+                                                             start, count, gp3, detected, flag0,
+                                                             bad, rerun, anchor_node, anchor_val);
+        if ((e = cudaMemcpyAsync(misc + 2, zinit, 16, cudaMemcpyHostToDevice, s))) return e;
+        close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2,
+                                                             rerun);
+        if ((e = cudaGetLastError())) return e;
+        if ((e = cudaMemcpyAsync(m, misc, sizeof(m), cudaMemcpyDeviceToHost, s))) return e;
+        if ((e = cudaStreamSynchronize(s))) return e;
+    }
     out->bad_input = m[4] != 0;
     out->count[0] = (int64_t)m[0];
     out->count[1] = (int64_t)m[1];
@@ -570,7 +747,9 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         memcpy(&v, &bits, 8);
         out->z[k] = v;
     }
-    out->height_th = th.height_th;
+    out->height_th = a.height_th;
+    out->anchor_node = anchor_node;
+    out->anchor_val = anchor_val;
     return cudaSuccess;
 }
 

@@ -37,6 +37,7 @@ EXPORTED = [
     "vll_set_height_range", "vll_select_mps", "vll_initialize_voxel",
     "vll_initialize_voxel_device", "vll_awncc_peaks_device", "vll_select_mps_device",
     "vll_set_height_range_device", "vll_blunder_detection_tin",
+    "vll_blunder_detection_tin_device", "vll_tin_rerun_count",
 ]
 
 _lib = None
@@ -113,6 +114,9 @@ def load():
     L.vll_select_mps_device.argtypes = L.vll_select_mps.argtypes
     L.vll_blunder_detection_tin.argtypes = [vp, D, i32, vp, i32, i32, dbl, vp, vp, i64, vp, i64,
                                             vp, vp, vp, vp]
+    L.vll_blunder_detection_tin_device.argtypes = L.vll_blunder_detection_tin.argtypes
+    L.vll_tin_rerun_count.argtypes = [vp]
+    L.vll_tin_rerun_count.restype = i64
     L.vll_set_height_range_device.argtypes = L.vll_set_height_range.argtypes
     _lib = L
     return L
@@ -332,6 +336,18 @@ class Context:
             int(count_bl), float(hinterval), pts.ctypes.data, detected.ctypes.data, len(pts),
             tris.ctypes.data, len(tris), inputs.gridpt3.ctypes.data, counts.ctypes.data,
             zext[0:1].ctypes.data, zext[1:2].ctypes.data))
+
+    def blunder_detection_tin_device(self, desc, iteration: int, d_ortho_ncc: int,
+                                     flag_blunder: bool, count_bl: int, hinterval: float,
+                                     d_pts: int, d_detected: int, n_pts: int, d_tris: int,
+                                     n_tris: int, d_gridpt3: int, counts: np.ndarray,
+                                     zext: np.ndarray) -> None:
+        """blunder_detection_TIN on device buffers (pointers); counts (int64[2])
+        and zext (float64[2]) are host arrays updated in place."""
+        self._check(load().vll_blunder_detection_tin_device(
+            self._h, C.byref(desc), int(iteration), d_ortho_ncc, int(bool(flag_blunder)),
+            int(count_bl), float(hinterval), d_pts, d_detected, int(n_pts), d_tris, int(n_tris),
+            d_gridpt3, counts.ctypes.data, zext[0:1].ctypes.data, zext[1:2].ctypes.data))
 
     def select_mps_device(self, desc, d_ncc: int, d_gridpt3: int, d_points: int, capacity: int,
                           *args) -> int:

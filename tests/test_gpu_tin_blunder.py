@@ -2,7 +2,10 @@
 (setsm_code.cpp:9158-9787): the fixtures made by the reference build, the
 reference build itself over levels, iterations and switches, and the C++
 drop-in with the reference's signature.  Point flags, the new-blunder marks,
-every UGRID field, the counts and the height extent must be identical."""
+every UGRID field, the counts and the height extent must be identical -- with
+the height-difference sums formed in parallel (the threshold band, the
+default), sequentially (SETSM_VLL_TIN_SUMS=exact), and with the band widened so
+that the point pass is undone and re-run (SETSM_VLL_TIN_SUMS=wideband)."""
 import ctypes as C
 
 import numpy as np
@@ -32,8 +35,20 @@ def assert_same(pts, det, gp3, counts, zext, w_pts, w_det, w_gp3, w_counts, w_ze
     assert np.array_equal(zext, w_zext)
 
 
+MODES = ["band", "exact", "wideband"]
+
+
+@pytest.fixture(params=MODES)
+def sums_mode(request, monkeypatch):
+    if request.param != "band":
+        monkeypatch.setenv("SETSM_VLL_TIN_SUMS", request.param)
+    else:
+        monkeypatch.delenv("SETSM_VLL_TIN_SUMS", raising=False)
+    return request.param
+
+
 @pytest.mark.parametrize("name", sorted(mg.GOLDEN_TINB))
-def test_matches_reference_fixture(gpu_ctx, name):
+def test_matches_reference_fixture(gpu_ctx, name, sums_mode):
     inp, pts, tris, oncc, z = mg.tinb_case(name)
     it, fb, cbl, hint = mg.GOLDEN_TINB[name]["call"]
     det, counts, zext = fresh_out(len(pts))
@@ -53,7 +68,7 @@ def test_matches_reference_fixture(gpu_ctx, name):
     (dict(seed=47, size=768, nodes=16, res=24.0, L=4, template=15, flagged_frac=0.3),
      (2, True, 1, 25.0)),
 ])
-def test_matches_reference_build(gpu_ctx, kw, call):
+def test_matches_reference_build(gpu_ctx, kw, call, sums_mode):
     import copy
     inp, pts, tris, oncc = cases.make_tin_blunder_case(**kw)
     ref = copy.copy(inp)
@@ -86,3 +101,36 @@ def test_level0_iteration3_does_nothing(gpu_ctx):
     det, counts, zext = fresh_out(len(pts))
     gpu_ctx.blunder_detection_tin(inp, 3, oncc, True, 1, 60.0, pts, det, tris, counts, zext)
     assert np.array_equal(pts["flag"], before["flag"]) and not det.any() and not counts.any()
+
+
+def test_device_entry_matches_fixture(gpu_ctx):
+    import torch
+    inp, pts, tris, oncc, z = mg.tinb_case("tinb_l1_anchor")
+    it, fb, cbl, hint = mg.GOLDEN_TINB["tinb_l1_anchor"]["call"]
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).cuda()
+    d_pts, d_tris, d_g, d_o = dev(pts), dev(tris), dev(inp.gridpt3), dev(oncc)
+    d_det = torch.zeros(len(pts), dtype=torch.uint8, device="cuda")
+    _, counts, zext = fresh_out(len(pts))
+    gpu_ctx.blunder_detection_tin_device(inp.desc(), it, d_o.data_ptr(), fb, cbl, hint,
+                                         d_pts.data_ptr(), d_det.data_ptr(), len(pts),
+                                         d_tris.data_ptr(), len(tris), d_g.data_ptr(), counts,
+                                         zext)
+    torch.cuda.synchronize()
+    assert_same(d_pts.cpu().numpy().view(abi.POINT3_DTYPE), d_det.cpu().numpy(),
+                d_g.cpu().numpy().view(abi.UGRID_DTYPE), counts, zext,
+                z["pts"].view(abi.POINT3_DTYPE), z["detected"], z["gp3"].view(abi.UGRID_DTYPE),
+                z["counts"], z["zext"])
+
+
+def test_wide_band_reruns_the_point_pass(gpu_ctx, monkeypatch):
+    """With the band widened by 1 m some comparison falls inside it: the pass
+    is undone and re-run (counted), and the result is still the reference's."""
+    monkeypatch.setenv("SETSM_VLL_TIN_SUMS", "wideband")
+    inp, pts, tris, oncc, z = mg.tinb_case("tinb_l0")
+    it, fb, cbl, hint = mg.GOLDEN_TINB["tinb_l0"]["call"]
+    det, counts, zext = fresh_out(len(pts))
+    before = vll.load().vll_tin_rerun_count(gpu_ctx._h)
+    gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
+    assert vll.load().vll_tin_rerun_count(gpu_ctx._h) == before + 1
+    assert_same(pts, det, inp.gridpt3, counts, zext, z["pts"].view(abi.POINT3_DTYPE),
+                z["detected"], z["gp3"].view(abi.UGRID_DTYPE), z["counts"], z["zext"])
