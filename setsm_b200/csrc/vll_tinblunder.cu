@@ -10,18 +10,22 @@
 // which of 1 / 3 lands first on a point that was 0 (set_blunder, :9121); the
 // closing pass turns 3 into 1, so the outputs do not depend on the race.
 //
-// GPU: the per-triangle terms in parallel, the FP64 sums by one warp in the
-// reference's triangle order (a sum's rounding depends on its order), the
-// per-point triangle lists by a stable radix sort of (point, triangle), the
-// point pass one thread per point with the same compare-and-swap marking, and
-// the closing pass with atomics (order-free counts, min / max).
+// GPU: the per-triangle terms in parallel (height differences, histogram,
+// per-point triangle counts), the two FP64 sums in parallel with a proven
+// bound on their distance from the reference's sequential sums (the height
+// threshold is then known to lie in a band; a point pass in which some
+// comparison falls inside the band is undone and run again with the sums in
+// the reference's order), the per-point triangle lists by counting and a
+// fill, the point pass one warp per point (lane k takes the point's k-th
+// triangle in triangle order, after a warp sort) with the same
+// compare-and-swap marking, and the closing pass with warp-aggregated atomics
+// (order-free counts, min / max).
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <limits>
 #include <vector>
 
-#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
@@ -49,9 +53,18 @@ __device__ __forceinline__ int64_t grid_index(const TinArgs &a, double x, double
 // statistics of the reference (:9200-9252) feed only an ortho-NCC threshold
 // that it overwrites with the level's constant (:9304-9313), so they are not
 // formed.
-__global__ void tri_terms_kernel(TinArgs a, const vll_point3 *pts, const vll_tri *tris,
-                                 double *dhv, uint32_t *hbin, uint32_t hdiffcount,
-                                 unsigned long long *n_valid, unsigned int *bad) {
+constexpr int kSmemBins = 2048;   // histogram bins kept in shared memory
+
+__global__ void __launch_bounds__(256)
+    tri_terms_kernel(TinArgs a, const vll_point3 *pts, const vll_tri *tris, double *dhv,
+                     uint32_t *hbin, uint32_t hdiffcount, unsigned long long *n_valid,
+                     unsigned int *count, unsigned int *bad) {
+    __shared__ uint32_t sh[kSmemBins];
+    const bool use_sh = hdiffcount <= (uint32_t)kSmemBins;
+    if (use_sh)
+        for (uint32_t i = threadIdx.x; i < hdiffcount; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    unsigned int nv = 0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < a.n_tris;
          t += (int64_t)gridDim.x * blockDim.x) {
         const vll_tri tr = tris[t];
@@ -60,6 +73,7 @@ __global__ void tri_terms_kernel(TinArgs a, const vll_point3 *pts, const vll_tri
         double z[3];
         for (int k = 0; k < 3; ++k) {
             if (v[k] < (uint64_t)a.n_pts) {
+                atomicAdd(count + v[k], 1u);
                 const vll_point3 p = pts[v[k]];
                 z[k] = p.z;
                 // int t_col / t_row and an int index, as the reference
@@ -78,11 +92,23 @@ __global__ void tri_terms_kernel(TinArgs a, const vll_point3 *pts, const vll_tri
             dh[2] = fabs(__dadd_rn(z[1], -z[2]));
             for (int k = 0; k < 3; ++k) {
                 const double f = (double)(uint32_t)dh[k];
-                if (f < (double)hdiffcount) atomicAdd(hbin + (uint32_t)f, 1u);
+                if (f < (double)hdiffcount) {
+                    if (use_sh)
+                        atomicAdd(sh + (uint32_t)f, 1u);
+                    else
+                        atomicAdd(hbin + (uint32_t)f, 1u);
+                }
             }
-            atomicAdd(n_valid, 1ull);
+            ++nv;
         }
         for (int k = 0; k < 3; ++k) dhv[3 * t + k] = dh[k];
+    }
+    nv = __reduce_add_sync(0xffffffffu, nv);
+    if ((threadIdx.x & 31) == 0 && nv) atomicAdd(n_valid, (unsigned long long)nv);
+    if (use_sh) {
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < hdiffcount; i += blockDim.x)
+            if (sh[i]) atomicAdd(hbin + i, sh[i]);
     }
 }
 
@@ -158,21 +184,62 @@ __global__ void __launch_bounds__(512) dh_serial_sum_kernel(int64_t n_vals,
     }
 }
 
-// (point, triangle) pairs in triangle order, 3 per triangle (invalid
-// vertices keyed past the points).
-__global__ void pair_kernel(TinArgs a, const vll_tri *tris, uint32_t *key, int32_t *val,
-                            unsigned int *count) {
+// The per-point triangle lists (the reference's savenode, :9190-9241): each
+// point's slots [start, start + count) take its triangles in arbitrary order
+// (the point pass orders them); a triangle listing a point twice is kept
+// twice, as there.
+__global__ void fill_kernel(TinArgs a, const vll_tri *tris, const int64_t *start,
+                            unsigned int *cursor, int32_t *list) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < a.n_tris;
          t += (int64_t)gridDim.x * blockDim.x) {
         const vll_tri tr = tris[t];
         const uint32_t v[3] = {tr.a, tr.b, tr.c};
-        for (int k = 0; k < 3; ++k) {
-            const bool ok = v[k] < (uint64_t)a.n_pts;
-            key[3 * t + k] = ok ? v[k] : (uint32_t)a.n_pts;
-            val[3 * t + k] = (int32_t)t;
-            if (ok) atomicAdd(count + v[k], 1u);
+        for (int k = 0; k < 3; ++k)
+            if (v[k] < (uint64_t)a.n_pts) list[start[v[k]] + atomicAdd(cursor + v[k], 1u)] = (int32_t)t;
+    }
+}
+
+// Ascending bitonic sort of one value per lane across the warp.
+__device__ __forceinline__ uint32_t warp_sort32(uint32_t v, int lane) {
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            v = keep_min ? min(v, o) : max(v, o);
         }
     }
+    return v;
+}
+
+// Lane k's triangle: the k-th smallest of the point's e list entries (with
+// multiplicity), for k < n_take <= 30; 0xffffffff on the other lanes.
+__device__ uint32_t lane_triangle(const int32_t *list, int64_t st, unsigned int e, int n_take,
+                                  int lane) {
+    uint32_t mine = 0xffffffffu;
+    if (e <= 32) {
+        mine = warp_sort32(lane < (int)e ? (uint32_t)list[st + lane] : 0xffffffffu, lane);
+    } else {
+        // a point of more than 32 triangles: select the smallest n_take by
+        // (triangle, slot) keys, one per round
+        unsigned long long last = 0;
+        for (int k = 0; k < n_take; ++k) {
+            unsigned long long best = ~0ull;
+            for (unsigned int j = lane; j < e; j += 32) {
+                const unsigned long long key =
+                    ((unsigned long long)(uint32_t)list[st + j] << 32) | j;
+                if ((k == 0 || key > last) && key < best) best = key;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long x = __shfl_xor_sync(0xffffffffu, best, o);
+                if (x < best) best = x;
+            }
+            if (lane == k) mine = (uint32_t)(best >> 32);
+            last = best;
+        }
+    }
+    return lane < n_take ? mine : 0xffffffffu;
 }
 
 // set_blunder (:9121-9156): a point that is still 0 takes `val`; the call
@@ -222,40 +289,47 @@ __device__ __forceinline__ bool above_th(double x, const TinArgs &a, unsigned in
     return hi;
 }
 
-// The point pass (:9426-9756).
-__global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
-                             const float *ortho_ncc, const int32_t *sorted_tri,
-                             const int64_t *start, const unsigned int *count, vll_ugrid *gp3,
-                             uint8_t *detected, const uint8_t *flag0, unsigned int *bad,
-                             unsigned int *rerun, int64_t *anchor_node, uint8_t *anchor_val) {
-    for (int64_t index = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; index < a.n_pts;
-         index += (int64_t)gridDim.x * blockDim.x) {
-        if (anchor_node) anchor_node[index] = -1;
+// The point pass (:9426-9756), one warp per point: lane k evaluates the
+// point's k-th triangle (the reference's loop iterations are independent but
+// for the counts, which the warp adds up, and the marks, which are
+// compare-and-swaps either way).
+__global__ void __launch_bounds__(256)
+    point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris, const float *ortho_ncc,
+                 const int32_t *list, const int64_t *start, const unsigned int *count,
+                 vll_ugrid *gp3, uint8_t *detected, const uint8_t *flag0, unsigned int *bad,
+                 unsigned int *rerun, int64_t *anchor_node, uint8_t *anchor_val) {
+    const int lane = threadIdx.x & 31;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t index = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; index < a.n_pts;
+         index += n_warps) {
+        if (anchor_node && lane == 0) anchor_node[index] = -1;
         if (flag0[index] == 1) continue;
         bool pt_is_blunder = false;
-        int count_pos = 0, count_neg = 0, cnt = 0;
-        bool check_neigh = false;
-        const int max_iter = count[index] < (unsigned)kMaxNodes ? (int)count[index] : kMaxNodes;
+        const unsigned int e = count[index];
+        const int max_iter = e < (unsigned)kMaxNodes ? (int)e : kMaxNodes;
         const vll_point3 rp = pts[index];
         const int64_t ref_index = grid_index(a, rp.x, rp.y);
         if (ref_index < 0 || ref_index >= a.n_nodes) {
-            atomicExch(bad, 1u);
+            if (lane == 0) atomicExch(bad, 1u);
             continue;
         }
         const float ref_oncc = ortho_ncc[ref_index];
         if (!a.is_ra && ref_oncc < a.th_ref_ncc && a.L >= 2) pt_is_blunder = true;
         const uint8_t anchor =
             (a.L >= 3 && a.iteration >= 4 && ref_oncc >= 0.95 && a.flag_blunder) ? 1 : 0;
-        if (anchor_node) {
-            anchor_node[index] = ref_index;
-            anchor_val[index] = anchor;
-        } else {
-            gp3[ref_index].anchor_flag = anchor;
+        if (lane == 0) {
+            if (anchor_node) {
+                anchor_node[index] = ref_index;
+                anchor_val[index] = anchor;
+            } else {
+                gp3[ref_index].anchor_flag = anchor;
+            }
         }
-        for (int it = 0; it < max_iter; ++it) {
-            const int64_t tc = sorted_tri[start[index] + it];
-            // triangle 0 is never used here, as in the reference (savenode > 0)
-            if (!(tc < a.n_tris && tc > 0)) continue;
+        const uint32_t tcu = lane_triangle(list, start[index], e, max_iter, lane);
+        bool counted = false, pos = false, neg = false, neigh = false;
+        // triangle 0 is never used here, as in the reference (savenode > 0)
+        if (lane < max_iter && tcu < (uint64_t)a.n_tris && tcu > 0) {
+            const int64_t tc = tcu;
             const vll_tri tr = tris[tc];
             const uint32_t tt[3] = {tr.a, tr.b, tr.c};
             int64_t reference_index = 0, t0 = 0, t1 = 0;
@@ -270,94 +344,99 @@ __global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                     t1 = tt[kk];
                 }
             }
-            if (!(reference_index < a.n_pts && t0 < a.n_pts && t1 < a.n_pts)) continue;
-            const vll_point3 p0 = pts[reference_index], p1 = pts[t0], p2 = pts[t1];
-            const double angle = normal_angle(p0, p1, p2);
-            const double dh1 = __dadd_rn(p0.z, -p1.z), dh2 = __dadd_rn(p0.z, -p2.z),
-                         dh3 = __dadd_rn(p1.z, -p2.z);
-            if (dh1 >= 0 && dh2 >= 0 && angle > 30) ++count_pos;
-            if (dh1 < 0 && dh2 < 0 && angle > 30) ++count_neg;
-            bool check_match = false;
-            if (a.L > 1)
-                check_match = true;
-            else if (a.L == 1)
-                check_match = a.iteration == 1 && a.count_bl <= 5;
-            else if (a.L == 0) {
-                if (a.iteration == 1 && a.count_bl <= 5)
+            if (reference_index < a.n_pts && t0 < a.n_pts && t1 < a.n_pts) {
+                counted = true;
+                const vll_point3 p0 = pts[reference_index], p1 = pts[t0], p2 = pts[t1];
+                const double angle = normal_angle(p0, p1, p2);
+                const double dh1 = __dadd_rn(p0.z, -p1.z), dh2 = __dadd_rn(p0.z, -p2.z),
+                             dh3 = __dadd_rn(p1.z, -p2.z);
+                if (dh1 >= 0 && dh2 >= 0 && angle > 30) pos = true;
+                if (dh1 < 0 && dh2 < 0 && angle > 30) neg = true;
+                bool check_match = false;
+                if (a.L > 1)
                     check_match = true;
-                else if (a.iteration == 2 && a.count_bl <= 5)
-                    check_match = false;
-            }
-            if (check_match) {
-                const double d1 = __dadd_rn(fabs(dh1), -fabs(dh2));
-                const double d2 = __dadd_rn(fabs(dh1), -fabs(dh3));
-                const double d3 = __dadd_rn(fabs(dh2), -fabs(dh3));
-                if (above_th(fabs(d1), a, rerun) || above_th(fabs(d2), a, rerun) ||
-                    above_th(fabs(d3), a, rerun)) {
-                    const int64_t order[3] = {reference_index, t0, t1};
-                    const double h[3] = {p0.z, p1.z, p2.z};
-                    const int64_t Index[3] = {grid_index(a, p0.x, p0.y), grid_index(a, p1.x, p1.y),
-                                              grid_index(a, p2.x, p2.y)};
-                    check_neigh = true;
-                    int mx, mn, md;
-                    if (h[0] > h[1]) {
-                        if (h[0] > h[2]) {
-                            mx = 0;
-                            if (h[1] > h[2]) {
-                                mn = 2;
-                                md = 1;
-                            } else {
-                                mn = 1;
-                                md = 2;
-                            }
-                        } else {
-                            mx = 2;
-                            mn = 1;
-                            md = 0;
-                        }
-                    } else {
-                        if (h[1] > h[2]) {
-                            mx = 1;
+                else if (a.L == 1)
+                    check_match = a.iteration == 1 && a.count_bl <= 5;
+                else if (a.L == 0) {
+                    if (a.iteration == 1 && a.count_bl <= 5)
+                        check_match = true;
+                    else if (a.iteration == 2 && a.count_bl <= 5)
+                        check_match = false;
+                }
+                if (check_match) {
+                    const double d1 = __dadd_rn(fabs(dh1), -fabs(dh2));
+                    const double d2 = __dadd_rn(fabs(dh1), -fabs(dh3));
+                    const double d3 = __dadd_rn(fabs(dh2), -fabs(dh3));
+                    if (above_th(fabs(d1), a, rerun) || above_th(fabs(d2), a, rerun) ||
+                        above_th(fabs(d3), a, rerun)) {
+                        const int64_t order[3] = {reference_index, t0, t1};
+                        const double h[3] = {p0.z, p1.z, p2.z};
+                        const int64_t Index[3] = {grid_index(a, p0.x, p0.y), grid_index(a, p1.x, p1.y),
+                                                  grid_index(a, p2.x, p2.y)};
+                        neigh = true;
+                        int mx, mn, md;
+                        if (h[0] > h[1]) {
                             if (h[0] > h[2]) {
-                                mn = 2;
+                                mx = 0;
+                                if (h[1] > h[2]) {
+                                    mn = 2;
+                                    md = 1;
+                                } else {
+                                    mn = 1;
+                                    md = 2;
+                                }
+                            } else {
+                                mx = 2;
+                                mn = 1;
                                 md = 0;
+                            }
+                        } else {
+                            if (h[1] > h[2]) {
+                                mx = 1;
+                                if (h[0] > h[2]) {
+                                    mn = 2;
+                                    md = 0;
+                                } else {
+                                    mn = 0;
+                                    md = 2;
+                                }
                             } else {
+                                mx = 2;
+                                md = 1;
                                 mn = 0;
-                                md = 2;
                             }
-                        } else {
-                            mx = 2;
-                            md = 1;
-                            mn = 0;
                         }
-                    }
-                    const double h1 = __dadd_rn(h[md], -h[mn]);
-                    const double h2 = __dadd_rn(h[mx], -h[md]);
-                    const double dh = __dadd_rn(h1, -h2);
-                    int64_t bn = -1;
-                    int pick = -1;
-                    if (dh > 0 && above_th(dh, a, rerun))
-                        pick = mn;
-                    else if (dh < 0 && above_th(fabs(dh), a, rerun))
-                        pick = mx;
-                    if (pick >= 0) {
-                        if (a.is_ra) {
-                            bn = order[pick];
-                        } else {
-                            const int64_t gi = Index[pick];
-                            if (gi < 0 || gi >= a.n_nodes) {
-                                atomicExch(bad, 1u);
+                        const double h1 = __dadd_rn(h[md], -h[mn]);
+                        const double h2 = __dadd_rn(h[mx], -h[md]);
+                        const double dh = __dadd_rn(h1, -h2);
+                        int64_t bn = -1;
+                        int pick = -1;
+                        if (dh > 0 && above_th(dh, a, rerun))
+                            pick = mn;
+                        else if (dh < 0 && above_th(fabs(dh), a, rerun))
+                            pick = mx;
+                        if (pick >= 0) {
+                            if (a.is_ra) {
+                                bn = order[pick];
                             } else {
-                                const double th = a.flag_blunder ? a.ortho_ncc_th : 100.0;
-                                if (ortho_ncc[gi] < th) bn = order[pick];
+                                const int64_t gi = Index[pick];
+                                if (gi < 0 || gi >= a.n_nodes) {
+                                    atomicExch(bad, 1u);
+                                } else {
+                                    const double th = a.flag_blunder ? a.ortho_ncc_th : 100.0;
+                                    if (ortho_ncc[gi] < th) bn = order[pick];
+                                }
                             }
                         }
+                        if (bn >= 0) set_blunder(pts, bn, 3, detected);
                     }
-                    if (bn >= 0) set_blunder(pts, bn, 3, detected);
                 }
             }
-            ++cnt;
         }
+        const int cnt = __popc(__ballot_sync(0xffffffffu, counted));
+        const int count_pos = __popc(__ballot_sync(0xffffffffu, pos));
+        const int count_neg = __popc(__ballot_sync(0xffffffffu, neg));
+        const bool check_neigh = __ballot_sync(0xffffffffu, neigh) != 0;
         if (a.is_ra) {
             if (check_neigh && !a.flag_blunder) pt_is_blunder = true;
             if ((count_pos >= (int)__dadd_rn(__dmul_rn((double)cnt, 0.7), 0.5) ||
@@ -395,7 +474,7 @@ __global__ void point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                 }
             }
         }
-        if (pt_is_blunder) set_blunder(pts, index, 1, detected);
+        if (pt_is_blunder && lane == 0) set_blunder(pts, index, 1, detected);
     }
 }
 
@@ -409,18 +488,36 @@ __device__ __forceinline__ unsigned long long dkey(double v) {
 __global__ void close_kernel(int64_t n_pts, vll_point3 *pts, unsigned long long *cnt,
                              unsigned long long *zkey, const unsigned int *rerun) {
     if (*rerun) return;   // the point pass runs again first
+    unsigned long long kept = 0, blunders = 0, zmin = ~0ull, zmax = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pts;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint8_t f = pts[i].flag;
         if (f == 1) {
-            atomicAdd(cnt + 1, 1ull);
+            ++blunders;
         } else if (f == 3) {
-            atomicAdd(cnt + 1, 1ull);
+            ++blunders;
             pts[i].flag = 1;
         } else {
-            atomicAdd(cnt, 1ull);
-            atomicMin(zkey, dkey(pts[i].z));
-            atomicMax(zkey + 1, dkey(pts[i].z));
+            ++kept;
+            const unsigned long long k = dkey(pts[i].z);
+            zmin = k < zmin ? k : zmin;
+            zmax = k > zmax ? k : zmax;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        kept += __shfl_xor_sync(0xffffffffu, kept, o);
+        blunders += __shfl_xor_sync(0xffffffffu, blunders, o);
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, zmin, o);
+        const unsigned long long b = __shfl_xor_sync(0xffffffffu, zmax, o);
+        zmin = a < zmin ? a : zmin;
+        zmax = b > zmax ? b : zmax;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (blunders) atomicAdd(cnt + 1, blunders);
+        if (kept) {
+            atomicAdd(cnt, kept);
+            atomicMin(zkey, zmin);
+            atomicMax(zkey + 1, zmax);
         }
     }
 }
@@ -454,16 +551,6 @@ unsigned blocks_for(int64_t n, int threads) {
 }
 
 size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
-
-size_t sort_tmp_bytes(int64_t n_pairs) {
-    size_t t = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t, (const uint32_t *)nullptr, (uint32_t *)nullptr,
-                                    (const int32_t *)nullptr, (int32_t *)nullptr, (int)n_pairs);
-    size_t u = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, u, (const unsigned int *)nullptr, (int64_t *)nullptr,
-                                  (int)1);
-    return t > u ? t : u;
-}
 
 size_t scan_tmp_bytes(int64_t n) {
     size_t u = 0;
@@ -577,10 +664,9 @@ void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], l
 
 size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount) {
     const int64_t np = 3 * n_tris;
-    size_t t = sort_tmp_bytes(np > 0 ? np : 1), u = scan_tmp_bytes(n_pts + 1);
-    return al(t > u ? t : u) + al(3 * n_tris * sizeof(double)) + al((hdiffcount + 1) * 4) +
-           al(64) + 4 * al(np * 4) + al((n_pts + 1) * 4) + al((n_pts + 1) * 8) + 2 * al(n_pts) +
-           al(128) + al(n_pts * 8) + al(n_pts);
+    return al(scan_tmp_bytes(n_pts + 1)) + al(3 * n_tris * sizeof(double)) +
+           al((hdiffcount + 1) * 4) + al((np > 0 ? np : 1) * 4) + al(2 * (n_pts + 1) * 4) +
+           al((n_pts + 1) * 8) + 2 * al(n_pts) + al(128) + al(n_pts * 8) + al(n_pts);
 }
 
 namespace {
@@ -602,8 +688,7 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                             uint32_t hdiffcount, int sums_mode, bool anchor_list,
                             void *scratch, size_t bytes, TinOutput *out, cudaStream_t s) {
     const int64_t np = 3 * a.n_tris;
-    size_t tmp_b = sort_tmp_bytes(np > 0 ? np : 1), u = scan_tmp_bytes(a.n_pts + 1);
-    if (u > tmp_b) tmp_b = u;
+    size_t tmp_b = scan_tmp_bytes(a.n_pts + 1);
     char *p = (char *)scratch;
     auto take = [&](size_t b) {
         void *r = p;
@@ -613,18 +698,16 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     void *tmp = take(tmp_b);
     double *dhv = (double *)take(3 * a.n_tris * sizeof(double));
     uint32_t *hbin = (uint32_t *)take((hdiffcount + 1) * 4);
-    double *sums = (double *)take(64);
-    uint32_t *key = (uint32_t *)take(np * 4);
-    uint32_t *skey = (uint32_t *)take(np * 4);
-    int32_t *val = (int32_t *)take(np * 4);
-    int32_t *sval = (int32_t *)take(np * 4);
-    unsigned int *count = (unsigned int *)take((a.n_pts + 1) * 4);
+    int32_t *list = (int32_t *)take((np > 0 ? np : 1) * 4);
+    unsigned int *count = (unsigned int *)take(2 * (a.n_pts + 1) * 4);
+    unsigned int *cursor = count + a.n_pts + 1;
     int64_t *start = (int64_t *)take((a.n_pts + 1) * 8);
     uint8_t *flag0 = (uint8_t *)take(a.n_pts);
     uint8_t *det0 = (uint8_t *)take(a.n_pts);
     // [0..1] counts, [2..3] z keys, [4] bad input, [5] valid triangles,
-    // [6] re-run due
+    // [6] re-run due, [8..9] the two sums (doubles)
     unsigned long long *misc = (unsigned long long *)take(128);
+    double *sums = reinterpret_cast<double *>(misc + 8);
     int64_t *anchor_node = (int64_t *)take(a.n_pts * 8);
     uint8_t *anchor_val = (uint8_t *)take(a.n_pts);
     if (!anchor_list) anchor_node = nullptr, anchor_val = nullptr;
@@ -634,32 +717,29 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     const bool exact = sums_mode == kTinSumsExact;
     cudaError_t e;
     if ((e = cudaMemsetAsync(hbin, 0, (hdiffcount + 1) * 4, s))) return e;
-    if ((e = cudaMemsetAsync(count, 0, (a.n_pts + 1) * 4, s))) return e;
+    if ((e = cudaMemsetAsync(count, 0, 2 * (a.n_pts + 1) * 4, s))) return e;
     if ((e = cudaMemsetAsync(misc, 0, 128, s))) return e;
-    if ((e = cudaMemsetAsync(sums, 0, 64, s))) return e;
     if (a.n_tris > 0) {
-        tri_terms_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, pts, tris, dhv, hbin,
-                                                                   hdiffcount, misc + 5, bad);
+        int64_t tb = (a.n_tris + 255) / 256;
+        if (tb > 148 * 4) tb = 148 * 4;   // bounds the per-block histogram flushes
+        tri_terms_kernel<<<(unsigned)tb, 256, 0, s>>>(a, pts, tris, dhv, hbin, hdiffcount,
+                                                      misc + 5, count, bad);
         if (exact)
             dh_serial_sum_kernel<<<1, 512, 0, s>>>(np, dhv, sums);
         else
             dh_psum_kernel<<<blocks_for(np, 256), 256, 0, s>>>(np, dhv, sums);
-        pair_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, tris, key, val, count);
         if ((e = cudaGetLastError())) return e;
-        int end_bit = 1;
-        while (end_bit < 32 && ((uint64_t)1 << end_bit) <= (uint64_t)a.n_pts) ++end_bit;
-        if ((e = cub::DeviceRadixSort::SortPairs(tmp, tmp_b, key, skey, val, sval, (int)np, 0,
-                                                 end_bit, s)))
-            return e;
     }
     if ((e = cub::DeviceScan::ExclusiveSum(tmp, tmp_b, count, start, (int)(a.n_pts + 1), s)))
         return e;
+    if (a.n_tris > 0) {
+        fill_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, tris, start, cursor, list);
+        if ((e = cudaGetLastError())) return e;
+    }
     // the sums, the histogram, the valid count and the input check back for
     // the thresholds
-    double hs[2];
     std::vector<uint32_t> hb(hdiffcount + 1);
-    unsigned long long hm[6];
-    if ((e = cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, s))) return e;
+    unsigned long long hm[10];
     if ((e = cudaMemcpyAsync(hb.data(), hbin, (hdiffcount + 1) * 4, cudaMemcpyDeviceToHost, s)))
         return e;
     if ((e = cudaMemcpyAsync(hm, misc, sizeof(hm), cudaMemcpyDeviceToHost, s))) return e;
@@ -668,14 +748,11 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         out->bad_input = 1;
         return cudaSuccess;
     }
+    double hs[2];
+    memcpy(hs, hm + 8, sizeof(hs));
     const long dh_count = (long)(3 * hm[5]);
     double sd[2], sd2[2];
     const bool band = !exact && std::isfinite(hs[0]) && std::isfinite(hs[1]);
-    if (band) {
-        sum_band(hs[0], np, sd);
-        sum_band(hs[1], np, sd2);
-    }
-    TinThresholds th;
     auto exact_sums = [&]() -> cudaError_t {
         cudaError_t e2;
         if (a.n_tris > 0) {
@@ -688,11 +765,16 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         sd2[0] = sd2[1] = hs[1];
         return cudaSuccess;
     };
-    if (!band && !exact && (e = exact_sums())) return e;
-    if (exact) {
+    if (band) {
+        sum_band(hs[0], np, sd);
+        sum_band(hs[1], np, sd2);
+    } else if (exact) {
         sd[0] = sd[1] = hs[0];
         sd2[0] = sd2[1] = hs[1];
+    } else if ((e = exact_sums())) {
+        return e;
     }
+    TinThresholds th;
     tin_thresholds(a, sd, sd2, dh_count, hb.data(), hdiffcount, &th);
     if (band && sums_mode == kTinSumsWideBand) {
         th.height_th -= 1.0;
@@ -703,14 +785,20 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     a.ortho_ncc_th = th.ortho_ncc_th;
     a.th_ref_ncc = th.th_ref_ncc;
     const unsigned long long zinit[2] = {~0ull, 0ull};
+    const unsigned pblocks = blocks_for(a.n_pts * 32, 256);
+    auto point_pass = [&]() -> cudaError_t {
+        point_kernel<<<pblocks, 256, 0, s>>>(a, pts, tris, ortho_ncc, list, start, count, gp3,
+                                             detected, flag0, bad, rerun, anchor_node,
+                                             anchor_val);
+        cudaError_t e2;
+        if ((e2 = cudaMemcpyAsync(misc + 2, zinit, 16, cudaMemcpyHostToDevice, s))) return e2;
+        close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2,
+                                                             rerun);
+        return cudaGetLastError();
+    };
     copy_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0, detected,
                                                                det0);
-    point_kernel<<<blocks_for(a.n_pts, 128), 128, 0, s>>>(a, pts, tris, ortho_ncc, sval, start,
-                                                         count, gp3, detected, flag0, bad, rerun,
-                                                         anchor_node, anchor_val);
-    if ((e = cudaMemcpyAsync(misc + 2, zinit, 16, cudaMemcpyHostToDevice, s))) return e;
-    close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2, rerun);
-    if ((e = cudaGetLastError())) return e;
+    if ((e = point_pass())) return e;
     unsigned long long m[7];
     if ((e = cudaMemcpyAsync(m, misc, sizeof(m), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
@@ -725,14 +813,8 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         if ((e = exact_sums())) return e;
         tin_thresholds(a, sd, sd2, dh_count, hb.data(), hdiffcount, &th);
         a.height_th = a.height_th_hi = th.height_th;
-        if ((e = cudaMemsetAsync(misc, 0, 128, s))) return e;
-        point_kernel<<<blocks_for(a.n_pts, 128), 128, 0, s>>>(a, pts, tris, ortho_ncc, sval,
-                                                             start, count, gp3, detected, flag0,
-                                                             bad, rerun, anchor_node, anchor_val);
-        if ((e = cudaMemcpyAsync(misc + 2, zinit, 16, cudaMemcpyHostToDevice, s))) return e;
-        close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2,
-                                                             rerun);
-        if ((e = cudaGetLastError())) return e;
+        if ((e = cudaMemsetAsync(misc, 0, 64, s))) return e;
+        if ((e = point_pass())) return e;
         if ((e = cudaMemcpyAsync(m, misc, sizeof(m), cudaMemcpyDeviceToHost, s))) return e;
         if ((e = cudaStreamSynchronize(s))) return e;
     }

@@ -134,3 +134,41 @@ def test_wide_band_reruns_the_point_pass(gpu_ctx, monkeypatch):
     assert vll.load().vll_tin_rerun_count(gpu_ctx._h) == before + 1
     assert_same(pts, det, inp.gridpt3, counts, zext, z["pts"].view(abi.POINT3_DTYPE),
                 z["detected"], z["gp3"].view(abi.UGRID_DTYPE), z["counts"], z["zext"])
+
+
+@pytest.mark.skipif(not refpy.available(), reason="reference build not available")
+@pytest.mark.parametrize("seed", [61, 62])
+def test_crowded_points_and_repeated_vertices(gpu_ctx, seed):
+    """Triangle lists beyond the Delaunay ones: two points in more than 32
+    triangles (the warp's selection of the first 30 in triangle order),
+    triangles listing a point twice (kept twice, as the reference's lists do)
+    and a vertex past the points.  A triangle (a, a, b) has a zero normal
+    when point b evaluates it, where the reference's SetNormalAngle leaves its
+    angle unset (SubFunctions.cpp:2999-3007), so b is a point the pass skips
+    (flag 1), and no vertex is point 0 (the unset third index)."""
+    import copy
+    inp, pts, tris, oncc = cases.make_tin_blunder_case(seed=seed, size=768, nodes=40, res=7.0)
+    rng = np.random.default_rng(seed)
+    n = len(pts)
+    extra = []
+    for hub in (3, n // 2):
+        others = np.setdiff1d(np.arange(1, n), [hub])
+        for _ in range(45):
+            j, k = rng.choice(others, 2, replace=False)
+            extra.append((hub, j, k) if rng.random() < 0.5 else (j, hub, k))
+    skipped = np.flatnonzero(pts["flag"] == 1)
+    active = np.setdiff1d(np.flatnonzero(pts["flag"] != 1), [0])
+    for _ in range(12):
+        extra.append((rng.choice(active),) * 2 + (rng.choice(skipped[skipped > 0]),))
+    extra.append((1, 2, n + 5))
+    ext = np.zeros(len(extra), dtype=tris.dtype)
+    ext["a"], ext["b"], ext["c"] = np.array(extra).T
+    mixed = np.concatenate([tris[:len(tris) // 2], ext, tris[len(tris) // 2:]])
+    ref = copy.copy(inp)
+    ref.gridpt3 = inp.gridpt3.copy()
+    r_pts, (r_det, r_counts, r_zext) = pts.copy(), fresh_out(n)
+    refpy.blunder_detection_tin(ref, 1, oncc.copy(), True, 1, 60.0, r_pts, r_det, mixed.copy(),
+                                r_counts, r_zext)
+    det, counts, zext = fresh_out(n)
+    gpu_ctx.blunder_detection_tin(inp, 1, oncc, True, 1, 60.0, pts, det, mixed, counts, zext)
+    assert_same(pts, det, inp.gridpt3, counts, zext, r_pts, r_det, ref.gridpt3, r_counts, r_zext)
