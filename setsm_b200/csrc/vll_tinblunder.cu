@@ -280,6 +280,24 @@ __device__ double normal_angle(const vll_point3 &p0, const vll_point3 &p1, const
     return angle;
 }
 
+// normal_angle(p0, p1, p2) > 30, the only use the point pass makes of the
+// angle: CUDA's acos (within a few ulp, the CUDA Math API's bound) decides it
+// unless the angle lies within 1e-9 degrees of 30 (an ulp of 30 is 3.6e-15),
+// where the correctly rounded angle does.
+__device__ bool angle_above_30(const vll_point3 &p0, const vll_point3 &p1, const vll_point3 &p2) {
+    const double ux = __dadd_rn(p1.x, -p0.x), uy = __dadd_rn(p1.y, -p0.y), uz = __dadd_rn(p1.z, -p0.z);
+    const double vx = __dadd_rn(p2.x, -p0.x), vy = __dadd_rn(p2.y, -p0.y), vz = __dadd_rn(p2.z, -p0.z);
+    const double nx = __dadd_rn(__dmul_rn(uy, vz), -__dmul_rn(vy, uz));
+    const double ny = -__dadd_rn(__dmul_rn(ux, vz), -__dmul_rn(vx, uz));
+    const double nz = __dadd_rn(__dmul_rn(ux, vy), -__dmul_rn(vx, uy));
+    const double norm =
+        sqrt(__dadd_rn(__dadd_rn(__dmul_rn(nx, nx), __dmul_rn(ny, ny)), __dmul_rn(nz, nz)));
+    if (norm == 0) return false;   // the angle normal_angle gives, 0
+    const double fast = __ddiv_rn(__dmul_rn(acos(__ddiv_rn(fabs(nz), norm)), 180.0), kPi);
+    if (!(fabs(__dadd_rn(fast, -30.0)) <= 1e-9)) return fast > 30;   // NaN: false either way
+    return normal_angle(p0, p1, p2) > 30;
+}
+
 // x > the reference's height threshold, which lies in [height_th,
 // height_th_hi]: when the two ends disagree the answer is not known and the
 // pass is marked for an exact re-run.
@@ -347,11 +365,14 @@ __global__ void __launch_bounds__(256)
             if (reference_index < a.n_pts && t0 < a.n_pts && t1 < a.n_pts) {
                 counted = true;
                 const vll_point3 p0 = pts[reference_index], p1 = pts[t0], p2 = pts[t1];
-                const double angle = normal_angle(p0, p1, p2);
                 const double dh1 = __dadd_rn(p0.z, -p1.z), dh2 = __dadd_rn(p0.z, -p2.z),
                              dh3 = __dadd_rn(p1.z, -p2.z);
-                if (dh1 >= 0 && dh2 >= 0 && angle > 30) pos = true;
-                if (dh1 < 0 && dh2 < 0 && angle > 30) neg = true;
+                // the angle only counts when both differences have one sign
+                if ((dh1 >= 0 && dh2 >= 0) || (dh1 < 0 && dh2 < 0)) {
+                    const bool steep = angle_above_30(p0, p1, p2);
+                    pos = dh1 >= 0 && dh2 >= 0 && steep;
+                    neg = dh1 < 0 && dh2 < 0 && steep;
+                }
                 bool check_match = false;
                 if (a.L > 1)
                     check_match = true;
@@ -516,7 +537,7 @@ __global__ void close_kernel(int64_t n_pts, vll_point3 *pts, unsigned long long 
         if (blunders) atomicAdd(cnt + 1, blunders);
         if (kept) {
             atomicAdd(cnt, kept);
-            atomicMin(zkey, zmin);
+            atomicMax(zkey, ~zmin);   // the minimum as the maximum complement: 0 starts both
             atomicMax(zkey + 1, zmax);
         }
     }
@@ -665,8 +686,9 @@ void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], l
 size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount) {
     const int64_t np = 3 * n_tris;
     return al(scan_tmp_bytes(n_pts + 1)) + al(3 * n_tris * sizeof(double)) +
-           al((hdiffcount + 1) * 4) + al((np > 0 ? np : 1) * 4) + al(2 * (n_pts + 1) * 4) +
-           al((n_pts + 1) * 8) + 2 * al(n_pts) + al(128) + al(n_pts * 8) + al(n_pts);
+           al(128 + (hdiffcount + 1) * 4) + al((np > 0 ? np : 1) * 4) +
+           al(2 * (n_pts + 1) * 4) + al((n_pts + 1) * 8) + 2 * al(n_pts) + al(n_pts * 8) +
+           al(n_pts);
 }
 
 namespace {
@@ -697,17 +719,19 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     };
     void *tmp = take(tmp_b);
     double *dhv = (double *)take(3 * a.n_tris * sizeof(double));
-    uint32_t *hbin = (uint32_t *)take((hdiffcount + 1) * 4);
+    // [0..1] counts, [2] complement of the minimum z key, [3] maximum z key,
+    // [4] bad input, [5] valid triangles, [6] re-run due, [8..9] the two sums
+    // (doubles); the histogram follows, so one copy brings both back
+    const size_t misc_b = 128 + (hdiffcount + 1) * 4;
+    unsigned long long *misc = (unsigned long long *)take(misc_b);
+    double *sums = reinterpret_cast<double *>(misc + 8);
+    uint32_t *hbin = reinterpret_cast<uint32_t *>(misc + 16);
     int32_t *list = (int32_t *)take((np > 0 ? np : 1) * 4);
     unsigned int *count = (unsigned int *)take(2 * (a.n_pts + 1) * 4);
     unsigned int *cursor = count + a.n_pts + 1;
     int64_t *start = (int64_t *)take((a.n_pts + 1) * 8);
     uint8_t *flag0 = (uint8_t *)take(a.n_pts);
     uint8_t *det0 = (uint8_t *)take(a.n_pts);
-    // [0..1] counts, [2..3] z keys, [4] bad input, [5] valid triangles,
-    // [6] re-run due, [8..9] the two sums (doubles)
-    unsigned long long *misc = (unsigned long long *)take(128);
-    double *sums = reinterpret_cast<double *>(misc + 8);
     int64_t *anchor_node = (int64_t *)take(a.n_pts * 8);
     uint8_t *anchor_val = (uint8_t *)take(a.n_pts);
     if (!anchor_list) anchor_node = nullptr, anchor_val = nullptr;
@@ -716,9 +740,8 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     unsigned int *rerun = reinterpret_cast<unsigned int *>(misc + 6);
     const bool exact = sums_mode == kTinSumsExact;
     cudaError_t e;
-    if ((e = cudaMemsetAsync(hbin, 0, (hdiffcount + 1) * 4, s))) return e;
+    if ((e = cudaMemsetAsync(misc, 0, misc_b, s))) return e;
     if ((e = cudaMemsetAsync(count, 0, 2 * (a.n_pts + 1) * 4, s))) return e;
-    if ((e = cudaMemsetAsync(misc, 0, 128, s))) return e;
     if (a.n_tris > 0) {
         int64_t tb = (a.n_tris + 255) / 256;
         if (tb > 148 * 4) tb = 148 * 4;   // bounds the per-block histogram flushes
@@ -738,12 +761,11 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     }
     // the sums, the histogram, the valid count and the input check back for
     // the thresholds
-    std::vector<uint32_t> hb(hdiffcount + 1);
-    unsigned long long hm[10];
-    if ((e = cudaMemcpyAsync(hb.data(), hbin, (hdiffcount + 1) * 4, cudaMemcpyDeviceToHost, s)))
-        return e;
-    if ((e = cudaMemcpyAsync(hm, misc, sizeof(hm), cudaMemcpyDeviceToHost, s))) return e;
+    std::vector<unsigned long long> host_misc((misc_b + 7) / 8);
+    if ((e = cudaMemcpyAsync(host_misc.data(), misc, misc_b, cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
+    const unsigned long long *hm = host_misc.data();
+    const uint32_t *hb = reinterpret_cast<const uint32_t *>(hm + 16);
     if (hm[4]) {
         out->bad_input = 1;
         return cudaSuccess;
@@ -775,7 +797,7 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         return e;
     }
     TinThresholds th;
-    tin_thresholds(a, sd, sd2, dh_count, hb.data(), hdiffcount, &th);
+    tin_thresholds(a, sd, sd2, dh_count, hb, hdiffcount, &th);
     if (band && sums_mode == kTinSumsWideBand) {
         th.height_th -= 1.0;
         th.height_th_hi += 1.0;
@@ -784,14 +806,11 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     a.height_th_hi = th.height_th_hi;
     a.ortho_ncc_th = th.ortho_ncc_th;
     a.th_ref_ncc = th.th_ref_ncc;
-    const unsigned long long zinit[2] = {~0ull, 0ull};
     const unsigned pblocks = blocks_for(a.n_pts * 32, 256);
     auto point_pass = [&]() -> cudaError_t {
         point_kernel<<<pblocks, 256, 0, s>>>(a, pts, tris, ortho_ncc, list, start, count, gp3,
                                              detected, flag0, bad, rerun, anchor_node,
                                              anchor_val);
-        cudaError_t e2;
-        if ((e2 = cudaMemcpyAsync(misc + 2, zinit, 16, cudaMemcpyHostToDevice, s))) return e2;
         close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2,
                                                              rerun);
         return cudaGetLastError();
@@ -811,7 +830,7 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                                                                       detected, det0);
         if ((e = cudaGetLastError())) return e;
         if ((e = exact_sums())) return e;
-        tin_thresholds(a, sd, sd2, dh_count, hb.data(), hdiffcount, &th);
+        tin_thresholds(a, sd, sd2, dh_count, hb, hdiffcount, &th);
         a.height_th = a.height_th_hi = th.height_th;
         if ((e = cudaMemsetAsync(misc, 0, 64, s))) return e;
         if ((e = point_pass())) return e;
@@ -823,7 +842,7 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     out->count[1] = (int64_t)m[1];
     out->has_z = m[0] > 0;
     for (int k = 0; k < 2; ++k) {
-        const unsigned long long b = m[2 + k];
+        const unsigned long long b = k == 0 ? ~m[2] : m[3];
         const unsigned long long bits = (b >> 63) ? (b & 0x7fffffffffffffffull) : ~b;
         double v;
         memcpy(&v, &bits, 8);
