@@ -42,15 +42,15 @@ __device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : 
 __device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }
 
 // One cell's samples (InterpolatePatch of both planes of both images at the
-// plane height), or false when the cell is outside the triangle or a window
-// corner leaves an image.  setsm_code.cpp:8331-8451.
-__device__ bool ortho_cell(const DevLevel &P, const double2 *__restrict__ lonlat, int ti,
-                           const P3 &T1, const P3 &T2, const P3 &T3, bool plane_ok, double A,
-                           double B, double C, double D, int64_t row, int64_t col, double v[4]) {
+// plane height) are cell_sample's, for a cell that cell_inside accepts;
+// setsm_code.cpp:8331-8451.
+// Whether the cell lies in the triangle: the three edge tests (D3DPOINT
+// differences; z unused, so the answer is the same at every height).
+__device__ bool cell_inside(const DevLevel &P, const P3 &T1, const P3 &T2, const P3 &T3,
+                            int64_t row, int64_t col) {
     const double gs = P.grid_res;
     const double cx = __dadd_rn(__dmul_rn((double)col, gs), P.boundary[0]);
     const double cy = __dadd_rn(__dmul_rn((double)row, gs), P.boundary[1]);
-    // Sum of the three edge tests (D3DPOINT differences, z unused)
     int sum = 3;
     if (__dadd_rn(__dmul_rn(__dadd_rn(T2.x, -T1.x), __dadd_rn(cy, -T1.y)),
                   -__dmul_rn(__dadd_rn(T2.y, -T1.y), __dadd_rn(cx, -T1.x))) <= 0)
@@ -61,7 +61,18 @@ __device__ bool ortho_cell(const DevLevel &P, const double2 *__restrict__ lonlat
     if (__dadd_rn(__dmul_rn(__dadd_rn(T1.x, -T3.x), __dadd_rn(cy, -T3.y)),
                   -__dmul_rn(__dadd_rn(T1.y, -T3.y), __dadd_rn(cx, -T3.x))) <= 0)
         --sum;
-    if (!(sum == 0 || sum == 3) || !plane_ok) return false;
+    return sum == 0 || sum == 3;
+}
+
+// The samples of a cell inside the triangle at the plane's height, or false
+// when the plane is degenerate or a window corner leaves an image.
+__device__ bool cell_sample(const DevLevel &P, const double2 *__restrict__ lonlat, int ti,
+                            bool plane_ok, double A, double B, double C, double D, int64_t row,
+                            int64_t col, double v[4]) {
+    if (!plane_ok) return false;
+    const double gs = P.grid_res;
+    const double cx = __dadd_rn(__dmul_rn((double)col, gs), P.boundary[0]);
+    const double cy = __dadd_rn(__dmul_rn((double)row, gs), P.boundary[1]);
     // Z = -1.0 * ((A x) + (B y) + D) / C
     const double z = __ddiv_rn(-__dadd_rn(__dadd_rn(__dmul_rn(A, cx), __dmul_rn(B, cy)), D), C);
     // the cell's longitude / latitude: from the grid-wide table when given
@@ -98,10 +109,25 @@ struct SearchOut {
     int selected;
 };
 
+// Per-warp shared staging.  The triangle's bounding box and which of its
+// cells lie inside do not depend on the swept height, so the inside cells are
+// listed once per triangle; when at most kCellCap are inside, each height
+// projects only those, 32 per step, and keeps their samples for both of
+// Correlate's passes.  Otherwise every box cell is tested per height and the
+// second pass recomputes its samples.  Either way the sums read the samples
+// back in cell order.
+constexpr int kCellCap = 256;
+struct CellStage {
+    double2 v[2 * kCellCap];        // item i: {img ref, img tgt}, {mag ref, mag tgt}
+    unsigned int valid[kCellCap / 32];
+    int32_t cell[kCellCap];         // the box's cells inside the triangle, in cell order
+};
+
 // VerticalLineLocus_Ortho for one triangle, by one warp (all lanes return
-// the same result).
+// the same result); st: the warp's staging.
 __device__ SearchOut ortho_search(const DevLevel &P, const double2 *__restrict__ lonlat,
-                                  double mpp, P3 r1, P3 r2, P3 tg, int64_t target_index) {
+                                  double mpp, P3 r1, P3 r2, P3 tg, int64_t target_index,
+                                  CellStage &st) {
     const int lane = threadIdx.x & 31;
     SearchOut o{-9999.0, 0.0, 0};
     double f_ncc = -1.0;
@@ -117,24 +143,41 @@ __device__ SearchOut ortho_search(const DevLevel &P, const double2 *__restrict__
     const double min_th_sncc = P.L < 4 ? 0.5 : 0.2;
     const double gs = P.grid_res;
     const int gw = (int)P.grid_w, gh = (int)P.grid_h;
+    // the bounding box of the cells (the reference recomputes it per height
+    // from the same x, y)
+    const double mn0 = dmin(dmin(r1.x, r2.x), tg.x), mn1 = dmin(dmin(r1.y, r2.y), tg.y);
+    const double mx0 = dmax(dmax(r1.x, r2.x), tg.x), mx1 = dmax(dmax(r1.y, r2.y), tg.y);
+    int pmin0 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mn0, -P.boundary[0]), gs), 0.5);
+    int pmin1 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mn1, -P.boundary[1]), gs), 0.5);
+    int pmax0 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mx0, -P.boundary[0]), gs), 0.5);
+    int pmax1 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mx1, -P.boundary[1]), gs), 0.5);
+    pmin0 -= 1;
+    pmin1 -= 1;
+    pmax0 += 1;
+    pmax1 += 1;
+    if (pmax0 >= gw) pmax0 = gw - 1;
+    if (pmax1 >= gh) pmax1 = gh - 1;
+    if (pmin0 < 0) pmin0 = 0;
+    if (pmin1 < 0) pmin1 = 0;
+    if (!(pmax1 - pmin1 > 0 && pmax0 - pmin0 > 0)) return o;   // every height skips
+    const int64_t ncol = pmax0 - pmin0 + 1;
+    const int64_t ncell = (int64_t)(pmax1 - pmin1 + 1) * ncol;
+    // the inside cells, in cell order
+    int64_t n_in = 0;
+    for (int64_t base = 0; base < ncell; base += 32) {
+        const int64_t i = base + lane;
+        const bool in = i < ncell && cell_inside(P, r1, r2, tg, pmin1 + i / ncol, pmin0 + i % ncol);
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        const int64_t at = n_in + __popc(m & ((1u << lane) - 1u));
+        if (in && at < kCellCap) st.cell[at] = (int32_t)i;
+        n_in += __popc(m);
+    }
+    __syncwarp();
+    const bool listed = n_in <= kCellCap;
+    const int64_t n_items = listed ? n_in : ncell;
     for (int64_t kh = 0; kh < n_heights; ++kh) {
         const float iter_height = (float)__dadd_rn((double)start_h, __dmul_rn((double)kh, hstep));
         const P3 T1 = r1, T2 = r2, T3 = {tg.x, tg.y, (double)iter_height};
-        const double mn0 = dmin(dmin(T1.x, T2.x), T3.x), mn1 = dmin(dmin(T1.y, T2.y), T3.y);
-        const double mx0 = dmax(dmax(T1.x, T2.x), T3.x), mx1 = dmax(dmax(T1.y, T2.y), T3.y);
-        int pmin0 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mn0, -P.boundary[0]), gs), 0.5);
-        int pmin1 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mn1, -P.boundary[1]), gs), 0.5);
-        int pmax0 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mx0, -P.boundary[0]), gs), 0.5);
-        int pmax1 = (int)__dadd_rn(__ddiv_rn(__dadd_rn(mx1, -P.boundary[1]), gs), 0.5);
-        pmin0 -= 1;
-        pmin1 -= 1;
-        pmax0 += 1;
-        pmax1 += 1;
-        if (pmax0 >= gw) pmax0 = gw - 1;
-        if (pmax1 >= gh) pmax1 = gh - 1;
-        if (pmin0 < 0) pmin0 = 0;
-        if (pmin1 < 0) pmin1 = 0;
-        if (!(pmax1 - pmin1 > 0 && pmax0 - pmin0 > 0)) continue;
         // the triangle's plane (the same for every cell of this height)
         const double v12x = __dadd_rn(T2.x, -T1.x), v12y = __dadd_rn(T2.y, -T1.y),
                      v12z = __dadd_rn(T2.z, -T1.z);
@@ -157,11 +200,10 @@ __device__ SearchOut ortho_search(const DevLevel &P, const double2 *__restrict__
             D = -__dadd_rn(__dadd_rn(__dmul_rn(A, T1.x), __dmul_rn(B, T1.y)), __dmul_rn(C, T1.z));
             plane_ok = C != 0;
         }
-        const int64_t ncol = pmax0 - pmin0 + 1;
-        const int64_t ncell = (int64_t)(pmax1 - pmin1 + 1) * ncol;
         double sum_ncc = 0;
         int count_ncc = 0;
         int sum_count_n = 0;
+        const bool cached = listed;
         for (int ti = 1; ti < P.num_images; ++ti) {
             if (!P.im[ti].selected) continue;
             // pass 0: sums for the means; pass 1: centred products
@@ -169,19 +211,33 @@ __device__ SearchOut ortho_search(const DevLevel &P, const double2 *__restrict__
             double m[4] = {0, 0, 0, 0};
             int count_n = 0;
             for (int pass = 0; pass < 2; ++pass) {
-                for (int64_t base = 0; base < ncell; base += 32) {
+                for (int64_t base = 0; base < n_items; base += 32) {
                     const int64_t i = base + lane;
-                    double v[4] = {0, 0, 0, 0};
-                    bool ok = false;
-                    if (i < ncell)
-                        ok = ortho_cell(P, lonlat, ti, T1, T2, T3, plane_ok, A, B, C, D,
-                                        pmin1 + i / ncol, pmin0 + i % ncol, v);
-                    const unsigned valid = __ballot_sync(0xffffffffu, ok);
+                    // staged item of this chunk's first lane: the chunk's own
+                    // slots when the items are cached, else slots 0..31
+                    const int64_t first = cached ? base : 0;
+                    unsigned valid;
+                    if (pass == 0 || !cached) {
+                        double v[4] = {0, 0, 0, 0};
+                        bool ok = false;
+                        if (i < n_items) {
+                            const int64_t c = listed ? (int64_t)st.cell[i] : i;
+                            const int64_t row = pmin1 + c / ncol, col = pmin0 + c % ncol;
+                            ok = (listed || cell_inside(P, T1, T2, T3, row, col)) &&
+                                 cell_sample(P, lonlat, ti, plane_ok, A, B, C, D, row, col, v);
+                        }
+                        valid = __ballot_sync(0xffffffffu, ok);
+                        st.v[2 * (first + lane)] = make_double2(v[0], v[1]);
+                        st.v[2 * (first + lane) + 1] = make_double2(v[2], v[3]);
+                        if (cached && lane == 0) st.valid[base >> 5] = valid;
+                    } else {
+                        valid = st.valid[base >> 5];
+                    }
+                    __syncwarp();
                     for (int j = 0; j < 32; ++j) {
-                        double u[4];
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) u[c] = __shfl_sync(0xffffffffu, v[c], j);
                         if (!((valid >> j) & 1u)) continue;
+                        const double2 a = st.v[2 * (first + j)], b = st.v[2 * (first + j) + 1];
+                        const double u[4] = {a.x, a.y, b.x, b.y};
                         if (pass == 0) {
 #pragma unroll
                             for (int c = 0; c < 4; ++c) s[c] = __dadd_rn(s[c], u[c]);
@@ -197,6 +253,7 @@ __device__ SearchOut ortho_search(const DevLevel &P, const double2 *__restrict__
                             s[5] = __dadd_rn(s[5], __dmul_rn(er, er));
                         }
                     }
+                    __syncwarp();   // the slots are rewritten by the next chunk
                 }
                 if (pass == 0) {
                     if (count_n < 1) break;
@@ -263,9 +320,10 @@ __global__ void __launch_bounds__(32) ortho_search_kernel(const DevLevel *__rest
                                                           double mpp, const vll_point3 *pts3,
                                                           int64_t target_index, double *out) {
     const DevLevel &P = *Pp;
+    __shared__ CellStage st;
     const SearchOut o = ortho_search(P, nullptr, mpp, P3{pts3[0].x, pts3[0].y, pts3[0].z},
                                      P3{pts3[1].x, pts3[1].y, pts3[1].z},
-                                     P3{pts3[2].x, pts3[2].y, pts3[2].z}, target_index);
+                                     P3{pts3[2].x, pts3[2].y, pts3[2].z}, target_index, st);
     if (threadIdx.x == 0) {
         out[0] = o.f_height;
         out[1] = o.f_sncc;
@@ -275,7 +333,7 @@ __global__ void __launch_bounds__(32) ortho_search_kernel(const DevLevel *__rest
 
 // Ortho_blunder, first (parallel) loop over the triangles (setsm_code.cpp:
 // 8060-8146): one warp per triangle.
-__global__ void __launch_bounds__(128) tri_search_kernel(const DevLevel *__restrict__ Pp,
+__global__ void __launch_bounds__(128, 3) tri_search_kernel(const DevLevel *__restrict__ Pp,
                                                          double mpp, const vll_point3 *pts,
                                                          int64_t n_pts, const vll_tri *tris,
                                                          int64_t n_tris, const int64_t *tri_nodes,
@@ -284,6 +342,8 @@ __global__ void __launch_bounds__(128) tri_search_kernel(const DevLevel *__restr
                                                          uint32_t *sort_key,
                                                          const double2 *__restrict__ lonlat) {
     const DevLevel &P = *Pp;
+    __shared__ CellStage stage[4];   // one per warp of the 128-thread block
+    CellStage &st = stage[threadIdx.x >> 5];
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const uint32_t none = (uint32_t)n_pts;
@@ -325,7 +385,7 @@ __global__ void __launch_bounds__(128) tri_search_kernel(const DevLevel *__restr
                         tnode = n3;
                         tpt = tr.c;
                     }
-                    const SearchOut o = ortho_search(P, lonlat, mpp, r1, r2, tg, tnode);
+                    const SearchOut o = ortho_search(P, lonlat, mpp, r1, r2, tg, tnode, st);
                     if (o.f_height != -9999.0) {
                         u = 1;
                         key = tpt;
