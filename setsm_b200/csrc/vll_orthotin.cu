@@ -9,11 +9,14 @@
 // each target image, and the Pearson correlation of the sampled intensities
 // and magnitudes (Correlate, SubFunctions.cpp:974-1018) picks the height.
 //
-// GPU layout: one warp per triangle.  Lanes sample 32 cells at a time; every
-// sum is then accumulated in the reference's cell order (lane-ordered shuffle
-// loop), so the FP64 results are the reference's bit for bit.  Correlate's
-// two passes recompute the samples instead of storing them, which bounds the
-// memory by nothing but the triangle.  The sequential "apply" pass of
+// GPU layout: one warp per triangle.  The triangle's box and its inside cells
+// do not depend on the swept height, so the inside cells are listed once;
+// each height projects only those, 32 at a time, and stages their samples in
+// shared memory for both of Correlate's passes.  Every sum is accumulated in
+// the reference's cell order (each lane reads the staged samples in
+// sequence), so the FP64 results are the reference's bit for bit.  A
+// triangle with more than 256 inside cells tests its box per height and
+// recomputes the samples in the second pass.  The sequential "apply" pass of
 // Ortho_blunder is restated in parallel with the same result: triangles that
 // found a height are grouped by target point (stable radix sort), each
 // point's triangles are walked in triangle order to find the record-breakers
