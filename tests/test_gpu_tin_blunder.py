@@ -172,3 +172,28 @@ def test_crowded_points_and_repeated_vertices(gpu_ctx, seed):
     det, counts, zext = fresh_out(n)
     gpu_ctx.blunder_detection_tin(inp, 1, oncc, True, 1, 60.0, pts, det, mixed, counts, zext)
     assert_same(pts, det, inp.gridpt3, counts, zext, r_pts, r_det, ref.gridpt3, r_counts, r_zext)
+
+
+def test_invalid_inputs_fail_and_leave_buffers(gpu_ctx):
+    """A point whose grid node lies outside the grid, a negative Hinterval and
+    a missing output fail with VLL_ERR_INVALID; the host buffers keep their
+    contents."""
+    inp, pts, tris, oncc, _ = mg.tinb_case("tinb_l0")
+    it, fb, cbl, hint = mg.GOLDEN_TINB["tinb_l0"]["call"]
+    g0 = inp.gridpt3.copy()
+    bad = pts.copy()
+    bad["y"][5] = inp.boundary[3] + 50 * inp.grid_resolution   # rows past the top
+    before = bad.copy()
+    det, counts, zext = fresh_out(len(pts))
+    with pytest.raises(vll.VLLError) as e:
+        gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, bad, det, tris, counts, zext)
+    assert e.value.code == abi.VLL_ERR_INVALID
+    # fields, not bytes: numpy's copy of a padded record leaves the padding
+    for f in ("x", "y", "z", "flag"):
+        assert np.array_equal(bad[f], before[f])
+    assert not det.any() and not counts.any()
+    assert cases.field_mismatch(inp.gridpt3, g0) == {}
+    with pytest.raises(vll.VLLError):
+        gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, -1.0, pts, det, tris, counts, zext)
+    # the context stays usable
+    gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
