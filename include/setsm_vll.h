@@ -549,6 +549,18 @@ int vll_debug_ortho_raster(vll_context *ctx, const vll_level_desc *desc, const v
                            int use_b, double im_res, int ti, double *out, int64_t capacity,
                            int64_t *width, int64_t *height);
 
+/* Diagnostics (host only, no GPU): blunder_detection_TIN's height threshold
+ * (setsm_code.cpp:9320-9418) bounded from sums formed in any order.
+ * sd / sd2: the sums of the m_terms height differences and of their squares
+ * in some order; dh_count, hbin[hdiffcount]: the count and the histogram of
+ * their integer parts.  exact != 0 takes sd / sd2 as the reference's own
+ * sequential sums.  [*lo, *hi] receives the band that holds the reference's
+ * threshold (lo == hi when it is known exactly). */
+int vll_debug_tin_threshold(int pyramid_step, int iteration, int is_ra, double grid_resolution,
+                            double hinterval, double sd, double sd2, int64_t m_terms,
+                            int64_t dh_count, const uint32_t *hbin, uint32_t hdiffcount,
+                            int exact, double *lo, double *hi);
+
 /* ---- image preprocessing (SubFunctions.cpp:2418-2560, Template.hpp:82) -- */
 /* Sobel magnitude (uint16) and 20-degree direction bin per pixel, on host
  * buffers; bit-exact with MakeSobelMagnitudeImage + Orientation. */

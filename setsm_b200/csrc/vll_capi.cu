@@ -792,6 +792,25 @@ int64_t vll_launch_count(const vll_context *ctx) { return ctx ? ctx->launches_to
 
 int64_t vll_tin_rerun_count(const vll_context *ctx) { return ctx ? ctx->tin_reruns : 0; }
 
+int vll_debug_tin_threshold(int pyramid_step, int iteration, int is_ra, double grid_resolution,
+                            double hinterval, double sd, double sd2, int64_t m_terms,
+                            int64_t dh_count, const uint32_t *hbin, uint32_t hdiffcount,
+                            int exact, double *lo, double *hi) {
+    if (!lo || !hi || (hdiffcount > 0 && !hbin) || pyramid_step < 0 || pyramid_step > 12 ||
+        m_terms < 0 || dh_count < 0)
+        return VLL_ERR_INVALID;
+    vll::TinArgs a;
+    memset(&a, 0, sizeof(a));
+    a.L = pyramid_step;
+    a.iteration = iteration;
+    a.is_ra = is_ra != 0;
+    a.gs = grid_resolution;
+    a.hinterval = hinterval;
+    vll::tin_threshold_band(a, sd, sd2, m_terms, (long)dh_count, hbin, hdiffcount, exact != 0, lo,
+                            hi);
+    return VLL_OK;
+}
+
 int64_t vll_voxel_count(const vll_nccresult *ncc, int64_t n) {
     if (!ncc || n <= 0) return 0;
     int64_t s = 0;

@@ -92,6 +92,11 @@ struct TinOutput {
 // bound the reference's height threshold (equal when lo == hi).
 void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], long dh_count,
                     const uint32_t *hbin, uint32_t hdiffcount, TinThresholds *th);
+// The height-threshold band from sums in any order of m_terms terms (exact:
+// the sums are the reference's own).
+void tin_threshold_band(const TinArgs &a, double sd, double sd2, int64_t m_terms, long dh_count,
+                        const uint32_t *hbin, uint32_t hdiffcount, bool exact, double *lo,
+                        double *hi);
 // anchor_list: the pass leaves gp3 alone and lists its anchor_flag writes
 // (TinOutput::anchor_node / anchor_val) for the caller to apply.
 size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount);

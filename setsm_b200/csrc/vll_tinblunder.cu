@@ -692,6 +692,24 @@ size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount) {
 }
 
 namespace {
+void sum_band(double s, int64_t m, double out[2]);
+}
+
+void tin_threshold_band(const TinArgs &a, double sd, double sd2, int64_t m_terms, long dh_count,
+                        const uint32_t *hbin, uint32_t hdiffcount, bool exact, double *lo,
+                        double *hi) {
+    double b1[2] = {sd, sd}, b2[2] = {sd2, sd2};
+    if (!exact) {
+        sum_band(sd, m_terms, b1);
+        sum_band(sd2, m_terms, b2);
+    }
+    TinThresholds th;
+    tin_thresholds(a, b1, b2, dh_count, hbin, hdiffcount, &th);
+    *lo = th.height_th;
+    *hi = th.height_th_hi;
+}
+
+namespace {
 
 // The sums' bound (lo, hi) around the reference's sequential sums, given the
 // sums s in another order of m terms >= 0: |seq - s| <= 2 (m-1) u (1 + O(u))

@@ -37,7 +37,7 @@ EXPORTED = [
     "vll_set_height_range", "vll_select_mps", "vll_initialize_voxel",
     "vll_initialize_voxel_device", "vll_awncc_peaks_device", "vll_select_mps_device",
     "vll_set_height_range_device", "vll_blunder_detection_tin",
-    "vll_blunder_detection_tin_device", "vll_tin_rerun_count",
+    "vll_blunder_detection_tin_device", "vll_tin_rerun_count", "vll_debug_tin_threshold",
 ]
 
 _lib = None
@@ -117,6 +117,8 @@ def load():
     L.vll_blunder_detection_tin_device.argtypes = L.vll_blunder_detection_tin.argtypes
     L.vll_tin_rerun_count.argtypes = [vp]
     L.vll_tin_rerun_count.restype = i64
+    L.vll_debug_tin_threshold.argtypes = [i32, i32, i32, dbl, dbl, dbl, dbl, i64, i64, vp,
+                                          C.c_uint32, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.vll_set_height_range_device.argtypes = L.vll_set_height_range.argtypes
     _lib = L
     return L
