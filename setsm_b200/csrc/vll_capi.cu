@@ -1441,12 +1441,13 @@ int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccre
     const int64_t N = desc->grid_width * desc->grid_height;
     if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
     if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
-    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
     VLL_CUDA(ctx, ensure(ctx->tin_pts, (size_t)(capacity > 0 ? capacity : 1) * sizeof(vll_point3)));
+    // the grid coordinates stay on the host: the points come back with their
+    // node in x and take the coordinates here
     rc = select_mps_run(ctx, desc, (const vll_nccresult *)ctx->ncc.p, (vll_ugrid *)ctx->gp3.p,
-                        (const double *)ctx->pts.p, th_roh, th_roh_min, th_roh_start,
-                        th_roh_next, iteration, mpp, final_level_iteration, mpp_stereo_angle,
-                        (vll_point3 *)ctx->tin_pts.p, capacity, count);
+                        nullptr, th_roh, th_roh_min, th_roh_start, th_roh_next, iteration, mpp,
+                        final_level_iteration, mpp_stereo_angle, (vll_point3 *)ctx->tin_pts.p,
+                        capacity, count);
     if (rc) return rc;   // host buffers untouched
     VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
                                   cudaMemcpyDeviceToHost, ctx->stream));
@@ -1454,6 +1455,11 @@ int vll_select_mps(vll_context *ctx, const vll_level_desc *desc, const vll_nccre
         VLL_CUDA(ctx, cudaMemcpyAsync(points, ctx->tin_pts.p, (size_t)*count * sizeof(vll_point3),
                                       cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int64_t j = 0; j < *count; ++j) {
+        const int64_t node = (int64_t)points[j].x;
+        points[j].x = desc->grid_pts[2 * node];
+        points[j].y = desc->grid_pts[2 * node + 1];
+    }
     return VLL_OK;
 }
 

@@ -39,7 +39,8 @@ __global__ void roh_hist_kernel(const vll_nccresult *__restrict__ ncc, int64_t n
 __device__ __forceinline__ double dq_grid(int16_t v) { return __ddiv_rn((double)v, 1000.0); }
 
 // The per-node decision (setsm_code.cpp:8658-8891).  Writes the node's
-// UGRID and, for a selected node, keep[i] = 1 and its point.
+// UGRID and, for a selected node, keep[i] = 1 and its point (without
+// grid_pts, the point's x holds the node index, exact in a double).
 __global__ void select_kernel(const vll_nccresult *__restrict__ ncc, vll_ugrid *gp3,
                               const double *__restrict__ grid_pts, int64_t n, SelectArgs a,
                               int *keep, vll_point3 *cand) {
@@ -157,8 +158,12 @@ __global__ void select_kernel(const vll_nccresult *__restrict__ ncc, vll_ugrid *
             keep[i] = 1;
             vll_point3 p;
             memset(&p, 0, sizeof(p));
-            p.x = grid_pts[2 * i];
-            p.y = grid_pts[2 * i + 1];
+            if (grid_pts) {
+                p.x = grid_pts[2 * i];
+                p.y = grid_pts[2 * i + 1];
+            } else {
+                p.x = (double)i;   // the node: the caller fills the coordinates
+            }
             p.z = z;
             p.flag = 0;
             cand[i] = p;
