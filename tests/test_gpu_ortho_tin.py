@@ -48,6 +48,9 @@ def test_ortho_blunder_matches_reference_fixture(gpu_ctx, name):
     (dict(seed=33, size=768, nodes=24, res=12.0, L=1, template=15), 2.5),
     (dict(seed=34, size=768, nodes=24, res=16.0, L=2, template=15, range_m=80.0), 3.0),
     (dict(seed=35, size=512, nodes=32, res=8.0, n_images=3, anchor_frac=0.4), 1.5),
+    # sparse points: triangles of up to ~1200 cells, many with more than the
+    # 256 inside cells a warp stages (the per-height box path)
+    (dict(seed=37, size=768, nodes=128, res=2.0, point_frac=0.002), 1.5),
 ])
 def test_ortho_blunder_matches_reference_build(gpu_ctx, kw, mpp):
     inp, pts, tris = cases.make_tin_case(**kw)
@@ -83,6 +86,7 @@ def searchable(inp, pts, tris):
 @pytest.mark.parametrize("kw,mpp", [
     (dict(seed=41, size=768, nodes=40, res=7.0), 1.5),
     (dict(seed=42, size=768, nodes=24, res=16.0, L=2, template=15), 1.0),
+    (dict(seed=43, size=768, nodes=128, res=2.0, point_frac=0.0015), 1.5),
 ])
 def test_single_search_matches_reference(gpu_ctx, kw, mpp):
     inp, pts, tris = cases.make_tin_case(**kw)
