@@ -101,6 +101,11 @@ __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict
     float *buf1 = buf0 + max_h;
     const int64_t W = P.grid_w, Hh = P.grid_h;
     const double step = P.height_step;
+    // a power-of-two step divides exactly as a multiplication by its
+    // reciprocal (also a power of two): the same bits as the division
+    int step_exp = 0;
+    const bool step_pow2 = step > 0 && frexp(step, &step_exp) == 0.5;
+    const double inv_step = step_pow2 ? ldexp(1.0, 1 - step_exp) : 0.0;
     const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t line = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp; line < n_lines;
          line += warps_total) {
@@ -154,7 +159,8 @@ __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict
                     const double wncc = dq_voxel(vrow[h].INCC);
                     // (float iter_height - short minHeight) is a float subtraction in
                     // the reference, then divided by the double step
-                    const int i0 = (int)__ddiv_rn((double)__fsub_rn(hgt, (float)T.minHeight), step);
+                    const double dh = (double)__fsub_rn(hgt, (float)T.minHeight);
+                    const int i0 = (int)(step_pow2 ? __dmul_rn(dh, inv_step) : __ddiv_rn(dh, step));
                     const int i1 = i0 - kPHS, i2 = i0 + kPHS;
                     double V1 = 0, V2 = 0, V3 = 0;
                     const double V4 = __dadd_rn((double)max_w, -kP2);
