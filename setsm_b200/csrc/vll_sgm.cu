@@ -15,13 +15,17 @@
 // node.  All 8 directions run in one launch, each storing its path costs per
 // slot, and a second pass adds the 8 in the reference's order (the float sums
 // come out the same); when the 8 stores do not fit the scratch budget, one
-// launch per direction accumulates in order instead.  In both, the previous node's costs and the current ones live in two
-// shared-memory rows of the warp.  A diagonal direction's paths start from two
+// launch per direction accumulates in order instead.  In both, the previous
+// node's costs and the current ones live in two shared-memory rows of the
+// warp, and the path's voxel rows are copied into a four-row shared-memory
+// ring two nodes ahead of their step (cp.async).  A diagonal direction's paths start from two
 // walls (a column of rows and a row of columns); the path that starts at their
 // common corner is walked by both of the reference's loops, so its nodes get
 // the same contribution twice -- here one warp walks it and adds it twice.
 #include <algorithm>
+#include <climits>
 #include <cstdint>
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
 #include "vll_device.cuh"
@@ -80,10 +84,53 @@ __host__ __device__ __forceinline__ int64_t lines_of(int dir, int64_t W, int64_t
     return dir < 2 ? H : (dir < 4 ? W : H + W);
 }
 
+// The records of one path node the recurrence reads (warp-uniform).
+struct NodeRec {
+    int64_t off;             // the node's first voxel in the packed rows
+    int n;                   // NumOfHeight
+    int16_t min_h, max_w;    // NCCresult minHeight, max_WNCC
+    int16_t g_min, g_max;    // UGRID minHeight, maxHeight
+};
+
+__device__ __forceinline__ NodeRec load_rec(const DevLevel &P, int64_t q) {
+    const vll_nccresult R = P.ncc[q];
+    const vll_ugrid g = P.gp3[q];
+    NodeRec x;
+    x.off = P.vox_off[q];
+    x.n = R.NumOfHeight;
+    x.min_h = R.minHeight;
+    x.max_w = R.max_WNCC;
+    x.g_min = g.minHeight;
+    x.g_max = g.maxHeight;
+    return x;
+}
+
+// Voxel rows in flight per warp: node j's row is read at step j, node j-1's
+// (its flags) too, and node j+2's is being copied, so four slots.
+constexpr int kRing = 4;
+constexpr int kRowsPerWarp = 2 + kRing;   // two cost rows, kRing voxel rows
+
+// Asynchronous copy of a node's voxel row (4-byte words) into a ring slot;
+// one commit group per call, empty when the node is past the path's end.
+__device__ __forceinline__ void issue_row(uint32_t *dst, const vll_voxel *src, int n, bool live,
+                                          int lane) {
+    if (live)
+        for (int h = lane; h < n; h += 32) __pipeline_memcpy_async(dst + h, src + h, 4);
+    __pipeline_commit();
+}
+
+__device__ __forceinline__ uint8_t vox_flag(uint32_t w) { return (uint8_t)(w & 0xffu); }
+__device__ __forceinline__ int16_t vox_incc(uint32_t w) { return (int16_t)(w >> 16); }
+
 // One direction's path costs.  Accumulating form (lr == nullptr): the costs
 // are added into sumcost (one launch per direction, in order).  Storing form:
 // blockIdx.y is the direction and every slot's cost goes to lr[dir][slot]
 // (0 where the reference adds nothing), for sgm_sum_kernel.
+//
+// A path is a chain of steps, each waiting for its node's voxel row, so the
+// rows are copied into shared memory two nodes ahead (cp.async) and the
+// nodes' records loaded four ahead; a step then waits only for a row issued
+// two steps earlier.
 __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict__ Pp, int dir,
                                                       int64_t n_lines, float *__restrict__ sumcost,
                                                       int max_h, float *__restrict__ lr,
@@ -97,8 +144,9 @@ __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict
     }
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float *buf0 = sm_lh + (size_t)warp * 2 * max_h;
+    float *buf0 = sm_lh + (size_t)warp * kRowsPerWarp * max_h;
     float *buf1 = buf0 + max_h;
+    uint32_t *ring = reinterpret_cast<uint32_t *>(buf1 + max_h);
     const int64_t W = P.grid_w, Hh = P.grid_h;
     const double step = P.height_step;
     // a power-of-two step divides exactly as a multiplication by its
@@ -113,140 +161,153 @@ __global__ void __launch_bounds__(128) sgm_dir_kernel(const DevLevel *__restrict
         int dr, dc;
         bool twice;
         if (!path_of(dir, line, W, Hh, r, c, dr, dc, twice)) continue;
+        const int64_t len_r = dr > 0 ? Hh - r : (dr < 0 ? r + 1 : INT64_MAX);
+        const int64_t len_c = dc > 0 ? W - c : (dc < 0 ? c + 1 : INT64_MAX);
+        const int64_t len = len_r < len_c ? len_r : len_c;   // nodes on the path
+        auto node = [&](int64_t j) { return (r + j * dr) * W + (c + j * dc); };
+        // records of nodes j .. j+4
+        NodeRec q0, q1, q2, q3, q4;
+        q0 = load_rec(P, node(0));
+        q1 = len > 1 ? load_rec(P, node(1)) : q0;
+        q2 = len > 2 ? load_rec(P, node(2)) : q0;
+        q3 = len > 3 ? load_rec(P, node(3)) : q0;
+        q4 = len > 4 ? load_rec(P, node(4)) : q0;
+        issue_row(ring, P.vox + q0.off, q0.n, true, lane);
+        issue_row(ring + max_h, P.vox + q1.off, q1.n, len > 1, lane);
         float *pre = buf0, *cur = buf1;
-        // ---- first node: SGM_start_pos (:6755-6767) ----
-        {
-            const int64_t pt = r * W + c;
-            const vll_nccresult R = P.ncc[pt];
-            const vll_ugrid g = P.gp3[pt];
-            const vll_voxel *vrow = P.vox + P.vox_off[pt];
-            float *sc = sumcost + P.vox_off[pt];
-            for (int h = lane; h < R.NumOfHeight; h += 32) {
-                const float hgt = (float)__dadd_rn((double)R.minHeight, __dmul_rn((double)h, step));
-                float v = 0.f;
-                if (hgt >= (float)g.minHeight && hgt <= (float)g.maxHeight) {
-                    v = (float)dq_voxel(vrow[h].INCC);
-                    if (!lr) {
-                        float s = sc[h] + v;
-                        if (twice) s = s + v;
-                        sc[h] = s;
-                    }
-                }
-                if (lr) lr[P.vox_off[pt] + h] = v;
-                pre[h] = v;
-            }
+        NodeRec T = q0;   // previous node
+        for (int64_t j = 0; j < len; ++j) {
+            issue_row(ring + ((j + 2) & (kRing - 1)) * max_h, P.vox + q2.off, q2.n, j + 2 < len,
+                      lane);
+            __pipeline_wait_prior(2);   // node j's row (the two newest may still fly)
             __syncwarp();
-        }
-        // ---- following nodes: SGM_con_pos (:6769-6999) ----
-        for (;;) {
-            const int64_t tr = r, tc = c;   // previous node
-            r += dr;
-            c += dc;
-            if (r < 0 || r >= Hh || c < 0 || c >= W) break;
-            const int64_t pt = r * W + c, tp = tr * W + tc;
-            const vll_nccresult R = P.ncc[pt];
-            const vll_nccresult T = P.ncc[tp];
-            const vll_ugrid g = P.gp3[pt];
-            const vll_voxel *vrow = P.vox + P.vox_off[pt];
-            const vll_voxel *trow = P.vox + P.vox_off[tp];
-            float *sc = sumcost + P.vox_off[pt];
-            const float max_w = (float)dq_result(T.max_WNCC);
-            const int tn = T.NumOfHeight;
-            for (int h = lane; h < R.NumOfHeight; h += 32) {
-                const float hgt = (float)__dadd_rn((double)R.minHeight, __dmul_rn((double)h, step));
-                float out = 0.f;
-                if (hgt >= (float)g.minHeight && hgt <= (float)g.maxHeight) {
-                    const double wncc = dq_voxel(vrow[h].INCC);
-                    // (float iter_height - short minHeight) is a float subtraction in
-                    // the reference, then divided by the double step
-                    const double dh = (double)__fsub_rn(hgt, (float)T.minHeight);
-                    const int i0 = (int)(step_pow2 ? __dmul_rn(dh, inv_step) : __ddiv_rn(dh, step));
-                    const int i1 = i0 - kPHS, i2 = i0 + kPHS;
-                    double V1 = 0, V2 = 0, V3 = 0;
-                    const double V4 = __dadd_rn((double)max_w, -kP2);
-                    double m;
-                    if (i0 == 0 && i2 >= 0 && i2 < tn) {
-                        const bool f = trow[i0].flag_cal, f2 = trow[i2].flag_cal;
-                        if (f && f2) {
-                            V2 = __dadd_rn((double)pre[i2], -kP1);
-                            V3 = (double)pre[i0];
-                            m = dmax(dmax(V2, V3), V4);
-                        } else if (f) {
-                            V3 = (double)pre[i0];
-                            m = dmax(V3, V4);
-                        } else if (f2) {
-                            V2 = __dadd_rn((double)pre[i2], -kP1);
-                            m = dmax(V2, V4);
-                        } else {
-                            m = V4;
+            const uint32_t *vrow = ring + (j & (kRing - 1)) * max_h;
+            const uint32_t *trow = ring + ((j - 1) & (kRing - 1)) * max_h;
+            const NodeRec R = q0;
+            float *sc = sumcost + R.off;
+            if (j == 0) {
+                // ---- first node: SGM_start_pos (:6755-6767) ----
+                for (int h = lane; h < R.n; h += 32) {
+                    const float hgt = (float)__dadd_rn((double)R.min_h, __dmul_rn((double)h, step));
+                    float v = 0.f;
+                    if (hgt >= (float)R.g_min && hgt <= (float)R.g_max) {
+                        v = (float)dq_voxel(vox_incc(vrow[h]));
+                        if (!lr) {
+                            float s = sc[h] + v;
+                            if (twice) s = s + v;
+                            sc[h] = s;
                         }
-                    } else if (i0 == tn - 1 && i1 >= 0 && i1 < tn) {
-                        const bool f = trow[i0].flag_cal, f1 = trow[i1].flag_cal;
-                        if (f && f1) {
-                            V1 = __dadd_rn((double)pre[i1], -kP1);
-                            V3 = (double)pre[i0];
-                            m = dmax(dmax(V1, V3), V4);
-                        } else if (f) {
-                            V3 = (double)pre[i0];
-                            m = dmax(V3, V4);
-                        } else if (f1) {
-                            V1 = __dadd_rn((double)pre[i1], -kP1);
-                            m = dmax(V1, V4);
-                        } else {
-                            m = V4;
-                        }
-                    } else if (i0 > 0 && i0 < tn - 1 && i1 >= 0 && i1 < tn && i2 >= 0 && i2 < tn) {
-                        const bool f = trow[i0].flag_cal, f1 = trow[i1].flag_cal,
-                                   f2 = trow[i2].flag_cal;
-                        if (f && f1 && f2) {
-                            V1 = __dadd_rn((double)pre[i1], -kP1);
-                            V2 = __dadd_rn((double)pre[i2], -kP1);
-                            V3 = (double)pre[i0];
-                            m = dmax(dmax(dmax(V1, V2), V3), V4);
-                        } else if (f && f1) {
-                            V1 = __dadd_rn((double)pre[i1], -kP1);
-                            V3 = (double)pre[i0];
-                            m = dmax(dmax(V1, V3), V4);
-                        } else if (f1 && f2) {
-                            // V3 keeps its initial 0 and takes part (setsm_code.cpp:6917-6925)
-                            V1 = __dadd_rn((double)pre[i1], -kP1);
-                            V2 = __dadd_rn((double)pre[i2], -kP1);
-                            m = dmax(dmax(dmax(V1, V2), V3), V4);
-                        } else if (f && f2) {
-                            V2 = __dadd_rn((double)pre[i2], -kP1);
-                            V3 = (double)pre[i0];
-                            m = dmax(dmax(V2, V3), V4);
-                        } else if (f) {
-                            V3 = (double)pre[i0];
-                            m = dmax(V3, V4);
-                        } else if (f1) {
-                            V1 = __dadd_rn((double)pre[i1], -kP1);
-                            m = dmax(V1, V4);
-                        } else if (f2) {
-                            V2 = __dadd_rn((double)pre[i2], -kP1);
-                            m = dmax(V2, V4);
-                        } else {
-                            m = V4;
-                        }
-                    } else {
-                        m = V4;
                     }
-                    const double t = __dadd_rn(m, -(double)max_w);
-                    out = (float)__dadd_rn(wncc, t);
-                    if (!lr) {
-                        float s = sc[h] + out;
-                        if (twice) s = s + out;
-                        sc[h] = s;
-                    }
+                    if (lr) lr[R.off + h] = v;
+                    pre[h] = v;
                 }
-                if (lr) lr[P.vox_off[pt] + h] = out;
-                cur[h] = out;
+            } else {
+                // ---- following nodes: SGM_con_pos (:6769-6999) ----
+                const float max_w = (float)dq_result(T.max_w);
+                const int tn = T.n;
+                for (int h = lane; h < R.n; h += 32) {
+                    const float hgt = (float)__dadd_rn((double)R.min_h, __dmul_rn((double)h, step));
+                    float out = 0.f;
+                    if (hgt >= (float)R.g_min && hgt <= (float)R.g_max) {
+                        const double wncc = dq_voxel(vox_incc(vrow[h]));
+                        // (float iter_height - short minHeight) is a float subtraction in
+                        // the reference, then divided by the double step
+                        const double dh = (double)__fsub_rn(hgt, (float)T.min_h);
+                        const int i0 = (int)(step_pow2 ? __dmul_rn(dh, inv_step) : __ddiv_rn(dh, step));
+                        const int i1 = i0 - kPHS, i2 = i0 + kPHS;
+                        double V1 = 0, V2 = 0, V3 = 0;
+                        const double V4 = __dadd_rn((double)max_w, -kP2);
+                        double m;
+                        if (i0 == 0 && i2 >= 0 && i2 < tn) {
+                            const bool f = vox_flag(trow[i0]), f2 = vox_flag(trow[i2]);
+                            if (f && f2) {
+                                V2 = __dadd_rn((double)pre[i2], -kP1);
+                                V3 = (double)pre[i0];
+                                m = dmax(dmax(V2, V3), V4);
+                            } else if (f) {
+                                V3 = (double)pre[i0];
+                                m = dmax(V3, V4);
+                            } else if (f2) {
+                                V2 = __dadd_rn((double)pre[i2], -kP1);
+                                m = dmax(V2, V4);
+                            } else {
+                                m = V4;
+                            }
+                        } else if (i0 == tn - 1 && i1 >= 0 && i1 < tn) {
+                            const bool f = vox_flag(trow[i0]), f1 = vox_flag(trow[i1]);
+                            if (f && f1) {
+                                V1 = __dadd_rn((double)pre[i1], -kP1);
+                                V3 = (double)pre[i0];
+                                m = dmax(dmax(V1, V3), V4);
+                            } else if (f) {
+                                V3 = (double)pre[i0];
+                                m = dmax(V3, V4);
+                            } else if (f1) {
+                                V1 = __dadd_rn((double)pre[i1], -kP1);
+                                m = dmax(V1, V4);
+                            } else {
+                                m = V4;
+                            }
+                        } else if (i0 > 0 && i0 < tn - 1 && i1 >= 0 && i1 < tn && i2 >= 0 && i2 < tn) {
+                            const bool f = vox_flag(trow[i0]), f1 = vox_flag(trow[i1]),
+                                       f2 = vox_flag(trow[i2]);
+                            if (f && f1 && f2) {
+                                V1 = __dadd_rn((double)pre[i1], -kP1);
+                                V2 = __dadd_rn((double)pre[i2], -kP1);
+                                V3 = (double)pre[i0];
+                                m = dmax(dmax(dmax(V1, V2), V3), V4);
+                            } else if (f && f1) {
+                                V1 = __dadd_rn((double)pre[i1], -kP1);
+                                V3 = (double)pre[i0];
+                                m = dmax(dmax(V1, V3), V4);
+                            } else if (f1 && f2) {
+                                // V3 keeps its initial 0 and takes part (setsm_code.cpp:6917-6925)
+                                V1 = __dadd_rn((double)pre[i1], -kP1);
+                                V2 = __dadd_rn((double)pre[i2], -kP1);
+                                m = dmax(dmax(dmax(V1, V2), V3), V4);
+                            } else if (f && f2) {
+                                V2 = __dadd_rn((double)pre[i2], -kP1);
+                                V3 = (double)pre[i0];
+                                m = dmax(dmax(V2, V3), V4);
+                            } else if (f) {
+                                V3 = (double)pre[i0];
+                                m = dmax(V3, V4);
+                            } else if (f1) {
+                                V1 = __dadd_rn((double)pre[i1], -kP1);
+                                m = dmax(V1, V4);
+                            } else if (f2) {
+                                V2 = __dadd_rn((double)pre[i2], -kP1);
+                                m = dmax(V2, V4);
+                            } else {
+                                m = V4;
+                            }
+                        } else {
+                            m = V4;
+                        }
+                        const double t = __dadd_rn(m, -(double)max_w);
+                        out = (float)__dadd_rn(wncc, t);
+                        if (!lr) {
+                            float s = sc[h] + out;
+                            if (twice) s = s + out;
+                            sc[h] = s;
+                        }
+                    }
+                    if (lr) lr[R.off + h] = out;
+                    cur[h] = out;
+                }
+                float *tmp = pre;
+                pre = cur;
+                cur = tmp;
             }
-            __syncwarp();
-            float *tmp = pre;
-            pre = cur;
-            cur = tmp;
+            __syncwarp();   // node j-1's row slot is refilled at the next step
+            T = q0;
+            q0 = q1;
+            q1 = q2;
+            q2 = q3;
+            q3 = q4;
+            if (j + 5 < len) q4 = load_rec(P, node(j + 5));
         }
+        __pipeline_wait_prior(0);
         __syncwarp();
     }
 }
@@ -304,7 +365,7 @@ cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int m
         if (e != cudaSuccess) return e;
     }
     if (max_h < 1) max_h = 1;
-    const size_t per_warp = (size_t)2 * max_h * sizeof(float);
+    const size_t per_warp = (size_t)kRowsPerWarp * max_h * sizeof(float);
     if (per_warp > 200 * 1024) return cudaErrorInvalidValue;
     int warps = (int)std::min<size_t>(4, (200 * 1024) / per_warp);
     if (warps < 1) warps = 1;
