@@ -1587,9 +1587,10 @@ static int tin_blunder_run(vll_context *ctx, const vll_level_desc *desc, int ite
         for (int64_t i = 0; i < n_pts; ++i)
             if (node[i] >= 0) host_gp3[node[i]].anchor_flag = val[i];
     }
-    // terms, sums, scan (2), fill, snapshot, point pass, close; a re-run adds
-    // the undo, the sequential sums, the point pass and close
-    ctx->launches_total += (n_tris > 0 ? 8 : 5) + (out.rerun ? (n_tris > 0 ? 4 : 3) : 0);
+    // terms, sums, scan (2), fill, thresholds, snapshot, point pass, close; a
+    // re-run adds the undo, the sequential sums, the thresholds, the point
+    // pass and close
+    ctx->launches_total += (n_tris > 0 ? 9 : 6) + (out.rerun ? (n_tris > 0 ? 5 : 4) : 0);
     ctx->tin_reruns += out.rerun;
     blunder_count[0] += out.count[0];
     blunder_count[1] += out.count[1];

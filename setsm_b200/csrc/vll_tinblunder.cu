@@ -315,7 +315,13 @@ __global__ void __launch_bounds__(256)
     point_kernel(TinArgs a, vll_point3 *pts, const vll_tri *tris, const float *ortho_ncc,
                  const int32_t *list, const int64_t *start, const unsigned int *count,
                  vll_ugrid *gp3, uint8_t *detected, const uint8_t *flag0, unsigned int *bad,
-                 unsigned int *rerun, int64_t *anchor_node, uint8_t *anchor_val) {
+                 unsigned int *rerun, int64_t *anchor_node, uint8_t *anchor_val,
+                 const double *th) {
+    if (*bad) return;   // a triangle's vertex outside the grid: the call fails
+    a.height_th = th[0];
+    a.height_th_hi = th[1];
+    a.ortho_ncc_th = th[2];
+    a.th_ref_ncc = th[3];
     const int lane = threadIdx.x & 31;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t index = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; index < a.n_pts;
@@ -507,8 +513,9 @@ __device__ __forceinline__ unsigned long long dkey(double v) {
 // The closing pass (:9765-9781): blunder counts, 3 -> 1, the height extent
 // of the remaining points.
 __global__ void close_kernel(int64_t n_pts, vll_point3 *pts, unsigned long long *cnt,
-                             unsigned long long *zkey, const unsigned int *rerun) {
-    if (*rerun) return;   // the point pass runs again first
+                             unsigned long long *zkey, const unsigned int *rerun,
+                             const unsigned int *bad) {
+    if (*rerun || *bad) return;   // the point pass runs again first, or the call fails
     unsigned long long kept = 0, blunders = 0, zmin = ~0ull, zmax = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_pts;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -587,7 +594,7 @@ namespace {
 // The reference's height threshold as a function of up_3sigma (:9362-9418):
 // clamp(up, H/2, H) from level 3 on, min(up, th80, 50) below; a NaN up
 // compares false, as +inf would.  Non-decreasing in up.
-double height_th_of(bool ge3, double H, uint32_t th80, double up) {
+__host__ __device__ double height_th_of(bool ge3, double H, uint32_t th80, double up) {
     if (ge3) {
         double h = H;
         if (up < h) h = up < h / 2.0 ? h / 2.0 : up;
@@ -598,10 +605,11 @@ double height_th_of(bool ge3, double H, uint32_t th80, double up) {
     return h;
 }
 
-}  // namespace
-
-void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], long dh_count,
-                    const uint32_t *hbin, uint32_t hdiffcount, TinThresholds *th) {
+// The thresholds of the level from the sums' bounds (sd, sd2: [lo, hi]),
+// their count and th80, the 99th-percentile bin of the height differences
+// (used below level 3); host and device share it.
+__host__ __device__ void thresholds_of(const TinArgs &a, const double sd[2], const double sd2[2],
+                                       long dh_count, uint32_t th80, TinThresholds *th) {
     const int L = a.L, it = a.iteration;
     // the ortho-NCC threshold of the level (:9304-9313; the statistics-based
     // value computed before it is overwritten there)
@@ -634,9 +642,118 @@ void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], l
         if (a.is_ra == 1) th2 = gsd * 30;
         H = a.hinterval < th2 ? a.hinterval : th2;
     }
+    double lo, hi;
+    if (ge3 && !check_dh) {
+        lo = hi = height_th_of(true, H, th80, H);
+    } else {
+        // up = mean + 3 std, evaluated as the reference does; each operation
+        // is non-decreasing in its operand (or non-increasing, for the
+        // subtrahend) over sums >= 0, and rounding to nearest is
+        // monotone, so the corners of the sums' box bound the reference's
+        // rounded value
+        const double n = (double)dh_count;
+        const double mean_lo = sd[0] / n, mean_hi = sd[1] / n;
+        const double vn_lo = sd2[0] - sd[1] * sd[1] / n, vn_hi = sd2[1] - sd[0] * sd[0] / n;
+        const double not_a_number = nan("");
+        if (vn_hi < 0) {
+            lo = hi = height_th_of(ge3, H, th80, not_a_number);   // sqrt of a negative: NaN
+        } else if (vn_lo < 0) {
+            // std >= 0, or NaN (which compares as +inf)
+            lo = height_th_of(ge3, H, th80, mean_lo);
+            hi = height_th_of(ge3, H, th80, not_a_number);
+        } else {
+            lo = height_th_of(ge3, H, th80, mean_lo + 3 * sqrt(vn_lo / n));
+            hi = height_th_of(ge3, H, th80, mean_hi + 3 * sqrt(vn_hi / n));
+        }
+        if (hi < lo) hi = lo;
+    }
+    th->height_th = lo;
+    th->height_th_hi = hi;
+    th->ortho_ncc_th = ortho_ncc_th;
+    th->th_ref_ncc = th_ref_ncc;
+}
+
+// The sums' bound (lo, hi) around the reference's sequential sums, given the
+// sums s in another order of m terms >= 0: |seq - s| <= 2 (m-1) u (1 + O(u))
+// * exact, and exact <= s (1 + (m-1) u (1 + O(u))); 3 m u covers both.
+__host__ __device__ void sum_band(double s, int64_t m, double out[2]) {
+    const double e = s * (3.0 * (double)m * 0x1p-53) * (1.0 + 0x1p-40);
+    out[0] = nextafter(s - e, -INFINITY);
+    if (out[0] < 0) out[0] = 0;
+    out[1] = nextafter(s + e, INFINITY);
+}
+
+// Slots of the per-call counters (unsigned long long): [0..1] counts, [2]
+// complement of the minimum z key, [3] maximum z key, [4] bad input, [5]
+// valid triangles, [6] re-run due, [8..9] the two sums (doubles), [10..13]
+// the thresholds (doubles: band low, band high, ortho NCC, reference NCC);
+// the histogram follows at [16].
+constexpr int kMiscSums = 8, kMiscTh = 10, kMiscHist = 16;
+
+// The level's thresholds on the device, after the sums: th80 by a warp's
+// prefix sums over the histogram (32-bit, wrapping as the reference's
+// counter), then the band from the sums (mode: kTinSums*; `exact`: the sums
+// are the reference's own).
+__global__ void threshold_kernel(TinArgs a, unsigned long long *misc, uint32_t hdiffcount,
+                                 int64_t m_terms, int mode, int exact) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t *hbin = reinterpret_cast<const uint32_t *>(misc + kMiscHist);
+    const long dh_count = (long)(3 * misc[5]);
+    uint32_t th80 = 1000;
+    if (a.L < 3) {
+        uint32_t carry = 0;
+        bool found = false;
+        for (uint32_t base = 0; base < hdiffcount && !found; base += 32) {
+            const uint32_t t = base + lane;
+            uint32_t v = t < hdiffcount ? hbin[t] : 0u;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += x;
+            }
+            const uint32_t cum = carry + v;
+            const double per = __dmul_rn(__ddiv_rn((double)cum, (double)dh_count), 100.0);
+            const unsigned hit = __ballot_sync(0xffffffffu, t < hdiffcount && per > 99);
+            if (hit) {
+                th80 = base + (uint32_t)(__ffs(hit) - 1);
+                found = true;
+            }
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (!found) th80 = hdiffcount - 1u;   // the reference's t - 1 after the loop
+    }
+    if (lane != 0) return;
+    double *md = reinterpret_cast<double *>(misc);
+    const double s = md[kMiscSums], s2 = md[kMiscSums + 1];
+    double sd[2] = {s, s}, sd2[2] = {s2, s2};
+    const bool finite = isfinite(s) && isfinite(s2);
+    if (!exact && finite) {
+        sum_band(s, m_terms, sd);
+        sum_band(s2, m_terms, sd2);
+    }
+    TinThresholds th;
+    thresholds_of(a, sd, sd2, dh_count, th80, &th);
+    if (!exact && !finite) {
+        // a sum that is not finite: every compared value falls inside the
+        // band, so a pass that compares anything re-runs on the ordered sums
+        th.height_th = -INFINITY;
+        th.height_th_hi = INFINITY;
+    } else if (!exact && mode == kTinSumsWideBand) {
+        th.height_th -= 1.0;
+        th.height_th_hi += 1.0;
+    }
+    md[kMiscTh] = th.height_th;
+    md[kMiscTh + 1] = th.height_th_hi;
+    md[kMiscTh + 2] = th.ortho_ncc_th;
+    md[kMiscTh + 3] = th.th_ref_ncc;
+}
+
+}  // namespace
+
+void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], long dh_count,
+                    const uint32_t *hbin, uint32_t hdiffcount, TinThresholds *th) {
     // levels 0-2: the 99th percentile of the integer height differences
     uint32_t th80 = 1000;
-    if (!ge3) {
+    if (a.L < 3) {
         uint32_t total_dh = 0;
         long t = 0;
         bool found = false;
@@ -651,36 +768,7 @@ void tin_thresholds(const TinArgs &a, const double sd[2], const double sd2[2], l
         }
         if (!found) th80 = (uint32_t)(t - 1);
     }
-    double lo, hi;
-    if (ge3 && !check_dh) {
-        lo = hi = height_th_of(true, H, th80, H);
-    } else {
-        // up = mean + 3 std, evaluated as the reference does; each operation
-        // is non-decreasing in its operand (or non-increasing, for the
-        // subtrahend) over sums >= 0, and rounding to nearest is
-        // monotone, so the corners of the sums' box bound the reference's
-        // rounded value
-        const double n = (double)dh_count;
-        auto var_num = [&](double s, double s2) { return s2 - s * s / n; };
-        const double mean_lo = sd[0] / n, mean_hi = sd[1] / n;
-        const double vn_lo = var_num(sd[1], sd2[0]), vn_hi = var_num(sd[0], sd2[1]);
-        const double nan = std::numeric_limits<double>::quiet_NaN();
-        if (vn_hi < 0) {
-            lo = hi = height_th_of(ge3, H, th80, nan);   // sqrt of a negative: NaN
-        } else if (vn_lo < 0) {
-            // std >= 0, or NaN (which compares as +inf)
-            lo = height_th_of(ge3, H, th80, mean_lo);
-            hi = height_th_of(ge3, H, th80, nan);
-        } else {
-            lo = height_th_of(ge3, H, th80, mean_lo + 3 * sqrt(vn_lo / n));
-            hi = height_th_of(ge3, H, th80, mean_hi + 3 * sqrt(vn_hi / n));
-        }
-        if (hi < lo) hi = lo;
-    }
-    th->height_th = lo;
-    th->height_th_hi = hi;
-    th->ortho_ncc_th = ortho_ncc_th;
-    th->th_ref_ncc = th_ref_ncc;
+    thresholds_of(a, sd, sd2, dh_count, th80, th);
 }
 
 size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount) {
@@ -689,10 +777,6 @@ size_t tin_blunder_scratch(int64_t n_pts, int64_t n_tris, uint32_t hdiffcount) {
            al(128 + (hdiffcount + 1) * 4) + al((np > 0 ? np : 1) * 4) +
            al(2 * (n_pts + 1) * 4) + al((n_pts + 1) * 8) + 2 * al(n_pts) + al(n_pts * 8) +
            al(n_pts);
-}
-
-namespace {
-void sum_band(double s, int64_t m, double out[2]);
 }
 
 void tin_threshold_band(const TinArgs &a, double sd, double sd2, int64_t m_terms, long dh_count,
@@ -709,19 +793,6 @@ void tin_threshold_band(const TinArgs &a, double sd, double sd2, int64_t m_terms
     *hi = th.height_th_hi;
 }
 
-namespace {
-
-// The sums' bound (lo, hi) around the reference's sequential sums, given the
-// sums s in another order of m terms >= 0: |seq - s| <= 2 (m-1) u (1 + O(u))
-// * exact, and exact <= s (1 + (m-1) u (1 + O(u))); 3 m u covers both.
-void sum_band(double s, int64_t m, double out[2]) {
-    const double e = s * (3.0 * (double)m * 0x1p-53) * (1.0 + 0x1p-40);
-    out[0] = std::nextafter(s - e, -INFINITY);
-    if (out[0] < 0) out[0] = 0;
-    out[1] = std::nextafter(s + e, INFINITY);
-}
-
-}  // namespace
 
 cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
                             const float *ortho_ncc, vll_ugrid *gp3, uint8_t *detected,
@@ -737,13 +808,11 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     };
     void *tmp = take(tmp_b);
     double *dhv = (double *)take(3 * a.n_tris * sizeof(double));
-    // [0..1] counts, [2] complement of the minimum z key, [3] maximum z key,
-    // [4] bad input, [5] valid triangles, [6] re-run due, [8..9] the two sums
-    // (doubles); the histogram follows, so one copy brings both back
-    const size_t misc_b = 128 + (hdiffcount + 1) * 4;
+    const size_t misc_b = 8 * kMiscHist + (hdiffcount + 1) * 4;
     unsigned long long *misc = (unsigned long long *)take(misc_b);
-    double *sums = reinterpret_cast<double *>(misc + 8);
-    uint32_t *hbin = reinterpret_cast<uint32_t *>(misc + 16);
+    double *sums = reinterpret_cast<double *>(misc + kMiscSums);
+    const double *th = reinterpret_cast<const double *>(misc + kMiscTh);
+    uint32_t *hbin = reinterpret_cast<uint32_t *>(misc + kMiscHist);
     int32_t *list = (int32_t *)take((np > 0 ? np : 1) * 4);
     unsigned int *count = (unsigned int *)take(2 * (a.n_pts + 1) * 4);
     unsigned int *cursor = count + a.n_pts + 1;
@@ -773,84 +842,38 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
     }
     if ((e = cub::DeviceScan::ExclusiveSum(tmp, tmp_b, count, start, (int)(a.n_pts + 1), s)))
         return e;
-    if (a.n_tris > 0) {
-        fill_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, tris, start, cursor, list);
-        if ((e = cudaGetLastError())) return e;
-    }
-    // the sums, the histogram, the valid count and the input check back for
-    // the thresholds
-    std::vector<unsigned long long> host_misc((misc_b + 7) / 8);
-    if ((e = cudaMemcpyAsync(host_misc.data(), misc, misc_b, cudaMemcpyDeviceToHost, s))) return e;
-    if ((e = cudaStreamSynchronize(s))) return e;
-    const unsigned long long *hm = host_misc.data();
-    const uint32_t *hb = reinterpret_cast<const uint32_t *>(hm + 16);
-    if (hm[4]) {
-        out->bad_input = 1;
-        return cudaSuccess;
-    }
-    double hs[2];
-    memcpy(hs, hm + 8, sizeof(hs));
-    const long dh_count = (long)(3 * hm[5]);
-    double sd[2], sd2[2];
-    const bool band = !exact && std::isfinite(hs[0]) && std::isfinite(hs[1]);
-    auto exact_sums = [&]() -> cudaError_t {
-        cudaError_t e2;
-        if (a.n_tris > 0) {
-            dh_serial_sum_kernel<<<1, 512, 0, s>>>(np, dhv, sums);
-            if ((e2 = cudaGetLastError())) return e2;
-            if ((e2 = cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, s))) return e2;
-            if ((e2 = cudaStreamSynchronize(s))) return e2;
-        }
-        sd[0] = sd[1] = hs[0];
-        sd2[0] = sd2[1] = hs[1];
-        return cudaSuccess;
-    };
-    if (band) {
-        sum_band(hs[0], np, sd);
-        sum_band(hs[1], np, sd2);
-    } else if (exact) {
-        sd[0] = sd[1] = hs[0];
-        sd2[0] = sd2[1] = hs[1];
-    } else if ((e = exact_sums())) {
-        return e;
-    }
-    TinThresholds th;
-    tin_thresholds(a, sd, sd2, dh_count, hb, hdiffcount, &th);
-    if (band && sums_mode == kTinSumsWideBand) {
-        th.height_th -= 1.0;
-        th.height_th_hi += 1.0;
-    }
-    a.height_th = th.height_th;
-    a.height_th_hi = th.height_th_hi;
-    a.ortho_ncc_th = th.ortho_ncc_th;
-    a.th_ref_ncc = th.th_ref_ncc;
+    if (a.n_tris > 0) fill_kernel<<<blocks_for(a.n_tris, 256), 256, 0, s>>>(a, tris, start, cursor, list);
+    // the thresholds on the device: the point pass follows without a host wait
+    threshold_kernel<<<1, 32, 0, s>>>(a, misc, hdiffcount, np, sums_mode, exact ? 1 : 0);
+    copy_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0, detected,
+                                                               det0);
     const unsigned pblocks = blocks_for(a.n_pts * 32, 256);
     auto point_pass = [&]() -> cudaError_t {
         point_kernel<<<pblocks, 256, 0, s>>>(a, pts, tris, ortho_ncc, list, start, count, gp3,
                                              detected, flag0, bad, rerun, anchor_node,
-                                             anchor_val);
+                                             anchor_val, th);
         close_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, misc, misc + 2,
-                                                             rerun);
+                                                             rerun, bad);
         return cudaGetLastError();
     };
-    copy_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0, detected,
-                                                               det0);
     if ((e = point_pass())) return e;
-    unsigned long long m[7];
+    unsigned long long m[kMiscHist];
     if ((e = cudaMemcpyAsync(m, misc, sizeof(m), cudaMemcpyDeviceToHost, s))) return e;
     if ((e = cudaStreamSynchronize(s))) return e;
     out->rerun = 0;
     if (m[6] && !m[4]) {
         // a comparison fell inside the band: undo the pass and run it again
-        // with the threshold from the sequential sums
+        // with the threshold from the sums in the reference's order
         out->rerun = 1;
         restore_flags_kernel<<<blocks_for(a.n_pts, 256), 256, 0, s>>>(a.n_pts, pts, flag0,
                                                                       detected, det0);
-        if ((e = cudaGetLastError())) return e;
-        if ((e = exact_sums())) return e;
-        tin_thresholds(a, sd, sd2, dh_count, hb, hdiffcount, &th);
-        a.height_th = a.height_th_hi = th.height_th;
-        if ((e = cudaMemsetAsync(misc, 0, 64, s))) return e;
+        if (a.n_tris > 0) dh_serial_sum_kernel<<<1, 512, 0, s>>>(np, dhv, sums);
+        else if ((e = cudaMemsetAsync(sums, 0, 16, s))) return e;
+        threshold_kernel<<<1, 32, 0, s>>>(a, misc, hdiffcount, np, sums_mode, 1);
+        // counts, z keys and the re-run flag start again ([4] bad and [5] the
+        // valid count stay)
+        if ((e = cudaMemsetAsync(misc, 0, 32, s))) return e;
+        if ((e = cudaMemsetAsync(misc + 6, 0, 8, s))) return e;
         if ((e = point_pass())) return e;
         if ((e = cudaMemcpyAsync(m, misc, sizeof(m), cudaMemcpyDeviceToHost, s))) return e;
         if ((e = cudaStreamSynchronize(s))) return e;
@@ -866,7 +889,9 @@ cudaError_t run_tin_blunder(TinArgs a, vll_point3 *pts, const vll_tri *tris,
         memcpy(&v, &bits, 8);
         out->z[k] = v;
     }
-    out->height_th = a.height_th;
+    double th_lo;
+    memcpy(&th_lo, &m[kMiscTh], 8);
+    out->height_th = th_lo;
     out->anchor_node = anchor_node;
     out->anchor_val = anchor_val;
     return cudaSuccess;
