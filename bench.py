@@ -57,12 +57,13 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv")
+        self.path = None
 
     def start(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        import tempfile
         try:
-            self.f = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix=f"clocks_gpu{self.index}_", suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
@@ -145,78 +146,190 @@ def sum_over_ranks(world, x: float) -> float:
 # ---------------------------------------------------------------------------
 # CPU reference leg
 # ---------------------------------------------------------------------------
+# The reference's VerticalLineLocus is timed on a band of grid rows in the
+# middle of the grid holding at least this fraction of the nodes, per window.
+REF_NODE_FRACTION = 0.01
+# Image rows kept around a band's projected footprint: the rotated 11x11
+# window (radius <= 9 px) plus the orientation window (6 px) and Sobel (1 px),
+# with room to spare.
+REF_FOOTPRINT_MARGIN = 48
+# Rows discarded at each cut edge of a preprocessed crop: Sobel reads one row
+# and the orientation window six rows past a pixel, so rows further than this
+# from a cut are the full image's values.
+REF_CROP_EDGE = 16
+
 _EVAL_COUNTS = {}
 
 
-def band_evals(inp, ctx, key) -> int:
-    """Evaluations (ComputeMultiNCC calls) of a band.  With a GPU context the
-    matcher counts them on the identical inputs; without one (the reference
-    arm, which runs none of this repository's GPU code on its path) the C
-    restatement of the path counts them, once per band, outside any timing."""
+def ref_band(wl, evals_budget: float = 5e6) -> tuple:
+    """(first row, rows) of the reference band: >= REF_NODE_FRACTION of the
+    nodes (plus one row), or more rows on grids where that is cheap."""
+    from setsm_b200 import workloads
+    H = wl.grid.height
+    rows = max(int(math.ceil(H * REF_NODE_FRACTION)) + 1, workloads.rows_for_budget(wl, evals_budget))
+    rows = min(H, rows)
+    return (H - rows) // 2, rows
+
+
+def band_footprint(wl, r0: int, rows: int) -> list:
+    """Image-row range [y0, y1) of each image that the band's nodes can reach:
+    every node projected at its minimum and maximum height, plus
+    REF_FOOTPRINT_MARGIN rows."""
+    import torch
+    from setsm_b200 import synth
+    W = wl.grid.width
+    sl = slice(r0 * W, (r0 + rows) * W)
+    wgs = torch.from_numpy(np.ascontiguousarray(wl.host["wgs"][sl]))
+    n = wl.scene.spec.image_size
+    out = []
+    for ci in range(2):
+        lines = []
+        for f in ("minHeight", "maxHeight"):
+            h = torch.from_numpy(wl.gp3[f][sl].astype(np.float64))
+            _, line = synth.rpc_eval(wl.scene.rpcs[ci], wgs[:, 0], wgs[:, 1], h)
+            lines.append(line)
+        line = torch.cat(lines)
+        y0 = max(0, int(math.floor(float(line.min()))) - REF_FOOTPRINT_MARGIN)
+        y1 = min(n, int(math.ceil(float(line.max()))) + REF_FOOTPRINT_MARGIN)
+        out.append((y0, y1))
+    return out
+
+
+def reference_planes(wl, footprints: list) -> dict:
+    """Magnitude and orientation planes made by the reference's own
+    MakeSobelMagnitudeImage and Orientation (SubFunctions.cpp:2418, :2473) on
+    crops of the images around `footprints` (one [y0, y1) row range per
+    image and band), written into zero full-size planes."""
+    from oracle import refpy
+    n = wl.scene.spec.image_size
+    mags = [np.zeros((n, n), np.uint16) for _ in range(2)]
+    oris = [np.zeros((n, n), np.uint8) for _ in range(2)]
+    for fp in footprints:
+        for ci, (y0, y1) in enumerate(fp):
+            c0 = max(0, y0 - REF_CROP_EDGE)
+            c1 = min(n, y1 + REF_CROP_EDGE)
+            m, o = refpy.preprocess(wl.host["img"][ci][c0:c1], 15)
+            mags[ci][y0:y1] = m[y0 - c0:y1 - c0]
+            oris[ci][y0:y1] = o[y0 - c0:y1 - c0]
+    return {"mag": mags, "ori": oris}
+
+
+def band_evals(inp, key) -> int:
+    """Evaluations (ComputeMultiNCC calls) of a band, counted once per band by
+    the C restatement of the path on the identical inputs, outside any timed
+    region (the reference's function returns no such count)."""
     if key not in _EVAL_COUNTS:
-        if ctx is not None:
-            _EVAL_COUNTS[key] = int(ctx.vertical_line_locus(inp, inp.new_nccresult(), None,
-                                                            "split").evals)
-        else:
-            from oracle import oraclepy
-            oraclepy.set_threads(os.cpu_count() or 1)
-            _EVAL_COUNTS[key] = int(oraclepy.vertical_line_locus(inp, inp.new_nccresult(),
-                                                                 want_evals=True)[1])
+        from oracle import oraclepy
+        oraclepy.set_threads(os.cpu_count() or 1)
+        _EVAL_COUNTS[key] = int(oraclepy.vertical_line_locus(inp, inp.new_nccresult(),
+                                                             want_evals=True)[1])
     return _EVAL_COUNTS[key]
 
 
-def cpu_reference(wl, ctx, budget_s: float, templates) -> dict:
-    """Reference SETSM (oracle/_ref, OpenMP on every host core) on a band of
-    grid rows sized for about `budget_s` seconds of CPU work per window."""
-    from oracle import refpy
-    from setsm_b200 import workloads
-    if not refpy.available():
-        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                "sample": "reference build missing (oracle/_ref not built)"}
-    cores = os.cpu_count() or 1
-    refpy.set_threads(cores)
-    total_evals, total_s, parts = 0, 0.0, []
-    for tmpl in templates:
-        rate_guess = (2.0e5 if tmpl == 11 else 1.0e5) * cores
-        rows = workloads.rows_for_budget(wl, rate_guess * budget_s)
-        r0 = max(0, wl.grid.height // 2 - rows // 2)
-        inp = wl.host_inputs(tmpl, rows=(r0, r0 + rows))
-        evals = band_evals(inp, ctx, (tmpl, r0, rows))
-        ncc = inp.new_nccresult()
+class ReferenceLeg:
+    """The reference SETSM code (oracle/_ref, OpenMP on every host core) on a
+    band of grid rows of the workload, one band per window, with planes made by
+    the reference's own preprocessing.  Nothing of this repository's GPU
+    library runs here."""
+
+    def __init__(self, wl, templates):
+        from oracle import refpy
+        self.ok = refpy.available()
+        self.wl = wl
+        self.templates = templates
+        self.cores = os.cpu_count() or 1
+        if not self.ok:
+            return
+        refpy.set_threads(self.cores)
+        self.r0, self.rows = ref_band(wl)
+        self.footprint = band_footprint(wl, self.r0, self.rows)
         t = time.perf_counter()
-        refpy.vertical_line_locus(inp, ncc)
-        dt = time.perf_counter() - t
-        total_evals += evals
-        total_s += dt
-        parts.append(f"{rows} rows x {wl.grid.width} nodes, {workloads.WINDOW_OF_TEMPLATE[tmpl]}: "
-                     f"{evals} evals in {dt:.2f} s")
-    return {"value": total_evals / total_s, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": "; ".join(parts)}
+        self.planes = reference_planes(wl, [self.footprint])
+        self.prep_s = time.perf_counter() - t
+        self.inputs = {tm: wl.host_inputs(tm, rows=(self.r0, self.r0 + self.rows),
+                                          planes=self.planes) for tm in templates}
+        self.evals = {tm: band_evals(self.inputs[tm], (tm, self.r0, self.rows))
+                      for tm in templates}
+        self.last_ncc = {}
+
+    def run(self, rows: int | None = None) -> dict:
+        """One pass of every window over the band (or over its first `rows`
+        rows, for untimed warm-ups); returns the measured sample."""
+        from oracle import refpy
+        from setsm_b200 import workloads
+        if not self.ok:
+            return {"value": None, "unit": UNIT, "cores": self.cores, "kind": "reference",
+                    "sample": "reference build missing (oracle/_ref not built)"}
+        total_evals, total_s, parts = 0, 0.0, []
+        for tm in self.templates:
+            inp = self.inputs[tm]
+            if rows is not None:
+                inp = self.wl.host_inputs(tm, rows=(self.r0, self.r0 + rows), planes=self.planes)
+            ncc = inp.new_nccresult()
+            t = time.perf_counter()
+            refpy.vertical_line_locus(inp, ncc)
+            dt = time.perf_counter() - t
+            if rows is not None:
+                continue
+            self.last_ncc[tm] = ncc
+            total_evals += self.evals[tm]
+            total_s += dt
+            parts.append(f"{self.rows} rows x {self.wl.grid.width} nodes "
+                         f"({100.0 * self.rows / self.wl.grid.height:.2f} % of the grid), "
+                         f"{workloads.WINDOW_OF_TEMPLATE[tm]}: {self.evals[tm]} evals in {dt:.2f} s")
+        if rows is not None:
+            return {}
+        return {"value": total_evals / total_s, "unit": UNIT, "cores": self.cores,
+                "kind": "reference", "sample": "; ".join(parts)}
+
+    def parity(self, gpu_ncc: dict, gpu_planes: dict | None = None) -> dict:
+        """The last band results against the GPU's whole-grid NCCresult of the
+        same rows (every field), and the reference-made planes against the
+        GPU-made ones over the band's footprint rows."""
+        from tests.cases import field_mismatch
+        W = self.wl.grid.width
+        sl = slice(self.r0 * W, (self.r0 + self.rows) * W)
+        out = {"rows": [self.r0, self.r0 + self.rows], "nodes": self.rows * W, "windows": {}}
+        for tm in self.templates:
+            from setsm_b200 import workloads
+            a = self.last_ncc[tm]
+            b = gpu_ncc[tm][sl]
+            mism = field_mismatch(a, b)
+            ran = a["check_height_change"] > 0
+            dh = np.abs(a["result2"][ran].astype(np.float64) - b["result2"][ran].astype(np.float64))
+            out["windows"][workloads.WINDOW_OF_TEMPLATE[tm]] = {
+                "fields_mismatched": mism, "nodes_mismatched": int(sum(
+                    np.count_nonzero(a[f] != b[f]) for f in a.dtype.names if f in mism)),
+                "max_height_err_m": float(dh.max()) if dh.size else 0.0}
+        if gpu_planes is not None:
+            same = True
+            for ci, (y0, y1) in enumerate(self.footprint):
+                same &= bool(np.array_equal(self.planes["mag"][ci][y0:y1], gpu_planes["mag"][ci][y0:y1]))
+                same &= bool(np.array_equal(self.planes["ori"][ci][y0:y1], gpu_planes["ori"][ci][y0:y1]))
+            out["planes_identical_on_footprint"] = same
+        return out
 
 
 def run_reference_arm(args):
     world, rank, local = dist_setup(args.gpus)
     if rank != 0:
         return
-    import torch
-    from setsm_b200 import vll, workloads
-    ctx = vll.Context(0)
+    from setsm_b200 import workloads
     t0 = time.time()
-    wl = workloads.build(args.config, ctx, device="cuda:0", seed=1)
-    log(f"workload built in {time.time() - t0:.1f} s")
+    # the synthetic scene is generated with torch; this repository's GPU
+    # library is not loaded in this process
+    wl = workloads.build(args.config, None, device="cuda:0" if _cuda() else "cpu", seed=1)
     templates = workloads.CONFIGS[args.config]["templates"]
-    budget = args.cpu_seconds / max(1, args.steps)
-    # inputs are generated on the GPU (synthetic scene, magnitude / orientation
-    # planes bit-identical with the reference's preprocessing); the timed path
-    # is the reference's own VerticalLineLocus on the host cores alone
-    del ctx
+    leg = ReferenceLeg(wl, templates)
+    log(f"workload built in {time.time() - t0:.1f} s; reference planes in "
+        f"{getattr(leg, 'prep_s', 0.0):.1f} s; band rows {getattr(leg, 'rows', 0)}")
     for _ in range(args.warmup):
-        cpu_reference(wl, None, budget, templates)
+        leg.run(rows=2)
     vals = []
     cb = None
     t = time.perf_counter()
     for _ in range(args.steps):
-        cb = cpu_reference(wl, None, budget, templates)
+        cb = leg.run()
         vals.append(cb["value"] or 0.0)
     elapsed = time.perf_counter() - t
     value = statistics.mean(vals) if vals else None
@@ -231,13 +344,17 @@ def run_reference_arm(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-    del torch
+
+
+def _cuda() -> bool:
+    import torch
+    return torch.cuda.is_available()
 
 
 # DRAM bytes per evaluation of the window kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) on the reduced C2 workload:
-# 1228.4 MB / 121.53 M evaluations (7x7), 1225.9 MB / 121.28 M (11x11);
-# profiles/window_kernel_c2_small.md.  Traffic scales with the evaluations.
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the reduced C2 workload
+# (--config c2_small): 1228.4 MB / 121.53 M evaluations (7x7), 1225.9 MB /
+# 121.28 M (11x11).  Traffic scales with the evaluations.
 DRAM_BYTES_PER_EVAL = {11: 1228.4e6 / 121.53e6, 15: 1225.9e6 / 121.28e6}
 
 
@@ -263,6 +380,28 @@ def config_block(args, wl) -> dict:
         "l2": "inputs larger than L2 (images 2 x 1.25 GiB with magnitude and orientation)",
         "parallelism": f"replicas x{args.gpus} (independent scenes per GPU)",
     }
+
+
+def slot_accuracy(ctx, wl, templates, r0: int, rows: int) -> dict:
+    """Max |delta NCC| of the split kernel's FP32 window values against the
+    FP64 kernel's, slot by slot, on a band of grid rows of the workload (the
+    split pipeline settles every decision within its error band of 4e-6 in
+    FP64, which is exact while this error stays below half the band)."""
+    from setsm_b200 import workloads
+    out = {}
+    for t in templates:
+        inp = wl.host_inputs(t, rows=(r0, r0 + rows))
+        r32, off = ctx.debug_slot_rho(inp, inp.new_nccresult(), "split")
+        r64, _ = ctx.debug_slot_rho(inp, inp.new_nccresult(), "plain")
+        both = ~np.isnan(r32) & ~np.isnan(r64)
+        err = np.abs(r32[both] - r64[both])
+        out[workloads.WINDOW_OF_TEMPLATE[t]] = {
+            "slots": int(both.sum()), "max_abs_dncc": float(err.max()) if err.size else 0.0,
+            "p9999_abs_dncc": float(np.quantile(err, 0.9999)) if err.size else 0.0,
+            "same_slots_evaluated": bool(np.array_equal(np.isnan(r32), np.isnan(r64))),
+            "within_half_band": bool(err.size == 0 or err.max() < 2e-6)}
+    out["rows"] = [r0, r0 + rows]
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -304,7 +443,14 @@ def run_ours(args):
     for _ in range(max(3, args.warmup)):
         ref_stats = one_step(args.kernel)
     evals_step = {t: ref_stats[t].evals for t in templates}
-    ncc_split = workloads.ncc_host(wl)
+    # every window's whole-grid result, each from a cleared NCCresult array
+    # (parity legs below compare against these)
+    gpu_ncc = {}
+    for t in templates:
+        wl.d_ncc.zero_()
+        ctx.vertical_line_locus_device(descs[t], wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr(),
+                                       None, None, args.kernel, stats=False)
+        gpu_ncc[t] = workloads.ncc_host(wl)
     barrier(world)
 
     # ---- timed: resident inputs ----
@@ -379,33 +525,52 @@ def run_ours(args):
     # ---- plain FP64 GPU drop-in on the same workload + parity ----
     fp64 = None
     if not args.skip_fp64 and rank == 0:
-        e2 = torch.cuda.Event(enable_timing=True)
-        e3 = torch.cuda.Event(enable_timing=True)
-        e2.record(stream)
-        st_plain = one_step("plain")
-        e3.record(stream)
-        torch.cuda.synchronize(dev)
-        plain_ms = e2.elapsed_time(e3)
-        ncc_plain = workloads.ncc_host(wl)
         from tests.cases import field_mismatch
-        ran = ncc_plain["check_height_change"] > 0
-        valid = ran & (ncc_plain["result4"] > 0)
-        same_h = (ncc_plain["result2"] == ncc_split["result2"]) & \
-                 (ncc_plain["result0"] == ncc_split["result0"])
-        ties = valid & (ncc_plain["result0"] == ncc_plain["result1"])
-        fp64 = {"value": sum(s.evals for s in st_plain.values()) / (plain_ms / 1e3), "unit": UNIT,
-                "ms_per_step": plain_ms,
-                "speedup_split_vs_fp64": (sum(s.evals for s in st_plain.values()) / (plain_ms / 1e3))
-                and value / world / (sum(s.evals for s in st_plain.values()) / (plain_ms / 1e3)),
-                "last_window_mismatch_fields": field_mismatch(ncc_plain, ncc_split),
-                "identical_peak_rate": float(same_h[valid].mean()) if valid.any() else None,
-                "tie_rate": float(ties.sum() / max(1, valid.sum())),
-                "nodes_with_peaks": int(valid.sum())}
-        # restore the split result in the buffer (not needed further)
+        plain_ms, plain_evals = 0.0, 0
+        mism, n_valid, n_same, n_ties = {}, 0, 0, 0
+        for t in templates:
+            wl.d_ncc.zero_()
+            e2 = torch.cuda.Event(enable_timing=True)
+            e3 = torch.cuda.Event(enable_timing=True)
+            e2.record(stream)
+            st = ctx.vertical_line_locus_device(descs[t], wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr(),
+                                                None, None, "plain")
+            e3.record(stream)
+            torch.cuda.synchronize(dev)
+            plain_ms += e2.elapsed_time(e3)
+            plain_evals += st.evals
+            ncc_plain = workloads.ncc_host(wl)
+            ncc_split = gpu_ncc[t]
+            mism[workloads.WINDOW_OF_TEMPLATE[t]] = field_mismatch(ncc_plain, ncc_split)
+            valid = (ncc_plain["check_height_change"] > 0) & (ncc_plain["result4"] > 0)
+            same_h = (ncc_plain["result2"] == ncc_split["result2"]) & \
+                     (ncc_plain["result0"] == ncc_split["result0"])
+            n_valid += int(valid.sum())
+            n_same += int((same_h & valid).sum())
+            n_ties += int((valid & (ncc_plain["result0"] == ncc_plain["result1"])).sum())
+        plain_rate = plain_evals / (plain_ms / 1e3)
+        fp64 = {"value": plain_rate, "unit": UNIT, "ms_per_step": plain_ms,
+                "speedup_split_vs_fp64": value / world / plain_rate,
+                "mismatched_fields_per_window": mism,
+                "identical_peak_rate": n_same / n_valid if n_valid else None,
+                "tie_rate": n_ties / max(1, n_valid),
+                "tie_note": "nodes whose two top peaks quantise to the same rho*1000 in the "
+                            "FP64 kernel (the reference's own ties); their heights are identical too",
+                "nodes_with_peaks": n_valid}
 
+    # ---- FP32 window error against FP64, slot by slot, on a band of rows ----
+    accuracy = None
     cpu = None
+    leg = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        cpu = cpu_reference(wl, ctx, args.cpu_seconds, templates)
+        leg = ReferenceLeg(wl, templates)
+        if leg.ok:
+            accuracy = slot_accuracy(ctx, wl, templates, leg.r0, leg.rows)
+            leg.run(rows=2)
+            cpu = leg.run()
+            cpu["parity_vs_gpu"] = leg.parity(gpu_ncc, {"mag": wl.host["mag"], "ori": wl.host["ori"]})
+        else:
+            cpu = leg.run()
 
     if rank == 0:
         line = {
@@ -420,7 +585,7 @@ def run_ours(args):
                          "traffic_unit": "bytes per window launch (mean of the step's windows)",
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
                                            "of the window kernel on the reduced C2 case, scaled "
-                                           "by evaluations (profiles/window_kernel_c2_small.md)",
+                                           "by evaluations (ncu, reduced C2 case)",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                          "kernel": "window_kernel", "per_window": per_window},
             "e2e": e2e,
@@ -428,6 +593,7 @@ def run_ours(args):
             "tuning": tuned["tuning"] if tuned else None,
             "fp64_rechecks_per_step": rechecks / args.steps,
             "fp64_plain_gpu": fp64,
+            "accuracy_vs_fp64": accuracy,
             "cpu_baseline": cpu,
             "clocks": clk,
         }
@@ -1307,7 +1473,8 @@ def main():
                              "blunder", "ortho_tin", "height_range", "select_mps",
                              "voxel_iter", "tin_blunder"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="end-to-end steps of the default config (0: as many as --steps)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
@@ -1324,6 +1491,8 @@ def main():
     ap.add_argument("--c5-max-batch", type=int, default=32)
     ap.add_argument("--c5-fp64-sample", type=int, default=8)
     args = ap.parse_args()
+    if args.e2e_steps <= 0:
+        args.e2e_steps = args.steps
     if args.impl == "reference":
         run_reference_arm(args)
     elif args.config in ("c3", "c4"):

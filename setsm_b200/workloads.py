@@ -95,10 +95,15 @@ class Workload:
         return (d, self.d_gp3.data_ptr() + r0 * W * abi.UGRID_DTYPE.itemsize,
                 self.d_ncc.data_ptr() + r0 * W * abi.NCCRESULT_DTYPE.itemsize)
 
-    def host_inputs(self, template: int, rows: tuple | None = None) -> level.LevelInputs:
-        """LevelInputs on the pinned host copies (optionally a band of grid rows)."""
+    def host_inputs(self, template: int, rows: tuple | None = None,
+                    planes: dict | None = None) -> level.LevelInputs:
+        """LevelInputs on the pinned host copies (optionally a band of grid
+        rows; `planes` = {"mag": [..], "ori": [..]} replaces the magnitude
+        and orientation planes)."""
         h = self.host
-        imgs = [level.ImageLevel(image=h["img"][ci], mag=h["mag"][ci], ori=h["ori"][ci],
+        mags = (planes or h)["mag"]
+        oris = (planes or h)["ori"]
+        imgs = [level.ImageLevel(image=h["img"][ci], mag=mags[ci], ori=oris[ci],
                                  rpc=self.scene.rpcs[ci]) for ci in range(2)]
         W = self.grid.width
         if rows is None:
@@ -115,13 +120,17 @@ class Workload:
 
 
 def _pinned(t: torch.Tensor) -> np.ndarray:
-    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=torch.cuda.is_available())
     h.copy_(t)
     return h.numpy()
 
 
 def build(name: str, ctx, device: str = "cuda", seed: int = 1, keep_host: bool = True) -> Workload:
-    """Builds a workload on `device` with the library's preprocessing kernels."""
+    """Builds a workload on `device` with the library's preprocessing kernels.
+
+    With `ctx` None the magnitude and orientation planes are not made (the
+    library is not used at all): the caller supplies host planes in
+    ``wl.host["mag"]`` / ``wl.host["ori"]`` before calling `host_inputs`."""
     cfg = CONFIGS[name]
     dev = torch.device(device)
     spec = synth.SceneSpec(seed=seed, image_size=cfg["image_size"])
@@ -130,10 +139,12 @@ def build(name: str, ctx, device: str = "cuda", seed: int = 1, keep_host: bool =
     wl_imgs, wl_mags, wl_oris = [], [], []
     for ci in range(2):
         img = scene.images[ci].contiguous()
+        wl_imgs.append(img)
+        if ctx is None:
+            continue
         mag = torch.empty_like(img)
         ori = torch.empty((n, n), dtype=torch.uint8, device=dev)
         ctx.preprocess_device(img.data_ptr(), n, n, mag.data_ptr(), ori.data_ptr())
-        wl_imgs.append(img)
         wl_mags.append(mag)
         wl_oris.append(ori)
     extent = n * spec.gsd
@@ -156,14 +167,15 @@ def build(name: str, ctx, device: str = "cuda", seed: int = 1, keep_host: bool =
     if keep_host:
         wl.host = {
             "img": [_pinned(t).view(np.uint16) for t in wl_imgs],
-            "mag": [_pinned(t).view(np.uint16) for t in wl_mags],
-            "ori": [_pinned(t) for t in wl_oris],
+            "mag": [_pinned(t).view(np.uint16) for t in wl_mags] or None,
+            "ori": [_pinned(t) for t in wl_oris] or None,
             "wgs": _pinned(wl.d_wgs),
             "pts": _pinned(wl.d_pts),
         }
         gp3_pinned = _pinned(wl.d_gp3).view(abi.UGRID_DTYPE)
         wl.gp3 = gp3_pinned
-    torch.cuda.synchronize(dev)
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
     return wl
 
 
