@@ -271,15 +271,23 @@ int64_t vll_launch_count(const vll_context *ctx);
  * cudaMalloc, cudaFree or allocating library routine; no vll_context is used.
  *   - All pointers are DEVICE pointers (as for
  *     vll_vertical_line_locus_device); `stream` is a cudaStream_t (NULL =
- *     legacy default stream).  The call waits for its work to finish.
+ *     legacy default stream).  The call waits on the host for its work to
+ *     finish before it returns.
  *   - Memory-tight route only (check_matching_rate = 1), stereo, levels
  *     without orthoimage GNCC; anything else returns VLL_ERR_UNSUPPORTED.
- *   - Grids whose nodes and height slots do not fit the 64 MiB array (roughly
- *     55k nodes at ~120 slots each) return VLL_ERR_CAPACITY before any output
- *     is written; `err_buf` receives a message.
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *   - Grids whose per-node scratch (20 bytes a node) does not fit the 64 MiB
+ *     array (about 3.3 M nodes) return VLL_ERR_CAPACITY before any output is
+ *     written; `err_buf` receives a message.  The rest of the array holds
+ *     the FP32 values of the few nodes queued for the exact FP64 pass; a node
+ *     that finds it full is evaluated wholly in FP64, so results never depend
+ *     on its size (only the time does).
+ *   - The array is committed on a device when this library's module is
+ *     loaded there; under CUDA's lazy module loading that is this call's
+ *     first use on the device, so make a first call before a memory pool
+ *     reserves the device's memory.  That call also looks up the array's
+ *     device address (cudaGetSymbolAddress) with the device current; make it
+ *     before any stream capture.  The address is looked up again when the
+ *     device's context changed (after cudaDeviceReset).
  *   - Every call shares the one array, which keeps the previous call's
  *     contents; calls that overlap on the GPU (different streams or threads
  *     at the same time) race on it and must be serialised by the caller.
@@ -287,6 +295,27 @@ int64_t vll_launch_count(const vll_context *ctx);
 int vll_vertical_line_locus_noalloc(const vll_level_desc *desc, const vll_ugrid *d_gridpt3,
                                     vll_nccresult *d_nccresult, void *stream,
                                     int64_t *accessable_grid, char *err_buf, int err_len);
+
+/*
+ * TINCreate_list (SubFunctions.cpp:2768-2846): the Delaunay triangulation of
+ * the matched points, each snapped to the level's grid (column and row =
+ * 0.5 + the offset from min_max[0] / min_max[1] in `resolution` cells,
+ * truncated), as the reference's ordered list of vertex-index triples: the
+ * triangles of its divide and conquer (grid_triangulation.cpp, co-circular
+ * ties decided as there), listed point by point in grid order.  The points'
+ * grid cells must be distinct (else VLL_ERR_INVALID); grids wider or taller
+ * than 32767 cells return VLL_ERR_INVALID (the reference exits).  `count`
+ * receives the list's length; a list longer than `capacity` returns
+ * VLL_ERR_CAPACITY with `count` set and `tris` unwritten.  Fewer than 3 points
+ * give an empty list.  The reference also returns its triangulation object
+ * (for TINUpdate_list); this call returns the list only.
+ */
+int vll_tin_create(vll_context *ctx, const vll_point3 *pts, int64_t n_pts, const double min_max[4],
+                   double resolution, vll_tri *tris, int64_t capacity, int64_t *count);
+/* The same on DEVICE points and triangle arrays (min_max stays on the host). */
+int vll_tin_create_device(vll_context *ctx, const vll_point3 *d_pts, int64_t n_pts,
+                          const double min_max[4], double resolution, vll_tri *d_tris,
+                          int64_t capacity, int64_t *count);
 
 /* ---- batches: many tiles / pyramid levels in one pass ------------------- */
 /* One level of a batch: a descriptor whose every pointer is on the DEVICE (as

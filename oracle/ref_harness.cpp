@@ -644,4 +644,30 @@ int ref_layout(int64_t *out, int cap) {
     return nv;
 }
 
+/* TINCreate_list (SubFunctions.cpp:2768-2846): the ordered triangle list of
+ * the points (vertex indices); the triangulation object is deleted.  Returns
+ * the list's length (the first `cap` triangles are copied out). */
+long ref_tin_create(const vll_point3 *pts, long n, const double *min_max, double resolution,
+                    vll_tri *out, long cap) {
+    D3DPOINT *p = new D3DPOINT[n > 0 ? n : 1];
+    for (long i = 0; i < n; ++i) {
+        p[i].m_X = pts[i].x;
+        p[i].m_Y = pts[i].y;
+        p[i].m_Z = pts[i].z;
+        p[i].flag = pts[i].flag;
+    }
+    vector<UI3DPOINT> tris;
+    double mm[4] = {min_max[0], min_max[1], min_max[2], min_max[3]};
+    int count_tri = 0;
+    FullTriangulation *t = TINCreate_list(p, (int)n, &tris, mm, &count_tri, resolution);
+    delete t;
+    delete[] p;
+    for (size_t i = 0; i < tris.size() && (long)i < cap; ++i) {
+        out[i].a = tris[i].m_X;
+        out[i].b = tris[i].m_Y;
+        out[i].c = tris[i].m_Z;
+    }
+    return (long)tris.size();
+}
+
 }  // extern "C"

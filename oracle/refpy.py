@@ -58,6 +58,8 @@ def lib():
         L.ref_awncc.argtypes = [C.POINTER(abi.LevelDesc), vp, vp, vp, C.c_long]
         L.ref_awncc.restype = None
         L.ref_sobel.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp]
+        L.ref_tin_create.argtypes = [vp, C.c_long, vp, C.c_double, vp, C.c_long]
+        L.ref_tin_create.restype = C.c_long
         L.ref_orientation.argtypes = [C.c_uint32, C.c_uint32, vp, vp, C.c_int, vp]
         L.ref_pyramid_down.argtypes = [C.c_uint32, C.c_uint32, vp, vp]
         L.ref_rpc_project.argtypes = [C.POINTER(abi.ImageDesc), C.c_long, vp, vp, vp, vp]
@@ -461,3 +463,19 @@ def blunder_detection_tin(inputs, iteration, ortho_ncc, flag_blunder, count_bl, 
             int(count_bl), float(hinterval), pts.ctypes.data, detected.ctypes.data, len(pts),
             tris.ctypes.data, len(tris), inputs.gridpt3.ctypes.data, counts.ctypes.data,
             zext.ctypes.data))
+
+
+def tin_create(pts: np.ndarray, min_max, resolution: float) -> np.ndarray:
+    """The reference's TINCreate_list (SubFunctions.cpp:2768-2846): its ordered
+    triangle list (vertex indices) of the points."""
+    pts = np.ascontiguousarray(pts, dtype=abi.POINT3_DTYPE)
+    mm = np.ascontiguousarray(min_max, dtype=np.float64)
+    cap = 2 * len(pts) + 16
+    while True:
+        out = np.zeros(cap, dtype=abi.TRI_DTYPE)
+        with _StdoutToStderr():
+            n = lib().ref_tin_create(pts.ctypes.data, len(pts), mm.ctypes.data, float(resolution),
+                                     out.ctypes.data, cap)
+        if n <= cap:
+            return out[:n]
+        cap = n

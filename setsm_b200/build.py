@@ -32,6 +32,7 @@ SOURCES = {
     "vll_selectmps.cu": ["-fmad=false"],
     "vll_initvoxel.cu": ["-fmad=false"],
     "vll_tinblunder.cu": ["-fmad=false"],
+    "vll_tin.cu": ["-fmad=false"],
     "vll_split.cu": [],
     "vll_capi.cu": [],
     "vll_shim.cu": [],

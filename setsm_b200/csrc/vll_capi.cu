@@ -67,6 +67,7 @@ struct vll_context {
     Buf sumcost;                       // SGM aggregation (float per voxel slot)
     Buf sgm_lr;                        // SGM: the 8 directions' costs per slot
     Buf tin_pts, tin_tris, tin_scratch;  // Ortho_blunder: points, triangles, work arrays
+    vll::TinWork tin_work;             // TINCreate_list: work arrays
     vll::SplitBuffers split;
     vll::SplitTuning tuning;
     void *set = nullptr;               // SetResources of batch calls (vll_capi.cu)
@@ -520,8 +521,6 @@ int finish_set(vll_context *ctx, SetResources &r, const vll::SplitBuffers &b, in
     unsigned long long ctl[8] = {};
     VLL_CUDA(ctx, cudaMemcpyAsync(ctl, b.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (ctl[5]) return fail(ctx, VLL_ERR_INVALID,
-                            "the levels' height slots changed since the plan was made");
     if (accessable)
         for (int l = 0; l < n; ++l) accessable[l] = (int64_t)acc[l];
     if (stats) {
@@ -755,6 +754,7 @@ void vll_destroy(vll_context *ctx) {
     release(ctx->tin_pts);
     release(ctx->tin_tris);
     release(ctx->tin_scratch);
+    vll::tin_release(ctx->tin_work);
     vll::split_release(ctx->split);
     if (ctx->set) {
         release_set(*(SetResources *)ctx->set);
@@ -2070,6 +2070,56 @@ int vll_get_tuning(const vll_context *ctx, vll_tuning *t) {
     t->blocks_per_sm = ctx->tuning.blocks_per_sm;
     t->grab = ctx->tuning.grab;
     t->box_margin = ctx->tuning.box_margin;
+    return VLL_OK;
+}
+
+// ---- TINCreate_list (SubFunctions.cpp:2768-2846) ------------------------------
+static int tin_create_check(vll_context *ctx, const void *pts, int64_t n_pts,
+                            const double *min_max, double resolution, const void *tris,
+                            int64_t capacity, int64_t *count) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (!min_max || !count || (n_pts > 0 && !pts) || (capacity > 0 && !tris))
+        return fail(ctx, VLL_ERR_INVALID, "null argument");
+    if (n_pts < 0 || capacity < 0) return fail(ctx, VLL_ERR_INVALID, "negative count");
+    if (!(resolution > 0) || !(min_max[2] >= min_max[0]) || !(min_max[3] >= min_max[1]))
+        return fail(ctx, VLL_ERR_INVALID, "invalid resolution or extent");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    return VLL_OK;
+}
+
+int vll_tin_create_device(vll_context *ctx, const vll_point3 *d_pts, int64_t n_pts,
+                          const double min_max[4], double resolution, vll_tri *d_tris,
+                          int64_t capacity, int64_t *count) {
+    NvtxRange nvtx_range("vll_tin_create_device");
+    int rc = tin_create_check(ctx, d_pts, n_pts, min_max, resolution, d_tris, capacity, count);
+    if (rc) return rc;
+    std::string err;
+    rc = vll::run_tin_create(ctx->tin_work, d_pts, n_pts, min_max, resolution, d_tris, capacity,
+                             count, ctx->stream, &err);
+    if (rc) return fail(ctx, rc, err);
+    ctx->launches_total += 1;
+    return VLL_OK;
+}
+
+int vll_tin_create(vll_context *ctx, const vll_point3 *pts, int64_t n_pts, const double min_max[4],
+                   double resolution, vll_tri *tris, int64_t capacity, int64_t *count) {
+    NvtxRange nvtx_range("vll_tin_create");
+    int rc = tin_create_check(ctx, pts, n_pts, min_max, resolution, tris, capacity, count);
+    if (rc) return rc;
+    VLL_CUDA(ctx, ensure(ctx->tin_pts, (size_t)std::max<int64_t>(n_pts, 1) * sizeof(vll_point3)));
+    VLL_CUDA(ctx, ensure(ctx->tin_tris, (size_t)std::max<int64_t>(capacity, 1) * sizeof(vll_tri)));
+    if (n_pts > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(ctx->tin_pts.p, pts, (size_t)n_pts * sizeof(vll_point3),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+    std::string err;
+    rc = vll::run_tin_create(ctx->tin_work, (const vll_point3 *)ctx->tin_pts.p, n_pts, min_max,
+                             resolution, (vll_tri *)ctx->tin_tris.p, capacity, count, ctx->stream,
+                             &err);
+    if (rc) return fail(ctx, rc, err);
+    if (*count > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(tris, ctx->tin_tris.p, (size_t)*count * sizeof(vll_tri),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return VLL_OK;
 }
 

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "setsm_vll.h"
 
@@ -159,5 +161,17 @@ cudaError_t launch_orientation(const uint16_t *mag, const uint8_t *bin, uint32_t
                                int half, const double *wt, uint8_t *ori, cudaStream_t s);
 cudaError_t launch_pyramid(const uint16_t *src, uint32_t w, uint32_t h, const double *f,
                            uint16_t *out, cudaStream_t s);
+
+// vll_tin.cu: TINCreate_list.  TinWork holds the device work arrays between
+// calls (grown on demand); run_tin_create writes the ordered triangle list of
+// the n points (device) into d_tris (capacity entries; *count = the list's
+// length), returning a VLL_* status and a message in *err.
+struct TinWork {
+    std::vector<std::pair<void *, size_t>> bufs;
+};
+void tin_release(TinWork &w);
+int run_tin_create(TinWork &w, const vll_point3 *d_pts, int64_t n, const double min_max[4],
+                   double resolution, vll_tri *d_tris, int64_t capacity, int64_t *count,
+                   cudaStream_t s, std::string *err);
 
 }  // namespace vll

@@ -33,6 +33,7 @@
 #include <mutex>
 #include <vector>
 #include <cub/device/device_scan.cuh>
+#include <cuda.h>
 
 #include "vll_exact.cuh"
 #include "vll_internal.h"
@@ -98,7 +99,6 @@ __global__ void __launch_bounds__(256) prep_kernel(const LevelSet S,
                                                    const double *__restrict__ gsum,
                                                    const double *__restrict__ gcnt,
                                                    int32_t *__restrict__ node_k,
-                                                   int32_t *__restrict__ item_cnt,
                                                    unsigned long long *__restrict__ counters,
                                                    unsigned long long *__restrict__ acc_level) {
     unsigned long long acc = 0, acc_l = 0;
@@ -143,34 +143,10 @@ __global__ void __launch_bounds__(256) prep_kernel(const LevelSet S,
             }
         }
         node_k[gn] = K;
-        item_cnt[gn] = (K + 31) / 32;
     }
     if (acc_l) atomicAdd(&acc_level[cur], acc_l);
     for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0 && acc) atomicAdd(&counters[0], acc);
-}
-
-// Stops the rest of a planned (graph-replayed) pipeline when the slot or item
-// totals differ from the ones its buffers were sized for (the height ranges
-// changed since the plan was made): sets ctl[5], which the later kernels test.
-__global__ void guard_kernel(const int64_t *__restrict__ slot_total,
-                             const int64_t *__restrict__ item_total, int64_t slots, int64_t items,
-                             unsigned long long *__restrict__ ctl) {
-    if (threadIdx.x == 0 && blockIdx.x == 0 && (*slot_total != slots || *item_total != items))
-        ctl[5] = 1;
-}
-
-__global__ void __launch_bounds__(256) items_kernel(int64_t n, const int32_t *__restrict__ item_cnt,
-                                                    const int64_t *__restrict__ item_off,
-                                                    int64_t *__restrict__ items,
-                                                    const unsigned long long *__restrict__ stop) {
-    if (*stop) return;
-    for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < n;
-         pt += (int64_t)gridDim.x * blockDim.x) {
-        const int c = item_cnt[pt];
-        const int64_t o = item_off[pt];
-        for (int i = 0; i < c; ++i) items[o + i] = (pt << 16) | (int64_t)(32 * i);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -248,6 +224,241 @@ __device__ __forceinline__ bool near_trunc(double v) {
 }
 
 
+
+// ---------------------------------------------------------------------------
+// FindPeakNcc decisions over the slots of one node, lane-parallel (shared by
+// the window kernel's FP32 pass and the exact pass)
+// ---------------------------------------------------------------------------
+// FindPeakNcc's sign rule for the direction from b to a (setsm_code.cpp:6676-6692)
+__device__ __forceinline__ int dir_sign(double a, double b) {
+    double d;
+    if (a >= 0 && b >= 0)
+        d = a - b;
+    else if (a < 0 && b < 0)
+        d = -(fabs(a) - fabs(b));
+    else if (a >= 0 && b < 0)
+        d = 1;
+    else
+        d = -1;
+    return d > 0 ? 1 : (d < 0 ? -1 : 0);
+}
+
+__device__ __forceinline__ bool bit(const uint32_t *m, int k) { return (m[k >> 5] >> (k & 31)) & 1u; }
+__device__ __forceinline__ void set_bit(uint32_t *m, int k) { atomicOr(&m[k >> 5], 1u << (k & 31)); }
+
+// Index of the last evaluated slot before k (or -1); `carry` is the last
+// evaluated slot of earlier 32-slot groups.
+__device__ __forceinline__ int prev_eval(uint32_t mask, int lane, int carry) {
+    const uint32_t below = mask & ((1u << lane) - 1u);
+    return below ? (31 - __clz(below)) : carry;
+}
+
+// Bit masks over the slots of one node (kSlotCap at most), in shared memory.
+struct SlotMasks {
+    uint32_t evaluated[kSlotCap / 32];   // slot evaluated (not skipped / rejected)
+    uint32_t need[kSlotCap / 32];        // slot needs an exact FP64 value
+    uint32_t peak[kSlotCap / 32];        // slot is a FindPeakNcc peak
+};
+
+// One pass of FindPeakNcc's decisions over a node's K slot values, every lane
+// taking one slot of each 32-slot group:
+//  (a) the direction of each slot and whether its predecessor is a peak (a
+//      slot's direction depends only on it and the previous evaluated
+//      slot); near ties, and values near zero, mark both slots `need`;
+//  (a2) peaks whose rounding to rho*1000 could enter or reorder the top two
+//      (a peak more than 0.002 + 2 bands below the second best rounds
+//      strictly below it) and round ambiguously;
+//  (b) the maximum (max_WNCC), and slots near it that round ambiguously.
+// `val(k, ex)` gives slot k's value and whether it is exact (exact values
+// never need re-evaluation).  Returns the maximum.
+template <class Val>
+__device__ double scan_pass(const DevLevel &P, bool check_height_change, int K, SlotMasks &M,
+                            Val val, int lane) {
+    int carry = -1;
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        const int k = k0 + lane;
+        const uint32_t em = M.evaluated[k0 >> 5];
+        const bool ev = k < K && ((em >> lane) & 1u);
+        const int p_in = prev_eval(em, lane, -1);
+        const int p = p_in >= 0 ? k0 + p_in : carry;
+        bool need_me = false, need_p = false;
+        if (ev && P.cmr && p >= 0) {
+            int pp = -1;
+            const int pg = p >> 5, pl = p & 31;
+            const uint32_t pm = M.evaluated[pg] & ((1u << pl) - 1u);
+            if (pm) {
+                pp = (pg << 5) + 31 - __clz(pm);
+            } else {
+                for (int gi = pg - 1; gi >= 0 && pp < 0; --gi)
+                    if (M.evaluated[gi]) pp = (gi << 5) + 31 - __clz(M.evaluated[gi]);
+            }
+            bool ex_k, ex_p;
+            const double v = val(k, ex_k);
+            const double pv = val(p, ex_p);
+            if (!(ex_k && ex_p) && (fabs(v - pv) < kBand || fabs(v) < kBand || fabs(pv) < kBand)) {
+                need_me = !ex_k;
+                need_p = !ex_p;
+            }
+            // direction of k (td) and of p (dp): a peak at p needs dp > 0 and
+            // td < 0 (the first evaluated slot's direction is -1)
+            const int td = dir_sign(v, pv);
+            int dp = -1;
+            if (pp >= 0) {
+                bool ex_pp;
+                dp = dir_sign(pv, val(pp, ex_pp));
+            }
+            if (pv != -1 && dp > 0 && td < 0) set_bit(M.peak, p);
+        }
+        if (need_me) set_bit(M.need, k);
+        if (need_p) set_bit(M.need, p);
+        const uint32_t any = em & ((k0 + 32 <= K) ? 0xffffffffu : ((1u << (K - k0)) - 1u));
+        if (any) carry = k0 + 31 - __clz(any);
+    }
+    __syncwarp();
+    if (P.cmr) {
+        double b1 = -1e30, b2 = -1e30;
+        for (int k = lane; k < K; k += 32) {
+            if (!bit(M.peak, k)) continue;
+            bool ex;
+            const double v = val(k, ex);
+            if (v > b1) {
+                b2 = b1;
+                b1 = v;
+            } else if (v > b2) {
+                b2 = v;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double o1 = __shfl_xor_sync(0xffffffffu, b1, o);
+            const double o2 = __shfl_xor_sync(0xffffffffu, b2, o);
+            const double n1 = fmax(b1, o1);
+            const double n2 = fmax(fmin(b1, o1), fmax(b2, o2));
+            b1 = n1;
+            b2 = n2;
+        }
+        const double thr = (b2 > -1e29 ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
+        for (int k = lane; k < K; k += 32) {
+            if (!bit(M.peak, k)) continue;
+            bool ex;
+            const double v = val(k, ex);
+            if (!ex && v >= thr && near_round(v)) set_bit(M.need, k);
+        }
+    }
+    __syncwarp();
+    double m = -100;
+    for (int k = lane; k < K; k += 32) {
+        if (!bit(M.evaluated, k)) continue;
+        bool ex;
+        const double v = val(k, ex);
+        if (m < v) m = v;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (check_height_change) {
+        for (int k = lane; k < K; k += 32) {
+            if (!bit(M.evaluated, k)) continue;
+            bool ex;
+            const double v = val(k, ex);
+            if (!ex && v >= m - kBand && near_round(v)) set_bit(M.need, k);
+        }
+    }
+    __syncwarp();
+    return m;
+}
+
+// FindPeakNcc's ordered top-two fold over the marked peaks (one lane).
+template <class Val>
+__device__ void fold_peaks(const DevLevel &P, vll_nccresult &R, int K, int start_H,
+                           const uint32_t *peak, Val val) {
+    for (int i = 0; i < (K + 31) / 32; ++i) {
+        uint32_t pm = peak[i];
+        while (pm) {
+            const int b = __ffs(pm) - 1;
+            pm &= pm - 1;
+            const int p = (i << 5) + b;
+            bool ex;
+            const double pv = val(p, ex);
+            const float ph = slot_height(P, start_H, R.minHeight, p);
+            if (R.result4 < 10) R.result4 += 1;
+            const int16_t qpre = q_result(pv);
+            if (R.result0 < qpre) {
+                const double t1 = dq_result(R.result0);
+                R.result0 = qpre;
+                const float t2 = R.result2;
+                R.result2 = ph;
+                const int16_t q1 = q_result(t1);
+                if (R.result1 < q1) {
+                    R.result1 = q1;
+                    R.result3 = t2;
+                }
+            } else if (R.result1 < qpre) {
+                R.result1 = qpre;
+                R.result3 = ph;
+            }
+        }
+    }
+}
+
+// A node settled entirely in exact FP64 (eval_slot: the reference's
+// operation order), the warp's lanes evaluating 32 slots at a time; lane 0
+// folds each chunk into FindPeakNcc and the maximum in slot order, so no
+// per-slot buffer is needed.  Voxel rows get the exact flags and INCC.
+// `first` = this is the node's first evaluation (counted as evaluations and
+// written to the debug slot values), otherwise a re-evaluation.
+__device__ void node_exact_chunked(const DevLevel &P, int64_t pt, int K, const PatchSrc &S,
+                                   const PatchSrc &Sn, double cnt_g, double sum_g,
+                                   vll_nccresult R, vll_voxel *vrow, double *chunk, int lane,
+                                   bool first, unsigned long long &count) {
+    const vll_ugrid g = P.gp3[pt];
+    const int start_H = g.minHeight, end_H = g.maxHeight;
+    PeakState st;
+    peak_init(st);
+    double max_w = -100;
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        const int k = k0 + lane;
+        double out = (double)kNotEvaluated;
+        if (k < K) {
+            const float hgt = slot_height(P, start_H, R.minHeight, k);
+            if (hgt >= (float)start_H && hgt <= (float)end_H) {
+                const SlotOut o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
+                if (o.evaluated) {
+                    out = o.rho;
+                    if (vrow) {
+                        if (o.all_pos) vrow[k].flag_cal = 1;
+                        vrow[k].INCC = o.count_incc > 0
+                                           ? q_voxel(__ddiv_rn(o.sum_incc, o.count_incc))
+                                           : q_voxel(-1.0);
+                    }
+                    if (first && P.dbg_rho) P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
+                    count++;
+                } else if (o.orient_reject) {
+                    out = (double)kRejected;
+                    if (vrow) vrow[k].flag_cal = 0;
+                }
+            }
+        }
+        chunk[lane] = out;
+        __syncwarp();
+        if (lane == 0) {
+            const int n = min(32, K - k0);
+            for (int i = 0; i < n; ++i) {
+                const double v = chunk[i];
+                if (isinf(v)) continue;
+                if (P.cmr) find_peak(st, v, slot_height(P, start_H, R.minHeight, k0 + i), R);
+                if (max_w < v) max_w = v;
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        if (R.check_height_change) R.max_WNCC = q_result(max_w);
+        P.ncc[pt] = R;
+    }
+    __syncwarp();
+}
+
+
 // ---------------------------------------------------------------------------
 // window kernel
 // ---------------------------------------------------------------------------
@@ -261,9 +472,15 @@ __device__ __forceinline__ bool near_trunc(double v) {
 #endif
 constexpr int kWinWarps = VLL_WIN_WARPS;
 
+// Per-warp shared state of the window kernel: the node's RPC cubics, the
+// FP32 values and masks of its slots, and the exact pass's chunk.
 struct WinShared {
     double horner[2][4][4];          // [image][num/den poly][a0..a3]
     double hnorm[2][2];              // [image] {h_off, 1 / h_scale}
+    double chunk[32];                // exact values of one 32-slot chunk
+    float vals[kSlotCap];            // FP32 rho per slot (+inf skipped, -inf rejected)
+    SlotMasks m;
+    uint64_t mbar;                   // completion of the footprint's bulk copies
 };
 
 __host__ __device__ constexpr size_t win_boxes_offset() {
@@ -285,33 +502,43 @@ __device__ __forceinline__ void window_any(int H, const float4 *qr, int rbw, flo
     }
 }
 
-// One persistent launch over the (node, 32-slot) items of every level of the
-// set; items are in level order, so warps of a launch mostly run one window
-// size at a time.
+// One persistent launch over the nodes of every level of the set (a warp per
+// node, nodes taken from a global queue in level order).  Per node: the RPC
+// cubics once; then for each group of 32 height slots (a lane per slot) the
+// FP64 geometry, the staged footprints and the FP32 window statistics; then
+// FindPeakNcc / max_WNCC on the FP32 values in the warp.  A node whose every
+// decision lies outside the error band is written here; any other node is
+// queued for the exact pass with its FP32 values (NaN marking the slots that
+// need an exact value) in the pending buffer, or with offset -1 (evaluated
+// wholly in FP64 there) when the buffer is full.  Nodes of combined-level
+// INCC, or with more slots than kSlotCap, are evaluated here wholly in FP64.
 __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
-    const LevelSet LS, const int64_t *__restrict__ items, int64_t n_items,
-    const int64_t *__restrict__ slot_off, const double *__restrict__ gsum,
-    const double *__restrict__ gcnt, float2 *__restrict__ rho,
-    unsigned long long *__restrict__ counters, unsigned long long *__restrict__ queue,
-    int warp_quads, int grab, const unsigned long long *__restrict__ stop) {
+    const LevelSet LS, const int32_t *__restrict__ node_k, const double *__restrict__ gsum,
+    const double *__restrict__ gcnt, float *__restrict__ pend_vals, int64_t pend_cap,
+    int64_t *__restrict__ pend_node, int64_t *__restrict__ pend_off,
+    unsigned long long *__restrict__ counters, unsigned long long *__restrict__ ctl,
+    int warp_quads, int warp_raw, int grab) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (*stop) return;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     WinShared &W = reinterpret_cast<WinShared *>(smem_raw)[warp];
     float4 *boxes = reinterpret_cast<float4 *>(smem_raw + win_boxes_offset()) + (size_t)warp * warp_quads;
+    unsigned char *raw = smem_raw + win_boxes_offset() + (size_t)kWinWarps * warp_quads * sizeof(float4) +
+                         (size_t)warp * warp_raw;
+    if (lane == 0) mbar_init(&W.mbar);
+    __syncwarp();
+    uint32_t phase = 0;   // parity of the mbarrier phase the next copies complete
     unsigned long long evals = 0;
     for (;;) {
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(queue, (unsigned long long)grab);
+        if (lane == 0) base = atomicAdd(&ctl[0], (unsigned long long)grab);
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= (unsigned long long)n_items) break;
+        if (base >= (unsigned long long)LS.total) break;
         for (int gi = 0; gi < grab; ++gi) {
-            const int64_t it = (int64_t)base + gi;
-            if (it >= n_items) break;
-            const int64_t code = items[it];
-            const int64_t gn = code >> 16;
-            const int k0 = (int)(code & 0xFFFF);
+            const int64_t gn = (int64_t)base + gi;
+            if (gn >= LS.total) break;
+            const int K = node_k[gn];
+            if (K == 0) continue;
             const int lvl = level_of(LS, gn);
             const DevLevel &P = LS.lv[lvl];
             const int64_t pt = gn - __ldg(LS.base + lvl);
@@ -319,197 +546,277 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             const DevImage &ri = P.im[P.ref];
             const DevImage &tI = P.im[1];
             const bool voxels = P.vox && !P.cmr && !P.is_ra;
+            vll_voxel *vrow = voxels ? P.vox + P.vox_off[pt] : nullptr;
+            const vll_ugrid gg = P.gp3[pt];
+            const int start_H = gg.minHeight, end_H = gg.maxHeight;
+            // the record (as prep left it) is read again where it is written;
+            // per-node values below are reloaded where used, to keep them out
+            // of the registers of the window arithmetic
+            const int ncc_min = P.ncc[pt].minHeight;
+            const bool chc = P.ncc[pt].check_height_change != 0;
+            if (P.combined_incc || K > kSlotCap) {
+                // combined-level INCC (setsm_code.cpp:6378-6464: the windows at
+                // this level and the next finer one, the averaged orientation
+                // and both bounds tests), or a range longer than the shared
+                // slot buffer: the node goes to the exact pass, to be evaluated
+                // there wholly in FP64 (offset -2: not evaluated yet)
+                if (lane == 0) {
+                    const unsigned long long idx = atomicAdd(&ctl[2], 1ull);
+                    pend_node[idx] = gn;
+                    pend_off[idx] = -2;
+                }
+                continue;
+            }
             // 16-byte aligned image rows allow 128-bit staging loads
             const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
                                 ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
                                   reinterpret_cast<uintptr_t>(tI.img) |
                                   reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
             const double inv_s = 1.0 / (double)(1 << P.L);
-            const int64_t so = slot_off[gn];
-            const int K = (int)(slot_off[gn + 1] - so);
-            const int k = k0 + lane;
-            const vll_ugrid gg = P.gp3[pt];
-            const int start_H = gg.minHeight, end_H = gg.maxHeight;
-            const int ncc_min = P.ncc[pt].minHeight;
-            const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
-            const double cnt_g = gcnt ? gcnt[gn] : 0.0, sum_g = gsum ? gsum[gn] : 0.0;
-            if (P.combined_incc) {
-                // combined-level INCC (setsm_code.cpp:6378-6464): the windows
-                // at this level and the next finer one, the averaged
-                // orientation and both bounds tests, in exact FP64
-                // (eval_slot); the exact pass settles these nodes wholly.
-                if (k < K) {
-                    float rho_v = kNotEvaluated;
-                    const float hgt = slot_height(P, start_H, ncc_min, k);
-                    SlotOut o;
-                    o.evaluated = o.orient_reject = o.all_pos = false;
-                    if (hgt >= (float)start_H && hgt <= (float)end_H) {
-                        PatchSrc S, Sn;
-                        make_src(P, 1, S, Sn);
-                        o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
-                    }
-                    double incc = -1.0;
-                    if (o.evaluated) {
-                        rho_v = (float)o.rho;
-                        incc = o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc) : -1.0;
-                        evals++;
-                    } else if (o.orient_reject) {
-                        rho_v = kRejected;
-                    }
-                    rho[so + k] = make_float2(rho_v, (float)incc);
-                    if (P.dbg_rho && o.evaluated) P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
-                    if (voxels) {
-                        vll_voxel *v = P.vox + P.vox_off[pt] + k;
-                        if (o.orient_reject) v->flag_cal = 0;
-                        if (o.evaluated) {
-                            if (o.all_pos) v->flag_cal = 1;
-                            v->INCC = q_voxel(incc);
-                        }
-                    }
-                }
-                __syncwarp();
-                continue;
-            }
             // per-node RPC cubics: lanes 0..7 = (image, polynomial)
             if (lane < 8) {
                 const int im = lane >> 2, j = lane & 3;
                 const double *rpc = (im == 0 ? ri : tI).rpc;
-                node_horner_poly(rpc, lon, lat, j, W.horner[im][j]);
+                node_horner_poly(rpc, P.grid_wgs[2 * pt], P.grid_wgs[2 * pt + 1], j,
+                                 W.horner[im][j]);
                 if (j == 0) {
                     W.hnorm[im][0] = rpc[4];
                     W.hnorm[im][1] = 1.0 / rpc[9];
                 }
             }
+            if (lane < kSlotCap / 32) {
+                W.m.evaluated[lane] = 0;
+                W.m.need[lane] = 0;
+                W.m.peak[lane] = 0;
+            }
             __syncwarp();
-            // ---- per-lane geometry ----
-            int status = 0;   // 0 idle/skip, 1 orientation reject, 2 evaluate
-            double2 rp = make_double2(0, 0), tp = make_double2(0, 0);
-            int rot = kRotOffset;
-            float hgt = 0.f;
-            if (k < K) {
-                hgt = slot_height(P, start_H, ncc_min, k);
-                if (hgt >= (float)start_H && hgt <= (float)end_H) {
-                    bool edge = false;
-                    rp = fast_coord(W.horner[0], W.hnorm[0], ri, (double)hgt, inv_s, edge);
-                    tp = fast_coord(W.horner[1], W.hnorm[1], tI, (double)hgt, inv_s, edge);
-                    if (edge) {
-                        rp = to_pyramid(rpc_project(ri.rpc, ri.adj, lon, lat, (double)hgt), ri.sx, ri.sy, P.L);
-                        tp = to_pyramid(rpc_project(tI.rpc, tI.adj, lon, lat, (double)hgt), tI.sx, tI.sy, P.L);
-                    }
-                    if (in_image(rp, ri.w, ri.h) && in_image(tp, tI.w, tI.h)) {
-                        const int od = (int)ri.ori[(int64_t)(int)rp.y * ri.w + (int)rp.x] -
-                                       (int)tI.ori[(int64_t)(int)tp.y * tI.w + (int)tp.x];
-                        bool ok = true;
-                        if (!P.is_ra && P.L >= 3) {
-                            const double a = __dmul_rn((double)od, P.bin_angle);
-                            ok = a < 90 && a > -90;
+            for (int k0 = 0; k0 < K; k0 += 32) {
+                const int k = k0 + lane;
+                // ---- per-lane geometry ----
+                int status = 0;   // 0 idle/skip, 1 orientation reject, 2 evaluate
+                double2 rp = make_double2(0, 0), tp = make_double2(0, 0);
+                int rot = kRotOffset;
+                float hgt = 0.f;
+                if (k < K) {
+                    hgt = slot_height(P, start_H, ncc_min, k);
+                    if (hgt >= (float)start_H && hgt <= (float)end_H) {
+                        bool edge = false;
+                        rp = fast_coord(W.horner[0], W.hnorm[0], ri, (double)hgt, inv_s, edge);
+                        tp = fast_coord(W.horner[1], W.hnorm[1], tI, (double)hgt, inv_s, edge);
+                        if (edge) {
+                            const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
+                            rp = to_pyramid(rpc_project(ri.rpc, ri.adj, lon, lat, (double)hgt), ri.sx, ri.sy, P.L);
+                            tp = to_pyramid(rpc_project(tI.rpc, tI.adj, lon, lat, (double)hgt), tI.sx, tI.sy, P.L);
                         }
-                        status = ok ? 2 : 1;
-                        rot = 2 * od + kRotOffset;
+                        if (in_image(rp, ri.w, ri.h) && in_image(tp, tI.w, tI.h)) {
+                            const int od = (int)ri.ori[(int64_t)(int)rp.y * ri.w + (int)rp.x] -
+                                           (int)tI.ori[(int64_t)(int)tp.y * tI.w + (int)tp.x];
+                            bool ok = true;
+                            if (!P.is_ra && P.L >= 3) {
+                                const double a = __dmul_rn((double)od, P.bin_angle);
+                                ok = a < 90 && a > -90;
+                            }
+                            status = ok ? 2 : 1;
+                            rot = 2 * od + kRotOffset;
+                        }
                     }
                 }
-            }
-            // ---- footprint of the evaluating lanes ----
-            const float cf = (float)P.rot_cos[rot], sf = (float)P.rot_sin[rot];
-            const int rix = (int)floor(rp.x), riy = (int)floor(rp.y);
-            const int tix = (int)floor(tp.x), tiy = (int)floor(tp.y);
-            const int R = (int)ceilf((fabsf(cf) + fabsf(sf)) * (float)H) + 1;
-            const bool inside = status == 2 && rix - H >= 0 && riy - H >= 0 &&
-                                rix + H + 2 < (int)ri.w && riy + H + 2 < (int)ri.h && tix - R >= 0 &&
-                                tiy - R >= 0 && tix + R + 2 < (int)tI.w && tiy + R + 2 < (int)tI.h;
-            int rx0 = inside ? rix - H : INT_MAX, ry0 = inside ? riy - H : INT_MAX;
-            int rx1 = inside ? rix + H + 1 : INT_MIN, ry1 = inside ? riy + H + 1 : INT_MIN;
-            int tx0 = inside ? tix - R : INT_MAX, ty0 = inside ? tiy - R : INT_MAX;
-            int tx1 = inside ? tix + R + 1 : INT_MIN, ty1 = inside ? tiy + R + 1 : INT_MIN;
-            rx0 = __reduce_min_sync(0xffffffffu, rx0);
-            ry0 = __reduce_min_sync(0xffffffffu, ry0);
-            rx1 = __reduce_max_sync(0xffffffffu, rx1);
-            ry1 = __reduce_max_sync(0xffffffffu, ry1);
-            tx0 = __reduce_min_sync(0xffffffffu, tx0);
-            ty0 = __reduce_min_sync(0xffffffffu, ty0);
-            tx1 = __reduce_max_sync(0xffffffffu, tx1);
-            ty1 = __reduce_max_sync(0xffffffffu, ty1);
-            bool staged = false;
-            int rbw = 0, rbh = 0, tbw = 0;
-            if (__any_sync(0xffffffffu, inside)) {
-                const int rw = rx1 - rx0 + 1, tw = tx1 - tx0 + 1;
-                // odd row strides spread consecutive rows over the shared-memory bank groups
-                rbw = rw | 1;
-                rbh = ry1 - ry0 + 1;
-                tbw = tw | 1;
-                const int tbh = ty1 - ty0 + 1;
-                if (rbw * rbh + tbw * tbh <= warp_quads) {
-                    float sI = 0.f, sM = 0.f, tsI = 0.f, tsM = 0.f;
-                    if (lane == 0) {
-                        const int64_t pc = (int64_t)(ry0 + rbh / 2) * ri.w + (rx0 + rbw / 2);
-                        sI = (float)__ldg(ri.img + pc);
-                        sM = (float)__ldg(ri.mag + pc);
-                        const int64_t p2 = (int64_t)(ty0 + tbh / 2) * tI.w + (tx0 + tbw / 2);
-                        tsI = (float)__ldg(tI.img + p2);
-                        tsM = (float)__ldg(tI.mag + p2);
+                // ---- footprint of the evaluating lanes ----
+                const float cf = (float)P.rot_cos[rot], sf = (float)P.rot_sin[rot];
+                const int rix = (int)floor(rp.x), riy = (int)floor(rp.y);
+                const int tix = (int)floor(tp.x), tiy = (int)floor(tp.y);
+                // target footprint radius: the window is the square |col|, |row| <= H
+                // cut by the disc of radius H + 1, so a rotation moves its samples
+                // at most min((|c| + |s|) H, H + 1) from the centre (+1 for the
+                // bilinear neighbour and FP32 rounding)
+                const int R = min((int)ceilf((fabsf(cf) + fabsf(sf)) * (float)H) + 1, H + 2);
+                const bool inside = status == 2 && rix - H >= 0 && riy - H >= 0 &&
+                                    rix + H + 2 < (int)ri.w && riy + H + 2 < (int)ri.h && tix - R >= 0 &&
+                                    tiy - R >= 0 && tix + R + 2 < (int)tI.w && tiy + R + 2 < (int)tI.h;
+                int rx0 = inside ? rix - H : INT_MAX, ry0 = inside ? riy - H : INT_MAX;
+                int rx1 = inside ? rix + H + 1 : INT_MIN, ry1 = inside ? riy + H + 1 : INT_MIN;
+                int tx0 = inside ? tix - R : INT_MAX, ty0 = inside ? tiy - R : INT_MAX;
+                int tx1 = inside ? tix + R + 1 : INT_MIN, ty1 = inside ? tiy + R + 1 : INT_MIN;
+                rx0 = __reduce_min_sync(0xffffffffu, rx0);
+                ry0 = __reduce_min_sync(0xffffffffu, ry0);
+                rx1 = __reduce_max_sync(0xffffffffu, rx1);
+                ry1 = __reduce_max_sync(0xffffffffu, ry1);
+                tx0 = __reduce_min_sync(0xffffffffu, tx0);
+                ty0 = __reduce_min_sync(0xffffffffu, ty0);
+                tx1 = __reduce_max_sync(0xffffffffu, tx1);
+                ty1 = __reduce_max_sync(0xffffffffu, ty1);
+                bool staged = false;
+                int rbw = 0, rbh = 0, tbw = 0;
+                if (__any_sync(0xffffffffu, inside)) {
+                    const int rw = rx1 - rx0 + 1, tw = tx1 - tx0 + 1;
+                    // odd row strides spread consecutive rows over the shared-memory bank groups
+                    rbw = rw | 1;
+                    rbh = ry1 - ry0 + 1;
+                    tbw = tw | 1;
+                    const int tbh = ty1 - ty0 + 1;
+                    // raw rows of the boxes for the bulk copies: texels [xa, xa + 8 n)
+                    // of each row, covering the pairs' right texels
+                    const int rxa = rx0 & ~7, txa = tx0 & ~7;
+                    const int rnb = ((rx1 + 1 - rxa) / 8 + 1) * 16;
+                    const int tnb = ((tx1 + 1 - txa) / 8 + 1) * 16;
+                    const int raw_bytes = 2 * (rbh * rnb + tbh * tnb);
+                    if (rbw * rbh + tbw * tbh <= warp_quads && vec_ok && raw_bytes <= warp_raw) {
+                        // ---- bulk copies (TMA) of the raw rows, then conversion ----
+                        unsigned char *rI = raw, *rM = raw + rbh * rnb;
+                        unsigned char *tIr = raw + 2 * rbh * rnb, *tMr = tIr + tbh * tnb;
+                        if (lane == 0) mbar_arrive_expect(&W.mbar, (uint32_t)raw_bytes);
+                        __syncwarp();
+                        for (int i = lane; i < 2 * (rbh + tbh); i += 32) {
+                            const bool ref = i < 2 * rbh;
+                            const int j = ref ? i : i - 2 * rbh;
+                            const int bh = ref ? rbh : tbh;
+                            const bool magp = j >= bh;
+                            const int r = magp ? j - bh : j;
+                            const DevImage &im = ref ? ri : tI;
+                            const uint16_t *plane = magp ? im.mag : im.img;
+                            const int nb = ref ? rnb : tnb;
+                            const uint16_t *src =
+                                plane + (int64_t)((ref ? ry0 : ty0) + r) * im.w + (ref ? rxa : txa);
+                            unsigned char *dst = (ref ? (magp ? rM : rI) : (magp ? tMr : tIr)) + r * nb;
+                            bulk_g2s(dst, src, (uint32_t)nb, &W.mbar);
+                        }
+                        if (!mbar_wait(&W.mbar, phase, 2000000000ll)) {
+                            // the copies did not complete within ~1 s: report, wait
+                            // once more (bounded) for them, and stop this warp
+                            if (lane == 0) atomicExch(&counters[3], 1ull);
+                            mbar_wait(&W.mbar, phase, 2000000000ll);
+                            return;
+                        }
+                        phase ^= 1u;
+                        // box shifts: the centre texels
+                        const int rc = (rbh / 2) * rnb + 2 * (rx0 + rw / 2 - rxa);
+                        const int tc = (tbh / 2) * tnb + 2 * (tx0 + tw / 2 - txa);
+                        const float sI = (float)*reinterpret_cast<const uint16_t *>(rI + rc);
+                        const float sM = (float)*reinterpret_cast<const uint16_t *>(rM + rc);
+                        const float tsI = (float)*reinterpret_cast<const uint16_t *>(tIr + tc);
+                        const float tsM = (float)*reinterpret_cast<const uint16_t *>(tMr + tc);
+                        const bool z1 = stage_from_raw(boxes, rbw, rI, rM, rnb, rxa, rx0, rw, rbh,
+                                                       sI, sM, lane);
+                        const bool z2 = stage_from_raw(boxes + rbw * rbh, tbw, tIr, tMr, tnb, txa,
+                                                       tx0, tw, tbh, tsI, tsM, lane);
+                        // the raw rows are rewritten by the next copies
+                        fence_async_shared();
+                        __syncwarp();
+                        staged = !(z1 || z2);
+                    } else if (rbw * rbh + tbw * tbh <= warp_quads) {
+                        float sI = 0.f, sM = 0.f, tsI = 0.f, tsM = 0.f;
+                        if (lane == 0) {
+                            const int64_t pc = (int64_t)(ry0 + rbh / 2) * ri.w + (rx0 + rbw / 2);
+                            sI = (float)__ldg(ri.img + pc);
+                            sM = (float)__ldg(ri.mag + pc);
+                            const int64_t p2 = (int64_t)(ty0 + tbh / 2) * tI.w + (tx0 + tbw / 2);
+                            tsI = (float)__ldg(tI.img + p2);
+                            tsM = (float)__ldg(tI.mag + p2);
+                        }
+                        sI = __shfl_sync(0xffffffffu, sI, 0);
+                        sM = __shfl_sync(0xffffffffu, sM, 0);
+                        tsI = __shfl_sync(0xffffffffu, tsI, 0);
+                        tsM = __shfl_sync(0xffffffffu, tsM, 0);
+                        bool z1, z2;
+                        if (vec_ok) {
+                            z1 = stage_box_vec(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh, sI,
+                                               sM, lane);
+                            z2 = stage_box_vec(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0, ty0,
+                                               tw, tbh, tsI, tsM, lane);
+                        } else {
+                            z1 = stage_box_strided(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh,
+                                                   sI, sM, lane);
+                            z2 = stage_box_strided(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0,
+                                                   ty0, tw, tbh, tsI, tsM, lane);
+                        }
+                        __syncwarp();
+                        staged = !(z1 || z2);
                     }
-                    sI = __shfl_sync(0xffffffffu, sI, 0);
-                    sM = __shfl_sync(0xffffffffu, sM, 0);
-                    tsI = __shfl_sync(0xffffffffu, tsI, 0);
-                    tsM = __shfl_sync(0xffffffffu, tsM, 0);
-                    bool z1, z2;
-                    if (vec_ok) {
-                        z1 = stage_box_vec(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh, sI,
-                                           sM, lane);
-                        z2 = stage_box_vec(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0, ty0,
-                                           tw, tbh, tsI, tsM, lane);
+                }
+                float rho_v = kNotEvaluated, incc_v = 0.f;
+                bool all_pos = false;
+                if (status == 1) {
+                    rho_v = kRejected;
+                } else if (status == 2) {
+                    if (staged && inside) {
+                        float incc;
+                        bool unsure = false;
+                        window_any(H, boxes + (riy - H - ry0) * rbw + (rix - H - rx0), rbw,
+                                   (float)(rp.x - (double)rix), (float)(rp.y - (double)riy),
+                                   boxes + rbw * rbh + (tiy - ty0) * tbw + (tix - tx0), tbw,
+                                   (float)(tp.x - (double)tix), (float)(tp.y - (double)tiy), cf, sf,
+                                   incc, unsure);
+                        const bool has = incc != -2.0f;
+                        const double incc_d = has ? (double)incc : -1.0;
+                        double rho_d;
+                        const double cnt_g = gcnt ? gcnt[gn] : 0.0;
+                        if (P.check_ortho && cnt_g > 0)
+                            rho_d = has ? incc_d * P.alpha + (gsum[gn] / cnt_g) * P.beta
+                                        : __ddiv_rn(0.0, 0.0);
+                        else
+                            rho_d = incc_d;
+                        rho_v = (float)rho_d;
+                        incc_v = unsure ? __int_as_float(0x7fc00000) : (float)incc_d;
+                        all_pos = true;   // window inside the image, no zero texels
                     } else {
-                        z1 = stage_box_strided(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh,
-                                               sI, sM, lane);
-                        z2 = stage_box_strided(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0,
-                                               ty0, tw, tbh, tsI, tsM, lane);
+                        // window not staged (near an image edge, a zero texel in
+                        // the boxes, or boxes beyond the budget): the exact pass
+                        // evaluates the slot in FP64
+                        rho_v = 0.f;
+                        incc_v = __int_as_float(0x7fc00000);
                     }
-                    __syncwarp();
-                    staged = !(z1 || z2);
+                    evals++;
                 }
+
+                const bool ev = k < K && status == 2;
+                const bool nd = ev && (isnan(incc_v) || (voxels && near_trunc((double)incc_v)));
+                if (k < K) W.vals[k] = rho_v;
+                const uint32_t em = __ballot_sync(0xffffffffu, ev);
+                const uint32_t nm = __ballot_sync(0xffffffffu, nd);
+                if (lane == 0) {
+                    W.m.evaluated[k0 >> 5] = em;
+                    W.m.need[k0 >> 5] = nm;
+                }
+                if (P.dbg_rho && status == 2) P.dbg_rho[P.dbg_off[pt] + k] = (double)rho_v;
+                if (k < K && voxels) {
+                    vll_voxel *v = vrow + k;
+                    if (status == 1) v->flag_cal = 0;
+                    if (status == 2) {
+                        if (all_pos) v->flag_cal = 1;
+                        v->INCC = q_voxel(isnan(incc_v) ? 0.0 : (double)incc_v);
+                    }
+                }
+                __syncwarp();
             }
-            float rho_v = kNotEvaluated, incc_v = 0.f;
-            bool all_pos = false;
-            if (status == 1) {
-                rho_v = kRejected;
-            } else if (status == 2) {
-                if (staged && inside) {
-                    float incc;
-                    bool unsure = false;
-                    window_any(H, boxes + (riy - H - ry0) * rbw + (rix - H - rx0), rbw,
-                               (float)(rp.x - (double)rix), (float)(rp.y - (double)riy),
-                               boxes + rbw * rbh + (tiy - ty0) * tbw + (tix - tx0), tbw,
-                               (float)(tp.x - (double)tix), (float)(tp.y - (double)tiy), cf, sf,
-                               incc, unsure);
-                    const bool has = incc != -2.0f;
-                    const double incc_d = has ? (double)incc : -1.0;
-                    double rho_d;
-                    if (P.check_ortho && cnt_g > 0)
-                        rho_d = has ? incc_d * P.alpha + (sum_g / cnt_g) * P.beta : __ddiv_rn(0.0, 0.0);
-                    else
-                        rho_d = incc_d;
-                    rho_v = (float)rho_d;
-                    incc_v = unsure ? __int_as_float(0x7fc00000) : (float)incc_d;
-                    all_pos = true;   // window inside the image, no zero texels
-                } else {
-                    PatchSrc S, Sn;
-                    make_src(P, 1, S, Sn);
-                    const SlotOut o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
-                    all_pos = o.all_pos;
-                    rho_v = (float)o.rho;
-                    incc_v = (float)(o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc) : -1.0);
+            // FindPeakNcc and max_WNCC on the FP32 values
+            auto fval = [&](int kk, bool &ex) {
+                ex = false;
+                return (double)W.vals[kk];
+            };
+            const double max_w = scan_pass(P, chc, K, W.m, fval, lane);
+            int n_need = 0;
+            for (int i = 0; i < (K + 31) / 32; ++i) n_need += __popc(W.m.need[i]);
+            if (n_need == 0) {
+                if (lane == 0) {
+                    vll_nccresult R = P.ncc[pt];
+                    if (P.cmr) fold_peaks(P, R, K, start_H, W.m.peak, fval);
+                    if (R.check_height_change) R.max_WNCC = q_result(max_w);
+                    P.ncc[pt] = R;
                 }
-                evals++;
-            }
-            if (k < K) rho[so + k] = make_float2(rho_v, incc_v);
-            if (P.dbg_rho && status == 2) P.dbg_rho[P.dbg_off[pt] + k] = (double)rho_v;
-            if (k < K && voxels) {
-                vll_voxel *v = P.vox + P.vox_off[pt] + k;
-                if (status == 1) v->flag_cal = 0;
-                if (status == 2) {
-                    if (all_pos) v->flag_cal = 1;
-                    v->INCC = q_voxel(isnan(incc_v) ? 0.0 : (double)incc_v);
+            } else {
+                long long off = -1;
+                if (lane == 0) {
+                    off = (long long)atomicAdd(&ctl[4], (unsigned long long)K);
+                    if (off + K > pend_cap) off = -1;
+                    const unsigned long long idx = atomicAdd(&ctl[2], 1ull);
+                    pend_node[idx] = gn;
+                    pend_off[idx] = off;
                 }
+                off = __shfl_sync(0xffffffffu, off, 0);
+                if (off >= 0)
+                    for (int kk = lane; kk < K; kk += 32)
+                        pend_vals[off + kk] = bit(W.m.need, kk) ? __int_as_float(0x7fc00000)
+                                                                : W.vals[kk];
             }
             __syncwarp();
         }
@@ -519,191 +826,20 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// scan kernel: one thread per node over the FP32 slot values
-// ---------------------------------------------------------------------------
-// FindPeakNcc's sign rule for the direction from b to a (setsm_code.cpp:6676-6692)
-__device__ __forceinline__ int dir_sign(double a, double b) {
-    double d;
-    if (a >= 0 && b >= 0)
-        d = a - b;
-    else if (a < 0 && b < 0)
-        d = -(fabs(a) - fabs(b));
-    else if (a >= 0 && b < 0)
-        d = 1;
-    else
-        d = -1;
-    return d > 0 ? 1 : (d < 0 ? -1 : 0);
-}
-
-// The FindPeakNcc scan and max_WNCC of every node on its FP32 values: a node
-// whose every decision lies outside the band kBand of its boundary (direction
-// ties and signs, rounding of the top-two peaks and of the maximum, voxel
-// truncation) gets its results written here; any other node is queued for the
-// exact FP64 pass (peaks_kernel).
-//
-// A persistent state machine: every lane advances one slot of its current
-// node per iteration and fetches its next node from a queue (warp-aggregated
-// atomics) when its node is done, so lanes of a warp stay busy whatever the
-// spread of K (8..512) among the nodes they hold.  One pass over the slots:
-// two of the checks need the node's final maximum and top two -- whether a
-// slot at or near the maximum rounds ambiguously, and whether a peak at or
-// above the top-two threshold does; both are monotone in the value, so the
-// maximum over the ambiguously rounding slots (and over such peaks), kept
-// during the pass, decides them exactly at its end.
-__global__ void __launch_bounds__(256) scan_queue_kernel(const LevelSet LS,
-                                                         const int64_t *__restrict__ slot_off,
-                                                         const float2 *__restrict__ rho,
-                                                         int64_t *__restrict__ pending,
-                                                         unsigned long long *__restrict__ ctl) {
-    if (ctl[5]) return;
-    const int lane = threadIdx.x & 31;
-    unsigned long long *queue = ctl + 4;
-    // per-lane state
-    bool active = true;       // this lane still has (or may fetch) work
-    bool have = false;        // a node is loaded
-    int64_t gn = 0, pt = 0;
-    const DevLevel *Pp = nullptr;
-    const float2 *rv = nullptr;
-    int K = 0, k = 0, check_rho = 0, direction = 0, start_H = 0;
-    bool need = false, voxels = false;
-    double pre_rho = -1.0, max_w = -100, b1 = -1e30, b2 = -1e30;
-    double max_amb = -1e30, max_amb_peak = -1e30;   // ambiguous roundings seen
-    float pre_h = 0.f;
-    vll_nccresult R;
-    for (;;) {
-        // ---- fetch nodes for the lanes that need one --------------------------
-        const bool want = active && !have;
-        const uint32_t wm = __ballot_sync(0xffffffffu, want);
-        if (wm) {
-            const int leader = __ffs(wm) - 1;
-            unsigned long long b = 0;
-            if (lane == leader) b = atomicAdd(queue, (unsigned long long)__popc(wm));
-            b = __shfl_sync(0xffffffffu, b, leader);
-            if (want) {
-                const unsigned long long idx = b + __popc(wm & ((1u << lane) - 1u));
-                if (idx >= (unsigned long long)LS.total) {
-                    active = false;
-                } else {
-                    gn = (int64_t)idx;
-                    const int64_t so = slot_off[gn];
-                    K = (int)(slot_off[gn + 1] - so);
-                    if (K > 0) {
-                        const int lvl = level_of(LS, gn);
-                        Pp = LS.lv + lvl;
-                        pt = gn - __ldg(LS.base + lvl);
-                        rv = rho + so;
-                        R = Pp->ncc[pt];
-                        start_H = Pp->gp3[pt].minHeight;
-                        voxels = Pp->vox && !Pp->cmr && !Pp->is_ra;
-                        need = K > kSlotCap;
-                        k = 0;
-                        check_rho = 0;
-                        max_amb = -1e30;
-                        max_amb_peak = -1e30;
-                        direction = 0;
-                        pre_rho = -1.0;
-                        max_w = -100;
-                        b1 = -1e30;
-                        b2 = -1e30;
-                        pre_h = 0.f;
-                        have = true;
-                    }
-                }
-            }
-        }
-        if (!__any_sync(0xffffffffu, active)) break;
-        // ---- one slot of the current node -------------------------------------
-        if (have) {
-            const DevLevel &P = *Pp;
-            if (!need && k < K) {
-                const float2 v2 = __ldg(rv + k);
-                if (v2.x != kNotEvaluated && v2.x != kRejected) {
-                    const double v = (double)v2.x;
-                    if (isnan(v2.y) || (voxels && near_trunc((double)v2.y))) need = true;
-                    if (near_round(v) && v > max_amb) max_amb = v;
-                    if (P.cmr) {
-                        if (check_rho && (fabs(v - pre_rho) < kBand || fabs(v) < kBand ||
-                                          fabs(pre_rho) < kBand))
-                            need = true;
-                        int td = dir_sign(v, pre_rho);
-                        if (!check_rho) {
-                            check_rho = 1;
-                            td = -1;
-                        } else if (pre_rho != -1 && direction > 0 && td < 0) {
-                            if (near_round(pre_rho) && pre_rho > max_amb_peak)
-                                max_amb_peak = pre_rho;
-                            if (pre_rho > b1) {
-                                b2 = b1;
-                                b1 = pre_rho;
-                            } else if (pre_rho > b2) {
-                                b2 = pre_rho;
-                            }
-                            if (R.result4 < 10) R.result4 += 1;
-                            const int16_t qpre = q_result(pre_rho);
-                            if (R.result0 < qpre) {
-                                const double t1 = dq_result(R.result0);
-                                R.result0 = qpre;
-                                const float t2 = R.result2;
-                                R.result2 = pre_h;
-                                const int16_t q1 = q_result(t1);
-                                if (R.result1 < q1) {
-                                    R.result1 = q1;
-                                    R.result3 = t2;
-                                }
-                            } else if (R.result1 < qpre) {
-                                R.result1 = qpre;
-                                R.result3 = pre_h;
-                            }
-                        }
-                        pre_rho = v;
-                        pre_h = slot_height(P, start_H, R.minHeight, k);
-                        direction = td;
-                    }
-                    if (max_w < v) max_w = v;
-                }
-                ++k;
-            }
-            if (!need && k >= K) {
-                // rounding of the maximum, and of peaks that can reach the top
-                // two (a peak more than 0.002 + 2 bands below the second best
-                // rounds strictly below it)
-                const double thr = (b2 > -1e29 ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
-                if (R.check_height_change && max_amb >= max_w - kBand) need = true;
-                if (P.cmr && max_amb_peak > -1e29 && max_amb_peak >= thr) need = true;
-            }
-            if (need || k >= K) {
-                if (need) {
-                    pending[atomicAdd(&ctl[2], 1ull)] = gn;
-                    atomicAdd(&ctl[3], 1ull);
-                } else {
-                    if (R.check_height_change) R.max_WNCC = q_result(max_w);
-                    P.ncc[pt] = R;
-                }
-                have = false;
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// peak kernel: one warp per node
+// peak kernel: the exact pass, one warp per queued node
 // ---------------------------------------------------------------------------
 constexpr int kPeakWarps = 4;
 
 struct WarpShared {
     float rho[kSlotCap];
-    uint32_t evaluated[kSlotCap / 32];
-    uint32_t need[kSlotCap / 32];
+    SlotMasks m;
     uint32_t exact[kSlotCap / 32];
-    uint32_t peak[kSlotCap / 32];
     int exact_k[kExactCap];
     double exact_rho[kExactCap];
     double exact_incc[kExactCap];
+    double chunk[32];
     int n_exact;
 };
-
-__device__ __forceinline__ bool bit(const uint32_t *m, int k) { return (m[k >> 5] >> (k & 31)) & 1u; }
-__device__ __forceinline__ void set_bit(uint32_t *m, int k) { atomicOr(&m[k >> 5], 1u << (k & 31)); }
 
 // value of slot k for the scan: exact if re-checked, else the FP32 one
 __device__ __forceinline__ double slot_value(const WarpShared &w, int k, bool &ex) {
@@ -713,13 +849,6 @@ __device__ __forceinline__ double slot_value(const WarpShared &w, int k, bool &e
             if (w.exact_k[i] == k) return w.exact_rho[i];
     }
     return (double)w.rho[k];
-}
-
-// Index of the last evaluated slot before k (or -1); `carry` is the last
-// evaluated slot of earlier 32-slot groups.
-__device__ __forceinline__ int prev_eval(uint32_t mask, int lane, int carry) {
-    const uint32_t below = mask & ((1u << lane) - 1u);
-    return below ? (31 - __clz(below)) : carry;
 }
 
 // Exact FP64 evaluation of one slot by the whole warp, bit-identical with
@@ -845,52 +974,6 @@ __device__ __noinline__ SlotOut eval_slot_warp(const DevLevel &P, int64_t pt, co
     return o;
 }
 
-// A node settled entirely in exact FP64, the warp's lanes evaluating 32 slots
-// at a time (eval_slot: the reference's operation order).  The exact values
-// overwrite the node's slot buffer (one double per float2 slot, markers kept
-// as +-inf), then lane 0 runs FindPeakNcc and the maximum over them and writes
-// the node's results; voxel rows get the exact INCC.
-__device__ void node_exact_warp(const DevLevel &P, int64_t pt, int K, float2 *rv,
-                                const PatchSrc &S, const PatchSrc &Sn, double cnt_g, double sum_g,
-                                vll_nccresult R, vll_voxel *vrow, int lane,
-                                unsigned long long &rechecks) {
-    const int start_H = P.gp3[pt].minHeight;
-    double *dv = reinterpret_cast<double *>(rv);
-    for (int k0 = 0; k0 < K; k0 += 32) {
-        const int k = k0 + lane;
-        if (k < K) {
-            const float2 v = rv[k];
-            double out = (double)v.x;   // markers stay +-inf
-            if (v.x != kNotEvaluated && v.x != kRejected) {
-                const float hgt = slot_height(P, start_H, R.minHeight, k);
-                const SlotOut o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
-                out = o.rho;
-                if (vrow) {
-                    if (o.all_pos) vrow[k].flag_cal = 1;
-                    vrow[k].INCC = o.count_incc > 0 ? q_voxel(__ddiv_rn(o.sum_incc, o.count_incc))
-                                                     : q_voxel(-1.0);
-                }
-                rechecks++;
-            }
-            dv[k] = out;
-        }
-    }
-    __syncwarp();
-    if (lane == 0) {
-        PeakState st;
-        peak_init(st);
-        double max_w = -100;
-        for (int k = 0; k < K; ++k) {
-            const double v = dv[k];
-            if (isinf(v)) continue;
-            if (P.cmr) find_peak(st, v, slot_height(P, start_H, R.minHeight, k), R);
-            if (max_w < v) max_w = v;
-        }
-        if (R.check_height_change) R.max_WNCC = q_result(max_w);
-        P.ncc[pt] = R;
-    }
-    __syncwarp();
-}
 
 // bytes of eval_slot_warp scratch for window half-size H
 __host__ __device__ constexpr size_t exact_scratch_bytes(int H) {
@@ -911,32 +994,35 @@ __device__ __forceinline__ SlotOut eval_slot_warp_any(const DevLevel &P, int64_t
     }
 }
 
-// The exact path for the nodes the scan kernel could not settle in FP32.
+// The exact pass for the nodes the window kernel could not settle in FP32:
+// the decisions within the error band are re-taken on exact FP64 values of
+// the slots involved (rounds of scan and re-evaluation); a node with more
+// slots to re-evaluate than kExactCap, or still unsettled after kMaxRounds,
+// or queued without its FP32 values, is evaluated wholly in FP64.
 // `max_h`: the largest window half-size of the level set (scratch layout).
 __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
-    const LevelSet LS, int max_h, const int64_t *__restrict__ slot_off,
-    const float2 *__restrict__ rho, const double *__restrict__ gsum, const double *__restrict__ gcnt,
-    unsigned long long *__restrict__ counters, unsigned long long *__restrict__ queue,
-    const int64_t *__restrict__ pending, const unsigned long long *__restrict__ n_pending,
-    const unsigned long long *__restrict__ stop) {
+    const LevelSet LS, int max_h, const int32_t *__restrict__ node_k,
+    const float *__restrict__ pend_vals, const int64_t *__restrict__ pend_node,
+    const int64_t *__restrict__ pend_off, const double *__restrict__ gsum,
+    const double *__restrict__ gcnt, unsigned long long *__restrict__ counters,
+    unsigned long long *__restrict__ ctl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    if (*stop) return;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     WarpShared &W = reinterpret_cast<WarpShared *>(smem_raw)[warp];
     constexpr size_t ws = (sizeof(WarpShared) + 15) & ~(size_t)15;
     const size_t xs = (exact_scratch_bytes(max_h) + 15) & ~(size_t)15;
     double *boxes = reinterpret_cast<double *>(smem_raw + ws * kPeakWarps + xs * warp);
-    unsigned long long rechecks = 0;
-    const unsigned long long n_pend = *n_pending;
+    unsigned long long rechecks = 0, evals = 0;
+    const unsigned long long n_pend = ctl[2];
     for (;;) {
         unsigned long long idx = 0;
-        if (lane == 0) idx = atomicAdd(queue, 1ull);
+        if (lane == 0) idx = atomicAdd(&ctl[1], 1ull);
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= n_pend) break;
-        const int64_t gn = pending[idx];
-        const int64_t so = slot_off[gn];
-        const int K = (int)(slot_off[gn + 1] - so);
+        const int64_t gn = pend_node[idx];
+        const int64_t off = pend_off[idx];
+        const int K = node_k[gn];
         if (K == 0) continue;
         const int lvl = level_of(LS, gn);
         const DevLevel &P = LS.lv[lvl];
@@ -948,179 +1034,66 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
         const int start_H = P.gp3[pt].minHeight;
         const double cnt_g = gcnt ? gcnt[gn] : 0.0, sum_g = gsum ? gsum[gn] : 0.0;
         vll_voxel *vrow = voxels ? P.vox + P.vox_off[pt] : nullptr;
-        if (K > kSlotCap || P.combined_incc) {
-            // more slots than the shared scan buffer holds, or a combined-level
-            // INCC node (whose per-slot re-checks need both levels): all slots
-            // exactly
-            node_exact_warp(P, pt, K, const_cast<float2 *>(rho) + so, S, Sn, cnt_g, sum_g, R, vrow,
-                            lane, rechecks);
+        if (off < 0 || K > kSlotCap || P.combined_incc) {
+            // queued without FP32 values: not evaluated yet (-2: combined-level
+            // INCC or more slots than kSlotCap), or the pending buffer was full
+            const bool first = off == -2;
+            if (lane == 0) atomicAdd(&counters[5], 1ull);
+            node_exact_chunked(P, pt, K, S, Sn, cnt_g, sum_g, R, vrow, W.chunk, lane, first,
+                               first ? evals : rechecks);
             continue;
         }
-        for (int i = lane; i < kSlotCap / 32; i += 32) {
-            W.evaluated[i] = 0;
-            W.need[i] = 0;
-            W.exact[i] = 0;
-            W.peak[i] = 0;
+        if (lane < kSlotCap / 32) {
+            W.m.evaluated[lane] = 0;
+            W.m.need[lane] = 0;
+            W.m.peak[lane] = 0;
+            W.exact[lane] = 0;
         }
         if (lane == 0) W.n_exact = 0;
         __syncwarp();
         for (int k0 = 0; k0 < K; k0 += 32) {
             const int k = k0 + lane;
-            float2 v = make_float2(kNotEvaluated, 0.f);
-            if (k < K) v = rho[so + k];
-            const bool ev = k < K && v.x != kNotEvaluated && v.x != kRejected;
-            const bool nd = ev && (isnan(v.y) || (voxels && near_trunc((double)v.y)));
+            float v = kNotEvaluated;
+            if (k < K) v = pend_vals[off + k];
+            const bool ev = k < K && !isinf(v);
+            const bool nd = ev && isnan(v);
             const uint32_t em = __ballot_sync(0xffffffffu, ev);
             const uint32_t nm = __ballot_sync(0xffffffffu, nd);
-            if (k < K) W.rho[k] = v.x;
+            if (k < K) W.rho[k] = nd ? 0.f : v;
             if (lane == 0) {
-                W.evaluated[k0 >> 5] = em;
-                W.need[k0 >> 5] = nm;
+                W.m.evaluated[k0 >> 5] = em;
+                W.m.need[k0 >> 5] = nm;
             }
         }
         __syncwarp();
+        auto xval = [&](int kk, bool &ex) { return slot_value(W, kk, ex); };
         // ---- scan, re-check, repeat ----
         double max_w = -100;
         bool redone = false;
         for (int round = 0;; ++round) {
-            // (a) directions, near ties and peaks, lane-parallel per 32-slot group
-            int carry = -1;
-            for (int k0 = 0; k0 < K; k0 += 32) {
-                const int k = k0 + lane;
-                const uint32_t em = W.evaluated[k0 >> 5];
-                const bool ev = k < K && ((em >> lane) & 1u);
-                // previous evaluated slot, and the one before it
-                const int p_in = prev_eval(em, lane, -1);
-                const int p = p_in >= 0 ? k0 + p_in : carry;
-                int pp = -1;
-                if (p >= 0) {
-                    const int pg = p >> 5, pl = p & 31;
-                    const uint32_t pm = W.evaluated[pg] & ((1u << pl) - 1u);
-                    if (pm)
-                        pp = (pg << 5) + 31 - __clz(pm);
-                    else {
-                        for (int gi = pg - 1; gi >= 0 && pp < 0; --gi)
-                            if (W.evaluated[gi]) pp = (gi << 5) + 31 - __clz(W.evaluated[gi]);
-                    }
-                }
-                bool need_me = false, need_p = false;
-                if (ev) {
-                    bool ex_k, ex_p = true;
-                    const double v = slot_value(W, k, ex_k);
-                    if (P.cmr && p >= 0) {
-                        const double pv = slot_value(W, p, ex_p);
-                        if (!(ex_k && ex_p) &&
-                            (fabs(v - pv) < kBand || fabs(v) < kBand || fabs(pv) < kBand)) {
-                            need_me = !ex_k;
-                            need_p = !ex_p;
-                        }
-                        // direction of k (td) and of p (dp): a peak at p needs
-                        // dp > 0 and td < 0 (first evaluated slot: td = -1)
-                        auto sgn = [](double a, double b) {
-                            double d;
-                            if (a >= 0 && b >= 0)
-                                d = a - b;
-                            else if (a < 0 && b < 0)
-                                d = -(fabs(a) - fabs(b));
-                            else if (a >= 0 && b < 0)
-                                d = 1;
-                            else
-                                d = -1;
-                            return d > 0 ? 1 : (d < 0 ? -1 : 0);
-                        };
-                        const int td = sgn(v, pv);
-                        int dp = -1;
-                        if (pp >= 0) {
-                            bool ex_pp;
-                            const double ppv = slot_value(W, pp, ex_pp);
-                            dp = sgn(pv, ppv);
-                        }
-                        const bool is_peak = pv != -1 && dp > 0 && td < 0;
-                        if (is_peak) set_bit(W.peak, p);
-                    }
-                }
-                if (need_me) set_bit(W.need, k);
-                if (need_p) set_bit(W.need, p);
-                const uint32_t any = em & ((k0 + 32 <= K) ? 0xffffffffu : ((1u << (K - k0)) - 1u));
-                if (any) carry = k0 + 31 - __clz(any);
-            }
-            __syncwarp();
-            // (a2) rounding of peak values that can reach the top two: a peak
-            // more than 0.002 (+ the band) below the second-best peak rounds
-            // strictly below it and can neither enter nor reorder the top two
-            if (P.cmr) {
-                double b1 = -1e30, b2 = -1e30;
-                for (int k = lane; k < K; k += 32) {
-                    if (!bit(W.peak, k)) continue;
-                    bool ex;
-                    const double v = slot_value(W, k, ex);
-                    if (v > b1) {
-                        b2 = b1;
-                        b1 = v;
-                    } else if (v > b2) {
-                        b2 = v;
-                    }
-                }
-#pragma unroll
-                for (int o = 16; o; o >>= 1) {
-                    const double o1 = __shfl_xor_sync(0xffffffffu, b1, o);
-                    const double o2 = __shfl_xor_sync(0xffffffffu, b2, o);
-                    const double n1 = fmax(b1, o1);
-                    const double n2 = fmax(fmin(b1, o1), fmax(b2, o2));
-                    b1 = n1;
-                    b2 = n2;
-                }
-                const double thr = (b2 > -1e29 ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
-                for (int k = lane; k < K; k += 32) {
-                    if (!bit(W.peak, k)) continue;
-                    bool ex;
-                    const double v = slot_value(W, k, ex);
-                    if (!ex && v >= thr && near_round(v)) set_bit(W.need, k);
-                }
-            }
-            __syncwarp();
-            // (b) the maximum and its rounding
-            double m = -100;
-            for (int k = lane; k < K; k += 32) {
-                if (!bit(W.evaluated, k)) continue;
-                bool ex;
-                const double v = slot_value(W, k, ex);
-                if (m < v) m = v;
-            }
-#pragma unroll
-            for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-            max_w = m;
-            if (R.check_height_change) {
-                for (int k = lane; k < K; k += 32) {
-                    if (!bit(W.evaluated, k)) continue;
-                    bool ex;
-                    const double v = slot_value(W, k, ex);
-                    if (!ex && v >= max_w - kBand && near_round(v)) set_bit(W.need, k);
-                }
-            }
-            __syncwarp();
-            // (c) slots still needing an exact value
+            max_w = scan_pass(P, R.check_height_change != 0, K, W.m, xval, lane);
+            // slots still needing an exact value
             int n_need = 0;
-            for (int i = 0; i < (K + 31) / 32; ++i) n_need += __popc(W.need[i] & ~W.exact[i]);
+            for (int i = 0; i < (K + 31) / 32; ++i) n_need += __popc(W.m.need[i] & ~W.exact[i]);
             if (n_need == 0) break;
             const bool overflow = W.n_exact + n_need > kExactCap || round + 1 >= kMaxRounds;
             if (lane == 0) atomicAdd(&counters[6], 1ull);
             if (overflow) {
                 if (lane == 0) atomicAdd(&counters[5], 1ull);
                 // give up on the FP32 values: the whole node exactly
-                node_exact_warp(P, pt, K, const_cast<float2 *>(rho) + so, S, Sn, cnt_g, sum_g, R,
-                                vrow, lane, rechecks);
+                node_exact_chunked(P, pt, K, S, Sn, cnt_g, sum_g, R, vrow, W.chunk, lane, false,
+                                   rechecks);
                 redone = true;   // results already written
                 break;
             }
             // compact the list and evaluate it lane-parallel in FP64
             int base = W.n_exact;
             for (int i = 0; i < (K + 31) / 32; ++i) {
-                const uint32_t todo = W.need[i] & ~W.exact[i];
+                const uint32_t todo = W.m.need[i] & ~W.exact[i];
                 const int k = (i << 5) + lane;
                 const bool mine = (todo >> lane) & 1u;
-                const int off = __popc(todo & ((1u << lane) - 1u));
-                if (mine) W.exact_k[base + off] = k;
+                const int o = __popc(todo & ((1u << lane) - 1u));
+                if (mine) W.exact_k[base + o] = k;
                 base += __popc(todo);
             }
             __syncwarp();
@@ -1133,7 +1106,10 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
                 if (lane == 0) {
                     W.exact_rho[j] = o.rho;
                     W.exact_incc[j] = o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc) : -1.0;
-                    if (vrow) vrow[k].INCC = q_voxel(W.exact_incc[j]);
+                    if (vrow) {
+                        if (o.all_pos) vrow[k].flag_cal = 1;
+                        vrow[k].INCC = q_voxel(W.exact_incc[j]);
+                    }
                     rechecks++;
                 }
                 __syncwarp();
@@ -1141,49 +1117,26 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
             __syncwarp();
             for (int j = W.n_exact + lane; j < base; j += 32) set_bit(W.exact, W.exact_k[j]);
             if (lane == 0) W.n_exact = base;
-            for (int i = lane; i < kSlotCap / 32; i += 32) W.peak[i] = 0;
+            if (lane < kSlotCap / 32) W.m.peak[lane] = 0;
             __syncwarp();
         }
         if (redone) continue;   // the node went through the FP64 path
-        // ---- ordered fold over the peaks (FindPeakNcc's top-2 rule) ----
-        if (P.cmr && lane == 0) {
-            for (int i = 0; i < (K + 31) / 32; ++i) {
-                uint32_t pm = W.peak[i];
-                while (pm) {
-                    const int b = __ffs(pm) - 1;
-                    pm &= pm - 1;
-                    const int p = (i << 5) + b;
-                    bool ex;
-                    const double pv = slot_value(W, p, ex);
-                    const float ph = slot_height(P, start_H, R.minHeight, p);
-                    if (R.result4 < 10) R.result4 += 1;
-                    const int16_t qpre = q_result(pv);
-                    if (R.result0 < qpre) {
-                        const double t1 = dq_result(R.result0);
-                        R.result0 = qpre;
-                        const float t2 = R.result2;
-                        R.result2 = ph;
-                        const int16_t q1 = q_result(t1);
-                        if (R.result1 < q1) {
-                            R.result1 = q1;
-                            R.result3 = t2;
-                        }
-                    } else if (R.result1 < qpre) {
-                        R.result1 = qpre;
-                        R.result3 = ph;
-                    }
-                }
-            }
-        }
         if (lane == 0) {
+            if (P.cmr) fold_peaks(P, R, K, start_H, W.m.peak, xval);
             if (R.check_height_change) R.max_WNCC = q_result(max_w);
             P.ncc[pt] = R;
         }
         __syncwarp();
     }
-    for (int o = 16; o; o >>= 1) rechecks += __shfl_down_sync(0xffffffffu, rechecks, o);
+    for (int o = 16; o; o >>= 1) {
+        rechecks += __shfl_down_sync(0xffffffffu, rechecks, o);
+        evals += __shfl_down_sync(0xffffffffu, evals, o);
+    }
     if (lane == 0 && rechecks) atomicAdd(&counters[2], rechecks);
+    if (lane == 0 && evals) atomicAdd(&counters[1], evals);
 }
+
+
 
 // ---------------------------------------------------------------------------
 // host driver
@@ -1221,14 +1174,21 @@ void host_rpc(const double *rpc, double lon, double lat, double h, double &x, do
     x = c[2] / c[3] * rpc[6] + rpc[1];
 }
 
-// Texel-pair budget per warp: the boxes covering 32 consecutive height slots
-// of one node in both images -- the reference window and the target window
-// (rotated up to 45 degrees) swept along their epipolar lines.  The sweep
-// per slot is measured from the RPCs over the image footprint; the budget is
-// the worst case with a 25% margin (a larger footprint falls back to FP64).
-int window_warp_quads(const DevLevel &P, float margin) {
+// Shared-memory budget per warp: the boxes covering 32 consecutive height
+// slots of one node in both images -- the reference window and the target
+// window (rotated; its samples lie within H + 1 of the centre) swept along
+// their epipolar lines -- as texel pairs, and the raw rows the bulk copies
+// bring (8 texels of alignment slack per row).  The sweep per slot, along x
+// and y, is measured from the RPCs over the image footprint; the budget is
+// the worst case times `margin` (a larger footprint falls back to FP64).
+struct WarpBudget {
+    int quads;   // float4 texel pairs
+    int raw;     // bytes of raw rows (multiple of 16)
+};
+
+WarpBudget window_warp_budget(const DevLevel &P, float margin) {
     const int H = P.H;
-    double rate[2] = {0, 0};
+    double rx[2] = {0, 0}, ry[2] = {0, 0};
     for (int ti = 0; ti < 2; ++ti) {
         const double *r = P.im[ti].rpc;
         for (int a = -1; a <= 1; ++a)
@@ -1237,25 +1197,41 @@ int window_warp_quads(const DevLevel &P, float margin) {
                 double x0, y0, x1, y1;
                 host_rpc(r, lon, lat, r[4] - 50.0, x0, y0);
                 host_rpc(r, lon, lat, r[4] + 50.0, x1, y1);
-                const double d = std::max(fabs(x1 - x0), fabs(y1 - y0)) / 100.0 / (1 << P.L);
-                rate[ti] = std::max(rate[ti], d);
+                rx[ti] = std::max(rx[ti], fabs(x1 - x0) / 100.0 / (1 << P.L));
+                ry[ti] = std::max(ry[ti], fabs(y1 - y0) / 100.0 / (1 << P.L));
             }
     }
-    const double sweep0 = 31.0 * P.height_step * rate[0], sweep1 = 31.0 * P.height_step * rate[1];
-    const int side = 2 * H + 3;
-    const int rside = 2 * ((int)ceilf(1.4143f * H) + 1) + 3;
-    const double need = (side + 1.0) * (side + sweep0 + 2.0) + (rside + 1.0) * (rside + sweep1 + 2.0);
-    int q = (int)(need * (margin > 0 ? margin : 1.1f)) + 32;
-    const int cap = (int)((200 * 1024 - win_boxes_offset()) / (kWinWarps * sizeof(float4)));
-    return std::min(q, cap);
+    const double m = margin > 0 ? margin : 1.1;
+    const int side[2] = {2 * H + 3, 2 * (H + 2) + 3};   // pairs of one slot's box (+1 slack)
+    double quads = 0, raw = 0;
+    for (int ti = 0; ti < 2; ++ti) {
+        const double w = side[ti] + 31.0 * P.height_step * rx[ti] + 2.0;
+        const double h = side[ti] + 31.0 * P.height_step * ry[ti] + 2.0;
+        quads += (w + 1.0) * h;                              // odd row stride
+        raw += 2.0 * h * (std::ceil((w + 9.0) / 8.0) * 16.0);  // two planes
+    }
+    WarpBudget wb;
+    wb.quads = (int)(quads * m) + 32;
+    wb.raw = (((int)(raw * m) + 256) + 15) & ~15;
+    // at most ~200 KB for the block
+    const size_t per_warp = (200 * 1024 - win_boxes_offset()) / kWinWarps;
+    if ((size_t)wb.quads * sizeof(float4) + wb.raw > per_warp) {
+        const double f = (double)per_warp / ((double)wb.quads * sizeof(float4) + wb.raw);
+        wb.quads = (int)(wb.quads * f);
+        wb.raw = ((int)(wb.raw * f)) & ~15;
+    }
+    return wb;
 }
 
-
-// Box budget of a level set: the largest of its levels' budgets.
-int set_warp_quads(const DevLevel *hl, int n, float margin) {
-    int q = 1;
+// Budget of a level set: the largest of its levels' budgets.
+WarpBudget set_warp_budget(const DevLevel *hl, int n, float margin) {
+    WarpBudget q{1, 16};
     for (int l = 0; l < n; ++l)
-        if (hl[l].n_nodes > 0) q = std::max(q, window_warp_quads(hl[l], margin));
+        if (hl[l].n_nodes > 0) {
+            const WarpBudget b = window_warp_budget(hl[l], margin);
+            q.quads = std::max(q.quads, b.quads);
+            q.raw = std::max(q.raw, b.raw);
+        }
     return q;
 }
 
@@ -1266,12 +1242,13 @@ int set_max_h(const DevLevel *hl, int n) {
     return h;
 }
 
-cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const int64_t *items,
-                          int64_t n_items, const int64_t *slot_off, const double *gsum,
-                          const double *gcnt, float2 *rho, unsigned long long *counters,
-                          unsigned long long *ctl, const SplitTuning &tu, cudaStream_t s) {
-    const int wq = set_warp_quads(hl, n, tu.box_margin);
-    const size_t smem = win_boxes_offset() + (size_t)kWinWarps * wq * sizeof(float4);
+cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const int32_t *node_k,
+                          const double *gsum, const double *gcnt, float *pend_vals,
+                          int64_t pend_cap, int64_t *pend_node, int64_t *pend_off,
+                          unsigned long long *counters, unsigned long long *ctl,
+                          const SplitTuning &tu, cudaStream_t s) {
+    const WarpBudget wb = set_warp_budget(hl, n, tu.box_margin);
+    const size_t smem = win_boxes_offset() + (size_t)kWinWarps * (wb.quads * sizeof(float4) + wb.raw);
     int dev = 0;
     cudaGetDevice(&dev);
     cudaError_t e = cudaFuncSetAttribute(window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1283,17 +1260,16 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
     if (tu.blocks_per_sm > 0 && tu.blocks_per_sm < per_sm) per_sm = tu.blocks_per_sm;
     if (per_sm < 1) per_sm = 1;
     const int grab = tu.grab > 0 ? std::min(tu.grab, 64) : 1;
-    window_kernel<<<sms * per_sm, kWinWarps * 32, smem, s>>>(LS, items, n_items, slot_off, gsum,
-                                                             gcnt, rho, counters, ctl + 0, wq,
-                                                             grab, ctl + 5);
+    window_kernel<<<sms * per_sm, kWinWarps * 32, smem, s>>>(LS, node_k, gsum, gcnt, pend_vals,
+                                                             pend_cap, pend_node, pend_off,
+                                                             counters, ctl, wb.quads, wb.raw, grab);
     return cudaGetLastError();
 }
 
-cudaError_t launch_peaks(const LevelSet &LS, int max_h, const int64_t *slot_off, const float2 *rho,
+cudaError_t launch_peaks(const LevelSet &LS, int max_h, const int32_t *node_k,
+                         const float *pend_vals, const int64_t *pend_node, const int64_t *pend_off,
                          const double *gsum, const double *gcnt, unsigned long long *counters,
-                         unsigned long long *queue, const int64_t *pending,
-                         const unsigned long long *n_pending, const unsigned long long *stop,
-                         cudaStream_t s) {
+                         unsigned long long *ctl, cudaStream_t s) {
     const size_t ws = (sizeof(WarpShared) + 15) & ~(size_t)15;
     const size_t xs = (exact_scratch_bytes(max_h) + 15) & ~(size_t)15;
     const size_t smem = (ws + xs) * kPeakWarps;
@@ -1306,37 +1282,39 @@ cudaError_t launch_peaks(const LevelSet &LS, int max_h, const int64_t *slot_off,
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, peaks_kernel, kPeakWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
-    peaks_kernel<<<sms * per_sm, kPeakWarps * 32, smem, s>>>(LS, max_h, slot_off, rho, gsum, gcnt,
-                                                             counters, queue, pending, n_pending,
-                                                             stop);
+    peaks_kernel<<<sms * per_sm, kPeakWarps * 32, smem, s>>>(LS, max_h, node_k, pend_vals,
+                                                             pend_node, pend_off, gsum, gcnt,
+                                                             counters, ctl);
     return cudaGetLastError();
 }
 
-// the window / peak stages of the pipeline on given buffers
-cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, const int64_t *items,
-                             int64_t n_items, const int64_t *slot_off, const double *gsum,
-                             const double *gcnt, float2 *rho, unsigned long long *counters,
-                             unsigned long long *ctl, int64_t *pending, const SplitTuning &tu,
-                             cudaStream_t s, SplitTiming *tm) {
-    cudaError_t e = launch_window(hl, n, LS, items, n_items, slot_off, gsum, gcnt, rho, counters,
-                                  ctl, tu, s);
+// the window and exact stages of the pipeline on given buffers (ctl cleared
+// by the caller: [0] node queue, [1] exact-pass queue, [2] queued nodes,
+// [4] pending-buffer cursor)
+cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, const int32_t *node_k,
+                             const double *gsum, const double *gcnt, float *pend_vals,
+                             int64_t pend_cap, int64_t *pend_node, int64_t *pend_off,
+                             unsigned long long *counters, unsigned long long *ctl,
+                             const SplitTuning &tu, cudaStream_t s, SplitTiming *tm) {
+    cudaError_t e = launch_window(hl, n, LS, node_k, gsum, gcnt, pend_vals, pend_cap, pend_node,
+                                  pend_off, counters, ctl, tu, s);
     if (e != cudaSuccess) return e;
-    if (tm && tm->enabled) cudaEventRecord(tm->ev[5], s);
-    {
-        int dev = 0, sms = 148, per_sm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_queue_kernel, 256, 0);
-        if (per_sm < 1) per_sm = 1;
-        const int64_t want = (LS.total + 255) / 256;
-        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * per_sm));
-        scan_queue_kernel<<<blocks, 256, 0, s>>>(LS, slot_off, rho, pending, ctl);
+    if (tm && tm->enabled) {
+        cudaEventRecord(tm->ev[5], s);
+        cudaEventRecord(tm->ev[6], s);
     }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (tm && tm->enabled) cudaEventRecord(tm->ev[6], s);
-    return launch_peaks(LS, set_max_h(hl, n), slot_off, rho, gsum, gcnt, counters, ctl + 1,
-                        pending, ctl + 2, ctl + 5, s);
+    return launch_peaks(LS, set_max_h(hl, n), node_k, pend_vals, pend_node, pend_off, gsum, gcnt,
+                        counters, ctl, s);
+}
+
+// Slots of FP32 values the pending buffer holds for a pass of n_slots slots:
+// an eighth of them (a few percent of nodes are queued for the exact pass),
+// at least 4 M; SETSM_VLL_PENDING_SLOTS overrides it (a node that finds the
+// buffer full is evaluated wholly in FP64 instead).
+int64_t pending_capacity(int64_t n_slots) {
+    const char *env = getenv("SETSM_VLL_PENDING_SLOTS");
+    if (env && *env) return std::max<int64_t>(0, atoll(env));
+    return std::min<int64_t>(n_slots, std::max<int64_t>(n_slots / 8, (int64_t)1 << 22));
 }
 
 }  // namespace
@@ -1347,14 +1325,14 @@ bool split_supported(const DevLevel &P) {
 }
 
 void split_release(SplitBuffers &b) {
-    void **all[] = {&b.node_k, &b.slot_off, &b.item_cnt, &b.item_off, &b.items, &b.rho, &b.gsum,
-                    &b.gcnt, &b.re_items, &b.re_out, &b.node_re, &b.scan_tmp, &b.ctl, &b.pending,
-                    &b.base, &b.acc_level};
+    void **all[] = {&b.node_k, &b.slot_off, &b.rho, &b.gsum, &b.gcnt, &b.scan_tmp, &b.ctl,
+                    &b.pending, &b.pend_off, &b.base, &b.acc_level};
     for (void **p : all) {
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
-    b.cap_nodes = b.cap_slots = b.cap_items = b.cap_re = b.cap_scan = b.cap_levels = 0;
+    b.cap_nodes = b.cap_slots = b.cap_scan = b.cap_levels = 0;
+    b.pend_cap = 0;
 }
 
 #define SPLIT_CUDA(call)                       \
@@ -1367,7 +1345,8 @@ void split_release(SplitBuffers &b) {
     } while (0)
 
 // Phase 1 of a pass over a level set: node-sized buffers, the level table,
-// GNCC, prep and the two prefix sums (all enqueued on s, no host wait).
+// GNCC, prep and the prefix sum of the slot counts (all enqueued on s, no
+// host wait).
 cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl, int n_levels,
                         unsigned long long *counters, cudaStream_t s, std::string *err,
                         SplitTiming *tm, LevelSet *LS_out, double **gsum_out, double **gcnt_out,
@@ -1384,13 +1363,10 @@ cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
     }
     const int64_t N = base[n_levels];
     if ((size_t)(N + 1) > b.cap_nodes) {
-        void **nb[] = {&b.node_k, &b.item_cnt};
-        for (void **p : nb) {
-            if (*p) cudaFree(*p);
-            *p = nullptr;
-            SPLIT_CUDA(cudaMalloc(p, (size_t)(N + 1) * sizeof(int32_t)));
-        }
-        void **nb8[] = {&b.slot_off, &b.item_off, &b.gsum, &b.gcnt, &b.pending};
+        if (b.node_k) cudaFree(b.node_k);
+        b.node_k = nullptr;
+        SPLIT_CUDA(cudaMalloc(&b.node_k, (size_t)(N + 1) * sizeof(int32_t)));
+        void **nb8[] = {&b.slot_off, &b.gsum, &b.gcnt, &b.pending, &b.pend_off};
         for (void **p : nb8) {
             if (*p) cudaFree(*p);
             *p = nullptr;
@@ -1407,12 +1383,10 @@ cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
         b.cap_levels = (size_t)n_levels + 1;
     }
     if (!b.ctl) SPLIT_CUDA(cudaMalloc(&b.ctl, 8 * sizeof(unsigned long long)));
-    size_t tmp1 = 0, tmp2 = 0;
-    SPLIT_CUDA(scan64(nullptr, tmp1, (const int32_t *)b.node_k,
-                                             (int64_t *)b.slot_off, (int)(N + 1), s));
-    SPLIT_CUDA(scan64(nullptr, tmp2, (const int32_t *)b.item_cnt,
-                                             (int64_t *)b.item_off, (int)(N + 1), s));
-    SPLIT_CUDA(grow(b.scan_tmp, b.cap_scan, std::max(tmp1, tmp2)));
+    size_t tmp1 = 0;
+    SPLIT_CUDA(scan64(nullptr, tmp1, (const int32_t *)b.node_k, (int64_t *)b.slot_off,
+                      (int)(N + 1), s));
+    SPLIT_CUDA(grow(b.scan_tmp, b.cap_scan, tmp1));
     // the level table is uploaded outside any capture (plan time) by the caller
     // of split_front when capturing; here it is copied on the stream
     if (!b.capturing)
@@ -1421,7 +1395,6 @@ cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
     *LS_out = LevelSet{dl, (const int64_t *)b.base, n_levels, N};
     SPLIT_CUDA(cudaMemsetAsync(b.ctl, 0, 8 * sizeof(unsigned long long), s));
     SPLIT_CUDA(cudaMemsetAsync(b.node_k, 0, (size_t)(N + 1) * sizeof(int32_t), s));
-    SPLIT_CUDA(cudaMemsetAsync(b.item_cnt, 0, (size_t)(N + 1) * sizeof(int32_t), s));
     double *gsum = nullptr, *gcnt = nullptr;
     mark(0);
     if (any_ortho) {
@@ -1435,84 +1408,61 @@ cudaError_t split_front(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
     }
     mark(1);
     prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(*LS_out, gsum, gcnt, (int32_t *)b.node_k,
-                                                          (int32_t *)b.item_cnt, counters,
+                                                          counters,
                                                           (unsigned long long *)b.acc_level);
     SPLIT_CUDA(cudaGetLastError());
     ++*launches;
     mark(2);
     tmp1 = b.cap_scan;
-    SPLIT_CUDA(scan64(b.scan_tmp, tmp1, (const int32_t *)b.node_k,
-                                             (int64_t *)b.slot_off, (int)(N + 1), s));
-    tmp2 = b.cap_scan;
-    SPLIT_CUDA(scan64(b.scan_tmp, tmp2, (const int32_t *)b.item_cnt,
-                                             (int64_t *)b.item_off, (int)(N + 1), s));
-    *launches += 4;   // two scans of two kernels each
+    SPLIT_CUDA(scan64(b.scan_tmp, tmp1, (const int32_t *)b.node_k, (int64_t *)b.slot_off,
+                      (int)(N + 1), s));
+    *launches += 2;   // one scan of two kernels
     mark(3);
     *gsum_out = gsum;
     *gcnt_out = gcnt;
     return cudaSuccess;
 }
 
-// Phase 2: the work list, the persistent window launch, the scan and the
-// exact pass, on buffers sized for n_slots / n_items.
+// Phase 2: the persistent window launch and the exact pass.
 cudaError_t split_back(SplitBuffers &b, const DevLevel *hl, int n_levels, const LevelSet &LS,
-                       const double *gsum, const double *gcnt, int64_t n_slots, int64_t n_items,
-                       unsigned long long *counters, const SplitTuning &tu, cudaStream_t s,
-                       std::string *err, SplitTiming *tm, int64_t *launches) {
+                       const double *gsum, const double *gcnt, unsigned long long *counters,
+                       const SplitTuning &tu, cudaStream_t s, std::string *err, SplitTiming *tm,
+                       int64_t *launches) {
     auto mark = [&](int i) {
         if (tm && tm->enabled) cudaEventRecord(tm->ev[i], s);
     };
-    const int64_t N = LS.total;
-    unsigned long long *ctl = (unsigned long long *)b.ctl;
-    guard_kernel<<<1, 32, 0, s>>>((const int64_t *)b.slot_off + N, (const int64_t *)b.item_off + N,
-                                  n_slots, n_items, ctl);
-    SPLIT_CUDA(cudaGetLastError());
-    ++*launches;
-    if (n_items > 0) {
-        items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, (const int32_t *)b.item_cnt,
-                                                               (const int64_t *)b.item_off,
-                                                               (int64_t *)b.items, ctl + 5);
-        SPLIT_CUDA(cudaGetLastError());
-        ++*launches;
-        mark(4);
-        cudaError_t e = window_and_peaks(hl, n_levels, LS, (const int64_t *)b.items, n_items,
-                                         (const int64_t *)b.slot_off, gsum, gcnt, (float2 *)b.rho,
-                                         counters, ctl, (int64_t *)b.pending, tu, s, tm);
-        if (e != cudaSuccess) {
-            *err = "window / peak kernel launch";
-            return e;
-        }
-        *launches += 3;
-        mark(7);
-    } else {
-        mark(4);
-        mark(5);
-        mark(6);
-        mark(7);
+    mark(4);
+    cudaError_t e = window_and_peaks(hl, n_levels, LS, (const int32_t *)b.node_k, gsum, gcnt,
+                                     (float *)b.rho, b.pend_cap, (int64_t *)b.pending,
+                                     (int64_t *)b.pend_off, counters,
+                                     (unsigned long long *)b.ctl, tu, s, tm);
+    if (e != cudaSuccess) {
+        *err = "window / exact kernel launch";
+        return e;
     }
+    *launches += 2;
+    mark(7);
     mark(8);
     return cudaSuccess;
 }
 
-// Sizes the slot and item buffers from the totals of a completed front phase.
+// Sizes the pending buffer from the slot total of a completed front phase
+// (one host wait).
 cudaError_t split_size(SplitBuffers &b, int64_t N, cudaStream_t s, std::string *err,
-                       int64_t *n_slots, int64_t *n_items) {
-    int64_t totals[2];
-    SPLIT_CUDA(cudaMemcpyAsync(&totals[0], (int64_t *)b.slot_off + N, 8, cudaMemcpyDeviceToHost, s));
-    SPLIT_CUDA(cudaMemcpyAsync(&totals[1], (int64_t *)b.item_off + N, 8, cudaMemcpyDeviceToHost, s));
+                       int64_t *n_slots) {
+    int64_t total = 0;
+    SPLIT_CUDA(cudaMemcpyAsync(&total, (int64_t *)b.slot_off + N, 8, cudaMemcpyDeviceToHost, s));
     SPLIT_CUDA(cudaStreamSynchronize(s));
-    *n_slots = totals[0];
-    *n_items = totals[1];
-    if (*n_slots < 0 || *n_items < 0) {
-        *err = "slot / item totals overflow";
+    *n_slots = total;
+    if (total < 0) {
+        *err = "slot total overflow";
         return cudaErrorInvalidValue;
     }
+    const int64_t cap = pending_capacity(total);
     size_t c = b.cap_slots;
-    SPLIT_CUDA(grow(b.rho, c, (size_t)*n_slots * sizeof(float2)));
+    SPLIT_CUDA(grow(b.rho, c, (size_t)std::max<int64_t>(cap, 1) * sizeof(float)));
     b.cap_slots = c;
-    c = b.cap_items;
-    SPLIT_CUDA(grow(b.items, c, (size_t)*n_items * sizeof(int64_t)));
-    b.cap_items = c;
+    b.pend_cap = cap;
     return cudaSuccess;
 }
 
@@ -1526,11 +1476,10 @@ cudaError_t run_split_set(SplitBuffers &b, const DevLevel *hl, const DevLevel *d
     cudaError_t e = split_front(b, hl, dl, n_levels, counters, s, err, tm, &LS, &gsum, &gcnt,
                                 &launches);
     if (e != cudaSuccess) return e;
-    int64_t n_slots = 0, n_items = 0;
-    e = split_size(b, LS.total, s, err, &n_slots, &n_items);
+    int64_t n_slots = 0;
+    e = split_size(b, LS.total, s, err, &n_slots);
     if (e != cudaSuccess) return e;
-    e = split_back(b, hl, n_levels, LS, gsum, gcnt, n_slots, n_items, counters, tu, s, err, tm,
-                   &launches);
+    e = split_back(b, hl, n_levels, LS, gsum, gcnt, counters, tu, s, err, tm, &launches);
     if (e != cudaSuccess) return e;
     if (tm) {
         tm->slots = n_slots;
@@ -1539,10 +1488,11 @@ cudaError_t run_split_set(SplitBuffers &b, const DevLevel *hl, const DevLevel *d
     return cudaSuccess;
 }
 
-// Planned pass: sizes every buffer with one uncaptured front phase, then
+// Planned pass: sizes the buffers with one uncaptured front phase, then
 // captures front + back into a CUDA graph that later replays with no host
-// wait.  The plan holds while the levels' height ranges keep their slot and
-// item totals; a replay with other totals sets ctl[5] and does nothing.
+// wait.  The buffers depend on the node count only (the pending buffer's
+// size steers performance, not correctness), so replays stay valid when the
+// levels' height ranges change.
 cudaError_t split_plan(SplitPlan &pl, SplitBuffers &b, const DevLevel *hl, const DevLevel *dl,
                        int n_levels, unsigned long long *counters, cudaStream_t s,
                        std::string *err, const SplitTuning &tu,
@@ -1559,7 +1509,7 @@ cudaError_t split_plan(SplitPlan &pl, SplitBuffers &b, const DevLevel *hl, const
     e = split_front(b, hl, dl, n_levels, counters, s, err, nullptr, &LS, &gsum, &gcnt,
                                 &launches);
     if (e != cudaSuccess) return e;
-    e = split_size(b, LS.total, s, err, &pl.n_slots, &pl.n_items);
+    e = split_size(b, LS.total, s, err, &pl.n_slots);
     if (e != cudaSuccess) return e;
     if (pl.exec) {
         cudaGraphExecDestroy(pl.exec);
@@ -1574,8 +1524,7 @@ cudaError_t split_plan(SplitPlan &pl, SplitBuffers &b, const DevLevel *hl, const
         e = split_front(b, hl, dl, n_levels, counters, s, err, nullptr, &LS, &gsum, &gcnt,
                         &launches);
     if (e == cudaSuccess)
-        e = split_back(b, hl, n_levels, LS, gsum, gcnt, pl.n_slots, pl.n_items, counters, tu, s,
-                       err, nullptr, &launches);
+        e = split_back(b, hl, n_levels, LS, gsum, gcnt, counters, tu, s, err, nullptr, &launches);
     cudaError_t e2 = cudaStreamEndCapture(s, &graph);
     b.capturing = false;
     if (e != cudaSuccess) {
@@ -1625,42 +1574,55 @@ namespace {
 
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[256] = {};
+unsigned long long g_noalloc_ctx[256] = {};
 
-// Device address of the scratch array for the current device, looked up once
-// per device (host code cannot use the symbol's address directly).
+// Unique id of the calling thread's current context (0 when unknown),
+// through the driver entry points (no link against the driver library).
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)f;
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c) get_id(c, &id);
+    return id;
+}
+
+// Device address of the scratch array for the current device: looked up
+// (cudaGetSymbolAddress, host code cannot use the symbol's address) on the
+// first call on a device, and again when the device's context changed.
 cudaError_t noalloc_scratch(void **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+    // 0 when this thread has no current context yet (the lookup makes the
+    // device's primary context current)
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_noalloc_ptr[dev] = p;
+        g_noalloc_ctx[dev] = current_context_id();
     }
     *out = g_noalloc_ptr[dev];
     return cudaSuccess;
-}
-
-// Slot count per node without touching any output (same tests as prep_kernel
-// on the memory-tight route), so that capacity is checked before writing.
-__global__ void __launch_bounds__(256) noalloc_count_kernel(const DevLevel *__restrict__ Pp,
-                                                            int32_t *__restrict__ node_k,
-                                                            int32_t *__restrict__ item_cnt) {
-    const DevLevel &P = *Pp;
-    for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.n_nodes;
-         pt += (int64_t)gridDim.x * blockDim.x) {
-        int K = 0;
-        const vll_ugrid g = P.gp3[pt];
-        const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
-        if (check_image_boundary(P, lon, lat, (double)g.minHeight, (double)g.maxHeight, P.H) &&
-            !blunder_cell(P, g))
-            K = (uint16_t)(int)__ddiv_rn((double)(g.maxHeight - g.minHeight), P.height_step);
-        node_k[pt] = K;
-        item_cnt[pt] = (K + 31) / 32;
-    }
 }
 
 struct Carver {
@@ -1708,32 +1670,34 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     P.vox = nullptr;
     P.vox_off = nullptr;
     void *base = nullptr;
-    if (noalloc_scratch(&base) != cudaSuccess)
-        return fail(VLL_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
+    if (const cudaError_t se = noalloc_scratch(&base); se != cudaSuccess) {
+        char m[200];
+        snprintf(m, sizeof m, "device address of the %zu MiB scratch array: %s",
+                 kNoAllocScratchBytes >> 20, cudaGetErrorString(se));
+        return fail(VLL_ERR_CUDA, m);
+    }
     const int64_t N = P.n_nodes;
     Carver cv{(unsigned char *)base, 0, kNoAllocScratchBytes};
     DevLevel *dP = (DevLevel *)cv.take(sizeof(DevLevel));
     unsigned long long *ctl = (unsigned long long *)cv.take(8 * sizeof(unsigned long long));
-    unsigned long long *counters = (unsigned long long *)cv.take(4 * sizeof(unsigned long long));
+    unsigned long long *counters = (unsigned long long *)cv.take(8 * sizeof(unsigned long long));
     int32_t *node_k = (int32_t *)cv.take((size_t)(N + 1) * 4);
-    int32_t *item_cnt = (int32_t *)cv.take((size_t)(N + 1) * 4);
-    int64_t *slot_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
-    int64_t *item_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
     int64_t *pending = (int64_t *)cv.take((size_t)(N + 1) * 8);
+    int64_t *pend_off = (int64_t *)cv.take((size_t)(N + 1) * 8);
     int64_t *lbase = (int64_t *)cv.take(2 * 8);
     unsigned long long *acc_level = (unsigned long long *)cv.take(2 * 8);
-    size_t scan_bytes = 0;
-    if (scan64(nullptr, scan_bytes, (const int32_t *)node_k, slot_off,
-                                      (int)(N + 1), s) != cudaSuccess)
-        return fail(VLL_ERR_CUDA, "scan size query failed");
-    void *scan_tmp = cv.take(scan_bytes);
-    if (!dP || !ctl || !counters || !node_k || !item_cnt || !slot_off || !item_off || !pending ||
-        !lbase || !acc_level || !scan_tmp) {
+    if (!dP || !ctl || !counters || !node_k || !pending || !pend_off || !lbase || !acc_level) {
         char m[160];
         snprintf(m, sizeof m, "grid of %lld nodes exceeds the %zu MiB scratch array",
                  (long long)N, kNoAllocScratchBytes >> 20);
         return fail(VLL_ERR_CAPACITY, m);
     }
+    // the rest of the array holds the FP32 slot values of the nodes queued
+    // for the exact pass; a node that finds it full is evaluated wholly in
+    // FP64 there, so its size affects speed only
+    const size_t used = (cv.used + 255) & ~(size_t)255;
+    float *pend_vals = (float *)((unsigned char *)base + used);
+    const int64_t pend_cap = (int64_t)((kNoAllocScratchBytes - used) / sizeof(float));
 #define NA_CUDA(call)                                                     \
     do {                                                                  \
         if ((call) != cudaSuccess) return fail(VLL_ERR_CUDA, #call);      \
@@ -1741,7 +1705,7 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     NA_CUDA(cudaMemcpyAsync(dP, &P, sizeof(DevLevel), cudaMemcpyHostToDevice, s));
     // the array keeps the previous call's contents: clear what must start at zero
     NA_CUDA(cudaMemsetAsync(ctl, 0, 8 * sizeof(unsigned long long), s));
-    NA_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), s));
+    NA_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), s));
     NA_CUDA(cudaMemsetAsync(acc_level, 0, 2 * 8, s));
     static thread_local int64_t lbase_host[2];
     lbase_host[0] = 0;
@@ -1749,49 +1713,12 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     NA_CUDA(cudaMemcpyAsync(lbase, lbase_host, sizeof(lbase_host), cudaMemcpyHostToDevice, s));
     const LevelSet LS{dP, lbase, 1, N};
     NA_CUDA(cudaMemsetAsync(node_k, 0, (size_t)(N + 1) * 4, s));
-    NA_CUDA(cudaMemsetAsync(item_cnt, 0, (size_t)(N + 1) * 4, s));
-    // capacity: count slots and items first, without writing any output
-    noalloc_count_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(dP, node_k, item_cnt);
-    NA_CUDA(cudaGetLastError());
-    size_t t1 = scan_bytes;
-    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)node_k, slot_off,
-                                          (int)(N + 1), s));
-    t1 = scan_bytes;
-    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
-                                          (int)(N + 1), s));
-    int64_t totals[2] = {0, 0};
-    NA_CUDA(cudaMemcpyAsync(&totals[0], slot_off + N, 8, cudaMemcpyDeviceToHost, s));
-    NA_CUDA(cudaMemcpyAsync(&totals[1], item_off + N, 8, cudaMemcpyDeviceToHost, s));
-    NA_CUDA(cudaStreamSynchronize(s));
-    const int64_t n_slots = totals[0], n_items = totals[1];
-    int64_t *items = (int64_t *)cv.take((size_t)(n_items > 0 ? n_items : 1) * 8);
-    float2 *rho = (float2 *)cv.take((size_t)(n_slots > 0 ? n_slots : 1) * sizeof(float2));
-    if (!items || !rho) {
-        char m[200];
-        snprintf(m, sizeof m,
-                 "%lld nodes with %lld height slots exceed the %zu MiB scratch array",
-                 (long long)N, (long long)n_slots, kNoAllocScratchBytes >> 20);
-        return fail(VLL_ERR_CAPACITY, m);
-    }
     // the pipeline proper (same kernels and order as run_split)
-    NA_CUDA(cudaMemsetAsync(node_k, 0, (size_t)(N + 1) * 4, s));
-    NA_CUDA(cudaMemsetAsync(item_cnt, 0, (size_t)(N + 1) * 4, s));
-    prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(LS, nullptr, nullptr, node_k, item_cnt,
-                                                          counters, acc_level);
+    prep_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(LS, nullptr, nullptr, node_k, counters,
+                                                          acc_level);
     NA_CUDA(cudaGetLastError());
-    t1 = scan_bytes;
-    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)node_k, slot_off,
-                                          (int)(N + 1), s));
-    t1 = scan_bytes;
-    NA_CUDA(scan64(scan_tmp, t1, (const int32_t *)item_cnt, item_off,
-                                          (int)(N + 1), s));
-    if (n_items > 0) {
-        items_kernel<<<grid_1d(N, 256, 148 * 32), 256, 0, s>>>(N, item_cnt, item_off, items,
-                                                               ctl + 5);
-        NA_CUDA(cudaGetLastError());
-        NA_CUDA(window_and_peaks(&P, 1, LS, items, n_items, slot_off, nullptr, nullptr, rho,
-                                 counters, ctl, pending, SplitTuning(), s, nullptr));
-    }
+    NA_CUDA(window_and_peaks(&P, 1, LS, node_k, nullptr, nullptr, pend_vals, pend_cap, pending,
+                             pend_off, counters, ctl, SplitTuning(), s, nullptr));
     unsigned long long acc = 0;
     NA_CUDA(cudaMemcpyAsync(&acc, counters, sizeof(acc), cudaMemcpyDeviceToHost, s));
     NA_CUDA(cudaStreamSynchronize(s));

@@ -14,23 +14,19 @@ struct DevLevel;
 
 // Device scratch of the split pipeline, grown on demand and owned by a context.
 struct SplitBuffers {
-    void *node_k = nullptr;        // int32  [N]   slots per active node (0 = inactive)
-    void *slot_off = nullptr;      // int64  [N+1] slot offsets
-    void *item_cnt = nullptr;      // int32  [N]   work items per node
-    void *item_off = nullptr;      // int64  [N+1]
-    void *items = nullptr;         // int64  [n_items]  (node << 16 | k0)
-    void *rho = nullptr;           // float2 [slots] (temp_rho, INCC average)
+    void *node_k = nullptr;        // int32  [N+1] slots per active node (0 = inactive)
+    void *slot_off = nullptr;      // int64  [N+1] prefix sum of node_k (the slot total)
+    void *rho = nullptr;           // float  [pend_cap] FP32 slot values of queued nodes
     void *gsum = nullptr;          // double [N] GNCC sums (FP64)
     void *gcnt = nullptr;          // double [N]
-    void *re_items = nullptr;      // int64  [max_re] (node << 16 | k)
-    void *re_out = nullptr;        // double [2 * max_re]
-    void *node_re = nullptr;       // int64  [N] (start << 8 | count) of a node's re-checks
     void *scan_tmp = nullptr;      // cub temporary storage
-    void *ctl = nullptr;           // uint64 [8] queue head, counts, flags
-    void *pending = nullptr;       // int64  [N]  nodes awaiting the exact re-scan
+    void *ctl = nullptr;           // uint64 [8] queue heads, counts, cursor
+    void *pending = nullptr;       // int64  [N]  nodes queued for the exact pass
+    void *pend_off = nullptr;      // int64  [N]  their offsets in rho (-1: none)
     void *base = nullptr;          // int64  [levels+1] first global node of each level
     void *acc_level = nullptr;     // uint64 [levels+1] Accessable_grid of each level
-    size_t cap_nodes = 0, cap_slots = 0, cap_items = 0, cap_re = 0, cap_scan = 0, cap_levels = 0;
+    size_t cap_nodes = 0, cap_slots = 0, cap_scan = 0, cap_levels = 0;
+    int64_t pend_cap = 0;          // slots of rho in use
     std::vector<int64_t> h_base;   // host copy of the level table
     bool capturing = false;        // enqueueing into a stream capture
 };
@@ -38,7 +34,7 @@ struct SplitBuffers {
 // Launch parameters of the window kernel that the autotuner chooses.
 struct SplitTuning {
     int blocks_per_sm = 0;      // CTAs per SM (0: the occupancy maximum)
-    int grab = 1;               // work items taken per queue access
+    int grab = 1;               // nodes taken per queue access
     float box_margin = 1.1f;    // footprint budget over the swept-box estimate
 };
 
@@ -46,7 +42,7 @@ struct SplitTuning {
 struct SplitPlan {
     SplitBuffers bufs;
     cudaGraphExec_t exec = nullptr;
-    int64_t n_slots = 0, n_items = 0, launches = 0;
+    int64_t n_slots = 0, launches = 0;
 };
 
 void split_release(SplitBuffers &b);
@@ -74,9 +70,9 @@ cudaError_t run_split(SplitBuffers &b, const DevLevel &P, const DevLevel *dP,
 
 // The same pipeline over a set of levels (tiles and / or pyramid levels)
 // whose blocks are hl (host copies) and dl (device array): one prep pass, one
-// persistent window launch draining all levels' (node, 32-slot) items, one
-// scan and one exact pass.  Per-level Accessable_grid counts are left in
-// b.acc_level[0..n_levels).
+// persistent window launch draining all levels' nodes (FindPeakNcc in the
+// same warp), and one exact pass over the nodes it queued.  Per-level
+// Accessable_grid counts are left in b.acc_level[0..n_levels).
 cudaError_t run_split_set(SplitBuffers &b, const DevLevel *hl, const DevLevel *dl, int n_levels,
                           unsigned long long *counters, cudaStream_t s, std::string *err,
                           SplitTiming *timing, const SplitTuning &tuning);

@@ -293,6 +293,114 @@ __device__ __forceinline__ bool stage_box_vec(float4 *__restrict__ dst, int ds,
     return __any_sync(0xffffffffu, (zacc & 0x80008000u) != 0 || z8);
 }
 
+// ---- footprint staging by the bulk-copy (TMA) engine ------------------------
+// The rows of a box are copied raw (uint16) from global to shared memory by
+// cp.async.bulk, one copy per row and plane, completing on the warp's
+// mbarrier; the warp then converts them to texel pairs with 128-bit shared
+// loads (stage_from_raw).
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One arrival that also expects `bytes` of asynchronous copies.
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, uint32_t bytes) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
+        "r"(bytes)
+        : "memory");
+}
+
+// Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from global to this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Waits for phase `parity` of `bar` to complete, for at most ~`limit`
+// cycles; returns false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > limit) return false;
+    }
+}
+
+// Orders this thread's earlier generic shared-memory accesses before later
+// asynchronous-proxy (bulk copy) writes to the same memory.
+__device__ __forceinline__ void fence_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Texel pairs of box [x0, x0+bw) x rows [0, bh) from raw rows staged in
+// shared memory: rawI / rawM hold, per box row, the uint16 texels
+// [xa, xa + 8 * nb / 16) (xa = x0 rounded down to 8, rows of nb bytes).
+// Each lane converts 8-texel chunks read with 128-bit loads, as
+// stage_box_vec does from global memory; returns (warp-uniform) whether an
+// intensity texel of the chunks is zero.
+__device__ __forceinline__ bool stage_from_raw(float4 *__restrict__ dst, int ds,
+                                               const unsigned char *__restrict__ rawI,
+                                               const unsigned char *__restrict__ rawM, int nb,
+                                               int xa, int x0, int bw, int bh, float sI, float sM,
+                                               int lane) {
+    uint32_t zacc = 0;
+    bool z8 = false;
+    const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
+    const int x1 = x0 + bw - 1;   // last pair's left texel
+    const int nch = nb / 16;
+    const int n = nch * bh;
+    for (int i = lane; i < n; i += 32) {
+        const int by = i / nch;
+        const int c = i - by * nch;
+        const int xc = xa + 8 * c;
+        const int ro = by * nb + 16 * c;
+        const uint4 vi = *reinterpret_cast<const uint4 *>(rawI + ro);
+        const uint4 vm = *reinterpret_cast<const uint4 *>(rawM + ro);
+        const bool need9 = xc + 7 <= x1;   // the 8th pair needs texel xc + 8
+        const uint32_t i8 = need9 ? *reinterpret_cast<const uint16_t *>(rawI + ro + 16) : 1u;
+        const uint32_t m8 = need9 ? *reinterpret_cast<const uint16_t *>(rawM + ro + 16) : 0u;
+        zacc |= zero_half(vi.x) | zero_half(vi.y) | zero_half(vi.z) | zero_half(vi.w);
+        z8 |= i8 == 0;
+        float2 f[9];
+        f[0] = texel_pair(vi.x, vm.x, 0x7610, ns);
+        f[1] = texel_pair(vi.x, vm.x, 0x7632, ns);
+        f[2] = texel_pair(vi.y, vm.y, 0x7610, ns);
+        f[3] = texel_pair(vi.y, vm.y, 0x7632, ns);
+        f[4] = texel_pair(vi.z, vm.z, 0x7610, ns);
+        f[5] = texel_pair(vi.z, vm.z, 0x7632, ns);
+        f[6] = texel_pair(vi.w, vm.w, 0x7610, ns);
+        f[7] = texel_pair(vi.w, vm.w, 0x7632, ns);
+        f[8] = texel_pair(i8, m8, 0x7610, ns);
+        float4 *drow = dst + by * ds;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int x = xc + t;
+            if (x >= x0 && x <= x1) drow[x - x0] = make_float4(f[t].x, f[t].y, f[t + 1].x, f[t + 1].y);
+        }
+    }
+    return __any_sync(0xffffffffu, (zacc & 0x80008000u) != 0 || z8);
+}
+
 // Scalar staging of a box whose destination rows have stride `ds` pairs
 // (used when image rows are not 16-byte aligned).
 __device__ __forceinline__ bool stage_box_strided(float4 *__restrict__ dst, int ds,

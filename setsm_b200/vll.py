@@ -38,6 +38,7 @@ EXPORTED = [
     "vll_initialize_voxel_device", "vll_awncc_peaks_device", "vll_select_mps_device",
     "vll_set_height_range_device", "vll_blunder_detection_tin",
     "vll_blunder_detection_tin_device", "vll_tin_rerun_count", "vll_debug_tin_threshold",
+    "vll_tin_create", "vll_tin_create_device",
 ]
 
 _lib = None
@@ -120,6 +121,8 @@ def load():
     L.vll_debug_tin_threshold.argtypes = [i32, i32, i32, dbl, dbl, dbl, dbl, i64, i64, vp,
                                           C.c_uint32, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.vll_set_height_range_device.argtypes = L.vll_set_height_range.argtypes
+    L.vll_tin_create.argtypes = [vp, vp, i64, vp, dbl, vp, i64, C.POINTER(i64)]
+    L.vll_tin_create_device.argtypes = L.vll_tin_create.argtypes
     _lib = L
     return L
 
@@ -372,6 +375,34 @@ class Context:
             int(iteration), float(mpp), int(bool(lcmr)), float(seed_dem_sigma), C.byref(lo),
             C.byref(hi)))
         return lo.value, hi.value
+
+    def tin_create(self, pts: np.ndarray, min_max, resolution: float) -> np.ndarray:
+        """TINCreate_list (SubFunctions.cpp:2768-2846): the ordered triangle list
+        (vertex indices into `pts`, POINT3_DTYPE records) of the points
+        snapped to the grid of `resolution` cells from min_max[0:2]."""
+        pts = np.ascontiguousarray(pts, dtype=abi.POINT3_DTYPE)
+        mm = np.ascontiguousarray(min_max, dtype=np.float64)
+        cap = 2 * len(pts) + 16
+        while True:
+            out = np.zeros(cap, dtype=abi.TRI_DTYPE)
+            n = C.c_int64(0)
+            rc = load().vll_tin_create(self._h, pts.ctypes.data, len(pts), mm.ctypes.data,
+                                       float(resolution), out.ctypes.data, cap, C.byref(n))
+            if rc == abi.VLL_ERR_CAPACITY and n.value > cap:
+                cap = n.value
+                continue
+            self._check(rc)
+            return out[:n.value]
+
+    def tin_create_device(self, d_pts: int, n_pts: int, min_max, resolution: float, d_tris: int,
+                          capacity: int) -> int:
+        """TINCreate_list on device buffers; returns the number of triangles."""
+        mm = np.ascontiguousarray(min_max, dtype=np.float64)
+        n = C.c_int64(0)
+        self._check(load().vll_tin_create_device(self._h, d_pts, int(n_pts), mm.ctypes.data,
+                                                 float(resolution), d_tris, int(capacity),
+                                                 C.byref(n)))
+        return n.value
 
     def set_height_range(self, inputs, pts: np.ndarray, tris: np.ndarray, iteration: int,
                          mpp: float, level_check_matching_rate: bool,

@@ -47,6 +47,26 @@ def test_vertical_line_locus_matches_oracle(gpu_ctx, name, kernel):
         assert cases.field_mismatch(ncc, o["ncc"]) == {}
 
 
+@pytest.mark.parametrize("cap", ["0", "40"])
+@pytest.mark.parametrize("name", ["m7", "m11", "v7_gncc", "v7_it2", "l3_m"])
+def test_full_pending_buffer_stays_exact(gpu_ctx, name, cap, monkeypatch):
+    """Nodes the FP32 pass cannot settle are queued with their FP32 values in
+    a pending buffer of limited size; a node that finds it full is evaluated
+    wholly in FP64 by the exact pass.  With no room (0) or room for a node
+    or so (40 slots), every record and voxel is still the oracle's."""
+    if name not in cases.CASES:
+        pytest.skip(f"no case {name}")
+    monkeypatch.setenv("SETSM_VLL_PENDING_SLOTS", cap)
+    o = oracle_run(name)
+    inp, ncc, vox, st = replay(gpu_ctx, o, "split")
+    assert st.accessable_grid == o["acc"]
+    assert cases.field_mismatch(ncc, o["vll_ncc"]) == {}
+    if vox is not None:
+        assert cases.field_mismatch(vox, o["vll_vox"]) == {}
+    if cap == "0":
+        assert st.fp64_nodes == st.exact_nodes
+
+
 def test_split_is_deterministic_and_counts(gpu_ctx):
     o = oracle_run("m7")
     _, n1, _, s1 = replay(gpu_ctx, o, "split")

@@ -73,10 +73,21 @@ def test_noalloc_matches_regular_entry_point(gpu_ctx):
 
 
 def test_noalloc_rejects_oversize_grid_before_writing(gpu_ctx):
+    """A 2048^2 grid (4.2 M nodes): its per-node scratch arrays alone exceed
+    the 64 MiB array, so the call is refused before any output is written."""
     import torch
-    inp = cases.make_case(nodes=400, res=0.9, n_heights=64)
-    d, d_gp3, keep = _device_case(torch, inp)
-    init = inp.new_nccresult()
+    inp = cases.make_case(**cases.CASES["m7"])
+    d, _, keep = _device_case(torch, inp)
+    side = 2048
+    n = side * side
+    d.grid_width = side
+    d.grid_height = side
+    wgs = torch.zeros(n * 16, dtype=torch.uint8, device="cuda")
+    pts = torch.zeros(n * 16, dtype=torch.uint8, device="cuda")
+    d.grid_wgs = wgs.data_ptr()
+    d.grid_pts = pts.data_ptr()
+    d_gp3 = torch.zeros(n * abi.UGRID_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    init = np.zeros(n, dtype=abi.NCCRESULT_DTYPE)
     init["result0"] = 123
     d_out = torch.from_numpy(init.view(np.uint8).copy()).cuda()
     rc, acc, msg = _noalloc(d, d_gp3.data_ptr(), d_out.data_ptr())
