@@ -253,6 +253,36 @@ int vll_debug_slot_rho(vll_context *ctx, const vll_level_desc *desc, const vll_u
  * counts of nodes, 32-slot passes, FP64 slow-path lanes, un-staged passes,
  * whole-node FP64 fallbacks, scan rounds and re-checked slots. */
 
+/*
+ * Residency of the host-buffer calls.  Matching_SETSM calls VerticalLineLocus
+ * once per iteration on the same level images (setsm_code.cpp:3774-3844) and
+ * passes its voxel rows through InitializeVoxel, VerticalLineLocus and AWNCC
+ * only.  With VLL_RESIDENT_PLANES, the image planes (intensity, magnitude,
+ * orientation, next level) and the grid's coordinate arrays of
+ * vll_vertical_line_locus stay on the device between calls and are sent
+ * again only when their host pointer, size or a sampled fingerprint of
+ * their bytes (64 spread 64-byte blocks) changes; a caller that rewrites a
+ * plane in place between calls without any of these changing must clear the
+ * flag.  With VLL_RESIDENT_VOXELS, vll_initialize_voxel called with a NULL
+ * output pointer keeps its output packing in the context (the input rows
+ * are `voxels_in` when given, else the context's packing when its length
+ * equals the old NumOfHeight sum, else none), and vll_vertical_line_locus /
+ * vll_awncc_peaks called with a NULL voxel pointer use that packing in place
+ * (its length must equal the sum of NumOfHeight); vll_resident_voxels copies
+ * it out.  Both flags are off by default.
+ */
+enum {
+    VLL_RESIDENT_PLANES = 1,
+    VLL_RESIDENT_VOXELS = 2
+};
+int vll_set_residency(vll_context *ctx, int flags);
+int vll_get_residency(const vll_context *ctx);
+/* Forgets the resident voxel packing (a new grid or level). */
+int vll_resident_reset(vll_context *ctx);
+/* Copies the resident voxel packing to `voxels` (capacity entries); `total`
+ * receives its length (VLL_ERR_CAPACITY when it does not fit). */
+int vll_resident_voxels(vll_context *ctx, vll_voxel *voxels, int64_t capacity, int64_t *total);
+
 /* Use `stream` (a cudaStream_t) for this context's work; NULL restores a
  * private stream.  vll_get_stream returns the stream in use. */
 int vll_set_stream(vll_context *ctx, void *stream);

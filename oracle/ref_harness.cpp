@@ -422,6 +422,38 @@ long ref_call_vertical_line_locus(void *fn, const vll_level_desc *d, const vll_u
     return acc;
 }
 
+/* Matching_SETSM's voxel-route inner loop (setsm_code.cpp:3743-3844) over
+ * `n_iter` iterations on ONE VOXEL** array: InitializeVoxel, VerticalLineLocus
+ * and AWNCC per iteration (iteration numbers in iters[]), through the
+ * functions at fn_init / fn_vll / fn_awncc (nullptr: the reference's own),
+ * rows freed at the end as the caller does (:4581-4585).  gridpt3 and ncc
+ * in/out; acc[i] receives each iteration's Accessable_grid. */
+void ref_call_voxel_iterations(void *fn_init, void *fn_vll, void *fn_awncc, const vll_level_desc *d,
+                               vll_ugrid *gridpt3, vll_nccresult *ncc, int n_iter,
+                               const int *iters, long *acc) {
+    RefLevel L(d);
+    const long n = L.grid_length;
+    VOXEL **rows = (VOXEL **)calloc((size_t)n, sizeof(VOXEL *));
+    init_voxel_signature fi = fn_init ? reinterpret_cast<init_voxel_signature>(fn_init)
+                                      : &InitializeVoxel;
+    vll_signature fv = fn_vll ? reinterpret_cast<vll_signature>(fn_vll) : &VerticalLineLocus;
+    awncc_signature fa = fn_awncc ? reinterpret_cast<awncc_signature>(fn_awncc) : &AWNCC;
+    const int max_voxel = (int)((d->minmax_height[1] - d->minmax_height[0]) / d->height_step);
+    for (int k = 0; k < n_iter; ++k) {
+        L.iteration = (unsigned char)iters[k];
+        fi(L.proinfo, rows, L.li, reinterpret_cast<UGRID *>(gridpt3),
+           reinterpret_cast<NCCresult *>(ncc), iters[k], d->minmax_height);
+        acc[k] = fv(rows, L.proinfo, reinterpret_cast<NCCresult *>(ncc), L.li,
+                    reinterpret_cast<const UGRID *>(gridpt3), (uint8)iters[k], d->minmax_height);
+        fa(L.proinfo, rows, L.grid_size, reinterpret_cast<UGRID *>(gridpt3),
+           reinterpret_cast<NCCresult *>(ncc), d->height_step, (uint8)d->pyramid_step,
+           (uint8)iters[k], max_voxel);
+    }
+    for (long i = 0; i < n; ++i)
+        if (rows[i]) free(rows[i]);
+    free(rows);
+}
+
 /* VerticalLineLocus_Ortho (setsm_code.cpp:8234-8533) for the triangle
  * three[0..2] = ref1, ref2, target; out = {F_Height, F_sncc} (F_sncc keeps
  * the value passed in out[1] when no height is found); returns its value. */

@@ -479,3 +479,22 @@ def tin_create(pts: np.ndarray, min_max, resolution: float) -> np.ndarray:
         if n <= cap:
             return out[:n]
         cap = n
+
+
+def call_voxel_iterations(fns, inputs, ncc: np.ndarray, iters) -> list:
+    """InitializeVoxel -> VerticalLineLocus -> AWNCC per iteration on one
+    VOXEL** array, through the functions at fns = (init, vll, awncc)
+    addresses (None: the reference's own); gridpt3 / ncc in place.  Returns
+    each iteration's Accessable_grid."""
+    L = lib()
+    vp = C.c_void_p
+    L.ref_call_voxel_iterations.argtypes = [vp, vp, vp, C.POINTER(abi.LevelDesc), vp, vp, C.c_int,
+                                            vp, vp]
+    L.ref_call_voxel_iterations.restype = None
+    d = inputs.desc()
+    it = np.ascontiguousarray(iters, dtype=np.int32)
+    acc = np.zeros(len(it), dtype=np.int64)
+    with _StdoutToStderr():
+        L.ref_call_voxel_iterations(fns[0], fns[1], fns[2], C.byref(d), inputs.gridpt3.ctypes.data,
+                                    ncc.ctypes.data, len(it), it.ctypes.data, acc.ctypes.data)
+    return [int(a) for a in acc]

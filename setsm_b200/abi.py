@@ -15,6 +15,8 @@ VLL_ABI_VERSION = 3
 VLL_MAX_IMAGES = 8
 
 VLL_OK = 0
+VLL_RESIDENT_PLANES = 1
+VLL_RESIDENT_VOXELS = 2
 VLL_ERR_INVALID = -1
 VLL_ERR_UNSUPPORTED = -2
 VLL_ERR_CUDA = -3

@@ -24,6 +24,10 @@ namespace {
 struct Buf {
     void *p = nullptr;
     size_t cap = 0;
+    // the host bytes the buffer holds a copy of (resident planes)
+    const void *src = nullptr;
+    size_t src_bytes = 0;
+    uint64_t src_fp = 0;
 };
 
 cudaError_t ensure(Buf &b, size_t n) {
@@ -32,6 +36,7 @@ cudaError_t ensure(Buf &b, size_t n) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
+    b.src = nullptr;
     cudaError_t e = cudaMalloc(&b.p, n);
     if (e == cudaSuccess) b.cap = n;
     return e;
@@ -41,6 +46,26 @@ void release(Buf &b) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
+    b.src = nullptr;
+}
+
+// Fingerprint of a host buffer: FNV-1a over 64 blocks of 64 bytes spread
+// evenly over it (the whole buffer when it is smaller than 8 KB), the last
+// 64 bytes and the size.
+uint64_t sample_fingerprint(const void *p, size_t n) {
+    const unsigned char *b = (const unsigned char *)p;
+    uint64_t h = 1469598103934665603ull ^ (uint64_t)n;
+    auto mix = [&](size_t off, size_t len) {
+        for (size_t i = 0; i < len; ++i) h = (h ^ b[off + i]) * 1099511628211ull;
+    };
+    if (n <= 8192) {
+        mix(0, n);
+        return h;
+    }
+    const size_t step = (n - 64) / 63;
+    for (int k = 0; k < 64; ++k) mix((size_t)k * step, 64);
+    mix(n - 64, 64);
+    return h;
 }
 
 thread_local std::string g_last_error;
@@ -68,6 +93,10 @@ struct vll_context {
     Buf sgm_lr;                        // SGM: the 8 directions' costs per slot
     Buf tin_pts, tin_tris, tin_scratch;  // Ortho_blunder: points, triangles, work arrays
     vll::TinWork tin_work;             // TINCreate_list: work arrays
+    int residency = 0;                 // VLL_RESIDENT_* flags
+    Buf rvox, rvox_off;                // resident voxel packing and its offsets
+    int64_t rvox_total = -1;           // its length (-1: none)
+    int64_t rvox_nodes = 0;
     vll::SplitBuffers split;
     vll::SplitTuning tuning;
     void *set = nullptr;               // SetResources of batch calls (vll_capi.cu)
@@ -556,7 +585,23 @@ float *sgm_scratch(vll_context *ctx, int64_t n_slots) {
 
 int upload(vll_context *ctx, Buf &b, const void *src, size_t n) {
     VLL_CUDA(ctx, ensure(b, n));
+    b.src = nullptr;
     if (n) VLL_CUDA(ctx, cudaMemcpyAsync(b.p, src, n, cudaMemcpyHostToDevice, ctx->stream));
+    return VLL_OK;
+}
+
+// An image plane or grid array: with VLL_RESIDENT_PLANES, sent only when
+// the buffer does not hold these host bytes already (pointer, size and
+// sampled fingerprint).
+int upload_plane(vll_context *ctx, Buf &b, const void *src, size_t n) {
+    if (!(ctx->residency & VLL_RESIDENT_PLANES)) return upload(ctx, b, src, n);
+    const uint64_t fp = sample_fingerprint(src, n);
+    if (b.p && b.src == src && b.src_bytes == n && b.src_fp == fp) return VLL_OK;
+    int rc = upload(ctx, b, src, n);
+    if (rc) return rc;
+    b.src = src;
+    b.src_bytes = n;
+    b.src_fp = fp;
     return VLL_OK;
 }
 
@@ -751,6 +796,8 @@ void vll_destroy(vll_context *ctx) {
     release(ctx->pre_ori);
     release(ctx->sumcost);
     release(ctx->sgm_lr);
+    release(ctx->rvox);
+    release(ctx->rvox_off);
     release(ctx->tin_pts);
     release(ctx->tin_tris);
     release(ctx->tin_scratch);
@@ -834,12 +881,19 @@ int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc, const 
     const int64_t N = P.n_nodes;
     const bool voxel_route = !P.cmr && !P.is_ra;
     std::vector<int64_t> off;
+    bool resident_vox = false;
     if (voxel_route) {
         off.resize((size_t)N + 1);
         off[0] = 0;
         for (int64_t i = 0; i < N; ++i) off[i + 1] = off[i] + nccresult[i].NumOfHeight;
-        if (off[N] > 0 && (!voxels || voxel_capacity < off[N]))
+        resident_vox = !voxels && (ctx->residency & VLL_RESIDENT_VOXELS);
+        if (resident_vox) {
+            if (ctx->rvox_total != off[N] || ctx->rvox_nodes != N)
+                return fail(ctx, VLL_ERR_INVALID,
+                            "no resident voxel packing matching sum(NumOfHeight)");
+        } else if (off[N] > 0 && (!voxels || voxel_capacity < off[N])) {
             return fail(ctx, VLL_ERR_CAPACITY, "voxel buffer smaller than sum(NumOfHeight)");
+        }
     }
     // images (only what the level reads)
     const bool next = vll::needs_next(P);
@@ -848,9 +902,9 @@ int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc, const 
         if (!s.selected) continue;
         if (!s.image || !s.mag || !s.ori) return fail(ctx, VLL_ERR_INVALID, "null image plane");
         const size_t n = (size_t)s.width * s.height;
-        if ((rc = upload(ctx, ctx->img[ti][0], s.image, n * 2))) return rc;
-        if ((rc = upload(ctx, ctx->img[ti][1], s.mag, n * 2))) return rc;
-        if ((rc = upload(ctx, ctx->img[ti][2], s.ori, n))) return rc;
+        if ((rc = upload_plane(ctx, ctx->img[ti][0], s.image, n * 2))) return rc;
+        if ((rc = upload_plane(ctx, ctx->img[ti][1], s.mag, n * 2))) return rc;
+        if ((rc = upload_plane(ctx, ctx->img[ti][2], s.ori, n))) return rc;
         P.im[ti].img = (const uint16_t *)ctx->img[ti][0].p;
         P.im[ti].mag = (const uint16_t *)ctx->img[ti][1].p;
         P.im[ti].ori = (const uint8_t *)ctx->img[ti][2].p;
@@ -858,23 +912,26 @@ int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc, const 
             if (!s.image_next || !s.mag_next || !s.ori_next || s.width_next < 2 || s.height_next < 2)
                 return fail(ctx, VLL_ERR_INVALID, "combined level needs the next pyramid level");
             const size_t nn = (size_t)s.width_next * s.height_next;
-            if ((rc = upload(ctx, ctx->img[ti][3], s.image_next, nn * 2))) return rc;
-            if ((rc = upload(ctx, ctx->img[ti][4], s.mag_next, nn * 2))) return rc;
-            if ((rc = upload(ctx, ctx->img[ti][5], s.ori_next, nn))) return rc;
+            if ((rc = upload_plane(ctx, ctx->img[ti][3], s.image_next, nn * 2))) return rc;
+            if ((rc = upload_plane(ctx, ctx->img[ti][4], s.mag_next, nn * 2))) return rc;
+            if ((rc = upload_plane(ctx, ctx->img[ti][5], s.ori_next, nn))) return rc;
             P.im[ti].img_n = (const uint16_t *)ctx->img[ti][3].p;
             P.im[ti].mag_n = (const uint16_t *)ctx->img[ti][4].p;
             P.im[ti].ori_n = (const uint8_t *)ctx->img[ti][5].p;
         }
     }
-    if ((rc = upload(ctx, ctx->wgs, desc->grid_wgs, (size_t)N * 16))) return rc;
-    if ((rc = upload(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
+    if ((rc = upload_plane(ctx, ctx->wgs, desc->grid_wgs, (size_t)N * 16))) return rc;
+    if ((rc = upload_plane(ctx, ctx->pts, desc->grid_pts, (size_t)N * 16))) return rc;
     if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
     if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
     P.grid_wgs = (const double *)ctx->wgs.p;
     P.grid_pts = (const double *)ctx->pts.p;
     P.gp3 = (const vll_ugrid *)ctx->gp3.p;
     P.ncc = (vll_nccresult *)ctx->ncc.p;
-    if (voxel_route) {
+    if (voxel_route && resident_vox) {
+        P.vox = (vll_voxel *)ctx->rvox.p;
+        P.vox_off = (const int64_t *)ctx->rvox_off.p;
+    } else if (voxel_route) {
         if ((rc = upload(ctx, ctx->voxoff, off.data(), off.size() * sizeof(int64_t)))) return rc;
         if ((rc = upload(ctx, ctx->vox, voxels, (size_t)off[N] * sizeof(vll_voxel)))) return rc;
         P.vox = (vll_voxel *)ctx->vox.p;
@@ -885,7 +942,7 @@ int vll_vertical_line_locus(vll_context *ctx, const vll_level_desc *desc, const 
     if (rc) return rc;
     VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->ncc.p, (size_t)N * sizeof(vll_nccresult),
                                   cudaMemcpyDeviceToHost, ctx->stream));
-    if (voxel_route && off[N] > 0)
+    if (voxel_route && !resident_vox && off[N] > 0)
         VLL_CUDA(ctx, cudaMemcpyAsync(voxels, ctx->vox.p, (size_t)off[N] * sizeof(vll_voxel),
                                       cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1014,16 +1071,26 @@ int vll_awncc_peaks(vll_context *ctx, const vll_level_desc *desc, const vll_ugri
         off[i + 1] = off[i] + nccresult[i].NumOfHeight;
         if (nccresult[i].NumOfHeight > max_h) max_h = nccresult[i].NumOfHeight;
     }
-    if (off[N] > 0 && (!voxels || voxel_capacity < off[N]))
+    const bool resident_vox = !voxels && (ctx->residency & VLL_RESIDENT_VOXELS);
+    if (resident_vox) {
+        if (ctx->rvox_total != off[N] || ctx->rvox_nodes != N)
+            return fail(ctx, VLL_ERR_INVALID, "no resident voxel packing matching sum(NumOfHeight)");
+    } else if (off[N] > 0 && (!voxels || voxel_capacity < off[N])) {
         return fail(ctx, VLL_ERR_CAPACITY, "voxel buffer smaller than sum(NumOfHeight)");
+    }
     if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
     if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
-    if ((rc = upload(ctx, ctx->voxoff, off.data(), off.size() * sizeof(int64_t)))) return rc;
-    if ((rc = upload(ctx, ctx->vox, voxels, (size_t)off[N] * sizeof(vll_voxel)))) return rc;
     P.gp3 = (const vll_ugrid *)ctx->gp3.p;
     P.ncc = (vll_nccresult *)ctx->ncc.p;
-    P.vox = (vll_voxel *)ctx->vox.p;
-    P.vox_off = (const int64_t *)ctx->voxoff.p;
+    if (resident_vox) {
+        P.vox = (vll_voxel *)ctx->rvox.p;
+        P.vox_off = (const int64_t *)ctx->rvox_off.p;
+    } else {
+        if ((rc = upload(ctx, ctx->voxoff, off.data(), off.size() * sizeof(int64_t)))) return rc;
+        if ((rc = upload(ctx, ctx->vox, voxels, (size_t)off[N] * sizeof(vll_voxel)))) return rc;
+        P.vox = (vll_voxel *)ctx->vox.p;
+        P.vox_off = (const int64_t *)ctx->voxoff.p;
+    }
     if ((rc = upload_level_block(ctx, P))) return rc;
     if (!ctx->e0) {
         VLL_CUDA(ctx, cudaEventCreate(&ctx->e0));
@@ -1253,7 +1320,7 @@ static int init_voxel_run(vll_context *ctx, const vll_level_desc *desc, vll_ugri
     const int64_t N = P.n_nodes;
     if (N > 0x7fffffff) return fail(ctx, VLL_ERR_INVALID, "grid too large");
     if (!grid_on_device) {
-        if ((rc = upload(ctx, ctx->wgs, desc->grid_wgs, (size_t)N * 16))) return rc;
+        if ((rc = upload_plane(ctx, ctx->wgs, desc->grid_wgs, (size_t)N * 16))) return rc;
         P.grid_wgs = (const double *)ctx->wgs.p;
     }
     P.gp3 = d_gp3;
@@ -1277,13 +1344,67 @@ static int init_voxel_run(vll_context *ctx, const vll_level_desc *desc, vll_ugri
     return VLL_OK;
 }
 
+// InitializeVoxel with the voxel packing kept in the context: the input rows
+// are the caller's (the first call of a session) or the previous packing
+// (when its length matches the old NumOfHeight sum); the output replaces it.
+// Records go both ways, voxels stay on the device.
+static int init_voxel_resident(vll_context *ctx, const vll_level_desc *desc, vll_ugrid *gridpt3,
+                               vll_nccresult *nccresult, const vll_voxel *voxels_in,
+                               int64_t old_total, int64_t *n_out) {
+    const int64_t N = desc->grid_width * desc->grid_height;
+    int rc;
+    if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
+    if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
+    const vll_voxel *d_vin = nullptr;
+    if (voxels_in && old_total > 0) {
+        if ((rc = upload(ctx, ctx->rvox, voxels_in, (size_t)old_total * sizeof(vll_voxel))))
+            return rc;
+        d_vin = (const vll_voxel *)ctx->rvox.p;
+    } else if (ctx->rvox_total == old_total && ctx->rvox_nodes == N && old_total > 0) {
+        d_vin = (const vll_voxel *)ctx->rvox.p;
+    }
+    // the output packing goes to ctx->vox (then swapped in), sized from the
+    // ranges and grown once if that estimate falls short
+    int64_t cap = 1;
+    for (int64_t i = 0; i < N; ++i) {
+        const int64_t span = (int64_t)gridpt3[i].maxHeight - gridpt3[i].minHeight +
+                             (int64_t)nccresult[i].maxHeight - nccresult[i].minHeight;
+        cap += (int64_t)((span < 0 ? -span : span) / desc->height_step) + 8 +
+               nccresult[i].NumOfHeight;
+    }
+    VLL_CUDA(ctx, ensure(ctx->voxoff, (size_t)(N + 1) * sizeof(int64_t)));
+    int64_t total = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        VLL_CUDA(ctx, ensure(ctx->vox, (size_t)cap * sizeof(vll_voxel)));
+        ctx->vox.src = nullptr;
+        rc = init_voxel_run(ctx, desc, (vll_ugrid *)ctx->gp3.p, (vll_nccresult *)ctx->ncc.p, d_vin,
+                            (vll_voxel *)ctx->vox.p, cap, (int64_t *)ctx->voxoff.p, &total, false,
+                            nullptr);
+        if (rc != VLL_ERR_CAPACITY) break;
+        cap = total;
+    }
+    *n_out = total;
+    if (rc) return rc == VLL_ERR_CAPACITY ? fail(ctx, rc, "voxel packing estimate") : rc;
+    std::swap(ctx->vox, ctx->rvox);
+    std::swap(ctx->voxoff, ctx->rvox_off);
+    ctx->rvox_total = total;
+    ctx->rvox_nodes = N;
+    VLL_CUDA(ctx, cudaMemcpyAsync(gridpt3, ctx->gp3.p, (size_t)N * sizeof(vll_ugrid),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaMemcpyAsync(nccresult, ctx->ncc.p, (size_t)N * sizeof(vll_nccresult),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
 int vll_initialize_voxel(vll_context *ctx, const vll_level_desc *desc, vll_ugrid *gridpt3,
                          vll_nccresult *nccresult, const vll_voxel *voxels_in,
                          vll_voxel *voxels_out, int64_t capacity, int64_t *n_out) {
     NvtxRange nvtx_range("vll_initialize_voxel");
     if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    const bool resident = !voxels_out && (ctx->residency & VLL_RESIDENT_VOXELS);
     if (!desc || !gridpt3 || !nccresult || !n_out || !desc->grid_wgs || capacity < 0 ||
-        (capacity > 0 && !voxels_out))
+        (capacity > 0 && !voxels_out && !resident))
         return fail(ctx, VLL_ERR_INVALID, "null argument");
     VLL_CUDA(ctx, cudaSetDevice(ctx->device));
     const int64_t N = desc->grid_width * desc->grid_height;
@@ -1291,6 +1412,8 @@ int vll_initialize_voxel(vll_context *ctx, const vll_level_desc *desc, vll_ugrid
     int64_t old_total = 0;
     for (int64_t i = 0; i < N; ++i) old_total += nccresult[i].NumOfHeight;
     int rc;
+    if (resident)
+        return init_voxel_resident(ctx, desc, gridpt3, nccresult, voxels_in, old_total, n_out);
     if ((rc = upload(ctx, ctx->gp3, gridpt3, (size_t)N * sizeof(vll_ugrid)))) return rc;
     if ((rc = upload(ctx, ctx->ncc, nccresult, (size_t)N * sizeof(vll_nccresult)))) return rc;
     const vll_voxel *d_vin = nullptr;
@@ -2118,6 +2241,40 @@ int vll_tin_create(vll_context *ctx, const vll_point3 *pts, int64_t n_pts, const
     if (rc) return fail(ctx, rc, err);
     if (*count > 0)
         VLL_CUDA(ctx, cudaMemcpyAsync(tris, ctx->tin_tris.p, (size_t)*count * sizeof(vll_tri),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return VLL_OK;
+}
+
+// ---- residency of the host-buffer calls ------------------------------------
+int vll_set_residency(vll_context *ctx, int flags) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    if (flags & ~(VLL_RESIDENT_PLANES | VLL_RESIDENT_VOXELS))
+        return fail(ctx, VLL_ERR_INVALID, "unknown residency flag");
+    ctx->residency = flags;
+    if (!(flags & VLL_RESIDENT_VOXELS)) ctx->rvox_total = -1;
+    return VLL_OK;
+}
+
+int vll_get_residency(const vll_context *ctx) { return ctx ? ctx->residency : 0; }
+
+int vll_resident_reset(vll_context *ctx) {
+    if (!ctx) return fail(nullptr, VLL_ERR_INVALID, "null context");
+    ctx->rvox_total = -1;
+    ctx->rvox_nodes = 0;
+    return VLL_OK;
+}
+
+int vll_resident_voxels(vll_context *ctx, vll_voxel *voxels, int64_t capacity, int64_t *total) {
+    if (!ctx || !total) return fail(ctx, VLL_ERR_INVALID, "null argument");
+    if (ctx->rvox_total < 0) return fail(ctx, VLL_ERR_INVALID, "no resident voxel packing");
+    *total = ctx->rvox_total;
+    if (ctx->rvox_total > capacity || (ctx->rvox_total > 0 && !voxels))
+        return fail(ctx, VLL_ERR_CAPACITY, "resident packing longer than the buffer");
+    VLL_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (ctx->rvox_total > 0)
+        VLL_CUDA(ctx, cudaMemcpyAsync(voxels, ctx->rvox.p,
+                                      (size_t)ctx->rvox_total * sizeof(vll_voxel),
                                       cudaMemcpyDeviceToHost, ctx->stream));
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return VLL_OK;

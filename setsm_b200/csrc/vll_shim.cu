@@ -16,6 +16,15 @@ struct ShimState {
     vll_context *ctx = nullptr;
     int kernel = VLL_KERNEL_SPLIT;
     std::vector<vll_voxel> packed;
+    bool resident_voxels = false;   // SETSM_VLL_RESIDENT (read per call)
+    // The VOXEL** array whose rows the context holds on the device, and the
+    // drop-in that last wrote them there.  A session continues only along
+    // InitializeVoxel -> VerticalLineLocus -> AWNCC -> InitializeVoxel ... on
+    // the same array; any other order (a reference function in between, a
+    // new array) falls back to the host rows.
+    tagVoxelinfo **session = nullptr;
+    int64_t session_nodes = 0;
+    enum { kNone, kInit, kVll, kAwncc } last = kNone;
 };
 
 ShimState &state() {
@@ -39,6 +48,18 @@ vll_context *shim_context() {
         if (vll_create(dev ? atoi(dev) : 0, &s.ctx) != VLL_OK)
             die("cannot create the GPU context", vll_last_error(nullptr));
     }
+    // SETSM_VLL_RESIDENT: unset = image planes and grid arrays stay on the
+    // device between calls (re-sent when pointer, size or fingerprint
+    // change); "1" = voxel rows also stay there between the InitializeVoxel,
+    // VerticalLineLocus and AWNCC drop-ins (when all three replace the
+    // reference's, called as Matching_SETSM calls them); "0" = nothing stays
+    const char *res = getenv("SETSM_VLL_RESIDENT");
+    int flags = VLL_RESIDENT_PLANES;
+    if (res && strcmp(res, "0") == 0) flags = 0;
+    if (res && strcmp(res, "1") == 0) flags = VLL_RESIDENT_PLANES | VLL_RESIDENT_VOXELS;
+    s.resident_voxels = (flags & VLL_RESIDENT_VOXELS) != 0;
+    if (vll_get_residency(s.ctx) != flags && vll_set_residency(s.ctx, flags) != VLL_OK)
+        die("cannot set residency", vll_last_error(s.ctx));
     return s.ctx;
 }
 
@@ -140,9 +161,14 @@ int VerticalLineLocus(tagVoxelinfo **grid_voxel, const ProjectInfo *proinfo,
 
     const int64_t n = d.grid_width * d.grid_height;
     const bool voxel_route = !d.check_matching_rate && !d.is_ra;
+    // within an InitializeVoxel session the rows are on the device already
+    const bool in_session = voxel_route && st.resident_voxels && grid_voxel &&
+                            grid_voxel == st.session && n == st.session_nodes &&
+                            st.last == ShimState::kInit;
+    st.last = in_session ? ShimState::kVll : ShimState::kNone;
     vll_voxel *vox = nullptr;
     int64_t nvox = 0;
-    if (voxel_route && grid_voxel) {
+    if (voxel_route && grid_voxel && !in_session) {
         for (int64_t i = 0; i < n; ++i) nvox += nccresult[i].NumOfHeight;
         st.packed.resize((size_t)(nvox > 0 ? nvox : 1));
         vox = st.packed.data();
@@ -252,9 +278,40 @@ void InitializeVoxel(const ProjectInfo *proinfo, tagVoxelinfo **grid_voxel, tagl
                              (int64_t)nccresult[i].maxHeight - nccresult[i].minHeight;
         cap += (int64_t)((span < 0 ? -span : span) / d.height_step) + 8 + old_n[(size_t)i];
     }
-    // the rows are rebuilt here from the new NumOfHeight, so no old rows go up
     int64_t total = 0;
-    for (int attempt = 0; attempt < 2; ++attempt) {
+    if (st.resident_voxels) {
+        // a new VOXEL** array starts a new session; rows it already holds
+        // (carried over by the reference) start the device packing
+        const vll_voxel *vin = nullptr;
+        if (grid_voxel != st.session || n != st.session_nodes || st.last != ShimState::kAwncc) {
+            vll_resident_reset(ctx);
+            st.session = grid_voxel;
+            st.session_nodes = n;
+            int64_t old_total = 0;
+            for (int64_t i = 0; i < n; ++i) old_total += old_n[(size_t)i];
+            if (old_total > 0) {
+                st.packed.resize((size_t)old_total);
+                int64_t o = 0;
+                for (int64_t i = 0; i < n; ++i) {
+                    const int k = old_n[(size_t)i];
+                    if (k <= 0) continue;
+                    if (grid_voxel[i])
+                        memcpy(st.packed.data() + o, grid_voxel[i], (size_t)k * sizeof(vll_voxel));
+                    else
+                        memset(st.packed.data() + o, 0, (size_t)k * sizeof(vll_voxel));
+                    o += k;
+                }
+                vin = st.packed.data();
+            }
+        }
+        if (vll_initialize_voxel(ctx, &d, reinterpret_cast<vll_ugrid *>(GridPT3),
+                                 reinterpret_cast<vll_nccresult *>(nccresult), vin, nullptr, 0,
+                                 &total) != VLL_OK)
+            die("InitializeVoxel: GPU call failed", vll_last_error(ctx));
+        st.last = ShimState::kInit;
+    }
+    // the rows are rebuilt here from the new NumOfHeight, so no old rows go up
+    for (int attempt = 0; attempt < 2 && !st.resident_voxels; ++attempt) {
         st.packed.resize((size_t)cap);
         const int rc = vll_initialize_voxel(ctx, &d, reinterpret_cast<vll_ugrid *>(GridPT3),
                                             reinterpret_cast<vll_nccresult *>(nccresult), nullptr,
@@ -312,20 +369,25 @@ void AWNCC(ProjectInfo *proinfo, tagVoxelinfo **grid_voxel, tagCSize Size_Grid2D
         d.images[ti].width = d.images[ti].height = 2;
     }
     const int64_t n = d.grid_width * d.grid_height;
+    const bool in_session = st.resident_voxels && grid_voxel && grid_voxel == st.session &&
+                            n == st.session_nodes && st.last == ShimState::kVll;
+    st.last = in_session ? ShimState::kAwncc : ShimState::kNone;
     int64_t nvox = 0;
-    for (int64_t i = 0; i < n; ++i) nvox += nccresult[i].NumOfHeight;
-    st.packed.resize((size_t)(nvox > 0 ? nvox : 1));
-    int64_t o = 0;
-    for (int64_t i = 0; i < n; ++i) {
-        const int k = nccresult[i].NumOfHeight;
-        if (k > 0) {
-            memcpy(st.packed.data() + o, grid_voxel[i], (size_t)k * sizeof(vll_voxel));
-            o += k;
+    if (!in_session) {
+        for (int64_t i = 0; i < n; ++i) nvox += nccresult[i].NumOfHeight;
+        st.packed.resize((size_t)(nvox > 0 ? nvox : 1));
+        int64_t o = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const int k = nccresult[i].NumOfHeight;
+            if (k > 0) {
+                memcpy(st.packed.data() + o, grid_voxel[i], (size_t)k * sizeof(vll_voxel));
+                o += k;
+            }
         }
     }
     if (vll_awncc_peaks(ctx, &d, reinterpret_cast<const vll_ugrid *>(GridPT3),
-                        reinterpret_cast<vll_nccresult *>(nccresult), st.packed.data(), nvox,
-                        nullptr) != VLL_OK)
+                        reinterpret_cast<vll_nccresult *>(nccresult),
+                        in_session ? nullptr : st.packed.data(), nvox, nullptr) != VLL_OK)
         die("AWNCC: GPU call failed", vll_last_error(ctx));
 }
 

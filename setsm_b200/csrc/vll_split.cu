@@ -430,7 +430,10 @@ __device__ void node_exact_chunked(const DevLevel &P, int64_t pt, int K, const P
                                            ? q_voxel(__ddiv_rn(o.sum_incc, o.count_incc))
                                            : q_voxel(-1.0);
                     }
-                    if (first && P.dbg_rho) P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
+                    // debug values: every slot on a first evaluation, else only
+                    // slots that have no FP32 value (NaN)
+                    if (P.dbg_rho && (first || isnan(P.dbg_rho[P.dbg_off[pt] + k])))
+                        P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
                     count++;
                 } else if (o.orient_reject) {
                     out = (double)kRejected;
@@ -734,7 +737,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     }
                 }
                 float rho_v = kNotEvaluated, incc_v = 0.f;
-                bool all_pos = false;
+                bool all_pos = false, deferred = false;
                 if (status == 1) {
                     rho_v = kRejected;
                 } else if (status == 2) {
@@ -764,6 +767,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                         // evaluates the slot in FP64
                         rho_v = 0.f;
                         incc_v = __int_as_float(0x7fc00000);
+                        deferred = true;
                     }
                     evals++;
                 }
@@ -777,7 +781,9 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     W.m.evaluated[k0 >> 5] = em;
                     W.m.need[k0 >> 5] = nm;
                 }
-                if (P.dbg_rho && status == 2) P.dbg_rho[P.dbg_off[pt] + k] = (double)rho_v;
+                if (P.dbg_rho && status == 2)
+                    P.dbg_rho[P.dbg_off[pt] + k] = deferred ? __longlong_as_double(0x7ff8000000000000ll)
+                                                            : (double)rho_v;
                 if (k < K && voxels) {
                     vll_voxel *v = vrow + k;
                     if (status == 1) v->flag_cal = 0;
@@ -1104,6 +1110,8 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
                 const SlotOut o = eval_slot_warp_any(P, pt, S, hh, cnt_g, sum_g,
                                                     reinterpret_cast<double *>(boxes), lane);
                 if (lane == 0) {
+                    if (P.dbg_rho && o.evaluated && isnan(P.dbg_rho[P.dbg_off[pt] + k]))
+                        P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
                     W.exact_rho[j] = o.rho;
                     W.exact_incc[j] = o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc) : -1.0;
                     if (vrow) {

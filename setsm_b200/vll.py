@@ -39,6 +39,7 @@ EXPORTED = [
     "vll_set_height_range_device", "vll_blunder_detection_tin",
     "vll_blunder_detection_tin_device", "vll_tin_rerun_count", "vll_debug_tin_threshold",
     "vll_tin_create", "vll_tin_create_device",
+    "vll_set_residency", "vll_get_residency", "vll_resident_reset", "vll_resident_voxels",
 ]
 
 _lib = None
@@ -123,6 +124,10 @@ def load():
     L.vll_set_height_range_device.argtypes = L.vll_set_height_range.argtypes
     L.vll_tin_create.argtypes = [vp, vp, i64, vp, dbl, vp, i64, C.POINTER(i64)]
     L.vll_tin_create_device.argtypes = L.vll_tin_create.argtypes
+    L.vll_set_residency.argtypes = [vp, i32]
+    L.vll_get_residency.argtypes = [vp]
+    L.vll_resident_reset.argtypes = [vp]
+    L.vll_resident_voxels.argtypes = [vp, vp, i64, C.POINTER(i64)]
     _lib = L
     return L
 
@@ -213,14 +218,15 @@ class Context:
             diag.update({n: int(v) for n, v in zip(self.DIAG_NAMES, dg) if n != "_"})
         return out[:off[-1]], off
 
-    def awncc(self, inputs, nccresult: np.ndarray, voxels: np.ndarray) -> abi.Stats:
+    def awncc(self, inputs, nccresult: np.ndarray, voxels: np.ndarray | None) -> abi.Stats:
         """AWNCC over the packed voxel rows (setsm_code.cpp:7001-7702): the
         semi-global aggregation when Pyramid_step <= SGM_py, then the peak loop."""
         d = inputs.desc()
         st = abi.Stats()
-        vptr = voxels.ctypes.data if voxels.size else None
+        vptr = voxels.ctypes.data if voxels is not None and voxels.size else None
+        cap = voxels.size if voxels is not None else 0
         self._check(load().vll_awncc_peaks(self._h, C.byref(d), inputs.gridpt3.ctypes.data,
-                                           nccresult.ctypes.data, vptr, voxels.size, C.byref(st)))
+                                           nccresult.ctypes.data, vptr, cap, C.byref(st)))
         return st
 
     # ---- orthoimage-window variants ------------------------------------------------
@@ -281,6 +287,39 @@ class Context:
                                              len(pts), tris.ctypes.data, len(tris),
                                              inputs.gridpt3.ctypes.data, C.byref(rounds)))
         return rounds.value
+
+    # ---- residency of the host-buffer calls -----------------------------------------
+    def set_residency(self, planes: bool = False, voxels: bool = False) -> None:
+        """Image planes / grid arrays kept on the device between calls
+        (re-sent when their pointer, size or sampled fingerprint changes), and
+        the voxel packing kept between InitializeVoxel, VerticalLineLocus and
+        AWNCC calls given no voxel array (initialize_voxel_resident)."""
+        self._check(load().vll_set_residency(self._h, (abi.VLL_RESIDENT_PLANES if planes else 0)
+                                             | (abi.VLL_RESIDENT_VOXELS if voxels else 0)))
+
+    def resident_reset(self) -> None:
+        self._check(load().vll_resident_reset(self._h))
+
+    def resident_voxels(self) -> np.ndarray:
+        """A host copy of the resident voxel packing."""
+        n = C.c_int64(0)
+        rc = load().vll_resident_voxels(self._h, None, 0, C.byref(n))
+        if rc not in (abi.VLL_OK, abi.VLL_ERR_CAPACITY):
+            self._check(rc)
+        out = np.zeros(max(n.value, 1), dtype=abi.VOXEL_DTYPE)
+        self._check(load().vll_resident_voxels(self._h, out.ctypes.data, out.size, C.byref(n)))
+        return out[: n.value]
+
+    def initialize_voxel_resident(self, inputs, ncc: np.ndarray,
+                                  voxels_in: np.ndarray | None = None) -> int:
+        """InitializeVoxel keeping the new packing on the device (residency
+        with voxels on); returns its length."""
+        d = inputs.desc()
+        n = C.c_int64()
+        vin = voxels_in.ctypes.data if voxels_in is not None and voxels_in.size else None
+        self._check(load().vll_initialize_voxel(self._h, C.byref(d), inputs.gridpt3.ctypes.data,
+                                                ncc.ctypes.data, vin, None, 0, C.byref(n)))
+        return n.value
 
     def initialize_voxel(self, inputs, ncc: np.ndarray,
                          voxels_in: np.ndarray | None = None) -> np.ndarray:

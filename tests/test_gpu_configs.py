@@ -28,7 +28,7 @@ def _ncc_of(wl, ctx, template, kernel):
     from setsm_b200 import workloads
     wl.d_ncc.zero_()
     st = ctx.vertical_line_locus_device(wl.device_desc(template), wl.d_gp3.data_ptr(),
-                                        wl.d_ncc.data_ptr(), None, None, kernel)
+                                        wl.d_ncc.data_ptr(), None, None, kernel, stats=True)
     return workloads.ncc_host(wl), st
 
 
