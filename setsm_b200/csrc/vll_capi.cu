@@ -337,6 +337,8 @@ int run_device(vll_context *ctx, DevLevel &P, int kernel, vll_stats *stats) {
     if (rc) return rc;
     VLL_CUDA(ctx, ensure(ctx->counters, 8 * sizeof(unsigned long long)));
     VLL_CUDA(ctx, cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned long long), ctx->stream));
+    if (kernel != VLL_KERNEL_FP64_PLAIN && vll::split_supported(P))
+        vll::split_prepare_tma(P, ctx->tuning.box_margin);
     rc = upload_level_block(ctx, P);
     if (rc) return rc;
     const DevLevel *dP = (const DevLevel *)ctx->level.p;
@@ -495,6 +497,7 @@ int prepare_set(vll_context *ctx, SetResources &r, const vll_level_io *levels, i
             }
         }
     }
+    for (int l = 0; l < n; ++l) vll::split_prepare_tma(r.hl[l], ctx->tuning.box_margin);
     VLL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // staging may be in flight
     if (r.staging_cap < (size_t)n) {
         if (r.staging) cudaFreeHost(r.staging);

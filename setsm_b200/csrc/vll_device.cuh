@@ -75,6 +75,12 @@ struct DevLevel {
     double rot_cos[kRotTable];      // cos(-theta) for diff_theta = (i-kRotOffset)/2
     double rot_sin[kRotTable];
     DevImage im[VLL_MAX_IMAGES];
+    // Footprint tiles of the split kernel's window staging: tensor maps (TMA)
+    // of the reference [0] and target [1] images' intensity [.][0] and
+    // magnitude [.][1] planes with the level's tile of tma_w x tma_h texels
+    // (tma_w a multiple of 8), or tma_w[0] == 0 (staging by loads).
+    alignas(64) unsigned char tmap[2][2][128];
+    int tma_w[2], tma_h[2];
 };
 
 // ---- quantisers (Template.hpp:964-993) ------------------------------------

@@ -59,7 +59,7 @@ inline cudaError_t scan64(void *tmp, size_t &bytes, const int32_t *in, int64_t *
 constexpr float kBand = 4e-6f;
 constexpr double kEdge = 1e-7;          // coordinate distance to an integer / clamp
 constexpr int kSlotCap = 512;           // slots per node the peak kernel holds in shared memory
-constexpr int kExactCap = 64;           // exact slot values per node before a full FP64 pass
+constexpr int kWarpPerSlotMax = 8;      // re-checks per round done a warp per slot (more: a lane each)
 constexpr int kMaxRounds = 3;           // scan / re-check rounds before a full FP64 pass
 
 // Per-slot markers in the rho buffer (.x):
@@ -480,14 +480,22 @@ constexpr int kWinWarps = VLL_WIN_WARPS;
 struct WinShared {
     double horner[2][4][4];          // [image][num/den poly][a0..a3]
     double hnorm[2][2];              // [image] {h_off, 1 / h_scale}
-    double chunk[32];                // exact values of one 32-slot chunk
-    float vals[kSlotCap];            // FP32 rho per slot (+inf skipped, -inf rejected)
-    SlotMasks m;
+    vll_nccresult R;                 // the node's record, folded by lane 0
+    float vals[kSlotCap];            // FP32 rho per slot (+inf skipped, -inf rejected,
+                                     // NaN: no usable FP32 value)
+    float pre_v;                     // the scan's last evaluated slot: value,
+    int pre_dir, pre_k;              // direction and index
+    bool have;
     uint64_t mbar;                   // completion of the footprint's bulk copies
 };
 
 __host__ __device__ constexpr size_t win_boxes_offset() {
     return (sizeof(WinShared) * kWinWarps + 15) & ~(size_t)15;
+}
+
+// the TMA tiles follow the boxes, 128-byte aligned (warp_raw is a multiple of 128)
+__host__ __device__ constexpr size_t win_raw_offset(int warp_quads) {
+    return (win_boxes_offset() + (size_t)kWinWarps * warp_quads * 16 + 127) & ~(size_t)127;
 }
 
 // FP32 window statistics of one slot for the level's window half-size
@@ -521,13 +529,12 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     int64_t *__restrict__ pend_node, int64_t *__restrict__ pend_off,
     unsigned long long *__restrict__ counters, unsigned long long *__restrict__ ctl,
     int warp_quads, int warp_raw, int grab) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     WinShared &W = reinterpret_cast<WinShared *>(smem_raw)[warp];
     float4 *boxes = reinterpret_cast<float4 *>(smem_raw + win_boxes_offset()) + (size_t)warp * warp_quads;
-    unsigned char *raw = smem_raw + win_boxes_offset() + (size_t)kWinWarps * warp_quads * sizeof(float4) +
-                         (size_t)warp * warp_raw;
+    unsigned char *raw = smem_raw + win_raw_offset(warp_quads) + (size_t)warp * warp_raw;
     if (lane == 0) mbar_init(&W.mbar);
     __syncwarp();
     uint32_t phase = 0;   // parity of the mbarrier phase the next copies complete
@@ -587,11 +594,17 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     W.hnorm[im][1] = 1.0 / rpc[9];
                 }
             }
-            if (lane < kSlotCap / 32) {
-                W.m.evaluated[lane] = 0;
-                W.m.need[lane] = 0;
-                W.m.peak[lane] = 0;
+            if (lane == 0) {
+                W.R = P.ncc[pt];
+                W.have = false;
+                W.pre_v = -1.0f;
+                W.pre_dir = 0;
+                W.pre_k = -1;
             }
+            // per-lane running values of the streamed scan
+            float vmax = -100.0f, amb = -INFINITY, amb_peak = -INFINITY;
+            float b1 = -INFINITY, b2 = -INFINITY;
+            bool need = false;
             __syncwarp();
             for (int k0 = 0; k0 < K; k0 += 32) {
                 const int k = k0 + lane;
@@ -657,31 +670,32 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     rbh = ry1 - ry0 + 1;
                     tbw = tw | 1;
                     const int tbh = ty1 - ty0 + 1;
-                    // raw rows of the boxes for the bulk copies: texels [xa, xa + 8 n)
-                    // of each row, covering the pairs' right texels
+                    // the level's TMA tiles: texels [xa, xa + tma_w) x rows [y0, y0 +
+                    // tma_h) of each plane, xa = x0 rounded down to 8 (16 bytes)
                     const int rxa = rx0 & ~7, txa = tx0 & ~7;
-                    const int rnb = ((rx1 + 1 - rxa) / 8 + 1) * 16;
-                    const int tnb = ((tx1 + 1 - txa) / 8 + 1) * 16;
-                    const int raw_bytes = 2 * (rbh * rnb + tbh * tnb);
-                    if (rbw * rbh + tbw * tbh <= warp_quads && vec_ok && raw_bytes <= warp_raw) {
-                        // ---- bulk copies (TMA) of the raw rows, then conversion ----
-                        unsigned char *rI = raw, *rM = raw + rbh * rnb;
-                        unsigned char *tIr = raw + 2 * rbh * rnb, *tMr = tIr + tbh * tnb;
-                        if (lane == 0) mbar_arrive_expect(&W.mbar, (uint32_t)raw_bytes);
-                        __syncwarp();
-                        for (int i = lane; i < 2 * (rbh + tbh); i += 32) {
-                            const bool ref = i < 2 * rbh;
-                            const int j = ref ? i : i - 2 * rbh;
-                            const int bh = ref ? rbh : tbh;
-                            const bool magp = j >= bh;
-                            const int r = magp ? j - bh : j;
-                            const DevImage &im = ref ? ri : tI;
-                            const uint16_t *plane = magp ? im.mag : im.img;
-                            const int nb = ref ? rnb : tnb;
-                            const uint16_t *src =
-                                plane + (int64_t)((ref ? ry0 : ty0) + r) * im.w + (ref ? rxa : txa);
-                            unsigned char *dst = (ref ? (magp ? rM : rI) : (magp ? tMr : tIr)) + r * nb;
-                            bulk_g2s(dst, src, (uint32_t)nb, &W.mbar);
+                    const int tw0 = P.tma_w[0], th0 = P.tma_h[0];
+                    const int tw1 = P.tma_w[1], th1 = P.tma_h[1];
+                    const int rtile = (tw0 * th0 * 2 + 127) & ~127;   // bytes per plane tile
+                    const int ttile = (tw1 * th1 * 2 + 127) & ~127;
+                    const bool tma = tw0 > 0 && rx1 + 2 - rxa <= tw0 && rbh <= th0 &&
+                                     tx1 + 2 - txa <= tw1 && tbh <= th1 &&
+                                     2 * (rtile + ttile) <= warp_raw;
+                    if (rbw * rbh + tbw * tbh <= warp_quads && tma) {
+                        // ---- four tile copies (TMA), then conversion ----
+                        unsigned char *rI = raw, *rM = raw + rtile;
+                        unsigned char *tIr = raw + 2 * rtile, *tMr = tIr + ttile;
+                        if (lane == 0) {
+                            const void *m0 = P.tmap[0][0], *m1 = P.tmap[0][1];
+                            const void *m2 = P.tmap[1][0], *m3 = P.tmap[1][1];
+                            tmap_acquire(m0);
+                            tmap_acquire(m1);
+                            tmap_acquire(m2);
+                            tmap_acquire(m3);
+                            mbar_arrive_expect(&W.mbar, (uint32_t)(2 * (tw0 * th0 + tw1 * th1) * 2));
+                            tma_tile_2d(rI, m0, rxa, ry0, &W.mbar);
+                            tma_tile_2d(rM, m1, rxa, ry0, &W.mbar);
+                            tma_tile_2d(tIr, m2, txa, ty0, &W.mbar);
+                            tma_tile_2d(tMr, m3, txa, ty0, &W.mbar);
                         }
                         if (!mbar_wait(&W.mbar, phase, 2000000000ll)) {
                             // the copies did not complete within ~1 s: report, wait
@@ -691,6 +705,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                             return;
                         }
                         phase ^= 1u;
+                        const int rnb = 2 * tw0, tnb = 2 * tw1;   // tile row bytes
                         // box shifts: the centre texels
                         const int rc = (rbh / 2) * rnb + 2 * (rx0 + rw / 2 - rxa);
                         const int tc = (tbh / 2) * tnb + 2 * (tx0 + tw / 2 - txa);
@@ -702,7 +717,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                                                        sI, sM, lane);
                         const bool z2 = stage_from_raw(boxes + rbw * rbh, tbw, tIr, tMr, tnb, txa,
                                                        tx0, tw, tbh, tsI, tsM, lane);
-                        // the raw rows are rewritten by the next copies
+                        // the tiles are rewritten by the next copies
                         fence_async_shared();
                         __syncwarp();
                         staged = !(z1 || z2);
@@ -772,15 +787,89 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     evals++;
                 }
 
+                // ---- FindPeakNcc streamed over this group of 32 slots ----
+                // (setsm_code.cpp:6672-6752 on the FP32 values; every decision
+                // within the error band, and every value the FP32 pass could not
+                // take -- deferred windows, unsure variances, voxel truncations
+                // near an integer, NaN --, sends the node to the exact pass)
                 const bool ev = k < K && status == 2;
-                const bool nd = ev && (isnan(incc_v) || (voxels && near_trunc((double)incc_v)));
-                if (k < K) W.vals[k] = rho_v;
+                const bool unusable = ev && (isnan(incc_v) || isnan(rho_v) ||
+                                             (voxels && near_trunc((double)incc_v)));
+                if (k < K) W.vals[k] = unusable ? __int_as_float(0x7fc00000) : rho_v;
+                bool band = unusable;
                 const uint32_t em = __ballot_sync(0xffffffffu, ev);
-                const uint32_t nm = __ballot_sync(0xffffffffu, nd);
-                if (lane == 0) {
-                    W.m.evaluated[k0 >> 5] = em;
-                    W.m.need[k0 >> 5] = nm;
+                if (em) {
+                    const int p_in = prev_eval(em, lane, -1);
+                    const float pv_in = __shfl_sync(0xffffffffu, rho_v, p_in < 0 ? 0 : p_in);
+                    const bool has_p = p_in >= 0 || W.have;
+                    const float pv = p_in >= 0 ? pv_in : W.pre_v;
+                    // direction of this slot: the sign of the change (the
+                    // reference's sign rule reduces to it); -1 on the first one
+                    const int td = has_p ? (rho_v > pv) - (rho_v < pv) : -1;
+                    const int td_in = __shfl_sync(0xffffffffu, td, p_in < 0 ? 0 : p_in);
+                    const int dp = p_in >= 0 ? td_in : W.pre_dir;
+                    bool is_peak = false;
+                    if (ev && !unusable) {
+                        const float fv = rho_v;
+                        if (fv > vmax) vmax = fv;
+                        if (near_round((double)fv) && fv > amb) amb = fv;
+                        if (P.cmr && has_p) {
+                            if (fabsf(fv - pv) < kBand || fabsf(fv) < kBand || fabsf(pv) < kBand)
+                                band = true;
+                            is_peak = pv != -1.0f && dp > 0 && td < 0;
+                        }
+                    }
+                    if (is_peak) {
+                        if (near_round((double)pv) && pv > amb_peak) amb_peak = pv;
+                        if (pv > b1) {
+                            b2 = b1;
+                            b1 = pv;
+                        } else if (pv > b2) {
+                            b2 = pv;
+                        }
+                    }
+                    // the ordered top-two fold of this group's peaks (lane 0)
+                    uint32_t pm = __ballot_sync(0xffffffffu, is_peak);
+                    const int p_slot = p_in >= 0 ? k0 + p_in : W.pre_k;
+                    while (pm) {
+                        const int b = __ffs(pm) - 1;
+                        pm &= pm - 1;
+                        const float val = __shfl_sync(0xffffffffu, pv, b);
+                        const int ps = __shfl_sync(0xffffffffu, p_slot, b);
+                        if (lane == 0) {
+                            vll_nccresult &R = W.R;
+                            const float ph = slot_height(P, start_H, ncc_min, ps);
+                            if (R.result4 < 10) R.result4 += 1;
+                            const int16_t qpre = q_result((double)val);
+                            if (R.result0 < qpre) {
+                                const double t1 = dq_result(R.result0);
+                                R.result0 = qpre;
+                                const float t2 = R.result2;
+                                R.result2 = ph;
+                                const int16_t q1 = q_result(t1);
+                                if (R.result1 < q1) {
+                                    R.result1 = q1;
+                                    R.result3 = t2;
+                                }
+                            } else if (R.result1 < qpre) {
+                                R.result1 = qpre;
+                                R.result3 = ph;
+                            }
+                        }
+                    }
+                    // carry the last evaluated slot into the next group
+                    const int last = 31 - __clz(em);
+                    const float lv = __shfl_sync(0xffffffffu, rho_v, last);
+                    const int ld = __shfl_sync(0xffffffffu, td, last);
+                    __syncwarp();
+                    if (lane == 0) {
+                        W.pre_v = lv;
+                        W.pre_dir = ld;
+                        W.pre_k = k0 + last;
+                        W.have = true;
+                    }
                 }
+                if (__any_sync(0xffffffffu, band)) need = true;
                 if (P.dbg_rho && status == 2)
                     P.dbg_rho[P.dbg_off[pt] + k] = deferred ? __longlong_as_double(0x7ff8000000000000ll)
                                                             : (double)rho_v;
@@ -794,19 +883,30 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 }
                 __syncwarp();
             }
-            // FindPeakNcc and max_WNCC on the FP32 values
-            auto fval = [&](int kk, bool &ex) {
-                ex = false;
-                return (double)W.vals[kk];
-            };
-            const double max_w = scan_pass(P, chc, K, W.m, fval, lane);
-            int n_need = 0;
-            for (int i = 0; i < (K + 31) / 32; ++i) n_need += __popc(W.m.need[i]);
-            if (n_need == 0) {
+            // the maximum, and roundings that could change the maximum or the
+            // top two (a peak more than 0.002 + 2 bands below the second best
+            // rounds strictly below it)
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+                amb = fmaxf(amb, __shfl_xor_sync(0xffffffffu, amb, o));
+                amb_peak = fmaxf(amb_peak, __shfl_xor_sync(0xffffffffu, amb_peak, o));
+                const float o1 = __shfl_xor_sync(0xffffffffu, b1, o);
+                const float o2 = __shfl_xor_sync(0xffffffffu, b2, o);
+                const float n1 = fmaxf(b1, o1);
+                const float n2 = fmaxf(fminf(b1, o1), fmaxf(b2, o2));
+                b1 = n1;
+                b2 = n2;
+            }
+            if (chc && (double)amb >= (double)vmax - (double)kBand) need = true;
+            if (P.cmr && amb_peak > -1e29f) {
+                const double thr = (double)(b2 > -1e29f ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
+                if ((double)amb_peak >= thr) need = true;
+            }
+            if (!need) {
                 if (lane == 0) {
-                    vll_nccresult R = P.ncc[pt];
-                    if (P.cmr) fold_peaks(P, R, K, start_H, W.m.peak, fval);
-                    if (R.check_height_change) R.max_WNCC = q_result(max_w);
+                    vll_nccresult R = W.R;
+                    if (R.check_height_change) R.max_WNCC = q_result((double)vmax);
                     P.ncc[pt] = R;
                 }
             } else {
@@ -820,9 +920,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 }
                 off = __shfl_sync(0xffffffffu, off, 0);
                 if (off >= 0)
-                    for (int kk = lane; kk < K; kk += 32)
-                        pend_vals[off + kk] = bit(W.m.need, kk) ? __int_as_float(0x7fc00000)
-                                                                : W.vals[kk];
+                    for (int kk = lane; kk < K; kk += 32) pend_vals[off + kk] = W.vals[kk];
             }
             __syncwarp();
         }
@@ -838,23 +936,17 @@ constexpr int kPeakWarps = 4;
 
 struct WarpShared {
     float rho[kSlotCap];
+    double xrho[kSlotCap];           // exact value of each re-checked slot
+    int todo[kSlotCap];              // this round's slots to re-check
     SlotMasks m;
     uint32_t exact[kSlotCap / 32];
-    int exact_k[kExactCap];
-    double exact_rho[kExactCap];
-    double exact_incc[kExactCap];
     double chunk[32];
-    int n_exact;
 };
 
 // value of slot k for the scan: exact if re-checked, else the FP32 one
 __device__ __forceinline__ double slot_value(const WarpShared &w, int k, bool &ex) {
     ex = bit(w.exact, k);
-    if (ex) {
-        for (int i = 0; i < w.n_exact; ++i)
-            if (w.exact_k[i] == k) return w.exact_rho[i];
-    }
-    return (double)w.rho[k];
+    return ex ? w.xrho[k] : (double)w.rho[k];
 }
 
 // Exact FP64 evaluation of one slot by the whole warp, bit-identical with
@@ -1002,9 +1094,9 @@ __device__ __forceinline__ SlotOut eval_slot_warp_any(const DevLevel &P, int64_t
 
 // The exact pass for the nodes the window kernel could not settle in FP32:
 // the decisions within the error band are re-taken on exact FP64 values of
-// the slots involved (rounds of scan and re-evaluation); a node with more
-// slots to re-evaluate than kExactCap, or still unsettled after kMaxRounds,
-// or queued without its FP32 values, is evaluated wholly in FP64.
+// the slots involved (rounds of scan and re-evaluation: a few slots a warp
+// each, more a lane each); a node still unsettled after kMaxRounds, or
+// queued without its FP32 values, is evaluated wholly in FP64.
 // `max_h`: the largest window half-size of the level set (scratch layout).
 __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
     const LevelSet LS, int max_h, const int32_t *__restrict__ node_k,
@@ -1055,7 +1147,6 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
             W.m.peak[lane] = 0;
             W.exact[lane] = 0;
         }
-        if (lane == 0) W.n_exact = 0;
         __syncwarp();
         for (int k0 = 0; k0 < K; k0 += 32) {
             const int k = k0 + lane;
@@ -1082,7 +1173,7 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
             int n_need = 0;
             for (int i = 0; i < (K + 31) / 32; ++i) n_need += __popc(W.m.need[i] & ~W.exact[i]);
             if (n_need == 0) break;
-            const bool overflow = W.n_exact + n_need > kExactCap || round + 1 >= kMaxRounds;
+            const bool overflow = round + 1 >= kMaxRounds;
             if (lane == 0) atomicAdd(&counters[6], 1ull);
             if (overflow) {
                 if (lane == 0) atomicAdd(&counters[5], 1ull);
@@ -1092,39 +1183,54 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
                 redone = true;   // results already written
                 break;
             }
-            // compact the list and evaluate it lane-parallel in FP64
-            int base = W.n_exact;
+            // compact the list of slots to re-check
+            int n_todo = 0;
             for (int i = 0; i < (K + 31) / 32; ++i) {
                 const uint32_t todo = W.m.need[i] & ~W.exact[i];
-                const int k = (i << 5) + lane;
-                const bool mine = (todo >> lane) & 1u;
-                const int o = __popc(todo & ((1u << lane) - 1u));
-                if (mine) W.exact_k[base + o] = k;
-                base += __popc(todo);
+                if ((todo >> lane) & 1u) W.todo[n_todo + __popc(todo & ((1u << lane) - 1u))] = (i << 5) + lane;
+                n_todo += __popc(todo);
             }
             __syncwarp();
-            // exact values, one slot at a time, the whole warp per slot
-            for (int j = W.n_exact; j < base; ++j) {
-                const int k = W.exact_k[j];
-                const float hh = slot_height(P, start_H, R.minHeight, k);
-                const SlotOut o = eval_slot_warp_any(P, pt, S, hh, cnt_g, sum_g,
-                                                    reinterpret_cast<double *>(boxes), lane);
-                if (lane == 0) {
+            if (n_todo <= kWarpPerSlotMax) {
+                // a few slots: the whole warp per slot
+                for (int j = 0; j < n_todo; ++j) {
+                    const int k = W.todo[j];
+                    const float hh = slot_height(P, start_H, R.minHeight, k);
+                    const SlotOut o = eval_slot_warp_any(P, pt, S, hh, cnt_g, sum_g,
+                                                        reinterpret_cast<double *>(boxes), lane);
+                    if (lane == 0) {
+                        if (P.dbg_rho && o.evaluated && isnan(P.dbg_rho[P.dbg_off[pt] + k]))
+                            P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
+                        W.xrho[k] = o.rho;
+                        if (vrow) {
+                            if (o.all_pos) vrow[k].flag_cal = 1;
+                            vrow[k].INCC = q_voxel(o.count_incc > 0
+                                                       ? __ddiv_rn(o.sum_incc, o.count_incc)
+                                                       : -1.0);
+                        }
+                        rechecks++;
+                    }
+                    __syncwarp();
+                }
+            } else {
+                // many (windows the FP32 pass could not stage): a lane per slot
+                for (int j = lane; j < n_todo; j += 32) {
+                    const int k = W.todo[j];
+                    const float hh = slot_height(P, start_H, R.minHeight, k);
+                    const SlotOut o = eval_slot(P, pt, 1, S, Sn, hh, cnt_g, sum_g);
                     if (P.dbg_rho && o.evaluated && isnan(P.dbg_rho[P.dbg_off[pt] + k]))
                         P.dbg_rho[P.dbg_off[pt] + k] = o.rho;
-                    W.exact_rho[j] = o.rho;
-                    W.exact_incc[j] = o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc) : -1.0;
+                    W.xrho[k] = o.rho;
                     if (vrow) {
                         if (o.all_pos) vrow[k].flag_cal = 1;
-                        vrow[k].INCC = q_voxel(W.exact_incc[j]);
+                        vrow[k].INCC = q_voxel(o.count_incc > 0 ? __ddiv_rn(o.sum_incc, o.count_incc)
+                                                                : -1.0);
                     }
                     rechecks++;
                 }
-                __syncwarp();
             }
             __syncwarp();
-            for (int j = W.n_exact + lane; j < base; j += 32) set_bit(W.exact, W.exact_k[j]);
-            if (lane == 0) W.n_exact = base;
+            for (int j = lane; j < n_todo; j += 32) set_bit(W.exact, W.todo[j]);
             if (lane < kSlotCap / 32) W.m.peak[lane] = 0;
             __syncwarp();
         }
@@ -1182,23 +1288,22 @@ void host_rpc(const double *rpc, double lon, double lat, double h, double &x, do
     x = c[2] / c[3] * rpc[6] + rpc[1];
 }
 
-// Shared-memory budget per warp: the boxes covering 32 consecutive height
-// slots of one node in both images -- the reference window and the target
-// window (rotated; its samples lie within H + 1 of the centre) swept along
-// their epipolar lines -- as texel pairs, and the raw rows the bulk copies
-// bring (8 texels of alignment slack per row).  The sweep per slot, along x
-// and y, is measured from the RPCs over the image footprint; the budget is
-// the worst case times `margin` (a larger footprint falls back to FP64).
-struct WarpBudget {
-    int quads;   // float4 texel pairs
-    int raw;     // bytes of raw rows (multiple of 16)
+// The boxes covering 32 consecutive height slots of one node in both images
+// -- the reference window and the target window (rotated; its samples lie
+// within H + 1 of the centre) swept along their epipolar lines -- in texel
+// pairs (w x h), per image [0] reference, [1] target.  The sweep per slot,
+// along x and y, is measured from the RPCs over the image footprint; the
+// boxes are the worst case times `margin` (an item with a larger footprint
+// falls back to slower staging or to FP64).
+struct WindowBoxes {
+    int w[2], h[2];
 };
 
-WarpBudget window_warp_budget(const DevLevel &P, float margin) {
+WindowBoxes window_boxes(const DevLevel &P, float margin) {
     const int H = P.H;
     double rx[2] = {0, 0}, ry[2] = {0, 0};
     for (int ti = 0; ti < 2; ++ti) {
-        const double *r = P.im[ti].rpc;
+        const double *r = P.im[ti == 0 ? P.ref : 1].rpc;
         for (int a = -1; a <= 1; ++a)
             for (int b = -1; b <= 1; ++b) {
                 const double lon = r[2] + 0.8 * a * r[7], lat = r[3] + 0.8 * b * r[8];
@@ -1211,29 +1316,41 @@ WarpBudget window_warp_budget(const DevLevel &P, float margin) {
     }
     const double m = margin > 0 ? margin : 1.1;
     const int side[2] = {2 * H + 3, 2 * (H + 2) + 3};   // pairs of one slot's box (+1 slack)
-    double quads = 0, raw = 0;
+    WindowBoxes B;
     for (int ti = 0; ti < 2; ++ti) {
-        const double w = side[ti] + 31.0 * P.height_step * rx[ti] + 2.0;
-        const double h = side[ti] + 31.0 * P.height_step * ry[ti] + 2.0;
-        quads += (w + 1.0) * h;                              // odd row stride
-        raw += 2.0 * h * (std::ceil((w + 9.0) / 8.0) * 16.0);  // two planes
+        B.w[ti] = (int)std::ceil((side[ti] + 31.0 * P.height_step * rx[ti]) * m);
+        B.h[ti] = (int)std::ceil((side[ti] + 31.0 * P.height_step * ry[ti]) * m);
     }
+    return B;
+}
+
+// Shared-memory budget per warp: the boxes as texel pairs (odd row strides)
+// and, where the level has TMA tiles, the four tiles.
+struct WarpBudget {
+    int quads;   // float4 texel pairs
+    int raw;     // bytes of TMA tiles (multiple of 128)
+};
+
+WarpBudget window_warp_budget(const DevLevel &P, float margin) {
+    const WindowBoxes B = window_boxes(P, margin);
     WarpBudget wb;
-    wb.quads = (int)(quads * m) + 32;
-    wb.raw = (((int)(raw * m) + 256) + 15) & ~15;
-    // at most ~200 KB for the block
-    const size_t per_warp = (200 * 1024 - win_boxes_offset()) / kWinWarps;
-    if ((size_t)wb.quads * sizeof(float4) + wb.raw > per_warp) {
-        const double f = (double)per_warp / ((double)wb.quads * sizeof(float4) + wb.raw);
-        wb.quads = (int)(wb.quads * f);
-        wb.raw = ((int)(wb.raw * f)) & ~15;
-    }
+    wb.quads = (B.w[0] + 1) * B.h[0] + (B.w[1] + 1) * B.h[1] + 32;
+    wb.raw = 128;
+    if (P.tma_w[0] > 0)
+        wb.raw = 2 * (((P.tma_w[0] * P.tma_h[0] * 2 + 127) & ~127) +
+                      ((P.tma_w[1] * P.tma_h[1] * 2 + 127) & ~127));
+    // at most ~200 KB for the block: beyond, the tiles go (staging by loads)
+    // and then the boxes shrink
+    const size_t per_warp = (200 * 1024 - win_boxes_offset()) / kWinWarps - 128;
+    if ((size_t)wb.quads * sizeof(float4) + wb.raw > per_warp) wb.raw = 128;
+    if ((size_t)wb.quads * sizeof(float4) + wb.raw > per_warp)
+        wb.quads = (int)((per_warp - wb.raw) / sizeof(float4));
     return wb;
 }
 
 // Budget of a level set: the largest of its levels' budgets.
 WarpBudget set_warp_budget(const DevLevel *hl, int n, float margin) {
-    WarpBudget q{1, 16};
+    WarpBudget q{1, 128};
     for (int l = 0; l < n; ++l)
         if (hl[l].n_nodes > 0) {
             const WarpBudget b = window_warp_budget(hl[l], margin);
@@ -1256,7 +1373,7 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
                           unsigned long long *counters, unsigned long long *ctl,
                           const SplitTuning &tu, cudaStream_t s) {
     const WarpBudget wb = set_warp_budget(hl, n, tu.box_margin);
-    const size_t smem = win_boxes_offset() + (size_t)kWinWarps * (wb.quads * sizeof(float4) + wb.raw);
+    const size_t smem = win_raw_offset(wb.quads) + (size_t)kWinWarps * wb.raw;
     int dev = 0;
     cudaGetDevice(&dev);
     cudaError_t e = cudaFuncSetAttribute(window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1326,6 +1443,66 @@ int64_t pending_capacity(int64_t n_slots) {
 }
 
 }  // namespace
+
+namespace {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+}  // namespace
+
+void split_prepare_tma(DevLevel &P, float margin) {
+    P.tma_w[0] = P.tma_w[1] = P.tma_h[0] = P.tma_h[1] = 0;
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc || !split_supported(P) || P.combined_incc) return;
+    const WindowBoxes B = window_boxes(P, margin);
+    int tw[2], th[2];
+    for (int ti = 0; ti < 2; ++ti) {
+        const DevImage &im = P.im[ti == 0 ? P.ref : 1];
+        // tiles need 16-byte aligned rows; the tile width covers the box's
+        // pairs, their right texels and the rounding of x down to 8
+        if (im.w % 8 || !im.img || !im.mag || (reinterpret_cast<uintptr_t>(im.img) & 15) ||
+            (reinterpret_cast<uintptr_t>(im.mag) & 15))
+            return;
+        tw[ti] = (B.w[ti] + 1 + 7 + 7) & ~7;
+        th[ti] = B.h[ti];
+        if (tw[ti] > 256 || th[ti] > 256) return;
+        for (int pl = 0; pl < 2; ++pl) {
+            const cuuint64_t dims[2] = {im.w, im.h};
+            const cuuint64_t strides[1] = {(cuuint64_t)im.w * 2};
+            const cuuint32_t box[2] = {(cuuint32_t)tw[ti], (cuuint32_t)th[ti]};
+            const cuuint32_t estr[2] = {1, 1};
+            void *base = const_cast<uint16_t *>(pl == 0 ? im.img : im.mag);
+            if (enc(reinterpret_cast<CUtensorMap *>(P.tmap[ti][pl]), CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
+                    base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return;
+        }
+    }
+    for (int ti = 0; ti < 2; ++ti) {
+        P.tma_w[ti] = tw[ti];
+        P.tma_h[ti] = th[ti];
+    }
+}
 
 bool split_supported(const DevLevel &P) {
     return P.num_images == 2 && P.ref == 0 && P.im[1].selected && !P.is_ra && P.H >= 2 &&
@@ -1710,6 +1887,7 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     do {                                                                  \
         if ((call) != cudaSuccess) return fail(VLL_ERR_CUDA, #call);      \
     } while (0)
+    split_prepare_tma(P, SplitTuning().box_margin);
     NA_CUDA(cudaMemcpyAsync(dP, &P, sizeof(DevLevel), cudaMemcpyHostToDevice, s));
     // the array keeps the previous call's contents: clear what must start at zero
     NA_CUDA(cudaMemsetAsync(ctl, 0, 8 * sizeof(unsigned long long), s));

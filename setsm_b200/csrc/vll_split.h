@@ -53,6 +53,12 @@ void split_release(SplitBuffers &b);
 // the plain FP64 kernel.
 bool split_supported(const DevLevel &P);
 
+// Encodes the level's TMA tiles (tensor maps of the reference and target
+// planes, tile sized from the footprint sweep times `margin`) into P, or
+// leaves them off (P.tma_w[0] = 0) where they do not apply.  Call on the host
+// copy with its device image pointers, before it is copied to the device.
+void split_prepare_tma(DevLevel &P, float margin);
+
 // Runs the split pipeline for a level whose DevLevel block is at dP (device)
 // and mirrored in P (host).  counters: [0] accessable, [1] evals,
 // [2] FP64 re-checks, [3] error flag.

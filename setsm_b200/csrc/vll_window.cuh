@@ -353,21 +353,19 @@ __device__ __forceinline__ void fence_async_shared() {
 }
 
 // Texel pairs of box [x0, x0+bw) x rows [0, bh) from raw rows staged in
-// shared memory: rawI / rawM hold, per box row, the uint16 texels
-// [xa, xa + 8 * nb / 16) (xa = x0 rounded down to 8, rows of nb bytes).
-// Each lane converts 8-texel chunks read with 128-bit loads, as
-// stage_box_vec does from global memory; returns (warp-uniform) whether an
-// intensity texel of the chunks is zero.
+// shared memory: rawI / rawM hold, per box row (stride `nb` bytes), the
+// uint16 texels from xa = x0 rounded down to 8 on.  Each lane converts
+// 8-texel chunks read with 128-bit loads; returns (warp-uniform) whether an
+// intensity texel of the box's pairs ([x0, x0 + bw]) is zero.
 __device__ __forceinline__ bool stage_from_raw(float4 *__restrict__ dst, int ds,
                                                const unsigned char *__restrict__ rawI,
                                                const unsigned char *__restrict__ rawM, int nb,
                                                int xa, int x0, int bw, int bh, float sI, float sM,
                                                int lane) {
-    uint32_t zacc = 0;
-    bool z8 = false;
+    bool zero = false;
     const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
-    const int x1 = x0 + bw - 1;   // last pair's left texel
-    const int nch = nb / 16;
+    const int x1 = x0 + bw - 1;                 // last pair's left texel
+    const int nch = (x1 + 1 - xa) / 8 + 1;      // chunks covering [xa, x1 + 1]
     const int n = nch * bh;
     for (int i = lane; i < n; i += 32) {
         const int by = i / nch;
@@ -376,11 +374,17 @@ __device__ __forceinline__ bool stage_from_raw(float4 *__restrict__ dst, int ds,
         const int ro = by * nb + 16 * c;
         const uint4 vi = *reinterpret_cast<const uint4 *>(rawI + ro);
         const uint4 vm = *reinterpret_cast<const uint4 *>(rawM + ro);
-        const bool need9 = xc + 7 <= x1;   // the 8th pair needs texel xc + 8
+        const bool need9 = xc + 7 <= x1;        // the 8th pair needs texel xc + 8
         const uint32_t i8 = need9 ? *reinterpret_cast<const uint16_t *>(rawI + ro + 16) : 1u;
         const uint32_t m8 = need9 ? *reinterpret_cast<const uint16_t *>(rawM + ro + 16) : 0u;
-        zacc |= zero_half(vi.x) | zero_half(vi.y) | zero_half(vi.z) | zero_half(vi.w);
-        z8 |= i8 == 0;
+        const uint32_t w[4] = {vi.x, vi.y, vi.z, vi.w};
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int x = xc + t;
+            const uint32_t tex = (w[t >> 1] >> (16 * (t & 1))) & 0xFFFFu;
+            if (x >= x0 && x <= x1 + 1 && tex == 0) zero = true;
+        }
+        zero |= i8 == 0;
         float2 f[9];
         f[0] = texel_pair(vi.x, vm.x, 0x7610, ns);
         f[1] = texel_pair(vi.x, vm.x, 0x7632, ns);
@@ -398,7 +402,25 @@ __device__ __forceinline__ bool stage_from_raw(float4 *__restrict__ dst, int ds,
             if (x >= x0 && x <= x1) drow[x - x0] = make_float4(f[t].x, f[t].y, f[t + 1].x, f[t + 1].y);
         }
     }
-    return __any_sync(0xffffffffu, (zacc & 0x80008000u) != 0 || z8);
+    return __any_sync(0xffffffffu, zero);
+}
+
+// 2-D tile of a tensor map (TMA, no multicast) into this CTA's shared memory
+// at `dst` (128-byte aligned): x (innermost, a multiple of 16 bytes) and y
+// are the tile's first texel; completes `bytes` of the tile on `bar`.
+__device__ __forceinline__ void tma_tile_2d(void *dst, const void *tmap, int x, int y,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];" ::"r"(smem_addr(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Makes a tensor map written to global memory by the host visible to the
+// TMA unit before its first use by this thread.
+__device__ __forceinline__ void tmap_acquire(const void *tmap) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
 }
 
 // Scalar staging of a box whose destination rows have stride `ds` pairs
