@@ -448,8 +448,9 @@ def run_ours(args):
     gpu_ncc = {}
     for t in templates:
         wl.d_ncc.zero_()
+        torch.cuda.synchronize(dev)   # the library runs on its own stream
         ctx.vertical_line_locus_device(descs[t], wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr(),
-                                       None, None, args.kernel, stats=False)
+                                       None, None, args.kernel, stats=True)
         gpu_ncc[t] = workloads.ncc_host(wl)
     barrier(world)
 
@@ -530,11 +531,12 @@ def run_ours(args):
         mism, n_valid, n_same, n_ties = {}, 0, 0, 0
         for t in templates:
             wl.d_ncc.zero_()
+            torch.cuda.synchronize(dev)
             e2 = torch.cuda.Event(enable_timing=True)
             e3 = torch.cuda.Event(enable_timing=True)
             e2.record(stream)
             st = ctx.vertical_line_locus_device(descs[t], wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr(),
-                                                None, None, "plain")
+                                                None, None, "plain", stats=True)
             e3.record(stream)
             torch.cuda.synchronize(dev)
             plain_ms += e2.elapsed_time(e3)

@@ -449,8 +449,11 @@ void ref_call_voxel_iterations(void *fn_init, void *fn_vll, void *fn_awncc, cons
            reinterpret_cast<NCCresult *>(ncc), d->height_step, (uint8)d->pyramid_step,
            (uint8)iters[k], max_voxel);
     }
+    // InitializeVoxel frees a row without clearing its pointer when the row
+    // drops to zero heights; the rows still owned are the NumOfHeight > 0 ones
+    // (the release at setsm_code.cpp:4576-4585)
     for (long i = 0; i < n; ++i)
-        if (rows[i]) free(rows[i]);
+        if (ncc[i].NumOfHeight > 0 && rows[i]) free(rows[i]);
     free(rows);
 }
 

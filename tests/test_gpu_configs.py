@@ -26,7 +26,9 @@ pytestmark = [pytest.mark.gpu,
 
 def _ncc_of(wl, ctx, template, kernel):
     from setsm_b200 import workloads
+    import torch
     wl.d_ncc.zero_()
+    torch.cuda.synchronize()   # the library runs on its own stream
     st = ctx.vertical_line_locus_device(wl.device_desc(template), wl.d_gp3.data_ptr(),
                                         wl.d_ncc.data_ptr(), None, None, kernel, stats=True)
     return workloads.ncc_host(wl), st
