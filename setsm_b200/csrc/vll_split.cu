@@ -474,19 +474,49 @@ __device__ void node_exact_chunked(const DevLevel &P, int64_t pt, int K, const P
 #define VLL_WIN_MINB 3
 #endif
 constexpr int kWinWarps = VLL_WIN_WARPS;
+constexpr int kWinMaxBlocksPerSm = 2048 / (kWinWarps * 32);
+constexpr int kZeroCap = 32;          // zero intensity texels listed per staged group
 
-// Per-warp shared state of the window kernel: the node's RPC cubics, the
-// FP32 values and masks of its slots, and the exact pass's chunk.
+// Node flags of the window kernel
+constexpr uint32_t kNfCmr = 1u;       // memory-tight route (FindPeakNcc on the values)
+constexpr uint32_t kNfOri = 2u;       // orientation-difference test (level >= 3)
+constexpr uint32_t kNfVox = 4u;       // voxel rows written
+constexpr uint32_t kNfChc = 8u;       // check_height_change (max_WNCC written)
+constexpr uint32_t kNfGncc = 16u;     // rho blends the INCC with the node's GNCC
+constexpr uint32_t kNfVec = 32u;      // image rows 16-byte aligned (vector staging)
+constexpr uint32_t kNfTma = 64u;      // the level has tensor maps for its footprints
+constexpr uint32_t kNfDbg = 128u;     // per-slot debug values written
+
+// Per-node state of the window kernel in shared memory: the RPC cubics, the
+// level constants the slot loop reads (here rather than from the level block
+// in global memory), the record folded by lane 0 and the streamed scan's
+// carry.  A warp holds two: the node of the group being evaluated and the
+// node of the group being fetched.
+struct NodeCtx {
+    double horner[2][4][4];           // [image][num/den poly][a0..a3]
+    double hnorm[2][2];               // [image] {h_off, 1 / h_scale}
+    double geo[2][8];                 // [image] adj0, adj1, rpc0, rpc1, rpc5, rpc6, sx, sy
+    double inv_s, hbase, hstep, bin_angle, alpha, gterm;
+    const uint16_t *img[2], *mag[2];
+    const uint8_t *ori[2];
+    const DevLevel *P;
+    vll_voxel *vrow;
+    int64_t gn, pt;
+    uint32_t w[2], h[2];
+    int tma_w[2], tma_h[2];
+    int K, H, start_H, end_H;
+    uint32_t flags;
+    vll_nccresult R;
+    float pre_v;                      // streamed scan: the last evaluated slot's value,
+    int pre_dir, pre_k, have;         // direction and index, and whether there is one
+};
+
+// Per-warp shared state of the window kernel.
 struct WinShared {
-    double horner[2][4][4];          // [image][num/den poly][a0..a3]
-    double hnorm[2][2];              // [image] {h_off, 1 / h_scale}
-    vll_nccresult R;                 // the node's record, folded by lane 0
-    float vals[kSlotCap];            // FP32 rho per slot (+inf skipped, -inf rejected,
-                                     // NaN: no usable FP32 value)
-    float pre_v;                     // the scan's last evaluated slot: value,
-    int pre_dir, pre_k;              // direction and index
-    bool have;
-    uint64_t mbar;                   // completion of the footprint's bulk copies
+    NodeCtx node[2];
+    uint32_t zl[kZeroCap];            // zero intensity texels of the staged boxes
+    int zn;                           // their count (more than kZeroCap: not listed)
+    uint64_t mbar;                    // completion of the group's tile copies
 };
 
 __host__ __device__ constexpr size_t win_boxes_offset() {
@@ -501,429 +531,627 @@ __host__ __device__ constexpr size_t win_raw_offset(int warp_quads) {
 // FP32 window statistics of one slot for the level's window half-size
 // (the window code is unrolled per half-size; a batch may mix them).
 __device__ __forceinline__ void window_any(int H, const float4 *qr, int rbw, float rfx, float rfy,
-                                           const float4 *qt, int tbw, float tfx, float tfy,
-                                           float c, float s, float &incc, bool &unsure) {
+                                           const TgtBox &tb, float tfx, float tfy, float c,
+                                           float s, float &incc, bool &unsure) {
     switch (H) {
-        case 2: window_fp32<2>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
-        case 3: window_fp32<3>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
-        case 4: window_fp32<4>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
-        case 5: window_fp32<5>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
-        case 6: window_fp32<6>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
-        default: window_fp32<7>(qr, rbw, rfx, rfy, qt, tbw, tfx, tfy, c, s, incc, unsure); break;
+        case 2: window_fp32<2>(qr, rbw, rfx, rfy, tb, tfx, tfy, c, s, incc, unsure); break;
+        case 3: window_fp32<3>(qr, rbw, rfx, rfy, tb, tfx, tfy, c, s, incc, unsure); break;
+        case 4: window_fp32<4>(qr, rbw, rfx, rfy, tb, tfx, tfy, c, s, incc, unsure); break;
+        case 5: window_fp32<5>(qr, rbw, rfx, rfy, tb, tfx, tfy, c, s, incc, unsure); break;
+        case 6: window_fp32<6>(qr, rbw, rfx, rfy, tb, tfx, tfy, c, s, incc, unsure); break;
+        default: window_fp32<7>(qr, rbw, rfx, rfy, tb, tfx, tfy, c, s, incc, unsure); break;
     }
 }
 
-// One persistent launch over the nodes of every level of the set (a warp per
-// node, nodes taken from a global queue in level order).  Per node: the RPC
-// cubics once; then for each group of 32 height slots (a lane per slot) the
-// FP64 geometry, the staged footprints and the FP32 window statistics; then
-// FindPeakNcc / max_WNCC on the FP32 values in the warp.  A node whose every
-// decision lies outside the error band is written here; any other node is
-// queued for the exact pass with its FP32 values (NaN marking the slots that
-// need an exact value) in the pending buffer, or with offset -1 (evaluated
-// wholly in FP64 there) when the buffer is full.  Nodes of combined-level
-// INCC, or with more slots than kSlotCap, are evaluated here wholly in FP64.
+// Fills the warp's node context for global node gn (level lvl, K slots);
+// every lane takes part, the context is complete after the final __syncwarp.
+__device__ __noinline__ void node_setup(NodeCtx &N, const LevelSet &LS, int lvl, int64_t gn, int K,
+                                        const double *__restrict__ gsum,
+                                        const double *__restrict__ gcnt, int lane) {
+    const DevLevel &P = LS.lv[lvl];
+    const int64_t pt = gn - __ldg(LS.base + lvl);
+    if (lane < 8) {
+        // per-node RPC cubics: lanes 0..7 = (image, polynomial)
+        const int im = lane >> 2, j = lane & 3;
+        const double *rpc = P.im[im == 0 ? P.ref : 1].rpc;
+        node_horner_poly(rpc, P.grid_wgs[2 * pt], P.grid_wgs[2 * pt + 1], j, N.horner[im][j]);
+        if (j == 0) {
+            N.hnorm[im][0] = rpc[4];
+            N.hnorm[im][1] = 1.0 / rpc[9];
+        }
+    } else if (lane < 10) {
+        const int im = lane - 8;
+        const DevImage &I = P.im[im == 0 ? P.ref : 1];
+        double *g = N.geo[im];
+        g[0] = I.adj[0];
+        g[1] = I.adj[1];
+        g[2] = I.rpc[0];
+        g[3] = I.rpc[1];
+        g[4] = I.rpc[5];
+        g[5] = I.rpc[6];
+        g[6] = I.sx;
+        g[7] = I.sy;
+        N.img[im] = I.img;
+        N.mag[im] = I.mag;
+        N.ori[im] = I.ori;
+        N.w[im] = I.w;
+        N.h[im] = I.h;
+        N.tma_w[im] = P.tma_w[im];
+        N.tma_h[im] = P.tma_h[im];
+    } else if (lane == 10) {
+        const vll_ugrid g = P.gp3[pt];
+        const vll_nccresult R = P.ncc[pt];
+        const DevImage &ri = P.im[P.ref], &tI = P.im[1];
+        N.P = &P;
+        N.gn = gn;
+        N.pt = pt;
+        N.K = K;
+        N.H = P.H;
+        N.start_H = g.minHeight;
+        N.end_H = g.maxHeight;
+        N.R = R;
+        N.hbase = (double)((P.is_ra || P.cmr) ? g.minHeight : R.minHeight);
+        N.hstep = P.height_step;
+        N.inv_s = 1.0 / (double)(1 << P.L);
+        N.bin_angle = P.bin_angle;
+        N.alpha = P.alpha;
+        const double cnt_g = gcnt ? gcnt[gn] : 0.0;
+        const bool gncc = P.check_ortho && cnt_g > 0;
+        N.gterm = gncc ? (gsum[gn] / cnt_g) * P.beta : 0.0;
+        const bool voxels = P.vox && !P.cmr && !P.is_ra;
+        N.vrow = voxels ? P.vox + P.vox_off[pt] : nullptr;
+        const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
+                            ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
+                              reinterpret_cast<uintptr_t>(tI.img) |
+                              reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
+        N.flags = (P.cmr ? kNfCmr : 0u) | ((!P.is_ra && P.L >= 3) ? kNfOri : 0u) |
+                  (voxels ? kNfVox : 0u) | (R.check_height_change ? kNfChc : 0u) |
+                  (gncc ? kNfGncc : 0u) | (vec_ok ? kNfVec : 0u) | (P.tma_w[0] > 0 ? kNfTma : 0u) |
+                  (P.dbg_rho ? kNfDbg : 0u);
+        N.pre_v = -1.0f;
+        N.pre_dir = 0;
+        N.pre_k = -1;
+        N.have = 0;
+    } else if (lane == 11 && P.tma_w[0] > 0) {
+        // tensor maps written by the host: visible to this lane's copies
+        tmap_acquire(P.tmap[0][0]);
+        tmap_acquire(P.tmap[0][1]);
+        tmap_acquire(P.tmap[1][0]);
+        tmap_acquire(P.tmap[1][1]);
+    }
+    __syncwarp();
+}
+
+// Image coordinate (pyramid level) of one slot of node N in image im from
+// the node's cubics (fast_coord's arithmetic on the node context).
+__device__ __forceinline__ double2 node_coord(const NodeCtx &N, int im, double hgt, bool &edge) {
+    const double H = (hgt - N.hnorm[im][0]) * N.hnorm[im][1];
+    double v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double *a = N.horner[im][j];
+        v[j] = fma(fma(fma(a[3], H, a[2]), H, a[1]), H, a[0]);
+    }
+    const double *g = N.geo[im];
+    double y = g[0] + ((v[0] * fast_rcp(v[1], edge)) * g[4] + g[2]);
+    double x = g[1] + ((v[2] * fast_rcp(v[3], edge)) * g[5] + g[3]);
+    const double ymax = g[2] + g[4] * 1.2, xmax = g[3] + g[5] * 1.2;
+    if (fabs(y) < kEdge || fabs(y - ymax) < kEdge || fabs(x) < kEdge || fabs(x - xmax) < kEdge)
+        edge = true;
+    y = y < 0 ? 0 : (y > ymax ? ymax : y);
+    x = x < 0 ? 0 : (x > xmax ? xmax : x);
+    const double px = x * N.inv_s - g[6], py = y * N.inv_s - g[7];   // inv_s = 2^-L (exact)
+    const double fx = px - floor(px), fy = py - floor(py);
+    if (fx < kEdge || fx > 1.0 - kEdge || fy < kEdge || fy > 1.0 - kEdge) edge = true;
+    return make_double2(px, py);
+}
+
+// Both images' coordinates of a slot by the reference's own RPC order (the
+// slots whose fast coordinates lie too close to an integer or a clamp).
+__device__ __noinline__ void slot_coords_exact(const NodeCtx &N, double hgt, double2 &rp,
+                                               double2 &tp) {
+    const DevLevel &P = *N.P;
+    const double lon = P.grid_wgs[2 * N.pt], lat = P.grid_wgs[2 * N.pt + 1];
+#pragma unroll 1
+    for (int im = 0; im < 2; ++im) {
+        const DevImage &I = P.im[im == 0 ? P.ref : 1];
+        const double2 q = to_pyramid(rpc_project(I.rpc, I.adj, lon, lat, hgt), I.sx, I.sy, P.L);
+        if (im == 0)
+            rp = q;
+        else
+            tp = q;
+    }
+}
+
+// One persistent launch over the nodes of every level of the set, a warp per
+// node, nodes taken from a global queue in level order; each node's slots in
+// groups of 32 (a lane per slot).  The groups form one stream per warp that
+// is software-pipelined: while the window statistics of a group are
+// computed, the footprints of the next group (of this node or the next one)
+// are already being copied into shared memory by the TMA engine.  Per group:
+//   fetch     FP64 geometry of the 32 slots (RPC cubics of the node, the
+//             reference's RPC order near integers and clamps), orientation,
+//             the boxes covering the footprints, four tile copies;
+//   stage     (a group later) conversion of the tiles to FP32 box texels,
+//             listing zero intensity texels;
+//   evaluate  FP32 window statistics of every slot whose footprint holds no
+//             zero texel, then FindPeakNcc / max_WNCC streamed over the group.
+// A node whose every decision lies outside the error band is written here;
+// any other node is queued for the exact pass with its FP32 values (NaN
+// marking the slots that need an exact value) in the pending buffer, or with
+// offset -1 (evaluated wholly in FP64 there) when the buffer is full.  Nodes
+// of combined-level INCC, or with more slots than kSlotCap, are queued with
+// offset -2 (evaluated wholly in FP64 by the exact pass).
 __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     const LevelSet LS, const int32_t *__restrict__ node_k, const double *__restrict__ gsum,
     const double *__restrict__ gcnt, float *__restrict__ pend_vals, int64_t pend_cap,
     int64_t *__restrict__ pend_node, int64_t *__restrict__ pend_off,
-    unsigned long long *__restrict__ counters, unsigned long long *__restrict__ ctl,
-    int warp_quads, int warp_raw, int grab) {
+    float *__restrict__ warp_vals, unsigned long long *__restrict__ counters,
+    unsigned long long *__restrict__ ctl, int warp_quads, int warp_raw, int grab) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     WinShared &W = reinterpret_cast<WinShared *>(smem_raw)[warp];
-    float4 *boxes = reinterpret_cast<float4 *>(smem_raw + win_boxes_offset()) + (size_t)warp * warp_quads;
+    const uint32_t box_off = (uint32_t)(win_boxes_offset() + (size_t)warp * warp_quads * 16);
+    float4 *boxes = reinterpret_cast<float4 *>(smem_raw + box_off);
     unsigned char *raw = smem_raw + win_raw_offset(warp_quads) + (size_t)warp * warp_raw;
+    // the FP32 values of the warp's current node (read back only by the lane
+    // that wrote them, when the node is queued for the exact pass)
+    float *wv = warp_vals + ((size_t)blockIdx.x * kWinWarps + warp) * kSlotCap;
     if (lane == 0) mbar_init(&W.mbar);
     __syncwarp();
     uint32_t phase = 0;   // parity of the mbarrier phase the next copies complete
     unsigned long long evals = 0;
+    // node queue: batches of `grab` nodes
+    unsigned long long qbase = 0;
+    int qi = grab;
+    bool qdone = false;
+    // the last fetched group: its node's context, first slot and the node's slot count
+    int pb = 1, pk0 = 0, pK = 0;
+    // the fetched group, per lane: status | inside << 2 | target radius << 8,
+    // reference window and target centre offsets in the boxes (row << 16 |
+    // column), fractions and the rotation
+    int nst = 0;
+    uint32_t nro = 0, nto = 0;
+    float nrfx = 0.f, nrfy = 0.f, ntfx = 0.f, ntfy = 0.f, ncf = 1.f, nsf = 0.f;
+    // ... and its boxes (warp-uniform): mode 0 none / 1 tiles / 2 loads
+    int nmode = 0, nrx0 = 0, nry0 = 0, nrw = 0, nrbh = 0, ntx0 = 0, nty0 = 0, ntw = 0, ntbh = 0;
+    // the group being evaluated
+    bool have_cur = false;
+    int cb = 0, ck0 = 0;
+    // per-lane running values of the streamed scan over the current node
+    float vmax = -100.0f, amb = -INFINITY, amb_peak = -INFINITY;
+    float b1 = -INFINITY, b2 = -INFINITY;
+    bool need = false;
     for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(&ctl[0], (unsigned long long)grab);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= (unsigned long long)LS.total) break;
-        for (int gi = 0; gi < grab; ++gi) {
-            const int64_t gn = (int64_t)base + gi;
-            if (gn >= LS.total) break;
-            const int K = node_k[gn];
-            if (K == 0) continue;
-            const int lvl = level_of(LS, gn);
-            const DevLevel &P = LS.lv[lvl];
-            const int64_t pt = gn - __ldg(LS.base + lvl);
-            const int H = P.H;
-            const DevImage &ri = P.im[P.ref];
-            const DevImage &tI = P.im[1];
-            const bool voxels = P.vox && !P.cmr && !P.is_ra;
-            vll_voxel *vrow = voxels ? P.vox + P.vox_off[pt] : nullptr;
-            const vll_ugrid gg = P.gp3[pt];
-            const int start_H = gg.minHeight, end_H = gg.maxHeight;
-            // the record (as prep left it) is read again where it is written;
-            // per-node values below are reloaded where used, to keep them out
-            // of the registers of the window arithmetic
-            const int ncc_min = P.ncc[pt].minHeight;
-            const bool chc = P.ncc[pt].check_height_change != 0;
-            if (P.combined_incc || K > kSlotCap) {
-                // combined-level INCC (setsm_code.cpp:6378-6464: the windows at
-                // this level and the next finer one, the averaged orientation
-                // and both bounds tests), or a range longer than the shared
-                // slot buffer: the node goes to the exact pass, to be evaluated
-                // there wholly in FP64 (offset -2: not evaluated yet)
-                if (lane == 0) {
-                    const unsigned long long idx = atomicAdd(&ctl[2], 1ull);
-                    pend_node[idx] = gn;
-                    pend_off[idx] = -2;
-                }
-                continue;
-            }
-            // 16-byte aligned image rows allow 128-bit staging loads
-            const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
-                                ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
-                                  reinterpret_cast<uintptr_t>(tI.img) |
-                                  reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
-            const double inv_s = 1.0 / (double)(1 << P.L);
-            // per-node RPC cubics: lanes 0..7 = (image, polynomial)
-            if (lane < 8) {
-                const int im = lane >> 2, j = lane & 3;
-                const double *rpc = (im == 0 ? ri : tI).rpc;
-                node_horner_poly(rpc, P.grid_wgs[2 * pt], P.grid_wgs[2 * pt + 1], j,
-                                 W.horner[im][j]);
-                if (j == 0) {
-                    W.hnorm[im][0] = rpc[4];
-                    W.hnorm[im][1] = 1.0 / rpc[9];
-                }
-            }
-            if (lane == 0) {
-                W.R = P.ncc[pt];
-                W.have = false;
-                W.pre_v = -1.0f;
-                W.pre_dir = 0;
-                W.pre_k = -1;
-            }
-            // per-lane running values of the streamed scan
-            float vmax = -100.0f, amb = -INFINITY, amb_peak = -INFINITY;
-            float b1 = -INFINITY, b2 = -INFINITY;
-            bool need = false;
+        const int st = nst;
+        const uint32_t ro = nro, to = nto;
+        const float rfx = nrfx, rfy = nrfy, tfx = ntfx, tfy = ntfy, cf = ncf, sf = nsf;
+        const int rbw = nrw | 1, rbh = nrbh, tbw = ntw | 1, tbh = ntbh;
+        bool staged = false;
+        // ---- stage the current group's boxes ----
+        if (have_cur && nmode != 0) {
+            const NodeCtx &C = W.node[cb];
+            if (lane == 0) W.zn = 0;
             __syncwarp();
-            for (int k0 = 0; k0 < K; k0 += 32) {
-                const int k = k0 + lane;
-                // ---- per-lane geometry ----
-                int status = 0;   // 0 idle/skip, 1 orientation reject, 2 evaluate
-                double2 rp = make_double2(0, 0), tp = make_double2(0, 0);
-                int rot = kRotOffset;
-                float hgt = 0.f;
-                if (k < K) {
-                    hgt = slot_height(P, start_H, ncc_min, k);
-                    if (hgt >= (float)start_H && hgt <= (float)end_H) {
-                        bool edge = false;
-                        rp = fast_coord(W.horner[0], W.hnorm[0], ri, (double)hgt, inv_s, edge);
-                        tp = fast_coord(W.horner[1], W.hnorm[1], tI, (double)hgt, inv_s, edge);
-                        if (edge) {
-                            const double lon = P.grid_wgs[2 * pt], lat = P.grid_wgs[2 * pt + 1];
-                            rp = to_pyramid(rpc_project(ri.rpc, ri.adj, lon, lat, (double)hgt), ri.sx, ri.sy, P.L);
-                            tp = to_pyramid(rpc_project(tI.rpc, tI.adj, lon, lat, (double)hgt), tI.sx, tI.sy, P.L);
-                        }
-                        if (in_image(rp, ri.w, ri.h) && in_image(tp, tI.w, tI.h)) {
-                            const int od = (int)ri.ori[(int64_t)(int)rp.y * ri.w + (int)rp.x] -
-                                           (int)tI.ori[(int64_t)(int)tp.y * tI.w + (int)tp.x];
-                            bool ok = true;
-                            if (!P.is_ra && P.L >= 3) {
-                                const double a = __dmul_rn((double)od, P.bin_angle);
-                                ok = a < 90 && a > -90;
-                            }
-                            status = ok ? 2 : 1;
-                            rot = 2 * od + kRotOffset;
-                        }
-                    }
+            float4 *tbox = boxes + rbw * rbh;
+            if (nmode == 1) {
+                if (!__all_sync(0xffffffffu, mbar_wait(&W.mbar, phase, 2000000000ll))) {
+                    // the copies did not complete within ~1 s: report, wait
+                    // once more (bounded) for them, and stop this warp
+                    if (lane == 0) atomicExch(&counters[3], 1ull);
+                    mbar_wait(&W.mbar, phase, 2000000000ll);
+                    return;
                 }
-                // ---- footprint of the evaluating lanes ----
-                const float cf = (float)P.rot_cos[rot], sf = (float)P.rot_sin[rot];
-                const int rix = (int)floor(rp.x), riy = (int)floor(rp.y);
-                const int tix = (int)floor(tp.x), tiy = (int)floor(tp.y);
-                // target footprint radius: the window is the square |col|, |row| <= H
-                // cut by the disc of radius H + 1, so a rotation moves its samples
-                // at most min((|c| + |s|) H, H + 1) from the centre (+1 for the
-                // bilinear neighbour and FP32 rounding)
-                const int R = min((int)ceilf((fabsf(cf) + fabsf(sf)) * (float)H) + 1, H + 2);
-                const bool inside = status == 2 && rix - H >= 0 && riy - H >= 0 &&
-                                    rix + H + 2 < (int)ri.w && riy + H + 2 < (int)ri.h && tix - R >= 0 &&
-                                    tiy - R >= 0 && tix + R + 2 < (int)tI.w && tiy + R + 2 < (int)tI.h;
-                int rx0 = inside ? rix - H : INT_MAX, ry0 = inside ? riy - H : INT_MAX;
-                int rx1 = inside ? rix + H + 1 : INT_MIN, ry1 = inside ? riy + H + 1 : INT_MIN;
-                int tx0 = inside ? tix - R : INT_MAX, ty0 = inside ? tiy - R : INT_MAX;
-                int tx1 = inside ? tix + R + 1 : INT_MIN, ty1 = inside ? tiy + R + 1 : INT_MIN;
-                rx0 = __reduce_min_sync(0xffffffffu, rx0);
-                ry0 = __reduce_min_sync(0xffffffffu, ry0);
-                rx1 = __reduce_max_sync(0xffffffffu, rx1);
-                ry1 = __reduce_max_sync(0xffffffffu, ry1);
-                tx0 = __reduce_min_sync(0xffffffffu, tx0);
-                ty0 = __reduce_min_sync(0xffffffffu, ty0);
-                tx1 = __reduce_max_sync(0xffffffffu, tx1);
-                ty1 = __reduce_max_sync(0xffffffffu, ty1);
-                bool staged = false;
-                int rbw = 0, rbh = 0, tbw = 0;
-                if (__any_sync(0xffffffffu, inside)) {
-                    const int rw = rx1 - rx0 + 1, tw = tx1 - tx0 + 1;
-                    // odd row strides spread consecutive rows over the shared-memory bank groups
-                    rbw = rw | 1;
-                    rbh = ry1 - ry0 + 1;
-                    tbw = tw | 1;
-                    const int tbh = ty1 - ty0 + 1;
-                    // the level's TMA tiles: texels [xa, xa + tma_w) x rows [y0, y0 +
-                    // tma_h) of each plane, xa = x0 rounded down to 8 (16 bytes)
-                    const int rxa = rx0 & ~7, txa = tx0 & ~7;
-                    const int tw0 = P.tma_w[0], th0 = P.tma_h[0];
-                    const int tw1 = P.tma_w[1], th1 = P.tma_h[1];
-                    const int rtile = (tw0 * th0 * 2 + 127) & ~127;   // bytes per plane tile
-                    const int ttile = (tw1 * th1 * 2 + 127) & ~127;
-                    const bool tma = tw0 > 0 && rx1 + 2 - rxa <= tw0 && rbh <= th0 &&
-                                     tx1 + 2 - txa <= tw1 && tbh <= th1 &&
-                                     2 * (rtile + ttile) <= warp_raw;
-                    if (rbw * rbh + tbw * tbh <= warp_quads && tma) {
-                        // ---- four tile copies (TMA), then conversion ----
-                        unsigned char *rI = raw, *rM = raw + rtile;
-                        unsigned char *tIr = raw + 2 * rtile, *tMr = tIr + ttile;
-                        if (lane == 0) {
-                            const void *m0 = P.tmap[0][0], *m1 = P.tmap[0][1];
-                            const void *m2 = P.tmap[1][0], *m3 = P.tmap[1][1];
-                            tmap_acquire(m0);
-                            tmap_acquire(m1);
-                            tmap_acquire(m2);
-                            tmap_acquire(m3);
-                            mbar_arrive_expect(&W.mbar, (uint32_t)(2 * (tw0 * th0 + tw1 * th1) * 2));
-                            tma_tile_2d(rI, m0, rxa, ry0, &W.mbar);
-                            tma_tile_2d(rM, m1, rxa, ry0, &W.mbar);
-                            tma_tile_2d(tIr, m2, txa, ty0, &W.mbar);
-                            tma_tile_2d(tMr, m3, txa, ty0, &W.mbar);
-                        }
-                        if (!mbar_wait(&W.mbar, phase, 2000000000ll)) {
-                            // the copies did not complete within ~1 s: report, wait
-                            // once more (bounded) for them, and stop this warp
-                            if (lane == 0) atomicExch(&counters[3], 1ull);
-                            mbar_wait(&W.mbar, phase, 2000000000ll);
-                            return;
-                        }
-                        phase ^= 1u;
-                        const int rnb = 2 * tw0, tnb = 2 * tw1;   // tile row bytes
-                        // box shifts: the centre texels
-                        const int rc = (rbh / 2) * rnb + 2 * (rx0 + rw / 2 - rxa);
-                        const int tc = (tbh / 2) * tnb + 2 * (tx0 + tw / 2 - txa);
-                        const float sI = (float)*reinterpret_cast<const uint16_t *>(rI + rc);
-                        const float sM = (float)*reinterpret_cast<const uint16_t *>(rM + rc);
-                        const float tsI = (float)*reinterpret_cast<const uint16_t *>(tIr + tc);
-                        const float tsM = (float)*reinterpret_cast<const uint16_t *>(tMr + tc);
-                        const bool z1 = stage_from_raw(boxes, rbw, rI, rM, rnb, rxa, rx0, rw, rbh,
-                                                       sI, sM, lane);
-                        const bool z2 = stage_from_raw(boxes + rbw * rbh, tbw, tIr, tMr, tnb, txa,
-                                                       tx0, tw, tbh, tsI, tsM, lane);
-                        // the tiles are rewritten by the next copies
-                        fence_async_shared();
-                        __syncwarp();
-                        staged = !(z1 || z2);
-                    } else if (rbw * rbh + tbw * tbh <= warp_quads) {
-                        float sI = 0.f, sM = 0.f, tsI = 0.f, tsM = 0.f;
-                        if (lane == 0) {
-                            const int64_t pc = (int64_t)(ry0 + rbh / 2) * ri.w + (rx0 + rbw / 2);
-                            sI = (float)__ldg(ri.img + pc);
-                            sM = (float)__ldg(ri.mag + pc);
-                            const int64_t p2 = (int64_t)(ty0 + tbh / 2) * tI.w + (tx0 + tbw / 2);
-                            tsI = (float)__ldg(tI.img + p2);
-                            tsM = (float)__ldg(tI.mag + p2);
-                        }
-                        sI = __shfl_sync(0xffffffffu, sI, 0);
-                        sM = __shfl_sync(0xffffffffu, sM, 0);
-                        tsI = __shfl_sync(0xffffffffu, tsI, 0);
-                        tsM = __shfl_sync(0xffffffffu, tsM, 0);
-                        bool z1, z2;
-                        if (vec_ok) {
-                            z1 = stage_box_vec(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh, sI,
-                                               sM, lane);
-                            z2 = stage_box_vec(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0, ty0,
-                                               tw, tbh, tsI, tsM, lane);
-                        } else {
-                            z1 = stage_box_strided(boxes, rbw, ri.img, ri.mag, ri.w, rx0, ry0, rw, rbh,
-                                                   sI, sM, lane);
-                            z2 = stage_box_strided(boxes + rbw * rbh, tbw, tI.img, tI.mag, tI.w, tx0,
-                                                   ty0, tw, tbh, tsI, tsM, lane);
-                        }
-                        __syncwarp();
-                        staged = !(z1 || z2);
-                    }
+                phase ^= 1u;
+                const int tw0 = C.tma_w[0], tw1 = C.tma_w[1];
+                const int rtile = (tw0 * C.tma_h[0] * 2 + 127) & ~127;   // bytes per plane tile
+                const int ttile = (tw1 * C.tma_h[1] * 2 + 127) & ~127;
+                const unsigned char *rI = raw, *rM = raw + rtile;
+                const unsigned char *tIr = raw + 2 * rtile, *tMr = tIr + ttile;
+                const int rxa = nrx0 & ~7, txa = ntx0 & ~7;
+                const int rnb = 2 * tw0, tnb = 2 * tw1;   // tile row bytes
+                // box shifts: the centre texels
+                const int rc = (rbh / 2) * rnb + 2 * (nrx0 + nrw / 2 - rxa);
+                const int tc = (tbh / 2) * tnb + 2 * (ntx0 + ntw / 2 - txa);
+                const float sI = (float)*reinterpret_cast<const uint16_t *>(rI + rc);
+                const float sM = (float)*reinterpret_cast<const uint16_t *>(rM + rc);
+                const float tsI = (float)*reinterpret_cast<const uint16_t *>(tIr + tc);
+                const float tsM = (float)*reinterpret_cast<const uint16_t *>(tMr + tc);
+                convert_tile<false>(boxes, rbw, rI, rM, rnb, rxa, nrx0, nrw, rbh, sI, sM, W.zl,
+                                    &W.zn, kZeroCap, 0u, lane);
+                convert_tile<true>(tbox, tbw, tIr, tMr, tnb, txa, ntx0, ntw, tbh, tsI, tsM, W.zl,
+                                   &W.zn, kZeroCap, 0x80000000u, lane);
+                // the tiles are rewritten by the next group's copies
+                fence_async_shared();
+                __syncwarp();
+            } else {
+                float sI = 0.f, sM = 0.f, tsI = 0.f, tsM = 0.f;
+                if (lane == 0) {
+                    const int64_t pc = (int64_t)(nry0 + rbh / 2) * C.w[0] + (nrx0 + rbw / 2);
+                    sI = (float)__ldg(C.img[0] + pc);
+                    sM = (float)__ldg(C.mag[0] + pc);
+                    const int64_t p2 = (int64_t)(nty0 + tbh / 2) * C.w[1] + (ntx0 + tbw / 2);
+                    tsI = (float)__ldg(C.img[1] + p2);
+                    tsM = (float)__ldg(C.mag[1] + p2);
                 }
-                float rho_v = kNotEvaluated, incc_v = 0.f;
-                bool all_pos = false, deferred = false;
-                if (status == 1) {
-                    rho_v = kRejected;
-                } else if (status == 2) {
-                    if (staged && inside) {
-                        float incc;
-                        bool unsure = false;
-                        window_any(H, boxes + (riy - H - ry0) * rbw + (rix - H - rx0), rbw,
-                                   (float)(rp.x - (double)rix), (float)(rp.y - (double)riy),
-                                   boxes + rbw * rbh + (tiy - ty0) * tbw + (tix - tx0), tbw,
-                                   (float)(tp.x - (double)tix), (float)(tp.y - (double)tiy), cf, sf,
-                                   incc, unsure);
-                        const bool has = incc != -2.0f;
-                        const double incc_d = has ? (double)incc : -1.0;
-                        double rho_d;
-                        const double cnt_g = gcnt ? gcnt[gn] : 0.0;
-                        if (P.check_ortho && cnt_g > 0)
-                            rho_d = has ? incc_d * P.alpha + (gsum[gn] / cnt_g) * P.beta
-                                        : __ddiv_rn(0.0, 0.0);
-                        else
-                            rho_d = incc_d;
-                        rho_v = (float)rho_d;
-                        incc_v = unsure ? __int_as_float(0x7fc00000) : (float)incc_d;
-                        all_pos = true;   // window inside the image, no zero texels
-                    } else {
-                        // window not staged (near an image edge, a zero texel in
-                        // the boxes, or boxes beyond the budget): the exact pass
-                        // evaluates the slot in FP64
-                        rho_v = 0.f;
-                        incc_v = __int_as_float(0x7fc00000);
-                        deferred = true;
-                    }
-                    evals++;
+                sI = __shfl_sync(0xffffffffu, sI, 0);
+                sM = __shfl_sync(0xffffffffu, sM, 0);
+                tsI = __shfl_sync(0xffffffffu, tsI, 0);
+                tsM = __shfl_sync(0xffffffffu, tsM, 0);
+                bool z;
+                if (C.flags & kNfVec) {
+                    z = stage_box_vec<false>(boxes, rbw, C.img[0], C.mag[0], C.w[0], nrx0, nry0,
+                                             nrw, rbh, sI, sM, lane);
+                    z |= stage_box_vec<true>(tbox, tbw, C.img[1], C.mag[1], C.w[1], ntx0, nty0,
+                                             ntw, tbh, tsI, tsM, lane);
+                } else {
+                    z = stage_box_strided<false>(boxes, rbw, C.img[0], C.mag[0], C.w[0], nrx0,
+                                                 nry0, nrw, rbh, sI, sM, lane);
+                    z |= stage_box_strided<true>(tbox, tbw, C.img[1], C.mag[1], C.w[1], ntx0,
+                                                 nty0, ntw, tbh, tsI, tsM, lane);
                 }
-
-                // ---- FindPeakNcc streamed over this group of 32 slots ----
-                // (setsm_code.cpp:6672-6752 on the FP32 values; every decision
-                // within the error band, and every value the FP32 pass could not
-                // take -- deferred windows, unsure variances, voxel truncations
-                // near an integer, NaN --, sends the node to the exact pass)
-                const bool ev = k < K && status == 2;
-                const bool unusable = ev && (isnan(incc_v) || isnan(rho_v) ||
-                                             (voxels && near_trunc((double)incc_v)));
-                if (k < K) W.vals[k] = unusable ? __int_as_float(0x7fc00000) : rho_v;
-                bool band = unusable;
-                const uint32_t em = __ballot_sync(0xffffffffu, ev);
-                if (em) {
-                    const int p_in = prev_eval(em, lane, -1);
-                    const float pv_in = __shfl_sync(0xffffffffu, rho_v, p_in < 0 ? 0 : p_in);
-                    const bool has_p = p_in >= 0 || W.have;
-                    const float pv = p_in >= 0 ? pv_in : W.pre_v;
-                    // direction of this slot: the sign of the change (the
-                    // reference's sign rule reduces to it); -1 on the first one
-                    const int td = has_p ? (rho_v > pv) - (rho_v < pv) : -1;
-                    const int td_in = __shfl_sync(0xffffffffu, td, p_in < 0 ? 0 : p_in);
-                    const int dp = p_in >= 0 ? td_in : W.pre_dir;
-                    bool is_peak = false;
-                    if (ev && !unusable) {
-                        const float fv = rho_v;
-                        if (fv > vmax) vmax = fv;
-                        if (near_round((double)fv) && fv > amb) amb = fv;
-                        if (P.cmr && has_p) {
-                            if (fabsf(fv - pv) < kBand || fabsf(fv) < kBand || fabsf(pv) < kBand)
-                                band = true;
-                            is_peak = pv != -1.0f && dp > 0 && td < 0;
-                        }
-                    }
-                    if (is_peak) {
-                        if (near_round((double)pv) && pv > amb_peak) amb_peak = pv;
-                        if (pv > b1) {
-                            b2 = b1;
-                            b1 = pv;
-                        } else if (pv > b2) {
-                            b2 = pv;
-                        }
-                    }
-                    // the ordered top-two fold of this group's peaks (lane 0)
-                    uint32_t pm = __ballot_sync(0xffffffffu, is_peak);
-                    const int p_slot = p_in >= 0 ? k0 + p_in : W.pre_k;
-                    while (pm) {
-                        const int b = __ffs(pm) - 1;
-                        pm &= pm - 1;
-                        const float val = __shfl_sync(0xffffffffu, pv, b);
-                        const int ps = __shfl_sync(0xffffffffu, p_slot, b);
-                        if (lane == 0) {
-                            vll_nccresult &R = W.R;
-                            const float ph = slot_height(P, start_H, ncc_min, ps);
-                            if (R.result4 < 10) R.result4 += 1;
-                            const int16_t qpre = q_result((double)val);
-                            if (R.result0 < qpre) {
-                                const double t1 = dq_result(R.result0);
-                                R.result0 = qpre;
-                                const float t2 = R.result2;
-                                R.result2 = ph;
-                                const int16_t q1 = q_result(t1);
-                                if (R.result1 < q1) {
-                                    R.result1 = q1;
-                                    R.result3 = t2;
-                                }
-                            } else if (R.result1 < qpre) {
-                                R.result1 = qpre;
-                                R.result3 = ph;
-                            }
-                        }
-                    }
-                    // carry the last evaluated slot into the next group
-                    const int last = 31 - __clz(em);
-                    const float lv = __shfl_sync(0xffffffffu, rho_v, last);
-                    const int ld = __shfl_sync(0xffffffffu, td, last);
-                    __syncwarp();
-                    if (lane == 0) {
-                        W.pre_v = lv;
-                        W.pre_dir = ld;
-                        W.pre_k = k0 + last;
-                        W.have = true;
-                    }
-                }
-                if (__any_sync(0xffffffffu, band)) need = true;
-                if (P.dbg_rho && status == 2)
-                    P.dbg_rho[P.dbg_off[pt] + k] = deferred ? __longlong_as_double(0x7ff8000000000000ll)
-                                                            : (double)rho_v;
-                if (k < K && voxels) {
-                    vll_voxel *v = vrow + k;
-                    if (status == 1) v->flag_cal = 0;
-                    if (status == 2) {
-                        if (all_pos) v->flag_cal = 1;
-                        v->INCC = q_voxel(isnan(incc_v) ? 0.0 : (double)incc_v);
-                    }
-                }
+                // a zero texel in these boxes sends every slot to the exact pass
+                if (z && lane == 0) W.zn = kZeroCap + 1;
                 __syncwarp();
             }
-            // the maximum, and roundings that could change the maximum or the
-            // top two (a peak more than 0.002 + 2 bands below the second best
-            // rounds strictly below it)
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-                amb = fmaxf(amb, __shfl_xor_sync(0xffffffffu, amb, o));
-                amb_peak = fmaxf(amb_peak, __shfl_xor_sync(0xffffffffu, amb_peak, o));
-                const float o1 = __shfl_xor_sync(0xffffffffu, b1, o);
-                const float o2 = __shfl_xor_sync(0xffffffffu, b2, o);
-                const float n1 = fmaxf(b1, o1);
-                const float n2 = fmaxf(fminf(b1, o1), fmaxf(b2, o2));
-                b1 = n1;
-                b2 = n2;
-            }
-            if (chc && (double)amb >= (double)vmax - (double)kBand) need = true;
-            if (P.cmr && amb_peak > -1e29f) {
-                const double thr = (double)(b2 > -1e29f ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
-                if ((double)amb_peak >= thr) need = true;
-            }
-            if (!need) {
-                if (lane == 0) {
-                    vll_nccresult R = W.R;
-                    if (R.check_height_change) R.max_WNCC = q_result((double)vmax);
-                    P.ncc[pt] = R;
+            staged = true;
+        }
+
+        // ---- fetch the next group: node, geometry, boxes, tile copies ----
+        bool have_next = false;
+        if (pK > 0 && pk0 + 32 < pK) {
+            pk0 += 32;
+            have_next = true;
+        } else {
+            pK = 0;
+            while (!qdone) {
+                if (qi >= grab) {
+                    unsigned long long b = 0;
+                    if (lane == 0) b = atomicAdd(&ctl[0], (unsigned long long)grab);
+                    qbase = __shfl_sync(0xffffffffu, b, 0);
+                    qi = 0;
                 }
-            } else {
-                long long off = -1;
-                if (lane == 0) {
-                    off = (long long)atomicAdd(&ctl[4], (unsigned long long)K);
-                    if (off + K > pend_cap) off = -1;
-                    const unsigned long long idx = atomicAdd(&ctl[2], 1ull);
-                    pend_node[idx] = gn;
-                    pend_off[idx] = off;
+                const int64_t gn = (int64_t)qbase + qi++;
+                if (gn >= LS.total) {
+                    qdone = true;
+                    break;
                 }
-                off = __shfl_sync(0xffffffffu, off, 0);
-                if (off >= 0)
-                    for (int kk = lane; kk < K; kk += 32) pend_vals[off + kk] = W.vals[kk];
+                const int K = node_k[gn];
+                if (K == 0) continue;
+                const int lvl = level_of(LS, gn);
+                if (LS.lv[lvl].combined_incc || K > kSlotCap) {
+                    // combined-level INCC (setsm_code.cpp:6378-6464: the windows at
+                    // this level and the next finer one, the averaged orientation
+                    // and both bounds tests), or a range longer than the slot
+                    // scratch: the node is evaluated wholly in FP64 by the exact
+                    // pass (offset -2: not evaluated yet)
+                    if (lane == 0) {
+                        const unsigned long long idx = atomicAdd(&ctl[2], 1ull);
+                        pend_node[idx] = gn;
+                        pend_off[idx] = -2;
+                    }
+                    continue;
+                }
+                pb ^= 1;
+                node_setup(W.node[pb], LS, lvl, gn, K, gsum, gcnt, lane);
+                pk0 = 0;
+                pK = K;
+                have_next = true;
+                break;
+            }
+        }
+        nmode = 0;
+        if (have_next) {
+            const NodeCtx &N = W.node[pb];
+            const int k = pk0 + lane;
+            const int H = N.H;
+            int status = 0;   // 0 idle/skip, 1 orientation reject, 2 evaluate
+            double2 rp = make_double2(0, 0), tp = make_double2(0, 0);
+            int rot = kRotOffset;
+            if (k < N.K) {
+                const float hgt = (float)__dadd_rn(N.hbase, __dmul_rn((double)k, N.hstep));
+                if (hgt >= (float)N.start_H && hgt <= (float)N.end_H) {
+                    bool edge = false;
+                    rp = node_coord(N, 0, (double)hgt, edge);
+                    tp = node_coord(N, 1, (double)hgt, edge);
+                    if (edge) slot_coords_exact(N, (double)hgt, rp, tp);
+                    if (in_image(rp, N.w[0], N.h[0]) && in_image(tp, N.w[1], N.h[1])) {
+                        const int od = (int)N.ori[0][(int64_t)(int)rp.y * N.w[0] + (int)rp.x] -
+                                       (int)N.ori[1][(int64_t)(int)tp.y * N.w[1] + (int)tp.x];
+                        bool ok = true;
+                        if (N.flags & kNfOri) {
+                            const double a = __dmul_rn((double)od, N.bin_angle);
+                            ok = a < 90 && a > -90;
+                        }
+                        status = ok ? 2 : 1;
+                        rot = 2 * od + kRotOffset;
+                    }
+                }
+            }
+            const float cfv = (float)N.P->rot_cos[rot], sfv = (float)N.P->rot_sin[rot];
+            const int rix = (int)floor(rp.x), riy = (int)floor(rp.y);
+            const int tix = (int)floor(tp.x), tiy = (int)floor(tp.y);
+            // target footprint radius: the window is the square |col|, |row| <= H
+            // cut by the disc of radius H + 1, so a rotation moves its samples
+            // at most min((|c| + |s|) H, H + 1) from the centre (+1 for the
+            // bilinear neighbour and FP32 rounding)
+            const int R = min((int)ceilf((fabsf(cfv) + fabsf(sfv)) * (float)H) + 1, H + 2);
+            const bool inside = status == 2 && rix - H >= 0 && riy - H >= 0 &&
+                                rix + H + 2 < (int)N.w[0] && riy + H + 2 < (int)N.h[0] &&
+                                tix - R >= 0 && tiy - R >= 0 && tix + R + 2 < (int)N.w[1] &&
+                                tiy + R + 2 < (int)N.h[1];
+            const int rx0 = __reduce_min_sync(0xffffffffu, inside ? rix - H : INT_MAX);
+            const int ry0 = __reduce_min_sync(0xffffffffu, inside ? riy - H : INT_MAX);
+            const int rx1 = __reduce_max_sync(0xffffffffu, inside ? rix + H + 1 : INT_MIN);
+            const int ry1 = __reduce_max_sync(0xffffffffu, inside ? riy + H + 1 : INT_MIN);
+            const int tx0 = __reduce_min_sync(0xffffffffu, inside ? tix - R : INT_MAX);
+            const int ty0 = __reduce_min_sync(0xffffffffu, inside ? tiy - R : INT_MAX);
+            const int tx1 = __reduce_max_sync(0xffffffffu, inside ? tix + R + 1 : INT_MIN);
+            const int ty1 = __reduce_max_sync(0xffffffffu, inside ? tiy + R + 1 : INT_MIN);
+            nst = status | (inside ? 4 : 0) | (R << 8);
+            nro = inside ? ((uint32_t)(riy - H - ry0) << 16) | (uint32_t)(rix - H - rx0) : 0u;
+            nto = inside ? ((uint32_t)(tiy - ty0) << 16) | (uint32_t)(tix - tx0) : 0u;
+            nrfx = (float)(rp.x - (double)rix);
+            nrfy = (float)(rp.y - (double)riy);
+            ntfx = (float)(tp.x - (double)tix);
+            ntfy = (float)(tp.y - (double)tiy);
+            ncf = cfv;
+            nsf = sfv;
+            if (rx0 != INT_MAX) {
+                // pairs [x0, x1] of rows [y0, y1]; odd row strides spread
+                // consecutive rows over the shared-memory bank groups
+                nrx0 = rx0;
+                nry0 = ry0;
+                nrw = rx1 - rx0 + 1;
+                nrbh = ry1 - ry0 + 1;
+                ntx0 = tx0;
+                nty0 = ty0;
+                ntw = tx1 - tx0 + 1;
+                ntbh = ty1 - ty0 + 1;
+                const bool fits = (nrw | 1) * nrbh + (ntw | 1) * ntbh <= warp_quads;
+                // the level's TMA tiles: texels [xa, xa + tma_w) x rows [y0, y0 +
+                // tma_h) of each plane, xa = x0 rounded down to 8 (16 bytes)
+                const int rxa = rx0 & ~7, txa = tx0 & ~7;
+                const int tw0 = N.tma_w[0], th0 = N.tma_h[0];
+                const int tw1 = N.tma_w[1], th1 = N.tma_h[1];
+                const int rtile = (tw0 * th0 * 2 + 127) & ~127;   // bytes per plane tile
+                const int ttile = (tw1 * th1 * 2 + 127) & ~127;
+                const bool tma = (N.flags & kNfTma) && rx1 + 2 - rxa <= tw0 && nrbh <= th0 &&
+                                 tx1 + 2 - txa <= tw1 && ntbh <= th1 &&
+                                 2 * (rtile + ttile) <= warp_raw;
+                if (fits && tma) {
+                    nmode = 1;
+                    if (lane == 0) {
+                        const DevLevel &P = *N.P;
+                        unsigned char *rI = raw, *rM = raw + rtile;
+                        unsigned char *tIr = raw + 2 * rtile, *tMr = tIr + ttile;
+                        mbar_arrive_expect(&W.mbar, (uint32_t)(2 * (tw0 * th0 + tw1 * th1) * 2));
+                        tma_tile_2d(rI, P.tmap[0][0], rxa, ry0, &W.mbar);
+                        tma_tile_2d(rM, P.tmap[0][1], rxa, ry0, &W.mbar);
+                        tma_tile_2d(tIr, P.tmap[1][0], txa, ty0, &W.mbar);
+                        tma_tile_2d(tMr, P.tmap[1][1], txa, ty0, &W.mbar);
+                    }
+                } else if (fits) {
+                    nmode = 2;
+                }
+            }
+        }
+
+        // ---- evaluate the current group ----
+        if (have_cur) {
+            NodeCtx &C = W.node[cb];
+            const int K = C.K;
+            const int k = ck0 + lane;
+            const int status = st & 3;
+            const bool inside = (st & 4) != 0;
+            const uint32_t flags = C.flags;
+            // a zero intensity texel within the slot's footprints: the
+            // reference drops the samples whose interpolated intensity is not
+            // positive, which FP32 on shifted texels cannot decide
+            bool zero_hit = false;
+            if (staged && status == 2 && inside) {
+                const int zn = W.zn;
+                if (zn > kZeroCap) {
+                    zero_hit = true;
+                } else if (zn > 0) {
+                    const int H = C.H, R = st >> 8;
+                    const int rxo = (int)(ro & 0xFFFFu), ryo = (int)(ro >> 16);
+                    const int txo = (int)(to & 0xFFFFu), tyo = (int)(to >> 16);
+                    for (int i = 0; i < zn; ++i) {
+                        const uint32_t e = W.zl[i];
+                        const int ex = (int)(e & 0xFFFFu), ey = (int)((e >> 16) & 0x7FFFu);
+                        if (e & 0x80000000u)
+                            zero_hit |= ex >= txo - R && ex <= txo + R + 1 && ey >= tyo - R &&
+                                        ey <= tyo + R + 1;
+                        else
+                            zero_hit |= ex >= rxo && ex <= rxo + 2 * H + 1 && ey >= ryo &&
+                                        ey <= ryo + 2 * H + 1;
+                    }
+                }
+            }
+            float rho_v = kNotEvaluated, incc_v = 0.f;
+            bool all_pos = false, deferred = false;
+            if (status == 1) {
+                rho_v = kRejected;
+            } else if (status == 2) {
+                if (staged && inside && !zero_hit) {
+                    float incc;
+                    bool unsure = false;
+                    const float4 *qr = boxes + (int)(ro >> 16) * rbw + (int)(ro & 0xFFFFu);
+                    const uint32_t tcen =
+                        box_off + (uint32_t)(rbw * rbh + (int)(to >> 16) * tbw + (int)(to & 0xFFFFu)) * 16u;
+                    window_any(C.H, qr, rbw, rfx, rfy, tgt_box(smem_raw, tcen, (uint32_t)tbw * 16u),
+                               tfx, tfy, cf, sf, incc, unsure);
+                    const bool has = incc != -2.0f;
+                    const double incc_d = has ? (double)incc : -1.0;
+                    double rho_d;
+                    if (flags & kNfGncc)
+                        rho_d = has ? incc_d * C.alpha + C.gterm : __ddiv_rn(0.0, 0.0);
+                    else
+                        rho_d = incc_d;
+                    rho_v = (float)rho_d;
+                    incc_v = unsure ? __int_as_float(0x7fc00000) : (float)incc_d;
+                    all_pos = true;   // window inside the image, no zero texels
+                } else {
+                    // window not staged (near an image edge, a zero texel in
+                    // its footprint, or boxes beyond the budget): the exact pass
+                    // evaluates the slot in FP64
+                    rho_v = 0.f;
+                    incc_v = __int_as_float(0x7fc00000);
+                    deferred = true;
+                }
+                evals++;
+            }
+
+            // ---- FindPeakNcc streamed over this group of 32 slots ----
+            // (setsm_code.cpp:6672-6752 on the FP32 values; every decision
+            // within the error band, and every value the FP32 pass could not
+            // take -- deferred windows, unsure variances, voxel truncations
+            // near an integer, NaN --, sends the node to the exact pass)
+            const bool voxels = (flags & kNfVox) != 0;
+            const bool ev = k < K && status == 2;
+            const bool unusable = ev && (isnan(incc_v) || isnan(rho_v) ||
+                                         (voxels && near_trunc((double)incc_v)));
+            if (k < K) wv[k] = unusable ? __int_as_float(0x7fc00000) : rho_v;
+            bool band = unusable;
+            const uint32_t em = __ballot_sync(0xffffffffu, ev);
+            if (em) {
+                const int p_in = prev_eval(em, lane, -1);
+                const float pv_in = __shfl_sync(0xffffffffu, rho_v, p_in < 0 ? 0 : p_in);
+                const bool has_p = p_in >= 0 || C.have;
+                const float pv = p_in >= 0 ? pv_in : C.pre_v;
+                // direction of this slot: the sign of the change (the
+                // reference's sign rule reduces to it); -1 on the first one
+                const int td = has_p ? (rho_v > pv) - (rho_v < pv) : -1;
+                const int td_in = __shfl_sync(0xffffffffu, td, p_in < 0 ? 0 : p_in);
+                const int dp = p_in >= 0 ? td_in : C.pre_dir;
+                bool is_peak = false;
+                if (ev && !unusable) {
+                    const float fv = rho_v;
+                    if (fv > vmax) vmax = fv;
+                    if (near_round((double)fv) && fv > amb) amb = fv;
+                    if ((flags & kNfCmr) && has_p) {
+                        if (fabsf(fv - pv) < kBand || fabsf(fv) < kBand || fabsf(pv) < kBand)
+                            band = true;
+                        is_peak = pv != -1.0f && dp > 0 && td < 0;
+                    }
+                }
+                if (is_peak) {
+                    if (near_round((double)pv) && pv > amb_peak) amb_peak = pv;
+                    if (pv > b1) {
+                        b2 = b1;
+                        b1 = pv;
+                    } else if (pv > b2) {
+                        b2 = pv;
+                    }
+                }
+                // the ordered top-two fold of this group's peaks (lane 0)
+                uint32_t pm = __ballot_sync(0xffffffffu, is_peak);
+                const int p_slot = p_in >= 0 ? ck0 + p_in : C.pre_k;
+                while (pm) {
+                    const int b = __ffs(pm) - 1;
+                    pm &= pm - 1;
+                    const float val = __shfl_sync(0xffffffffu, pv, b);
+                    const int ps = __shfl_sync(0xffffffffu, p_slot, b);
+                    if (lane == 0) {
+                        vll_nccresult &R = C.R;
+                        const float ph = (float)__dadd_rn(C.hbase, __dmul_rn((double)ps, C.hstep));
+                        if (R.result4 < 10) R.result4 += 1;
+                        const int16_t qpre = q_result((double)val);
+                        if (R.result0 < qpre) {
+                            const double t1 = dq_result(R.result0);
+                            R.result0 = qpre;
+                            const float t2 = R.result2;
+                            R.result2 = ph;
+                            const int16_t q1 = q_result(t1);
+                            if (R.result1 < q1) {
+                                R.result1 = q1;
+                                R.result3 = t2;
+                            }
+                        } else if (R.result1 < qpre) {
+                            R.result1 = qpre;
+                            R.result3 = ph;
+                        }
+                    }
+                }
+                // carry the last evaluated slot into the next group
+                const int last = 31 - __clz(em);
+                const float lv = __shfl_sync(0xffffffffu, rho_v, last);
+                const int ld = __shfl_sync(0xffffffffu, td, last);
+                __syncwarp();
+                if (lane == 0) {
+                    C.pre_v = lv;
+                    C.pre_dir = ld;
+                    C.pre_k = ck0 + last;
+                    C.have = 1;
+                }
+            }
+            if (__any_sync(0xffffffffu, band)) need = true;
+            if (status == 2 && (flags & kNfDbg))
+                C.P->dbg_rho[C.P->dbg_off[C.pt] + k] =
+                    deferred ? __longlong_as_double(0x7ff8000000000000ll) : (double)rho_v;
+            if (k < K && voxels) {
+                vll_voxel *v = C.vrow + k;
+                if (status == 1) v->flag_cal = 0;
+                if (status == 2) {
+                    if (all_pos) v->flag_cal = 1;
+                    v->INCC = q_voxel(isnan(incc_v) ? 0.0 : (double)incc_v);
+                }
             }
             __syncwarp();
+            if (ck0 + 32 >= K) {
+                // ---- the node's last group: write it, or queue it ----
+                // the maximum, and roundings that could change the maximum or
+                // the top two (a peak more than 0.002 + 2 bands below the
+                // second best rounds strictly below it)
+#pragma unroll
+                for (int o = 16; o; o >>= 1) {
+                    vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+                    amb = fmaxf(amb, __shfl_xor_sync(0xffffffffu, amb, o));
+                    amb_peak = fmaxf(amb_peak, __shfl_xor_sync(0xffffffffu, amb_peak, o));
+                    const float o1 = __shfl_xor_sync(0xffffffffu, b1, o);
+                    const float o2 = __shfl_xor_sync(0xffffffffu, b2, o);
+                    const float n1 = fmaxf(b1, o1);
+                    const float n2 = fmaxf(fminf(b1, o1), fmaxf(b2, o2));
+                    b1 = n1;
+                    b2 = n2;
+                }
+                if ((flags & kNfChc) && (double)amb >= (double)vmax - (double)kBand) need = true;
+                if ((flags & kNfCmr) && amb_peak > -1e29f) {
+                    const double thr =
+                        (double)(b2 > -1e29f ? b2 : b1) - 0.002 - 2.0 * (double)kBand;
+                    if ((double)amb_peak >= thr) need = true;
+                }
+                if (!need) {
+                    if (lane == 0) {
+                        vll_nccresult R = C.R;
+                        if (R.check_height_change) R.max_WNCC = q_result((double)vmax);
+                        C.P->ncc[C.pt] = R;
+                    }
+                } else {
+                    long long off = -1;
+                    if (lane == 0) {
+                        off = (long long)atomicAdd(&ctl[4], (unsigned long long)K);
+                        if (off + K > pend_cap) off = -1;
+                        const unsigned long long idx = atomicAdd(&ctl[2], 1ull);
+                        pend_node[idx] = C.gn;
+                        pend_off[idx] = off;
+                    }
+                    off = __shfl_sync(0xffffffffu, off, 0);
+                    if (off >= 0)
+                        for (int kk = lane; kk < K; kk += 32) pend_vals[off + kk] = wv[kk];
+                }
+                vmax = -100.0f;
+                amb = amb_peak = b1 = b2 = -INFINITY;
+                need = false;
+                __syncwarp();
+            }
         }
+        if (!have_next) break;
+        have_cur = true;
+        cb = pb;
+        ck0 = pk0;
     }
     for (int o = 16; o; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
     if (lane == 0 && evals) atomicAdd(&counters[1], evals);
@@ -1104,7 +1332,7 @@ __global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
     const int64_t *__restrict__ pend_off, const double *__restrict__ gsum,
     const double *__restrict__ gcnt, unsigned long long *__restrict__ counters,
     unsigned long long *__restrict__ ctl) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     WarpShared &W = reinterpret_cast<WarpShared *>(smem_raw)[warp];
@@ -1383,11 +1611,15 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel, kWinWarps * 32, smem);
     if (tu.blocks_per_sm > 0 && tu.blocks_per_sm < per_sm) per_sm = tu.blocks_per_sm;
-    if (per_sm < 1) per_sm = 1;
+    per_sm = std::max(1, std::min(per_sm, kWinMaxBlocksPerSm));
     const int grab = tu.grab > 0 ? std::min(tu.grab, 64) : 1;
+    // the warps' slot scratch follows the pending buffer's pend_cap values
+    // (window_scratch_floats sizes it for the largest grid)
+    float *warp_vals = pend_vals + pend_cap;
     window_kernel<<<sms * per_sm, kWinWarps * 32, smem, s>>>(LS, node_k, gsum, gcnt, pend_vals,
                                                              pend_cap, pend_node, pend_off,
-                                                             counters, ctl, wb.quads, wb.raw, grab);
+                                                             warp_vals, counters, ctl, wb.quads,
+                                                             wb.raw, grab);
     return cudaGetLastError();
 }
 
@@ -1430,6 +1662,15 @@ cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, cons
     }
     return launch_peaks(LS, set_max_h(hl, n), node_k, pend_vals, pend_node, pend_off, gsum, gcnt,
                         counters, ctl, s);
+}
+
+// Floats of per-warp slot scratch the window kernel needs after the pending
+// buffer's values: kSlotCap per warp of the largest grid on this device.
+int64_t window_scratch_floats() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (int64_t)sms * kWinMaxBlocksPerSm * kWinWarps * kSlotCap;
 }
 
 // Slots of FP32 values the pending buffer holds for a pass of n_slots slots:
@@ -1645,7 +1886,7 @@ cudaError_t split_size(SplitBuffers &b, int64_t N, cudaStream_t s, std::string *
     }
     const int64_t cap = pending_capacity(total);
     size_t c = b.cap_slots;
-    SPLIT_CUDA(grow(b.rho, c, (size_t)std::max<int64_t>(cap, 1) * sizeof(float)));
+    SPLIT_CUDA(grow(b.rho, c, (size_t)(cap + window_scratch_floats()) * sizeof(float)));
     b.cap_slots = c;
     b.pend_cap = cap;
     return cudaSuccess;
@@ -1882,7 +2123,15 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     // FP64 there, so its size affects speed only
     const size_t used = (cv.used + 255) & ~(size_t)255;
     float *pend_vals = (float *)((unsigned char *)base + used);
-    const int64_t pend_cap = (int64_t)((kNoAllocScratchBytes - used) / sizeof(float));
+    // ... after the window kernel's per-warp slot scratch is set aside
+    const int64_t pend_cap = (int64_t)((kNoAllocScratchBytes - used) / sizeof(float)) -
+                             window_scratch_floats();
+    if (pend_cap < 0) {
+        char m[160];
+        snprintf(m, sizeof m, "grid of %lld nodes exceeds the %zu MiB scratch array",
+                 (long long)N, kNoAllocScratchBytes >> 20);
+        return fail(VLL_ERR_CAPACITY, m);
+    }
 #define NA_CUDA(call)                                                     \
     do {                                                                  \
         if ((call) != cudaSuccess) return fail(VLL_ERR_CUDA, #call);      \

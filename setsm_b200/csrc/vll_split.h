@@ -16,7 +16,8 @@ struct DevLevel;
 struct SplitBuffers {
     void *node_k = nullptr;        // int32  [N+1] slots per active node (0 = inactive)
     void *slot_off = nullptr;      // int64  [N+1] prefix sum of node_k (the slot total)
-    void *rho = nullptr;           // float  [pend_cap] FP32 slot values of queued nodes
+    void *rho = nullptr;           // float  [pend_cap] FP32 slot values of queued nodes, then
+                                   // the window kernel's per-warp slot scratch
     void *gsum = nullptr;          // double [N] GNCC sums (FP64)
     void *gcnt = nullptr;          // double [N]
     void *scan_tmp = nullptr;      // cub temporary storage

@@ -678,9 +678,9 @@ __host__ __device__ void thresholds_of(const TinArgs &a, const double sd[2], con
 // * exact, and exact <= s (1 + (m-1) u (1 + O(u))); 3 m u covers both.
 __host__ __device__ void sum_band(double s, int64_t m, double out[2]) {
     const double e = s * (3.0 * (double)m * 0x1p-53) * (1.0 + 0x1p-40);
-    out[0] = nextafter(s - e, -INFINITY);
+    out[0] = nextafter(s - e, -(double)INFINITY);
     if (out[0] < 0) out[0] = 0;
-    out[1] = nextafter(s + e, INFINITY);
+    out[1] = nextafter(s + e, (double)INFINITY);
 }
 
 // Slots of the per-call counters (unsigned long long): [0..1] counts, [2]

@@ -64,13 +64,30 @@ struct Acc2 {
     float2 sl, sr, sll, srr, slr;
 };
 
+// The target box lives in the block's shared memory at byte offsets from
+// `base`; `tq` is the offset of the window centre's texel, biased so that
+// the fixed-point bits of the round-to-nearest constant index it directly:
+// offset of texel (cx + dx, cy + dy) = tq + bits(M + dy) * row + bits(M + dx) * 16
+// (mod 2^32), M = 1.5 * 2^23.
+struct TgtBox {
+    const unsigned char *base;   // shared-memory window of the block
+    uint32_t tq;                 // biased offset (see above)
+    uint32_t row;                // row stride in bytes
+};
+
+__device__ __forceinline__ TgtBox tgt_box(const unsigned char *base, uint32_t centre_off,
+                                          uint32_t row) {
+    return TgtBox{base, centre_off - 0x4B400000u * (row + 16u), row};
+}
+
 struct WinCtx {
     float2 w00, w10, w01, w11;   // reference bilinear weights (same for all samples), broadcast
     float2 ncl;                  // -(reference centre sample) per plane
     float2 ntc;                  // -(target centre sample) per plane
     float2 cs;                   // target rotation (cos(-theta), sin(-theta))
     float2 nsc;                  // (-sin(-theta), cos(-theta))
-    int rbw, tbw;                // staged box row strides (texel pairs)
+    int rbw;                     // reference box row stride (texel pairs)
+    TgtBox tb;
 };
 
 // Reference-window sample from the staged pairs of rows y (a) and y+1 (b),
@@ -83,20 +100,21 @@ __device__ __forceinline__ float2 ref_sample(const WinCtx &x, const float4 &a, c
     return __ffma2_rn(x.w11, hi2(b), l);
 }
 
-// Target sample at box-relative position f (x, y): floor and fraction through
-// the 1.5*2^23 round-to-nearest constant, then bilinear on both planes.
-__device__ __forceinline__ float2 tgt_sample(const float4 *__restrict__ qt, int tbw, float2 f,
-                                             float2 init) {
+// Target sample at centre-relative position f (x, y): floor and fraction
+// through the 1.5*2^23 round-to-nearest constant, then bilinear on both
+// planes.  Target texels are staged as {I(x), M(x), I(x+1) - I(x),
+// M(x+1) - M(x)} (the differences of integers are exact, so each row's
+// interpolation rounds once, as I(x) + fx * (I(x+1) - I(x))).
+__device__ __forceinline__ float2 tgt_sample(const TgtBox &tb, float2 f, float2 init) {
     const float2 t = __fadd2_rn(__fadd2_rn(f, make_float2(-0.5f, -0.5f)), bc2(kMagic));
     const float2 fr = __fadd2_rn(f, __ffma2_rn(t, make_float2(-1.f, -1.f), bc2(kMagic)));
-    const int ix = __float_as_int(t.x) - 0x4B400000;
-    const int iy = __float_as_int(t.y) - 0x4B400000;
-    const float4 *p = qt + iy * tbw + ix;
-    const float4 ta = p[0];
-    const float4 tb = p[tbw];
+    const uint32_t a = (uint32_t)__float_as_int(t.y) * tb.row +
+                       ((uint32_t)__float_as_int(t.x) << 4) + tb.tq;
+    const float4 ta = *reinterpret_cast<const float4 *>(tb.base + a);
+    const float4 tv = *reinterpret_cast<const float4 *>(tb.base + a + tb.row);
     const float2 fx = bc2(fr.x), fy = bc2(fr.y);
-    const float2 top = __ffma2_rn(fx, sub2(hi2(ta), lo2(ta)), lo2(ta));
-    const float2 bot = __ffma2_rn(fx, sub2(hi2(tb), lo2(tb)), lo2(tb));
+    const float2 top = __ffma2_rn(fx, hi2(ta), lo2(ta));
+    const float2 bot = __ffma2_rn(fx, hi2(tv), lo2(tv));
     return __fadd2_rn(__ffma2_rn(fy, sub2(bot, top), top), init);
 }
 
@@ -111,8 +129,7 @@ __host__ __device__ constexpr int row_cmin(int H, int AR) {
 // columns unrolled, each accumulating into its compile-time ring.
 template <int H, int AR>
 __device__ __forceinline__ void win_row(const WinCtx &x, int row, const float4 *__restrict__ qr,
-                                        const float4 *__restrict__ qt, float2 tf,
-                                        Acc2 (&acc)[3]) {
+                                        float2 tf, Acc2 (&acc)[3]) {
     const float4 *q0 = qr + (row + H) * x.rbw;
     const float4 *q1 = q0 + x.rbw;
     const float2 b = __ffma2_rn(x.nsc, bc2((float)row), tf);
@@ -140,7 +157,7 @@ __device__ __forceinline__ void win_row(const WinCtx &x, int row, const float4 *
             l = ref_sample(x, make_float4(a0.z, a0.w, a1.x, a1.y),
                            make_float4(b0.z, b0.w, b1.x, b1.y), x.ncl);
         }
-        const float2 r = tgt_sample(qt, x.tbw, __ffma2_rn(x.cs, bc2((float)col), b), x.ntc);
+        const float2 r = tgt_sample(x.tb, __ffma2_rn(x.cs, bc2((float)col), b), x.ntc);
         Acc2 &u = acc[ring];
         u.sl = __fadd2_rn(u.sl, l);
         u.sr = __fadd2_rn(u.sr, r);
@@ -154,13 +171,12 @@ __device__ __forceinline__ void win_row(const WinCtx &x, int row, const float4 *
 // symmetric), so each pattern's unrolled code serves two rows.
 template <int H, int AR>
 __device__ __forceinline__ void win_rows(const WinCtx &x, const float4 *__restrict__ qr,
-                                         const float4 *__restrict__ qt, float2 tf,
-                                         Acc2 (&acc)[3]) {
+                                         float2 tf, Acc2 (&acc)[3]) {
     if constexpr (AR <= H) {
 #pragma unroll 1
         for (int sgn = (AR == 0 ? 1 : -1); sgn <= 1; sgn += 2)
-            win_row<H, AR>(x, sgn * AR, qr, qt, tf, acc);
-        win_rows<H, AR + 1>(x, qr, qt, tf, acc);
+            win_row<H, AR>(x, sgn * AR, qr, tf, acc);
+        win_rows<H, AR + 1>(x, qr, tf, acc);
     }
 }
 
@@ -179,14 +195,14 @@ __device__ __forceinline__ void add_to(Acc2 &w, const Acc2 &a) {
 
 // FP32 multi-window NCC of one slot (ComputeMultiNCC over the three nested
 // sub-windows, intensity and magnitude, SubFunctions.cpp:3328-3360) from the
-// staged texel pairs.  qr: top-left texel pair of the reference window;
-// qt: target texel pair at the window centre; (rfx, rfy), (tfx, tfy): the
-// fractional positions.  Sums are shifted by each window's centre sample.
+// staged texels.  qr: top-left texel pair of the reference window; tb: the
+// target box addressed from the window centre's texel; (rfx, rfy), (tfx,
+// tfy): the fractional positions.  Sums are shifted by each window's centre
+// sample.
 template <int H>
 __device__ __forceinline__ void window_fp32(const float4 *__restrict__ qr, int rbw, float rfx,
-                                            float rfy, const float4 *__restrict__ qt, int tbw,
-                                            float tfx, float tfy, float c, float s,
-                                            float &incc_avg, bool &unsure) {
+                                            float rfy, const TgtBox &tb, float tfx, float tfy,
+                                            float c, float s, float &incc_avg, bool &unsure) {
     Acc2 acc[3];
     const float2 z = make_float2(0.f, 0.f);
 #pragma unroll
@@ -199,15 +215,15 @@ __device__ __forceinline__ void window_fp32(const float4 *__restrict__ qr, int r
     x.cs = make_float2(c, s);
     x.nsc = make_float2(-s, c);
     x.rbw = rbw;
-    x.tbw = tbw;
+    x.tb = tb;
     const float2 tf = make_float2(tfx, tfy);
     {
         const float2 cl = ref_sample(x, qr[H * rbw + H], qr[(H + 1) * rbw + H], z);
-        const float2 ct = tgt_sample(qt, tbw, tf, z);
+        const float2 ct = tgt_sample(tb, tf, z);
         x.ncl = make_float2(-cl.x, -cl.y);
         x.ntc = make_float2(-ct.x, -ct.y);
     }
-    win_rows<H, 0>(x, qr, qt, tf, acc);
+    win_rows<H, 0>(x, qr, tf, acc);
     // nested windows: 2 = ring 2; 1 = rings 1+2; 0 = all rings
     constexpr int n2 = ring_count(H, 2);
     constexpr int n1 = n2 + ring_count(H, 1);
@@ -244,12 +260,50 @@ __device__ __forceinline__ float2 texel_pair(uint32_t wi, uint32_t wm, uint32_t 
 // Non-zero when some 16-bit half of w is zero.
 __device__ __forceinline__ uint32_t zero_half(uint32_t w) { return (w - 0x00010001u) & ~w; }
 
-// Vectorised staging of the box: each lane converts one 8-texel,
+// Staged texel of the box at x from the converted texels f[t] (x) and f[t+1]
+// (x + 1): reference boxes hold pairs {I(x), M(x), I(x+1), M(x+1)}, target
+// boxes (kDiff) {I(x), M(x), I(x+1) - I(x), M(x+1) - M(x)}.
+template <bool kDiff>
+__device__ __forceinline__ float4 box_texel(float2 a, float2 b) {
+    if constexpr (kDiff) {
+        const float2 d = sub2(b, a);
+        return make_float4(a.x, a.y, d.x, d.y);
+    } else {
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
+// Converts the nine texels of one 8-texel chunk (words vi/vm, ninth texel
+// i8/m8) and stores the box texels of [xc, xc + 8) that lie in [x0, x1].
+template <bool kDiff>
+__device__ __forceinline__ void store_chunk(float4 *__restrict__ drow, const uint4 &vi,
+                                            const uint4 &vm, uint32_t i8, uint32_t m8, int xc,
+                                            int x0, int x1, float2 ns) {
+    float2 f[9];
+    f[0] = texel_pair(vi.x, vm.x, 0x7610, ns);
+    f[1] = texel_pair(vi.x, vm.x, 0x7632, ns);
+    f[2] = texel_pair(vi.y, vm.y, 0x7610, ns);
+    f[3] = texel_pair(vi.y, vm.y, 0x7632, ns);
+    f[4] = texel_pair(vi.z, vm.z, 0x7610, ns);
+    f[5] = texel_pair(vi.z, vm.z, 0x7632, ns);
+    f[6] = texel_pair(vi.w, vm.w, 0x7610, ns);
+    f[7] = texel_pair(vi.w, vm.w, 0x7632, ns);
+    f[8] = texel_pair(i8, m8, 0x7610, ns);
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int x = xc + t;
+        if (x >= x0 && x <= x1) drow[x - x0] = box_texel<kDiff>(f[t], f[t + 1]);
+    }
+}
+
+// Vectorised staging of the box by loads: each lane converts one 8-texel,
 // 16-byte-aligned chunk of a box row per plane (two 128-bit loads) into up to
-// eight texel pairs.  Requires the image rows to start on 16-byte boundaries
+// eight box texels.  Requires the image rows to start on 16-byte boundaries
 // (width multiple of 8 and 16-byte aligned planes); `dst` rows have stride
-// `ds` pairs.  Returns (warp-uniform) whether an intensity texel of the loaded
-// chunks is zero (a superset of the box: the caller then takes the exact path).
+// `ds` texels.  Returns (warp-uniform) whether an intensity texel of the
+// loaded chunks is zero (a superset of the box: the caller then takes the
+// exact path).
+template <bool kDiff>
 __device__ __forceinline__ bool stage_box_vec(float4 *__restrict__ dst, int ds,
                                               const uint16_t *__restrict__ I,
                                               const uint16_t *__restrict__ M, uint32_t W, int x0,
@@ -258,7 +312,7 @@ __device__ __forceinline__ bool stage_box_vec(float4 *__restrict__ dst, int ds,
     bool z8 = false;
     const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
     const int xa = x0 & ~7;
-    const int x1 = x0 + bw - 1;                 // last pair's left texel
+    const int x1 = x0 + bw - 1;                 // last texel's left texel
     const int nch = ((x1 + 1) - xa) / 8 + 1;    // chunks covering [xa, x1 + 1]
     const int n = nch * bh;
     for (int i = lane; i < n; i += 32) {
@@ -268,36 +322,43 @@ __device__ __forceinline__ bool stage_box_vec(float4 *__restrict__ dst, int ds,
         const int64_t row = (int64_t)(y0 + by) * W;
         const uint4 vi = __ldg(reinterpret_cast<const uint4 *>(I + row + xc));
         const uint4 vm = __ldg(reinterpret_cast<const uint4 *>(M + row + xc));
-        const bool need9 = xc + 7 <= x1;        // the 8th pair needs texel xc + 8
+        const bool need9 = xc + 7 <= x1;        // the 8th texel needs texel xc + 8
         const uint32_t i8 = need9 ? __ldg(I + row + xc + 8) : 1u;
         const uint32_t m8 = need9 ? __ldg(M + row + xc + 8) : 0u;
         zacc |= zero_half(vi.x) | zero_half(vi.y) | zero_half(vi.z) | zero_half(vi.w);
         z8 |= i8 == 0;
-        float2 f[9];
-        f[0] = texel_pair(vi.x, vm.x, 0x7610, ns);
-        f[1] = texel_pair(vi.x, vm.x, 0x7632, ns);
-        f[2] = texel_pair(vi.y, vm.y, 0x7610, ns);
-        f[3] = texel_pair(vi.y, vm.y, 0x7632, ns);
-        f[4] = texel_pair(vi.z, vm.z, 0x7610, ns);
-        f[5] = texel_pair(vi.z, vm.z, 0x7632, ns);
-        f[6] = texel_pair(vi.w, vm.w, 0x7610, ns);
-        f[7] = texel_pair(vi.w, vm.w, 0x7632, ns);
-        f[8] = texel_pair(i8, m8, 0x7610, ns);
-        float4 *drow = dst + by * ds;
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-            const int x = xc + t;
-            if (x >= x0 && x <= x1) drow[x - x0] = make_float4(f[t].x, f[t].y, f[t + 1].x, f[t + 1].y);
-        }
+        store_chunk<kDiff>(dst + by * ds, vi, vm, i8, m8, xc, x0, x1, ns);
     }
     return __any_sync(0xffffffffu, (zacc & 0x80008000u) != 0 || z8);
 }
 
-// ---- footprint staging by the bulk-copy (TMA) engine ------------------------
-// The rows of a box are copied raw (uint16) from global to shared memory by
-// cp.async.bulk, one copy per row and plane, completing on the warp's
-// mbarrier; the warp then converts them to texel pairs with 128-bit shared
-// loads (stage_from_raw).
+// Scalar staging of a box whose destination rows have stride `ds` texels
+// (used when image rows are not 16-byte aligned).
+template <bool kDiff>
+__device__ __forceinline__ bool stage_box_strided(float4 *__restrict__ dst, int ds,
+                                                  const uint16_t *__restrict__ I,
+                                                  const uint16_t *__restrict__ M, uint32_t W, int x0,
+                                                  int y0, int bw, int bh, float sI, float sM, int lane) {
+    bool zero = false;
+    const int n = bw * bh;
+    for (int i = lane; i < n; i += 32) {
+        const int by = i / bw;
+        const int bx = i - by * bw;
+        const int64_t p = (int64_t)(y0 + by) * W + (x0 + bx);
+        const uint16_t a = __ldg(I + p), b = __ldg(I + p + 1);
+        const uint16_t cm = __ldg(M + p), d = __ldg(M + p + 1);
+        zero |= (a == 0) | (b == 0);
+        dst[by * ds + bx] = box_texel<kDiff>(make_float2((float)a - sI, (float)cm - sM),
+                                             make_float2((float)b - sI, (float)d - sM));
+    }
+    return __any_sync(0xffffffffu, zero);
+}
+
+// ---- footprint staging by the tensor-memory-access (TMA) engine --------------
+// Each group's footprints are copied raw (uint16) from global to shared
+// memory as four 2-D tiles (intensity and magnitude of both images) that
+// complete on the warp's mbarrier; the warp then converts them to box texels
+// with 128-bit shared loads (convert_tile).
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -315,16 +376,6 @@ __device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, uint32_t bytes
         "{\n\t.reg .b64 st;\n\t"
         "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_addr(bar)),
         "r"(bytes)
-        : "memory");
-}
-
-// Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned)
-// from global to this CTA's shared memory, completing on `bar`.
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
 
@@ -347,67 +398,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long l
 }
 
 // Orders this thread's earlier generic shared-memory accesses before later
-// asynchronous-proxy (bulk copy) writes to the same memory.
+// asynchronous-proxy (TMA) writes to the same memory.
 __device__ __forceinline__ void fence_async_shared() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// Texel pairs of box [x0, x0+bw) x rows [0, bh) from raw rows staged in
-// shared memory: rawI / rawM hold, per box row (stride `nb` bytes), the
-// uint16 texels from xa = x0 rounded down to 8 on.  Each lane converts
-// 8-texel chunks read with 128-bit loads; returns (warp-uniform) whether an
-// intensity texel of the box's pairs ([x0, x0 + bw]) is zero.
-__device__ __forceinline__ bool stage_from_raw(float4 *__restrict__ dst, int ds,
-                                               const unsigned char *__restrict__ rawI,
-                                               const unsigned char *__restrict__ rawM, int nb,
-                                               int xa, int x0, int bw, int bh, float sI, float sM,
-                                               int lane) {
-    bool zero = false;
-    const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
-    const int x1 = x0 + bw - 1;                 // last pair's left texel
-    const int nch = (x1 + 1 - xa) / 8 + 1;      // chunks covering [xa, x1 + 1]
-    const int n = nch * bh;
-    for (int i = lane; i < n; i += 32) {
-        const int by = i / nch;
-        const int c = i - by * nch;
-        const int xc = xa + 8 * c;
-        const int ro = by * nb + 16 * c;
-        const uint4 vi = *reinterpret_cast<const uint4 *>(rawI + ro);
-        const uint4 vm = *reinterpret_cast<const uint4 *>(rawM + ro);
-        const bool need9 = xc + 7 <= x1;        // the 8th pair needs texel xc + 8
-        const uint32_t i8 = need9 ? *reinterpret_cast<const uint16_t *>(rawI + ro + 16) : 1u;
-        const uint32_t m8 = need9 ? *reinterpret_cast<const uint16_t *>(rawM + ro + 16) : 0u;
-        const uint32_t w[4] = {vi.x, vi.y, vi.z, vi.w};
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-            const int x = xc + t;
-            const uint32_t tex = (w[t >> 1] >> (16 * (t & 1))) & 0xFFFFu;
-            if (x >= x0 && x <= x1 + 1 && tex == 0) zero = true;
-        }
-        zero |= i8 == 0;
-        float2 f[9];
-        f[0] = texel_pair(vi.x, vm.x, 0x7610, ns);
-        f[1] = texel_pair(vi.x, vm.x, 0x7632, ns);
-        f[2] = texel_pair(vi.y, vm.y, 0x7610, ns);
-        f[3] = texel_pair(vi.y, vm.y, 0x7632, ns);
-        f[4] = texel_pair(vi.z, vm.z, 0x7610, ns);
-        f[5] = texel_pair(vi.z, vm.z, 0x7632, ns);
-        f[6] = texel_pair(vi.w, vm.w, 0x7610, ns);
-        f[7] = texel_pair(vi.w, vm.w, 0x7632, ns);
-        f[8] = texel_pair(i8, m8, 0x7610, ns);
-        float4 *drow = dst + by * ds;
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-            const int x = xc + t;
-            if (x >= x0 && x <= x1) drow[x - x0] = make_float4(f[t].x, f[t].y, f[t + 1].x, f[t + 1].y);
-        }
-    }
-    return __any_sync(0xffffffffu, zero);
-}
-
 // 2-D tile of a tensor map (TMA, no multicast) into this CTA's shared memory
 // at `dst` (128-byte aligned): x (innermost, a multiple of 16 bytes) and y
-// are the tile's first texel; completes `bytes` of the tile on `bar`.
+// are the tile's first texel; completes the tile's bytes on `bar`.
 __device__ __forceinline__ void tma_tile_2d(void *dst, const void *tmap, int x, int y,
                                             uint64_t *bar) {
     asm volatile(
@@ -423,63 +421,57 @@ __device__ __forceinline__ void tmap_acquire(const void *tmap) {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
 }
 
-// Scalar staging of a box whose destination rows have stride `ds` pairs
-// (used when image rows are not 16-byte aligned).
-__device__ __forceinline__ bool stage_box_strided(float4 *__restrict__ dst, int ds,
-                                                  const uint16_t *__restrict__ I,
-                                                  const uint16_t *__restrict__ M, uint32_t W, int x0,
-                                                  int y0, int bw, int bh, float sI, float sM, int lane) {
-    bool zero = false;
-    const int n = bw * bh;
+// Box texels of [x0, x0 + bw) x rows [0, bh) from the raw tiles in shared
+// memory: rawI / rawM hold, per box row (stride `nb` bytes), the uint16
+// texels from xa = x0 rounded down to 8 on.  Each lane converts 8-texel
+// chunks read with 128-bit loads.  Zero intensity texels among the texels
+// the box reads ([x0, x0 + bw] of each row) are listed in `zl` as
+// tag | row << 16 | (x - x0), counted in *zn (entries beyond `cap` are
+// counted, not stored).
+template <bool kDiff>
+__device__ __forceinline__ void convert_tile(float4 *__restrict__ dst, int ds,
+                                             const unsigned char *__restrict__ rawI,
+                                             const unsigned char *__restrict__ rawM, int nb,
+                                             int xa, int x0, int bw, int bh, float sI, float sM,
+                                             uint32_t *zl, int *zn, int cap, uint32_t tag,
+                                             int lane) {
+    const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
+    const int x1 = x0 + bw - 1;                 // last box texel
+    const int nch = (x1 + 1 - xa) / 8 + 1;      // chunks covering [xa, x1 + 1]
+    const int n = nch * bh;
+    // chunk i = (row by, column c): the lane's first chunk, then steps of 32
+    int by = lane / nch, c = lane - by * nch;
+    const int dby = 32 / nch, dc = 32 - dby * nch;
     for (int i = lane; i < n; i += 32) {
-        const int by = i / bw;
-        const int bx = i - by * bw;
-        const int64_t p = (int64_t)(y0 + by) * W + (x0 + bx);
-        const uint16_t a = __ldg(I + p), b = __ldg(I + p + 1);
-        const uint16_t cm = __ldg(M + p), d = __ldg(M + p + 1);
-        zero |= (a == 0) | (b == 0);
-        dst[by * ds + bx] = make_float4((float)a - sI, (float)cm - sM, (float)b - sI, (float)d - sM);
-    }
-    return __any_sync(0xffffffffu, zero);
-}
-
-// Stages the texel pairs of box [x0, x0+bw) x [y0, y0+bh) of one image into
-// shared memory as float4 {I(x)-sI, M(x)-sM, I(x+1)-sI, M(x+1)-sM}; returns
-// true (warp-uniform) when some intensity texel in the box is zero.
-__device__ __forceinline__ bool stage_box(float4 *__restrict__ dst, const uint16_t *__restrict__ I,
-                                          const uint16_t *__restrict__ M, uint32_t W, int x0, int y0,
-                                          int bw, int bh, float sI, float sM, int lane) {
-    bool zero = false;
-    const int n = bw * bh;
-    // four texel pairs per lane in flight before any is converted, so the
-    // global-load latency is paid once per batch instead of once per pair
-    constexpr int U = 4;
-    for (int base = lane; base < n; base += 32 * U) {
-        uint16_t a[U], b[U], cm[U], d[U];
+        const int xc = xa + 8 * c;
+        const int ro = by * nb + 16 * c;
+        const uint4 vi = *reinterpret_cast<const uint4 *>(rawI + ro);
+        const uint4 vm = *reinterpret_cast<const uint4 *>(rawM + ro);
+        const bool need9 = xc + 7 <= x1;        // the 8th texel needs texel xc + 8
+        const uint32_t i8 = need9 ? *reinterpret_cast<const uint16_t *>(rawI + ro + 16) : 1u;
+        const uint32_t m8 = need9 ? *reinterpret_cast<const uint16_t *>(rawM + ro + 16) : 0u;
+        const uint32_t zw = zero_half(vi.x) | zero_half(vi.y) | zero_half(vi.z) | zero_half(vi.w);
+        if ((zw & 0x80008000u) != 0 || i8 == 0) {
+            // rare: list the zero texels of the range the box reads
+            const uint32_t w[4] = {vi.x, vi.y, vi.z, vi.w};
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int i = base + 32 * u;
-            if (i < n) {
-                const int by = i / bw;
-                const int bx = i - by * bw;
-                const int64_t p = (int64_t)(y0 + by) * W + (x0 + bx);
-                a[u] = __ldg(I + p);
-                b[u] = __ldg(I + p + 1);
-                cm[u] = __ldg(M + p);
-                d[u] = __ldg(M + p + 1);
+            for (int t = 0; t < 9; ++t) {
+                const int x = xc + t;
+                const uint32_t tex = t < 8 ? (w[t >> 1] >> (16 * (t & 1))) & 0xFFFFu : i8;
+                if (x >= x0 && x <= x1 + 1 && tex == 0) {
+                    const int k = atomicAdd(zn, 1);
+                    if (k < cap) zl[k] = tag | ((uint32_t)by << 16) | (uint32_t)(x - x0);
+                }
             }
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int i = base + 32 * u;
-            if (i < n) {
-                zero |= (a[u] == 0) | (b[u] == 0);
-                dst[i] = make_float4((float)a[u] - sI, (float)cm[u] - sM, (float)b[u] - sI,
-                                     (float)d[u] - sM);
-            }
+        store_chunk<kDiff>(dst + by * ds, vi, vm, i8, m8, xc, x0, x1, ns);
+        by += dby;
+        c += dc;
+        if (c >= nch) {
+            c -= nch;
+            ++by;
         }
     }
-    return __any_sync(0xffffffffu, zero);
 }
 
 }  // namespace vll
