@@ -393,7 +393,8 @@ void vll_plan_destroy(vll_plan *plan);
 /* ---- launch tuning (chosen by setsm_b200/autotune.py) -------------------- */
 typedef struct vll_tuning {
     int32_t blocks_per_sm;   /* window kernel CTAs per SM; 0 = occupancy maximum   */
-    int32_t grab;            /* work items a warp takes per queue access (1..64)  */
+    int32_t grab;            /* nodes a warp takes per queue access (1..64; 0:
+                                default 8; at most 32 are used)                  */
     float box_margin;        /* shared-memory footprint budget over the estimate  */
     int32_t _pad;
 } vll_tuning;

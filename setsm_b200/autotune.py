@@ -6,8 +6,8 @@ sizes and the epipolar sweep of the scenes.  The tunable parameters
 (``vll_tuning``, include/setsm_vll.h) are:
 
 * ``blocks_per_sm`` -- CTAs of 4 warps per SM (0 = the occupancy maximum);
-* ``grab``          -- (node, 32-slot) work items a warp takes per queue access,
-                       i.e. the chunk of the queue a warp owns at a time;
+* ``grab``          -- nodes a warp takes per queue access (at most 32 are
+                       used), i.e. the chunk of the queue a warp owns at a time;
 * ``box_margin``    -- the per-warp shared-memory budget for the staged image
                        footprints over the swept-box estimate (larger boxes keep
                        rare wide footprints on the FP32 path, smaller ones raise
@@ -25,10 +25,10 @@ import json
 import os
 import time
 
-DEFAULT = {"blocks_per_sm": 0, "grab": 1, "box_margin": 1.1}
+DEFAULT = {"blocks_per_sm": 0, "grab": 8, "box_margin": 1.1}
 
 CANDIDATES = [dict(blocks_per_sm=b, grab=g, box_margin=m)
-              for b, g, m in itertools.product((0, 2), (1, 2, 4, 8), (1.0, 1.1, 1.25))]
+              for b, g, m in itertools.product((0, 2), (1, 4, 8, 16, 32), (1.0, 1.1, 1.25))]
 
 
 def cache_path() -> str:

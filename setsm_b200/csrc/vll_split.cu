@@ -511,6 +511,21 @@ struct NodeCtx {
     int pre_dir, pre_k, have;         // direction and index, and whether there is one
 };
 
+// The constants of the launch's first level, loaded once per block: node
+// set-ups on that level (every node of a single-level call) read them from
+// shared memory and fetch only the node's own records from global memory.
+struct LevelConst {
+    double rpc[2][90];                // [image] RPC00B block (offsets, scales, 4 x 20 terms)
+    double geo[2][8];                 // as NodeCtx::geo
+    double inv_s, hstep, bin_angle, alpha, beta;
+    const uint16_t *img[2], *mag[2];
+    const uint8_t *ori[2];
+    uint32_t w[2], h[2];
+    int tma_w[2], tma_h[2];
+    int H, is_ra, cmr, check_ortho, voxels;
+    uint32_t flags;                   // kNfOri | kNfVec | kNfTma | kNfDbg
+};
+
 // Per-warp shared state of the window kernel.
 struct WinShared {
     NodeCtx node[2];
@@ -519,8 +534,59 @@ struct WinShared {
     uint64_t mbar;                    // completion of the group's tile copies
 };
 
-__host__ __device__ constexpr size_t win_boxes_offset() {
+__host__ __device__ constexpr size_t win_level_offset() {
     return (sizeof(WinShared) * kWinWarps + 15) & ~(size_t)15;
+}
+
+__host__ __device__ constexpr size_t win_boxes_offset() {
+    return (win_level_offset() + sizeof(LevelConst) + 15) & ~(size_t)15;
+}
+
+// Fills the block's LevelConst from level P (every thread of the block takes
+// part; the caller synchronises the block afterwards).
+__device__ void level_const_load(LevelConst &C, const DevLevel &P) {
+    const int t = threadIdx.x, nt = blockDim.x;
+    for (int i = t; i < 180; i += nt) {
+        const int im = i / 90;
+        C.rpc[im][i - im * 90] = P.im[im == 0 ? P.ref : 1].rpc[i - im * 90];
+    }
+    if (t < 2) {
+        const DevImage &I = P.im[t == 0 ? P.ref : 1];
+        double *g = C.geo[t];
+        g[0] = I.adj[0];
+        g[1] = I.adj[1];
+        g[2] = I.rpc[0];
+        g[3] = I.rpc[1];
+        g[4] = I.rpc[5];
+        g[5] = I.rpc[6];
+        g[6] = I.sx;
+        g[7] = I.sy;
+        C.img[t] = I.img;
+        C.mag[t] = I.mag;
+        C.ori[t] = I.ori;
+        C.w[t] = I.w;
+        C.h[t] = I.h;
+        C.tma_w[t] = P.tma_w[t];
+        C.tma_h[t] = P.tma_h[t];
+    } else if (t == 2) {
+        const DevImage &ri = P.im[P.ref], &tI = P.im[1];
+        C.inv_s = 1.0 / (double)(1 << P.L);
+        C.hstep = P.height_step;
+        C.bin_angle = P.bin_angle;
+        C.alpha = P.alpha;
+        C.beta = P.beta;
+        C.H = P.H;
+        C.is_ra = P.is_ra;
+        C.cmr = P.cmr;
+        C.check_ortho = P.check_ortho;
+        C.voxels = P.vox && !P.cmr && !P.is_ra;
+        const bool vec_ok = (ri.w % 8 == 0) && (tI.w % 8 == 0) &&
+                            ((reinterpret_cast<uintptr_t>(ri.img) | reinterpret_cast<uintptr_t>(ri.mag) |
+                              reinterpret_cast<uintptr_t>(tI.img) |
+                              reinterpret_cast<uintptr_t>(tI.mag)) & 15) == 0;
+        C.flags = ((!P.is_ra && P.L >= 3) ? kNfOri : 0u) | (vec_ok ? kNfVec : 0u) |
+                  (P.tma_w[0] > 0 ? kNfTma : 0u) | (P.dbg_rho ? kNfDbg : 0u);
+    }
 }
 
 // the TMA tiles follow the boxes, 128-byte aligned (warp_raw is a multiple of 128)
@@ -547,9 +613,71 @@ __device__ __forceinline__ void window_any(int H, const float4 *qr, int rbw, flo
 // every lane takes part, the context is complete after the final __syncwarp.
 __device__ __noinline__ void node_setup(NodeCtx &N, const LevelSet &LS, int lvl, int64_t gn, int K,
                                         const double *__restrict__ gsum,
-                                        const double *__restrict__ gcnt, int lane) {
+                                        const double *__restrict__ gcnt,
+                                        const LevelConst *lc, int lane) {
     const DevLevel &P = LS.lv[lvl];
     const int64_t pt = gn - __ldg(LS.base + lvl);
+    if (lc) {
+        // the level's constants from the block's copy; the node's own
+        // records from global memory, one load per lane
+        if (lane < 8) {
+            const int im = lane >> 2, j = lane & 3;
+            const double *rpc = lc->rpc[im];
+            node_horner_poly(rpc, P.grid_wgs[2 * pt], P.grid_wgs[2 * pt + 1], j, N.horner[im][j]);
+            if (j == 0) {
+                N.hnorm[im][0] = rpc[4];
+                N.hnorm[im][1] = 1.0 / rpc[9];
+            }
+        } else if (lane < 26) {
+            const int i = lane - 8;   // 16 geo values, then 2 lanes of pointers
+            if (i < 16) {
+                N.geo[i >> 3][i & 7] = lc->geo[i >> 3][i & 7];
+            } else {
+                const int im = i - 16;
+                N.img[im] = lc->img[im];
+                N.mag[im] = lc->mag[im];
+                N.ori[im] = lc->ori[im];
+                N.w[im] = lc->w[im];
+                N.h[im] = lc->h[im];
+                N.tma_w[im] = lc->tma_w[im];
+                N.tma_h[im] = lc->tma_h[im];
+            }
+        } else if (lane == 26) {
+            const vll_ugrid g = P.gp3[pt];
+            const vll_nccresult R = P.ncc[pt];
+            const double cnt_g = gcnt ? gcnt[gn] : 0.0;
+            const double sum_g = gcnt ? gsum[gn] : 0.0;
+            N.P = &P;
+            N.gn = gn;
+            N.pt = pt;
+            N.K = K;
+            N.H = lc->H;
+            N.start_H = g.minHeight;
+            N.end_H = g.maxHeight;
+            N.R = R;
+            N.hbase = (double)((lc->is_ra || lc->cmr) ? g.minHeight : R.minHeight);
+            N.hstep = lc->hstep;
+            N.inv_s = lc->inv_s;
+            N.bin_angle = lc->bin_angle;
+            N.alpha = lc->alpha;
+            const bool gncc = lc->check_ortho && cnt_g > 0;
+            N.gterm = gncc ? (sum_g / cnt_g) * lc->beta : 0.0;
+            N.vrow = lc->voxels ? P.vox + P.vox_off[pt] : nullptr;
+            N.flags = lc->flags | (lc->cmr ? kNfCmr : 0u) | (lc->voxels ? kNfVox : 0u) |
+                      (R.check_height_change ? kNfChc : 0u) | (gncc ? kNfGncc : 0u);
+            N.pre_v = -1.0f;
+            N.pre_dir = 0;
+            N.pre_k = -1;
+            N.have = 0;
+        } else if (lane == 27 && (lc->flags & kNfTma)) {
+            tmap_acquire(P.tmap[0][0]);
+            tmap_acquire(P.tmap[0][1]);
+            tmap_acquire(P.tmap[1][0]);
+            tmap_acquire(P.tmap[1][1]);
+        }
+        __syncwarp();
+        return;
+    }
     if (lane < 8) {
         // per-node RPC cubics: lanes 0..7 = (image, polynomial)
         const int im = lane >> 2, j = lane & 3;
@@ -698,13 +826,15 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     // the FP32 values of the warp's current node (read back only by the lane
     // that wrote them, when the node is queued for the exact pass)
     float *wv = warp_vals + ((size_t)blockIdx.x * kWinWarps + warp) * kSlotCap;
+    LevelConst &LC = *reinterpret_cast<LevelConst *>(smem_raw + win_level_offset());
+    level_const_load(LC, LS.lv[0]);
     if (lane == 0) mbar_init(&W.mbar);
-    __syncwarp();
+    __syncthreads();
     uint32_t phase = 0;   // parity of the mbarrier phase the next copies complete
     unsigned long long evals = 0;
     // node queue: batches of `grab` nodes
     unsigned long long qbase = 0;
-    int qi = grab;
+    int qi = grab, qk = 0;
     bool qdone = false;
     // the last fetched group: its node's context, first slot and the node's slot count
     int pb = 1, pk0 = 0, pK = 0;
@@ -758,12 +888,19 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 const float sM = (float)*reinterpret_cast<const uint16_t *>(rM + rc);
                 const float tsI = (float)*reinterpret_cast<const uint16_t *>(tIr + tc);
                 const float tsM = (float)*reinterpret_cast<const uint16_t *>(tMr + tc);
-                convert_tile<false>(boxes, rbw, rI, rM, rnb, rxa, nrx0, nrw, rbh, sI, sM, W.zl,
-                                    &W.zn, kZeroCap, 0u, lane);
-                convert_tile<true>(tbox, tbw, tIr, tMr, tnb, txa, ntx0, ntw, tbh, tsI, tsM, W.zl,
-                                   &W.zn, kZeroCap, 0x80000000u, lane);
-                // the tiles are rewritten by the next group's copies
-                fence_async_shared();
+                // reference box (pairs), then target box (value + difference)
+#pragma unroll 1
+                for (int im = 0; im < 2; ++im) {
+                    if (im == 0)
+                        convert_tile(boxes, rbw, rI, rM, rnb, rxa, nrx0, nrw, rbh, sI, sM, 0.f,
+                                     W.zl, &W.zn, kZeroCap, 0u, lane);
+                    else
+                        convert_tile(tbox, tbw, tIr, tMr, tnb, txa, ntx0, ntw, tbh, tsI, tsM, -1.f,
+                                     W.zl, &W.zn, kZeroCap, 0x80000000u, lane);
+                }
+                // the tiles are rewritten by the next group's copies: every
+                // value read from them has been stored into the boxes, so the
+                // reads are complete once the warp has synchronised
                 __syncwarp();
             } else {
                 float sI = 0.f, sM = 0.f, tsI = 0.f, tsM = 0.f;
@@ -807,17 +944,21 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             pK = 0;
             while (!qdone) {
                 if (qi >= grab) {
+                    // a batch of `grab` nodes and their slot counts (lane i: node i)
                     unsigned long long b = 0;
                     if (lane == 0) b = atomicAdd(&ctl[0], (unsigned long long)grab);
                     qbase = __shfl_sync(0xffffffffu, b, 0);
+                    qk = (lane < grab && (int64_t)qbase + lane < LS.total)
+                             ? node_k[(int64_t)qbase + lane] : 0;
                     qi = 0;
                 }
-                const int64_t gn = (int64_t)qbase + qi++;
+                const int64_t gn = (int64_t)qbase + qi;
+                const int K = __shfl_sync(0xffffffffu, qk, qi);
+                ++qi;
                 if (gn >= LS.total) {
                     qdone = true;
                     break;
                 }
-                const int K = node_k[gn];
                 if (K == 0) continue;
                 const int lvl = level_of(LS, gn);
                 if (LS.lv[lvl].combined_incc || K > kSlotCap) {
@@ -834,7 +975,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     continue;
                 }
                 pb ^= 1;
-                node_setup(W.node[pb], LS, lvl, gn, K, gsum, gcnt, lane);
+                node_setup(W.node[pb], LS, lvl, gn, K, gsum, gcnt, lvl == 0 ? &LC : nullptr, lane);
                 pk0 = 0;
                 pK = K;
                 have_next = true;
@@ -853,8 +994,14 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 const float hgt = (float)__dadd_rn(N.hbase, __dmul_rn((double)k, N.hstep));
                 if (hgt >= (float)N.start_H && hgt <= (float)N.end_H) {
                     bool edge = false;
-                    rp = node_coord(N, 0, (double)hgt, edge);
-                    tp = node_coord(N, 1, (double)hgt, edge);
+#pragma unroll 1
+                    for (int im = 0; im < 2; ++im) {
+                        const double2 q = node_coord(N, im, (double)hgt, edge);
+                        if (im == 0)
+                            rp = q;
+                        else
+                            tp = q;
+                    }
                     if (edge) slot_coords_exact(N, (double)hgt, rp, tp);
                     if (in_image(rp, N.w[0], N.h[0]) && in_image(tp, N.w[1], N.h[1])) {
                         const int od = (int)N.ori[0][(int64_t)(int)rp.y * N.w[0] + (int)rp.x] -
@@ -1037,6 +1184,10 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                         is_peak = pv != -1.0f && dp > 0 && td < 0;
                     }
                 }
+                // each peak's rounded value and height (its lane), then the
+                // ordered top-two fold of this group's peaks (lane 0)
+                int q_l = 0;
+                float ph_l = 0.f;
                 if (is_peak) {
                     if (near_round((double)pv) && pv > amb_peak) amb_peak = pv;
                     if (pv > b1) {
@@ -1045,20 +1196,19 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     } else if (pv > b2) {
                         b2 = pv;
                     }
+                    const int p_slot = p_in >= 0 ? ck0 + p_in : C.pre_k;
+                    q_l = q_result((double)pv);
+                    ph_l = (float)__dadd_rn(C.hbase, __dmul_rn((double)p_slot, C.hstep));
                 }
-                // the ordered top-two fold of this group's peaks (lane 0)
                 uint32_t pm = __ballot_sync(0xffffffffu, is_peak);
-                const int p_slot = p_in >= 0 ? ck0 + p_in : C.pre_k;
                 while (pm) {
                     const int b = __ffs(pm) - 1;
                     pm &= pm - 1;
-                    const float val = __shfl_sync(0xffffffffu, pv, b);
-                    const int ps = __shfl_sync(0xffffffffu, p_slot, b);
+                    const int16_t qpre = (int16_t)__shfl_sync(0xffffffffu, q_l, b);
+                    const float ph = __shfl_sync(0xffffffffu, ph_l, b);
                     if (lane == 0) {
                         vll_nccresult &R = C.R;
-                        const float ph = (float)__dadd_rn(C.hbase, __dmul_rn((double)ps, C.hstep));
                         if (R.result4 < 10) R.result4 += 1;
-                        const int16_t qpre = q_result((double)val);
                         if (R.result0 < qpre) {
                             const double t1 = dq_result(R.result0);
                             R.result0 = qpre;
@@ -1612,7 +1762,8 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel, kWinWarps * 32, smem);
     if (tu.blocks_per_sm > 0 && tu.blocks_per_sm < per_sm) per_sm = tu.blocks_per_sm;
     per_sm = std::max(1, std::min(per_sm, kWinMaxBlocksPerSm));
-    const int grab = tu.grab > 0 ? std::min(tu.grab, 64) : 1;
+    // nodes per queue access (their slot counts are read one per lane)
+    const int grab = tu.grab > 0 ? std::min(tu.grab, 32) : 1;
     // the warps' slot scratch follows the pending buffer's pend_cap values
     // (window_scratch_floats sizes it for the largest grid)
     float *warp_vals = pend_vals + pend_cap;

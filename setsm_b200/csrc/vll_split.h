@@ -35,7 +35,7 @@ struct SplitBuffers {
 // Launch parameters of the window kernel that the autotuner chooses.
 struct SplitTuning {
     int blocks_per_sm = 0;      // CTAs per SM (0: the occupancy maximum)
-    int grab = 1;               // nodes taken per queue access
+    int grab = 8;               // nodes taken per queue access (at most 32)
     float box_margin = 1.1f;    // footprint budget over the swept-box estimate
 };
 

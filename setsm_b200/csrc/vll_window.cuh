@@ -423,52 +423,56 @@ __device__ __forceinline__ void tmap_acquire(const void *tmap) {
 
 // Box texels of [x0, x0 + bw) x rows [0, bh) from the raw tiles in shared
 // memory: rawI / rawM hold, per box row (stride `nb` bytes), the uint16
-// texels from xa = x0 rounded down to 8 on.  Each lane converts 8-texel
-// chunks read with 128-bit loads.  Zero intensity texels among the texels
-// the box reads ([x0, x0 + bw] of each row) are listed in `zl` as
+// texels from xa = x0 rounded down to 8 on.  One box texel per lane and
+// step: its two texels of each plane become {v(x), v(x+1) + dm * v(x)}
+// (dm = 0: reference pairs; dm = -1: target value and difference, exact for
+// integers), each value placed in the mantissa of 2^23 and shifted by
+// -(2^23 + shift) in one exact addition.  Zero intensity texels among the
+// texels the box reads ([x0, x0 + bw] of each row) are listed in `zl` as
 // tag | row << 16 | (x - x0), counted in *zn (entries beyond `cap` are
 // counted, not stored).
-template <bool kDiff>
 __device__ __forceinline__ void convert_tile(float4 *__restrict__ dst, int ds,
                                              const unsigned char *__restrict__ rawI,
                                              const unsigned char *__restrict__ rawM, int nb,
                                              int xa, int x0, int bw, int bh, float sI, float sM,
-                                             uint32_t *zl, int *zn, int cap, uint32_t tag,
-                                             int lane) {
+                                             float dm, uint32_t *zl, int *zn, int cap,
+                                             uint32_t tag, int lane) {
     const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
-    const int x1 = x0 + bw - 1;                 // last box texel
-    const int nch = (x1 + 1 - xa) / 8 + 1;      // chunks covering [xa, x1 + 1]
-    const int n = nch * bh;
-    // chunk i = (row by, column c): the lane's first chunk, then steps of 32
-    int by = lane / nch, c = lane - by * nch;
-    const int dby = 32 / nch, dc = 32 - dby * nch;
-    for (int i = lane; i < n; i += 32) {
-        const int xc = xa + 8 * c;
-        const int ro = by * nb + 16 * c;
-        const uint4 vi = *reinterpret_cast<const uint4 *>(rawI + ro);
-        const uint4 vm = *reinterpret_cast<const uint4 *>(rawM + ro);
-        const bool need9 = xc + 7 <= x1;        // the 8th texel needs texel xc + 8
-        const uint32_t i8 = need9 ? *reinterpret_cast<const uint16_t *>(rawI + ro + 16) : 1u;
-        const uint32_t m8 = need9 ? *reinterpret_cast<const uint16_t *>(rawM + ro + 16) : 0u;
-        const uint32_t zw = zero_half(vi.x) | zero_half(vi.y) | zero_half(vi.z) | zero_half(vi.w);
-        if ((zw & 0x80008000u) != 0 || i8 == 0) {
-            // rare: list the zero texels of the range the box reads
-            const uint32_t w[4] = {vi.x, vi.y, vi.z, vi.w};
-#pragma unroll
-            for (int t = 0; t < 9; ++t) {
-                const int x = xc + t;
-                const uint32_t tex = t < 8 ? (w[t >> 1] >> (16 * (t & 1))) & 0xFFFFu : i8;
-                if (x >= x0 && x <= x1 + 1 && tex == 0) {
-                    const int k = atomicAdd(zn, 1);
-                    if (k < cap) zl[k] = tag | ((uint32_t)by << 16) | (uint32_t)(x - x0);
-                }
+    const float2 dm2 = bc2(dm);
+    const int n = bw * bh;
+    const unsigned char *rI = rawI + 2 * (x0 - xa);
+    const unsigned char *rM = rawM + 2 * (x0 - xa);
+    // box texel (row by, column bx): the lane's first, then steps of 32
+    int by = lane / bw, bx = lane - by * bw;
+    const int dby = 32 / bw, dbx = 32 - dby * bw;
+    for (int q = lane; q < n; q += 32) {
+        const int ro = by * nb + 2 * bx;
+        const uint32_t i0 = *reinterpret_cast<const uint16_t *>(rI + ro);
+        const uint32_t i1 = *reinterpret_cast<const uint16_t *>(rI + ro + 2);
+        const uint32_t m0 = *reinterpret_cast<const uint16_t *>(rM + ro);
+        const uint32_t m1 = *reinterpret_cast<const uint16_t *>(rM + ro + 2);
+        const bool last = bx == bw - 1;   // the row's last texel also reads texel bw
+        if (i0 == 0 || (last && i1 == 0)) {
+            // rare: list the zero texels
+            if (i0 == 0) {
+                const int k = atomicAdd(zn, 1);
+                if (k < cap) zl[k] = tag | ((uint32_t)by << 16) | (uint32_t)bx;
+            }
+            if (last && i1 == 0) {
+                const int k = atomicAdd(zn, 1);
+                if (k < cap) zl[k] = tag | ((uint32_t)by << 16) | (uint32_t)(bx + 1);
             }
         }
-        store_chunk<kDiff>(dst + by * ds, vi, vm, i8, m8, xc, x0, x1, ns);
+        const float2 a = __fadd2_rn(make_float2(__int_as_float(i0 | 0x4B000000u),
+                                                __int_as_float(m0 | 0x4B000000u)), ns);
+        const float2 b = __fadd2_rn(make_float2(__int_as_float(i1 | 0x4B000000u),
+                                                __int_as_float(m1 | 0x4B000000u)), ns);
+        const float2 h = __ffma2_rn(dm2, a, b);
+        dst[by * ds + bx] = make_float4(a.x, a.y, h.x, h.y);
+        bx += dbx;
         by += dby;
-        c += dc;
-        if (c >= nch) {
-            c -= nch;
+        if (bx >= bw) {
+            bx -= bw;
             ++by;
         }
     }

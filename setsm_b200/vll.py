@@ -525,7 +525,7 @@ class Context:
         """CUDA-graph plan of a batch (see vll_plan_create)."""
         return Plan(self, levels)
 
-    def set_tuning(self, blocks_per_sm: int = 0, grab: int = 1, box_margin: float = 1.1) -> None:
+    def set_tuning(self, blocks_per_sm: int = 0, grab: int = 8, box_margin: float = 1.1) -> None:
         t = abi.Tuning(int(blocks_per_sm), int(grab), float(box_margin), 0)
         self._check(load().vll_set_tuning(self._h, C.byref(t)))
 
