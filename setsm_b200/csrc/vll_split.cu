@@ -1692,12 +1692,15 @@ WindowBoxes window_boxes(const DevLevel &P, float margin) {
                 ry[ti] = std::max(ry[ti], fabs(y1 - y0) / 100.0 / (1 << P.L));
             }
     }
+    // one slot's box (texel pairs, rows: the reference window 2H + 2, the
+    // target's rotated footprint 2(H + 2) + 2), plus the sweep of 31 height
+    // steps with the margin, plus one texel of rounding
     const double m = margin > 0 ? margin : 1.1;
-    const int side[2] = {2 * H + 3, 2 * (H + 2) + 3};   // pairs of one slot's box (+1 slack)
+    const int side[2] = {2 * H + 2, 2 * (H + 2) + 2};
     WindowBoxes B;
     for (int ti = 0; ti < 2; ++ti) {
-        B.w[ti] = (int)std::ceil((side[ti] + 31.0 * P.height_step * rx[ti]) * m);
-        B.h[ti] = (int)std::ceil((side[ti] + 31.0 * P.height_step * ry[ti]) * m);
+        B.w[ti] = side[ti] + (int)std::ceil(31.0 * P.height_step * rx[ti] * m) + 1;
+        B.h[ti] = side[ti] + (int)std::ceil(31.0 * P.height_step * ry[ti] * m) + 1;
     }
     return B;
 }
@@ -1712,7 +1715,8 @@ struct WarpBudget {
 WarpBudget window_warp_budget(const DevLevel &P, float margin) {
     const WindowBoxes B = window_boxes(P, margin);
     WarpBudget wb;
-    wb.quads = (B.w[0] + 1) * B.h[0] + (B.w[1] + 1) * B.h[1] + 32;
+    // boxes up to the budget's sides, rows of odd stride
+    wb.quads = (B.w[0] | 1) * B.h[0] + (B.w[1] | 1) * B.h[1];
     wb.raw = 128;
     if (P.tma_w[0] > 0)
         wb.raw = 2 * (((P.tma_w[0] * P.tma_h[0] * 2 + 127) & ~127) +
