@@ -663,12 +663,24 @@ def run_multi(args):
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record(stream)
+    per_level = []
     for lv in mw.levels:
-        ctx.vertical_line_locus_device(lv.desc, lv.d_gp3.data_ptr(), lv.d_ncc.data_ptr(), None,
-                                       None, "split")
+        stl = ctx.vertical_line_locus_device(lv.desc, lv.d_gp3.data_ptr(), lv.d_ncc.data_ptr(),
+                                             None, None, "split", stats=True)
+        per_level.append(stl)
     e3.record(stream)
     torch.cuda.synchronize(dev)
     per_level_ms = e2.elapsed_time(e3)
+    # the separate calls' records against the batch's, level by level
+    parity = {"levels": len(mw.levels), "nodes": int(mw.n_nodes), "fields_mismatched": {},
+              "accessable_equal": all(int(per_level[i].accessable_grid) == int(acc[i])
+                                      for i in range(len(mw.levels)))}
+    for i, lv in enumerate(mw.levels):
+        got = lv.d_ncc.cpu().numpy().view(abi.NCCRESULT_DTYPE)
+        for k, v in cases_field_mismatch(got, ncc_batch[i]).items():
+            parity["fields_mismatched"][k] = parity["fields_mismatched"].get(k, 0) + v
+    level_rows = [{"level": lv.name, "nodes": int(lv.n_nodes), "evals": int(per_level[i].evals),
+                   "accessable": int(acc[i])} for i, lv in enumerate(mw.levels)]
     # plain FP64 per level on a sample of levels (about 1e9 evaluations at most)
     fp64 = None
     if not args.skip_fp64 and rank == 0:
@@ -710,8 +722,10 @@ def run_multi(args):
                       "4 px per node, convergence 20-40 deg, own DEM and TIN ranges K 8-512 at "
                       "0.5 m), 7x7, one persistent launch per step, CUDA graph",
                 "c4": "C4: 5-level pyramid of a 16384^2 pair (9x9 sigma 1.5 downsample), grids "
-                      "32 m -> 2 m, K 256 -> 16, 7x7 and 11x11 at every level, one persistent "
-                      "launch per step, CUDA graph"}[args.config],
+                      "32 m -> 2 m, K 256 -> 16, each finer level's ranges +-3 sigma around the "
+                      "previous level's matches (SelectMPs, TIN) interpolated at its nodes, "
+                      "7x7 and 11x11 at every level, one persistent launch per step, "
+                      "CUDA graph"}[args.config],
                 "levels": len(mw.levels), "nodes": mw.n_nodes, "evals_per_step": evals_step,
                 "tuning": tuned["tuning"], "l2": "inputs larger than L2",
                 "parallelism": f"replicas x{world}"},
@@ -722,6 +736,9 @@ def run_multi(args):
                                                  "algorithmic bytes per evaluation of the windows"},
             "per_level_split_calls": {"value": evals_step / (per_level_ms / 1e3), "unit": UNIT,
                                       "ms": per_level_ms},
+            "levels": level_rows,
+            "parity_batch_vs_calls": parity,
+            "range_chain": mw.info or None,
             "gpu_launches": int(launches),
             "fp64_plain_gpu": fp64,
             "clocks": clk,
@@ -1440,9 +1457,10 @@ def run_c5(args):
               for sid in range(args.c5_scenes)]
     log(f"[rank {rank}] {len(scenes)} resident scenes built in {time.time() - t0:.1f} s "
         f"({torch.cuda.memory_allocated(dev) / 1e9:.1f} GB)")
-    warm = serving.poisson_requests(16, 200.0, scenes, seed=1000 + rank)
+    mix = dict(levels=(0, 1, 2, 3, 4), templates=(11, 15))
+    warm = serving.poisson_requests(16, 200.0, scenes, seed=1000 + rank, **mix)
     serving.Server(scenes, device=local, hbm_budget=args.c5_budget * 1e9).run(warm, realtime=False)
-    reqs = serving.poisson_requests(args.c5_requests, args.c5_rate, scenes, seed=7 + rank)
+    reqs = serving.poisson_requests(args.c5_requests, args.c5_rate, scenes, seed=7 + rank, **mix)
     clocks = Clocks(local)
     clocks.start()
     srv = serving.Server(scenes, device=local, hbm_budget=args.c5_budget * 1e9,
@@ -1450,6 +1468,16 @@ def run_c5(args):
     barrier(world)
     rep = srv.run(reqs, realtime=True)
     clk = clocks.stop()
+    # the same mix below saturation: the rate scaled so that the offered load
+    # is half of what the first run served, for steady-state latencies
+    load = rep["offered_slots_per_s"] / max(rep["served_slots_per_s"], 1e-9)
+    rate2 = args.c5_rate * min(1.0, 0.5 / max(load, 1e-9))
+    n2 = max(50, min(args.c5_requests, int(rate2 * 60)))
+    reqs2 = serving.poisson_requests(n2, rate2, scenes, seed=17 + rank, **mix)
+    srv2 = serving.Server(scenes, device=local, hbm_budget=args.c5_budget * 1e9,
+                          max_batch=args.c5_max_batch, n_workers=2)
+    barrier(world)
+    rep2 = srv2.run(reqs2, realtime=True)
     # sequential plain FP64 on a sample of the same requests
     by_sid = {rs.sid: rs for rs in scenes}
     ev, ms = 0, 0.0
@@ -1469,12 +1497,20 @@ def run_c5(args):
             "dtype": "f32 window sums, f64 RPC and decisions", "data": "synthetic",
             "config": {"workload": f"C5 serving: Poisson {args.c5_rate:g} req/s, "
                                    f"{args.c5_requests} requests, grid 64^2-1024^2 and K 8-512 "
-                                   f"log-uniform, level 0, 7x7, {args.c5_scenes} resident "
+                                   f"log-uniform, pyramid levels 0-4 and 7x7 / 11x11 windows "
+                                   f"drawn uniformly, {args.c5_scenes} resident "
                                    f"{args.c5_image}^2 pairs with 5-level pyramids, HBM budget "
                                    f"{args.c5_budget:g} GB, continuous batching on 2 streams",
                        "parallelism": f"replicas x{world}"},
             "serving": rep,
             "latency_ms": {"p50": rep["p50_ms"], "p99": rep["p99_ms"]},
+            "offered_vs_served_slots_per_s": [rep["offered_slots_per_s"],
+                                              rep["served_slots_per_s"]],
+            "below_saturation": {"rate_req_per_s": rate2, "requests": n2,
+                                 "offered_slots_per_s": rep2["offered_slots_per_s"],
+                                 "served_slots_per_s": rep2["served_slots_per_s"],
+                                 "evals_per_s": rep2["evals_per_s"],
+                                 "latency_ms": {"p50": rep2["p50_ms"], "p99": rep2["p99_ms"]}},
             "fp64_plain_sequential": {"value": ev / (ms / 1e3), "unit": UNIT,
                                       "requests": len(sample),
                                       "timing": "host wall clock per request (synchronous)"},
@@ -1488,6 +1524,153 @@ def run_c5(args):
         dist.destroy_process_group()
 
 
+def run_shard(args):
+    """One scene of the config split into grid-row bands, one per rank
+    (strong scaling).  Every rank builds the same seeded scene, keeps only its
+    band's image footprint (shard.footprint_of) on its GPU, matches its rows
+    with each window, and the NCCresult bands are all-gathered with
+    dist.all_gather_into_tensor (NCCL) after each call, so every rank holds
+    the whole grid's records as a full call would leave them.  Rank 0 checks
+    the gathered grid against the whole-grid call on the same scene."""
+    world, rank, local = dist_setup(args.gpus)
+    import torch
+    from setsm_b200 import shard, vll, workloads
+
+    dev = torch.device("cuda", local)
+    ctx = vll.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.time()
+    wl = workloads.build(args.config, ctx, device=f"cuda:{local}", seed=1, keep_host=False)
+    templates = workloads.CONFIGS[args.config]["templates"]
+    W, Hg = wl.grid.width, wl.grid.height
+    whole = {}
+    if rank == 0:
+        # the whole-grid call on the same scene (parity reference)
+        for t in templates:
+            wl.d_ncc.zero_()
+            torch.cuda.synchronize(dev)
+            st = ctx.vertical_line_locus_device(wl.device_desc(t), wl.d_gp3.data_ptr(),
+                                                wl.d_ncc.data_ptr(), None, None, args.kernel,
+                                                stats=True)
+            whole[t] = (workloads.ncc_host(wl), int(st.accessable_grid))
+    r0, r1 = shard.row_bands(Hg, world)[rank]
+    band = wl.device_band(r0, r1)
+    # the whole planes and the whole-grid record array are released: the
+    # rank keeps its band's footprint
+    wl.d_img, wl.d_mag, wl.d_ori = [], [], []
+    wl.d_ncc = None
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    descs = {t: band.desc(t) for t in templates}
+    rows_max = max(b1 - b0 for b0, b1 in shard.row_bands(Hg, world))
+    band_ncc = torch.zeros(max(1, rows_max * W) * shard.NCC_BYTES, dtype=torch.uint8, device=dev)
+    log(f"[rank {rank}] band rows [{r0}, {r1}) of {Hg}, footprint planes "
+        f"{band.image_bytes() / 2**20:.0f} MiB, built in {time.time() - t0:.1f} s")
+
+    def one_step():
+        # (the call's statistics carry Accessable_grid, as the whole-grid leg's do)
+        out = {}
+        with torch.cuda.stream(stream):
+            for t in templates:
+                st = ctx.vertical_line_locus_device(descs[t], band.d_gridpt3(),
+                                                    band_ncc.data_ptr(), None, None,
+                                                    args.kernel, stats=True)
+                acc = int(st.accessable_grid)
+                if world > 1:
+                    full, acc = shard.gather_bands_tensor(band_ncc, acc, W, Hg, device=dev)
+                else:
+                    full = band_ncc
+                out[t] = (st, full, acc)
+        return out
+
+    for _ in range(max(3, args.warmup)):
+        warm = one_step()
+    evals_rank = sum(warm[t][0].evals for t in templates)
+    # parity: each window's gathered grid from a cleared band array
+    parity = None
+    for t in templates:
+        band_ncc.zero_()
+        torch.cuda.synchronize(dev)
+        with torch.cuda.stream(stream):
+            st = ctx.vertical_line_locus_device(descs[t], band.d_gridpt3(), band_ncc.data_ptr(),
+                                                None, None, args.kernel, stats=True)
+            acc = int(st.accessable_grid)
+            if world > 1:
+                full, acc = shard.gather_bands_tensor(band_ncc, acc, W, Hg, device=dev)
+            else:
+                full = band_ncc
+        torch.cuda.synchronize(dev)
+        if rank == 0:
+            got = full[:W * Hg * shard.NCC_BYTES].cpu().numpy().view(whole[t][0].dtype)
+            mism = cases_field_mismatch(got, whole[t][0])
+            p = parity or {"nodes": int(W * Hg), "fields_mismatched": {}, "accessable_equal": True}
+            for k, v in mism.items():
+                p["fields_mismatched"][k] = p["fields_mismatched"].get(k, 0) + v
+            p["accessable_equal"] = p["accessable_equal"] and acc == whole[t][1]
+            parity = p
+    barrier(world)
+
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = ctx.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    e0.record(stream)
+    for _ in range(args.steps):
+        one_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
+    launches = ctx.launch_count() - launches0
+    evals_total = sum_over_ranks(world, evals_rank * args.steps)
+    value = evals_total / (ms / 1e3)
+    img_mib = max_over_ranks(world, band.image_bytes() / 2**20)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 window sums, f64 RPC and decisions", "data": "synthetic",
+            "config": {"workload": config_block(args, wl)["workload"], "nodes": int(W * Hg),
+                       "windows": [workloads.WINDOW_OF_TEMPLATE[t] for t in templates],
+                       "kernel": args.kernel,
+                       "l2": "inputs larger than L2 (band footprints of 16384^2 planes)",
+                       "parallelism": f"row bands x{world}, NCCresult bands all-gathered "
+                                      "(all_gather_into_tensor) after every call"},
+            "shard": {"bands": [list(b) for b in shard.row_bands(Hg, world)],
+                      "max_footprint_planes_mib": img_mib,
+                      "parity_vs_whole_grid": parity},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cases_field_mismatch(got, want) -> dict:
+    """Mismatching records per NCCresult field (numpy structured arrays)."""
+    out = {}
+    for name in want.dtype.names:
+        a, b = got[name], want[name]
+        if a.dtype.kind == "f":
+            n = int(np.count_nonzero(a.view(np.uint32 if a.itemsize == 4 else np.uint64) !=
+                                     b.view(np.uint32 if b.itemsize == 4 else np.uint64)))
+        else:
+            n = int(np.count_nonzero(a != b))
+        if n:
+            out[name] = n
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1499,6 +1682,8 @@ def main():
                              "blunder", "ortho_tin", "height_range", "select_mps",
                              "voxel_iter", "tin_blunder"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
+    ap.add_argument("--shard", action="store_true",
+                    help="one scene split into grid-row bands over the ranks (strong scaling)")
     ap.add_argument("--e2e-steps", type=int, default=0,
                     help="end-to-end steps of the default config (0: as many as --steps)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -1521,6 +1706,8 @@ def main():
         args.e2e_steps = args.steps
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.shard:
+        run_shard(args)
     elif args.config in ("c3", "c4"):
         run_multi(args)
     elif args.config == "c5":

@@ -561,7 +561,11 @@ int vll_blunder_detection_tin(vll_context *ctx, const vll_level_desc *desc, int 
                               double *maxz_mp);
 /* The same on device data (ortho_ncc, pts, detected_blunders, tris and
  * gridpt3 are device pointers; blunder_count, minz_mp and maxz_mp are host
- * pointers).  Waits. */
+ * pointers).  Waits.  A point whose grid node lies outside the grid is found
+ * during the point pass: the call then returns VLL_ERR_INVALID with the
+ * device buffers pts[].flag, detected_blunders and gridpt3[].anchor_flag
+ * partly written (undefined); the host outputs are unchanged.  (The host
+ * entry leaves every caller buffer as it was.) */
 int vll_blunder_detection_tin_device(vll_context *ctx, const vll_level_desc *desc, int iteration,
                                      const float *d_ortho_ncc, int flag_blunder, int count_bl,
                                      double hinterval, vll_point3 *d_pts,

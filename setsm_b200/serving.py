@@ -282,7 +282,14 @@ class Server:
                 if bs[j][1] >= bs[i][2]:
                     break
                 overlap += min(bs[i][2], bs[j][2]) - bs[j][1]
+        arr = [r.arrival for r in self.finished]
+        slots = sum(r.n * r.n * r.k for r in self.finished)
+        span = max(arr) - min(arr) if len(arr) > 1 else 0.0
         return {"requests": len(self.finished), "batches": len(self.batches),
+                # candidate slots (grid nodes x heights) requested per second of
+                # arrivals, and served per second of the makespan
+                "offered_slots_per_s": slots / span if span > 0 else 0.0,
+                "served_slots_per_s": slots / makespan if makespan > 0 else 0.0,
                 "mean_batch": float(np.mean([b[0] for b in self.batches])),
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "max_ms": float(lat.max()), "evals": int(evals),
@@ -292,9 +299,11 @@ class Server:
 
 
 def poisson_requests(n: int, rate: float, scenes: list, seed: int = 7, grid_min: int = 64,
-                     grid_max: int = 1024, levels=(0,), template: int = 11) -> list:
+                     grid_max: int = 1024, levels=(0,), templates=(11,)) -> list:
     """n requests with Poisson arrivals at `rate` per second; grid side and
-    candidate count log-uniform in [grid_min, grid_max] and [8, 512]."""
+    candidate count log-uniform in [grid_min, grid_max] and [8, 512]; the
+    pyramid level and the window drawn uniformly from `levels` and
+    `templates` (a level's grid is at 2 m << level, clipped to its scene)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -302,6 +311,7 @@ def poisson_requests(n: int, rate: float, scenes: list, seed: int = 7, grid_min:
         t += rng.exponential(1.0 / rate)
         rs = scenes[int(rng.integers(len(scenes)))]
         L = int(rng.choice(levels))
+        template = int(rng.choice(templates))
         spacing = 2.0 * (1 << L)
         side_max = int(rs.scene.spec.image_size * rs.scene.spec.gsd / spacing)
         n_side = int(round(math.exp(rng.uniform(math.log(grid_min), math.log(grid_max)))))

@@ -26,7 +26,9 @@ import math
 
 import numpy as np
 
-from . import level
+from . import abi, level
+
+NCC_BYTES = abi.NCCRESULT_DTYPE.itemsize   # bytes of one NCCresult record
 
 # Margin (pyramid pixels) kept around the projected footprint: the largest
 # window radius (half-size 8, rotated: 8 * sqrt(2) + 2) plus the image
@@ -70,17 +72,23 @@ def footprint(inputs: level.LevelInputs, r0: int, r1: int, ti: int, pyramid_step
     level's full-image pixel coordinates) that the band's nodes can touch."""
     W = inputs.grid_width
     sl = slice(r0 * W, r1 * W)
-    wgs = inputs.grid_wgs[sl]
-    g = inputs.gridpt3[sl]
     im = inputs.images[ti]
+    return footprint_of(inputs.grid_wgs[sl], inputs.gridpt3[sl], im.rpc, im.adjust,
+                        pyramid_step, margin)
+
+
+def footprint_of(wgs: np.ndarray, g: np.ndarray, rpc: np.ndarray, adjust, pyramid_step: int,
+                 margin: int = MARGIN):
+    """The box of `footprint` for grid nodes `wgs` (lon, lat) with UGRID rows
+    `g`, in an image of RPC `rpc` and (line, sample) adjustment `adjust`."""
     lo = g["minHeight"].astype(np.float64)
     hi = g["maxHeight"].astype(np.float64)
     hs = [lo, hi, 0.5 * (lo + hi), g["Height"].astype(np.float64)]
     xs, ys = [], []
     for h in hs:
-        x, y = _rpc_eval(im.rpc, wgs[:, 0], wgs[:, 1], h)
-        xs.append(x + im.adjust[1])
-        ys.append(y + im.adjust[0])
+        x, y = _rpc_eval(rpc, wgs[:, 0], wgs[:, 1], h)
+        xs.append(x + adjust[1])
+        ys.append(y + adjust[0])
     scale = 1.0 / (1 << pyramid_step)
     x = np.concatenate(xs) * scale
     y = np.concatenate(ys) * scale
@@ -171,19 +179,41 @@ def match_band(ctx, inputs: level.LevelInputs, rank: int, world: int, kernel: st
     return ncc, acc, (r0, r1)
 
 
-def gather_bands(ncc_band: np.ndarray, acc: int, grid_width: int, grid_height: int, group=None):
-    """All-gathers the bands' NCCresult rows over torch.distributed (gloo on
-    CPU, NCCL between GPUs); returns the whole grid's NCCresult and the summed
-    Accessable_grid on every rank."""
+def gather_bands(ncc_band: np.ndarray, acc: int, grid_width: int, grid_height: int, group=None,
+                 device=None):
+    """All-gathers the bands' NCCresult rows over torch.distributed; returns
+    the whole grid's NCCresult and the summed Accessable_grid on every rank.
+    `device` is where the collective's buffers live (None: the CPU, for
+    gloo; a CUDA device for NCCL)."""
+    import torch
+    full, total = gather_bands_tensor(torch.from_numpy(ncc_band.view(np.uint8).copy()), acc,
+                                      grid_width, grid_height, group=group, device=device)
+    return full.cpu().numpy().view(ncc_band.dtype), total
+
+
+def gather_bands_tensor(band, acc: int, grid_width: int, grid_height: int, group=None,
+                        device=None):
+    """The same for a band held as a uint8 tensor (its rows' records first,
+    any length up to the largest band's bytes): every rank's band is padded
+    to the largest band and gathered with one all_gather_into_tensor; the
+    counts are summed with all_reduce.  Returns (whole-grid uint8 tensor,
+    Accessable_grid) on `device`."""
+    import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
-    parts = [None] * world
-    dist.all_gather_object(parts, (ncc_band.view(np.uint8).tobytes(), int(acc)), group=group)
-    full = np.zeros(grid_width * grid_height, dtype=ncc_band.dtype)
-    total = 0
-    for k, (buf, a) in enumerate(parts):
-        r0, r1 = row_bands(grid_height, world)[k]
-        full[r0 * grid_width:r1 * grid_width] = np.frombuffer(buf, dtype=np.uint8).view(
-            ncc_band.dtype)
-        total += a
-    return full, total
+    bands = row_bands(grid_height, world)
+    rec = NCC_BYTES
+    cap = max(r1 - r0 for r0, r1 in bands) * grid_width * rec
+    dev = device if device is not None else band.device
+    send = torch.zeros(cap, dtype=torch.uint8, device=dev)
+    n = min(int(band.numel()), cap)
+    send[:n].copy_(band.reshape(-1)[:n])
+    recv = torch.empty(world * cap, dtype=torch.uint8, device=dev)
+    dist.all_gather_into_tensor(recv, send, group=group)
+    cnt = torch.tensor([int(acc)], dtype=torch.int64, device=dev)
+    dist.all_reduce(cnt, group=group)
+    full = torch.empty(grid_width * grid_height * rec, dtype=torch.uint8, device=dev)
+    for k, (r0, r1) in enumerate(bands):
+        nb = (r1 - r0) * grid_width * rec
+        full[r0 * grid_width * rec:r0 * grid_width * rec + nb].copy_(recv[k * cap:k * cap + nb])
+    return full, int(cnt.item())

@@ -70,7 +70,9 @@ class Workload:
             self.grid.height, self.grid.boundary, self.gp3, **self.level_kwargs(template))
         d = li.desc()
         n = self.scene.spec.image_size
-        for ci in range(2):
+        # (a Workload whose whole planes were released after cropping bands
+        # has none: DeviceBand.desc sets the crops')
+        for ci in range(len(self.d_img)):
             e = d.images[ci]
             e.image = self.d_img[ci].data_ptr()
             e.mag = self.d_mag[ci].data_ptr()
@@ -94,6 +96,29 @@ class Workload:
         d.grid_wgs = self.d_wgs.data_ptr() + r0 * W * 16
         return (d, self.d_gp3.data_ptr() + r0 * W * abi.UGRID_DTYPE.itemsize,
                 self.d_ncc.data_ptr() + r0 * W * abi.NCCRESULT_DTYPE.itemsize)
+
+    def device_band(self, r0: int, r1: int) -> "DeviceBand":
+        """Grid rows [r0, r1) with each image plane cut, on the device, to the
+        band's footprint (shard.footprint_of: every projection of the band's
+        nodes over their height range, widened by the shard margin); the cut's
+        origin becomes the image's py_Startpos, as in shard.band_inputs.  The
+        whole-image planes are not referenced by the band."""
+        from . import shard
+        W = self.grid.width
+        sl = slice(r0 * W, r1 * W)
+        n = self.scene.spec.image_size
+        crops = []
+        for ci in range(2):
+            x0, x1, y0, y1 = shard.footprint_of(self.grid.wgs[sl], self.gp3[sl],
+                                                self.scene.rpcs[ci], (0.0, 0.0), 0)
+            x0, y0 = max(0, x0), max(0, y0)
+            x1, y1 = min(n, x1), min(n, y1)
+            if x1 - x0 < 2 or y1 - y0 < 2:
+                x0, y0, x1, y1 = 0, 0, 2, 2
+            crops.append(((x0, y0), self.d_img[ci][y0:y1, x0:x1].contiguous(),
+                          self.d_mag[ci][y0:y1, x0:x1].contiguous(),
+                          self.d_ori[ci][y0:y1, x0:x1].contiguous()))
+        return DeviceBand(self, r0, r1, crops)
 
     def host_inputs(self, template: int, rows: tuple | None = None,
                     planes: dict | None = None) -> level.LevelInputs:
@@ -123,6 +148,47 @@ def _pinned(t: torch.Tensor) -> np.ndarray:
     h = torch.empty(t.shape, dtype=t.dtype, pin_memory=torch.cuda.is_available())
     h.copy_(t)
     return h.numpy()
+
+
+@dataclass
+class DeviceBand:
+    """A band of grid rows on the device with its cropped image planes
+    (Workload.device_band)."""
+    wl: Workload
+    r0: int
+    r1: int
+    crops: list          # per image: ((x0, y0), image, magnitude, orientation)
+
+    @property
+    def n_nodes(self) -> int:
+        return (self.r1 - self.r0) * self.wl.grid.width
+
+    def desc(self, template: int) -> abi.LevelDesc:
+        """Level descriptor of the band: the band's grid rows (pointers into
+        the resident grid arrays), the cropped planes with their origins as
+        py_Startpos, and the whole tile's boundary."""
+        wl = self.wl
+        W = wl.grid.width
+        d = wl.device_desc(template)
+        d.grid_height = self.r1 - self.r0
+        d.grid_pts = wl.d_pts.data_ptr() + self.r0 * W * 16
+        d.grid_wgs = wl.d_wgs.data_ptr() + self.r0 * W * 16
+        for ci, ((x0, y0), img, mag, ori) in enumerate(self.crops):
+            e = d.images[ci]
+            e.image = img.data_ptr()
+            e.mag = mag.data_ptr()
+            e.ori = ori.data_ptr()
+            e.width = img.shape[1]
+            e.height = img.shape[0]
+            e.startpos[0] = float(x0)
+            e.startpos[1] = float(y0)
+        return d
+
+    def d_gridpt3(self) -> int:
+        return self.wl.d_gp3.data_ptr() + self.r0 * self.wl.grid.width * abi.UGRID_DTYPE.itemsize
+
+    def image_bytes(self) -> int:
+        return sum(t.numel() * t.element_size() for c in self.crops for t in c[1:])
 
 
 def build(name: str, ctx, device: str = "cuda", seed: int = 1, keep_host: bool = True) -> Workload:
@@ -238,6 +304,7 @@ class MultiWorkload:
     name: str
     levels: list
     scenes: list
+    info: dict = field(default_factory=dict)
 
     @property
     def n_nodes(self) -> int:
@@ -334,17 +401,90 @@ def build_c3(ctx, device: str = "cuda", seed: int = 1, n_tiles: int = 64,
     return MultiWorkload(name="c3", levels=levels, scenes=scenes)
 
 
+def tin_heights(pts: np.ndarray, tris: np.ndarray, grid) -> tuple:
+    """Heights at `grid`'s nodes interpolated linearly over a TIN (pts:
+    POINT3 records in projected metres, tris: vertex indices); nodes outside
+    every triangle take the height of the nearest point.  Returns (heights,
+    covered mask)."""
+    W, Hn, res = grid.width, grid.height, grid.resolution
+    x0, y0 = grid.boundary[0], grid.boundary[1]
+    h = np.full(W * Hn, np.nan)
+    if len(tris):
+        v = np.stack([tris["a"], tris["b"], tris["c"]], 1).astype(np.int64)
+        X, Y, Z = pts["x"][v], pts["y"][v], pts["z"][v]          # [T, 3]
+        det = (Y[:, 1] - Y[:, 2]) * (X[:, 0] - X[:, 2]) + (X[:, 2] - X[:, 1]) * (Y[:, 0] - Y[:, 2])
+        ok = np.abs(det) > 1e-12
+        X, Y, Z, det = X[ok], Y[ok], Z[ok], det[ok]
+        c0 = np.ceil((X.min(1) - x0) / res).astype(np.int64)
+        c1 = np.floor((X.max(1) - x0) / res).astype(np.int64)
+        r0 = np.ceil((Y.min(1) - y0) / res).astype(np.int64)
+        r1 = np.floor((Y.max(1) - y0) / res).astype(np.int64)
+        span = int(max(1, (c1 - c0).max(initial=0) + 1, (r1 - r0).max(initial=0) + 1))
+        for dr in range(span):
+            for dc in range(span):
+                c, r = c0 + dc, r0 + dr
+                m = (c <= c1) & (r <= r1) & (c >= 0) & (c < W) & (r >= 0) & (r < Hn)
+                if not m.any():
+                    continue
+                px, py = x0 + c[m] * res, y0 + r[m] * res
+                Xm, Ym, Zm, dm = X[m], Y[m], Z[m], det[m]
+                l0 = ((Ym[:, 1] - Ym[:, 2]) * (px - Xm[:, 2]) + (Xm[:, 2] - Xm[:, 1]) * (py - Ym[:, 2])) / dm
+                l1 = ((Ym[:, 2] - Ym[:, 0]) * (px - Xm[:, 2]) + (Xm[:, 0] - Xm[:, 2]) * (py - Ym[:, 2])) / dm
+                l2 = 1.0 - l0 - l1
+                inside = (l0 >= -1e-9) & (l1 >= -1e-9) & (l2 >= -1e-9)
+                idx = (r[m] * W + c[m])[inside]
+                h[idx] = (l0 * Zm[:, 0] + l1 * Zm[:, 1] + l2 * Zm[:, 2])[inside]
+    covered = np.isfinite(h)
+    if (~covered).any() and len(pts):
+        from scipy.spatial import cKDTree
+        tree = cKDTree(np.stack([pts["x"], pts["y"]], 1))
+        _, j = tree.query(grid.pts[~covered])
+        h[~covered] = pts["z"][j]
+    return h, covered
+
+
+def _match_level_points(ctx, lw: "LevelWork", grid, dev) -> tuple:
+    """The chain step of C4 on the device: VerticalLineLocus of level work
+    `lw` (synchronously), SelectMPs on its records (thresholds of a first iteration), and
+    TINCreate_list of the matched points.  Returns (points, triangles) on the
+    host."""
+    n = lw.n_nodes
+    ctx.vertical_line_locus_device(lw.desc, lw.d_gp3.data_ptr(), lw.d_ncc.data_ptr(), None,
+                                   None, "split")
+    d_g = lw.d_gp3.clone()        # SelectMPs updates its UGRID
+    torch.cuda.synchronize(dev)   # (the library runs on its own stream)
+    d_pts = torch.empty(n * abi.POINT3_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    n_pts = ctx.select_mps_device(lw.desc, lw.d_ncc.data_ptr(), d_g.data_ptr(), d_pts.data_ptr(),
+                                  n, 0.6, 0.2, 0.8, 0.7, 1, 1.5, 1, 10.0)
+    cap = 2 * max(n_pts, 1) + 16
+    d_tris = torch.empty(cap * abi.TRI_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    n_tris = ctx.tin_create_device(d_pts.data_ptr(), n_pts, grid.boundary, grid.resolution,
+                                   d_tris.data_ptr(), cap) if n_pts >= 3 else 0
+    pts = d_pts[:n_pts * abi.POINT3_DTYPE.itemsize].cpu().numpy().view(abi.POINT3_DTYPE)
+    tris = d_tris[:n_tris * abi.TRI_DTYPE.itemsize].cpu().numpy().view(abi.TRI_DTYPE)
+    return pts.copy(), tris.copy()
+
+
 # C4 candidates per level (level 4 .. 0) and grid spacing (m)
 C4_LEVELS = {4: (256, 32.0), 3: (128, 16.0), 2: (64, 8.0), 1: (32, 4.0), 0: (16, 2.0)}
 
 
 def build_c4(ctx, device: str = "cuda", seed: int = 1, image_size: int = 16384,
-             templates=(11, 15)) -> MultiWorkload:
+             templates=(11, 15), chain: bool = True) -> MultiWorkload:
     """C4: a 5-level pyramid of one stereo pair (the reference's 9x9,
     sigma = 1.5 Gaussian 2x downsample, CreateImagePyramid), grid spacing 32 m
     at level 4 down to 2 m at level 0, K = 256 .. 16 candidates per level at
-    that level's GetHeightStep around truth + N(0, sigma) with +-3 sigma
-    covering the range; every level with the 7x7 and 11x11 windows."""
+    that level's GetHeightStep, every level with the 7x7 and 11x11 windows.
+
+    Level 4 searches +-3 sigma around truth + N(0, sigma) (6 sigma = K steps).
+    With `chain`, every finer level's ranges follow the previous level's
+    matches, coarse to fine as Matching_SETSM carries them: the previous
+    level's 7x7 records -> SelectMPs -> TINCreate_list (all on the GPU) ->
+    heights interpolated over the TIN at the level's nodes, each node
+    searching +-3 sigma (K steps) around its interpolated height.  The chain
+    runs once while the workload is built; the timed batch then matches every
+    level and window with these ranges.  Per-level chain statistics are kept
+    in the workload's `info`."""
     dev = torch.device(device)
     spec = synth.SceneSpec(seed=seed, image_size=image_size)
     scene = synth.make_scene(spec, device=dev, rows_per_chunk=512)
@@ -358,14 +498,29 @@ def build_c4(ctx, device: str = "cuda", seed: int = 1, image_size: int = 16384,
             pyr[ci].append(out)
     planes = [[_planes(ctx, pyr[ci][lv]) for lv in range(5)] for ci in range(2)]
     scene.images = []
-    levels = []
+    levels, info, prev = [], {"chain": bool(chain), "levels": []}, None
     for L in (4, 3, 2, 1, 0):
         k, spacing = C4_LEVELS[L]
         n = int(round(image_size * spec.gsd / spacing))
         grid = synth.make_grid(scene, n, spacing, device=dev)
         gd = _grid_dev(grid, dev)
         step = height_step(L, spec.gsd)
-        lo, hi, centre = synth.ranges_uniform(grid, k, step, k * step / 6.0, seed=seed + 10 + L)
+        lv_info = {"level": L, "grid": n, "k": k, "height_step": step}
+        if prev is None:
+            lo, hi, centre = synth.ranges_uniform(grid, k, step, k * step / 6.0,
+                                                  seed=seed + 10 + L)
+        else:
+            centre, covered = tin_heights(prev[0], prev[1], grid)
+            span = k * step
+            lo = np.floor(centre - span / 2).astype(np.int64)
+            hi = lo + int(round(span))
+            err = np.abs(centre - grid.truth)
+            lv_info.update(from_points=int(len(prev[0])), from_triangles=int(len(prev[1])),
+                           tin_covered=float(covered.mean()),
+                           centre_err_m_p50=float(np.median(err)),
+                           centre_err_m_p90=float(np.percentile(err, 90)),
+                           truth_in_range=float(((grid.truth >= lo) & (grid.truth <= hi)).mean()))
+        info["levels"].append(lv_info)
         ims = []
         for ci in range(2):
             im = dict(rpc=scene.rpcs[ci], **planes[ci][L])
@@ -377,5 +532,9 @@ def build_c4(ctx, device: str = "cuda", seed: int = 1, image_size: int = 16384,
             levels.append(_level_work(f"L{L}_T{t}", ims, grid, gd, lo, hi, centre,
                                       pyramid_step=L, template=t, step=step,
                                       resolution=spec.gsd, param=scene.param, dev=dev))
+        if chain and L > 0:
+            lw = levels[-len(templates)]        # the level's first window
+            prev = _match_level_points(ctx, lw, grid, dev)
+            lw.d_ncc.zero_()
     torch.cuda.synchronize(dev)
-    return MultiWorkload(name="c4", levels=levels, scenes=[scene])
+    return MultiWorkload(name="c4", levels=levels, scenes=[scene], info=info)

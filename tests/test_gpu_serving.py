@@ -20,7 +20,7 @@ def scenes(gpu_ctx):
 
 def stream(scenes, n=24, seed=5):
     return serving.poisson_requests(n, 400.0, scenes, seed=seed, grid_min=12, grid_max=96,
-                                    levels=(0, 1))
+                                    levels=(0, 1), templates=(11, 15))
 
 
 def test_mixed_batches_equal_requests_alone(gpu_ctx, scenes):

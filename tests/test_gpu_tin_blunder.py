@@ -197,3 +197,27 @@ def test_invalid_inputs_fail_and_leave_buffers(gpu_ctx):
         gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, -1.0, pts, det, tris, counts, zext)
     # the context stays usable
     gpu_ctx.blunder_detection_tin(inp, it, oncc, fb, cbl, hint, pts, det, tris, counts, zext)
+
+
+@pytest.mark.skipif(not refpy.available(), reason="reference build not available")
+@pytest.mark.parametrize("big", [1e308, float("inf")])
+def test_overflowing_height_sums_rerun_exactly(gpu_ctx, big, monkeypatch):
+    """One point with a huge or infinite height makes the edges' height
+    difference sums overflow: the device sets the threshold band to
+    [-inf, inf], so the point pass is re-run with the sequential sums (counted)
+    and the result is the reference build's."""
+    import copy
+    monkeypatch.delenv("SETSM_VLL_TIN_SUMS", raising=False)
+    inp, pts, tris, oncc = cases.make_tin_blunder_case(seed=41, size=768, nodes=40, res=7.0)
+    pts["z"][len(pts) // 2] = big
+    ref = copy.copy(inp)
+    ref.gridpt3 = inp.gridpt3.copy()
+    r_pts = pts.copy()
+    r_det, r_counts, r_zext = fresh_out(len(pts))
+    refpy.blunder_detection_tin(ref, 1, oncc.copy(), True, 1, 60.0, r_pts, r_det, tris.copy(),
+                                r_counts, r_zext)
+    det, counts, zext = fresh_out(len(pts))
+    before = vll.load().vll_tin_rerun_count(gpu_ctx._h)
+    gpu_ctx.blunder_detection_tin(inp, 1, oncc, True, 1, 60.0, pts, det, tris, counts, zext)
+    assert vll.load().vll_tin_rerun_count(gpu_ctx._h) == before + 1
+    assert_same(pts, det, inp.gridpt3, counts, zext, r_pts, r_det, ref.gridpt3, r_counts, r_zext)

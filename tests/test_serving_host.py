@@ -22,7 +22,8 @@ class _RS:
 
 def test_poisson_stream_shapes():
     scenes = [_RS(0), _RS(1)]
-    reqs = serving.poisson_requests(2000, 200.0, scenes, seed=3, levels=(0, 1))
+    reqs = serving.poisson_requests(2000, 200.0, scenes, seed=3, levels=(0, 1),
+                                    templates=(11, 15))
     arr = np.array([r.arrival for r in reqs])
     assert np.all(np.diff(arr) > 0)
     rate = len(reqs) / arr[-1]
@@ -34,6 +35,7 @@ def test_poisson_stream_shapes():
     # log-uniform: about half the requests below the geometric mean
     assert 0.4 < np.mean(ks < np.sqrt(8 * 512)) < 0.6
     assert {r.sid for r in reqs} == {0, 1} and {r.level for r in reqs} == {0, 1}
+    assert {r.template for r in reqs} == {11, 15}
 
 
 def test_admission_respects_budget_in_arrival_order():

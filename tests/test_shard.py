@@ -92,7 +92,10 @@ def _rank_main(rank, world, port, result_path):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_gather_the_grid(tmp_path):
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_gather_the_grid(tmp_path, world):
+    """Bands matched by `world` gloo ranks and gathered with
+    all_gather_into_tensor (3 ranks: unequal bands, padded to the largest)."""
     import socket
 
     import torch.multiprocessing as mp
@@ -100,7 +103,7 @@ def test_two_gloo_ranks_gather_the_grid(tmp_path):
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
     path = str(tmp_path / "ncc.npy")
-    mp.start_processes(_rank_main, args=(2, port, path), nprocs=2, join=True,
+    mp.start_processes(_rank_main, args=(world, port, path), nprocs=world, join=True,
                        start_method="spawn")
     inp = cases.make_case(**GLOO_CASE)
     ncc_full, acc_full = full_result(inp)
