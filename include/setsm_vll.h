@@ -306,8 +306,9 @@ int64_t vll_launch_count(const vll_context *ctx);
  *   - Memory-tight route only (check_matching_rate = 1), stereo, levels
  *     without orthoimage GNCC; anything else returns VLL_ERR_UNSUPPORTED.
  *   - Grids whose per-node scratch (20 bytes a node) does not fit the 64 MiB
- *     array (about 3.3 M nodes) return VLL_ERR_CAPACITY before any output is
- *     written; `err_buf` receives a message.  The rest of the array holds
+ *     array beside the window kernel's per-warp slot scratch (2 KiB a warp,
+ *     about 3.5 MiB on a B200), about 3.1 M nodes, return VLL_ERR_CAPACITY
+ *     before any output is written; `err_buf` receives a message.  The rest of the array holds
  *     the FP32 values of the few nodes queued for the exact FP64 pass; a node
  *     that finds it full is evaluated wholly in FP64, so results never depend
  *     on its size (only the time does).

@@ -1749,6 +1749,8 @@ int set_max_h(const DevLevel *hl, int n) {
     return h;
 }
 
+int window_max_blocks_per_sm();
+
 cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const int32_t *node_k,
                           const double *gsum, const double *gcnt, float *pend_vals,
                           int64_t pend_cap, int64_t *pend_node, int64_t *pend_off,
@@ -1765,7 +1767,7 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, window_kernel, kWinWarps * 32, smem);
     if (tu.blocks_per_sm > 0 && tu.blocks_per_sm < per_sm) per_sm = tu.blocks_per_sm;
-    per_sm = std::max(1, std::min(per_sm, kWinMaxBlocksPerSm));
+    per_sm = std::max(1, std::min(per_sm, window_max_blocks_per_sm()));
     // nodes per queue access (their slot counts are read one per lane)
     const int grab = tu.grab > 0 ? std::min(tu.grab, 32) : 1;
     // the warps' slot scratch follows the pending buffer's pend_cap values
@@ -1819,13 +1821,28 @@ cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, cons
                         counters, ctl, s);
 }
 
+// Most window-kernel CTAs an SM can hold whatever the footprint budget (its
+// registers bound it; the launch never exceeds it).
+int window_max_blocks_per_sm() {
+    static int cached = 0;
+    if (!cached) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, window_kernel, kWinWarps * 32,
+                                                          win_boxes_offset()) != cudaSuccess ||
+            b < 1)
+            b = kWinMaxBlocksPerSm;
+        cached = std::min(b, kWinMaxBlocksPerSm);
+    }
+    return cached;
+}
+
 // Floats of per-warp slot scratch the window kernel needs after the pending
 // buffer's values: kSlotCap per warp of the largest grid on this device.
 int64_t window_scratch_floats() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return (int64_t)sms * kWinMaxBlocksPerSm * kWinWarps * kSlotCap;
+    return (int64_t)sms * window_max_blocks_per_sm() * kWinWarps * kSlotCap;
 }
 
 // Slots of FP32 values the pending buffer holds for a pass of n_slots slots:
