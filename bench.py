@@ -428,7 +428,7 @@ def run_ours(args):
         # per GPU and window set; results do not depend on the tuning)
         from setsm_b200 import autotune
         ios = [wl.device_band_io(t, args.tune_rows) for t in templates]
-        tuned = autotune.tune(ctx, ios, repeats=1)
+        tuned = autotune.tune(ctx, ios, repeats=2)
         log(f"[rank {rank}] tuning {tuned['tuning']} ({tuned.get('tuned_s', 'cached')} s)")
 
     def one_step(kernel, stats=True):
@@ -632,7 +632,7 @@ def run_multi(args):
     # tune on a spread of levels holding about 1e9 height slots
     slots = [lv.slots(lv.host_desc_kwargs["step"]) for lv in mw.levels]
     stride = max(1, int(math.ceil(sum(slots) / 1e9)))
-    tuned = autotune.tune(ctx, ios[::stride], repeats=1)
+    tuned = autotune.tune(ctx, ios[::stride], repeats=2)
     log(f"[rank {rank}] tuning {tuned['tuning']} ({tuned.get('tuned_s', 'cached')} s)")
     acc, st0 = ctx.batch(ios)
     evals_step = int(st0.evals)
@@ -1656,6 +1656,55 @@ def run_shard(args):
         dist.destroy_process_group()
 
 
+def run_phase_cycles(args):
+    """Where the window kernel's time goes, on the config's workload: the
+    library built with the phase counters
+    (setsm_b200/build.py build_phase_cycles) runs each window once after a
+    warm-up, and the line gives per 32-slot group the warp cycles of each
+    phase and their shares.  The counters add a clock read per phase, so the
+    launch time is reported beside the uninstrumented library's."""
+    import ctypes as C
+    import torch
+    from setsm_b200 import build as bld
+    from setsm_b200 import vll, workloads
+    names = ["tile_wait", "box_conversion", "node_setup", "geometry_and_tile_copies",
+             "window_statistics", "peak_scan_and_writes", "node_end"]
+    out = {}
+    for lib in (bld.LIB, bld.LIB_PHASES):
+        vll._lib = None
+        vll.LIB_PATH = lib
+        ctx = vll.Context(0)
+        wl = workloads.build(args.config, ctx, device="cuda:0", seed=1, keep_host=False)
+        torch.cuda.synchronize()
+        L = C.CDLL(lib)
+        for t in workloads.CONFIGS[args.config]["templates"]:
+            d = wl.device_desc(t)
+            ctx.vertical_line_locus_device(d, wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr(), None,
+                                           None, "split")
+            buf = (C.c_ulonglong * 16)()
+            if lib == bld.LIB_PHASES:
+                L.vll_window_phase_cycles(buf, 1)
+            wl.d_ncc.zero_()
+            torch.cuda.synchronize()
+            st = ctx.vertical_line_locus_device(d, wl.d_gp3.data_ptr(), wl.d_ncc.data_ptr(), None,
+                                                None, "split", stats=True)
+            w = out.setdefault(workloads.WINDOW_OF_TEMPLATE[t], {})
+            if lib == bld.LIB:
+                w["window_ms"] = st.window_ms
+                continue
+            L.vll_window_phase_cycles(buf, 1)
+            groups, nodes = int(buf[8]), int(buf[9])
+            tot = sum(buf[i] for i in range(7))
+            w.update({"window_ms_instrumented": st.window_ms, "groups": groups, "nodes": nodes,
+                      "cycles_per_group": {n: buf[i] / max(groups, 1) for i, n in enumerate(names)},
+                      "share": {n: buf[i] / max(tot, 1) for i, n in enumerate(names)}})
+        ctx.close()
+        del wl
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": "window kernel warp cycles per 32-slot group, by phase",
+                      "config": args.config, "windows": out}), flush=True)
+
+
 def cases_field_mismatch(got, want) -> dict:
     """Mismatching records per NCCresult field (numpy structured arrays)."""
     out = {}
@@ -1682,6 +1731,9 @@ def main():
                              "blunder", "ortho_tin", "height_range", "select_mps",
                              "voxel_iter", "tin_blunder"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
+    ap.add_argument("--phase-cycles", action="store_true",
+                    help="the window kernel's per-phase warp cycles on the config's scene "
+                         "(the library built with the phase counters)")
     ap.add_argument("--shard", action="store_true",
                     help="one scene split into grid-row bands over the ranks (strong scaling)")
     ap.add_argument("--e2e-steps", type=int, default=0,
@@ -1706,6 +1758,8 @@ def main():
         args.e2e_steps = args.steps
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.phase_cycles:
+        run_phase_cycles(args)
     elif args.shard:
         run_shard(args)
     elif args.config in ("c3", "c4"):

@@ -18,6 +18,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libsetsm_vll.so")
+# the same library with the window kernel's phase counters compiled in
+# (VLL_PHASE_CYCLES; bench.py --phase-cycles reads them)
+LIB_PHASES = os.path.join(LIBDIR, "libsetsm_vll_phases.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC,
@@ -87,5 +90,35 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
     return LIB
 
 
+def build_phase_cycles(verbose: bool = False, force: bool = False) -> str:
+    """lib/libsetsm_vll_phases.so: the library with vll_split.cu compiled
+    with -DVLL_PHASE_CYCLES (the other objects are the default build's)."""
+    build(verbose=verbose, force=force)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    src = os.path.join(CSRC, "vll_split.cu")
+    obj = os.path.join(BUILD, "vll_split_phases.o")
+    nv = nvcc()
+    if force or _stale(obj, [src] + headers):
+        cmd = [nv, *ARCH, *COMMON, "-DVLL_PHASE_CYCLES", "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed on vll_split.cu (phase counters)")
+    objs = [obj if s_ == "vll_split.cu" else os.path.join(BUILD, s_.replace(".cu", ".o"))
+            for s_ in SOURCES]
+    if force or _stale(LIB_PHASES, objs):
+        r = subprocess.run([nv, *ARCH, "-shared", "-o", LIB_PHASES, *objs, "-lcudart"],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("link failed (phase counters)")
+    return LIB_PHASES
+
+
 if __name__ == "__main__":
-    build(verbose=True, ptxas_info="-v" in sys.argv, force="-f" in sys.argv)
+    if "--phase-cycles" in sys.argv:
+        build_phase_cycles(verbose=True, force="-f" in sys.argv)
+    else:
+        build(verbose=True, ptxas_info="-v" in sys.argv, force="-f" in sys.argv)

@@ -487,6 +487,40 @@ constexpr uint32_t kNfVec = 32u;      // image rows 16-byte aligned (vector stag
 constexpr uint32_t kNfTma = 64u;      // the level has tensor maps for its footprints
 constexpr uint32_t kNfDbg = 128u;     // per-slot debug values written
 
+// Optional instrumentation of the window kernel's phases (compiled with
+// -DVLL_PHASE_CYCLES: `python -m setsm_b200.build --phase-cycles` builds
+// lib/libsetsm_vll_phases.so).  Each warp sums clock64 deltas per phase
+// (0 tile wait, 1 box conversion, 2 node set-up, 3 geometry and tile copies,
+// 4 window statistics, 5 FindPeakNcc scan and writes, 6 node end) and counts
+// groups and nodes; vll_window_phase_cycles reads the totals.  The kernel's
+// work is the same with and without it.
+#ifdef VLL_PHASE_CYCLES
+__device__ unsigned long long g_phase_cycles[16];
+#define PHASE_DECL                                 \
+    unsigned long long ph_[8] = {}, ph_n_[2] = {}; \
+    long long ph_t_ = clock64()
+#define PHASE(i)                                             \
+    do {                                                     \
+        const long long t_ = clock64();                      \
+        ph_[i] += (unsigned long long)(t_ - ph_t_);          \
+        ph_t_ = t_;                                          \
+    } while (0)
+#define PHASE_COUNT(i) (++ph_n_[i])
+#define PHASE_FLUSH()                                                      \
+    do {                                                                   \
+        if (lane == 0) {                                                   \
+            for (int i_ = 0; i_ < 8; ++i_) atomicAdd(&g_phase_cycles[i_], ph_[i_]); \
+            atomicAdd(&g_phase_cycles[8], ph_n_[0]);                       \
+            atomicAdd(&g_phase_cycles[9], ph_n_[1]);                       \
+        }                                                                  \
+    } while (0)
+#else
+#define PHASE_DECL (void)0
+#define PHASE(i) (void)0
+#define PHASE_COUNT(i) (void)0
+#define PHASE_FLUSH() (void)0
+#endif
+
 // Per-node state of the window kernel in shared memory: the RPC cubics, the
 // level constants the slot loop reads (here rather than from the level block
 // in global memory), the record folded by lane 0 and the streamed scan's
@@ -532,6 +566,7 @@ struct WinShared {
     uint32_t zl[kZeroCap];            // zero intensity texels of the staged boxes
     int zn;                           // their count (more than kZeroCap: not listed)
     uint64_t mbar;                    // completion of the group's tile copies
+    const DevLevel *tmap_level;       // level whose tensor maps lane 0 has acquired
 };
 
 __host__ __device__ constexpr size_t win_level_offset() {
@@ -669,11 +704,6 @@ __device__ __noinline__ void node_setup(NodeCtx &N, const LevelSet &LS, int lvl,
             N.pre_dir = 0;
             N.pre_k = -1;
             N.have = 0;
-        } else if (lane == 27 && (lc->flags & kNfTma)) {
-            tmap_acquire(P.tmap[0][0]);
-            tmap_acquire(P.tmap[0][1]);
-            tmap_acquire(P.tmap[1][0]);
-            tmap_acquire(P.tmap[1][1]);
         }
         __syncwarp();
         return;
@@ -740,12 +770,6 @@ __device__ __noinline__ void node_setup(NodeCtx &N, const LevelSet &LS, int lvl,
         N.pre_dir = 0;
         N.pre_k = -1;
         N.have = 0;
-    } else if (lane == 11 && P.tma_w[0] > 0) {
-        // tensor maps written by the host: visible to this lane's copies
-        tmap_acquire(P.tmap[0][0]);
-        tmap_acquire(P.tmap[0][1]);
-        tmap_acquire(P.tmap[1][0]);
-        tmap_acquire(P.tmap[1][1]);
     }
     __syncwarp();
 }
@@ -814,8 +838,9 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     const LevelSet LS, const int32_t *__restrict__ node_k, const double *__restrict__ gsum,
     const double *__restrict__ gcnt, float *__restrict__ pend_vals, int64_t pend_cap,
     int64_t *__restrict__ pend_node, int64_t *__restrict__ pend_off,
-    float *__restrict__ warp_vals, unsigned long long *__restrict__ counters,
-    unsigned long long *__restrict__ ctl, int warp_quads, int warp_raw, int grab) {
+    float *__restrict__ warp_vals, int64_t *__restrict__ fix_list, int64_t fix_cap,
+    unsigned long long *__restrict__ counters, unsigned long long *__restrict__ ctl,
+    int warp_quads, int warp_raw, int grab) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -828,7 +853,10 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     float *wv = warp_vals + ((size_t)blockIdx.x * kWinWarps + warp) * kSlotCap;
     LevelConst &LC = *reinterpret_cast<LevelConst *>(smem_raw + win_level_offset());
     level_const_load(LC, LS.lv[0]);
-    if (lane == 0) mbar_init(&W.mbar);
+    if (lane == 0) {
+        mbar_init(&W.mbar);
+        W.tmap_level = nullptr;
+    }
     __syncthreads();
     uint32_t phase = 0;   // parity of the mbarrier phase the next copies complete
     unsigned long long evals = 0;
@@ -853,6 +881,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     float vmax = -100.0f, amb = -INFINITY, amb_peak = -INFINITY;
     float b1 = -INFINITY, b2 = -INFINITY;
     bool need = false;
+    PHASE_DECL;
     for (;;) {
         const int st = nst;
         const uint32_t ro = nro, to = nto;
@@ -874,6 +903,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     return;
                 }
                 phase ^= 1u;
+                PHASE(0);
                 const int tw0 = C.tma_w[0], tw1 = C.tma_w[1];
                 const int rtile = (tw0 * C.tma_h[0] * 2 + 127) & ~127;   // bytes per plane tile
                 const int ttile = (tw1 * C.tma_h[1] * 2 + 127) & ~127;
@@ -934,6 +964,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             }
             staged = true;
         }
+        PHASE(1);
 
         // ---- fetch the next group: node, geometry, boxes, tile copies ----
         bool have_next = false;
@@ -982,6 +1013,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 break;
             }
         }
+        PHASE(2);
         nmode = 0;
         if (have_next) {
             const NodeCtx &N = W.node[pb];
@@ -1071,6 +1103,16 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     nmode = 1;
                     if (lane == 0) {
                         const DevLevel &P = *N.P;
+                        if (&P != W.tmap_level) {
+                            // the level's tensor maps were written by the host
+                            // (the level block is reused between calls): make
+                            // them visible to this thread's copies
+                            tmap_acquire(P.tmap[0][0]);
+                            tmap_acquire(P.tmap[0][1]);
+                            tmap_acquire(P.tmap[1][0]);
+                            tmap_acquire(P.tmap[1][1]);
+                            W.tmap_level = &P;
+                        }
                         unsigned char *rI = raw, *rM = raw + rtile;
                         unsigned char *tIr = raw + 2 * rtile, *tMr = tIr + ttile;
                         mbar_arrive_expect(&W.mbar, (uint32_t)(2 * (tw0 * th0 + tw1 * th1) * 2));
@@ -1085,6 +1127,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             }
         }
 
+        PHASE(3);
         // ---- evaluate the current group ----
         if (have_cur) {
             NodeCtx &C = W.node[cb];
@@ -1151,6 +1194,7 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 evals++;
             }
 
+            PHASE(4);
             // ---- FindPeakNcc streamed over this group of 32 slots ----
             // (setsm_code.cpp:6672-6752 on the FP32 values; every decision
             // within the error band, and every value the FP32 pass could not
@@ -1158,8 +1202,17 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             // near an integer, NaN --, sends the node to the exact pass)
             const bool voxels = (flags & kNfVox) != 0;
             const bool ev = k < K && status == 2;
-            const bool unusable = ev && (isnan(incc_v) || isnan(rho_v) ||
-                                         (voxels && near_trunc((double)incc_v)));
+            // a voxel INCC whose truncation FP32 cannot decide needs only its
+            // own exact value: the slot is listed for slot_fix_kernel (or,
+            // the list full, taken as unusable)
+            bool unusable = ev && (isnan(incc_v) || isnan(rho_v));
+            if (ev && !unusable && voxels && near_trunc((double)incc_v)) {
+                const unsigned long long q = atomicAdd(&ctl[5], 1ull);
+                if ((int64_t)q < fix_cap)
+                    fix_list[q] = C.gn * kSlotCap + k;
+                else
+                    unusable = true;
+            }
             if (k < K) wv[k] = unusable ? __int_as_float(0x7fc00000) : rho_v;
             bool band = unusable;
             const uint32_t em = __ballot_sync(0xffffffffu, ev);
@@ -1250,7 +1303,10 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 }
             }
             __syncwarp();
+            PHASE(5);
+            PHASE_COUNT(0);
             if (ck0 + 32 >= K) {
+                PHASE_COUNT(1);
                 // ---- the node's last group: write it, or queue it ----
                 // the maximum, and roundings that could change the maximum or
                 // the top two (a peak more than 0.002 + 2 bands below the
@@ -1298,13 +1354,49 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                 __syncwarp();
             }
         }
+        PHASE(6);
         if (!have_next) break;
         have_cur = true;
         cb = pb;
         ck0 = pk0;
     }
+    PHASE_FLUSH();
     for (int o = 16; o; o >>= 1) evals += __shfl_down_sync(0xffffffffu, evals, o);
     if (lane == 0 && evals) atomicAdd(&counters[1], evals);
+}
+
+// ---------------------------------------------------------------------------
+// slot fix: exact voxel INCC of the listed slots
+// ---------------------------------------------------------------------------
+// One lane per slot listed by the window kernel (node * kSlotCap + slot):
+// the slot is evaluated in exact FP64 (eval_slot, the reference's operation
+// order) and its voxel's INCC rewritten; the node's other outputs did not
+// depend on the truncation.
+__global__ void __launch_bounds__(128) slot_fix_kernel(const LevelSet LS,
+                                                       const int64_t *__restrict__ fix_list,
+                                                       int64_t fix_cap,
+                                                       const double *__restrict__ gsum,
+                                                       const double *__restrict__ gcnt,
+                                                       const unsigned long long *__restrict__ ctl) {
+    const int64_t n = min((int64_t)ctl[5], fix_cap);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = fix_list[i];
+        const int64_t gn = e / kSlotCap;
+        const int k = (int)(e - gn * kSlotCap);
+        const int lvl = level_of(LS, gn);
+        const DevLevel &P = LS.lv[lvl];
+        const int64_t pt = gn - __ldg(LS.base + lvl);
+        PatchSrc S, Sn;
+        make_src(P, 1, S, Sn);
+        const int start_H = P.gp3[pt].minHeight;
+        const float hgt = slot_height(P, start_H, P.ncc[pt].minHeight, k);
+        const double cnt_g = gcnt ? gcnt[gn] : 0.0, sum_g = gsum ? gsum[gn] : 0.0;
+        const SlotOut o = eval_slot(P, pt, 1, S, Sn, hgt, cnt_g, sum_g);
+        if (o.evaluated)
+            P.vox[P.vox_off[pt] + k].INCC =
+                o.count_incc > 0 ? q_voxel(__ddiv_rn(o.sum_incc, o.count_incc)) : q_voxel(-1.0);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1750,10 +1842,12 @@ int set_max_h(const DevLevel *hl, int n) {
 }
 
 int window_max_blocks_per_sm();
+int64_t window_scratch_floats();
 
 cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const int32_t *node_k,
                           const double *gsum, const double *gcnt, float *pend_vals,
                           int64_t pend_cap, int64_t *pend_node, int64_t *pend_off,
+                          int64_t *fix_list, int64_t fix_cap,
                           unsigned long long *counters, unsigned long long *ctl,
                           const SplitTuning &tu, cudaStream_t s) {
     const WarpBudget wb = set_warp_budget(hl, n, tu.box_margin);
@@ -1775,8 +1869,9 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
     float *warp_vals = pend_vals + pend_cap;
     window_kernel<<<sms * per_sm, kWinWarps * 32, smem, s>>>(LS, node_k, gsum, gcnt, pend_vals,
                                                              pend_cap, pend_node, pend_off,
-                                                             warp_vals, counters, ctl, wb.quads,
-                                                             wb.raw, grab);
+                                                             warp_vals, fix_list, fix_cap,
+                                                             counters, ctl, wb.quads, wb.raw,
+                                                             grab);
     return cudaGetLastError();
 }
 
@@ -1808,11 +1903,23 @@ cudaError_t launch_peaks(const LevelSet &LS, int max_h, const int32_t *node_k,
 cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, const int32_t *node_k,
                              const double *gsum, const double *gcnt, float *pend_vals,
                              int64_t pend_cap, int64_t *pend_node, int64_t *pend_off,
-                             unsigned long long *counters, unsigned long long *ctl,
-                             const SplitTuning &tu, cudaStream_t s, SplitTiming *tm) {
+                             int64_t fix_cap, unsigned long long *counters,
+                             unsigned long long *ctl, const SplitTuning &tu, cudaStream_t s,
+                             SplitTiming *tm) {
+    // the voxel slots listed for an exact INCC follow the warps' scratch
+    int64_t *fix_list = reinterpret_cast<int64_t *>(
+        pend_vals + ((pend_cap + window_scratch_floats() + 1) & ~(int64_t)1));
     cudaError_t e = launch_window(hl, n, LS, node_k, gsum, gcnt, pend_vals, pend_cap, pend_node,
-                                  pend_off, counters, ctl, tu, s);
+                                  pend_off, fix_list, fix_cap, counters, ctl, tu, s);
     if (e != cudaSuccess) return e;
+    if (fix_cap > 0) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        slot_fix_kernel<<<sms * 8, 128, 0, s>>>(LS, fix_list, fix_cap, gsum, gcnt, ctl);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     if (tm && tm->enabled) {
         cudaEventRecord(tm->ev[5], s);
         cudaEventRecord(tm->ev[6], s);
@@ -1931,6 +2038,7 @@ void split_release(SplitBuffers &b) {
     }
     b.cap_nodes = b.cap_slots = b.cap_scan = b.cap_levels = 0;
     b.pend_cap = 0;
+    b.fix_cap = 0;
 }
 
 #define SPLIT_CUDA(call)                       \
@@ -2032,22 +2140,29 @@ cudaError_t split_back(SplitBuffers &b, const DevLevel *hl, int n_levels, const 
     mark(4);
     cudaError_t e = window_and_peaks(hl, n_levels, LS, (const int32_t *)b.node_k, gsum, gcnt,
                                      (float *)b.rho, b.pend_cap, (int64_t *)b.pending,
-                                     (int64_t *)b.pend_off, counters,
+                                     (int64_t *)b.pend_off, b.fix_cap, counters,
                                      (unsigned long long *)b.ctl, tu, s, tm);
     if (e != cudaSuccess) {
         *err = "window / exact kernel launch";
         return e;
     }
-    *launches += 2;
+    *launches += 2 + (b.fix_cap > 0 ? 1 : 0);
     mark(7);
     mark(8);
     return cudaSuccess;
 }
 
+// Whether a level of the set writes voxel rows (the voxel route).
+bool voxel_route(const DevLevel *hl, int n) {
+    for (int l = 0; l < n; ++l)
+        if (hl[l].vox && !hl[l].cmr && !hl[l].is_ra) return true;
+    return false;
+}
+
 // Sizes the pending buffer from the slot total of a completed front phase
 // (one host wait).
 cudaError_t split_size(SplitBuffers &b, int64_t N, cudaStream_t s, std::string *err,
-                       int64_t *n_slots) {
+                       int64_t *n_slots, bool voxel_route) {
     int64_t total = 0;
     SPLIT_CUDA(cudaMemcpyAsync(&total, (int64_t *)b.slot_off + N, 8, cudaMemcpyDeviceToHost, s));
     SPLIT_CUDA(cudaStreamSynchronize(s));
@@ -2057,10 +2172,17 @@ cudaError_t split_size(SplitBuffers &b, int64_t N, cudaStream_t s, std::string *
         return cudaErrorInvalidValue;
     }
     const int64_t cap = pending_capacity(total);
+    // voxel-route levels list the slots whose INCC truncation needs an exact
+    // value (about 1 %; a slot that finds the list full goes to the exact pass)
+    const int64_t fix = voxel_route ? std::min<int64_t>(total, std::max<int64_t>(total / 32, 1 << 20))
+                                    : 0;
     size_t c = b.cap_slots;
-    SPLIT_CUDA(grow(b.rho, c, (size_t)(cap + window_scratch_floats()) * sizeof(float)));
+    SPLIT_CUDA(grow(b.rho, c,
+                    (size_t)(((cap + window_scratch_floats() + 1) & ~(int64_t)1) + 2 * fix) *
+                        sizeof(float)));
     b.cap_slots = c;
     b.pend_cap = cap;
+    b.fix_cap = fix;
     return cudaSuccess;
 }
 
@@ -2075,7 +2197,7 @@ cudaError_t run_split_set(SplitBuffers &b, const DevLevel *hl, const DevLevel *d
                                 &launches);
     if (e != cudaSuccess) return e;
     int64_t n_slots = 0;
-    e = split_size(b, LS.total, s, err, &n_slots);
+    e = split_size(b, LS.total, s, err, &n_slots, voxel_route(hl, n_levels));
     if (e != cudaSuccess) return e;
     e = split_back(b, hl, n_levels, LS, gsum, gcnt, counters, tu, s, err, tm, &launches);
     if (e != cudaSuccess) return e;
@@ -2107,7 +2229,7 @@ cudaError_t split_plan(SplitPlan &pl, SplitBuffers &b, const DevLevel *hl, const
     e = split_front(b, hl, dl, n_levels, counters, s, err, nullptr, &LS, &gsum, &gcnt,
                                 &launches);
     if (e != cudaSuccess) return e;
-    e = split_size(b, LS.total, s, err, &pl.n_slots);
+    e = split_size(b, LS.total, s, err, &pl.n_slots, voxel_route(hl, n_levels));
     if (e != cudaSuccess) return e;
     if (pl.exec) {
         cudaGraphExecDestroy(pl.exec);
@@ -2325,7 +2447,7 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
                                                           acc_level);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(window_and_peaks(&P, 1, LS, node_k, nullptr, nullptr, pend_vals, pend_cap, pending,
-                             pend_off, counters, ctl, SplitTuning(), s, nullptr));
+                             pend_off, 0, counters, ctl, SplitTuning(), s, nullptr));
     unsigned long long acc = 0;
     NA_CUDA(cudaMemcpyAsync(&acc, counters, sizeof(acc), cudaMemcpyDeviceToHost, s));
     NA_CUDA(cudaStreamSynchronize(s));
@@ -2333,3 +2455,19 @@ extern "C" int vll_vertical_line_locus_noalloc(const vll_level_desc *desc,
     if (accessable_grid) *accessable_grid = (int64_t)acc;
     return VLL_OK;
 }
+
+#ifdef VLL_PHASE_CYCLES
+// The window kernel's phase totals of the instrumented build (see
+// VLL_PHASE_CYCLES): out[0..6] warp cycles per phase, out[8] groups,
+// out[9] nodes, summed over the launches since the last reset.
+extern "C" int vll_window_phase_cycles(unsigned long long *out, int reset) {
+    if (out && cudaMemcpyFromSymbol(out, vll::g_phase_cycles, 16 * sizeof(unsigned long long)) !=
+                   cudaSuccess)
+        return -1;
+    if (reset) {
+        static const unsigned long long zero[16] = {};
+        if (cudaMemcpyToSymbol(vll::g_phase_cycles, zero, sizeof zero) != cudaSuccess) return -1;
+    }
+    return 0;
+}
+#endif

@@ -17,7 +17,8 @@ struct SplitBuffers {
     void *node_k = nullptr;        // int32  [N+1] slots per active node (0 = inactive)
     void *slot_off = nullptr;      // int64  [N+1] prefix sum of node_k (the slot total)
     void *rho = nullptr;           // float  [pend_cap] FP32 slot values of queued nodes, then
-                                   // the window kernel's per-warp slot scratch
+                                   // the window kernel's per-warp slot scratch, then the
+                                   // voxel slots listed for an exact INCC (int64 [fix_cap])
     void *gsum = nullptr;          // double [N] GNCC sums (FP64)
     void *gcnt = nullptr;          // double [N]
     void *scan_tmp = nullptr;      // cub temporary storage
@@ -28,6 +29,7 @@ struct SplitBuffers {
     void *acc_level = nullptr;     // uint64 [levels+1] Accessable_grid of each level
     size_t cap_nodes = 0, cap_slots = 0, cap_scan = 0, cap_levels = 0;
     int64_t pend_cap = 0;          // slots of rho in use
+    int64_t fix_cap = 0;           // int64 entries of the voxel slot-fix list after them
     std::vector<int64_t> h_base;   // host copy of the level table
     bool capturing = false;        // enqueueing into a stream capture
 };

@@ -409,6 +409,20 @@ def tin_heights(pts: np.ndarray, tris: np.ndarray, grid) -> tuple:
     W, Hn, res = grid.width, grid.height, grid.resolution
     x0, y0 = grid.boundary[0], grid.boundary[1]
     h = np.full(W * Hn, np.nan)
+
+    def fill(X, Y, Z, det, c, r):
+        # barycentric coordinates of nodes (c, r) in their triangles' rows
+        m = (c >= 0) & (c < W) & (r >= 0) & (r < Hn)
+        if not m.any():
+            return
+        X, Y, Z, det, c, r = X[m], Y[m], Z[m], det[m], c[m], r[m]
+        px, py = x0 + c * res, y0 + r * res
+        l0 = ((Y[:, 1] - Y[:, 2]) * (px - X[:, 2]) + (X[:, 2] - X[:, 1]) * (py - Y[:, 2])) / det
+        l1 = ((Y[:, 2] - Y[:, 0]) * (px - X[:, 2]) + (X[:, 0] - X[:, 2]) * (py - Y[:, 2])) / det
+        l2 = 1.0 - l0 - l1
+        inside = (l0 >= -1e-9) & (l1 >= -1e-9) & (l2 >= -1e-9)
+        h[(r * W + c)[inside]] = (l0 * Z[:, 0] + l1 * Z[:, 1] + l2 * Z[:, 2])[inside]
+
     if len(tris):
         v = np.stack([tris["a"], tris["b"], tris["c"]], 1).astype(np.int64)
         X, Y, Z = pts["x"][v], pts["y"][v], pts["z"][v]          # [T, 3]
@@ -419,21 +433,22 @@ def tin_heights(pts: np.ndarray, tris: np.ndarray, grid) -> tuple:
         c1 = np.floor((X.max(1) - x0) / res).astype(np.int64)
         r0 = np.ceil((Y.min(1) - y0) / res).astype(np.int64)
         r1 = np.floor((Y.max(1) - y0) / res).astype(np.int64)
-        span = int(max(1, (c1 - c0).max(initial=0) + 1, (r1 - r0).max(initial=0) + 1))
-        for dr in range(span):
-            for dc in range(span):
-                c, r = c0 + dc, r0 + dr
-                m = (c <= c1) & (r <= r1) & (c >= 0) & (c < W) & (r >= 0) & (r < Hn)
-                if not m.any():
-                    continue
-                px, py = x0 + c[m] * res, y0 + r[m] * res
-                Xm, Ym, Zm, dm = X[m], Y[m], Z[m], det[m]
-                l0 = ((Ym[:, 1] - Ym[:, 2]) * (px - Xm[:, 2]) + (Xm[:, 2] - Xm[:, 1]) * (py - Ym[:, 2])) / dm
-                l1 = ((Ym[:, 2] - Ym[:, 0]) * (px - Xm[:, 2]) + (Xm[:, 0] - Xm[:, 2]) * (py - Ym[:, 2])) / dm
-                l2 = 1.0 - l0 - l1
-                inside = (l0 >= -1e-9) & (l1 >= -1e-9) & (l2 >= -1e-9)
-                idx = (r[m] * W + c[m])[inside]
-                h[idx] = (l0 * Zm[:, 0] + l1 * Zm[:, 1] + l2 * Zm[:, 2])[inside]
+        span = np.maximum(c1 - c0, r1 - r0) + 1
+        small = span <= 8
+        # small triangles: every offset of an 8 x 8 box, vectorised over them
+        for dr in range(8):
+            for dc in range(8):
+                sel = small & (c0 + dc <= c1) & (r0 + dr <= r1)
+                if sel.any():
+                    fill(X[sel], Y[sel], Z[sel], det[sel], c0[sel] + dc, r0[sel] + dr)
+        # the few large ones (long triangles along the hull): each over its box
+        for t in np.nonzero(~small)[0]:
+            cc, rr = np.meshgrid(np.arange(max(c0[t], 0), min(c1[t], W - 1) + 1),
+                                 np.arange(max(r0[t], 0), min(r1[t], Hn - 1) + 1))
+            n = cc.size
+            if n:
+                rep = lambda a: np.repeat(a[t:t + 1], n, axis=0)
+                fill(rep(X), rep(Y), rep(Z), np.repeat(det[t], n), cc.ravel(), rr.ravel())
     covered = np.isfinite(h)
     if (~covered).any() and len(pts):
         from scipy.spatial import cKDTree
