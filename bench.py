@@ -352,10 +352,10 @@ def _cuda() -> bool:
 
 
 # DRAM bytes per evaluation of the window kernel measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) on the reduced C2 workload
-# (--config c2_small): 1228.4 MB / 121.53 M evaluations (7x7), 1225.9 MB /
-# 121.28 M (11x11).  Traffic scales with the evaluations.
-DRAM_BYTES_PER_EVAL = {11: 1228.4e6 / 121.53e6, 15: 1225.9e6 / 121.28e6}
+# (dram__bytes_read.sum + dram__bytes_write.sum, a one-pass capture) on the
+# full C2 launches: 4556.3 MB / 1993.23 M evaluations (7x7), 4637.4 MB /
+# 1992.24 M (11x11).
+DRAM_BYTES_PER_EVAL = {11: 4556.3e6 / 1993.23e6, 15: 4637.4e6 / 1992.24e6}
 
 
 def traffic_per_launch(evals_step: dict, templates) -> float:
@@ -586,8 +586,9 @@ def run_ours(args):
                          "traffic": traffic_per_launch(evals_step, templates),
                          "traffic_unit": "bytes per window launch (mean of the step's windows)",
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           "of the window kernel on the reduced C2 case, scaled "
-                                           "by evaluations (ncu, reduced C2 case)",
+                                           "of the window kernel's full C2 launches (one-pass "
+                                           "capture), per evaluation, times this step's "
+                                           "evaluations",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                          "kernel": "window_kernel", "per_window": per_window},
             "e2e": e2e,
@@ -948,6 +949,79 @@ def tin_workload(ctx):
     g0["Matched_flag"] = np.where(r < 0.2, 0, np.where(r < 0.4, 4, 1))
     g0["Mean_ortho_ncc"] = rng.integers(-1000, 1000, n).astype(np.int16)
     return inp, g0, pts0, delaunay(pts0)
+
+
+def run_tin_create(args):
+    """TINCreate_list (SubFunctions.cpp:2768-2846) on matched points of the
+    reduced C2 grid (1024^2 nodes at 2 m): 2 % of the nodes (21 k points, the
+    TIN workload's) and 50 % of them (524 k points), snapped to the grid.
+    GPU: vll_tin_create_device on resident points (CUDA events); e2e: the
+    host-buffer call; CPU: the reference's own TINCreate_list; the triangle
+    lists compared (identical, in order).  Metric: points per second."""
+    world, rank, local = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    import torch
+    from oracle import refpy
+    from setsm_b200 import abi, vll, workloads
+    ctx = vll.Context(0)
+    inp, _, pts21, _ = tin_workload(ctx)
+    bound = np.asarray(inp.boundary, dtype=np.float64)
+    res = float(inp.grid_resolution)
+    rng = np.random.default_rng(9)
+    sel = np.sort(rng.choice(inp.n, size=inp.n // 2, replace=False))
+    pts_half = np.zeros(len(sel), dtype=abi.POINT3_DTYPE)
+    pts_half["x"], pts_half["y"] = inp.grid_pts[sel, 0], inp.grid_pts[sel, 1]
+    pts_half["z"] = inp.gridpt3["Height"][sel]
+    pts_half["flag"] = 1
+    rows = {}
+    for name, pts in (("2%", pts21), ("50%", pts_half)):
+        t = time.perf_counter()
+        want = refpy.tin_create(pts, bound, res)
+        cpu_s = time.perf_counter() - t
+        d_pts = torch.from_numpy(pts.view(np.uint8).copy()).cuda()
+        cap = 2 * len(pts) + 16
+        d_tris = torch.zeros(cap * abi.TRI_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        for _ in range(max(3, args.warmup)):
+            ctx.tin_create_device(d_pts.data_ptr(), len(pts), bound, res, d_tris.data_ptr(), cap)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            n = ctx.tin_create_device(d_pts.data_ptr(), len(pts), bound, res, d_tris.data_ptr(),
+                                      cap)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        got = d_tris[:n * abi.TRI_DTYPE.itemsize].cpu().numpy().view(abi.TRI_DTYPE)
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            host = ctx.tin_create(pts, bound, res)
+        e2e_ms = (time.perf_counter() - t) * 1e3 / args.steps
+        rows[name] = {"points": int(len(pts)), "triangles": int(n), "device_ms": ms,
+                      "points_per_s": len(pts) / (ms / 1e3), "e2e_ms": e2e_ms,
+                      "cpu_reference_ms": cpu_s * 1e3,
+                      "cpu_points_per_s": len(pts) / cpu_s,
+                      "identical_to_reference": bool(got.tobytes() == want.tobytes() and
+                                                     host.tobytes() == want.tobytes())}
+    big = rows["50%"]
+    line = {
+        "metric": "points/s (TINCreate_list)", "value": big["points_per_s"], "unit": "points/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+        "ms_per_step": big["device_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64 grid coordinates", "data": "synthetic",
+        "config": {"workload": "matched points snapped to the reduced C2 grid (1024^2 nodes at "
+                               "2 m): 2 % and 50 % of the nodes; value: the 50 % set"},
+        "sets": rows,
+        "e2e": {"value": big["points"] / (big["e2e_ms"] / 1e3), "unit": "points/s",
+                "h2d_bytes_per_step": big["points"] * abi.POINT3_DTYPE.itemsize,
+                "d2h_bytes_per_step": big["triangles"] * abi.TRI_DTYPE.itemsize},
+        "cpu_baseline": {"value": big["cpu_points_per_s"], "unit": "points/s", "cores": 1,
+                         "kind": "reference", "sample": "the same 50 % point set"},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
 
 
 def run_height_range(args):
@@ -1729,7 +1803,7 @@ def main():
     ap.add_argument("--config", default="c2",
                     choices=["c1", "c2", "c2_small", "c3", "c4", "c5", "sgm", "seeddem",
                              "blunder", "ortho_tin", "height_range", "select_mps",
-                             "voxel_iter", "tin_blunder"])
+                             "voxel_iter", "tin_blunder", "tin_create"])
     ap.add_argument("--kernel", default="split", choices=["split", "plain"])
     ap.add_argument("--phase-cycles", action="store_true",
                     help="the window kernel's per-phase warp cycles on the config's scene "
@@ -1778,6 +1852,8 @@ def main():
         run_select_mps(args)
     elif args.config == "voxel_iter":
         run_voxel_iter(args)
+    elif args.config == "tin_create":
+        run_tin_create(args)
     elif args.config == "tin_blunder":
         run_tin_blunder(args)
     else:
