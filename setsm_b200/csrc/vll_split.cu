@@ -1568,7 +1568,10 @@ __device__ __forceinline__ SlotOut eval_slot_warp_any(const DevLevel &P, int64_t
 // each, more a lane each); a node still unsettled after kMaxRounds, or
 // queued without its FP32 values, is evaluated wholly in FP64.
 // `max_h`: the largest window half-size of the level set (scratch layout).
-__global__ void __launch_bounds__(kPeakWarps * 32) peaks_kernel(
+#ifndef VLL_PEAK_MINB
+#define VLL_PEAK_MINB 3
+#endif
+__global__ void __launch_bounds__(kPeakWarps * 32, VLL_PEAK_MINB) peaks_kernel(
     const LevelSet LS, int max_h, const int32_t *__restrict__ node_k,
     const float *__restrict__ pend_vals, const int64_t *__restrict__ pend_node,
     const int64_t *__restrict__ pend_off, const double *__restrict__ gsum,
