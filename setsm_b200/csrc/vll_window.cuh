@@ -423,8 +423,9 @@ __device__ __forceinline__ void tmap_acquire(const void *tmap) {
 
 // Box texels of [x0, x0 + bw) x rows [0, bh) from the raw tiles in shared
 // memory: rawI / rawM hold, per box row (stride `nb` bytes), the uint16
-// texels from xa = x0 rounded down to 8 on.  One box texel per lane and
-// step: its two texels of each plane become {v(x), v(x+1) + dm * v(x)}
+// texels from xa = x0 rounded down to 8 on.  Two adjacent box texels per
+// lane and step (three loads per plane give both): each box texel's two
+// texels of each plane become {v(x), v(x+1) + dm * v(x)}
 // (dm = 0: reference pairs; dm = -1: target value and difference, exact for
 // integers), each value placed in the mantissa of 2^23 and shifted by
 // -(2^23 + shift) in one exact addition.  Zero intensity texels among the
@@ -439,40 +440,54 @@ __device__ __forceinline__ void convert_tile(float4 *__restrict__ dst, int ds,
                                              uint32_t tag, int lane) {
     const float2 ns = make_float2(-(8388608.0f + sI), -(8388608.0f + sM));
     const float2 dm2 = bc2(dm);
-    const int n = bw * bh;
     const unsigned char *rI = rawI + 2 * (x0 - xa);
     const unsigned char *rM = rawM + 2 * (x0 - xa);
-    // box texel (row by, column bx): the lane's first, then steps of 32
-    int by = lane / bw, bx = lane - by * bw;
-    const int dby = 32 / bw, dbx = 32 - dby * bw;
-    for (int q = lane; q < n; q += 32) {
+    // box texels (row by, columns bx = 2 bq and bx + 1): the lane's first
+    // pair, then steps of 32 pairs
+    const int bp = (bw + 1) >> 1;            // texel pairs per row
+    const int n2 = bp * bh;
+    int by = lane / bp, bq = lane - by * bp;
+    const int dby = 32 / bp, dbq = 32 - dby * bp;
+    for (int q = lane; q < n2; q += 32) {
+        const int bx = 2 * bq;
+        const bool two = bx + 1 < bw;
         const int ro = by * nb + 2 * bx;
         const uint32_t i0 = *reinterpret_cast<const uint16_t *>(rI + ro);
         const uint32_t i1 = *reinterpret_cast<const uint16_t *>(rI + ro + 2);
         const uint32_t m0 = *reinterpret_cast<const uint16_t *>(rM + ro);
         const uint32_t m1 = *reinterpret_cast<const uint16_t *>(rM + ro + 2);
-        const bool last = bx == bw - 1;   // the row's last texel also reads texel bw
-        if (i0 == 0 || (last && i1 == 0)) {
-            // rare: list the zero texels
-            if (i0 == 0) {
-                const int k = atomicAdd(zn, 1);
-                if (k < cap) zl[k] = tag | ((uint32_t)by << 16) | (uint32_t)bx;
-            }
-            if (last && i1 == 0) {
-                const int k = atomicAdd(zn, 1);
-                if (k < cap) zl[k] = tag | ((uint32_t)by << 16) | (uint32_t)(bx + 1);
-            }
+        const uint32_t i2 = two ? *reinterpret_cast<const uint16_t *>(rI + ro + 4) : 1u;
+        const uint32_t m2 = two ? *reinterpret_cast<const uint16_t *>(rM + ro + 4) : 0u;
+        // zero texels among those the box reads ([0, bw] of the row): this
+        // lane lists texels bx and bx + 1, and texel bx + 2 when it ends the
+        // row (otherwise the next pair lists it)
+        const bool end2 = two && bx + 2 == bw;
+        if (i0 == 0 || i1 == 0 || (end2 && i2 == 0)) {
+            const uint32_t t3[3] = {i0, i1, i2};
+#pragma unroll
+            for (int t = 0; t < 3; ++t)
+                if (t3[t] == 0 && (t < 2 || end2)) {
+                    const int k = atomicAdd(zn, 1);
+                    if (k < cap) zl[k] = tag | ((uint32_t)by << 16) | (uint32_t)(bx + t);
+                }
         }
         const float2 a = __fadd2_rn(make_float2(__int_as_float(i0 | 0x4B000000u),
                                                 __int_as_float(m0 | 0x4B000000u)), ns);
         const float2 b = __fadd2_rn(make_float2(__int_as_float(i1 | 0x4B000000u),
                                                 __int_as_float(m1 | 0x4B000000u)), ns);
-        const float2 h = __ffma2_rn(dm2, a, b);
-        dst[by * ds + bx] = make_float4(a.x, a.y, h.x, h.y);
-        bx += dbx;
+        float4 *d = dst + by * ds + bx;
+        const float2 h0 = __ffma2_rn(dm2, a, b);
+        d[0] = make_float4(a.x, a.y, h0.x, h0.y);
+        if (two) {
+            const float2 c = __fadd2_rn(make_float2(__int_as_float(i2 | 0x4B000000u),
+                                                    __int_as_float(m2 | 0x4B000000u)), ns);
+            const float2 h1 = __ffma2_rn(dm2, b, c);
+            d[1] = make_float4(b.x, b.y, h1.x, h1.y);
+        }
+        bq += dbq;
         by += dby;
-        if (bx >= bw) {
-            bx -= bw;
+        if (bq >= bp) {
+            bq -= bp;
             ++by;
         }
     }
