@@ -868,10 +868,12 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     int pb = 1, pk0 = 0, pK = 0;
     // the fetched group, per lane: status | inside << 2 | target radius << 8,
     // reference window and target centre offsets in the boxes (row << 16 |
-    // column), fractions and the rotation
+    // column), fractions, and the two orientation bytes (loaded when the
+    // group is fetched, read when it is evaluated: the loads' latency passes
+    // under the evaluation of the group before)
     int nst = 0;
-    uint32_t nro = 0, nto = 0;
-    float nrfx = 0.f, nrfy = 0.f, ntfx = 0.f, ntfy = 0.f, ncf = 1.f, nsf = 0.f;
+    uint32_t nro = 0, nto = 0, nor0 = 0, nor1 = 0;
+    float nrfx = 0.f, nrfy = 0.f, ntfx = 0.f, ntfy = 0.f;
     // ... and its boxes (warp-uniform): mode 0 none / 1 tiles / 2 loads
     int nmode = 0, nrx0 = 0, nry0 = 0, nrw = 0, nrbh = 0, ntx0 = 0, nty0 = 0, ntw = 0, ntbh = 0;
     // the group being evaluated
@@ -884,8 +886,8 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
     PHASE_DECL;
     for (;;) {
         const int st = nst;
-        const uint32_t ro = nro, to = nto;
-        const float rfx = nrfx, rfy = nrfy, tfx = ntfx, tfy = ntfy, cf = ncf, sf = nsf;
+        const uint32_t ro = nro, to = nto, or0 = nor0, or1 = nor1;
+        const float rfx = nrfx, rfy = nrfy, tfx = ntfx, tfy = ntfy;
         const int rbw = nrw | 1, rbh = nrbh, tbw = ntw | 1, tbh = ntbh;
         bool staged = false;
         // ---- stage the current group's boxes ----
@@ -1019,9 +1021,9 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             const NodeCtx &N = W.node[pb];
             const int k = pk0 + lane;
             const int H = N.H;
-            int status = 0;   // 0 idle/skip, 1 orientation reject, 2 evaluate
+            int status = 0;   // 0 idle/skip, 2 inside both images
             double2 rp = make_double2(0, 0), tp = make_double2(0, 0);
-            int rot = kRotOffset;
+            uint32_t o0 = 0, o1 = 0;
             if (k < N.K) {
                 const float hgt = (float)__dadd_rn(N.hbase, __dmul_rn((double)k, N.hstep));
                 if (hgt >= (float)N.start_H && hgt <= (float)N.end_H) {
@@ -1036,26 +1038,20 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     }
                     if (edge) slot_coords_exact(N, (double)hgt, rp, tp);
                     if (in_image(rp, N.w[0], N.h[0]) && in_image(tp, N.w[1], N.h[1])) {
-                        const int od = (int)N.ori[0][(int64_t)(int)rp.y * N.w[0] + (int)rp.x] -
-                                       (int)N.ori[1][(int64_t)(int)tp.y * N.w[1] + (int)tp.x];
-                        bool ok = true;
-                        if (N.flags & kNfOri) {
-                            const double a = __dmul_rn((double)od, N.bin_angle);
-                            ok = a < 90 && a > -90;
-                        }
-                        status = ok ? 2 : 1;
-                        rot = 2 * od + kRotOffset;
+                        o0 = N.ori[0][(int64_t)(int)rp.y * N.w[0] + (int)rp.x];
+                        o1 = N.ori[1][(int64_t)(int)tp.y * N.w[1] + (int)tp.x];
+                        status = 2;
                     }
                 }
             }
-            const float cfv = (float)N.P->rot_cos[rot], sfv = (float)N.P->rot_sin[rot];
             const int rix = (int)floor(rp.x), riy = (int)floor(rp.y);
             const int tix = (int)floor(tp.x), tiy = (int)floor(tp.y);
             // target footprint radius: the window is the square |col|, |row| <= H
             // cut by the disc of radius H + 1, so a rotation moves its samples
-            // at most min((|c| + |s|) H, H + 1) from the centre (+1 for the
-            // bilinear neighbour and FP32 rounding)
-            const int R = min((int)ceilf((fabsf(cfv) + fabsf(sfv)) * (float)H) + 1, H + 2);
+            // at most H + 1 from the centre (+1 for the bilinear neighbour and
+            // FP32 rounding); the bound holds for every rotation, so the boxes
+            // are placed before the orientation bytes arrive
+            const int R = H + 2;
             const bool inside = status == 2 && rix - H >= 0 && riy - H >= 0 &&
                                 rix + H + 2 < (int)N.w[0] && riy + H + 2 < (int)N.h[0] &&
                                 tix - R >= 0 && tiy - R >= 0 && tix + R + 2 < (int)N.w[1] &&
@@ -1075,8 +1071,8 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             nrfy = (float)(rp.y - (double)riy);
             ntfx = (float)(tp.x - (double)tix);
             ntfy = (float)(tp.y - (double)tiy);
-            ncf = cfv;
-            nsf = sfv;
+            nor0 = o0;
+            nor1 = o1;
             if (rx0 != INT_MAX) {
                 // pairs [x0, x1] of rows [y0, y1]; odd row strides spread
                 // consecutive rows over the shared-memory bank groups
@@ -1133,9 +1129,22 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
             NodeCtx &C = W.node[cb];
             const int K = C.K;
             const int k = ck0 + lane;
-            const int status = st & 3;
             const bool inside = (st & 4) != 0;
             const uint32_t flags = C.flags;
+            // the orientation difference (setsm_code.cpp:6395-6427): the
+            // angle test and the target window's rotation
+            int status = st & 3;
+            float cf = 1.f, sf = 0.f;
+            if (status == 2) {
+                const int od = (int)or0 - (int)or1;
+                if (flags & kNfOri) {
+                    const double a = __dmul_rn((double)od, C.bin_angle);
+                    if (!(a < 90 && a > -90)) status = 1;
+                }
+                const int rot = 2 * od + kRotOffset;
+                cf = (float)C.P->rot_cos[rot];
+                sf = (float)C.P->rot_sin[rot];
+            }
             // a zero intensity texel within the slot's footprints: the
             // reference drops the samples whose interpolated intensity is not
             // positive, which FP32 on shifted texels cannot decide
@@ -1254,28 +1263,39 @@ __global__ void __launch_bounds__(kWinWarps * 32, VLL_WIN_MINB) window_kernel(
                     ph_l = (float)__dadd_rn(C.hbase, __dmul_rn((double)p_slot, C.hstep));
                 }
                 uint32_t pm = __ballot_sync(0xffffffffu, is_peak);
-                while (pm) {
-                    const int b = __ffs(pm) - 1;
-                    pm &= pm - 1;
-                    const int16_t qpre = (int16_t)__shfl_sync(0xffffffffu, q_l, b);
-                    const float ph = __shfl_sync(0xffffffffu, ph_l, b);
-                    if (lane == 0) {
-                        vll_nccresult &R = C.R;
-                        if (R.result4 < 10) R.result4 += 1;
-                        if (R.result0 < qpre) {
-                            const double t1 = dq_result(R.result0);
-                            R.result0 = qpre;
-                            const float t2 = R.result2;
-                            R.result2 = ph;
-                            const int16_t q1 = q_result(t1);
-                            if (R.result1 < q1) {
-                                R.result1 = q1;
-                                R.result3 = t2;
+                if (pm) {
+                    // the fold in registers on every lane (the same values);
+                    // the replaced maximum re-quantised, q_result(dq_result(x)),
+                    // is x for every int16 x (|x / 1000 * 1000 - x| < 1e-11)
+                    vll_nccresult &R = C.R;
+                    int16_t r0 = R.result0, r1 = R.result1;
+                    float r2 = R.result2, r3 = R.result3;
+                    int r4 = R.result4;
+                    do {
+                        const int b = __ffs(pm) - 1;
+                        pm &= pm - 1;
+                        const int16_t qpre = (int16_t)__shfl_sync(0xffffffffu, q_l, b);
+                        const float ph = __shfl_sync(0xffffffffu, ph_l, b);
+                        if (r4 < 10) ++r4;
+                        if (r0 < qpre) {
+                            if (r1 < r0) {
+                                r1 = r0;
+                                r3 = r2;
                             }
-                        } else if (R.result1 < qpre) {
-                            R.result1 = qpre;
-                            R.result3 = ph;
+                            r0 = qpre;
+                            r2 = ph;
+                        } else if (r1 < qpre) {
+                            r1 = qpre;
+                            r3 = ph;
                         }
+                    } while (pm);
+                    __syncwarp();
+                    if (lane == 0) {
+                        R.result0 = r0;
+                        R.result1 = r1;
+                        R.result2 = r2;
+                        R.result3 = r3;
+                        R.result4 = (decltype(R.result4))r4;
                     }
                 }
                 // carry the last evaluated slot into the next group

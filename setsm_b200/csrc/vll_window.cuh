@@ -446,8 +446,11 @@ __device__ __forceinline__ void convert_tile(float4 *__restrict__ dst, int ds,
     // pair, then steps of 32 pairs
     const int bp = (bw + 1) >> 1;            // texel pairs per row
     const int n2 = bp * bh;
-    int by = lane / bp, bq = lane - by * bp;
-    const int dby = 32 / bp, dbq = 32 - dby * bp;
+    // lane / bp and 32 / bp without an integer division: (n + 0.5) / bp lies
+    // at least 0.5 / bp from an integer, far beyond the quotient's FP32 error
+    const float rbp = __fdividef(1.f, (float)bp);
+    int by = (int)(((float)lane + 0.5f) * rbp), bq = lane - by * bp;
+    const int dby = (int)(32.5f * rbp), dbq = 32 - dby * bp;
     for (int q = lane; q < n2; q += 32) {
         const int bx = 2 * bq;
         const bool two = bx + 1 < bw;
