@@ -353,9 +353,9 @@ def _cuda() -> bool:
 
 # DRAM bytes per evaluation of the window kernel measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum, a one-pass capture) on the
-# full C2 launches: 4556.3 MB / 1993.23 M evaluations (7x7), 4637.4 MB /
+# full C2 launches: 4551.3 MB / 1993.23 M evaluations (7x7), 4633.3 MB /
 # 1992.24 M (11x11).
-DRAM_BYTES_PER_EVAL = {11: 4556.3e6 / 1993.23e6, 15: 4637.4e6 / 1992.24e6}
+DRAM_BYTES_PER_EVAL = {11: 4551.3e6 / 1993.23e6, 15: 4633.3e6 / 1992.24e6}
 
 
 def traffic_per_launch(evals_step: dict, templates) -> float:
