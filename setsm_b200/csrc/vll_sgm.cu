@@ -30,6 +30,7 @@
 
 #include "vll_device.cuh"
 #include "vll_internal.h"
+#include "vll_split.h"
 
 namespace vll {
 
@@ -370,7 +371,7 @@ cudaError_t launch_sgm(const DevLevel *dP, int64_t grid_w, int64_t grid_h, int m
     int warps = (int)std::min<size_t>(4, (200 * 1024) / per_warp);
     if (warps < 1) warps = 1;
     const size_t smem = per_warp * warps;
-    e = cudaFuncSetAttribute(sgm_dir_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = ensure_smem_limit((const void *)sgm_dir_kernel, smem);
     if (e != cudaSuccess) return e;
     if (lr) {
         // every direction at once (blockIdx.y); blocks beyond a direction's

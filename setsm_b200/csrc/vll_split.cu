@@ -1866,6 +1866,8 @@ int set_max_h(const DevLevel *hl, int n) {
 
 int window_max_blocks_per_sm();
 int64_t window_scratch_floats();
+unsigned long long current_context_id();
+
 
 cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const int32_t *node_k,
                           const double *gsum, const double *gcnt, float *pend_vals,
@@ -1877,8 +1879,7 @@ cudaError_t launch_window(const DevLevel *hl, int n, const LevelSet &LS, const i
     const size_t smem = win_raw_offset(wb.quads) + (size_t)kWinWarps * wb.raw;
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaError_t e = cudaFuncSetAttribute(window_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = ensure_smem_limit((const void *)window_kernel, smem);
     if (e != cudaSuccess) return e;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1907,8 +1908,7 @@ cudaError_t launch_peaks(const LevelSet &LS, int max_h, const int32_t *node_k,
     const size_t smem = (ws + xs) * kPeakWarps;
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaError_t e = cudaFuncSetAttribute(peaks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = ensure_smem_limit((const void *)peaks_kernel, smem);
     if (e != cudaSuccess) return e;
     int sms = 148, per_sm = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1986,6 +1986,39 @@ int64_t pending_capacity(int64_t n_slots) {
 }
 
 }  // namespace
+
+// Raises `func`'s dynamic shared-memory limit to at least `bytes` in the
+// calling thread's context and never lowers it.  The limit belongs to the
+// function in the whole context, and contexts used from several threads
+// launch the same kernel with different footprints: setting each launch's
+// own size could lower the limit under another thread's larger launch
+// (which then fails as an invalid argument).  Without a context id the
+// limit is set for every launch, as a single thread needs.
+cudaError_t ensure_smem_limit(const void *func, size_t bytes) {
+    static std::mutex mu;
+    struct Seen {
+        const void *func;
+        unsigned long long ctx;
+        size_t bytes;
+    };
+    static std::vector<Seen> seen;
+    const unsigned long long ctx = current_context_id();
+    if (ctx == 0)
+        return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    std::lock_guard<std::mutex> lk(mu);
+    for (Seen &t : seen)
+        if (t.func == func && t.ctx == ctx) {
+            if (bytes <= t.bytes) return cudaSuccess;
+            const cudaError_t e =
+                cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            if (e == cudaSuccess) t.bytes = bytes;
+            return e;
+        }
+    const cudaError_t e =
+        cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) seen.push_back(Seen{func, ctx, bytes});
+    return e;
+}
 
 namespace {
 

@@ -12,6 +12,10 @@ namespace vll {
 
 struct DevLevel;
 
+// Raises a kernel's dynamic shared-memory limit in the current context to at
+// least `bytes`, never lowering it (thread-safe; see vll_split.cu).
+cudaError_t ensure_smem_limit(const void *func, size_t bytes);
+
 // Device scratch of the split pipeline, grown on demand and owned by a context.
 struct SplitBuffers {
     void *node_k = nullptr;        // int32  [N+1] slots per active node (0 = inactive)
