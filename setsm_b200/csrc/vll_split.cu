@@ -2357,24 +2357,29 @@ unsigned long long g_noalloc_ctx[256] = {};
 unsigned long long current_context_id() {
     using GetCurrent = CUresult (*)(CUcontext *);
     using GetId = CUresult (*)(CUcontext, unsigned long long *);
-    static GetCurrent get_current = nullptr;
-    static GetId get_id = nullptr;
-    static bool looked_up = false;
-    if (!looked_up) {
-        looked_up = true;
-        void *f = nullptr;
+    struct Fns {
+        GetCurrent get_current = nullptr;
+        GetId get_id = nullptr;
+    };
+    // looked up once; the initialisation of a function-local static is
+    // thread-safe (callers run on several host threads)
+    static const Fns fns = [] {
+        Fns f;
+        void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            get_current = (GetCurrent)f;
-        f = nullptr;
-        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            f.get_current = (GetCurrent)p;
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            get_id = (GetId)f;
-    }
+            f.get_id = (GetId)p;
+        return f;
+    }();
     CUcontext c = nullptr;
     unsigned long long id = 0;
-    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c) get_id(c, &id);
+    if (fns.get_current && fns.get_id && fns.get_current(&c) == CUDA_SUCCESS && c)
+        fns.get_id(c, &id);
     return id;
 }
 
