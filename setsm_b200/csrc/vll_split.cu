@@ -1954,15 +1954,15 @@ cudaError_t window_and_peaks(const DevLevel *hl, int n, const LevelSet &LS, cons
 // Most window-kernel CTAs an SM can hold whatever the footprint budget (its
 // registers bound it; the launch never exceeds it).
 int window_max_blocks_per_sm() {
-    static int cached = 0;
-    if (!cached) {
+    // computed once (thread-safe initialisation of a function-local static)
+    static const int cached = [] {
         int b = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, window_kernel, kWinWarps * 32,
                                                           win_boxes_offset()) != cudaSuccess ||
             b < 1)
             b = kWinMaxBlocksPerSm;
-        cached = std::min(b, kWinMaxBlocksPerSm);
-    }
+        return std::min(b, kWinMaxBlocksPerSm);
+    }();
     return cached;
 }
 
