@@ -822,12 +822,15 @@ __device__ __noinline__ void slot_coords_exact(const NodeCtx &N, double hgt, dou
 // computed, the footprints of the next group (of this node or the next one)
 // are already being copied into shared memory by the TMA engine.  Per group:
 //   fetch     FP64 geometry of the 32 slots (RPC cubics of the node, the
-//             reference's RPC order near integers and clamps), orientation,
-//             the boxes covering the footprints, four tile copies;
+//             reference's RPC order near integers and clamps), the loads of
+//             the orientation bytes, the boxes covering the footprints, four
+//             tile copies;
 //   stage     (a group later) conversion of the tiles to FP32 box texels,
-//             listing zero intensity texels;
-//   evaluate  FP32 window statistics of every slot whose footprint holds no
-//             zero texel, then FindPeakNcc / max_WNCC streamed over the group.
+//             two per lane step, listing zero intensity texels;
+//   evaluate  the orientation test and rotation from the bytes loaded a
+//             group earlier, FP32 window statistics of every slot whose
+//             footprint holds no zero texel, then FindPeakNcc / max_WNCC
+//             streamed over the group (the top-two fold in registers).
 // A node whose every decision lies outside the error band is written here;
 // any other node is queued for the exact pass with its FP32 values (NaN
 // marking the slots that need an exact value) in the pending buffer, or with
