@@ -9,7 +9,9 @@ CPU:
 * the box conversion takes a lane's first texel pair and its step as
   (n + 0.5) * r truncated, r an FP32 reciprocal of the pairs per row bp with
   a relative error of a few ulp (__fdividef): the quotient equals n // bp
-  for every lane n <= 31, the step n = 32, and bp up to 4096."""
+  for every lane n <= 31, the step n = 32, and bp up to 4096;
+* the target box, placed before the orientation is known, covers every
+  rotated window (radius H + 2 around the centre texel)."""
 import numpy as np
 
 
@@ -37,3 +39,30 @@ def test_fp32_reciprocal_quotients_are_exact():
             r = np.nextafter(r, np.float32(step)).astype(np.float32)
         q = np.floor((n + np.float32(0.5)) * r[None, :]).astype(np.int64)
         assert np.array_equal(q, exact), k
+
+
+def test_target_box_radius_holds_for_every_rotation():
+    """The window kernel places the target box [centre - R, centre + R + 1]
+    with R = H + 2 before it knows the rotation: every sample of a window
+    rotated by any angle (FP32 positions, as the kernel computes them) reads
+    texels floor(f) and floor(f) + 1 inside it, f the sample's position from
+    the centre texel, whatever the centre's fraction."""
+    for H in range(2, 8):
+        R = H + 2
+        rows, cols = np.meshgrid(np.arange(-H, H + 1), np.arange(-H, H + 1), indexing="ij")
+        keep = rows * rows + cols * cols <= (H + 1) * (H + 1)
+        row = rows[keep].astype(np.float32)
+        col = cols[keep].astype(np.float32)
+        ang = np.deg2rad(np.arange(0.0, 360.0, 0.25))
+        c = np.cos(ang).astype(np.float32)[:, None]
+        s = np.sin(ang).astype(np.float32)[:, None]
+        for frac in (0.0, 0.25, 0.5, 0.75, np.nextafter(np.float32(1), np.float32(0))):
+            tf = np.float32(frac)
+            # the kernel: b = (-s, c) * row + tf, then f = (c, s) * col + b
+            bx = (-s * row + tf).astype(np.float32)
+            by = (c * row + tf).astype(np.float32)
+            fx = (c * col + bx).astype(np.float32)
+            fy = (s * col + by).astype(np.float32)
+            for f in (fx, fy):
+                lo = np.floor(f)
+                assert lo.min() >= -R and lo.max() + 1 <= R + 1, (H, frac)
