@@ -11,7 +11,10 @@ CPU:
   a relative error of a few ulp (__fdividef): the quotient equals n // bp
   for every lane n <= 31, the step n = 32, and bp up to 4096;
 * the target box, placed before the orientation is known, covers every
-  rotated window (radius H + 2 around the centre texel)."""
+  rotated window (radius H + 2 around the centre texel);
+* the fold in registers equals the reference's sequential fold with its
+  re-quantisation on random peak sequences (ties and int16 extremes
+  included)."""
 import numpy as np
 
 
@@ -66,3 +69,52 @@ def test_target_box_radius_holds_for_every_rotation():
             for f in (fx, fy):
                 lo = np.floor(f)
                 assert lo.min() >= -R and lo.max() + 1 <= R + 1, (H, frac)
+
+
+def _fold_reference(state, peaks):
+    """FindPeakNcc's ordered top-two update as the reference states it: the
+    replaced maximum re-quantised through dq_result / q_result."""
+    r0, r1, r2, r3, r4 = state
+    for q, h in peaks:
+        if r4 < 10:
+            r4 += 1
+        if r0 < q:
+            t1 = r0 / 1000.0
+            t2 = r2
+            r0, r2 = q, h
+            q1 = int(c_round(np.float64(t1) * 1000.0))
+            if r1 < q1:
+                r1, r3 = q1, t2
+        elif r1 < q:
+            r1, r3 = q, h
+    return r0, r1, r2, r3, r4
+
+
+def _fold_kernel(state, peaks):
+    """The window kernel's fold in registers (no re-quantisation)."""
+    r0, r1, r2, r3, r4 = state
+    for q, h in peaks:
+        if r4 < 10:
+            r4 += 1
+        if r0 < q:
+            if r1 < r0:
+                r1, r3 = r0, r2
+            r0, r2 = q, h
+        elif r1 < q:
+            r1, r3 = q, h
+    return r0, r1, r2, r3, r4
+
+
+def test_register_fold_equals_reference_fold():
+    rng = np.random.default_rng(7)
+    for trial in range(4000):
+        n = int(rng.integers(0, 12))
+        if trial % 3 == 0:   # ties and near-ties
+            qs = rng.integers(-5, 6, size=n) + int(rng.integers(-1000, 1000))
+        else:
+            qs = rng.integers(-32768, 32768, size=n)
+        peaks = [(int(q), float(h)) for q, h in zip(qs, rng.normal(0, 100, size=n))]
+        start = (int(rng.choice([-32768, -1000, 0, 500, 32767])),
+                 int(rng.choice([-32768, -1000, 0, 400, 32767])),
+                 float(rng.normal()), float(rng.normal()), int(rng.integers(0, 11)))
+        assert _fold_kernel(start, peaks) == _fold_reference(start, peaks), (start, peaks)
